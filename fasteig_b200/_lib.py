@@ -1,0 +1,80 @@
+"""ctypes binding of the C ABI declared in include/fasteig_b200.h.
+
+The shared library is built in-tree (``python -m fasteig_b200.build``). There is
+no fallback: if the library is missing or cannot be loaded, importing this
+module raises, so no caller can silently run without the CUDA backend.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libfasteig_b200.so"
+
+if not LIB_PATH.exists():
+    raise ImportError(f"fasteig_b200: CUDA library not built ({LIB_PATH}); "
+                      "run `python -m fasteig_b200.build`")
+
+lib = C.CDLL(str(LIB_PATH))
+
+i32, i64, f64, vp, sz = C.c_int32, C.c_int64, C.c_double, C.c_void_p, C.c_size_t
+P32 = C.POINTER(C.c_int32)
+PD = C.POINTER(C.c_double)
+
+_SIGS = {
+    "fe_version": (C.c_char_p, []),
+    "fe_last_error": (C.c_char_p, []),
+    "fe_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "fe_csr_create": (C.c_int, [i64, i64, i64, vp, vp, vp, C.POINTER(vp)]),
+    "fe_csr_destroy": (C.c_int, [vp]),
+    "fe_csr_info": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]),
+    "fe_csr_copy_to_host": (C.c_int, [vp, vp, vp, vp]),
+    "fe_spmm_csr_f64": (C.c_int, [vp, vp, i64, vp, i64, i64, f64, f64, vp]),
+    "fe_spmm_csr_f32": (C.c_int, [vp, vp, i64, vp, i64, i64, f64, f64, vp]),
+    "fe_cheb_step_f64": (C.c_int, [vp, vp, vp, vp, i64, i64, f64, f64, f64, vp]),
+    "fe_cheb_step_f32": (C.c_int, [vp, vp, vp, vp, i64, i64, f64, f64, f64, vp]),
+    "fe_cheb_filter_f64": (C.c_int, [vp, vp, vp, i64, i64, i32, f64, f64, vp]),
+    "fe_cheb_filter_f32": (C.c_int, [vp, vp, vp, i64, i64, i32, f64, f64, vp]),
+    "fe_gram_workspace_bytes": (sz, [i64, i64, i64]),
+    "fe_gram_f64": (C.c_int, [vp, i64, vp, i64, i64, i64, i64, vp, i64, vp, sz, vp]),
+    "fe_gram_f32": (C.c_int, [vp, i64, vp, i64, i64, i64, i64, vp, i64, vp, sz, vp]),
+    "fe_rotate_f64": (C.c_int, [vp, i64, vp, i64, vp, i64, i64, i64, i64, f64, f64, vp]),
+    "fe_rotate_f32": (C.c_int, [vp, i64, vp, i64, vp, i64, i64, i64, i64, f64, f64, vp]),
+    "fe_residual_workspace_bytes": (sz, [i64, i64]),
+    "fe_residual_norms_f64": (C.c_int, [vp, vp, vp, i64, i64, i64, vp, vp, i64, vp, vp, vp, vp,
+                                        sz, vp]),
+    "fe_residual_norms_f32": (C.c_int, [vp, vp, vp, i64, i64, i64, vp, vp, i64, vp, vp, vp, vp,
+                                        sz, vp]),
+    "fe_column_norms_f64": (C.c_int, [vp, i64, i64, i64, vp, vp, sz, vp]),
+    "fe_column_norms_f32": (C.c_int, [vp, i64, i64, i64, vp, vp, sz, vp]),
+    "fe_potrf_upper_f64": (C.c_int, [vp, i64, i64, vp, vp]),
+    "fe_trinv_upper_f64": (C.c_int, [vp, i64, vp, i64, i64, vp]),
+    "fe_symmetrize_f64": (C.c_int, [vp, i64, i64, vp]),
+    "fe_convert_f64_to_f32": (C.c_int, [vp, i64, vp, i64, i64, i64, vp]),
+    "fe_convert_f32_to_f64": (C.c_int, [vp, i64, vp, i64, i64, i64, vp]),
+    "fe_solve": (C.c_int, [vp, vp, C.c_char_p, vp, vp, vp, vp]),
+}
+
+for _name, (_res, _args) in _SIGS.items():
+    _fn = getattr(lib, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+EXPORTED = tuple(_SIGS)
+
+
+class FastEigError(RuntimeError):
+    """A fasteig_b200 C ABI call returned a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise FastEigError(status, lib.fe_last_error().decode(errors="replace"))
+
+
+def version() -> str:
+    return lib.fe_version().decode()

@@ -1,0 +1,580 @@
+// Dense tall-skinny block kernels: Gram X^T Y, rotation X*C, Ritz residuals
+// with column norms, column norms, precision conversion.
+//
+// Replaces (src/gpu/CudaMultiVector.cpp) transpose_multiply (:361-406: Dgemm
+// T,N plus a cudaMalloc/cudaFree and a device-to-host sync per call),
+// right_multiply_active_columns (:310-359: cudaMalloc + host-to-device copy of
+// C per call, Dgemm N,N), add_scaled_columns (:409-433: one Daxpy per column)
+// and column_norms (:435-474: one Dnrm2 per column + sync).
+//
+// These SIMT kernels are the precise path: Gram products are accumulated in
+// FP64 (products of FP32 inputs are exact in FP64), split over row chunks whose
+// partial Grams are reduced in a fixed order, so results are deterministic.
+
+#include "fe_common.cuh"
+
+#include <algorithm>
+
+namespace fe {
+namespace {
+
+// ---------------------------------------------------------------- Gram ----
+constexpr int kGT = 64;    // output tile (k and m)
+constexpr int kGK = 32;    // rows per smem stage
+constexpr int kGramTargetCtas = 592;  // about four CTAs per SM on 148 SMs
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+gram_partial_kernel(const T* __restrict__ X, int64_t ldx, const T* __restrict__ Y, int64_t ldy,
+                    int64_t n, int k, int m, int64_t rows_per_chunk,
+                    double* __restrict__ partial) {
+  __shared__ double Xs[kGK][kGT + 1];
+  __shared__ double Ys[kGK][kGT + 1];
+  const int tx = threadIdx.x % 16;
+  const int ty = threadIdx.x / 16;
+  const int i0 = blockIdx.x * kGT;
+  const int j0 = blockIdx.y * kGT;
+  const int64_t r_begin = static_cast<int64_t>(blockIdx.z) * rows_per_chunk;
+  const int64_t r_end = min(n, r_begin + rows_per_chunk);
+
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+
+  for (int64_t r0 = r_begin; r0 < r_end; r0 += kGK) {
+    // 32 rows x 64 columns per operand, 8 elements per thread, coalesced along columns.
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int idx = threadIdx.x + e * 256;
+      const int rr = idx / kGT;
+      const int cc = idx % kGT;
+      const int64_t r = r0 + rr;
+      double xv = 0.0, yv = 0.0;
+      if (r < r_end) {
+        if (i0 + cc < k) xv = static_cast<double>(X[r * ldx + i0 + cc]);
+        if (j0 + cc < m) yv = static_cast<double>(Y[r * ldy + j0 + cc]);
+      }
+      Xs[rr][cc] = xv;
+      Ys[rr][cc] = yv;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int rr = 0; rr < kGK; ++rr) {
+      double xv[4], yv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) xv[a] = Xs[rr][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) yv[b] = Ys[rr][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(xv[a], yv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+  double* out = partial + static_cast<int64_t>(blockIdx.z) * k * m;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + ty + 16 * a;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int j = j0 + tx + 16 * b;
+      if (i < k && j < m) out[static_cast<int64_t>(j) * k + i] = acc[a][b];
+    }
+  }
+}
+
+__global__ void gram_reduce_kernel(const double* __restrict__ partial, int chunks, int k, int m,
+                                   double* __restrict__ G, int64_t ldg) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t total = static_cast<int64_t>(k) * m;
+  if (idx >= total) return;
+  const int i = static_cast<int>(idx % k);
+  const int j = static_cast<int>(idx / k);
+  double s = 0.0;
+  for (int c = 0; c < chunks; ++c) s += partial[static_cast<int64_t>(c) * total + idx];
+  G[static_cast<int64_t>(j) * ldg + i] = s;
+}
+
+struct GramPlan {
+  int tiles_k, tiles_m, chunks;
+  int64_t rows_per_chunk;
+  size_t bytes;
+};
+
+GramPlan gram_plan(int64_t n, int64_t k, int64_t m) {
+  GramPlan p{};
+  p.tiles_k = static_cast<int>((k + kGT - 1) / kGT);
+  p.tiles_m = static_cast<int>((m + kGT - 1) / kGT);
+  const int64_t tiles = std::max<int64_t>(1, static_cast<int64_t>(p.tiles_k) * p.tiles_m);
+  int64_t chunks = (kGramTargetCtas + tiles - 1) / tiles;
+  chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, (n + 255) / 256));
+  int64_t rpc = (n + chunks - 1) / chunks;
+  rpc = ((rpc + kGK - 1) / kGK) * kGK;
+  chunks = std::max<int64_t>(1, (n + rpc - 1) / rpc);
+  p.chunks = static_cast<int>(chunks);
+  p.rows_per_chunk = rpc;
+  p.bytes = static_cast<size_t>(chunks) * k * m * sizeof(double);
+  return p;
+}
+
+// --------------------------------------------------------------- Rotation ----
+constexpr int kRT = 64;  // rows and output columns per tile
+constexpr int kRK = 32;  // inner (k) stage
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+rotate_kernel(const T* __restrict__ X, int64_t ldx, const double* __restrict__ C, int64_t ldc,
+              T* __restrict__ Y, int64_t ldy, int64_t n, int k, int m, T alpha, T beta,
+              int use_beta) {
+  __shared__ T Xs[kRT][kRK + 1];
+  __shared__ T Cs[kRK][kRT + 1];
+  const int tx = threadIdx.x % 16;
+  const int ty = threadIdx.x / 16;
+  const int j0 = blockIdx.x * kRT;
+  const int64_t r0 = static_cast<int64_t>(blockIdx.y) * kRT;
+
+  T acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+
+  for (int k0 = 0; k0 < k; k0 += kRK) {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int idx = threadIdx.x + e * 256;
+      // X tile: 64 rows x 32 inner, coalesced along inner index.
+      const int rr = idx / kRK;
+      const int kk = idx % kRK;
+      const int64_t r = r0 + rr;
+      Xs[rr][kk] = (r < n && k0 + kk < k) ? X[r * ldx + k0 + kk] : T(0);
+      // C tile: 32 inner x 64 columns, column-major source, coalesced along inner.
+      const int cj = idx / kRK;
+      const int ck = idx % kRK;
+      Cs[ck][cj] = (k0 + ck < k && j0 + cj < m)
+                       ? static_cast<T>(C[static_cast<int64_t>(j0 + cj) * ldc + k0 + ck])
+                       : T(0);
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < kRK; ++kk) {
+      T xv[4], cv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) xv[a] = Xs[ty + 16 * a][kk];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) cv[b] = Cs[kk][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(xv[a], cv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int64_t r = r0 + ty + 16 * a;
+    if (r >= n) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int j = j0 + tx + 16 * b;
+      if (j < m) {
+        T* y = Y + r * ldy + j;
+        T v = alpha * acc[a][b];
+        if (use_beta) v = fma(beta, *y, v);
+        *y = v;
+      }
+    }
+  }
+}
+
+// -------------------------------------------------- Residual and norms ----
+constexpr int kNormCols = 32;       // columns per CTA (one per lane)
+constexpr int kNormTargetChunks = 256;
+
+// R = AX - lambda * MX, per-column sums of squares of R and MX (FP64), per chunk.
+template <typename T>
+__global__ void __launch_bounds__(256)
+residual_partial_kernel(const T* __restrict__ AX, const T* __restrict__ X,
+                        const T* __restrict__ BX, int64_t ld, int64_t n, int m,
+                        const double* __restrict__ lambda, T* __restrict__ R, int64_t ldr,
+                        int64_t rows_per_chunk, double* __restrict__ partial, int mode) {
+  // mode 0: norms of X only (column_norms); mode 1: residual.
+  __shared__ double red[2][8][kNormCols];
+  const int lane = threadIdx.x % 32;
+  const int warp = threadIdx.x / 32;
+  const int j = blockIdx.x * kNormCols + lane;
+  const int64_t r_begin = static_cast<int64_t>(blockIdx.y) * rows_per_chunk;
+  const int64_t r_end = min(n, r_begin + rows_per_chunk);
+  double sr = 0.0, sx = 0.0;
+  if (j < m) {
+    const double lam = mode ? lambda[j] : 0.0;
+    const T* M = BX ? BX : X;
+    for (int64_t r = r_begin + warp; r < r_end; r += 8) {
+      const double mx = static_cast<double>(M[r * ld + j]);
+      sx = fma(mx, mx, sx);
+      if (mode) {
+        const T rv = static_cast<T>(static_cast<double>(AX[r * ld + j]) - lam * mx);
+        if (R) R[r * ldr + j] = rv;
+        const double rd = static_cast<double>(rv);
+        sr = fma(rd, rd, sr);
+      }
+    }
+  }
+  red[0][warp][lane] = sr;
+  red[1][warp][lane] = sx;
+  __syncthreads();
+  if (warp == 0 && j < m) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      a += red[0][w][lane];
+      b += red[1][w][lane];
+    }
+    double* out = partial + static_cast<int64_t>(blockIdx.y) * 2 * m;
+    out[j] = a;
+    out[m + j] = b;
+  }
+}
+
+__global__ void residual_finish_kernel(const double* __restrict__ partial, int chunks, int m,
+                                       const double* __restrict__ lambda, double* rnorm,
+                                       double* xnorm, double* rel, int mode) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  double a = 0.0, b = 0.0;
+  for (int c = 0; c < chunks; ++c) {
+    a += partial[static_cast<int64_t>(c) * 2 * m + j];
+    b += partial[static_cast<int64_t>(c) * 2 * m + m + j];
+  }
+  const double rn = sqrt(a);
+  const double xn = sqrt(b);
+  if (mode == 0) {
+    xnorm[j] = xn;
+    return;
+  }
+  if (rnorm) rnorm[j] = rn;
+  if (xnorm) xnorm[j] = xn;
+  if (rel) {
+    const double den = (1.0 + fabs(lambda[j])) * xn;
+    rel[j] = den > 0.0 ? rn / den : rn;
+  }
+}
+
+struct NormPlan {
+  int col_blocks, chunks;
+  int64_t rows_per_chunk;
+  size_t bytes;
+};
+
+NormPlan norm_plan(int64_t n, int64_t m) {
+  NormPlan p{};
+  p.col_blocks = static_cast<int>((m + kNormCols - 1) / kNormCols);
+  int64_t chunks = std::max<int64_t>(1, kNormTargetChunks / std::max(1, p.col_blocks));
+  chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, (n + 63) / 64));
+  int64_t rpc = (n + chunks - 1) / chunks;
+  p.rows_per_chunk = std::max<int64_t>(1, rpc);
+  p.chunks = static_cast<int>((n + p.rows_per_chunk - 1) / p.rows_per_chunk);
+  if (p.chunks < 1) p.chunks = 1;
+  p.bytes = static_cast<size_t>(p.chunks) * 2 * std::max<int64_t>(m, 1) * sizeof(double);
+  return p;
+}
+
+template <typename S, typename D>
+__global__ void convert_kernel(const S* __restrict__ src, int64_t lds, D* __restrict__ dst,
+                               int64_t ldd, int64_t n, int m) {
+  const int64_t total = n * m;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = idx / m;
+    const int c = static_cast<int>(idx % m);
+    dst[r * ldd + c] = static_cast<D>(src[r * lds + c]);
+  }
+}
+
+}  // namespace
+
+size_t gram_workspace_bytes(int64_t n, int64_t k, int64_t m) {
+  if (n <= 0 || k <= 0 || m <= 0) return 0;
+  return gram_plan(n, k, m).bytes;
+}
+
+template <typename T>
+void gram(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k, int64_t m,
+          double* G, int64_t ldg, void* ws, size_t ws_bytes, cudaStream_t s) {
+  FE_REQUIRE(n >= 0 && k >= 0 && m >= 0, "gram: negative dimension");
+  FE_REQUIRE(k <= 65535 * (int64_t)kGT && m <= 65535 * (int64_t)kGT, "gram: too many columns");
+  if (k == 0 || m == 0) return;
+  FE_REQUIRE(G && ldg >= k, "gram: invalid output");
+  if (n == 0) {
+    FE_CHECK_CUDA(cudaMemset2DAsync(G, ldg * sizeof(double), 0, k * sizeof(double), m, s));
+    return;
+  }
+  FE_REQUIRE(X && Y && ldx >= k && ldy >= m, "gram: invalid input block");
+  const GramPlan p = gram_plan(n, k, m);
+  FE_REQUIRE(ws && ws_bytes >= p.bytes, "gram: workspace too small");
+  dim3 grid(p.tiles_k, p.tiles_m, p.chunks);
+  gram_partial_kernel<T><<<grid, 256, 0, s>>>(X, ldx, Y, ldy, n, static_cast<int>(k),
+                                              static_cast<int>(m), p.rows_per_chunk,
+                                              static_cast<double*>(ws));
+  check_launch("gram_partial_kernel");
+  const int64_t total = k * m;
+  gram_reduce_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
+      static_cast<const double*>(ws), p.chunks, static_cast<int>(k), static_cast<int>(m), G, ldg);
+  check_launch("gram_reduce_kernel");
+}
+
+template void gram<double>(const double*, int64_t, const double*, int64_t, int64_t, int64_t,
+                           int64_t, double*, int64_t, void*, size_t, cudaStream_t);
+template void gram<float>(const float*, int64_t, const float*, int64_t, int64_t, int64_t,
+                          int64_t, double*, int64_t, void*, size_t, cudaStream_t);
+
+template <typename T>
+void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t ldy, int64_t n,
+            int64_t k, int64_t m, double alpha, double beta, cudaStream_t s) {
+  FE_REQUIRE(n >= 0 && k >= 0 && m >= 0, "rotate: negative dimension");
+  if (n == 0 || m == 0) return;
+  FE_REQUIRE(Y && ldy >= m, "rotate: invalid output block");
+  if (k == 0) {
+    // Y = beta * Y (alpha * X * C vanishes).
+    FE_REQUIRE(beta == 0.0, "rotate: k == 0 with beta != 0 is not supported");
+    FE_CHECK_CUDA(cudaMemset2DAsync(Y, ldy * sizeof(T), 0, m * sizeof(T), n, s));
+    return;
+  }
+  FE_REQUIRE(X && C && ldx >= k && ldc >= k, "rotate: invalid input");
+  FE_REQUIRE(!ranges_overlap(X, n, ldx, k, static_cast<const T*>(Y), n, ldy, m),
+             "rotate: X and Y overlap");
+  const int64_t row_tiles = (n + kRT - 1) / kRT;
+  FE_REQUIRE(row_tiles <= 65535LL * 32768LL, "rotate: too many rows");
+  const int64_t col_tiles = (m + kRT - 1) / kRT;
+  // Column tiles run fastest so the CTAs sharing an X row tile are adjacent (L2 reuse).
+  for (int64_t base = 0; base < row_tiles; base += 65535) {
+    const int64_t tiles = std::min<int64_t>(65535, row_tiles - base);
+    dim3 grid(static_cast<unsigned>(col_tiles), static_cast<unsigned>(tiles));
+    const int64_t r_off = base * kRT;
+    rotate_kernel<T><<<grid, 256, 0, s>>>(X + r_off * ldx, ldx, C, ldc, Y + r_off * ldy, ldy,
+                                          n - r_off, static_cast<int>(k), static_cast<int>(m),
+                                          T(alpha), T(beta), beta != 0.0 ? 1 : 0);
+    check_launch("rotate_kernel");
+  }
+}
+
+template void rotate<double>(const double*, int64_t, const double*, int64_t, double*, int64_t,
+                             int64_t, int64_t, int64_t, double, double, cudaStream_t);
+template void rotate<float>(const float*, int64_t, const double*, int64_t, float*, int64_t,
+                            int64_t, int64_t, int64_t, double, double, cudaStream_t);
+
+size_t residual_workspace_bytes(int64_t n, int64_t m) {
+  if (n <= 0 || m <= 0) return 0;
+  return norm_plan(n, m).bytes;
+}
+
+template <typename T>
+void residual_norms(const T* AX, const T* X, const T* BX, int64_t ld, int64_t n, int64_t m,
+                    const double* lambda, T* R, int64_t ldr, double* rnorm, double* xnorm,
+                    double* rel, void* ws, size_t ws_bytes, cudaStream_t s, int mode) {
+  FE_REQUIRE(n >= 0 && m >= 0, "residual_norms: negative dimension");
+  if (m == 0) return;
+  FE_REQUIRE(X && ld >= m, "residual_norms: invalid block");
+  if (mode) FE_REQUIRE(AX && lambda, "residual_norms: missing AX or lambda");
+  if (R) FE_REQUIRE(ldr >= m, "residual_norms: invalid R leading dimension");
+  FE_REQUIRE(m <= 65535LL * kNormCols, "residual_norms: too many columns");
+  const NormPlan p = norm_plan(std::max<int64_t>(n, 1), m);
+  FE_REQUIRE(ws && ws_bytes >= p.bytes, "residual_norms: workspace too small");
+  if (n == 0) {
+    FE_CHECK_CUDA(cudaMemsetAsync(ws, 0, p.bytes, s));
+  } else {
+    dim3 grid(p.col_blocks, p.chunks);
+    residual_partial_kernel<T><<<grid, 256, 0, s>>>(AX, X, BX, ld, n, static_cast<int>(m), lambda,
+                                                    R, ldr, p.rows_per_chunk,
+                                                    static_cast<double*>(ws), mode);
+    check_launch("residual_partial_kernel");
+  }
+  residual_finish_kernel<<<static_cast<unsigned>((m + 127) / 128), 128, 0, s>>>(
+      static_cast<const double*>(ws), n == 0 ? 1 : p.chunks, static_cast<int>(m), lambda, rnorm,
+      xnorm, rel, mode);
+  check_launch("residual_finish_kernel");
+}
+
+template void residual_norms<double>(const double*, const double*, const double*, int64_t,
+                                     int64_t, int64_t, const double*, double*, int64_t, double*,
+                                     double*, double*, void*, size_t, cudaStream_t, int);
+template void residual_norms<float>(const float*, const float*, const float*, int64_t, int64_t,
+                                    int64_t, const double*, float*, int64_t, double*, double*,
+                                    double*, void*, size_t, cudaStream_t, int);
+
+template <typename S, typename D>
+void convert(const S* src, int64_t lds, D* dst, int64_t ldd, int64_t n, int64_t m,
+             cudaStream_t s) {
+  FE_REQUIRE(n >= 0 && m >= 0 && lds >= m && ldd >= m, "convert: invalid shape");
+  if (n == 0 || m == 0) return;
+  const int64_t total = n * m;
+  const int64_t blocks = std::min<int64_t>((total + 255) / 256, 148 * 32);
+  convert_kernel<S, D><<<static_cast<unsigned>(blocks), 256, 0, s>>>(src, lds, dst, ldd, n,
+                                                                     static_cast<int>(m));
+  check_launch("convert_kernel");
+}
+
+template void convert<double, float>(const double*, int64_t, float*, int64_t, int64_t, int64_t,
+                                     cudaStream_t);
+template void convert<float, double>(const float*, int64_t, double*, int64_t, int64_t, int64_t,
+                                     cudaStream_t);
+template void convert<double, double>(const double*, int64_t, double*, int64_t, int64_t,
+                                      int64_t, cudaStream_t);
+template void convert<float, float>(const float*, int64_t, float*, int64_t, int64_t, int64_t,
+                                    cudaStream_t);
+
+}  // namespace fe
+
+using fe::guarded;
+
+extern "C" size_t fe_gram_workspace_bytes(int64_t n, int64_t k, int64_t m) {
+  return fe::gram_workspace_bytes(n, k, m);
+}
+
+extern "C" int fe_gram_f64(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t n,
+                           int64_t k, int64_t m, double* G, int64_t ldg, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  return guarded("fe_gram_f64", [&] {
+    fe::gram<double>(X, ldx, Y, ldy, n, k, m, G, ldg, workspace, workspace_bytes,
+                     fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_gram_f32(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n,
+                           int64_t k, int64_t m, double* G, int64_t ldg, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  return guarded("fe_gram_f32", [&] {
+    fe::gram<float>(X, ldx, Y, ldy, n, k, m, G, ldg, workspace, workspace_bytes,
+                    fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_rotate_f64(const double* X, int64_t ldx, const double* C, int64_t ldc,
+                             double* Y, int64_t ldy, int64_t n, int64_t k, int64_t m,
+                             double alpha, double beta, void* stream) {
+  return guarded("fe_rotate_f64", [&] {
+    fe::rotate<double>(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_rotate_f32(const float* X, int64_t ldx, const double* C, int64_t ldc, float* Y,
+                             int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha,
+                             double beta, void* stream) {
+  return guarded("fe_rotate_f32", [&] {
+    fe::rotate<float>(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, fe::as_stream(stream));
+  });
+}
+
+extern "C" size_t fe_residual_workspace_bytes(int64_t n, int64_t m) {
+  return fe::residual_workspace_bytes(n, m);
+}
+
+extern "C" int fe_residual_norms_f64(const double* AX, const double* X, const double* BX,
+                                     int64_t ld, int64_t n, int64_t m, const double* lambda,
+                                     double* R, int64_t ldr, double* rnorm, double* xnorm,
+                                     double* rel, void* workspace, size_t workspace_bytes,
+                                     void* stream) {
+  return guarded("fe_residual_norms_f64", [&] {
+    fe::residual_norms<double>(AX, X, BX, ld, n, m, lambda, R, ldr, rnorm, xnorm, rel, workspace,
+                               workspace_bytes, fe::as_stream(stream), 1);
+  });
+}
+
+extern "C" int fe_residual_norms_f32(const float* AX, const float* X, const float* BX,
+                                     int64_t ld, int64_t n, int64_t m, const double* lambda,
+                                     float* R, int64_t ldr, double* rnorm, double* xnorm,
+                                     double* rel, void* workspace, size_t workspace_bytes,
+                                     void* stream) {
+  return guarded("fe_residual_norms_f32", [&] {
+    fe::residual_norms<float>(AX, X, BX, ld, n, m, lambda, R, ldr, rnorm, xnorm, rel, workspace,
+                              workspace_bytes, fe::as_stream(stream), 1);
+  });
+}
+
+extern "C" int fe_column_norms_f64(const double* X, int64_t ld, int64_t n, int64_t m,
+                                   double* norms, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+  return guarded("fe_column_norms_f64", [&] {
+    fe::residual_norms<double>(nullptr, X, nullptr, ld, n, m, nullptr, nullptr, 0, nullptr, norms,
+                               nullptr, workspace, workspace_bytes, fe::as_stream(stream), 0);
+  });
+}
+
+extern "C" int fe_column_norms_f32(const float* X, int64_t ld, int64_t n, int64_t m,
+                                   double* norms, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+  return guarded("fe_column_norms_f32", [&] {
+    fe::residual_norms<float>(nullptr, X, nullptr, ld, n, m, nullptr, nullptr, 0, nullptr, norms,
+                              nullptr, workspace, workspace_bytes, fe::as_stream(stream), 0);
+  });
+}
+
+extern "C" int fe_convert_f64_to_f32(const double* src, int64_t lds, float* dst, int64_t ldd,
+                                     int64_t n, int64_t m, void* stream) {
+  return guarded("fe_convert_f64_to_f32", [&] {
+    fe::convert<double, float>(src, lds, dst, ldd, n, m, fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ldd,
+                                     int64_t n, int64_t m, void* stream) {
+  return guarded("fe_convert_f32_to_f64", [&] {
+    fe::convert<float, double>(src, lds, dst, ldd, n, m, fe::as_stream(stream));
+  });
+}
+
+// ------------------------------------------------------------ vectors ----
+namespace fe {
+namespace {
+
+// y = a*x + b*y on strided vectors (b == 0 overwrites).
+__global__ void vec_axpby_kernel(int64_t n, double a, const double* __restrict__ x, int64_t incx,
+                                 double b, double* y, int64_t incy) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double v = a * x[i * incx];
+    y[i * incy] = (b == 0.0) ? v : fma(b, y[i * incy], v);
+  }
+}
+
+// Counter-based uniform(-1,1) fill (splitmix64 of seed and element index).
+template <typename T>
+__global__ void fill_uniform_kernel(T* X, int64_t ld, int64_t n, int m, uint64_t seed) {
+  const int64_t total = n * m;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = idx / m;
+    const int c = static_cast<int>(idx % m);
+    uint64_t z = seed * 0x9E3779B97F4A7C15ull + static_cast<uint64_t>(c) * n + r + 1;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = static_cast<double>(z >> 11) * (1.0 / 9007199254740992.0);
+    X[r * ld + c] = static_cast<T>(2.0 * u - 1.0);
+  }
+}
+
+}  // namespace
+
+void vec_axpby(int64_t n, double a, const double* x, int64_t incx, double b, double* y,
+               int64_t incy, cudaStream_t s) {
+  if (n <= 0) return;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 16);
+  vec_axpby_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(n, a, x, incx, b, y, incy);
+  check_launch("vec_axpby_kernel");
+}
+
+template <typename T>
+void fill_uniform(T* X, int64_t ld, int64_t n, int64_t m, uint64_t seed, cudaStream_t s) {
+  if (n <= 0 || m <= 0) return;
+  const int64_t blocks = std::min<int64_t>((n * m + 255) / 256, 148 * 32);
+  fill_uniform_kernel<T><<<static_cast<unsigned>(blocks), 256, 0, s>>>(X, ld, n,
+                                                                       static_cast<int>(m), seed);
+  check_launch("fill_uniform_kernel");
+}
+template void fill_uniform<double>(double*, int64_t, int64_t, int64_t, uint64_t, cudaStream_t);
+template void fill_uniform<float>(float*, int64_t, int64_t, int64_t, uint64_t, cudaStream_t);
+
+}  // namespace fe

@@ -1,0 +1,290 @@
+// Small FP64 dense kernels that keep the k-by-k steps of Cholesky QR on the
+// device: upper Cholesky factorization with a device-side rank-loss flag,
+// triangular inverse, symmetrization. Also the CSR object, error reporting and
+// library identity of the C ABI.
+//
+// Replaces cusolverDnDpotrf + the info device-to-host copy + stream sync and
+// the cublasDtrsm of cuda_cholesky_qr_in_place (src/core/Orthogonalization.cpp:
+// 185-246). The reference's rank-loss return (-1 when potrf reports info > 0,
+// :224) becomes a device int that the host reads together with the other
+// per-iteration scalars.
+
+#include "fe_common.cuh"
+
+#include <cmath>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace fe {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+int num_sms() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
+  return sms > 0 ? sms : 148;
+}
+
+namespace {
+
+// Right-looking unblocked Cholesky in one CTA. G is column-major (ldg); on
+// return its upper triangle holds R (G = R^T R) and the strict lower part is 0.
+__global__ void __launch_bounds__(1024)
+potrf_upper_kernel(double* G, int k, int64_t ldg, int32_t* info) {
+  __shared__ double inv_pivot;
+  __shared__ int failed;
+  if (threadIdx.x == 0) failed = 0;
+  __syncthreads();
+  for (int j = 0; j < k; ++j) {
+    if (threadIdx.x == 0) {
+      const double d = G[static_cast<int64_t>(j) * ldg + j];
+      if (!(d > 0.0) || !isfinite(d)) {
+        failed = j + 1;
+      } else {
+        const double r = sqrt(d);
+        G[static_cast<int64_t>(j) * ldg + j] = r;
+        inv_pivot = 1.0 / r;
+      }
+    }
+    __syncthreads();
+    if (failed) break;
+    // Row j of R: R[j][c] = G[j][c] / r_jj for c > j.
+    for (int c = j + 1 + threadIdx.x; c < k; c += blockDim.x) {
+      G[static_cast<int64_t>(c) * ldg + j] *= inv_pivot;
+    }
+    __syncthreads();
+    // Trailing update of the upper triangle: G[a][c] -= R[j][a] R[j][c], j < a <= c.
+    const int t = k - j - 1;
+    const int64_t count = static_cast<int64_t>(t) * (t + 1) / 2;
+    for (int64_t idx = threadIdx.x; idx < count; idx += blockDim.x) {
+      // Map idx to (a, c) with a <= c in the trailing t-by-t triangle, column-wise:
+      // column cc holds rows 0..cc, offset cc*(cc+1)/2.
+      int cc = static_cast<int>((sqrt(8.0 * static_cast<double>(idx) + 1.0) - 1.0) * 0.5);
+      while (static_cast<int64_t>(cc + 1) * (cc + 2) / 2 <= idx) ++cc;
+      while (static_cast<int64_t>(cc) * (cc + 1) / 2 > idx) --cc;
+      const int aa = static_cast<int>(idx - static_cast<int64_t>(cc) * (cc + 1) / 2);
+      const int a = j + 1 + aa;
+      const int c = j + 1 + cc;
+      G[static_cast<int64_t>(c) * ldg + a] -=
+          G[static_cast<int64_t>(a) * ldg + j] * G[static_cast<int64_t>(c) * ldg + j];
+    }
+    __syncthreads();
+  }
+  // Zero the strict lower triangle.
+  for (int64_t idx = threadIdx.x; idx < static_cast<int64_t>(k) * k; idx += blockDim.x) {
+    const int r = static_cast<int>(idx % k);
+    const int c = static_cast<int>(idx / k);
+    if (r > c) G[static_cast<int64_t>(c) * ldg + r] = 0.0;
+  }
+  if (threadIdx.x == 0 && info) *info = failed;
+}
+
+// One warp per column c of Rinv: back substitution R x = e_c.
+__global__ void trinv_upper_kernel(const double* __restrict__ R, int64_t ldr,
+                                   double* __restrict__ Rinv, int64_t ldi, int k) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  const int lane = threadIdx.x % 32;
+  if (warp >= k) return;
+  const int c = warp;
+  double* x = Rinv + static_cast<int64_t>(c) * ldi;
+  for (int i = lane; i < k; i += 32) x[i] = 0.0;
+  __syncwarp();
+  if (lane == 0) x[c] = 1.0 / R[static_cast<int64_t>(c) * ldr + c];
+  __syncwarp();
+  for (int i = c - 1; i >= 0; --i) {
+    double s = 0.0;
+    for (int l = i + 1 + lane; l <= c; l += 32) s += R[static_cast<int64_t>(l) * ldr + i] * x[l];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) x[i] = -s / R[static_cast<int64_t>(i) * ldr + i];
+    __syncwarp();
+  }
+}
+
+__global__ void symmetrize_kernel(double* P, int k, int64_t ldp) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<int64_t>(k) * k) return;
+  const int r = static_cast<int>(idx % k);
+  const int c = static_cast<int>(idx / k);
+  if (r >= c) return;
+  const double a = P[static_cast<int64_t>(c) * ldp + r];
+  const double b = P[static_cast<int64_t>(r) * ldp + c];
+  const double s = 0.5 * (a + b);
+  P[static_cast<int64_t>(c) * ldp + r] = s;
+  P[static_cast<int64_t>(r) * ldp + c] = s;
+}
+
+}  // namespace
+
+void potrf_upper(double* G, int64_t k, int64_t ldg, int32_t* info, cudaStream_t s) {
+  FE_REQUIRE(k >= 0 && k <= 16384 && ldg >= k, "potrf_upper: invalid shape");
+  if (k == 0) {
+    if (info) FE_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int32_t), s));
+    return;
+  }
+  potrf_upper_kernel<<<1, 1024, 0, s>>>(G, static_cast<int>(k), ldg, info);
+  check_launch("potrf_upper_kernel");
+}
+
+void trinv_upper(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
+                 cudaStream_t s) {
+  FE_REQUIRE(k >= 0 && ldr >= k && ldi >= k, "trinv_upper: invalid shape");
+  if (k == 0) return;
+  FE_REQUIRE(R != Rinv, "trinv_upper: in-place inverse is not supported");
+  const int64_t threads = k * 32;
+  trinv_upper_kernel<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, s>>>(
+      R, ldr, Rinv, ldi, static_cast<int>(k));
+  check_launch("trinv_upper_kernel");
+}
+
+void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s) {
+  FE_REQUIRE(k >= 0 && ldp >= k, "symmetrize: invalid shape");
+  if (k == 0) return;
+  const int64_t total = k * k;
+  symmetrize_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
+      P, static_cast<int>(k), ldp);
+  check_launch("symmetrize_kernel");
+}
+
+// ------------------------------------------------------------------ CSR ----
+Csr* csr_create(int64_t rows, int64_t cols, int64_t nnz, const int32_t* rowptr,
+                const int32_t* colind, const double* values) {
+  // validate_csr_matrix_data (src/core/CsrMatrix.cpp:11-39)
+  FE_REQUIRE(rows >= 0 && cols >= 0, "CsrMatrixData: dimensions must be nonnegative.");
+  FE_REQUIRE(rows < 0x7fffffffLL && cols < 0x7fffffffLL, "CsrMatrixData: dimensions exceed int32.");
+  FE_REQUIRE(nnz >= 0 && nnz <= 0x7fffffffLL, "CsrMatrixData: nnz exceeds int32.");
+  FE_REQUIRE(rowptr != nullptr, "CsrMatrixData: rowptr size must be rows + 1.");
+  FE_REQUIRE(nnz == 0 || (colind && values), "CsrMatrixData: colind and values sizes differ.");
+  FE_REQUIRE(rowptr[0] == 0, "CsrMatrixData: rowptr must start at zero.");
+  FE_REQUIRE(rowptr[rows] == nnz, "CsrMatrixData: rowptr end must equal nnz.");
+  for (int64_t i = 1; i <= rows; ++i) {
+    FE_REQUIRE(rowptr[i] >= rowptr[i - 1], "CsrMatrixData: rowptr must be nondecreasing.");
+  }
+  for (int64_t e = 0; e < nnz; ++e) {
+    FE_REQUIRE(colind[e] >= 0 && colind[e] < cols, "CsrMatrixData: column index out of range.");
+  }
+  auto* A = new Csr();
+  A->rows = rows;
+  A->cols = cols;
+  A->nnz = nnz;
+  FE_CHECK_CUDA(cudaGetDevice(&A->device));
+  try {
+    FE_CHECK_CUDA(cudaMalloc(&A->rowptr, (rows + 1) * sizeof(int32_t)));
+    FE_CHECK_CUDA(cudaMalloc(&A->colind, std::max<int64_t>(nnz, 1) * sizeof(int32_t)));
+    FE_CHECK_CUDA(cudaMalloc(&A->val64, std::max<int64_t>(nnz, 1) * sizeof(double)));
+    FE_CHECK_CUDA(cudaMalloc(&A->val32, std::max<int64_t>(nnz, 1) * sizeof(float)));
+    FE_CHECK_CUDA(cudaMemcpy(A->rowptr, rowptr, (rows + 1) * sizeof(int32_t),
+                             cudaMemcpyHostToDevice));
+    if (nnz > 0) {
+      FE_CHECK_CUDA(cudaMemcpy(A->colind, colind, nnz * sizeof(int32_t), cudaMemcpyHostToDevice));
+      FE_CHECK_CUDA(cudaMemcpy(A->val64, values, nnz * sizeof(double), cudaMemcpyHostToDevice));
+      std::vector<float> v32(values, values + nnz);
+      FE_CHECK_CUDA(cudaMemcpy(A->val32, v32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice));
+    }
+  } catch (...) {
+    cudaFree(A->rowptr);
+    cudaFree(A->colind);
+    cudaFree(A->val64);
+    cudaFree(A->val32);
+    delete A;
+    throw;
+  }
+  return A;
+}
+
+void csr_destroy(Csr* A) {
+  if (!A) return;
+  cudaFree(A->rowptr);
+  cudaFree(A->colind);
+  cudaFree(A->val64);
+  cudaFree(A->val32);
+  delete A;
+}
+
+}  // namespace fe
+
+using fe::guarded;
+
+extern "C" const char* fe_version(void) { return "fasteig_b200 0.1.0 (sm_100a)"; }
+
+extern "C" const char* fe_last_error(void) { return fe::g_last_error.c_str(); }
+
+extern "C" int fe_device_count(int* count) {
+  return guarded("fe_device_count", [&] {
+    FE_REQUIRE(count, "null count");
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      c = 0;
+    }
+    *count = c;
+  });
+}
+
+extern "C" int fe_csr_create(int64_t rows, int64_t cols, int64_t nnz, const int32_t* rowptr,
+                             const int32_t* colind, const double* values, fe_csr_t* out) {
+  return guarded("fe_csr_create", [&] {
+    FE_REQUIRE(out, "null output handle");
+    *out = nullptr;
+    fe::Csr* A = fe::csr_create(rows, cols, nnz, rowptr, colind, values);
+    auto* h = new fe_csr();
+    h->m = *A;
+    delete A;  // ownership of the device arrays moves to the handle
+    *out = h;
+  });
+}
+
+extern "C" int fe_csr_destroy(fe_csr_t csr) {
+  return guarded("fe_csr_destroy", [&] {
+    if (!csr) return;
+    auto* A = new fe::Csr(csr->m);
+    fe::csr_destroy(A);
+    delete csr;
+  });
+}
+
+extern "C" int fe_csr_info(fe_csr_t csr, int64_t* rows, int64_t* cols, int64_t* nnz) {
+  return guarded("fe_csr_info", [&] {
+    FE_REQUIRE(csr, "null CSR handle");
+    if (rows) *rows = csr->m.rows;
+    if (cols) *cols = csr->m.cols;
+    if (nnz) *nnz = csr->m.nnz;
+  });
+}
+
+extern "C" int fe_csr_copy_to_host(fe_csr_t csr, int32_t* rowptr, int32_t* colind,
+                                   double* values) {
+  return guarded("fe_csr_copy_to_host", [&] {
+    FE_REQUIRE(csr && rowptr && (csr->m.nnz == 0 || (colind && values)), "null argument");
+    const fe::Csr& A = csr->m;
+    FE_CHECK_CUDA(cudaMemcpy(rowptr, A.rowptr, (A.rows + 1) * sizeof(int32_t),
+                             cudaMemcpyDeviceToHost));
+    if (A.nnz > 0) {
+      FE_CHECK_CUDA(cudaMemcpy(colind, A.colind, A.nnz * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      FE_CHECK_CUDA(cudaMemcpy(values, A.val64, A.nnz * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+  });
+}
+
+extern "C" int fe_potrf_upper_f64(double* G, int64_t k, int64_t ldg, int32_t* info,
+                                  void* stream) {
+  return guarded("fe_potrf_upper_f64",
+                 [&] { fe::potrf_upper(G, k, ldg, info, fe::as_stream(stream)); });
+}
+
+extern "C" int fe_trinv_upper_f64(const double* R, int64_t ldr, double* Rinv, int64_t ldi,
+                                  int64_t k, void* stream) {
+  return guarded("fe_trinv_upper_f64",
+                 [&] { fe::trinv_upper(R, ldr, Rinv, ldi, k, fe::as_stream(stream)); });
+}
+
+extern "C" int fe_symmetrize_f64(double* P, int64_t k, int64_t ldp, void* stream) {
+  return guarded("fe_symmetrize_f64", [&] { fe::symmetrize(P, k, ldp, fe::as_stream(stream)); });
+}

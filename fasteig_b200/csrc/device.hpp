@@ -1,0 +1,175 @@
+// Host-side helpers of the B200 backend: device buffers, row-major block views,
+// the kernel entry points shared across translation units, and small host
+// dense routines (symmetric Jacobi eigensolver for the Lanczos tridiagonal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "fe_common.cuh"
+
+namespace fe {
+
+// ---- kernels (defined in spmm.cu / blocks.cu / dense.cu) -----------------
+template <typename T>
+void csr_spmm(const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T* Z, int64_t ldz,
+              int64_t ncols, double alpha, double gamma, double beta, cudaStream_t s);
+template <typename T>
+void cheb_filter(const Csr& A, T* X, T* scratch, int64_t ld, int64_t ncols, int degree, double c,
+                 double d, cudaStream_t s);
+size_t gram_workspace_bytes(int64_t n, int64_t k, int64_t m);
+template <typename T>
+void gram(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k, int64_t m,
+          double* G, int64_t ldg, void* ws, size_t ws_bytes, cudaStream_t s);
+template <typename T>
+void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t ldy, int64_t n,
+            int64_t k, int64_t m, double alpha, double beta, cudaStream_t s);
+size_t residual_workspace_bytes(int64_t n, int64_t m);
+template <typename T>
+void residual_norms(const T* AX, const T* X, const T* BX, int64_t ld, int64_t n, int64_t m,
+                    const double* lambda, T* R, int64_t ldr, double* rnorm, double* xnorm,
+                    double* rel, void* ws, size_t ws_bytes, cudaStream_t s, int mode);
+template <typename S, typename D>
+void convert(const S* src, int64_t lds, D* dst, int64_t ldd, int64_t n, int64_t m, cudaStream_t s);
+void potrf_upper(double* G, int64_t k, int64_t ldg, int32_t* info, cudaStream_t s);
+void trinv_upper(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
+                 cudaStream_t s);
+void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s);
+
+// ---- owning device buffer --------------------------------------------------
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(size_t bytes) { resize(bytes); }
+  ~DeviceBuffer() { release(); }
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), bytes_(o.bytes_) {
+    o.p_ = nullptr;
+    o.bytes_ = 0;
+  }
+  DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+    if (this != &o) {
+      release();
+      p_ = o.p_;
+      bytes_ = o.bytes_;
+      o.p_ = nullptr;
+      o.bytes_ = 0;
+    }
+    return *this;
+  }
+  void resize(size_t bytes) {
+    if (bytes <= bytes_ && p_) return;
+    release();
+    if (bytes == 0) return;
+    cudaError_t e = cudaMalloc(&p_, bytes);
+    if (e != cudaSuccess) {
+      p_ = nullptr;
+      throw Error(FE_ERR_ALLOC, std::string("cudaMalloc(") + std::to_string(bytes) +
+                                    ") failed: " + cudaGetErrorString(e));
+    }
+    bytes_ = bytes;
+  }
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    bytes_ = 0;
+  }
+  void* get() const { return p_; }
+  size_t bytes() const { return bytes_; }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p_);
+  }
+
+ private:
+  void* p_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+// Row-major n-by-cols block with leading dimension ld (padded to 8 elements so
+// every row starts 16-byte aligned for vector loads and TMA tiles).
+template <typename T>
+struct Block {
+  DeviceBuffer buf;
+  int64_t n = 0, cols = 0, ld = 0;
+  void allocate(int64_t rows, int64_t c) {
+    n = rows;
+    cols = c;
+    ld = std::max<int64_t>(8, ((c + 7) / 8) * 8);
+    buf.resize(static_cast<size_t>(n) * ld * sizeof(T));
+  }
+  T* data() const { return buf.as<T>(); }
+  T* col(int64_t j) const { return buf.as<T>() + j; }
+};
+
+// ---- host small dense -----------------------------------------------------
+// Cyclic Jacobi eigensolver for a small symmetric matrix (column-major m-by-m).
+// Returns ascending eigenvalues; Z (column-major) holds the eigenvectors.
+inline void host_symmetric_eig(std::vector<double> A, int m, std::vector<double>& w,
+                               std::vector<double>& Z) {
+  Z.assign(static_cast<size_t>(m) * m, 0.0);
+  for (int i = 0; i < m; ++i) Z[static_cast<size_t>(i) * m + i] = 1.0;
+  auto a = [&](int r, int c) -> double& { return A[static_cast<size_t>(c) * m + r]; };
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int c = 0; c < m; ++c)
+      for (int r = 0; r < m; ++r) (r == c ? diag : off) += a(r, c) * a(r, c);
+    if (off <= 1e-30 * std::max(diag, 1e-300)) break;
+    for (int p = 0; p < m - 1; ++p) {
+      for (int q = p + 1; q < m; ++q) {
+        const double apq = a(p, q);
+        if (apq == 0.0) continue;
+        const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) /
+                         (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0);
+        const double s = t * c;
+        for (int k = 0; k < m; ++k) {  // columns p, q
+          const double akp = a(k, p), akq = a(k, q);
+          a(k, p) = c * akp - s * akq;
+          a(k, q) = s * akp + c * akq;
+        }
+        for (int k = 0; k < m; ++k) {  // rows p, q
+          const double apk = a(p, k), aqk = a(q, k);
+          a(p, k) = c * apk - s * aqk;
+          a(q, k) = s * apk + c * aqk;
+        }
+        for (int k = 0; k < m; ++k) {
+          double& zp = Z[static_cast<size_t>(p) * m + k];
+          double& zq = Z[static_cast<size_t>(q) * m + k];
+          const double zkp = zp, zkq = zq;
+          zp = c * zkp - s * zkq;
+          zq = s * zkp + c * zkq;
+        }
+      }
+    }
+  }
+  std::vector<int> order(m);
+  for (int i = 0; i < m; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return a(x, x) < a(y, y); });
+  w.resize(m);
+  std::vector<double> Zs(static_cast<size_t>(m) * m);
+  for (int j = 0; j < m; ++j) {
+    w[j] = a(order[j], order[j]);
+    std::memcpy(&Zs[static_cast<size_t>(j) * m], &Z[static_cast<size_t>(order[j]) * m],
+                sizeof(double) * m);
+  }
+  Z.swap(Zs);
+}
+
+}  // namespace fe
+
+namespace fe {
+void vec_axpby(int64_t n, double a, const double* x, int64_t incx, double b, double* y,
+               int64_t incy, cudaStream_t s);
+template <typename T>
+void fill_uniform(T* X, int64_t ld, int64_t n, int64_t m, uint64_t seed, cudaStream_t s);
+}  // namespace fe

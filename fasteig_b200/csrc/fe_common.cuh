@@ -1,0 +1,105 @@
+// Shared helpers for the fasteig_b200 CUDA backend (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/fasteig_b200.h"
+
+namespace fe {
+
+// Thread-local message behind fe_last_error().
+void set_last_error(const std::string& msg);
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define FE_CHECK_CUDA(call)                                                        \
+  do {                                                                             \
+    cudaError_t fe_err_ = (call);                                                  \
+    if (fe_err_ != cudaSuccess) {                                                  \
+      throw ::fe::Error(FE_ERR_CUDA, std::string(#call) + " failed: " +            \
+                                         cudaGetErrorString(fe_err_) + " @" +      \
+                                         __FILE__ + ":" + std::to_string(__LINE__)); \
+    }                                                                              \
+  } while (0)
+
+#define FE_REQUIRE(cond, msg)                                   \
+  do {                                                          \
+    if (!(cond)) throw ::fe::Error(FE_ERR_INVALID, (msg));       \
+  } while (0)
+
+// Run `body` converting exceptions into C status codes.
+template <typename F>
+int guarded(const char* where, F&& body) {
+  try {
+    body();
+    return FE_OK;
+  } catch (const Error& e) {
+    set_last_error(std::string(where) + ": " + e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_last_error(std::string(where) + ": host allocation failed");
+    return FE_ERR_ALLOC;
+  } catch (const std::exception& e) {
+    set_last_error(std::string(where) + ": " + e.what());
+    return FE_ERR_INVALID;
+  }
+}
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline void check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    throw Error(FE_ERR_CUDA, std::string(what) + " launch failed: " + cudaGetErrorString(e));
+  }
+}
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Do two row-major views (rows x cols, leading dimension ld) share an element?
+// Views of the same buffer with equal ld and disjoint column ranges do not.
+template <typename T>
+inline bool ranges_overlap(const T* a, int64_t rows_a, int64_t ld_a, int64_t cols_a,
+                           const T* b, int64_t rows_b, int64_t ld_b, int64_t cols_b) {
+  if (rows_a <= 0 || rows_b <= 0 || cols_a <= 0 || cols_b <= 0) return false;
+  const char* a0 = reinterpret_cast<const char*>(a);
+  const char* a1 = reinterpret_cast<const char*>(a + (rows_a - 1) * ld_a + cols_a);
+  const char* b0 = reinterpret_cast<const char*>(b);
+  const char* b1 = reinterpret_cast<const char*>(b + (rows_b - 1) * ld_b + cols_b);
+  if (!(a0 < b1 && b0 < a1)) return false;
+  if (ld_a == ld_b && cols_a <= ld_a && cols_b <= ld_b) {
+    const int64_t d = b - a;  // element offset of b relative to a
+    int64_t r = d % ld_a;
+    if (r < 0) r += ld_a;
+    // b's columns relative to a's row grid: [r, r+cols_b), possibly wrapping.
+    const bool hit = (r < cols_a) || (r + cols_b > ld_a && r + cols_b - ld_a > 0);
+    return hit;
+  }
+  return true;
+}
+
+// Device CSR operator: int32 indices, FP64 and FP32 values.
+struct Csr {
+  int64_t rows = 0, cols = 0, nnz = 0;
+  int32_t* rowptr = nullptr;
+  int32_t* colind = nullptr;
+  double* val64 = nullptr;
+  float* val32 = nullptr;
+  int device = 0;
+};
+
+int num_sms();
+
+}  // namespace fe
+
+struct fe_csr {
+  fe::Csr m;
+};

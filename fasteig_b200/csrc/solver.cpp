@@ -1,0 +1,647 @@
+// Device-resident solver drivers of the B200 backend.
+//
+// The reference runs each solver against its executor abstraction
+// (include/core/Executor.hpp:22-47) with host-synchronous orchestration: every
+// transpose_multiply, column_norms, potrf info and projected eigensolve returns
+// to the host (src/gpu/CudaMultiVector.cpp:389-405,455-473;
+// src/core/Orthogonalization.cpp:211-243). Here all n-by-block state stays in
+// HBM; per iteration only the k Ritz values, k relative residuals and the
+// Cholesky status word come back to the host, which is what the locking and
+// convergence logic of the reference needs.
+//
+// Chebyshev follows ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221).
+// Precision: "fp64" runs every block in FP64 (the plain path); "mixed" runs the
+// filter, SpMMs and rotations on FP32 blocks with FP64-accumulated Grams, FP64
+// Cholesky (two passes: CholQR2) and an FP64 projected eigensolve, then
+// switches the block to FP64 for the final sweeps once the FP32 residual floor
+// is reached.
+
+#include <cusolverDn.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <random>
+#include <sstream>
+
+#include "device.hpp"
+
+namespace fe {
+namespace {
+
+#define FE_CHECK_SOLVER(call)                                                               \
+  do {                                                                                      \
+    cusolverStatus_t st_ = (call);                                                          \
+    if (st_ != CUSOLVER_STATUS_SUCCESS) {                                                   \
+      throw ::fe::Error(FE_ERR_CUDA, std::string(#call) + " failed: status " +              \
+                                         std::to_string(static_cast<int>(st_)));            \
+    }                                                                                       \
+  } while (0)
+
+std::string lower(std::string s) {
+  for (auto& c : s) c = static_cast<char>(std::tolower(static_cast<unsigned char>(c)));
+  return s;
+}
+
+// Options with the reference's keys and defaults (include/fasteig_options.hpp:102-118),
+// plus this backend's extensions.
+struct Options {
+  std::string solver = "chebyshev";
+  std::string which = "sr";
+  int64_t nev = 10;
+  int64_t maxiter = 1000;
+  int64_t maxdim = 0;
+  int64_t maxblks = 10;
+  int64_t degree = 10;
+  int64_t blksize = 1;
+  double tol = 1.0e-8;
+  bool has_seed = false;
+  unsigned seed = 1;
+  int verbosity = 0;
+  // extensions
+  std::string precision = "fp64";  // fp64 | mixed
+  int64_t block = 0;               // Chebyshev subspace capacity override (0 = reference rule)
+  std::string bounds = "reference";  // reference | ritz
+  double amplification = 1.0e3;    // filter amplification cap at the lower bound
+  std::string init = "host";       // host (std::mt19937, bit-exact) | device
+  double mixed_switch = 2.0e-6;    // FP32 -> FP64 switch when max residual <= this
+
+  void parse(const char* text) {
+    if (!text) return;
+    std::string s(text);
+    for (auto& c : s)
+      if (c == ';' || c == ',') c = '\n';
+    std::istringstream in(s);
+    std::string line;
+    while (std::getline(in, line)) {
+      auto eq = line.find('=');
+      if (eq == std::string::npos) {
+        // also accept "key value" deck lines
+        std::istringstream ls(line);
+        std::string k, v;
+        if (!(ls >> k)) continue;
+        if (!(ls >> v)) throw Error(FE_ERR_INVALID, "option without value: " + k);
+        set(lower(k), v);
+        continue;
+      }
+      auto trim = [](std::string x) {
+        const auto b = x.find_first_not_of(" \t\r");
+        const auto e = x.find_last_not_of(" \t\r");
+        return b == std::string::npos ? std::string() : x.substr(b, e - b + 1);
+      };
+      const std::string k = lower(trim(line.substr(0, eq)));
+      const std::string v = trim(line.substr(eq + 1));
+      if (k.empty()) continue;
+      set(k, v);
+    }
+  }
+
+  void set(const std::string& k, const std::string& v) {
+    auto as_int = [&](const std::string& x) {
+      size_t pos = 0;
+      const long long r = std::stoll(x, &pos);
+      if (pos != x.size()) throw Error(FE_ERR_INVALID, "invalid integer for " + k + ": " + x);
+      return static_cast<int64_t>(r);
+    };
+    auto as_double = [&](const std::string& x) {
+      size_t pos = 0;
+      const double r = std::stod(x, &pos);
+      if (pos != x.size()) throw Error(FE_ERR_INVALID, "invalid number for " + k + ": " + x);
+      return r;
+    };
+    if (k == "solver") solver = lower(v);
+    else if (k == "which") which = lower(v);
+    else if (k == "nev") nev = as_int(v);
+    else if (k == "maxiter") maxiter = as_int(v);
+    else if (k == "maxdim") maxdim = as_int(v);
+    else if (k == "maxblks") maxblks = as_int(v);
+    else if (k == "degree") degree = as_int(v);
+    else if (k == "blksize") blksize = as_int(v);
+    else if (k == "tol") tol = as_double(v);
+    else if (k == "seed") {
+      const long long sd = std::stoll(v);
+      if (sd < 0) has_seed = false;
+      else if (sd > static_cast<long long>(std::numeric_limits<unsigned>::max()))
+        throw Error(FE_ERR_INVALID, "seed out of range for unsigned int");
+      else { has_seed = true; seed = static_cast<unsigned>(sd); }
+    } else if (k == "verbosity") verbosity = static_cast<int>(as_int(v));
+    else if (k == "precision") precision = lower(v);
+    else if (k == "block") block = as_int(v);
+    else if (k == "bounds") bounds = lower(v);
+    else if (k == "amplification") amplification = as_double(v);
+    else if (k == "init") init = lower(v);
+    else if (k == "mixed_switch") mixed_switch = as_double(v);
+    else if (k == "print_every" || k == "logfile" || k == "output_format" || k == "gpu_backend" ||
+             k == "shift" || k == "n") {
+      // accepted for deck compatibility; no effect on this backend
+    } else {
+      throw Error(FE_ERR_INVALID, "unknown option: " + k);
+    }
+  }
+  unsigned seed_or_default() const { return has_seed ? seed : 1u; }
+};
+
+struct Stats {
+  double iterations = 0, status = 0, seconds = 0, fp32_iterations = 0, fp64_iterations = 0;
+  double spmm_launches = 0, lower = 0, upper = 0;
+};
+
+class Context {
+ public:
+  cudaStream_t stream = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  Context() {
+    FE_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    FE_CHECK_SOLVER(cusolverDnCreate(&solver));
+    FE_CHECK_SOLVER(cusolverDnSetStream(solver, stream));
+  }
+  ~Context() {
+    if (solver) cusolverDnDestroy(solver);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void sync() { FE_CHECK_CUDA(cudaStreamSynchronize(stream)); }
+  template <typename T>
+  void to_host(T* dst, const T* src, size_t count) {
+    FE_CHECK_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, stream));
+  }
+  template <typename T>
+  void to_device(T* dst, const T* src, size_t count) {
+    FE_CHECK_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, stream));
+  }
+};
+
+// Host std::mt19937 draws in the reference's column-major order
+// (Executor::create_random_multivector, src/core/Executor.cpp:44-62), scattered into
+// a row-major host staging array and uploaded.
+template <typename T>
+void random_block_host(Context& ctx, Block<T>& X, int64_t cols, unsigned seed) {
+  std::mt19937 rng(seed);
+  std::uniform_real_distribution<double> dist(-1.0, 1.0);
+  std::vector<T> host(static_cast<size_t>(X.n) * X.ld, T(0));
+  for (int64_t j = 0; j < cols; ++j)
+    for (int64_t i = 0; i < X.n; ++i) host[static_cast<size_t>(i) * X.ld + j] = static_cast<T>(dist(rng));
+  FE_CHECK_CUDA(cudaMemcpyAsync(X.data(), host.data(), host.size() * sizeof(T),
+                                cudaMemcpyHostToDevice, ctx.stream));
+  ctx.sync();
+}
+
+// -------------------------------------------------------------------------
+// Lanczos spectral bounds: estimate_bounds_with_executor (src/ChebyshevSolver.cpp:26-49)
+// built on KrylovSubspace::build_one (src/core/KrylovSubspace.cpp:125-259) with
+// two-pass classical reorthogonalization; FP64 on the device, the steps x steps
+// tridiagonal eigensolve on the host (as CudaLanczosWorkspace returns its snapshot).
+// -------------------------------------------------------------------------
+void lanczos_bounds(Context& ctx, const Csr& A, double sign, unsigned seed, bool host_init,
+                    double& lower_out, double& upper_out) {
+  const int64_t n = A.rows;
+  const int64_t steps = std::min<int64_t>(20, n);
+  cudaStream_t s = ctx.stream;
+  DeviceBuffer Vb(static_cast<size_t>(n) * steps * sizeof(double));  // row-major n x steps
+  DeviceBuffer f(n * sizeof(double)), w(n * sizeof(double));
+  DeviceBuffer h(steps * sizeof(double)), hs(steps * sizeof(double)), nrm(sizeof(double));
+  const size_t gws = std::max(gram_workspace_bytes(n, steps, 1), residual_workspace_bytes(n, 1));
+  DeviceBuffer ws(std::max<size_t>(gws, 64));
+  double* V = Vb.as<double>();
+  const int64_t ld = steps;
+  if (host_init) {
+    std::mt19937 rng(seed);
+    std::uniform_real_distribution<double> dist(-1.0, 1.0);
+    std::vector<double> v(n);
+    for (auto& x : v) x = dist(rng);
+    ctx.to_device(f.as<double>(), v.data(), n);
+  } else {
+    fill_uniform<double>(f.as<double>(), 1, n, 1, seed, s);
+  }
+  std::vector<double> T(static_cast<size_t>(steps) * steps, 0.0);
+  auto norm = [&](const double* x) {
+    residual_norms<double>(nullptr, x, nullptr, 1, n, 1, nullptr, nullptr, 0, nullptr,
+                           nrm.as<double>(), nullptr, ws.get(), ws.bytes(), s, 0);
+    double r = 0;
+    ctx.to_host(&r, nrm.as<double>(), 1);
+    ctx.sync();
+    return r;
+  };
+  // Two-pass classical Gram-Schmidt of src against V[:, :k] into f; returns h[k-1].
+  auto orthogonalize = [&](int64_t k, const double* src) {
+    vec_axpby(n, 1.0, src, 1, 0.0, f.as<double>(), 1, s);
+    if (k == 0) return 0.0;
+    gram<double>(V, ld, f.as<double>(), 1, n, k, 1, h.as<double>(), k, ws.get(), ws.bytes(), s);
+    rotate<double>(V, ld, h.as<double>(), k, f.as<double>(), 1, n, k, 1, -1.0, 1.0, s);
+    gram<double>(V, ld, f.as<double>(), 1, n, k, 1, hs.as<double>(), k, ws.get(), ws.bytes(), s);
+    rotate<double>(V, ld, hs.as<double>(), k, f.as<double>(), 1, n, k, 1, -1.0, 1.0, s);
+    double a = 0, b = 0;
+    ctx.to_host(&a, h.as<double>() + k - 1, 1);
+    ctx.to_host(&b, hs.as<double>() + k - 1, 1);
+    ctx.sync();
+    return a + b;
+  };
+  double beta_next = 0.0;
+  for (int64_t it = 0; it < steps; ++it) {
+    bool restarted = false;
+    double beta = norm(f.as<double>());
+    if (!std::isfinite(beta)) throw Error(FE_ERR_NONFINITE, "Lanczos: non-finite residual norm");
+    if (!(beta > std::numeric_limits<double>::epsilon())) {
+      // restart_residual (src/core/KrylovSubspace.cpp:251-259)
+      DeviceBuffer cand(n * sizeof(double));
+      if (host_init) {
+        std::mt19937 rng(seed + static_cast<unsigned>(it + 1));
+        std::uniform_real_distribution<double> dist(-1.0, 1.0);
+        std::vector<double> v(n);
+        for (auto& x : v) x = dist(rng);
+        ctx.to_device(cand.as<double>(), v.data(), n);
+      } else {
+        fill_uniform<double>(cand.as<double>(), 1, n, 1, seed + it + 1, s);
+      }
+      orthogonalize(it, cand.as<double>());
+      restarted = true;
+      beta = norm(f.as<double>());
+      if (!(beta > std::numeric_limits<double>::epsilon()))
+        throw Error(FE_ERR_NONFINITE, "Lanczos: breakdown, unable to generate new basis vector.");
+    }
+    vec_axpby(n, 1.0 / beta, f.as<double>(), 1, 0.0, V + it, ld, s);
+    csr_spmm<double>(A, V + it, ld, w.as<double>(), 1, nullptr, 0, 1, sign, 0.0, 0.0, s);
+    const double alpha = orthogonalize(it + 1, w.as<double>());
+    beta_next = norm(f.as<double>());
+    if (!std::isfinite(beta_next)) throw Error(FE_ERR_NONFINITE, "Lanczos: non-finite norm");
+    const double rec_beta = restarted ? 0.0 : beta;
+    if (it != 0) {
+      T[static_cast<size_t>(it - 1) * steps + it] = rec_beta;
+      T[static_cast<size_t>(it) * steps + it - 1] = rec_beta;
+    }
+    T[static_cast<size_t>(it) * steps + it] = alpha;
+  }
+  std::vector<double> lam, Z;
+  host_symmetric_eig(T, static_cast<int>(steps), lam, Z);
+  double lo = std::numeric_limits<double>::infinity(), up = -lo;
+  for (int64_t j = 0; j < steps; ++j) {
+    // lanczos_absolute_residuals: rel*(1+|l|) = |beta_next * Z[m-1, j]|
+    const double r = std::fabs(beta_next * Z[static_cast<size_t>(j) * steps + steps - 1]);
+    lo = std::min(lo, lam[j] - r);
+    up = std::max(up, lam[j] + r);
+  }
+  if (!std::isfinite(lo) || !std::isfinite(up) || lo > up)
+    throw Error(FE_ERR_NONFINITE, "ChebyshevSolver: invalid spectral bound estimates.");
+  lower_out = lo;
+  upper_out = up;
+}
+
+// cusolverDnDsyevd on the device for the projected k-by-k matrix.
+class ProjectedEig {
+ public:
+  ProjectedEig(Context& ctx, int64_t cap) : ctx_(ctx), cap_(cap) {
+    DeviceBuffer P(static_cast<size_t>(cap) * cap * sizeof(double)), W(cap * sizeof(double));
+    int lwork = 0;
+    FE_CHECK_SOLVER(cusolverDnDsyevd_bufferSize(ctx.solver, CUSOLVER_EIG_MODE_VECTOR,
+                                                CUBLAS_FILL_MODE_UPPER, static_cast<int>(cap),
+                                                P.as<double>(), static_cast<int>(cap),
+                                                W.as<double>(), &lwork));
+    work_.resize(static_cast<size_t>(std::max(lwork, 1)) * sizeof(double));
+    lwork_ = lwork;
+    info_.resize(sizeof(int));
+  }
+  // P (k-by-k, ldp) is overwritten by eigenvectors; W gets ascending eigenvalues.
+  void run(double* P, int64_t k, int64_t ldp, double* W) {
+    FE_CHECK_SOLVER(cusolverDnDsyevd(ctx_.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,
+                                     static_cast<int>(k), P, static_cast<int>(ldp), W,
+                                     work_.as<double>(), lwork_, info_.as<int>()));
+  }
+  int* info() const { return info_.as<int>(); }
+
+ private:
+  Context& ctx_;
+  int64_t cap_;
+  DeviceBuffer work_, info_;
+  int lwork_ = 0;
+};
+
+// Per-precision block set of the Chebyshev iteration.
+template <typename T>
+struct ChebBlocks {
+  Block<T> V;   // "vectors": n x capacity
+  Block<T> S;   // filter scratch, also the A*X Ritz block
+  Block<T> Q;   // orthonormal basis
+  Block<T> AQ;  // A*Q
+  void allocate(int64_t n, int64_t cap) {
+    V.allocate(n, cap);
+    S.allocate(n, cap);
+    Q.allocate(n, cap);
+    AQ.allocate(n, cap);
+  }
+};
+
+struct SmallState {
+  DeviceBuffer G, Rinv, W, rel, rnorm, xnorm, info, gws, rws;
+  int64_t cap = 0;
+  void allocate(int64_t n, int64_t c) {
+    cap = c;
+    G.resize(static_cast<size_t>(c) * c * sizeof(double));
+    Rinv.resize(static_cast<size_t>(c) * c * sizeof(double));
+    W.resize(c * sizeof(double));
+    rel.resize(c * sizeof(double));
+    rnorm.resize(c * sizeof(double));
+    xnorm.resize(c * sizeof(double));
+    info.resize(4 * sizeof(int32_t));
+    gws.resize(std::max<size_t>(gram_workspace_bytes(n, c, c), 64));
+    rws.resize(std::max<size_t>(residual_workspace_bytes(n, c), 64));
+  }
+};
+
+// Cholesky QR of src (n x k) into dst: G = src^T src, R = chol(G), dst = src R^{-1}
+// (cuda_cholesky_qr_in_place, src/core/Orthogonalization.cpp:185-246).
+// The rank-loss flag accumulates into info[slot].
+template <typename T>
+void cholqr(Context& ctx, SmallState& sm, const T* src, int64_t lds, T* dst, int64_t ldd, int64_t n,
+            int64_t k, int slot) {
+  cudaStream_t s = ctx.stream;
+  double* G = sm.G.as<double>();
+  gram<T>(src, lds, src, lds, n, k, k, G, sm.cap, sm.gws.get(), sm.gws.bytes(), s);
+  potrf_upper(G, k, sm.cap, sm.info.as<int32_t>() + slot, s);
+  trinv_upper(G, sm.cap, sm.Rinv.as<double>(), sm.cap, k, s);
+  rotate<T>(src, lds, sm.Rinv.as<double>(), sm.cap, dst, ldd, n, k, k, 1.0, 0.0, s);
+}
+
+// Filter scaling (src/ChebyshevSolver.cpp:231-239) for a damped interval [cutoff, upper]
+// where the amplification at `lower` is `amp` (the reference: amp = 1e3).
+double reference_cutoff(double lower, double upper, int64_t degree, double amp) {
+  const double xlb = std::cosh(std::acosh(amp) / static_cast<double>(degree));
+  return (2.0 * lower + upper * (xlb - 1.0)) / (1.0 + xlb);
+}
+
+template <typename T>
+struct ChebLoop {
+  Context& ctx;
+  const Csr& A;
+  const Options& opt;
+  SmallState& sm;
+  ProjectedEig& eig;
+  ChebBlocks<T> b;
+  int64_t n, nev, cap, degree;
+  double sign, lower, upper;
+  bool cholqr2;
+
+  ChebLoop(Context& c, const Csr& a, const Options& o, SmallState& s, ProjectedEig& e, double sg,
+           double lo, double up, bool two_pass)
+      : ctx(c), A(a), opt(o), sm(s), eig(e), n(a.rows), nev(o.nev), degree(o.degree), sign(sg),
+        lower(lo), upper(up), cholqr2(two_pass) {}
+
+  // One filter + deflation + QR + Rayleigh-Ritz cycle (src/ChebyshevSolver.cpp:151-184).
+  // On return the host holds the Ritz values W[0:sub], residuals rel[0:sub] and info.
+  void iterate(int64_t locked, int64_t sub, double cutoff, std::vector<double>& W,
+               std::vector<double>& rel, int32_t* info_host, Stats& st) {
+    cudaStream_t s = ctx.stream;
+    const int64_t active = sub - locked;
+    FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, 4 * sizeof(int32_t), s));
+    // 1. Filter Y = T_degree(c*op + d*I) X_active, in place on V's active columns.
+    if (upper != cutoff) {
+      const double c = 2.0 / (upper - cutoff);
+      const double d = -(upper + cutoff) / (upper - cutoff);
+      if (!std::isfinite(c) || !std::isfinite(d))
+        throw Error(FE_ERR_NONFINITE, "ChebyshevSolver: invalid filter scaling.");
+      // The operator is sign*A: fold the sign into c.
+      filter(b.V.col(locked), b.V.ld, b.S.data(), b.S.ld, active, sign * c, d);
+      st.spmm_launches += static_cast<double>(degree);
+    }
+    // 2. Deflate against locked vectors with two-pass block Gram-Schmidt
+    // (block_gram_schmidt, src/core/Orthogonalization.cpp:482-527).
+    if (locked > 0) {
+      for (int pass = 0; pass < 2; ++pass) {
+        gram<T>(b.V.data(), b.V.ld, b.V.col(locked), b.V.ld, n, locked, active, sm.G.as<double>(),
+                sm.cap, sm.gws.get(), sm.gws.bytes(), s);
+        rotate<T>(b.V.data(), b.V.ld, sm.G.as<double>(), sm.cap, b.V.col(locked), b.V.ld, n,
+                  locked, active, -1.0, 1.0, s);
+      }
+    }
+    // 3. Cholesky QR of the current subspace (CholQR2 on FP32 blocks).
+    if (cholqr2) {
+      cholqr<T>(ctx, sm, b.V.data(), b.V.ld, b.S.data(), b.S.ld, n, sub, 0);
+      cholqr<T>(ctx, sm, b.S.data(), b.S.ld, b.Q.data(), b.Q.ld, n, sub, 1);
+    } else {
+      cholqr<T>(ctx, sm, b.V.data(), b.V.ld, b.Q.data(), b.Q.ld, n, sub, 0);
+    }
+    // 4. Rayleigh-Ritz: AQ = op*Q, P = Q^T AQ, eig(P), rotate Q and AQ, residuals.
+    csr_spmm<T>(A, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, nullptr, 0, sub, sign, 0.0, 0.0, s);
+    st.spmm_launches += 1;
+    double* P = sm.G.as<double>();
+    gram<T>(b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, n, sub, sub, P, sm.cap, sm.gws.get(),
+            sm.gws.bytes(), s);
+    symmetrize(P, sub, sm.cap, s);
+    eig.run(P, sub, sm.cap, sm.W.as<double>());
+    rotate<T>(b.Q.data(), b.Q.ld, P, sm.cap, b.V.data(), b.V.ld, n, sub, sub, 1.0, 0.0, s);
+    rotate<T>(b.AQ.data(), b.AQ.ld, P, sm.cap, b.S.data(), b.S.ld, n, sub, sub, 1.0, 0.0, s);
+    residual_norms<T>(b.S.data(), b.V.data(), nullptr, b.V.ld, n, sub, sm.W.as<double>(), nullptr,
+                      0, sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
+                      sm.rws.get(), sm.rws.bytes(), s, 1);
+    W.resize(sub);
+    rel.resize(sub);
+    ctx.to_host(W.data(), sm.W.as<double>(), sub);
+    ctx.to_host(rel.data(), sm.rel.as<double>(), sub);
+    ctx.to_host(info_host, sm.info.as<int32_t>(), 2);
+    ctx.to_host(info_host + 2, eig.info(), 1);
+    ctx.sync();
+  }
+
+  void filter(T* X, int64_t ldx, T* Sc, int64_t lds, int64_t cols, double c, double d) {
+    cudaStream_t s = ctx.stream;
+    // Y1 = c*A*Y0 + d*Y0 into scratch; Y_k = 2c*A*Y_{k-1} + 2d*Y_{k-1} - Y_{k-2} in place.
+    csr_spmm<T>(A, X, ldx, Sc, lds, nullptr, 0, cols, c, d, 0.0, s);
+    T* prev = X;
+    int64_t ldp = ldx;
+    T* cur = Sc;
+    int64_t ldc = lds;
+    for (int64_t k = 2; k <= degree; ++k) {
+      csr_spmm<T>(A, cur, ldc, prev, ldp, prev, ldp, cols, 2.0 * c, 2.0 * d, -1.0, s);
+      std::swap(prev, cur);
+      std::swap(ldp, ldc);
+    }
+    if (cur != X) {
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(X, ldx * sizeof(T), cur, ldc * sizeof(T), cols * sizeof(T),
+                                      n, cudaMemcpyDeviceToDevice, s));
+    }
+  }
+};
+
+struct SolveOut {
+  std::vector<double> values, rel;
+  int64_t iterations = 0;
+};
+
+// ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221) on the device.
+void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, double* residuals,
+                     double* eigenvectors, Stats& st) {
+  const int64_t n = A.rows;
+  const int64_t nev = opt.nev;
+  FE_REQUIRE(A.rows == A.cols, "ChebyshevSolver: matrix must be square.");
+  if (n <= 0 || nev <= 0 || nev > n)
+    throw Error(FE_ERR_INVALID, "ChebyshevSolver: nev must be in [1,n].");
+  if (opt.which != "sr" && opt.which != "lr")
+    throw Error(FE_ERR_INVALID, "ChebyshevSolver: only SR and LR are supported.");
+  FE_REQUIRE(opt.degree >= 1, "ChebyshevSolver: degree must be >= 1.");
+  FE_REQUIRE(opt.precision == "fp64" || opt.precision == "mixed",
+             "precision must be fp64 or mixed");
+  FE_REQUIRE(opt.bounds == "reference" || opt.bounds == "ritz", "bounds must be reference or ritz");
+  FE_REQUIRE(opt.init == "host" || opt.init == "device", "init must be host or device");
+  const bool flip = opt.which == "lr";
+  const double sign = flip ? -1.0 : 1.0;
+  const unsigned seed = opt.seed_or_default();
+  int64_t cap = nev + std::min(nev, n - nev);
+  if (opt.block > 0) cap = std::max(nev, std::min(opt.block, n));
+  const bool host_init = opt.init == "host";
+  const bool mixed = opt.precision == "mixed";
+
+  Context ctx;
+  SmallState sm;
+  sm.allocate(n, cap);
+  ProjectedEig eig(ctx, cap);
+
+  double lower = 0, upper = 0;
+  lanczos_bounds(ctx, A, sign, seed, host_init, lower, upper);
+  st.lower = lower;
+  st.upper = upper;
+
+  std::unique_ptr<ChebLoop<float>> l32;
+  std::unique_ptr<ChebLoop<double>> l64;
+  // Initial block and its Cholesky QR (src/ChebyshevSolver.cpp:94-107).
+  {
+    Block<double> V0;
+    V0.allocate(n, cap);
+    if (host_init) random_block_host<double>(ctx, V0, cap, seed);
+    else fill_uniform<double>(V0.data(), V0.ld, n, cap, seed, ctx.stream);
+    if (mixed) {
+      l32.reset(new ChebLoop<float>(ctx, A, opt, sm, eig, sign, lower, upper, true));
+      l32->b.allocate(n, cap);
+      // QR in FP64 then round the orthonormal block to FP32.
+      Block<double> Q0;
+      Q0.allocate(n, cap);
+      cholqr<double>(ctx, sm, V0.data(), V0.ld, Q0.data(), Q0.ld, n, cap, 0);
+      convert<double, float>(Q0.data(), Q0.ld, l32->b.V.data(), l32->b.V.ld, n, cap, ctx.stream);
+    } else {
+      l64.reset(new ChebLoop<double>(ctx, A, opt, sm, eig, sign, lower, upper, false));
+      l64->b.allocate(n, cap);
+      cholqr<double>(ctx, sm, V0.data(), V0.ld, l64->b.V.data(), l64->b.V.ld, n, cap, 0);
+    }
+    int32_t info = 0;
+    ctx.to_host(&info, sm.info.as<int32_t>(), 1);
+    ctx.sync();
+    if (info != 0) throw Error(FE_ERR_NOT_SPD, "ChebyshevSolver: initial Cholesky QR failed.");
+  }
+
+  int64_t locked = 0;
+  int64_t sub = nev;
+  int64_t sub_prev = 0;
+  std::vector<double> W, rel;
+  int64_t it_done = 0;
+  const double tol = opt.tol;
+  for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
+    // Damped interval [cutoff, upper]: the reference fixes the cutoff where the
+    // filter amplifies `lower` by 1e3. bounds=ritz (after the first cycle) damps
+    // from the largest Ritz value of the last Rayleigh-Ritz instead, lowered if
+    // needed so that the amplification at `lower` stays within the cap.
+    double cutoff = reference_cutoff(lower, upper, opt.degree, 1.0e3);
+    if (opt.bounds == "ritz" && sub_prev > 0) {
+      cutoff = std::min(W[sub_prev - 1],
+                        reference_cutoff(lower, upper, opt.degree, opt.amplification));
+    }
+    if (upper == lower) cutoff = upper;  // collapsed spectrum: no filtering
+    int32_t info[3] = {0, 0, 0};
+    if (l32) {
+      l32->iterate(locked, sub, cutoff, W, rel, info, st);
+      st.fp32_iterations += 1;
+    } else {
+      l64->iterate(locked, sub, cutoff, W, rel, info, st);
+      st.fp64_iterations += 1;
+    }
+    if (info[0] != 0 || info[1] != 0)
+      throw Error(FE_ERR_NOT_SPD, "ChebyshevSolver: Cholesky QR failed during filtering.");
+    if (info[2] != 0) throw Error(FE_ERR_CUDA, "ChebyshevSolver: projected eigensolve failed.");
+    for (int64_t j = 0; j < sub; ++j)
+      if (!std::isfinite(W[j]) || !std::isfinite(rel[j]))
+        throw Error(FE_ERR_NONFINITE, "ChebyshevSolver: non-finite Ritz values or residuals.");
+    sub_prev = sub;
+    // 4. Ordered locking (src/ChebyshevSolver.cpp:186-192).
+    locked = 0;
+    while (locked < nev && rel[locked] <= tol) ++locked;
+    sub = std::max(sub, nev + std::min(locked, cap - nev));
+    it_done = iter + 1;
+    double worst = 0.0;
+    for (int64_t j = 0; j < nev; ++j) worst = std::max(worst, rel[j]);
+    if (opt.verbosity >= 2) {
+      std::fprintf(stderr, "[fe] iter %lld %s sub %lld locked %lld worst %.3e cutoff %.6g\n",
+                   static_cast<long long>(iter + 1), l32 ? "fp32" : "fp64",
+                   static_cast<long long>(sub_prev), static_cast<long long>(locked), worst, cutoff);
+    }
+    if (worst <= tol) break;
+    if (l32 && worst <= std::max(opt.mixed_switch, tol)) {
+      // FP32 residual floor reached: continue on FP64 blocks.
+      l64.reset(new ChebLoop<double>(ctx, A, opt, sm, eig, sign, lower, upper, false));
+      l64->b.allocate(n, cap);
+      convert<float, double>(l32->b.V.data(), l32->b.V.ld, l64->b.V.data(), l64->b.V.ld, n, cap,
+                             ctx.stream);
+      ctx.sync();
+      l32.reset();
+    }
+  }
+  // Results: eigenvalues (sign restored), residuals, first nev Ritz vectors.
+  for (int64_t j = 0; j < nev; ++j) {
+    eigenvalues[j] = sign * W[j];
+    residuals[j] = rel[j];
+  }
+  if (eigenvectors) {
+    // Row-major device block -> column-major host n x nev (copy_to_host boundary).
+    std::vector<double> host(static_cast<size_t>(n) * nev);
+    if (l64) {
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(host.data(), nev * sizeof(double), l64->b.V.data(),
+                                      l64->b.V.ld * sizeof(double), nev * sizeof(double), n,
+                                      cudaMemcpyDeviceToHost, ctx.stream));
+    } else {
+      Block<double> tmp;
+      tmp.allocate(n, nev);
+      convert<float, double>(l32->b.V.data(), l32->b.V.ld, tmp.data(), tmp.ld, n, nev, ctx.stream);
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(host.data(), nev * sizeof(double), tmp.data(),
+                                      tmp.ld * sizeof(double), nev * sizeof(double), n,
+                                      cudaMemcpyDeviceToHost, ctx.stream));
+      ctx.sync();
+    }
+    ctx.sync();
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t j = 0; j < nev; ++j)
+        eigenvectors[static_cast<size_t>(j) * n + i] = host[static_cast<size_t>(i) * nev + j];
+  }
+  st.iterations = static_cast<double>(it_done);
+}
+
+}  // namespace
+}  // namespace fe
+
+extern "C" int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eigenvalues,
+                        double* residual_norms, double* eigenvectors, double* stats) {
+  return fe::guarded("fe_solve", [&] {
+    FE_REQUIRE(A, "null CSR handle");
+    FE_REQUIRE(eigenvalues && residual_norms, "null result arrays");
+    fe::Options opt;
+    opt.parse(options);
+    fe::Stats st;
+    const auto t0 = std::chrono::steady_clock::now();
+    FE_CHECK_CUDA(cudaSetDevice(A->m.device));
+    if (opt.solver == "chebyshev") {
+      FE_REQUIRE(B == nullptr, "ChebyshevSolver: generalized problems are not supported.");
+      fe::chebyshev_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
+    } else {
+      throw fe::Error(FE_ERR_UNSUPPORTED, "solver not available on this backend: " + opt.solver);
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    st.seconds = std::chrono::duration<double>(t1 - t0).count();
+    if (stats) {
+      stats[0] = st.iterations;
+      stats[1] = st.status;
+      stats[2] = st.seconds;
+      stats[3] = st.spmm_launches;
+      stats[4] = st.fp32_iterations;
+      stats[5] = st.fp64_iterations;
+      stats[6] = st.lower;
+      stats[7] = st.upper;
+    }
+  });
+}

@@ -1,0 +1,364 @@
+// CSR block SpMM and the fused Chebyshev three-term step for sm_100a.
+//
+// Replaces CudaCsrMatrix::apply_block (src/gpu/CudaCsrMatrix.cpp:196-223), which
+// runs one cuSPARSE SpMV per column and so streams the CSR arrays once per
+// column, and the copy/SpMV/axpy sequence of ChebyshevSolver::chebyshev_filter
+// (src/ChebyshevSolver.cpp:243-256), which makes about five passes over the
+// block per filter step.
+//
+// Layout: the dense blocks are row-major slabs, so the b values a CSR row
+// needs from one neighbour are contiguous. A group of G lanes owns one row;
+// each lane owns CPL 128-bit vectors of that row's b columns. Nonzeros are
+// fetched G at a time (one coalesced load of colind/values per group) and
+// broadcast with warp shuffles; every neighbour row of X is then read with
+// fully coalesced 128-bit loads. Accumulation is in the storage precision
+// (FP32 blocks: FP32 values and accumulators; FP64 blocks: FP64). The epilogue
+// fuses y = alpha*acc + gamma*x_row + beta*z_row and writes y once, which is
+// the whole Chebyshev step.
+//
+// Algorithmic bytes per launch (the roofline figure): nnz*(s+4) + 4*(n+1) +
+// 2*n*b*s for SpMM (X read once, Y written once), plus n*b*s for each of the
+// gamma (X row re-read, an L2 hit) and beta (Z read) terms that are active.
+
+#include "fe_common.cuh"
+
+#include <algorithm>
+
+namespace fe {
+namespace {
+
+template <typename T>
+struct VecT;
+template <>
+struct VecT<float> {
+  using type = float4;
+  static constexpr int width = 4;
+};
+template <>
+struct VecT<double> {
+  using type = double2;
+  static constexpr int width = 2;
+};
+
+template <typename T, int VEC>
+struct Pack {
+  T v[VEC];
+};
+
+template <typename T, int VEC>
+__device__ __forceinline__ Pack<T, VEC> load_pack(const T* p) {
+  Pack<T, VEC> r;
+  if constexpr (VEC == 4) {
+    float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+  } else if constexpr (VEC == 2) {
+    double2 t = __ldg(reinterpret_cast<const double2*>(p));
+    r.v[0] = t.x; r.v[1] = t.y;
+  } else {
+    r.v[0] = __ldg(p);
+  }
+  return r;
+}
+
+// Plain (coherent) load for blocks that may alias the output.
+template <typename T, int VEC>
+__device__ __forceinline__ Pack<T, VEC> load_pack_rw(const T* p) {
+  Pack<T, VEC> r;
+  if constexpr (VEC == 4) {
+    float4 t = *reinterpret_cast<const float4*>(p);
+    r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+  } else if constexpr (VEC == 2) {
+    double2 t = *reinterpret_cast<const double2*>(p);
+    r.v[0] = t.x; r.v[1] = t.y;
+  } else {
+    r.v[0] = *p;
+  }
+  return r;
+}
+
+template <typename T, int VEC>
+__device__ __forceinline__ void store_pack(T* p, const Pack<T, VEC>& r) {
+  if constexpr (VEC == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+  } else if constexpr (VEC == 2) {
+    *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
+  } else {
+    *p = r.v[0];
+  }
+}
+
+constexpr int kThreads = 256;
+
+// Y[row, c0:c1] = alpha * sum_k a_k X[col_k, c0:c1] + gamma * X[row, c0:c1]
+//                 + beta * Z[row, c0:c1]
+// blockIdx.y selects a column panel of width G*CPL*VEC.
+template <typename T, int VEC, int G, int CPL>
+__global__ void __launch_bounds__(kThreads)
+csr_spmm_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
+                const int32_t* __restrict__ colind, const T* __restrict__ vals,
+                const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
+                int64_t ldz, int ncols, T alpha, T gamma, T beta, int use_gamma,
+                int use_beta) {
+  constexpr int kRowsPerBlock = kThreads / G;
+  const int group = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  const int64_t row = static_cast<int64_t>(blockIdx.x) * kRowsPerBlock + group;
+  if (row >= nrows) return;  // whole group leaves together
+  const int panel0 = blockIdx.y * (G * CPL * VEC);
+  const int nvec = (min(ncols - panel0, G * CPL * VEC) + VEC - 1) / VEC;
+
+  unsigned mask;
+  if constexpr (G == 32) {
+    mask = 0xffffffffu;
+  } else {
+    const int warp_lane = threadIdx.x & 31;
+    mask = ((1u << G) - 1u) << (warp_lane - lane);
+  }
+
+  T acc[CPL][VEC];
+#pragma unroll
+  for (int i = 0; i < CPL; ++i)
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) acc[i][e] = T(0);
+
+  const int start = __ldg(rowptr + row);
+  const int end = __ldg(rowptr + row + 1);
+  const T* Xp = X + panel0;
+  for (int base = start; base < end; base += G) {
+    const int k = base + lane;
+    int c = 0;
+    T a = T(0);
+    if (k < end) {
+      c = __ldg(colind + k);
+      a = __ldg(vals + k);
+    }
+    const int cnt = min(G, end - base);
+    int t = 0;
+    // Two neighbours per trip: independent loads in flight.
+    for (; t + 1 < cnt; t += 2) {
+      const int c0 = __shfl_sync(mask, c, t, G);
+      const T a0 = __shfl_sync(mask, a, t, G);
+      const int c1 = __shfl_sync(mask, c, t + 1, G);
+      const T a1 = __shfl_sync(mask, a, t + 1, G);
+      const T* x0 = Xp + static_cast<int64_t>(c0) * ldx;
+      const T* x1 = Xp + static_cast<int64_t>(c1) * ldx;
+      Pack<T, VEC> p0[CPL], p1[CPL];
+#pragma unroll
+      for (int i = 0; i < CPL; ++i) {
+        const int v = lane + i * G;
+        if (v < nvec) {
+          p0[i] = load_pack<T, VEC>(x0 + v * VEC);
+          p1[i] = load_pack<T, VEC>(x1 + v * VEC);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < CPL; ++i) {
+        const int v = lane + i * G;
+        if (v < nvec) {
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) {
+            acc[i][e] = fma(a0, p0[i].v[e], acc[i][e]);
+            acc[i][e] = fma(a1, p1[i].v[e], acc[i][e]);
+          }
+        }
+      }
+    }
+    if (t < cnt) {
+      const int c0 = __shfl_sync(mask, c, t, G);
+      const T a0 = __shfl_sync(mask, a, t, G);
+      const T* x0 = Xp + static_cast<int64_t>(c0) * ldx;
+#pragma unroll
+      for (int i = 0; i < CPL; ++i) {
+        const int v = lane + i * G;
+        if (v < nvec) {
+          Pack<T, VEC> p = load_pack<T, VEC>(x0 + v * VEC);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) acc[i][e] = fma(a0, p.v[e], acc[i][e]);
+        }
+      }
+    }
+  }
+
+  T* yrow = Y + row * ldy + panel0;
+  const T* xrow = X + row * ldx + panel0;
+  const T* zrow = use_beta ? Z + row * ldz + panel0 : nullptr;
+#pragma unroll
+  for (int i = 0; i < CPL; ++i) {
+    const int v = lane + i * G;
+    if (v < nvec) {
+      Pack<T, VEC> out;
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) out.v[e] = alpha * acc[i][e];
+      if (use_gamma) {
+        Pack<T, VEC> xr = load_pack<T, VEC>(xrow + v * VEC);
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) out.v[e] = fma(gamma, xr.v[e], out.v[e]);
+      }
+      if (use_beta) {
+        Pack<T, VEC> zr = load_pack_rw<T, VEC>(zrow + v * VEC);
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) out.v[e] = fma(beta, zr.v[e], out.v[e]);
+      }
+      store_pack<T, VEC>(yrow + v * VEC, out);
+    }
+  }
+}
+
+template <typename T, int VEC, int G, int CPL>
+void launch_one(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, int64_t ldy,
+                const T* Z, int64_t ldz, int ncols, T alpha, T gamma, T beta, bool ug,
+                bool ub, cudaStream_t s) {
+  constexpr int rows_per_block = kThreads / G;
+  const int64_t blocks = (A.rows + rows_per_block - 1) / rows_per_block;
+  const int panel = G * CPL * VEC;
+  const int panels = (ncols + panel - 1) / panel;
+  FE_REQUIRE(blocks <= 0x7fffffffLL, "csr_spmm: too many rows for one launch");
+  dim3 grid(static_cast<unsigned>(blocks), static_cast<unsigned>(panels));
+  csr_spmm_kernel<T, VEC, G, CPL><<<grid, kThreads, 0, s>>>(
+      A.rows, A.rowptr, A.colind, vals, X, ldx, Y, ldy, Z, ldz, ncols, alpha, gamma, beta,
+      ug ? 1 : 0, ub ? 1 : 0);
+  check_launch("csr_spmm_kernel");
+}
+
+template <typename T, int VEC>
+void dispatch_vec(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, int64_t ldy,
+                  const T* Z, int64_t ldz, int ncols, T alpha, T gamma, T beta, bool ug,
+                  bool ub, cudaStream_t s) {
+  const int nvec = (ncols + VEC - 1) / VEC;
+#define FE_LAUNCH(G_, CPL_) \
+  launch_one<T, VEC, G_, CPL_>(A, vals, X, ldx, Y, ldy, Z, ldz, ncols, alpha, gamma, beta, ug, ub, s)
+  if (nvec <= 1) FE_LAUNCH(1, 1);
+  else if (nvec <= 2) FE_LAUNCH(2, 1);
+  else if (nvec <= 4) FE_LAUNCH(4, 1);
+  else if (nvec <= 8) FE_LAUNCH(8, 1);
+  else if (nvec <= 16) FE_LAUNCH(16, 1);
+  else if (nvec <= 32) FE_LAUNCH(32, 1);
+  else if (nvec <= 64) FE_LAUNCH(32, 2);
+  else if (nvec <= 96) FE_LAUNCH(32, 3);
+  else if (nvec <= 128) FE_LAUNCH(32, 4);
+  else if (nvec <= 160) FE_LAUNCH(32, 5);
+  else if (nvec <= 192) FE_LAUNCH(32, 6);
+  else FE_LAUNCH(32, 8);  // wider blocks run as column panels of 256 vectors
+#undef FE_LAUNCH
+}
+
+}  // namespace
+
+// Shared entry used by the C ABI and the host solver.
+template <typename T>
+void csr_spmm(const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T* Z, int64_t ldz,
+              int64_t ncols, double alpha, double gamma, double beta, cudaStream_t s) {
+  FE_REQUIRE(ncols >= 0 && ncols <= 0x7fffffff, "csr_spmm: invalid column count");
+  if (ncols == 0 || A.rows == 0) return;
+  FE_REQUIRE(X && Y, "csr_spmm: null block pointer");
+  FE_REQUIRE(ldx >= ncols && ldy >= ncols, "csr_spmm: leading dimension smaller than ncols");
+  const bool ub = beta != 0.0;
+  const bool ug = gamma != 0.0;
+  if (ub) {
+    FE_REQUIRE(Z != nullptr && ldz >= ncols, "csr_spmm: beta != 0 needs a Z block");
+  }
+  FE_REQUIRE(!ranges_overlap(X, A.cols, ldx, ncols, static_cast<const T*>(Y), A.rows, ldy, ncols),
+             "csr_spmm: X and Y overlap");
+  const T* vals = nullptr;
+  if constexpr (sizeof(T) == 8) vals = A.val64; else vals = A.val32;
+  constexpr int VEC = VecT<T>::width;
+  const bool vec_ok = ncols % VEC == 0 && ldx % VEC == 0 && ldy % VEC == 0 && aligned16(X) &&
+                      aligned16(Y) && (!ub || (ldz % VEC == 0 && aligned16(Z)));
+  if (vec_ok) {
+    dispatch_vec<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
+                         T(gamma), T(beta), ug, ub, s);
+  } else {
+    dispatch_vec<T, 1>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
+                       T(gamma), T(beta), ug, ub, s);
+  }
+}
+
+template void csr_spmm<double>(const Csr&, const double*, int64_t, double*, int64_t,
+                               const double*, int64_t, int64_t, double, double, double,
+                               cudaStream_t);
+template void csr_spmm<float>(const Csr&, const float*, int64_t, float*, int64_t, const float*,
+                              int64_t, int64_t, double, double, double, cudaStream_t);
+
+// In-place filter of degree `degree`: X <- T_degree(c*A + d*I) X, scratch holds Y_{k-1}.
+template <typename T>
+void cheb_filter(const Csr& A, T* X, T* scratch, int64_t ld, int64_t ncols, int degree, double c,
+                 double d, cudaStream_t s) {
+  FE_REQUIRE(degree >= 1, "cheb_filter: degree must be >= 1");
+  // Y1 = c*A*Y0 + d*Y0 into scratch; then Y_k overwrites Y_{k-2} in place.
+  csr_spmm<T>(A, X, ld, scratch, ld, nullptr, 0, ncols, c, d, 0.0, s);
+  T* prev = X;       // Y_{k-2}
+  T* cur = scratch;  // Y_{k-1}
+  for (int k = 2; k <= degree; ++k) {
+    csr_spmm<T>(A, cur, ld, prev, ld, prev, ld, ncols, 2.0 * c, 2.0 * d, -1.0, s);
+    std::swap(prev, cur);
+  }
+  if (cur != X) {
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(X, ld * sizeof(T), cur, ld * sizeof(T), ncols * sizeof(T),
+                                    A.rows, cudaMemcpyDeviceToDevice, s));
+  }
+}
+
+template void cheb_filter<double>(const Csr&, double*, double*, int64_t, int64_t, int, double,
+                                  double, cudaStream_t);
+template void cheb_filter<float>(const Csr&, float*, float*, int64_t, int64_t, int, double,
+                                 double, cudaStream_t);
+
+}  // namespace fe
+
+using fe::guarded;
+
+extern "C" int fe_spmm_csr_f64(fe_csr_t A, const double* X, int64_t ldx, double* Y, int64_t ldy,
+                               int64_t ncols, double alpha, double beta, void* stream) {
+  return guarded("fe_spmm_csr_f64", [&] {
+    FE_REQUIRE(A, "null CSR handle");
+    fe::csr_spmm<double>(A->m, X, ldx, Y, ldy, Y, ldy, ncols, alpha, 0.0, beta,
+                         fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_spmm_csr_f32(fe_csr_t A, const float* X, int64_t ldx, float* Y, int64_t ldy,
+                               int64_t ncols, double alpha, double beta, void* stream) {
+  return guarded("fe_spmm_csr_f32", [&] {
+    FE_REQUIRE(A, "null CSR handle");
+    fe::csr_spmm<float>(A->m, X, ldx, Y, ldy, Y, ldy, ncols, alpha, 0.0, beta,
+                        fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_cheb_step_f64(fe_csr_t A, const double* Ycur, const double* Yprev,
+                                double* Yout, int64_t ld, int64_t ncols, double alpha,
+                                double gamma, double beta, void* stream) {
+  return guarded("fe_cheb_step_f64", [&] {
+    FE_REQUIRE(A, "null CSR handle");
+    fe::csr_spmm<double>(A->m, Ycur, ld, Yout, ld, Yprev, ld, ncols, alpha, gamma, beta,
+                         fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_cheb_step_f32(fe_csr_t A, const float* Ycur, const float* Yprev, float* Yout,
+                                int64_t ld, int64_t ncols, double alpha, double gamma,
+                                double beta, void* stream) {
+  return guarded("fe_cheb_step_f32", [&] {
+    FE_REQUIRE(A, "null CSR handle");
+    fe::csr_spmm<float>(A->m, Ycur, ld, Yout, ld, Yprev, ld, ncols, alpha, gamma, beta,
+                        fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_cheb_filter_f64(fe_csr_t A, double* X, double* scratch, int64_t ld,
+                                  int64_t ncols, int32_t degree, double c, double d,
+                                  void* stream) {
+  return guarded("fe_cheb_filter_f64", [&] {
+    FE_REQUIRE(A, "null CSR handle");
+    fe::cheb_filter<double>(A->m, X, scratch, ld, ncols, degree, c, d, fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_cheb_filter_f32(fe_csr_t A, float* X, float* scratch, int64_t ld,
+                                  int64_t ncols, int32_t degree, double c, double d,
+                                  void* stream) {
+  return guarded("fe_cheb_filter_f32", [&] {
+    FE_REQUIRE(A, "null CSR handle");
+    fe::cheb_filter<float>(A->m, X, scratch, ld, ncols, degree, c, d, fe::as_stream(stream));
+  });
+}

@@ -1,0 +1,178 @@
+"""Python mirror of fasteig's public problem/options API on the B200 backend.
+
+``fasteig_options`` keeps the reference's key names and defaults
+(include/fasteig_options.hpp:102-118, set() keys src/fasteig_options.cpp:51-112);
+``fasteig_problem`` keeps ``solve(opts)``, ``eigenvalues()``, ``eigenvectors()``,
+``residual_norms()``, ``status()`` and ``last_iterations()``
+(include/fasteig_problem.hpp:33-108). Solves run through ``fe_solve`` of the C
+ABI; there is no CPU code path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from ._lib import check, lib
+
+_INT_KEYS = ("n", "nev", "maxiter", "maxdim", "maxblks", "degree", "blksize", "verbosity",
+             "print_every", "block")
+_FLOAT_KEYS = ("tol", "shift", "amplification", "mixed_switch")
+_STR_KEYS = ("which", "solver", "precision", "bounds", "init", "logfile", "output_format")
+
+
+class fasteig_options:  # noqa: N801 - reference class name
+    """Solver configuration (include/fasteig_options.hpp:21-134)."""
+
+    def __init__(self, n: int = 0):
+        self._kv = {"n": n, "nev": 10, "maxiter": 1000, "maxdim": 0, "maxblks": 10,
+                    "degree": 10, "blksize": 1, "which": "LM", "solver": "Lanczos",
+                    "shift": 0.0, "tol": 1.0e-8, "seed": None, "verbosity": 1,
+                    "print_every": 0}
+        self.v0 = None
+
+    def set(self, key: str, value) -> bool:
+        """fasteig_options::set: False for unknown keys, ValueError for bad values."""
+        k = key.lower()
+        if k == "seed":
+            s = int(value)
+            if s < 0:
+                self._kv["seed"] = None
+            elif s > 0xFFFFFFFF:
+                raise ValueError("seed out of range for unsigned int")
+            else:
+                self._kv["seed"] = s
+            return True
+        if k in _INT_KEYS:
+            self._kv[k] = int(value)
+        elif k in _FLOAT_KEYS:
+            self._kv[k] = float(value)
+        elif k in _STR_KEYS:
+            self._kv[k] = str(value)
+        elif k == "gpu_backend":
+            return True  # this backend is always the GPU
+        else:
+            return False
+        return True
+
+    def get(self, key: str):
+        k = key.lower()
+        if k not in self._kv:
+            raise KeyError(key)
+        return self._kv[k]
+
+    def validate(self) -> None:
+        """fasteig_options::validate essentials."""
+        if self._kv["nev"] <= 0:
+            raise ValueError("nev must be positive")
+        if self._kv["maxiter"] <= 0:
+            raise ValueError("maxiter must be positive")
+        if not self._kv["tol"] > 0:
+            raise ValueError("tol must be positive")
+
+    def nev(self) -> int:
+        return int(self._kv["nev"])
+
+    def to_text(self) -> str:
+        lines = []
+        for k, v in self._kv.items():
+            if k in ("n", "verbosity", "print_every", "logfile", "output_format") and k != "verbosity":
+                continue
+            if v is None:
+                continue
+            if k == "verbosity" and int(v) < 2:
+                continue
+            lines.append(f"{k}={v}")
+        return "\n".join(lines)
+
+
+class CsrMatrix:
+    """Device CSR operator owned by the backend (CudaCsrMatrix equivalent)."""
+
+    def __init__(self, n: int, rowptr, colind, values, cols: Optional[int] = None):
+        self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        self.colind = np.ascontiguousarray(colind, dtype=np.int32)
+        self.values = np.ascontiguousarray(values, dtype=np.float64)
+        self.rows = int(n)
+        self.cols = int(n if cols is None else cols)
+        h = C.c_void_p()
+        check(lib.fe_csr_create(self.rows, self.cols, int(self.values.size),
+                                self.rowptr.ctypes.data, self.colind.ctypes.data,
+                                self.values.ctypes.data, C.byref(h)))
+        self.handle = h
+
+    @property
+    def nnz(self) -> int:
+        return int(self.values.size)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib.fe_csr_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class fasteig_problem:  # noqa: N801 - reference class name
+    """Standard (A x = l x) or generalized (A x = l B x) sparse symmetric problem."""
+
+    def __init__(self, A: CsrMatrix, B: Optional[CsrMatrix] = None, solver: str = "Lanczos"):
+        self.A = A
+        self.B = B
+        self._solver = solver
+        self._eigvals = np.zeros(0)
+        self._resnrms = np.zeros(0)
+        self._eigvecs = np.zeros((A.rows, 0))
+        self._status = 0
+        self._iters = None
+        self.stats = {}
+
+    def n(self) -> int:
+        return self.A.rows
+
+    def is_generalized(self) -> bool:
+        return self.B is not None
+
+    def solve(self, opts: Optional[fasteig_options] = None, want_vectors: bool = True) -> int:
+        opts = opts or fasteig_options(self.n())
+        opts.validate()
+        text = opts.to_text()
+        if "solver=" not in text:
+            text += f"\nsolver={self._solver}"
+        nev = opts.nev()
+        vals = np.zeros(nev)
+        res = np.zeros(nev)
+        vecs = np.zeros((nev, self.n())) if want_vectors else None  # column-major n x nev
+        stats = np.zeros(8)
+        check(lib.fe_solve(self.A.handle, self.B.handle if self.B is not None else None,
+                           text.encode(), vals.ctypes.data, res.ctypes.data,
+                           vecs.ctypes.data if vecs is not None else None, stats.ctypes.data))
+        self._eigvals, self._resnrms = vals, res
+        self._eigvecs = vecs.T if vecs is not None else None
+        self._status = int(stats[1])
+        self._iters = int(stats[0])
+        self.stats = dict(iterations=int(stats[0]), status=int(stats[1]), seconds=float(stats[2]),
+                          spmm_launches=int(stats[3]), fp32_iterations=int(stats[4]),
+                          fp64_iterations=int(stats[5]), lower=float(stats[6]),
+                          upper=float(stats[7]))
+        return self._status
+
+    def eigenvalues(self) -> np.ndarray:
+        return self._eigvals
+
+    def eigenvectors(self) -> np.ndarray:
+        return self._eigvecs
+
+    def residual_norms(self) -> np.ndarray:
+        return self._resnrms
+
+    def status(self) -> int:
+        return self._status
+
+    def last_iterations(self):
+        return self._iters

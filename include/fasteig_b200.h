@@ -1,0 +1,201 @@
+/*
+ * fasteig_b200 — C ABI of the B200 (sm_100a) backend for fasteig's sparse
+ * symmetric eigensolver hot path.
+ *
+ * Conventions shared by every entry point:
+ *   - Return value: 0 on success, a negative FE_ERR_* code on failure.
+ *     fe_last_error() returns a message for the calling thread's last failure.
+ *     Errors never abort the process.
+ *   - Dense blocks ("multivectors") live in device memory ROW-MAJOR:
+ *     element (row i, column j) of a block with leading dimension ld is at
+ *     base[i * ld + j]. A column range is addressed by offsetting base.
+ *     (The reference stores column-major n-by-k blocks, ld = n,
+ *     src/gpu/CudaMultiVector.cpp:26-28; the row-major "slab" makes one CSR
+ *     row's neighbours contiguous 128-bit loads for SpMM.)
+ *   - Small matrices (Gram, rotation coefficients, Cholesky factors) are FP64,
+ *     column-major, in device memory, matching Eigen's MatrixXd convention
+ *     used by the reference's host-side small matrices.
+ *   - Every compute call is asynchronous on the given CUDA stream (a
+ *     cudaStream_t passed as void*, NULL = legacy default stream) and takes
+ *     caller-owned device pointers. Calls that need scratch space take a
+ *     caller-owned device workspace and report its size via *_workspace_bytes.
+ */
+#ifndef FASTEIG_B200_H
+#define FASTEIG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FE_OK 0
+#define FE_ERR_INVALID -1     /* invalid argument (shape, pointer, alignment) */
+#define FE_ERR_CUDA -2        /* CUDA runtime / library failure */
+#define FE_ERR_NOT_SPD -3     /* Cholesky rank loss (reference returns -1) */
+#define FE_ERR_NONFINITE -4   /* non-finite Ritz data / residuals */
+#define FE_ERR_ALLOC -5       /* device allocation failure */
+#define FE_ERR_UNSUPPORTED -6 /* option not supported by this backend */
+
+typedef struct fe_csr* fe_csr_t;
+
+/* Library identity and error reporting. */
+const char* fe_version(void);
+const char* fe_last_error(void);
+int fe_device_count(int* count);
+
+/* ---------------------------------------------------------------------
+ * CSR operator (replaces CudaCsrMatrix, src/gpu/CudaCsrMatrix.cpp:20-52,
+ * constructed from core::CsrMatrixData, include/core/CsrMatrix.hpp:18-27).
+ * The host arrays are validated exactly as validate_csr_matrix_data
+ * (src/core/CsrMatrix.cpp:11-39) and uploaded; FP64 and FP32 value copies
+ * are kept on the device.
+ * ------------------------------------------------------------------- */
+int fe_csr_create(int64_t rows, int64_t cols, int64_t nnz, const int32_t* rowptr,
+                  const int32_t* colind, const double* values, fe_csr_t* out);
+int fe_csr_destroy(fe_csr_t csr);
+int fe_csr_info(fe_csr_t csr, int64_t* rows, int64_t* cols, int64_t* nnz);
+/* Copies back the stored matrix (CsrMatrix::copy_to_host,
+ * include/core/CsrMatrix.hpp:35). Arrays must hold rows+1 / nnz / nnz items. */
+int fe_csr_copy_to_host(fe_csr_t csr, int32_t* rowptr, int32_t* colind, double* values);
+
+/* ---------------------------------------------------------------------
+ * Block SpMM (replaces LinearOperator::apply_block of a CSR matrix,
+ * include/core/LinearOperator.hpp:32-37; GPU: CudaCsrMatrix::apply_block,
+ * src/gpu/CudaCsrMatrix.cpp:196-223, a loop of ncols cuSPARSE SpMVs; CPU:
+ * CpuCsrMatrix::apply_block, src/core/CsrMatrix.cpp:209-245):
+ *     Y[:, 0:ncols] = alpha * A * X[:, 0:ncols] + beta * Y[:, 0:ncols]
+ * beta == 0 overwrites Y (NaN-safe), as the reference's setZero branch.
+ * X and Y must not overlap. _f32 computes with FP32 values and FP32
+ * accumulation on FP32 blocks.
+ * ------------------------------------------------------------------- */
+int fe_spmm_csr_f64(fe_csr_t A, const double* X, int64_t ldx, double* Y, int64_t ldy,
+                    int64_t ncols, double alpha, double beta, void* stream);
+int fe_spmm_csr_f32(fe_csr_t A, const float* X, int64_t ldx, float* Y, int64_t ldy,
+                    int64_t ncols, double alpha, double beta, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Fused Chebyshev three-term step (replaces the per-step copy_from +
+ * apply_block(2c, -1) + add_scaled_columns(2d) sequence of
+ * ChebyshevSolver::chebyshev_filter, src/ChebyshevSolver.cpp:243-256):
+ *     Yout = alpha * A * Ycur + gamma * Ycur + beta * Yprev
+ * Step 1 of the filter is (alpha, gamma, beta) = (c, d, 0) with Yprev unused;
+ * step k >= 2 is (2c, 2d, -1). Yout may alias Yprev (in-place update of the
+ * k-2 block); Ycur must not overlap Yout.
+ * ------------------------------------------------------------------- */
+int fe_cheb_step_f64(fe_csr_t A, const double* Ycur, const double* Yprev, double* Yout,
+                     int64_t ld, int64_t ncols, double alpha, double gamma, double beta,
+                     void* stream);
+int fe_cheb_step_f32(fe_csr_t A, const float* Ycur, const float* Yprev, float* Yout,
+                     int64_t ld, int64_t ncols, double alpha, double gamma, double beta,
+                     void* stream);
+/* Whole filter of degree `degree` in place on X (ChebyshevSolver::chebyshev_filter,
+ * src/ChebyshevSolver.cpp:223-258, with scaling (c, d) already computed);
+ * `scratch` is a second block of the same shape. */
+int fe_cheb_filter_f64(fe_csr_t A, double* X, double* scratch, int64_t ld, int64_t ncols,
+                       int32_t degree, double c, double d, void* stream);
+int fe_cheb_filter_f32(fe_csr_t A, float* X, float* scratch, int64_t ld, int64_t ncols,
+                       int32_t degree, double c, double d, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Gram G = X^T Y over all n rows (replaces MultiVector::transpose_multiply,
+ * src/gpu/CudaMultiVector.cpp:361-406, and the Gram Dgemm of Cholesky QR,
+ * src/core/Orthogonalization.cpp:202-209). X is n-by-k, Y is n-by-m; G is
+ * k-by-m FP64 column-major with leading dimension ldg. Products of the inputs
+ * are accumulated in FP64 (FP32 inputs: exact products, FP64 sums), split over
+ * row chunks whose partial Grams are reduced in a fixed order (deterministic).
+ * ------------------------------------------------------------------- */
+size_t fe_gram_workspace_bytes(int64_t n, int64_t k, int64_t m);
+int fe_gram_f64(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t n,
+                int64_t k, int64_t m, double* G, int64_t ldg, void* workspace,
+                size_t workspace_bytes, void* stream);
+int fe_gram_f32(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n,
+                int64_t k, int64_t m, double* G, int64_t ldg, void* workspace,
+                size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Rotation Y = alpha * X * C + beta * Y (replaces
+ * MultiVector::right_multiply_active_columns, src/gpu/CudaMultiVector.cpp:310-359,
+ * the triangular solve of Cholesky QR, src/core/Orthogonalization.cpp:227-235,
+ * applied as X * R^{-1}, and the X - V*H updates of block Gram-Schmidt,
+ * :554-601). X is n-by-k, C is k-by-m FP64 column-major (ldc), Y is n-by-m.
+ * _f32 rounds C to FP32 and accumulates in FP32. X and Y must not overlap.
+ * ------------------------------------------------------------------- */
+int fe_rotate_f64(const double* X, int64_t ldx, const double* C, int64_t ldc, double* Y,
+                  int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
+                  void* stream);
+int fe_rotate_f32(const float* X, int64_t ldx, const double* C, int64_t ldc, float* Y,
+                  int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
+                  void* stream);
+
+/* ---------------------------------------------------------------------
+ * Ritz residuals and column norms (replaces the copy + add_scaled_columns +
+ * 2 x column_norms sequence of extract_projected_ritz_pairs,
+ * src/core/RitzExtraction.cpp:125-139, and evaluate_ritz_pairs, :49-62):
+ *     R[:, j] = AX[:, j] - lambda[j] * MX[:, j]   (MX = X when BX is NULL)
+ *     rnorm[j] = ||R[:, j]||,  xnorm[j] = ||MX[:, j]||,
+ *     rel[j] = rnorm[j] / ((1 + |lambda[j]|) * xnorm[j])  (rnorm if the
+ *     denominator is not positive, as src/core/RitzExtraction.cpp:131-139).
+ * lambda, rnorm, xnorm, rel are FP64 device arrays of length m; R may be NULL
+ * (norms only). Norms are accumulated in FP64.
+ * ------------------------------------------------------------------- */
+size_t fe_residual_workspace_bytes(int64_t n, int64_t m);
+int fe_residual_norms_f64(const double* AX, const double* X, const double* BX, int64_t ld,
+                          int64_t n, int64_t m, const double* lambda, double* R, int64_t ldr,
+                          double* rnorm, double* xnorm, double* rel, void* workspace,
+                          size_t workspace_bytes, void* stream);
+int fe_residual_norms_f32(const float* AX, const float* X, const float* BX, int64_t ld,
+                          int64_t n, int64_t m, const double* lambda, float* R, int64_t ldr,
+                          double* rnorm, double* xnorm, double* rel, void* workspace,
+                          size_t workspace_bytes, void* stream);
+/* ||X[:, j]|| for j < m (MultiVector::column_norms, src/gpu/CudaMultiVector.cpp:435-474). */
+int fe_column_norms_f64(const double* X, int64_t ld, int64_t n, int64_t m, double* norms,
+                        void* workspace, size_t workspace_bytes, void* stream);
+int fe_column_norms_f32(const float* X, int64_t ld, int64_t n, int64_t m, double* norms,
+                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Small FP64 dense kernels (device-resident; replace cusolverDnDpotrf + its
+ * info device-to-host sync and cublasDtrsm, src/core/Orthogonalization.cpp:211-235).
+ * ------------------------------------------------------------------- */
+/* In place: upper Cholesky factor R of the k-by-k SPD matrix G (G = R^T R);
+ * the strictly lower part is zeroed. *info (device int) = 0 on success or
+ * j+1 when the j-th pivot is not positive/finite (rank loss: the reference's
+ * -1 return). */
+int fe_potrf_upper_f64(double* G, int64_t k, int64_t ldg, int32_t* info, void* stream);
+/* Rinv = R^{-1} for an upper-triangular k-by-k R (both column-major). */
+int fe_trinv_upper_f64(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
+                       void* stream);
+/* P = (P + P^T) / 2 in place (src/core/RitzExtraction.cpp:103). */
+int fe_symmetrize_f64(double* P, int64_t k, int64_t ldp, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Precision conversions between FP64 and FP32 blocks (row-major).
+ * ------------------------------------------------------------------- */
+int fe_convert_f64_to_f32(const double* src, int64_t lds, float* dst, int64_t ldd,
+                          int64_t n, int64_t m, void* stream);
+int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ldd,
+                          int64_t n, int64_t m, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Solver entry point (replaces fasteig_problem::solve for the Chebyshev,
+ * LOBPCG, Davidson and Krylov-Schur solvers on the CUDA executor,
+ * src/fasteig_problem.cpp:340-437, src/fasteig_solver.cpp:131-168).
+ * The problem is given as host CSR (full symmetric storage, as
+ * build_csr_from_sparse_matrix produces) and options as "key=value" lines
+ * with the reference's keys (src/fasteig_options.cpp:51-112: nev, maxiter,
+ * maxdim, maxblks, degree, which, solver, tol, seed, blksize) plus
+ * extensions (precision=fp64|mixed, block=<cols>, bounds=reference|ritz).
+ * Results: eigenvalues[nev], residual_norms[nev] (the reference's relative
+ * residual), eigenvectors n-by-nev column-major (may be NULL), stats[8] (may
+ * be NULL): iterations, status, solve seconds, SpMM launches, ...
+ * ------------------------------------------------------------------- */
+int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eigenvalues,
+             double* residual_norms, double* eigenvectors, double* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTEIG_B200_H */

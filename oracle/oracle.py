@@ -1,0 +1,823 @@
+"""CPU oracle for the fasteig sparse symmetric eigensolver hot path.
+
+TEST INFRASTRUCTURE ONLY. Nothing in the product path (``fasteig_b200``) may
+import, call or link this module. It is imported by ``tests/``, by
+``__graft_entry__.smoke()`` as the checker, and by ``bench.py``'s
+``cpu_baseline`` leg / ``--impl reference`` arm, where it stands in for the
+reference's CPU (Eigen) path, which cannot be compiled here because Eigen 3.4
+is not installed (the reference fetches it over the network,
+CMakeLists.txt:216,233-240).
+
+It is a plain FP64 NumPy/SciPy restatement of the reference's CPU backend.
+Every function names the reference file:line it follows (paths relative to
+the fasteig project root). Third-party arithmetic used by the reference
+(Eigen 3.4.0: ``SelfAdjointEigenSolver``, ``LLT``, ``HouseholderQR``,
+``JacobiSVD``) is restated with the equivalent LAPACK routines through NumPy:
+``eigh`` (syevd), ``cholesky`` (potrf), ``qr`` (geqrf/orgqr, same Householder
+sign convention as Eigen's ``makeHouseholder``), ``svd`` (gesdd).
+
+Parity pins (see tests/test_oracle_golden.py):
+  * tests/reference/SiO.out.121mpi (33,401 ScaLAPACK eigenvalues of SiO.mtx):
+    SR k=5 via Chebyshev, LOBPCG, Davidson and Krylov-Schur, checked with the
+    reference harness's rule |dl| <= 1e-10 + 1e-10 |l_ref| and residual <= 1e-8
+    (tests/scripts/run_case.py:246-260).
+  * tests/reference/KuuMuu_eig.txt (7,102 generalized eigenvalues).
+  * std::mt19937 / uniform_real_distribution bit-exact against a g++ build of
+    oracle/rng_golden.cpp.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+import scipy.sparse as sp
+
+EPS = np.finfo(np.float64).eps
+
+# --------------------------------------------------------------------------
+# Random initial blocks: src/core/Executor.cpp:20-62
+# std::mt19937(seed) + std::uniform_real_distribution<double>(-1, 1), with
+# libstdc++'s generate_canonical<double, 53> drawing two 32-bit words per value
+# (low word first). Column-major fill order.
+# --------------------------------------------------------------------------
+
+
+def mt19937_uniform(count: int, seed: int) -> np.ndarray:
+    """``count`` draws of uniform_real_distribution<double>(-1,1) from mt19937(seed)."""
+    bg = np.random.MT19937(0)
+    bg._legacy_seeding(int(seed) & 0xFFFFFFFF)  # init_genrand(seed): std::mt19937(seed)
+    raw = bg.random_raw(2 * count).astype(np.float64).reshape(count, 2)
+    canon = (raw[:, 0] + raw[:, 1] * 4294967296.0) / 18446744073709551616.0
+    canon = np.where(canon >= 1.0, np.nextafter(1.0, 0.0), canon)
+    return 2.0 * canon - 1.0
+
+
+def random_block(rows: int, cols: int, seed: int = 1) -> np.ndarray:
+    """Executor::create_random_multivector (src/core/Executor.cpp:44-62)."""
+    if rows <= 0 or cols <= 0:
+        raise ValueError("Executor::create_random_multivector: dimensions must be positive.")
+    v = mt19937_uniform(rows * cols, seed)
+    return v.reshape(cols, rows).T.copy()  # column-major fill
+
+
+def random_vector(size: int, seed: int = 1) -> np.ndarray:
+    """Executor::create_random_vector (src/core/Executor.cpp:20-34)."""
+    if size <= 0:
+        raise ValueError("Executor::create_random_vector: size must be positive.")
+    return mt19937_uniform(size, seed)
+
+
+# --------------------------------------------------------------------------
+# CSR matrices: include/core/CsrMatrix.hpp:18-27, src/core/CsrMatrix.cpp
+# --------------------------------------------------------------------------
+
+
+@dataclass
+class Csr:
+    rows: int
+    cols: int
+    rowptr: np.ndarray  # int32, rows+1
+    colind: np.ndarray  # int32, nnz
+    values: np.ndarray  # float64, nnz
+    _sp: Optional[sp.csr_matrix] = field(default=None, repr=False)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.values.size)
+
+    def scipy(self) -> sp.csr_matrix:
+        if self._sp is None:
+            self._sp = sp.csr_matrix((self.values, self.colind, self.rowptr),
+                                     shape=(self.rows, self.cols))
+        return self._sp
+
+
+def validate_csr(A: Csr) -> None:
+    """validate_csr_matrix_data (src/core/CsrMatrix.cpp:11-39)."""
+    if A.rows < 0 or A.cols < 0:
+        raise ValueError("CsrMatrixData: dimensions must be nonnegative.")
+    if A.rowptr.size != A.rows + 1:
+        raise ValueError("CsrMatrixData: rowptr size must be rows + 1.")
+    if A.colind.size != A.values.size:
+        raise ValueError("CsrMatrixData: colind and values sizes differ.")
+    if A.rowptr.size and A.rowptr[0] != 0:
+        raise ValueError("CsrMatrixData: rowptr must start at zero.")
+    if A.rowptr.size and A.rowptr[-1] != A.values.size:
+        raise ValueError("CsrMatrixData: rowptr end must equal nnz.")
+    if np.any(np.diff(A.rowptr) < 0):
+        raise ValueError("CsrMatrixData: rowptr must be nondecreasing.")
+    if A.colind.size and (A.colind.min() < 0 or A.colind.max() >= A.cols):
+        raise ValueError("CsrMatrixData: column index out of range.")
+
+
+def csr_from_triplets(n: int, rows, cols, vals, expand_symmetric: bool) -> Csr:
+    """Symmetric expansion and duplicate summation of a triangle.
+
+    fasteig_problem::build_sparse_matrix_from_triplets (src/fasteig_problem.cpp:474-506)
+    and build_csr_from_sparse_matrix (src/fasteig_problem.cpp:554-607): every
+    off-diagonal (r,c,v) also contributes (c,r,v); duplicates are summed; rows
+    are sorted by column (Eigen row-major compressed storage).
+    """
+    rows = np.asarray(rows, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    vals = np.asarray(vals, dtype=np.float64)
+    if expand_symmetric:
+        off = rows != cols
+        rows, cols, vals = (np.concatenate([rows, cols[off]]),
+                            np.concatenate([cols, rows[off]]),
+                            np.concatenate([vals, vals[off]]))
+    m = sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
+    m.sum_duplicates()
+    m.sort_indices()
+    return Csr(n, n, m.indptr.astype(np.int32), m.indices.astype(np.int32),
+               m.data.astype(np.float64))
+
+
+def read_mtx(path) -> Csr:
+    """MatrixMarket coordinate real {general,symmetric} reader (src/mmio.cpp:96 banner;
+    1-based indices; symmetric files store one triangle and are expanded as in
+    src/fasteig_problem.cpp:579-596)."""
+    with open(path, "r") as f:
+        banner = f.readline().lower().split()
+        if len(banner) < 5 or banner[0] != "%%matrixmarket" or banner[2] != "coordinate":
+            raise ValueError(f"{path}: unsupported MatrixMarket banner")
+        symmetric = banner[4] == "symmetric"
+        line = f.readline()
+        while line.startswith("%"):
+            line = f.readline()
+        nr, nc, nz = (int(t) for t in line.split())
+        data = np.loadtxt(f, dtype=np.float64, ndmin=2, max_rows=nz)
+    if nr != nc:
+        raise ValueError("CSR conversion requires a square matrix.")
+    return csr_from_triplets(nr, data[:, 0].astype(np.int64) - 1,
+                             data[:, 1].astype(np.int64) - 1, data[:, 2], symmetric)
+
+
+def csr_apply_block(A: Csr, X: np.ndarray, first_col: int, block: int, Y: np.ndarray,
+                    alpha: float = 1.0, beta: float = 0.0) -> None:
+    """CpuCsrMatrix::apply_block (src/core/CsrMatrix.cpp:209-245):
+    Y[:, :block] = beta*Y[:, :block] + alpha*A*X[:, first:first+block]; beta == 0
+    overwrites (NaN-safe)."""
+    if first_col < 0 or block <= 0 or first_col + block > X.shape[1]:
+        raise ValueError("CpuCsrMatrix::apply_block: invalid column range.")
+    if X.shape[0] != A.cols or Y.shape[0] != A.rows or Y.shape[1] < block:
+        raise ValueError("CpuCsrMatrix::apply_block: dimension mismatch.")
+    prod = A.scipy() @ X[:, first_col:first_col + block]
+    if beta == 0.0:
+        Y[:, :block] = alpha * prod
+    else:
+        Y[:, :block] = beta * Y[:, :block] + alpha * prod
+
+
+def csr_spmm_reference_loop(A: Csr, X: np.ndarray, alpha: float, beta: float,
+                            Y: np.ndarray) -> np.ndarray:
+    """Literal row loop of src/core/CsrMatrix.cpp:227-244 (small cases only):
+    scale Y by beta (or zero it), then for each nonzero in CSR order add
+    (alpha*a) * X[col, :] to the row."""
+    out = np.zeros_like(Y) if beta == 0.0 else beta * Y
+    for r in range(A.rows):
+        for k in range(A.rowptr[r], A.rowptr[r + 1]):
+            out[r, :] += (alpha * A.values[k]) * X[A.colind[k], :]
+    return out
+
+
+# --------------------------------------------------------------------------
+# QR factorizations: src/core/Orthogonalization.cpp
+# --------------------------------------------------------------------------
+
+
+def cholesky_qr(X: np.ndarray, gram: Optional[np.ndarray] = None):
+    """cholesky_qr / cholesky_qr_from_gram (src/core/Orthogonalization.cpp:49-57,290-297).
+    Returns (info, Q, R); info = -1 on rank loss (LLT failure)."""
+    if gram is None:
+        gram = X.T @ X
+    try:
+        L = np.linalg.cholesky(gram)
+    except np.linalg.LinAlgError:
+        return -1, None, None
+    R = L.T
+    Q = np.linalg.solve(R.T, X.T).T  # X * R^{-1}
+    return 0, Q, R
+
+
+def cholesky_qr2(X: np.ndarray):
+    """cholesky_qr2 (src/core/Orthogonalization.cpp:299-315)."""
+    info, q1, r1 = cholesky_qr(X)
+    if info != 0:
+        return info, None, None
+    info, Q, r2 = cholesky_qr(q1)
+    if info != 0:
+        return info, None, None
+    return 0, Q, r2 @ r1
+
+
+def householder_qr(X: np.ndarray):
+    """householder_qr (src/core/Orthogonalization.cpp:339-354): thin Q and upper R."""
+    Q, R = np.linalg.qr(X, mode="reduced")
+    return 0, Q, np.triu(R)
+
+
+def weighted_cholesky_qr(X: np.ndarray, BX: np.ndarray):
+    """B-weighted Cholesky QR (src/core/Orthogonalization.cpp:407-440): gram = X^T (BX),
+    symmetrized before the factorization."""
+    gram = X.T @ BX
+    gram = 0.5 * (gram + gram.T)
+    return cholesky_qr(X, gram)
+
+
+def block_gram_schmidt(V: np.ndarray, k: int, S: np.ndarray, dual: Optional[np.ndarray] = None):
+    """block_gram_schmidt (src/core/Orthogonalization.cpp:482-527): two-pass classical
+    block GS of S against V[:, :k]. Returns (info, residual, H)."""
+    if k == 0:
+        return 0, S.copy(), np.zeros((0, S.shape[1]))
+    Vk = V[:, :k]
+    BV = (dual if dual is not None else V)[:, :k]
+    H = BV.T @ S
+    R = S - Vk @ H
+    S2 = BV.T @ R
+    H = H + S2
+    R = R - Vk @ S2
+    return 0, R, H
+
+
+def orthonormalize_block(basis: np.ndarray, k: int, source: np.ndarray,
+                         rank_tolerance: float = 1e-12) -> Optional[np.ndarray]:
+    """orthonormalize_block (src/core/Orthogonalization.cpp:717-775)."""
+    n = source.shape[0]
+    if k == n:
+        return None
+    current = source
+    result = None
+    for _ in range(2):
+        norms = np.linalg.norm(current, axis=0)
+        if not np.all(np.isfinite(norms)):
+            raise RuntimeError("orthonormalize_block: non-finite column norms.")
+        scale = norms.max()
+        if scale == 0.0:
+            return None
+        _, orth, _ = block_gram_schmidt(basis, k, current)
+        _, Q, R = householder_qr(orth)
+        U, s, _ = np.linalg.svd(R)
+        capacity = min(current.shape[1], n - k)
+        rank = 0
+        while rank < capacity and s[rank] > rank_tolerance * scale:
+            rank += 1
+        if rank == 0:
+            return None
+        result = Q @ U[:, :rank]
+        current = result
+    return result
+
+
+# --------------------------------------------------------------------------
+# Ritz extraction: src/core/RitzExtraction.cpp, include/fasteig_solver.hpp:58-82
+# --------------------------------------------------------------------------
+
+
+def sort_indices(v: np.ndarray, which: str) -> np.ndarray:
+    """sort_indices (include/fasteig_solver.hpp:58-82): stable sorts."""
+    if which == "sr":
+        return np.argsort(v, kind="stable")
+    if which == "lr":
+        return np.argsort(-v, kind="stable")
+    if which == "sm":
+        return np.argsort(np.abs(v), kind="stable")
+    if which in ("lm", "sai"):
+        return np.argsort(-np.abs(v), kind="stable")
+    return np.arange(v.size)
+
+
+def select_ritz_indices(values: np.ndarray, which: str) -> np.ndarray:
+    """lanczos_select_ritz_indices (src/core/RitzExtraction.cpp:162-179), incl. BE."""
+    m = values.size
+    if which == "be":
+        idx = []
+        for i in range(m // 2):
+            idx.append(m - 1 - i)
+            idx.append(i)
+        if m % 2 == 1:
+            idx.append(m // 2)
+        return np.asarray(idx, dtype=np.int64)
+    return sort_indices(values, which)
+
+
+@dataclass
+class RitzPairs:
+    values: np.ndarray
+    relative_residuals: np.ndarray
+    coefficients: np.ndarray
+    vectors: np.ndarray
+    operator_vectors: np.ndarray
+    residuals: np.ndarray
+
+
+def extract_projected_ritz_pairs(projected: np.ndarray, basis: np.ndarray,
+                                 operator_basis: np.ndarray, active: int, requested: int,
+                                 which: str) -> RitzPairs:
+    """extract_projected_ritz_pairs (src/core/RitzExtraction.cpp:65-141)."""
+    m = active
+    P = projected[:m, :m]
+    P = 0.5 * (P + P.T)
+    w, Z = np.linalg.eigh(P)
+    idx = select_ritz_indices(w, which)[:requested]
+    vals = w[idx]
+    C = Z[:, idx]
+    Xr = basis[:, :m] @ C
+    AXr = operator_basis[:, :m] @ C
+    Rs = AXr - Xr * vals[None, :]
+    rn = np.linalg.norm(Rs, axis=0)
+    xn = np.linalg.norm(Xr, axis=0)
+    den = (1.0 + np.abs(vals)) * xn
+    rel = np.where(den > 0.0, rn / np.where(den > 0.0, den, 1.0), rn)
+    return RitzPairs(vals, rel, C, Xr, AXr, Rs)
+
+
+def evaluate_ritz_pairs(A: Csr, B: Optional[Csr], basis: np.ndarray, active: int,
+                        lam: np.ndarray, Csel: np.ndarray):
+    """evaluate_ritz_pairs (src/core/RitzExtraction.cpp:34-63): returns (Y, rel)."""
+    Y = basis[:, :active] @ Csel
+    AY = A.scipy() @ Y
+    BY = (B.scipy() @ Y) if B is not None else Y.copy()
+    bn = np.linalg.norm(BY, axis=0)
+    R = AY - BY * lam[None, :]
+    res = np.linalg.norm(R, axis=0)
+    den = (1.0 + np.abs(lam)) * bn
+    if np.any(~(den > 0.0)) or not np.all(np.isfinite(den)) or not np.all(np.isfinite(res)):
+        raise RuntimeError("evaluate_ritz_pairs: invalid vector or non-finite residual.")
+    return Y, res / den
+
+
+def residual_norms(A: Csr, B: Optional[Csr], lam: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """fasteig_solver::compute_residual_norms (src/fasteig_solver.cpp:89-129):
+    ||Ax - l Bx|| / ((1+|l|) ||Bx||) (B = I when absent)."""
+    AX = A.scipy() @ X
+    BX = (B.scipy() @ X) if B is not None else X
+    num = np.linalg.norm(AX - BX * lam[None, :], axis=0)
+    den = (1.0 + np.abs(lam)) * np.linalg.norm(BX, axis=0)
+    return np.where(den > 0.0, num / np.where(den > 0.0, den, 1.0), num)
+
+
+def residual_norms_baseline_def(A: Csr, B: Optional[Csr], lam: np.ndarray,
+                                X: np.ndarray) -> np.ndarray:
+    """The second residual definition reported beside the reference one:
+    ||Kx - l Mx|| / (|l| ||Mx||)."""
+    AX = A.scipy() @ X
+    BX = (B.scipy() @ X) if B is not None else X
+    num = np.linalg.norm(AX - BX * lam[None, :], axis=0)
+    den = np.abs(lam) * np.linalg.norm(BX, axis=0)
+    return np.where(den > 0.0, num / np.where(den > 0.0, den, 1.0), num)
+
+
+# --------------------------------------------------------------------------
+# Lanczos / Krylov subspace: src/core/KrylovSubspace.cpp:112-259,
+# src/core/LanczosWorkspace.cpp:25-107
+# --------------------------------------------------------------------------
+
+
+class _Lanczos:
+    """Scalar Lanczos with two-pass classical reorthogonalization, as built by
+    KrylovSubspace::build_one (src/core/KrylovSubspace.cpp:125-131) and recorded by
+    CpuLanczosWorkspace::record_step (src/core/LanczosWorkspace.cpp:25-40)."""
+
+    def __init__(self, A_apply, residual: np.ndarray, m: int, restart_seed: int,
+                 B_apply=None):
+        self.A_apply = A_apply
+        self.B_apply = B_apply
+        self.f = residual.copy()
+        self.n = residual.size
+        self.V = np.zeros((self.n, m))
+        self.BV = np.zeros((self.n, m)) if B_apply is not None else None
+        self.Bf = None
+        self.T = np.zeros((m, m))
+        self.beta_next = 0.0
+        self.restart_row = -1
+        self.seed = restart_seed
+        self.restarted = False
+
+    def residual_norm(self) -> float:
+        """KrylovSubspace::residual_norm (src/core/KrylovSubspace.cpp:162-178)."""
+        if self.B_apply is not None:
+            self.Bf = self.B_apply(self.f)
+            sq = float(self.f @ self.Bf)
+            if not math.isfinite(sq) or sq < 0.0:
+                raise RuntimeError("B must be positive definite (invalid B-norm).")
+            return math.sqrt(sq)
+        return float(np.linalg.norm(self.f))
+
+    def orthogonalize(self, k: int, src: np.ndarray) -> tuple[np.ndarray, float]:
+        """CpuMultiVector::orthogonalize_active_columns (src/core/MultiVector.cpp:153-185)."""
+        if k == 0:
+            return src.copy(), 0.0
+        Vk = self.V[:, :k]
+        W = self.BV[:, :k] if self.BV is not None else Vk
+        h = W.T @ src
+        r = src - Vk @ h
+        s = W.T @ r
+        r = r - Vk @ s
+        h = h + s
+        return r, float(h[k - 1])
+
+    def normalize_or_restart(self, it: int) -> float:
+        """src/core/KrylovSubspace.cpp:232-259."""
+        self.restarted = False
+        beta = self.residual_norm()
+        if not math.isfinite(beta):
+            raise RuntimeError("non-finite residual norm encountered.")
+        if beta > EPS:
+            return beta
+        cand = random_vector(self.n, self.seed + it + 1)
+        self.f, _ = self.orthogonalize(it, cand)
+        self.restarted = True
+        beta = self.residual_norm()
+        if beta <= EPS:
+            raise RuntimeError("breakdown, unable to generate new basis vector.")
+        return beta
+
+    def step(self, it: int) -> None:
+        beta = self.normalize_or_restart(it)
+        self.f = self.f / beta
+        self.V[:, it] = self.f
+        if self.BV is not None:
+            self.BV[:, it] = self.Bf / beta
+        rec_beta = 0.0 if self.restarted else beta
+        w = self.A_apply(self.V[:, it])
+        self.f, alpha = self.orthogonalize(it + 1, w)
+        beta_next = self.residual_norm()
+        if not math.isfinite(beta_next):
+            raise RuntimeError("non-finite next residual norm encountered.")
+        self.record(it, rec_beta, alpha, beta_next)
+
+    def record(self, it, beta, alpha, beta_next):
+        if it != 0 and it != self.restart_row:
+            self.T[it, it - 1] = beta
+            self.T[it - 1, it] = beta
+        self.T[it, it] = alpha
+        self.beta_next = beta_next
+        if it == self.restart_row:
+            self.restart_row = -1
+
+    def snapshot(self, m: int, nev: int, which: str):
+        """lanczos_compute_cpu_snapshot + lanczos_make_snapshot_from_eigendecomp
+        (src/core/RitzExtraction.cpp:181-217,252-266)."""
+        w, Z = np.linalg.eigh(self.T[:m, :m])
+        idx = select_ritz_indices(w, which)[:min(nev, m)]
+        lam = w[idx]
+        rel = np.abs(self.beta_next * Z[m - 1, idx]) / (1.0 + np.abs(lam))
+        return lam, rel, Z[:, idx]
+
+
+def estimate_bounds(A_apply, n: int, seed: int) -> tuple[float, float]:
+    """estimate_bounds_with_executor (src/ChebyshevSolver.cpp:26-49) with
+    lanczos_absolute_residuals (src/core/RitzExtraction.cpp:435-441)."""
+    steps = min(20, n)
+    lz = _Lanczos(A_apply, random_vector(n, seed), steps, seed)
+    for it in range(steps):
+        lz.step(it)
+    lam, rel, _ = lz.snapshot(steps, steps, "sr")
+    r = rel * (1.0 + np.abs(lam))
+    lower = float((lam - r).min())
+    upper = float((lam + r).max())
+    if not (math.isfinite(lower) and math.isfinite(upper)) or lower > upper:
+        raise RuntimeError("ChebyshevSolver: invalid spectral bound estimates.")
+    return lower, upper
+
+
+# --------------------------------------------------------------------------
+# Solvers
+# --------------------------------------------------------------------------
+
+
+@dataclass
+class SolveResult:
+    eigenvalues: np.ndarray
+    eigenvectors: np.ndarray
+    residual_norms: np.ndarray
+    iterations: int
+    status: int = 0
+    history: list = field(default_factory=list)
+
+
+def chebyshev_filter_coefficients(lower: float, upper: float, degree: int):
+    """Filter scaling of ChebyshevSolver::chebyshev_filter (src/ChebyshevSolver.cpp:231-239).
+    Returns (c, d) of the mapped operator c*H + d*I, or None for a collapsed spectrum."""
+    if upper == lower:
+        return None
+    amplification = 1.0e3
+    xlb = math.cosh(math.acosh(amplification) / degree)
+    cutoff = (2.0 * lower + upper * (xlb - 1.0)) / (1.0 + xlb)
+    c = 2.0 / (upper - cutoff)
+    d = -(upper + cutoff) / (upper - cutoff)
+    if not (math.isfinite(c) and math.isfinite(d)):
+        raise RuntimeError("ChebyshevSolver: invalid filter scaling.")
+    return c, d
+
+
+def chebyshev_filter(H_apply, X: np.ndarray, degree: int, lower: float, upper: float) -> np.ndarray:
+    """ChebyshevSolver::chebyshev_filter (src/ChebyshevSolver.cpp:223-258):
+    Y0 = X, Y1 = (cH + dI) X, Yk = 2 (cH + dI) Y_{k-1} - Y_{k-2}."""
+    cd = chebyshev_filter_coefficients(lower, upper, degree)
+    if cd is None:
+        return X
+    c, d = cd
+    prev = X
+    cur = c * H_apply(X) + d * X
+    for _ in range(2, degree + 1):
+        nxt = 2.0 * c * H_apply(cur) + 2.0 * d * cur - prev
+        prev, cur = cur, nxt
+    return cur
+
+
+def chebyshev_filter_window(H_apply, X: np.ndarray, degree: int, cutoff: float,
+                            upper: float) -> np.ndarray:
+    """Three-term filter damping [cutoff, upper] into [-1, 1] (adaptive-interval
+    extension; same recurrence as src/ChebyshevSolver.cpp:243-256)."""
+    if upper <= cutoff:
+        return X
+    c = 2.0 / (upper - cutoff)
+    d = -(upper + cutoff) / (upper - cutoff)
+    prev = X
+    cur = c * H_apply(X) + d * X
+    for _ in range(2, degree + 1):
+        nxt = 2.0 * c * H_apply(cur) + 2.0 * d * cur - prev
+        prev, cur = cur, nxt
+    return cur
+
+
+def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
+                    maxiter: int = 1000, which: str = "sr", seed: int = 1,
+                    block: Optional[int] = None, record_history: bool = False,
+                    bounds: str = "reference", amplification: float = math.inf) -> SolveResult:
+    """ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221).
+
+    ``block`` overrides the subspace capacity ``nev + min(nev, n - nev)``
+    (src/ChebyshevSolver.cpp:94); None keeps the reference behaviour.
+    ``bounds="ritz"`` is the adaptive-interval extension (not in the reference):
+    after each Rayleigh-Ritz the damped interval is [theta_max, upper], where
+    theta_max is the largest Ritz value of the subspace (Zhou & Saad, 2007), and
+    the cutoff is lowered where needed so that the filter's amplification at
+    the Lanczos lower bound stays within ``amplification``."""
+    n = A.rows
+    which = which.lower()
+    if n <= 0 or nev <= 0 or nev > n:
+        raise ValueError("ChebyshevSolver: nev must be in [1,n].")
+    if which not in ("sr", "lr"):
+        raise ValueError("ChebyshevSolver: only SR and LR are supported.")
+    sign = -1.0 if which == "lr" else 1.0
+    Hs = A.scipy()
+    H_apply = (lambda X: sign * (Hs @ X))
+    capacity = nev + min(nev, n - nev) if block is None else max(nev, min(block, n))
+    vectors = random_block(n, capacity, seed)
+    info, vectors, _ = cholesky_qr(vectors)
+    if info != 0:
+        raise RuntimeError("ChebyshevSolver: initial Cholesky QR failed.")
+    lower, upper = estimate_bounds(lambda v: sign * (Hs @ v), n, seed)
+
+    locked = 0
+    subspace_cols = nev
+    ritz = None
+    it_done = 0
+    history = []
+    for it in range(maxiter):
+        active = subspace_cols - locked
+        if bounds == "ritz" and ritz is not None:
+            cutoff = float(ritz.values[subspace_cols_prev - 1])
+            if math.isfinite(amplification):
+                xl = math.cosh(math.acosh(amplification) / degree)
+                cutoff = min(cutoff, (2.0 * lower + upper * (xl - 1.0)) / (1.0 + xl))
+            filtered = chebyshev_filter_window(H_apply, vectors[:, locked:locked + active].copy(),
+                                               degree, cutoff, upper)
+        else:
+            filtered = chebyshev_filter(H_apply, vectors[:, locked:locked + active].copy(),
+                                        degree, lower, upper)
+        if locked > 0:
+            _, filtered, _ = block_gram_schmidt(vectors, locked, filtered)
+        vectors[:, locked:locked + active] = filtered
+        basis = vectors[:, :subspace_cols].copy()
+        info, basis, _ = cholesky_qr(basis)
+        if info != 0:
+            raise RuntimeError("ChebyshevSolver: Cholesky QR failed during filtering.")
+        op_basis = H_apply(basis)
+        projected = basis.T @ op_basis
+        ritz = extract_projected_ritz_pairs(projected, basis, op_basis, subspace_cols,
+                                            subspace_cols, "sr")
+        if not (np.all(np.isfinite(ritz.values)) and np.all(np.isfinite(ritz.relative_residuals))):
+            raise RuntimeError("ChebyshevSolver: non-finite Ritz values or residuals.")
+        vectors[:, :subspace_cols] = ritz.vectors
+        subspace_cols_prev = subspace_cols
+        locked = 0
+        while locked < nev and ritz.relative_residuals[locked] <= tol:
+            locked += 1
+        subspace_cols = max(subspace_cols, nev + min(locked, capacity - nev))
+        it_done = it + 1
+        if record_history:
+            history.append((sign * ritz.values[:nev].copy(), ritz.relative_residuals[:nev].copy()))
+        if ritz.relative_residuals[:nev].max() <= tol:
+            break
+    return SolveResult(sign * ritz.values[:nev], ritz.vectors[:, :nev].copy(),
+                       ritz.relative_residuals[:nev].copy(), it_done, 0, history)
+
+
+def lobpcg_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
+                 which: str = "sr", seed: int = 1) -> SolveResult:
+    """LOBPCGSolver::solve (src/LOBPCGSolver.cpp:25-174): unpreconditioned LOBPCG,
+    block width nev, soft locking."""
+    n = A.rows
+    which = which.lower()
+    if n <= 0 or nev <= 0 or nev > n or maxiter <= 0:
+        raise ValueError("LOBPCGSolver: require 0 < nev <= n and maxiter > 0.")
+    if which not in ("sr", "lr"):
+        raise ValueError("LOBPCGSolver: only SR and LR are supported.")
+    sign = -1.0 if which == "lr" else 1.0
+    Hs = A.scipy()
+    H_apply = (lambda X: sign * (Hs @ X))
+    X = random_block(n, nev, seed)
+    _, X, _ = householder_qr(X)
+    capacity = min(n, 3 * nev)
+    AX = H_apply(X)
+    ritz = extract_projected_ritz_pairs(X.T @ AX, X, AX, nev, nev, "sr")
+    X = ritz.vectors
+    P = None
+    it_done = 0
+    for it in range(maxiter):
+        if not (np.all(np.isfinite(ritz.values)) and np.all(np.isfinite(ritz.relative_residuals))):
+            raise RuntimeError("LOBPCGSolver: non-finite Ritz values or residuals.")
+        if ritz.relative_residuals.max() <= tol:
+            break
+        active = [j for j in range(nev) if ritz.relative_residuals[j] > tol]
+        W_source = ritz.residuals[:, active]
+        _, X, _ = householder_qr(X)
+        basis = np.zeros((n, capacity))
+        basis[:, :nev] = X
+        cols = nev
+        W = orthonormalize_block(basis, cols, W_source)
+        if W is not None:
+            basis[:, cols:cols + W.shape[1]] = W
+            cols += W.shape[1]
+        if P is not None and cols < capacity:
+            Po = orthonormalize_block(basis, cols, P[:, active])
+            if Po is not None:
+                take = Po.shape[1]
+                basis[:, cols:cols + take] = Po
+                cols += take
+        op_basis = H_apply(basis[:, :cols])
+        projected = basis[:, :cols].T @ op_basis
+        ritz = extract_projected_ritz_pairs(projected, basis, op_basis, cols, nev, "sr")
+        if not (np.all(np.isfinite(ritz.values)) and np.all(np.isfinite(ritz.relative_residuals))):
+            raise RuntimeError("LOBPCGSolver: non-finite Ritz values or residuals.")
+        dc = ritz.coefficients.copy()
+        dc[:nev, :] = 0.0
+        P = basis[:, :cols] @ dc
+        X = ritz.vectors
+        it_done = it + 1
+        if ritz.relative_residuals.max() <= tol or cols == nev:
+            break
+    return SolveResult(sign * ritz.values, X.copy(), ritz.relative_residuals.copy(), it_done)
+
+
+def davidson_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
+                   which: str = "sr", seed: int = 1, maxblks: int = 10) -> SolveResult:
+    """DavidsonSolver::solve (src/DavidsonSolver.cpp:27-264): block Davidson with thick
+    restart and unpreconditioned corrections; locktol = min(1e-5, tol) (:126)."""
+    n = A.rows
+    which = which.lower()
+    if nev <= 0 or nev > n:
+        raise ValueError("DavidsonSolver: nev must be in [1,n].")
+    Hs = A.scipy()
+    H_apply = (lambda X: Hs @ X)
+    V0 = random_block(n, nev, seed)
+    info, V0, _ = cholesky_qr(V0)
+    if info != 0:
+        raise RuntimeError("DavidsonSolver: initial Cholesky QR failed.")
+    max_cols = min(n, maxblks * nev)
+    AV0 = H_apply(V0)
+    ritz = extract_projected_ritz_pairs(V0.T @ AV0, V0, AV0, nev, nev, which)
+    locktol = min(1.0e-5, tol)
+    it_done = 0
+    for it in range(maxiter):
+        _, Xr, _ = householder_qr(ritz.vectors)
+        AXr = H_apply(Xr)
+        basis = np.zeros((n, max_cols))
+        op_basis = np.zeros((n, max_cols))
+        basis[:, :nev] = Xr
+        op_basis[:, :nev] = AXr
+        projected = np.zeros((max_cols, max_cols))
+        projected[:nev, :nev] = Xr.T @ AXr
+        cols = nev
+        ritz = extract_projected_ritz_pairs(projected, basis, op_basis, nev, nev, which)
+        for _blk in range(1, maxblks):
+            active = [j for j in range(nev) if ritz.relative_residuals[j] > locktol]
+            cc = len(active)
+            if cc == 0 or cols + cc > max_cols:
+                break
+            src = ritz.residuals[:, active]
+            _, corr, _ = block_gram_schmidt(basis, cols, src)
+            _, corr, _ = householder_qr(corr)
+            Acorr = H_apply(corr)
+            cross = basis[:, :cols].T @ Acorr
+            diag = corr.T @ Acorr
+            diag = 0.5 * (diag + diag.T)
+            projected[:cols, cols:cols + cc] = cross
+            projected[cols:cols + cc, :cols] = cross.T
+            projected[cols:cols + cc, cols:cols + cc] = diag
+            basis[:, cols:cols + cc] = corr
+            op_basis[:, cols:cols + cc] = Acorr
+            cols += cc
+            ritz = extract_projected_ritz_pairs(projected, basis, op_basis, cols, nev, which)
+        it_done = it + 1
+        if ritz.relative_residuals.size > 0 and ritz.relative_residuals.max() < tol:
+            break
+    return SolveResult(ritz.values.copy(), ritz.vectors.copy(),
+                       ritz.relative_residuals.copy(), it_done)
+
+
+def krylov_schur_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
+                       which: str = "sr", seed: int = 1, maxdim: int = 0,
+                       B: Optional[Csr] = None) -> SolveResult:
+    """KrylovSchurSolver::solve (src/KrylovSchurSolver.cpp:28-160), standard problems
+    (B is None) and the B-metric Lanczos of src/core/KrylovSubspace.cpp:162-178 with an
+    explicit B^{-1}A operator for generalized problems (the reference's cuDSS/LU
+    factorization is replaced by a sparse direct solve here)."""
+    n = A.rows
+    which = which.lower()
+    m = min(max(2 * nev, 20, maxdim), n)
+    Hs = A.scipy()
+    if B is None:
+        A_apply = (lambda v: Hs @ v)
+        B_apply = None
+    else:
+        import scipy.sparse.linalg as spla
+        lu = spla.splu(B.scipy().tocsc())
+        Bs = B.scipy()
+        A_apply = (lambda v: lu.solve(Hs @ v))
+        B_apply = (lambda v: Bs @ v)
+    lz = _Lanczos(A_apply, random_vector(n, seed), m, seed, B_apply)
+    for col in range(m):
+        lz.step(col)
+    for it in range(1, maxiter + 1):
+        w, Z = np.linalg.eigh(lz.T[:m, :m])
+        idx = select_ritz_indices(w, which)
+        lam_all = w[idx]
+        C_all = Z[:, idx]
+        rel_all = np.abs(lz.beta_next * Z[m - 1, idx]) / (1.0 + np.abs(lam_all))
+        nconv = 0
+        for j in range(nev):
+            mag = abs(lam_all[j])
+            ok = (rel_all[j] <= tol) if B is not None else (rel_all[j] * (1.0 + mag) < tol * mag)
+            nconv += int(ok)
+        at_limit = (m == n) or (it == maxiter)
+        if nconv >= nev or at_limit:
+            Y, res = evaluate_ritz_pairs(A, B, lz.V, m, lam_all[:nev], C_all[:, :nev])
+            verified = bool(np.all(res <= tol))
+            if B is None or verified or at_limit:
+                status = 1 if (B is not None and not verified) else 0
+                return SolveResult(lam_all[:nev].copy(), Y, res, it, status)
+        spare = (m - nev) // 2
+        retained = nev + min(nconv, spare)
+        if retained == 1 and m > 3:
+            retained = m // 2
+        C = C_all[:, :retained]
+        lz.V[:, :retained] = lz.V[:, :m] @ C
+        if lz.BV is not None:
+            lz.BV[:, :retained] = lz.BV[:, :m] @ C
+        T = np.zeros_like(lz.T)
+        for j in range(retained):
+            T[j, j] = lam_all[j]
+            cpl = lz.beta_next * C_all[m - 1, j]
+            T[retained, j] = cpl
+            T[j, retained] = cpl
+        lz.T = T
+        lz.restart_row = retained
+        for col in range(retained, m):
+            lz.step(col)
+    raise RuntimeError("KrylovSchurSolver: unreachable solve termination.")
+
+
+# --------------------------------------------------------------------------
+# Reference spectra: tests/scripts/ref_eigs.py (parse) and run_case.py (select)
+# --------------------------------------------------------------------------
+
+
+def select_reference(values, which: str, count: int, shift: float = 0.0):
+    """select_reference (tests/scripts/run_case.py:207-221)."""
+    ordered = sorted(values)
+    which = which.upper()
+    if which == "SR":
+        return ordered[:count]
+    if which == "LR":
+        return ordered[::-1][:count]
+    if which == "SM":
+        return sorted(ordered, key=abs)[:count]
+    if which == "LM":
+        return sorted(ordered, key=abs, reverse=True)[:count]
+    if which == "BE":
+        return [ordered[-1 - i // 2] if i % 2 == 0 else ordered[i // 2] for i in range(count)]
+    if which == "SAI":
+        return sorted(sorted(ordered, key=lambda v: abs(v - shift))[:count])
+    raise ValueError(which)
+
+
+def eigenvalue_check(got, expected, atol: float = 1e-10, rtol: float = 1e-10):
+    """compare() of tests/scripts/run_case.py:246-260: |got-exp| <= atol + rtol*|exp|."""
+    return [abs(g - e) <= atol + rtol * abs(e) for g, e in zip(got, expected)]
