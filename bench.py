@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Benchmark: converged eigenpairs/s of the Chebyshev-filtered subspace iteration
+on the 2M-row well-potential problem (n = 128^3 = 2,097,152, 7-point Laplacian +
+32 Gaussian wells, 256 lowest pairs, block 320, degree 16, tol 1e-8), mixed
+precision on one B200, with the plain FP64 path measured beside it.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One step = one full solve (filter cycles until every requested pair has a
+relative residual <= 1e-8, or maxiter) of the same seeded input, already
+resident in HBM. Under torchrun every rank solves its own replica (the solve
+is one GPU's work; no data-path collective), so `scaling` is "weak" and `value`
+is the total converged pairs of all ranks / the max over ranks of the elapsed
+time. `--impl reference` times the CPU restatement of the reference path (the
+reference's Eigen build is unavailable: Eigen is not installed) on the host
+cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Converged eigenpairs/s (resid<=1e-8) vs FP64 plain; SpMM HBM GB/s; p99 latency"
+UNIT = "eigenpairs/s"
+
+
+def args_parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--side", type=int, default=128)
+    p.add_argument("--wells", type=int, default=32)
+    p.add_argument("--nev", type=int, default=256)
+    p.add_argument("--block", type=int, default=320)
+    p.add_argument("--degree", type=int, default=16)
+    p.add_argument("--tol", type=float, default=1e-8)
+    p.add_argument("--maxiter", type=int, default=300)
+    p.add_argument("--amplification", type=float, default=1e6)
+    p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison solve")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def config_dict(a, extra=None):
+    d = {"workload": "chebyshev_wells_128cube" if a.side == 128 else f"chebyshev_wells_{a.side}cube",
+         "n": a.side ** 3, "nnz": a.side ** 3 + 6 * (a.side - 1) * a.side ** 2,
+         "matrix": f"3D 7-point Dirichlet Laplacian {a.side}^3 + {a.wells} Gaussian wells (seeded)",
+         "solver": "Chebyshev", "nev": a.nev, "block": a.block, "degree": a.degree,
+         "tol": a.tol, "bounds": "ritz", "amplification_cap": a.amplification,
+         "precision": "mixed (FP32 filter/SpMM/rotation, FP64-accumulated Gram, FP64 "
+                      "Cholesky/eig/residual, FP64 final sweeps)",
+         "init": "device", "l2": "blocks (n x 320) >> 126 MB L2; no flush needed"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def clocks_sampler_start(path):
+    try:
+        f = open(path, "w")
+        proc = subprocess.Popen(
+            ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+             "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=f, stderr=subprocess.DEVNULL)
+        return proc, f
+    except Exception:
+        return None, None
+
+
+def clocks_sampler_stop(proc, f, path, device_index):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except Exception:
+        proc.kill()
+    f.close()
+    sm, mx, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in Path(path).read_text().splitlines():
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) < 9 or parts[0] != str(device_index):
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx = max(mx, float(parts[2]))
+        except ValueError:
+            continue
+        for nm, v in zip(names, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    if not sm:
+        return None
+    sm.sort()
+    return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the Chebyshev step from the committed ncu summary
+    (scaled to the full workload as that summary states), or None."""
+    p = ROOT / "profiles" / "cheb_step_f32_wells.md"
+    if not p.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_full_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+def build_matrix(a):
+    from fasteig_b200 import matrices as M
+    return M.laplacian_wells(a.side, wells=a.wells, seed=0)
+
+
+def solve_opts(a, precision, seed):
+    import fasteig_b200 as fe
+    o = fe.fasteig_options()
+    for k, v in dict(solver="Chebyshev", nev=a.nev, which="SR", tol=a.tol, maxiter=a.maxiter,
+                     seed=seed, degree=a.degree, block=a.block, bounds="ritz",
+                     amplification=a.amplification, precision=precision, init="device").items():
+        assert o.set(k, v), k
+    return o
+
+
+def roofline_cheb_step(a, H, dA, peak, launches=20):
+    """Time the dominant kernel (fused FP32 Chebyshev step, 320 columns) with CUDA
+    events on the stream it is launched on; achieved = algorithmic bytes / time."""
+    import torch
+    from fasteig_b200 import ops
+    n, b = H.n, a.block
+    X = torch.randn(n, b, device="cuda", dtype=torch.float32)
+    Z = torch.randn(n, b, device="cuda", dtype=torch.float32)
+    for _ in range(3):
+        ops.cheb_step(dA, X, Z, Z, 0.2, 0.1, -1.0)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(launches):
+        ops.cheb_step(dA, X, Z, Z, 0.2, 0.1, -1.0)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / launches
+    algo = H.nnz * (4 + 4) + 4 * (n + 1) + 3 * n * b * 4
+    achieved = algo / (ms * 1e-3) / 1e9
+    del X, Z
+    torch.cuda.empty_cache()
+    return {"kernel": "csr_spmm_kernel<float,4,32,3> (fused Chebyshev step, FP32, 320 cols)",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
+            "algorithmic_bytes": algo, "ms_per_launch": round(ms, 4)}
+
+
+def cpu_sample(a, H, iterations):
+    """Oracle (FP64 NumPy/SciPy restatement of the reference's CPU path) timed on the
+    host cores on a bounded sample of the same workload: one SpMM on a 32-column
+    slice of the n x 320 block (scaled x10, x17 per cycle: 16 filter steps + the
+    Rayleigh-Ritz apply) and one full-width Gram and rotation (x2 Gram, x3 rotation
+    per cycle), extrapolated to the GPU run's cycle count."""
+    import numpy as np
+    from oracle import oracle as O
+    A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
+    S = A.scipy()
+    rng = np.random.default_rng(0)
+    Xs = rng.standard_normal((H.n, 32))
+    t = time.perf_counter()
+    _ = S @ Xs
+    t_spmm32 = time.perf_counter() - t
+    X = rng.standard_normal((H.n, a.block))
+    t = time.perf_counter()
+    G = X.T @ X
+    t_gram = time.perf_counter() - t
+    C = rng.standard_normal((a.block, a.block))
+    t = time.perf_counter()
+    _ = X @ C
+    t_rot = time.perf_counter() - t
+    t = time.perf_counter()
+    np.linalg.eigh(0.5 * (G + G.T))
+    t_eig = time.perf_counter() - t
+    per_cycle = 17 * t_spmm32 * (a.block / 32) + 2 * t_gram + 3 * t_rot + t_eig
+    total = per_cycle * iterations
+    return {"value": round(a.nev / total, 4), "unit": UNIT, "cores": os.cpu_count(),
+            "kind": "port",
+            "sample": (f"oracle FP64: 1 SpMM of {H.n}x32 ({t_spmm32:.2f}s, scipy, 1 thread as the "
+                       f"reference's Eigen SpMM), 1 Gram {H.n}x{a.block} ({t_gram:.2f}s) and 1 "
+                       f"rotation ({t_rot:.2f}s, NumPy BLAS, all cores), eig {a.block} "
+                       f"({t_eig:.3f}s); cycle = 17 SpMM(320) + 2 Gram + 3 rotation + eig = "
+                       f"{per_cycle:.1f}s, x {iterations} cycles (GPU FP64 run) = {total:.0f}s "
+                       f"per solve"),
+            "seconds_per_cycle": round(per_cycle, 3)}
+
+
+def run_reference(a):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    H = build_matrix(a)
+    # Cycle count of the FP64 path on this workload (measured with the GPU FP64
+    # path, same algorithm); the CPU restatement needs the same number of cycles.
+    iters = int(os.environ.get("FE_CPU_CYCLES", "0")) or REFERENCE_CYCLES
+    vals = []
+    for i in range(a.warmup + a.steps):
+        r = cpu_sample(a, H, iters)
+        if i >= a.warmup:
+            vals.append(r)
+    v = sum(r["value"] for r in vals) / len(vals)
+    ms = a.nev / v * 1e3
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config_dict(a, {"precision": "fp64 (CPU restatement)"}),
+            "cpu_baseline": {k: vals[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["cpu_baseline"]["value"] = v
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# Filter cycles the FP64 path needs on the 128^3 well problem (bench.py FP64 run).
+REFERENCE_CYCLES = 40
+
+
+def main():
+    a = args_parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import fasteig_b200 as fe
+
+    H = build_matrix(a)
+    dA = fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values)
+    seed = 1 + rank
+    opts = solve_opts(a, "mixed", seed)
+
+    def solve_once(o, want_vectors=False):
+        p = fe.fasteig_problem(dA, solver="Chebyshev")
+        p.solve(o, want_vectors=want_vectors)
+        return p
+
+    for _ in range(a.warmup):
+        solve_once(opts)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    clk_path = tempfile.mktemp(prefix="fe_clocks_", suffix=".csv")
+    barrier()
+    proc, fh = clocks_sampler_start(clk_path)
+    launches0 = fe.lib.fe_launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    results = [solve_once(opts) for _ in range(a.steps)]
+    end.record()
+    barrier()
+    launches = fe.lib.fe_launch_count() - launches0
+    clocks = clocks_sampler_stop(proc, fh, clk_path, local)
+    elapsed = start.elapsed_time(end) / 1e3
+    converged = sum(int((p.residual_norms() <= a.tol).sum()) for p in results)
+    if world > 1:
+        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        c = torch.tensor([converged], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(c, op=torch.distributed.ReduceOp.SUM)
+        elapsed, converged = float(t.item()), int(c.item())
+    value = converged / elapsed
+    per_solve = [p.stats for p in results]
+    lat = sorted(s["seconds"] for s in per_solve)
+
+    extra = {}
+    peak, peak_kind = measured_peaks()
+    if rank == 0:
+        # End to end through the C ABI with host buffers: CSR upload from host arrays,
+        # solve, eigenvalues/residuals/eigenvectors back to host, inside the timed region.
+        t0 = time.perf_counter()
+        dA2 = fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values)
+        p2 = fe.fasteig_problem(dA2, solver="Chebyshev")
+        p2.solve(opts, want_vectors=True)
+        t_e2e = time.perf_counter() - t0
+        dA2.close()
+        e2e_pairs = int((p2.residual_norms() <= a.tol).sum())
+        h2d = H.rowptr.nbytes + H.colind.nbytes + H.values.nbytes
+        d2h = 8 * a.nev * (H.n + 2)
+        extra["e2e"] = {"value": round(e2e_pairs / t_e2e, 4), "unit": UNIT,
+                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                        "seconds": round(t_e2e, 3)}
+        del p2
+        fp64 = None
+        if not a.no_fp64:
+            o64 = solve_opts(a, "fp64", seed)
+            p64 = solve_once(o64)
+            c64 = int((p64.residual_norms() <= a.tol).sum())
+            fp64 = {"value": round(c64 / p64.stats["seconds"], 4), "unit": UNIT,
+                    "seconds": round(p64.stats["seconds"], 3), "cycles": p64.stats["iterations"],
+                    "converged": c64}
+            extra["fp64_plain"] = fp64
+            extra["mixed_vs_fp64"] = round((value / world) / fp64["value"], 3) if fp64["value"] else None
+        extra["roofline"] = roofline_cheb_step(a, H, dA, peak)
+        extra["roofline"]["peak_kind"] = f"{peak_kind} hbm_gbs (burst copy)"
+        if world == 1 and not a.no_cpu:
+            cycles = fp64["cycles"] if fp64 else REFERENCE_CYCLES
+            extra["cpu_baseline"] = cpu_sample(a, H, cycles)
+    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(elapsed / a.steps * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic", "impl": "b200",
+            "config": config_dict(a, {"parallelism": f"replicas x{world}"}),
+            "converged_pairs": converged, "latency_s": {"p50": lat[len(lat) // 2], "max": lat[-1]},
+            "cycles": [s["iterations"] for s in per_solve],
+            "fp32_cycles": [s["fp32_iterations"] for s in per_solve],
+            "gpu_launches": int(launches), "clocks": clocks}
+    line.update(extra)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -2,10 +2,28 @@
 eigensolver hot path (block SpMM, fused Chebyshev filter, CholQR and
 Rayleigh-Ritz block kernels) behind fasteig's problem/options API.
 
-Importing the package loads the in-tree CUDA library; it raises ImportError if
-the library has not been built. There is no CPU execution path.
+The CUDA library is loaded on first use of any public name; if it has not been
+built, that access raises ImportError. There is no CPU execution path.
+(``fasteig_b200.build`` and ``fasteig_b200.matrices`` import without it.)
 """
-from ._lib import FastEigError, lib, version  # noqa: F401
-from .problem import CsrMatrix, fasteig_options, fasteig_problem  # noqa: F401
+import importlib
 
-__all__ = ["CsrMatrix", "FastEigError", "fasteig_options", "fasteig_problem", "lib", "version"]
+_LAZY = {
+    "FastEigError": "._lib",
+    "lib": "._lib",
+    "version": "._lib",
+    "CsrMatrix": ".problem",
+    "fasteig_options": ".problem",
+    "fasteig_problem": ".problem",
+}
+
+__all__ = sorted(_LAZY)
+
+
+def __getattr__(name):
+    mod = _LAZY.get(name)
+    if mod is None:
+        raise AttributeError(f"module 'fasteig_b200' has no attribute {name!r}")
+    value = getattr(importlib.import_module(mod, __name__), name)
+    globals()[name] = value
+    return value

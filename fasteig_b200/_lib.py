@@ -25,6 +25,7 @@ _SIGS = {
     "fe_version": (C.c_char_p, []),
     "fe_last_error": (C.c_char_p, []),
     "fe_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "fe_launch_count": (C.c_int64, []),
     "fe_csr_create": (C.c_int, [i64, i64, i64, vp, vp, vp, C.POINTER(vp)]),
     "fe_csr_destroy": (C.c_int, [vp]),
     "fe_csr_info": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]),
@@ -53,6 +54,12 @@ _SIGS = {
     "fe_convert_f64_to_f32": (C.c_int, [vp, i64, vp, i64, i64, i64, vp]),
     "fe_convert_f32_to_f64": (C.c_int, [vp, i64, vp, i64, i64, i64, vp]),
     "fe_solve": (C.c_int, [vp, vp, C.c_char_p, vp, vp, vp, vp]),
+    "fe_gram_tf32x3_workspace_bytes": (sz, [i64, i64, i64]),
+    "fe_gram_tf32x3": (C.c_int, [vp, i64, vp, i64, i64, i64, i64, vp, i64, vp, sz, vp]),
+    "fe_rotate_tf32x3_workspace_bytes": (sz, [i64, i64]),
+    "fe_rotate_tf32x3": (C.c_int, [vp, i64, vp, i64, vp, i64, i64, i64, i64, f64, f64, vp, sz,
+                                   vp]),
+    "fe_device_status": (C.c_int, [C.POINTER(C.c_int32), C.c_int32]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

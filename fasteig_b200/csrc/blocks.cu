@@ -295,9 +295,15 @@ __global__ void convert_kernel(const S* __restrict__ src, int64_t lds, D* __rest
 
 }  // namespace
 
+// Workspace that suffices for every call with n' <= n, k' <= k, m' <= m, so a
+// caller can size it once for its largest block: chunks <= target/tiles' + 1 and
+// k'*m' <= tiles' * 64 * 64 bound the partial count by (target + tiles) tiles.
 size_t gram_workspace_bytes(int64_t n, int64_t k, int64_t m) {
   if (n <= 0 || k <= 0 || m <= 0) return 0;
-  return gram_plan(n, k, m).bytes;
+  const int64_t tiles = ((k + kGT - 1) / kGT) * ((m + kGT - 1) / kGT);
+  const int64_t by_tiles = (kGramTargetCtas + tiles) * int64_t(kGT) * kGT;
+  const int64_t by_rows = ((n + 255) / 256 + 1) * k * m;
+  return static_cast<size_t>(std::min(by_tiles, by_rows)) * sizeof(double);
 }
 
 template <typename T>
@@ -365,9 +371,12 @@ template void rotate<double>(const double*, int64_t, const double*, int64_t, dou
 template void rotate<float>(const float*, int64_t, const double*, int64_t, float*, int64_t,
                             int64_t, int64_t, int64_t, double, double, cudaStream_t);
 
+// Bound valid for every call with n' <= n and m' <= m (chunks never exceed the
+// target count nor one per 64 rows).
 size_t residual_workspace_bytes(int64_t n, int64_t m) {
   if (n <= 0 || m <= 0) return 0;
-  return norm_plan(n, m).bytes;
+  const int64_t chunks = std::min<int64_t>(kNormTargetChunks, (n + 63) / 64 + 1);
+  return static_cast<size_t>(chunks) * 2 * m * sizeof(double);
 }
 
 template <typename T>

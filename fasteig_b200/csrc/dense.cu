@@ -11,6 +11,7 @@
 
 #include "fe_common.cuh"
 
+#include <atomic>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -23,6 +24,11 @@ thread_local std::string g_last_error;
 }
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+std::atomic<int64_t> g_launches{0};
+}
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int num_sms() {
   int dev = 0, sms = 0;
@@ -214,6 +220,8 @@ using fe::guarded;
 extern "C" const char* fe_version(void) { return "fasteig_b200 0.1.0 (sm_100a)"; }
 
 extern "C" const char* fe_last_error(void) { return fe::g_last_error.c_str(); }
+
+extern "C" int64_t fe_launch_count(void) { return fe::g_launches.load(); }
 
 extern "C" int fe_device_count(int* count) {
   return guarded("fe_device_count", [&] {

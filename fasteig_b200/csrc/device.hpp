@@ -173,3 +173,15 @@ void vec_axpby(int64_t n, double a, const double* x, int64_t incx, double b, dou
 template <typename T>
 void fill_uniform(T* X, int64_t ld, int64_t n, int64_t m, uint64_t seed, cudaStream_t s);
 }  // namespace fe
+
+namespace fe {
+bool tc_gemm_available();
+size_t tc_gram_workspace_bytes(int64_t n, int64_t k, int64_t m);
+void gram_tc(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n, int64_t k,
+             int64_t m, double* G, int64_t ldg, void* ws, size_t ws_bytes, cudaStream_t s);
+size_t tc_rotate_workspace_bytes(int64_t k, int64_t m);
+void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float* Y, int64_t ldy,
+               int64_t n, int64_t k, int64_t m, double alpha, double beta, void* ws,
+               size_t ws_bytes, cudaStream_t s);
+int read_tc_status(bool clear);
+}  // namespace fe

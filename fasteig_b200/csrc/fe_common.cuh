@@ -55,7 +55,11 @@ int guarded(const char* where, F&& body) {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Number of this library's kernel launches since load (all threads).
+void count_launch();
+
 inline void check_launch(const char* what) {
+  count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     throw Error(FE_ERR_CUDA, std::string(what) + " launch failed: " + cudaGetErrorString(e));

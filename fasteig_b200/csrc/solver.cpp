@@ -68,6 +68,7 @@ struct Options {
   double amplification = 1.0e3;    // filter amplification cap at the lower bound
   std::string init = "host";       // host (std::mt19937, bit-exact) | device
   double mixed_switch = 2.0e-6;    // FP32 -> FP64 switch when max residual <= this
+  bool tensor_cores = true;        // FP32 Grams/rotations on tcgen05 (3xTF32)
 
   void parse(const char* text) {
     if (!text) return;
@@ -134,6 +135,7 @@ struct Options {
     else if (k == "amplification") amplification = as_double(v);
     else if (k == "init") init = lower(v);
     else if (k == "mixed_switch") mixed_switch = as_double(v);
+    else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
     else if (k == "print_every" || k == "logfile" || k == "output_format" || k == "gpu_backend" ||
              k == "shift" || k == "n") {
       // accepted for deck compatibility; no effect on this backend
@@ -333,10 +335,13 @@ struct ChebBlocks {
 };
 
 struct SmallState {
-  DeviceBuffer G, Rinv, W, rel, rnorm, xnorm, info, gws, rws;
+  DeviceBuffer G, Rinv, W, rel, rnorm, xnorm, info, gws, rws, cws;
   int64_t cap = 0;
-  void allocate(int64_t n, int64_t c) {
+  bool tensor_cores = false;  // FP32 Grams/rotations on tcgen05 (3xTF32)
+  int64_t precise_grams = 0;  // FP32 Cholesky passes redone with the FP64-accumulated Gram
+  void allocate(int64_t n, int64_t c, bool tc) {
     cap = c;
+    tensor_cores = tc;
     G.resize(static_cast<size_t>(c) * c * sizeof(double));
     Rinv.resize(static_cast<size_t>(c) * c * sizeof(double));
     W.resize(c * sizeof(double));
@@ -344,23 +349,69 @@ struct SmallState {
     rnorm.resize(c * sizeof(double));
     xnorm.resize(c * sizeof(double));
     info.resize(4 * sizeof(int32_t));
-    gws.resize(std::max<size_t>(gram_workspace_bytes(n, c, c), 64));
+    size_t g = gram_workspace_bytes(n, c, c);
+    if (tc) g = std::max(g, tc_gram_workspace_bytes(n, c, c));
+    gws.resize(std::max<size_t>(g, 64));
     rws.resize(std::max<size_t>(residual_workspace_bytes(n, c), 64));
+    if (tc) cws.resize(std::max<size_t>(tc_rotate_workspace_bytes(c, c), 64));
   }
 };
 
+inline bool tc_ok(const void* p, int64_t ld) {
+  return (reinterpret_cast<uintptr_t>(p) & 15u) == 0 && ld % 4 == 0;
+}
+
+// G (ldg) = X^T Y. FP32 blocks use the tensor-core split-TF32 Gram unless
+// `precise` asks for the FP64-accumulated one.
+template <typename T>
+void gram_block(SmallState& sm, const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n,
+                int64_t k, int64_t m, double* G, cudaStream_t s, bool precise = false) {
+  if constexpr (sizeof(T) == 4) {
+    if (sm.tensor_cores && !precise && ldx % 4 == 0 && ldy % 4 == 0 && n >= 128) {
+      gram_tc(X, ldx, Y, ldy, n, k, m, G, sm.cap, sm.gws.get(), sm.gws.bytes(), s);
+      return;
+    }
+  }
+  gram<T>(X, ldx, Y, ldy, n, k, m, G, sm.cap, sm.gws.get(), sm.gws.bytes(), s);
+}
+
+// Y = alpha X C + beta Y (C: FP64 column-major with leading dimension cap).
+template <typename T>
+void rotate_block(SmallState& sm, const T* X, int64_t ldx, const double* C, T* Y, int64_t ldy,
+                  int64_t n, int64_t k, int64_t m, double alpha, double beta, cudaStream_t s) {
+  if constexpr (sizeof(T) == 4) {
+    if (sm.tensor_cores && tc_ok(X, ldx) && n >= 128) {
+      rotate_tc(X, ldx, C, sm.cap, Y, ldy, n, k, m, alpha, beta, sm.cws.get(), sm.cws.bytes(), s);
+      return;
+    }
+  }
+  rotate<T>(X, ldx, C, sm.cap, Y, ldy, n, k, m, alpha, beta, s);
+}
+
 // Cholesky QR of src (n x k) into dst: G = src^T src, R = chol(G), dst = src R^{-1}
 // (cuda_cholesky_qr_in_place, src/core/Orthogonalization.cpp:185-246).
-// The rank-loss flag accumulates into info[slot].
+// The rank-loss flag accumulates into info[slot]. With tensor-core Grams, a
+// failed factorization is retried once with the FP64-accumulated Gram.
 template <typename T>
 void cholqr(Context& ctx, SmallState& sm, const T* src, int64_t lds, T* dst, int64_t ldd, int64_t n,
             int64_t k, int slot) {
   cudaStream_t s = ctx.stream;
   double* G = sm.G.as<double>();
-  gram<T>(src, lds, src, lds, n, k, k, G, sm.cap, sm.gws.get(), sm.gws.bytes(), s);
-  potrf_upper(G, k, sm.cap, sm.info.as<int32_t>() + slot, s);
+  int32_t* info = sm.info.as<int32_t>() + slot;
+  gram_block<T>(sm, src, lds, src, lds, n, k, k, G, s);
+  potrf_upper(G, k, sm.cap, info, s);
+  if (sizeof(T) == 4 && sm.tensor_cores) {
+    int32_t h = 0;
+    ctx.to_host(&h, info, 1);
+    ctx.sync();
+    if (h != 0) {
+      sm.precise_grams += 1;
+      gram_block<T>(sm, src, lds, src, lds, n, k, k, G, s, /*precise=*/true);
+      potrf_upper(G, k, sm.cap, info, s);
+    }
+  }
   trinv_upper(G, sm.cap, sm.Rinv.as<double>(), sm.cap, k, s);
-  rotate<T>(src, lds, sm.Rinv.as<double>(), sm.cap, dst, ldd, n, k, k, 1.0, 0.0, s);
+  rotate_block<T>(sm, src, lds, sm.Rinv.as<double>(), dst, ldd, n, k, k, 1.0, 0.0, s);
 }
 
 // Filter scaling (src/ChebyshevSolver.cpp:231-239) for a damped interval [cutoff, upper]
@@ -408,10 +459,10 @@ struct ChebLoop {
     // (block_gram_schmidt, src/core/Orthogonalization.cpp:482-527).
     if (locked > 0) {
       for (int pass = 0; pass < 2; ++pass) {
-        gram<T>(b.V.data(), b.V.ld, b.V.col(locked), b.V.ld, n, locked, active, sm.G.as<double>(),
-                sm.cap, sm.gws.get(), sm.gws.bytes(), s);
-        rotate<T>(b.V.data(), b.V.ld, sm.G.as<double>(), sm.cap, b.V.col(locked), b.V.ld, n,
-                  locked, active, -1.0, 1.0, s);
+        gram_block<T>(sm, b.V.data(), b.V.ld, b.V.col(locked), b.V.ld, n, locked, active,
+                      sm.G.as<double>(), s);
+        rotate_block<T>(sm, b.V.data(), b.V.ld, sm.G.as<double>(), b.V.col(locked), b.V.ld, n,
+                        locked, active, -1.0, 1.0, s);
       }
     }
     // 3. Cholesky QR of the current subspace (CholQR2 on FP32 blocks).
@@ -425,12 +476,11 @@ struct ChebLoop {
     csr_spmm<T>(A, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, nullptr, 0, sub, sign, 0.0, 0.0, s);
     st.spmm_launches += 1;
     double* P = sm.G.as<double>();
-    gram<T>(b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, n, sub, sub, P, sm.cap, sm.gws.get(),
-            sm.gws.bytes(), s);
+    gram_block<T>(sm, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, n, sub, sub, P, s);
     symmetrize(P, sub, sm.cap, s);
     eig.run(P, sub, sm.cap, sm.W.as<double>());
-    rotate<T>(b.Q.data(), b.Q.ld, P, sm.cap, b.V.data(), b.V.ld, n, sub, sub, 1.0, 0.0, s);
-    rotate<T>(b.AQ.data(), b.AQ.ld, P, sm.cap, b.S.data(), b.S.ld, n, sub, sub, 1.0, 0.0, s);
+    rotate_block<T>(sm, b.Q.data(), b.Q.ld, P, b.V.data(), b.V.ld, n, sub, sub, 1.0, 0.0, s);
+    rotate_block<T>(sm, b.AQ.data(), b.AQ.ld, P, b.S.data(), b.S.ld, n, sub, sub, 1.0, 0.0, s);
     residual_norms<T>(b.S.data(), b.V.data(), nullptr, b.V.ld, n, sub, sm.W.as<double>(), nullptr,
                       0, sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
                       sm.rws.get(), sm.rws.bytes(), s, 1);
@@ -493,7 +543,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
 
   Context ctx;
   SmallState sm;
-  sm.allocate(n, cap);
+  sm.allocate(n, cap, mixed && opt.tensor_cores && tc_gemm_available());
   ProjectedEig eig(ctx, cap);
 
   double lower = 0, upper = 0;
@@ -531,7 +581,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   int64_t locked = 0;
   int64_t sub = nev;
   int64_t sub_prev = 0;
-  std::vector<double> W, rel;
+  std::vector<double> W, rel, worst_history;
   int64_t it_done = 0;
   const double tol = opt.tol;
   for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
@@ -560,9 +610,12 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
       if (!std::isfinite(W[j]) || !std::isfinite(rel[j]))
         throw Error(FE_ERR_NONFINITE, "ChebyshevSolver: non-finite Ritz values or residuals.");
     sub_prev = sub;
-    // 4. Ordered locking (src/ChebyshevSolver.cpp:186-192).
+    // 4. Ordered locking (src/ChebyshevSolver.cpp:186-192). On FP32 blocks, whose
+    // residuals cannot reach tol, pairs lock at the FP32 floor (mixed_switch) so
+    // the spare columns still enter the subspace as the prefix converges.
+    const double lock_tol = l32 ? std::max(tol, opt.mixed_switch) : tol;
     locked = 0;
-    while (locked < nev && rel[locked] <= tol) ++locked;
+    while (locked < nev && rel[locked] <= lock_tol) ++locked;
     sub = std::max(sub, nev + std::min(locked, cap - nev));
     it_done = iter + 1;
     double worst = 0.0;
@@ -573,7 +626,13 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
                    static_cast<long long>(sub_prev), static_cast<long long>(locked), worst, cutoff);
     }
     if (worst <= tol) break;
-    if (l32 && worst <= std::max(opt.mixed_switch, tol)) {
+    worst_history.push_back(worst);
+    const size_t h = worst_history.size();
+    // Leave FP32 at its residual floor, or when the FP32 cycles stop reducing the
+    // worst residual (no 30% gain over three cycles).
+    const bool stalled = h >= 4 && worst > 0.7 * worst_history[h - 4];
+    if (l32 && (worst <= std::max(opt.mixed_switch, tol) || stalled)) {
+      worst_history.clear();
       // FP32 residual floor reached: continue on FP64 blocks.
       l64.reset(new ChebLoop<double>(ctx, A, opt, sm, eig, sign, lower, upper, false));
       l64->b.allocate(n, cap);
@@ -581,6 +640,8 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
                              ctx.stream);
       ctx.sync();
       l32.reset();
+      locked = 0;  // FP64 sweeps refine every pair to tol
+      while (locked < nev && rel[locked] <= tol) ++locked;
     }
   }
   // Results: eigenvalues (sign restored), residuals, first nev Ritz vectors.

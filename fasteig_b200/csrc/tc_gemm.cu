@@ -1,0 +1,710 @@
+// Tensor-core (tcgen05, TMEM accumulators, TMA-fed) split-TF32 kernels for the
+// tall-skinny FP32 block products of the mixed-precision path:
+//
+//   Gram      G = X^T Y           (X: n x k, Y: n x m; reduction over the n rows)
+//   Rotation  Y = alpha X C + beta Y  (X: n x k, C: k x m FP64 column-major)
+//
+// They replace the reference's cublasDgemm calls in transpose_multiply
+// (src/gpu/CudaMultiVector.cpp:395-405), right_multiply_active_columns (:353-358)
+// and Cholesky QR (src/core/Orthogonalization.cpp:202-235) for FP32 blocks.
+//
+// Precision ("3xTF32"): every FP32 operand x is split into x_hi = rna_tf32(x) and
+// x_lo = rna_tf32(x - x_hi), and the product is accumulated in FP32 TMEM as
+// x_hi*y_hi + x_hi*y_lo + x_lo*y_hi. Products of TF32 values are exact in FP32 and
+// the dropped x_lo*y_lo term is below 2^-22 |x y|, so the result carries FP32-level
+// error. The Gram is split over row chunks whose FP32 partial tiles are summed in
+// FP64 in a fixed order (deterministic).
+//
+// Pipeline per CTA (128-row MMA tile, N-tile of 160 columns, 3 smem stages):
+//   warp 0 lane 0 : TMA producer (2D tiled loads, 128-byte swizzle)
+//   warp 1        : TMEM allocator; lane 0 issues tcgen05.mma and commits
+//   warps 2..5    : split FP32 tiles into hi/lo in shared memory, then drain
+//                   TMEM (tcgen05.ld 32x32b) in the epilogue
+// All mbarrier waits are bounded; on timeout the kernel records an error code in
+// a device status word (fe_device_status) and leaves.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "fe_common.cuh"
+
+namespace fe {
+
+__device__ int g_tc_status = 0;  // 0 = ok, otherwise a code of the first failed wait
+
+namespace {
+
+constexpr int kM = 128;           // MMA M (TMEM lanes)
+constexpr int kN = 160;           // MMA N (columns per CTA tile)
+constexpr int kKB = 32;           // FP32 elements per 128-byte swizzle row
+constexpr int kStages = 3;
+constexpr int kThreads = 192;     // 6 warps
+constexpr int kSplitThreads = 128;
+constexpr uint32_t kTmemCols = 256;
+
+// Per-stage shared memory (bytes); every buffer is 1024-byte aligned.
+constexpr int kABytes = kM * kKB * 4;   // 16 KB
+constexpr int kBBytes = kN * kKB * 4;   // 20 KB
+constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: about two seconds of SM clock, then record `code` and give up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (true) {
+    for (int i = 0; i < 64; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (clock64() - t0 > 4000000000LL) {
+      atomicCAS(&g_tc_status, 0, code);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// UMMA shared-memory descriptor (SM100 version 1) with 128-byte swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes,
+                                              uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;  // version (SM100)
+  d |= static_cast<uint64_t>(2) << 61;  // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor: kind::tf32, FP32 accumulate, M = 128, N = kN.
+__host__ __device__ constexpr uint32_t idesc_tf32(bool a_mn_major, bool b_mn_major) {
+  return (1u << 4)                               // c_format = F32
+         | (2u << 7)                             // a_format = TF32
+         | (2u << 10)                            // b_format = TF32
+         | (static_cast<uint32_t>(a_mn_major) << 15) |
+         (static_cast<uint32_t>(b_mn_major) << 16) |
+         (static_cast<uint32_t>(kN >> 3) << 17)  // n_dim
+         | (static_cast<uint32_t>(kM >> 4) << 24);  // m_dim
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// Split n_vec16 16-byte chunks of raw FP32 data in place into hi, and into lo.
+__device__ __forceinline__ void split_tile(float* raw_hi, float* lo, int n_vec16, int tid) {
+  float4* h = reinterpret_cast<float4*>(raw_hi);
+  float4* l = reinterpret_cast<float4*>(lo);
+  for (int i = tid; i < n_vec16; i += kSplitThreads) {
+    float4 v = h[i];
+    float4 hi, lw;
+    hi.x = __uint_as_float(tf32_rna(v.x));
+    hi.y = __uint_as_float(tf32_rna(v.y));
+    hi.z = __uint_as_float(tf32_rna(v.z));
+    hi.w = __uint_as_float(tf32_rna(v.w));
+    lw.x = __uint_as_float(tf32_rna(v.x - hi.x));
+    lw.y = __uint_as_float(tf32_rna(v.y - hi.y));
+    lw.z = __uint_as_float(tf32_rna(v.z - hi.z));
+    lw.w = __uint_as_float(tf32_rna(v.w - hi.w));
+    h[i] = hi;
+    l[i] = lw;
+  }
+}
+
+struct Smem {
+  uint8_t* base;  // 1024-aligned
+  uint64_t* full;
+  uint64_t* empty;
+  uint64_t* split;
+  uint64_t* accum;
+  uint32_t* tmem_slot;
+  __device__ float* a_hi(int s) const { return reinterpret_cast<float*>(base + s * kStageBytes); }
+  __device__ float* a_lo(int s) const {
+    return reinterpret_cast<float*>(base + s * kStageBytes + kABytes);
+  }
+  __device__ float* b_hi(int s) const {
+    return reinterpret_cast<float*>(base + s * kStageBytes + 2 * kABytes);
+  }
+  __device__ float* b_lo(int s) const {
+    return reinterpret_cast<float*>(base + s * kStageBytes + 2 * kABytes + kBBytes);
+  }
+};
+
+__device__ __forceinline__ Smem carve(uint8_t* dyn) {
+  Smem s;
+  uintptr_t p = reinterpret_cast<uintptr_t>(dyn);
+  p = (p + 1023) & ~uintptr_t(1023);
+  s.base = reinterpret_cast<uint8_t*>(p);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s.base + kStages * kStageBytes);
+  s.full = bars;
+  s.empty = bars + kStages;
+  s.split = bars + 2 * kStages;
+  s.accum = bars + 3 * kStages;
+  s.tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * kStages + 1);
+  return s;
+}
+
+// Common prologue: barrier init (thread 0) and TMEM allocation (warp 1).
+__device__ __forceinline__ void prologue(const Smem& sm, int warp) {
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+      mbar_init(&sm.split[s], kSplitThreads);
+    }
+    mbar_init(sm.accum, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(sm.tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+}
+
+__device__ __forceinline__ void epilogue_dealloc(const Smem& sm, int warp, uint32_t tmem) {
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// MMA issue loop shared by both kernels. Operand descriptors per K-step (8
+// elements of K): K-major tiles advance 32 bytes inside the 128-byte swizzle
+// row; MN-major tiles advance one 1024-byte swizzle atom (8 rows).
+template <bool kMN>
+__device__ void mma_loop(const Smem& sm, uint32_t tmem, int nkb, uint32_t idesc) {
+  // K-major: SBO = 1024 (8 rows x 128 B), LBO unused (16). MN-major: LBO = bytes
+  // between 32-element column groups (one TMA box of 32 rows x 128 B = 4096),
+  // SBO = 1024 (8 rows).
+  const uint32_t lbo = kMN ? 4096u : 16u;
+  const uint32_t sbo = 1024u;
+  for (int kb = 0; kb < nkb; ++kb) {
+    const int s = kb % kStages;
+    const uint32_t ph = (kb / kStages) & 1u;
+    if (!mbar_wait(&sm.split[s], ph, 3)) return;
+    tc_fence_after();
+    const uint32_t ah = smem_u32(sm.a_hi(s)), al = smem_u32(sm.a_lo(s));
+    const uint32_t bh = smem_u32(sm.b_hi(s)), bl = smem_u32(sm.b_lo(s));
+#pragma unroll
+    for (int k = 0; k < kKB / 8; ++k) {
+      const uint32_t off = kMN ? k * 1024u : k * 32u;
+      const uint64_t dah = smem_desc(ah + off, lbo, sbo), dal = smem_desc(al + off, lbo, sbo);
+      const uint64_t dbh = smem_desc(bh + off, lbo, sbo), dbl = smem_desc(bl + off, lbo, sbo);
+      const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
+      umma_tf32(tmem, dah, dbh, idesc, acc);
+      umma_tf32(tmem, dah, dbl, idesc, 1u);
+      umma_tf32(tmem, dal, dbh, idesc, 1u);
+    }
+    umma_commit(&sm.empty[s]);
+  }
+  umma_commit(sm.accum);
+}
+
+// ------------------------------------------------------------------ Gram ----
+// grid.x = k_tiles * m_tiles (k tile fastest), grid.y = row chunks.
+// A = X^T (MN-major: 4 boxes of 32 columns x 32 rows), B = Y (MN-major, 5 boxes).
+// X and Y tensor maps start at columns aligned down to 16 bytes; sx/sy are the
+// column shifts of the caller's views (outputs are re-indexed).
+__global__ void __launch_bounds__(kThreads, 1)
+gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmY,
+               int64_t n, int k, int m, int sx, int sy, int k_tiles, int64_t rows_per_chunk,
+               float* __restrict__ partial) {
+  extern __shared__ uint8_t dyn_smem[];
+  const Smem sm = carve(dyn_smem);
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  const int ti = blockIdx.x % k_tiles;
+  const int tj = blockIdx.x / k_tiles;
+  const int i0 = ti * kM;   // tile origin in shifted (tensor-map) column space of X
+  const int j0 = tj * kN;
+  const int64_t r_begin = static_cast<int64_t>(blockIdx.y) * rows_per_chunk;
+  const int64_t r_end = min(n, r_begin + rows_per_chunk);
+  const int nkb = static_cast<int>((r_end - r_begin + kKB - 1) / kKB);
+
+  prologue(sm, warp);
+  const uint32_t tmem = *sm.tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % kStages;
+      const uint32_t ph = (kb / kStages) & 1u;
+      if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1)) break;
+      mbar_expect_tx(&sm.full[s], kABytes + kBBytes);
+      const int y = static_cast<int>(r_begin + static_cast<int64_t>(kb) * kKB);
+#pragma unroll
+      for (int c = 0; c < kM / 32; ++c)
+        tma_load_2d(sm.a_hi(s) + c * (32 * kKB), &tmX, i0 + 32 * c, y, &sm.full[s]);
+#pragma unroll
+      for (int c = 0; c < kN / 32; ++c)
+        tma_load_2d(sm.b_hi(s) + c * (32 * kKB), &tmY, j0 + 32 * c, y, &sm.full[s]);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) mma_loop<true>(sm, tmem, nkb, idesc_tf32(true, true));
+    __syncwarp();
+  } else if (warp >= 2) {
+    const int tid = threadIdx.x - 64;
+    // Rows past r_end inside the last block belong to the next chunk: zero them
+    // in the split so they do not enter this chunk's sum.
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % kStages;
+      const uint32_t ph = (kb / kStages) & 1u;
+      if (!mbar_wait(&sm.full[s], ph, 2)) break;
+      const int64_t y = r_begin + static_cast<int64_t>(kb) * kKB;
+      const int64_t left = r_end - y;
+      const int valid = left < kKB ? static_cast<int>(left) : kKB;
+      if (valid < kKB) {
+        // Row r of a box sits at byte r*128 (swizzle permutes 16-byte chunks
+        // within the row only), so zeroing whole 128-byte rows is layout-safe.
+        for (int idx = tid; idx < (kM / 32 + kN / 32) * (kKB - valid) * 32; idx += kSplitThreads) {
+          const int box = idx / ((kKB - valid) * 32);
+          const int rem = idx % ((kKB - valid) * 32);
+          const int row = valid + rem / 32;
+          const int e = rem % 32;
+          float* bp = box < kM / 32 ? sm.a_hi(s) + box * (32 * kKB)
+                                    : sm.b_hi(s) + (box - kM / 32) * (32 * kKB);
+          bp[row * 32 + e] = 0.0f;
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+      }
+      split_tile(sm.a_hi(s), sm.a_lo(s), kABytes / 16, tid);
+      split_tile(sm.b_hi(s), sm.b_lo(s), kBBytes / 16, tid);
+      fence_proxy_async();
+      mbar_arrive(&sm.split[s]);
+    }
+    // Epilogue: TMEM lane = output row i (within the k tile), column = j.
+    if (mbar_wait(sm.accum, 0, 4)) {
+      tc_fence_after();
+      const int q = warp % 4;
+      const int i = i0 + q * 32 + lane - sx;  // caller's column index in X
+      float* out = partial + static_cast<int64_t>(blockIdx.y) * k * m;
+      for (int c = 0; c < kN; c += 16) {
+        float v[16];
+        tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c, v);
+        if (i >= 0 && i < k) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int j = j0 + c + e - sy;
+            if (j >= 0 && j < m) out[static_cast<int64_t>(j) * k + i] = v[e];
+          }
+        }
+      }
+    }
+  }
+  epilogue_dealloc(sm, warp, tmem);
+}
+
+__global__ void gram_tc_reduce(const float* __restrict__ partial, int chunks, int k, int m,
+                               double* __restrict__ G, int64_t ldg) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t total = static_cast<int64_t>(k) * m;
+  if (idx >= total) return;
+  double s = 0.0;
+  for (int c = 0; c < chunks; ++c) s += static_cast<double>(partial[c * total + idx]);
+  G[(idx / k) * ldg + (idx % k)] = s;
+}
+
+// --------------------------------------------------------------- Rotation ----
+// grid.x = m tiles, grid.y = row tiles. A = X (K-major 128 rows x 32), B = C^T
+// split into hi/lo FP32 arrays of m_pad rows x k_pad (K-major, prepared by
+// rotate_prep_kernel).
+__global__ void __launch_bounds__(kThreads, 1)
+rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmCh,
+                 const __grid_constant__ CUtensorMap tmCl, int64_t n, int k, int m, int m_tiles,
+                 float* __restrict__ Y, int64_t ldy, float alpha, float beta, int use_beta,
+                 int vec_store) {
+  extern __shared__ uint8_t dyn_smem[];
+  const Smem sm = carve(dyn_smem);
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  const int j0 = static_cast<int>(blockIdx.x % m_tiles) * kN;
+  const int64_t r0 = static_cast<int64_t>(blockIdx.x / m_tiles) * kM;
+  const int nkb = (k + kKB - 1) / kKB;
+
+  prologue(sm, warp);
+  const uint32_t tmem = *sm.tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % kStages;
+      const uint32_t ph = (kb / kStages) & 1u;
+      if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1)) break;
+      mbar_expect_tx(&sm.full[s], kABytes + 2 * kBBytes);
+      tma_load_2d(sm.a_hi(s), &tmX, kb * kKB, static_cast<int>(r0), &sm.full[s]);
+      tma_load_2d(sm.b_hi(s), &tmCh, kb * kKB, j0, &sm.full[s]);
+      tma_load_2d(sm.b_lo(s), &tmCl, kb * kKB, j0, &sm.full[s]);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) mma_loop<false>(sm, tmem, nkb, idesc_tf32(false, false));
+    __syncwarp();
+  } else if (warp >= 2) {
+    const int tid = threadIdx.x - 64;
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % kStages;
+      const uint32_t ph = (kb / kStages) & 1u;
+      if (!mbar_wait(&sm.full[s], ph, 2)) break;
+      split_tile(sm.a_hi(s), sm.a_lo(s), kABytes / 16, tid);
+      fence_proxy_async();
+      mbar_arrive(&sm.split[s]);
+    }
+    if (mbar_wait(sm.accum, 0, 4)) {
+      tc_fence_after();
+      const int q = warp % 4;
+      const int64_t r = r0 + q * 32 + lane;
+      for (int c = 0; c < kN; c += 16) {
+        float v[16];
+        tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c, v);
+        if (r < n) {
+          float* yr = Y + r * ldy + j0 + c;
+          if (vec_store && j0 + c + 16 <= m) {
+#pragma unroll
+            for (int e = 0; e < 16; e += 4) {
+              float4 o = make_float4(alpha * v[e], alpha * v[e + 1], alpha * v[e + 2],
+                                     alpha * v[e + 3]);
+              if (use_beta) {
+                const float4 y = *reinterpret_cast<const float4*>(yr + e);
+                o.x = fmaf(beta, y.x, o.x);
+                o.y = fmaf(beta, y.y, o.y);
+                o.z = fmaf(beta, y.z, o.z);
+                o.w = fmaf(beta, y.w, o.w);
+              }
+              *reinterpret_cast<float4*>(yr + e) = o;
+            }
+          } else {
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              if (j0 + c + e < m) {
+                float out = alpha * v[e];
+                if (use_beta) out = fmaf(beta, yr[e], out);
+                yr[e] = out;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  epilogue_dealloc(sm, warp, tmem);
+}
+
+// C (k x m FP64 column-major) -> Ch, Cl (m_pad x k_pad FP32 row-major = C^T, K-major),
+// zero-padded.
+__global__ void rotate_prep_kernel(const double* __restrict__ C, int64_t ldc, int k, int m,
+                                   int k_pad, int m_pad, float* __restrict__ Ch,
+                                   float* __restrict__ Cl) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<int64_t>(k_pad) * m_pad) return;
+  const int kk = static_cast<int>(idx % k_pad);
+  const int j = static_cast<int>(idx / k_pad);
+  float hi = 0.0f, lo = 0.0f;
+  if (kk < k && j < m) {
+    const double c = C[static_cast<int64_t>(j) * ldc + kk];
+    const float cf = static_cast<float>(c);
+    hi = __uint_as_float(tf32_rna(cf));
+    lo = __uint_as_float(tf32_rna(static_cast<float>(c - static_cast<double>(hi))));
+  }
+  Ch[idx] = hi;
+  Cl[idx] = lo;
+}
+
+// ------------------------------------------------------------ host side ----
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  if (!fn) throw Error(FE_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  return fn;
+}
+
+// 2D FP32 tensor map over rows x cols (row stride ld elements), box box_x x box_y,
+// 128-byte swizzle, zero fill out of bounds.
+CUtensorMap make_map(const float* base, int64_t cols, int64_t rows, int64_t ld, int box_x,
+                     int box_y) {
+  FE_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15u) == 0, "tensor map base not 16-byte aligned");
+  FE_REQUIRE((ld * 4) % 16 == 0, "tensor map row stride not a multiple of 16 bytes");
+  CUtensorMap map;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld * 4)};
+  cuuint32_t box[2] = {static_cast<cuuint32_t>(box_x), static_cast<cuuint32_t>(box_y)};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base),
+                           dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(FE_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
+  return map;
+}
+
+void set_smem_attr(const void* kernel) {
+  FE_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kSmemBytes));
+}
+
+constexpr int kGramTcTargetChunks = 384;
+
+struct TcGramPlan {
+  int k_tiles, m_tiles, chunks;
+  int64_t rows_per_chunk;
+  size_t bytes;
+};
+
+TcGramPlan tc_gram_plan(int64_t n, int64_t kx, int64_t my, int64_t k, int64_t m) {
+  TcGramPlan p{};
+  p.k_tiles = static_cast<int>((kx + kM - 1) / kM);
+  p.m_tiles = static_cast<int>((my + kN - 1) / kN);
+  int64_t chunks = std::min<int64_t>(kGramTcTargetChunks, (n + 4 * kKB - 1) / (4 * kKB));
+  chunks = std::max<int64_t>(chunks, 1);
+  int64_t rpc = (n + chunks - 1) / chunks;
+  rpc = ((rpc + kKB - 1) / kKB) * kKB;
+  p.rows_per_chunk = rpc;
+  p.chunks = static_cast<int>((n + rpc - 1) / rpc);
+  p.bytes = static_cast<size_t>(p.chunks) * k * m * sizeof(float);
+  return p;
+}
+
+}  // namespace
+
+bool tc_gemm_available() {
+  static int ok = -1;
+  if (ok < 0) {
+    int dev = 0, major = 0, minor = 0;
+    ok = (cudaGetDevice(&dev) == cudaSuccess &&
+          cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) == cudaSuccess &&
+          cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) == cudaSuccess &&
+          major == 10 && minor == 0)
+             ? 1
+             : 0;
+  }
+  return ok == 1;
+}
+
+size_t tc_gram_workspace_bytes(int64_t n, int64_t k, int64_t m) {
+  if (n <= 0 || k <= 0 || m <= 0) return 0;
+  // bound over every call with n' <= n, k' <= k, m' <= m (chunk count <= target)
+  const int64_t chunks = std::min<int64_t>(kGramTcTargetChunks, (n + 4 * kKB - 1) / (4 * kKB));
+  return static_cast<size_t>(std::max<int64_t>(chunks, 1)) * k * m * sizeof(float);
+}
+
+// G = X^T Y (FP32 inputs, 3xTF32 tensor cores, FP64 reduction of chunk partials).
+void gram_tc(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n, int64_t k,
+             int64_t m, double* G, int64_t ldg, void* ws, size_t ws_bytes, cudaStream_t s) {
+  FE_REQUIRE(n > 0 && k > 0 && m > 0 && ldg >= k, "gram_tc: invalid shape");
+  FE_REQUIRE(n < (int64_t(1) << 31), "gram_tc: too many rows for 32-bit TMA coordinates");
+  const int sx = static_cast<int>((reinterpret_cast<uintptr_t>(X) & 15u) / 4);
+  const int sy = static_cast<int>((reinterpret_cast<uintptr_t>(Y) & 15u) / 4);
+  const float* Xa = X - sx;
+  const float* Ya = Y - sy;
+  const TcGramPlan p = tc_gram_plan(n, k + sx, m + sy, k, m);
+  FE_REQUIRE(ws && ws_bytes >= p.bytes, "gram_tc: workspace too small");
+  const CUtensorMap mx = make_map(Xa, k + sx, n, ldx, 32, kKB);
+  const CUtensorMap my = make_map(Ya, m + sy, n, ldy, 32, kKB);
+  static std::once_flag once;
+  std::call_once(once, [] { set_smem_attr(reinterpret_cast<const void*>(gram_tc_kernel)); });
+  dim3 grid(p.k_tiles * p.m_tiles, p.chunks);
+  gram_tc_kernel<<<grid, kThreads, kSmemBytes, s>>>(mx, my, n, static_cast<int>(k),
+                                                    static_cast<int>(m), sx, sy, p.k_tiles,
+                                                    p.rows_per_chunk, static_cast<float*>(ws));
+  check_launch("gram_tc_kernel");
+  const int64_t total = k * m;
+  gram_tc_reduce<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
+      static_cast<const float*>(ws), p.chunks, static_cast<int>(k), static_cast<int>(m), G, ldg);
+  check_launch("gram_tc_reduce");
+}
+
+size_t tc_rotate_workspace_bytes(int64_t k, int64_t m) {
+  if (k <= 0 || m <= 0) return 0;
+  const int64_t k_pad = ((k + kKB - 1) / kKB) * kKB;
+  const int64_t m_pad = ((m + kN - 1) / kN) * kN;
+  return static_cast<size_t>(2 * k_pad * m_pad) * sizeof(float);
+}
+
+// Y = alpha X C + beta Y (FP32 blocks, 3xTF32 tensor cores).
+void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float* Y, int64_t ldy,
+               int64_t n, int64_t k, int64_t m, double alpha, double beta, void* ws,
+               size_t ws_bytes, cudaStream_t s) {
+  FE_REQUIRE(n > 0 && k > 0 && m > 0, "rotate_tc: invalid shape");
+  FE_REQUIRE(n < (int64_t(1) << 31), "rotate_tc: too many rows for 32-bit TMA coordinates");
+  FE_REQUIRE((reinterpret_cast<uintptr_t>(X) & 15u) == 0, "rotate_tc: X not 16-byte aligned");
+  const int64_t k_pad = ((k + kKB - 1) / kKB) * kKB;
+  const int64_t m_pad = ((m + kN - 1) / kN) * kN;
+  FE_REQUIRE(ws && ws_bytes >= tc_rotate_workspace_bytes(k, m), "rotate_tc: workspace too small");
+  float* Ch = static_cast<float*>(ws);
+  float* Cl = Ch + k_pad * m_pad;
+  const int64_t total = k_pad * m_pad;
+  rotate_prep_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
+      C, ldc, static_cast<int>(k), static_cast<int>(m), static_cast<int>(k_pad),
+      static_cast<int>(m_pad), Ch, Cl);
+  check_launch("rotate_prep_kernel");
+  const CUtensorMap mx = make_map(X, k, n, ldx, kKB, kM);
+  const CUtensorMap mh = make_map(Ch, k_pad, m_pad, k_pad, kKB, kN);
+  const CUtensorMap ml = make_map(Cl, k_pad, m_pad, k_pad, kKB, kN);
+  static std::once_flag once;
+  std::call_once(once, [] { set_smem_attr(reinterpret_cast<const void*>(rotate_tc_kernel)); });
+  const int64_t row_tiles = (n + kM - 1) / kM;
+  const int64_t m_tiles = m_pad / kN;
+  FE_REQUIRE(row_tiles * m_tiles <= 2147483647LL, "rotate_tc: too many tiles");
+  const bool vec = (reinterpret_cast<uintptr_t>(Y) & 15u) == 0 && ldy % 4 == 0;
+  dim3 grid(static_cast<unsigned>(row_tiles * m_tiles));
+  rotate_tc_kernel<<<grid, kThreads, kSmemBytes, s>>>(mx, mh, ml, n, static_cast<int>(k),
+                                                      static_cast<int>(m),
+                                                      static_cast<int>(m_tiles), Y, ldy,
+                                                      static_cast<float>(alpha),
+                                                      static_cast<float>(beta), beta != 0.0,
+                                                      vec ? 1 : 0);
+  check_launch("rotate_tc_kernel");
+}
+
+int read_tc_status(bool clear) {
+  int v = 0;
+  FE_CHECK_CUDA(cudaMemcpyFromSymbol(&v, g_tc_status, sizeof(int)));
+  if (clear && v != 0) {
+    const int z = 0;
+    FE_CHECK_CUDA(cudaMemcpyToSymbol(g_tc_status, &z, sizeof(int)));
+  }
+  return v;
+}
+
+}  // namespace fe
+
+extern "C" int fe_device_status(int32_t* status, int32_t clear) {
+  return fe::guarded("fe_device_status", [&] {
+    FE_REQUIRE(status, "null status");
+    *status = fe::read_tc_status(clear != 0);
+  });
+}
+
+extern "C" size_t fe_gram_tf32x3_workspace_bytes(int64_t n, int64_t k, int64_t m) {
+  return fe::tc_gram_workspace_bytes(n, k, m);
+}
+
+extern "C" int fe_gram_tf32x3(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n,
+                              int64_t k, int64_t m, double* G, int64_t ldg, void* workspace,
+                              size_t workspace_bytes, void* stream) {
+  return fe::guarded("fe_gram_tf32x3", [&] {
+    FE_REQUIRE(fe::tc_gemm_available(), "tcgen05 kernels need an sm_100 device");
+    FE_REQUIRE(X && Y && ldx >= k && ldy >= m, "invalid input block");
+    FE_REQUIRE(ldx % 4 == 0 && ldy % 4 == 0, "leading dimensions must be multiples of 4");
+    fe::gram_tc(X, ldx, Y, ldy, n, k, m, G, ldg, workspace, workspace_bytes,
+                fe::as_stream(stream));
+  });
+}
+
+extern "C" size_t fe_rotate_tf32x3_workspace_bytes(int64_t k, int64_t m) {
+  return fe::tc_rotate_workspace_bytes(k, m);
+}
+
+extern "C" int fe_rotate_tf32x3(const float* X, int64_t ldx, const double* C, int64_t ldc,
+                                float* Y, int64_t ldy, int64_t n, int64_t k, int64_t m,
+                                double alpha, double beta, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+  return fe::guarded("fe_rotate_tf32x3", [&] {
+    FE_REQUIRE(fe::tc_gemm_available(), "tcgen05 kernels need an sm_100 device");
+    FE_REQUIRE(X && C && Y && ldx >= k && ldc >= k && ldy >= m, "invalid arguments");
+    FE_REQUIRE(ldx % 4 == 0, "ldx must be a multiple of 4");
+    FE_REQUIRE(!fe::ranges_overlap(X, n, ldx, k, static_cast<const float*>(Y), n, ldy, m),
+               "X and Y overlap");
+    fe::rotate_tc(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, workspace, workspace_bytes,
+                  fe::as_stream(stream));
+  });
+}

@@ -141,3 +141,36 @@ def trinv_upper(R: torch.Tensor) -> torch.Tensor:
     out = torch.empty_like(Rs)
     check(lib.fe_trinv_upper_f64(Rs.data_ptr(), k, out.data_ptr(), k, k, _stream()))
     return out.T
+
+
+def gram_tf32x3(X: torch.Tensor, Y: torch.Tensor) -> torch.Tensor:
+    """G = X^T Y on tensor cores (FP32 blocks, 3xTF32 split, FP64 chunk reduction)."""
+    ldx, ldy = _rowmajor(X, "X"), _rowmajor(Y, "Y")
+    n, k = X.shape
+    m = Y.shape[1]
+    Gt = torch.empty((m, k), dtype=torch.float64, device=X.device)
+    need = lib.fe_gram_tf32x3_workspace_bytes(n, k, m)
+    ws = torch.empty(max(need, 8), dtype=torch.uint8, device=X.device)
+    check(lib.fe_gram_tf32x3(X.data_ptr(), ldx, Y.data_ptr(), ldy, n, k, m, Gt.data_ptr(), k,
+                             ws.data_ptr(), need, _stream()))
+    return Gt.T
+
+
+def rotate_tf32x3(X: torch.Tensor, Cm: torch.Tensor, Y: torch.Tensor, alpha: float = 1.0,
+                  beta: float = 0.0):
+    """Y = alpha*X*C + beta*Y on tensor cores (FP32 blocks, 3xTF32 split)."""
+    ldx, ldy = _rowmajor(X, "X"), _rowmajor(Y, "Y")
+    n, k = X.shape
+    m = Cm.shape[1]
+    Cs = colmajor(Cm)
+    need = lib.fe_rotate_tf32x3_workspace_bytes(k, m)
+    ws = torch.empty(max(need, 8), dtype=torch.uint8, device=X.device)
+    check(lib.fe_rotate_tf32x3(X.data_ptr(), ldx, Cs.data_ptr(), k, Y.data_ptr(), ldy, n, k, m,
+                               float(alpha), float(beta), ws.data_ptr(), need, _stream()))
+    return Y
+
+
+def device_status(clear: bool = False) -> int:
+    v = C.c_int32()
+    check(lib.fe_device_status(C.byref(v), 1 if clear else 0))
+    return int(v.value)

@@ -44,6 +44,9 @@ typedef struct fe_csr* fe_csr_t;
 const char* fe_version(void);
 const char* fe_last_error(void);
 int fe_device_count(int* count);
+/* Kernel launches issued by this library since it was loaded (all threads);
+ * library calls made on its behalf (cuSOLVER) are not counted. */
+int64_t fe_launch_count(void);
 
 /* ---------------------------------------------------------------------
  * CSR operator (replaces CudaCsrMatrix, src/gpu/CudaCsrMatrix.cpp:20-52,
@@ -114,6 +117,15 @@ int fe_gram_f32(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_
                 int64_t k, int64_t m, double* G, int64_t ldg, void* workspace,
                 size_t workspace_bytes, void* stream);
 
+/* Tensor-core Gram of FP32 blocks (tcgen05, 3xTF32 split products accumulated
+ * in FP32 per row chunk, chunk partials summed in FP64): FP32-level accuracy
+ * relative to |X|^T |Y|, for the mixed-precision path. Same shapes as
+ * fe_gram_f32; workspace from fe_gram_tf32x3_workspace_bytes. */
+size_t fe_gram_tf32x3_workspace_bytes(int64_t n, int64_t k, int64_t m);
+int fe_gram_tf32x3(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n,
+                   int64_t k, int64_t m, double* G, int64_t ldg, void* workspace,
+                   size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------------
  * Rotation Y = alpha * X * C + beta * Y (replaces
  * MultiVector::right_multiply_active_columns, src/gpu/CudaMultiVector.cpp:310-359,
@@ -128,6 +140,16 @@ int fe_rotate_f64(const double* X, int64_t ldx, const double* C, int64_t ldc, do
 int fe_rotate_f32(const float* X, int64_t ldx, const double* C, int64_t ldc, float* Y,
                   int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
                   void* stream);
+/* Tensor-core rotation of FP32 blocks (tcgen05, 3xTF32 split of X and of C,
+ * FP32 accumulation). X must start 16-byte aligned with ldx a multiple of 4;
+ * the workspace holds the split FP32 copies of C. */
+size_t fe_rotate_tf32x3_workspace_bytes(int64_t k, int64_t m);
+int fe_rotate_tf32x3(const float* X, int64_t ldx, const double* C, int64_t ldc, float* Y,
+                     int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
+                     void* workspace, size_t workspace_bytes, void* stream);
+/* First failure code recorded by a bounded device-side wait of the tensor-core
+ * kernels (0 = none); clear != 0 resets it. */
+int fe_device_status(int32_t* status, int32_t clear);
 
 /* ---------------------------------------------------------------------
  * Ritz residuals and column norms (replaces the copy + add_scaled_columns +

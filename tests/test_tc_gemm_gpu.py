@@ -1,0 +1,83 @@
+"""tcgen05 split-TF32 Gram and rotation against FP64 references.
+
+Tolerance (componentwise): |G - G_ref| <= 4e-6 |X|^T|Y| for the Gram (3xTF32
+products carry ~2^-22 relative error, FP32 accumulation per 32-row block, FP64
+across chunks), |Y - Y_ref| <= (k + 4) 2^-22 (|X||C| + |beta||Y|) for the rotation.
+Each test also checks the device status word of the bounded waits."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def blk(n, b, seed, ld=None):
+    g = torch.Generator().manual_seed(seed)
+    ld = ld or b
+    t = torch.randn(n, ld, generator=g, dtype=torch.float64).float().cuda()
+    return t[:, :b] if ld != b else t
+
+
+@pytest.mark.parametrize("n,k,m", [(128, 8, 8), (1000, 17, 33), (4096, 128, 160), (5000, 160, 128),
+                                   (33333, 64, 320), (70001, 320, 320), (2048, 300, 5)])
+def test_gram_tf32x3(n, k, m):
+    from fasteig_b200 import ops
+    assert ops.device_status(clear=True) == 0
+    X = blk(n, k, 1, ld=((k + 3) // 4) * 4)
+    Y = blk(n, m, 2, ld=((m + 3) // 4) * 4)
+    G = ops.gram_tf32x3(X, Y)
+    torch.cuda.synchronize()
+    assert ops.device_status() == 0
+    X64, Y64 = X.double().cpu().numpy(), Y.double().cpu().numpy()
+    ref = X64.T @ Y64
+    scale = np.abs(X64).T @ np.abs(Y64)
+    err = np.abs(G.cpu().numpy() - ref)
+    assert np.all(err <= 4e-6 * scale + 1e-30), (err / scale).max()
+
+
+def test_gram_tf32x3_column_offset_views():
+    from fasteig_b200 import ops
+    base = blk(9000, 64, 3)
+    X = base[:, 0:13]       # aligned start
+    Y = base[:, 13:50]      # start not 16-byte aligned: shifted tensor map
+    G = ops.gram_tf32x3(X, Y)
+    torch.cuda.synchronize()
+    X64, Y64 = X.double().cpu().numpy(), Y.double().cpu().numpy()
+    np.testing.assert_allclose(G.cpu().numpy(), X64.T @ Y64, rtol=0,
+                               atol=4e-6 * (np.abs(X64).T @ np.abs(Y64)).max())
+
+
+def test_gram_tf32x3_deterministic():
+    from fasteig_b200 import ops
+    X = blk(100000, 96, 4)
+    assert torch.equal(ops.gram_tf32x3(X, X).clone(), ops.gram_tf32x3(X, X))
+
+
+@pytest.mark.parametrize("n,k,m", [(128, 8, 8), (1000, 17, 33), (4100, 320, 320), (777, 64, 160),
+                                   (20000, 256, 320), (3000, 5, 300)])
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.0, 1.0)])
+def test_rotate_tf32x3(n, k, m, alpha, beta):
+    from fasteig_b200 import ops
+    assert ops.device_status(clear=True) == 0
+    X = blk(n, k, 5, ld=((k + 3) // 4) * 4)
+    Y = blk(n, m, 6)
+    Cm = torch.randn(k, m, dtype=torch.float64, generator=torch.Generator().manual_seed(7)).cuda()
+    X64, Y64, C64 = X.double().cpu().numpy(), Y.double().cpu().numpy(), Cm.cpu().numpy()
+    ref = alpha * X64 @ C64 + (beta * Y64 if beta else 0.0)
+    ops.rotate_tf32x3(X, Cm, Y, alpha, beta)
+    torch.cuda.synchronize()
+    assert ops.device_status() == 0
+    scale = np.abs(X64) @ np.abs(C64) + (abs(beta) * np.abs(Y64) if beta else 0.0)
+    err = np.abs(Y.double().cpu().numpy() - ref)
+    assert np.all(err <= (k + 4) * 2.0 ** -22 * scale + 1e-30), (err / scale).max()
+
+
+def test_rotate_tf32x3_output_column_view():
+    from fasteig_b200 import ops
+    V = blk(5000, 40, 8)
+    Cm = torch.randn(13, 27, dtype=torch.float64).cuda()
+    ref = V[:, :13].double() @ Cm * -1.0 + V[:, 13:40].double()
+    ops.rotate_tf32x3(V[:, :13], Cm, V[:, 13:40], -1.0, 1.0)  # X - V*H into the next columns
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(V[:, 13:40].double().cpu().numpy(), ref.cpu().numpy(),
+                               rtol=0, atol=2e-5 * np.abs(ref.cpu().numpy()).max())
