@@ -60,6 +60,7 @@ _SIGS = {
     "fe_rotate_tf32x3": (C.c_int, [vp, i64, vp, i64, vp, i64, i64, i64, i64, f64, f64, vp, sz,
                                    vp]),
     "fe_device_status": (C.c_int, [C.POINTER(C.c_int32), C.c_int32]),
+    "fe_set_spmm_kernel": (C.c_int, [C.c_int32]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

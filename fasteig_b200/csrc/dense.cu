@@ -179,6 +179,8 @@ Csr* csr_create(int64_t rows, int64_t cols, int64_t nnz, const int32_t* rowptr,
   A->rows = rows;
   A->cols = cols;
   A->nnz = nnz;
+  for (int64_t i = 0; i < rows; ++i)
+    A->max_row_nnz = std::max<int64_t>(A->max_row_nnz, rowptr[i + 1] - rowptr[i]);
   FE_CHECK_CUDA(cudaGetDevice(&A->device));
   try {
     FE_CHECK_CUDA(cudaMalloc(&A->rowptr, (rows + 1) * sizeof(int32_t)));

@@ -98,6 +98,7 @@ struct Csr {
   double* val64 = nullptr;
   float* val32 = nullptr;
   int device = 0;
+  int64_t max_row_nnz = 0;
 };
 
 int num_sms();

@@ -242,7 +242,329 @@ void dispatch_vec(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, in
 #undef FE_LAUNCH
 }
 
+// ---------------------------------------------------------------------------
+// Bulk-copy pipelined SpMM (the path for matrices whose rows have at most a
+// few tens of nonzeros, e.g. the 7-, 13- and 27-point stencils).
+//
+// One warp owns a sequence of rows (row = global_warp + i * total_warps) and
+// keeps kPipeDepth rows in flight: for the next rows it issues one
+// cp.async.bulk (TMA bulk copy, 16-byte aligned, no registers held) per nonzero
+// to gather the neighbour rows of X, plus one for the Z row, into a per-warp
+// shared-memory stage tracked by an mbarrier with a transaction count. While
+// those copies land, the warp accumulates the previous row from shared memory.
+// This removes the chain of dependent global loads per row that bounds the
+// register-only kernel and keeps ~128 KB per SM in flight.
+// ---------------------------------------------------------------------------
+constexpr int kPipeWarps = 8;
+constexpr int kPipeDepth = 2;
+constexpr int kPipeMaxSlots = 32;
+constexpr int kPipeStageBytes = 10240;  // per warp and stage: slots * row bytes
+
+__device__ int g_spmm_status = 0;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void pipe_bar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
+}
+
+__device__ __forceinline__ void pipe_arrive_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool pipe_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait (about two seconds of SM clock); records `code` on timeout.
+__device__ __forceinline__ bool pipe_wait(uint64_t* bar, uint32_t parity, int code) {
+  if (pipe_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (true) {
+    for (int i = 0; i < 64; ++i)
+      if (pipe_try_wait(bar, parity)) return true;
+    if (clock64() - t0 > 4000000000LL) {
+      atomicCAS(&g_spmm_status, 0, code);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+template <typename T>
+struct PipeLayout {
+  uint64_t* bars;   // [warps][depth]
+  int32_t* nnz;     // [warps][depth]
+  int32_t* cols;    // [warps][depth][kPipeMaxSlots]
+  T* vals;          // [warps][depth][kPipeMaxSlots]
+  uint8_t* data;    // [warps][depth][slots][row_bytes]
+};
+
+template <typename T>
+__device__ __forceinline__ PipeLayout<T> pipe_layout(uint8_t* smem) {
+  PipeLayout<T> L;
+  L.bars = reinterpret_cast<uint64_t*>(smem);
+  L.nnz = reinterpret_cast<int32_t*>(smem + kPipeWarps * kPipeDepth * 8);
+  L.cols = L.nnz + kPipeWarps * kPipeDepth;
+  L.vals = reinterpret_cast<T*>(L.cols + kPipeWarps * kPipeDepth * kPipeMaxSlots);
+  uintptr_t d = reinterpret_cast<uintptr_t>(L.vals + kPipeWarps * kPipeDepth * kPipeMaxSlots);
+  d = (d + 127) & ~uintptr_t(127);
+  L.data = reinterpret_cast<uint8_t*>(d);
+  return L;
+}
+
+template <typename T>
+constexpr size_t pipe_smem_bytes() {
+  return kPipeWarps * kPipeDepth * (8 + 4 + kPipeMaxSlots * (4 + sizeof(T))) + 128 +
+         static_cast<size_t>(kPipeWarps) * kPipeDepth * kPipeStageBytes;
+}
+
+template <typename T, int VEC, int CPL>
+__global__ void __launch_bounds__(kPipeWarps * 32, 1)
+csr_spmm_pipe_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
+                     const int32_t* __restrict__ colind, const T* __restrict__ vals,
+                     const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
+                     int64_t ldz, int ncols, int panel_cols, int slots, T alpha, T gamma, T beta,
+                     int use_gamma, int use_beta) {
+  extern __shared__ __align__(128) uint8_t pipe_smem[];
+  const PipeLayout<T> L = pipe_layout<T>(pipe_smem);
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  const int panel0 = blockIdx.y * panel_cols;
+  const int width = min(panel_cols, ncols - panel0);
+  const uint32_t row_bytes = static_cast<uint32_t>(width) * sizeof(T);
+  const int nvec = width / VEC;
+  const int64_t gwarp = static_cast<int64_t>(blockIdx.x) * kPipeWarps + warp;
+  const int64_t twarps = static_cast<int64_t>(gridDim.x) * kPipeWarps;
+
+  uint64_t* bars = L.bars + warp * kPipeDepth;
+  int32_t* m_nnz = L.nnz + warp * kPipeDepth;
+  int32_t* m_cols = L.cols + warp * kPipeDepth * kPipeMaxSlots;
+  T* m_vals = L.vals + warp * kPipeDepth * kPipeMaxSlots;
+  uint8_t* m_data = L.data + static_cast<size_t>(warp) * kPipeDepth * kPipeStageBytes;
+
+  if (lane == 0) {
+    for (int s = 0; s < kPipeDepth; ++s) pipe_bar_init(&bars[s]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncwarp();
+
+  // Gather row r's neighbour rows (and its Z row) into stage s.
+  auto issue = [&](int64_t r, int s) {
+    const int start = __ldg(rowptr + r);
+    const int nnz = __ldg(rowptr + r + 1) - start;
+    uint8_t* stage = m_data + s * kPipeStageBytes;
+    if (nnz > slots - 1) {  // too many neighbours: the consumer reads them directly
+      if (lane == 0) {
+        m_nnz[s] = -1;
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&bars[s]))
+                     : "memory");
+      }
+      __syncwarp();
+      return;
+    }
+    int c = 0;
+    if (lane < nnz) {
+      c = __ldg(colind + start + lane);
+      m_cols[s * kPipeMaxSlots + lane] = c;
+      m_vals[s * kPipeMaxSlots + lane] = __ldg(vals + start + lane);
+    }
+    if (lane == 0) {
+      m_nnz[s] = nnz;
+      pipe_arrive_tx(&bars[s], static_cast<uint32_t>(nnz + use_beta) * row_bytes);
+    }
+    __syncwarp();
+    if (lane < nnz) bulk_g2s(stage + lane * row_bytes, X + static_cast<int64_t>(c) * ldx + panel0,
+                             row_bytes, &bars[s]);
+    if (use_beta && lane == 31)
+      bulk_g2s(stage + (slots - 1) * row_bytes, Z + r * ldz + panel0, row_bytes, &bars[s]);
+  };
+
+  for (int s = 0; s < kPipeDepth; ++s) {
+    const int64_t r = gwarp + s * twarps;
+    if (r < nrows) issue(r, s);
+  }
+
+  bool ok = true;
+  for (int64_t i = 0;; ++i) {
+    const int64_t r = gwarp + i * twarps;
+    if (r >= nrows) break;
+    const int s = static_cast<int>(i % kPipeDepth);
+    const uint32_t parity = static_cast<uint32_t>((i / kPipeDepth) & 1);
+    if (!pipe_wait(&bars[s], parity, 11)) {
+      ok = false;
+      break;
+    }
+    const int nnz = m_nnz[s];
+    const uint8_t* stage = m_data + s * kPipeStageBytes;
+    T acc[CPL][VEC];
+#pragma unroll
+    for (int q = 0; q < CPL; ++q)
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) acc[q][e] = T(0);
+    int self_slot = -1;
+    if (nnz >= 0) {
+      for (int k = 0; k < nnz; ++k) {
+        const T a = m_vals[s * kPipeMaxSlots + k];
+        if (m_cols[s * kPipeMaxSlots + k] == r) self_slot = k;
+        const T* xs = reinterpret_cast<const T*>(stage + k * row_bytes);
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) {
+          const int v = lane + q * 32;
+          if (v < nvec) {
+            const Pack<T, VEC> p = load_pack_rw<T, VEC>(xs + v * VEC);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) acc[q][e] = fma(a, p.v[e], acc[q][e]);
+          }
+        }
+      }
+    } else {
+      const int start = __ldg(rowptr + r);
+      const int end = __ldg(rowptr + r + 1);
+      for (int base = start; base < end; base += 32) {
+        const int k = base + lane;
+        int c = 0;
+        T a = T(0);
+        if (k < end) {
+          c = __ldg(colind + k);
+          a = __ldg(vals + k);
+        }
+        const int cnt = min(32, end - base);
+        for (int t = 0; t < cnt; ++t) {
+          const int c0 = __shfl_sync(0xffffffffu, c, t);
+          const T a0 = __shfl_sync(0xffffffffu, a, t);
+          const T* x0 = X + static_cast<int64_t>(c0) * ldx + panel0;
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) {
+            const int v = lane + q * 32;
+            if (v < nvec) {
+              const Pack<T, VEC> p = load_pack<T, VEC>(x0 + v * VEC);
+#pragma unroll
+              for (int e = 0; e < VEC; ++e) acc[q][e] = fma(a0, p.v[e], acc[q][e]);
+            }
+          }
+        }
+      }
+    }
+    const T* xself = (self_slot >= 0)
+                         ? reinterpret_cast<const T*>(stage + self_slot * row_bytes)
+                         : X + r * ldx + panel0;
+    const T* zrow = (nnz >= 0) ? reinterpret_cast<const T*>(stage + (slots - 1) * row_bytes)
+                               : Z + r * ldz + panel0;
+    T* yrow = Y + r * ldy + panel0;
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) {
+      const int v = lane + q * 32;
+      if (v < nvec) {
+        Pack<T, VEC> out;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) out.v[e] = alpha * acc[q][e];
+        if (use_gamma) {
+          const Pack<T, VEC> xr = load_pack_rw<T, VEC>(xself + v * VEC);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) out.v[e] = fma(gamma, xr.v[e], out.v[e]);
+        }
+        if (use_beta) {
+          const Pack<T, VEC> zr = load_pack_rw<T, VEC>(zrow + v * VEC);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) out.v[e] = fma(beta, zr.v[e], out.v[e]);
+        }
+        store_pack<T, VEC>(yrow + v * VEC, out);
+      }
+    }
+    __syncwarp();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    const int64_t rn = gwarp + (i + kPipeDepth) * twarps;
+    if (rn < nrows) issue(rn, s);
+  }
+  if (!ok) {
+    // Let copies already issued for this warp land before the CTA exits.
+    for (int s = 0; s < kPipeDepth; ++s) pipe_wait(&bars[s], 0, 12);
+  }
+}
+
+template <typename T, int VEC>
+bool try_pipe(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
+              int64_t ldz, int ncols, T alpha, T gamma, T beta, bool ug, bool ub, cudaStream_t s) {
+  // Panel width: the widest multiple of 32 vectors whose rows fit the stage
+  // with one slot per neighbour plus the Z row.
+  const int need_slots = static_cast<int>(A.max_row_nnz) + 1;
+  if (need_slots > kPipeMaxSlots) return false;
+  const int max_row_bytes = (kPipeStageBytes / need_slots) & ~15;
+  int panel = std::min(ncols, max_row_bytes / static_cast<int>(sizeof(T)));
+  panel = std::min(panel, 8 * 32 * VEC);  // CPL <= 8
+  if (panel < VEC || panel * static_cast<int>(sizeof(T)) % 16 != 0) return false;
+  if (panel < ncols) panel = (panel / (32 * VEC)) * 32 * VEC;  // full-warp panels when split
+  if (panel <= 0 || (ncols % panel) * sizeof(T) % 16 != 0) return false;
+  const int slots = std::min(kPipeMaxSlots, kPipeStageBytes / (panel * static_cast<int>(sizeof(T))));
+  if (slots < need_slots) return false;
+  const int cpl = (panel / VEC + 31) / 32;
+  const size_t smem = pipe_smem_bytes<T>();
+  static bool attr_set[9] = {false};
+  const int sms = num_sms();
+  dim3 grid(static_cast<unsigned>(sms), static_cast<unsigned>((ncols + panel - 1) / panel));
+#define FE_PIPE(CPL_)                                                                          \
+  do {                                                                                         \
+    auto kern = csr_spmm_pipe_kernel<T, VEC, CPL_>;                                            \
+    if (!attr_set[CPL_]) {                                                                     \
+      FE_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                         static_cast<int>(smem)));                             \
+      attr_set[CPL_] = true;                                                                   \
+    }                                                                                          \
+    kern<<<grid, kPipeWarps * 32, smem, s>>>(A.rows, A.rowptr, A.colind, vals, X, ldx, Y, ldy, \
+                                             Z, ldz, ncols, panel, slots, alpha, gamma, beta,  \
+                                             ug ? 1 : 0, ub ? 1 : 0);                          \
+    check_launch("csr_spmm_pipe_kernel");                                                      \
+  } while (0)
+  switch (cpl) {
+    case 1: FE_PIPE(1); break;
+    case 2: FE_PIPE(2); break;
+    case 3: FE_PIPE(3); break;
+    case 4: FE_PIPE(4); break;
+    case 5: FE_PIPE(5); break;
+    case 6: FE_PIPE(6); break;
+    default: FE_PIPE(8); break;
+  }
+#undef FE_PIPE
+  return true;
+}
+
 }  // namespace
+
+int read_spmm_status(bool clear) {
+  int v = 0;
+  FE_CHECK_CUDA(cudaMemcpyFromSymbol(&v, g_spmm_status, sizeof(int)));
+  if (clear && v != 0) {
+    const int z = 0;
+    FE_CHECK_CUDA(cudaMemcpyToSymbol(g_spmm_status, &z, sizeof(int)));
+  }
+  return v;
+}
+
+// Kernel selection for csr_spmm: "pipe" (bulk-copy pipelined) or "warp" (registers only).
+static int g_spmm_mode = 0;  // 0 = auto, 1 = force register kernel, 2 = prefer pipeline
+void set_spmm_mode(int mode) { g_spmm_mode = mode; }
 
 // Shared entry used by the C ABI and the host solver.
 template <typename T>
@@ -265,6 +587,12 @@ void csr_spmm(const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T*
   const bool vec_ok = ncols % VEC == 0 && ldx % VEC == 0 && ldy % VEC == 0 && aligned16(X) &&
                       aligned16(Y) && (!ub || (ldz % VEC == 0 && aligned16(Z)));
   if (vec_ok) {
+    // The pipelined kernel needs 16-byte aligned row gathers (vec_ok) and rows
+    // that fit a stage; it pays off once a row slab is at least 64 bytes.
+    if (g_spmm_mode != 1 && ncols * static_cast<int64_t>(sizeof(T)) >= 64 &&
+        try_pipe<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
+                         T(gamma), T(beta), ug, ub, s))
+      return;
     dispatch_vec<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                          T(gamma), T(beta), ug, ub, s);
   } else {

@@ -33,6 +33,9 @@
 
 namespace fe {
 
+int read_spmm_status(bool clear);
+void set_spmm_mode(int mode);
+
 __device__ int g_tc_status = 0;  // 0 = ok, otherwise a code of the first failed wait
 
 namespace {
@@ -115,15 +118,20 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-// UMMA shared-memory descriptor (SM100 version 1) with 128-byte swizzle.
+// UMMA shared-memory descriptor (SM100 version 1). Layout types: 2 = 128-byte
+// swizzle of 16-byte chunks (K-major operands); 1 = 128-byte swizzle of 32-byte
+// chunks, the only MN-major layout the tensor cores accept for TF32.
+constexpr uint32_t kLayoutSW128 = 2;
+constexpr uint32_t kLayoutSW128Base32 = 1;
+
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes,
-                                              uint32_t sbo_bytes) {
+                                              uint32_t sbo_bytes, uint32_t layout) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
   d |= static_cast<uint64_t>((lbo_bytes >> 4) & 0x3FFFu) << 16;
   d |= static_cast<uint64_t>((sbo_bytes >> 4) & 0x3FFFu) << 32;
   d |= static_cast<uint64_t>(1) << 46;  // version (SM100)
-  d |= static_cast<uint64_t>(2) << 61;  // SWIZZLE_128B
+  d |= static_cast<uint64_t>(layout & 7u) << 61;
   return d;
 }
 
@@ -265,14 +273,16 @@ __device__ __forceinline__ void epilogue_dealloc(const Smem& sm, int warp, uint3
 
 // MMA issue loop shared by both kernels. Operand descriptors per K-step (8
 // elements of K): K-major tiles advance 32 bytes inside the 128-byte swizzle
-// row; MN-major tiles advance one 1024-byte swizzle atom (8 rows).
+// row; MN-major tiles advance 8 rows (1024 bytes, two 4-row swizzle atoms).
 template <bool kMN>
 __device__ void mma_loop(const Smem& sm, uint32_t tmem, int nkb, uint32_t idesc) {
-  // K-major: SBO = 1024 (8 rows x 128 B), LBO unused (16). MN-major: LBO = bytes
-  // between 32-element column groups (one TMA box of 32 rows x 128 B = 4096),
-  // SBO = 1024 (8 rows).
+  // K-major (16-byte swizzle atoms of 8 rows x 128 B): SBO = 1024, LBO unused (16).
+  // MN-major (32-byte swizzle atoms of 4 rows x 128 B): LBO = bytes between
+  // 32-element column groups (one TMA box of 32 rows x 128 B = 4096), SBO = 512
+  // between 4-row groups.
   const uint32_t lbo = kMN ? 4096u : 16u;
-  const uint32_t sbo = 1024u;
+  const uint32_t sbo = kMN ? 512u : 1024u;
+  const uint32_t layout = kMN ? kLayoutSW128Base32 : kLayoutSW128;
   for (int kb = 0; kb < nkb; ++kb) {
     const int s = kb % kStages;
     const uint32_t ph = (kb / kStages) & 1u;
@@ -283,8 +293,10 @@ __device__ void mma_loop(const Smem& sm, uint32_t tmem, int nkb, uint32_t idesc)
 #pragma unroll
     for (int k = 0; k < kKB / 8; ++k) {
       const uint32_t off = kMN ? k * 1024u : k * 32u;
-      const uint64_t dah = smem_desc(ah + off, lbo, sbo), dal = smem_desc(al + off, lbo, sbo);
-      const uint64_t dbh = smem_desc(bh + off, lbo, sbo), dbl = smem_desc(bl + off, lbo, sbo);
+      const uint64_t dah = smem_desc(ah + off, lbo, sbo, layout);
+      const uint64_t dal = smem_desc(al + off, lbo, sbo, layout);
+      const uint64_t dbh = smem_desc(bh + off, lbo, sbo, layout);
+      const uint64_t dbl = smem_desc(bl + off, lbo, sbo, layout);
       const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
       umma_tf32(tmem, dah, dbh, idesc, acc);
       umma_tf32(tmem, dah, dbl, idesc, 1u);
@@ -518,9 +530,10 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // 2D FP32 tensor map over rows x cols (row stride ld elements), box box_x x box_y,
-// 128-byte swizzle, zero fill out of bounds.
+// 128-byte swizzle (16-byte chunks for K-major operands, 32-byte chunks for the
+// MN-major TF32 operands of the Gram), zero fill out of bounds.
 CUtensorMap make_map(const float* base, int64_t cols, int64_t rows, int64_t ld, int box_x,
-                     int box_y) {
+                     int box_y, bool swizzle_32b_atoms = false) {
   FE_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15u) == 0, "tensor map base not 16-byte aligned");
   FE_REQUIRE((ld * 4) % 16 == 0, "tensor map row stride not a multiple of 16 bytes");
   CUtensorMap map;
@@ -530,7 +543,9 @@ CUtensorMap make_map(const float* base, int64_t cols, int64_t rows, int64_t ld, 
   cuuint32_t estr[2] = {1, 1};
   CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base),
                            dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           swizzle_32b_atoms ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B
+                                             : CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw Error(FE_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
   return map;
@@ -597,8 +612,8 @@ void gram_tc(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n
   const float* Ya = Y - sy;
   const TcGramPlan p = tc_gram_plan(n, k + sx, m + sy, k, m);
   FE_REQUIRE(ws && ws_bytes >= p.bytes, "gram_tc: workspace too small");
-  const CUtensorMap mx = make_map(Xa, k + sx, n, ldx, 32, kKB);
-  const CUtensorMap my = make_map(Ya, m + sy, n, ldy, 32, kKB);
+  const CUtensorMap mx = make_map(Xa, k + sx, n, ldx, 32, kKB, true);
+  const CUtensorMap my = make_map(Ya, m + sy, n, ldy, 32, kKB, true);
   static std::once_flag once;
   std::call_once(once, [] { set_smem_attr(reinterpret_cast<const void*>(gram_tc_kernel)); });
   dim3 grid(p.k_tiles * p.m_tiles, p.chunks);
@@ -670,7 +685,16 @@ int read_tc_status(bool clear) {
 extern "C" int fe_device_status(int32_t* status, int32_t clear) {
   return fe::guarded("fe_device_status", [&] {
     FE_REQUIRE(status, "null status");
-    *status = fe::read_tc_status(clear != 0);
+    const int a = fe::read_tc_status(clear != 0);
+    const int b = fe::read_spmm_status(clear != 0);
+    *status = a != 0 ? a : b;
+  });
+}
+
+extern "C" int fe_set_spmm_kernel(int32_t mode) {
+  return fe::guarded("fe_set_spmm_kernel", [&] {
+    FE_REQUIRE(mode >= 0 && mode <= 1, "mode must be 0 (auto) or 1 (register kernel)");
+    fe::set_spmm_mode(mode);
   });
 }
 

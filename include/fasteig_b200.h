@@ -148,8 +148,12 @@ int fe_rotate_tf32x3(const float* X, int64_t ldx, const double* C, int64_t ldc, 
                      int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
                      void* workspace, size_t workspace_bytes, void* stream);
 /* First failure code recorded by a bounded device-side wait of the tensor-core
- * kernels (0 = none); clear != 0 resets it. */
+ * or pipelined SpMM kernels (0 = none); clear != 0 resets it. */
 int fe_device_status(int32_t* status, int32_t clear);
+/* SpMM kernel selection for all later calls in the process: 0 = automatic
+ * (bulk-copy pipelined kernel when the rows fit its stages, else the
+ * register kernel), 1 = always the register kernel. */
+int fe_set_spmm_kernel(int32_t mode);
 
 /* ---------------------------------------------------------------------
  * Ritz residuals and column norms (replaces the copy + add_scaled_columns +

@@ -73,6 +73,63 @@ def test_spmm_matches_oracle(dtype, n, b, alpha, beta):
     assert np.all(np.abs(got - ref) <= tol * scale + 1e-300)
 
 
+@pytest.fixture
+def register_kernel():
+    import fasteig_b200 as fe
+    assert fe.lib.fe_set_spmm_kernel(1) == 0
+    yield
+    assert fe.lib.fe_set_spmm_kernel(0) == 0
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("stencil", ["star1", "star2", "box"])
+@pytest.mark.parametrize("b", [16, 40, 320, 1000])
+def test_pipelined_and_register_spmm_agree_on_stencils(dtype, stencil, b):
+    """Bulk-copy pipelined kernel (7/13/27-point rows) vs the register kernel vs
+    the oracle, including multi-panel widths and the fused Chebyshev epilogue."""
+    import fasteig_b200 as fe
+    from fasteig_b200 import matrices as M, ops
+    from oracle import oracle as O
+    if stencil == "box":
+        H, _ = M.stiffness_mass_27pt(10, seed=1)
+    else:
+        H = M.laplacian_wells(10, wells=4, seed=1, stencil=stencil)
+    A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
+    dA = dev_csr(A)
+    X = block(H.n, b, dtype, 1)
+    Z = block(H.n, b, dtype, 2)
+    Xn, Zn = X.double().cpu().numpy(), Z.double().cpu().numpy()
+    ref = 0.7 * (A.scipy() @ Xn) - 0.2 * Xn - Zn
+    outs = []
+    for mode in (0, 1):
+        assert fe.lib.fe_set_spmm_kernel(mode) == 0
+        Zc = Z.clone()
+        ops.cheb_step(dA, X, Zc, Zc, 0.7, -0.2, -1.0)
+        torch.cuda.synchronize()
+        outs.append(Zc.double().cpu().numpy())
+    assert fe.lib.fe_set_spmm_kernel(0) == 0
+    assert ops.device_status(clear=True) == 0
+    scale = 0.7 * (absA(A) @ np.abs(Xn)) + 0.2 * np.abs(Xn) + np.abs(Zn)
+    tol = 1e-13 if dtype == torch.float64 else 4e-6
+    for got in outs:
+        assert np.all(np.abs(got - ref) <= tol * scale + 1e-300)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_spmm_register_kernel_forced(dtype, register_kernel):
+    from fasteig_b200 import ops
+    n, b = 3000, 320
+    A = rand_sym_csr(n, 0.003, seed=5)
+    dA = dev_csr(A)
+    X = block(n, b, dtype, 1)
+    Y = block(n, b, dtype, 2)
+    X64 = X.double().cpu().numpy()
+    ops.spmm(dA, X, Y)
+    torch.cuda.synchronize()
+    tol = 1e-13 if dtype == torch.float64 else 4e-6
+    assert np.all(np.abs(Y.double().cpu().numpy() - A.scipy() @ X64) <= tol * (absA(A) @ np.abs(X64)) + 1e-300)
+
+
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
 def test_spmm_unaligned_leading_dimension_scalar_path(dtype):
     from fasteig_b200 import ops
