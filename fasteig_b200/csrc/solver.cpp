@@ -67,7 +67,7 @@ struct Options {
   std::string bounds = "reference";  // reference | ritz
   double amplification = 1.0e3;    // filter amplification cap at the lower bound
   std::string init = "host";       // host (std::mt19937, bit-exact) | device
-  double mixed_switch = 2.0e-6;    // FP32 -> FP64 switch when max residual <= this
+  double mixed_switch = 4.0e-6;    // FP32 -> FP64 switch when max residual <= this
   bool tensor_cores = true;        // FP32 Grams/rotations on tcgen05 (3xTF32)
 
   void parse(const char* text) {
@@ -149,6 +149,31 @@ struct Options {
 struct Stats {
   double iterations = 0, status = 0, seconds = 0, fp32_iterations = 0, fp64_iterations = 0;
   double spmm_launches = 0, lower = 0, upper = 0;
+  // device time per phase (ms, CUDA events on the solver stream)
+  double filter_ms = 0, ortho_ms = 0, rr_ms = 0, precise_grams = 0;
+};
+
+// Events bracketing the phases of one filter cycle.
+struct PhaseEvents {
+  cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+  PhaseEvents() {
+    for (auto& x : e) FE_CHECK_CUDA(cudaEventCreate(&x));
+  }
+  ~PhaseEvents() {
+    for (auto& x : e)
+      if (x) cudaEventDestroy(x);
+  }
+  void record(int i, cudaStream_t s) { FE_CHECK_CUDA(cudaEventRecord(e[i], s)); }
+  // after a stream sync
+  void accumulate(Stats& st) {
+    float a = 0, b = 0, c = 0;
+    FE_CHECK_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
+    FE_CHECK_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
+    FE_CHECK_CUDA(cudaEventElapsedTime(&c, e[2], e[3]));
+    st.filter_ms += a;
+    st.ortho_ms += b;
+    st.rr_ms += c;
+  }
 };
 
 class Context {
@@ -432,6 +457,7 @@ struct ChebLoop {
   int64_t n, nev, cap, degree;
   double sign, lower, upper;
   bool cholqr2;
+  PhaseEvents ev;
 
   ChebLoop(Context& c, const Csr& a, const Options& o, SmallState& s, ProjectedEig& e, double sg,
            double lo, double up, bool two_pass)
@@ -445,6 +471,7 @@ struct ChebLoop {
     cudaStream_t s = ctx.stream;
     const int64_t active = sub - locked;
     FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, 4 * sizeof(int32_t), s));
+    ev.record(0, s);
     // 1. Filter Y = T_degree(c*op + d*I) X_active, in place on V's active columns.
     if (upper != cutoff) {
       const double c = 2.0 / (upper - cutoff);
@@ -455,6 +482,7 @@ struct ChebLoop {
       filter(b.V.col(locked), b.V.ld, b.S.data(), b.S.ld, active, sign * c, d);
       st.spmm_launches += static_cast<double>(degree);
     }
+    ev.record(1, s);
     // 2. Deflate against locked vectors with two-pass block Gram-Schmidt
     // (block_gram_schmidt, src/core/Orthogonalization.cpp:482-527).
     if (locked > 0) {
@@ -472,6 +500,7 @@ struct ChebLoop {
     } else {
       cholqr<T>(ctx, sm, b.V.data(), b.V.ld, b.Q.data(), b.Q.ld, n, sub, 0);
     }
+    ev.record(2, s);
     // 4. Rayleigh-Ritz: AQ = op*Q, P = Q^T AQ, eig(P), rotate Q and AQ, residuals.
     csr_spmm<T>(A, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, nullptr, 0, sub, sign, 0.0, 0.0, s);
     st.spmm_launches += 1;
@@ -490,7 +519,9 @@ struct ChebLoop {
     ctx.to_host(rel.data(), sm.rel.as<double>(), sub);
     ctx.to_host(info_host, sm.info.as<int32_t>(), 2);
     ctx.to_host(info_host + 2, eig.info(), 1);
+    ev.record(3, s);
     ctx.sync();
+    ev.accumulate(st);
   }
 
   void filter(T* X, int64_t ldx, T* Sc, int64_t lds, int64_t cols, double c, double d) {
@@ -644,10 +675,33 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
       while (locked < nev && rel[locked] <= tol) ++locked;
     }
   }
-  // Results: eigenvalues (sign restored), residuals, first nev Ritz vectors.
-  for (int64_t j = 0; j < nev; ++j) {
-    eigenvalues[j] = sign * W[j];
-    residuals[j] = rel[j];
+  // Results: eigenvalues (sign restored) and the FP64 residual check of the
+  // returned vectors on the device: ||A x - l x|| / ((1 + |l|) ||x||), which
+  // fasteig_problem::solve recomputes for non-Krylov solvers on the host
+  // (src/fasteig_problem.cpp:419-422, src/fasteig_solver.cpp:89-129).
+  for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = sign * W[j];
+  {
+    cudaStream_t s = ctx.stream;
+    Block<double> Xf, AXf;
+    const double* Xp = nullptr;
+    int64_t ldx = 0;
+    if (l64) {
+      Xp = l64->b.V.data();
+      ldx = l64->b.V.ld;
+    } else {
+      Xf.allocate(n, cap);
+      convert<float, double>(l32->b.V.data(), l32->b.V.ld, Xf.data(), Xf.ld, n, nev, s);
+      Xp = Xf.data();
+      ldx = Xf.ld;
+    }
+    AXf.allocate(n, cap);  // same leading dimension as the vector block
+    csr_spmm<double>(A, Xp, ldx, AXf.data(), AXf.ld, nullptr, 0, nev, 1.0, 0.0, 0.0, s);
+    ctx.to_device(sm.W.as<double>(), eigenvalues, nev);
+    residual_norms<double>(AXf.data(), Xp, nullptr, ldx, n, nev, sm.W.as<double>(), nullptr, 0,
+                           sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
+                           sm.rws.get(), sm.rws.bytes(), s, 1);
+    ctx.to_host(residuals, sm.rel.as<double>(), nev);
+    ctx.sync();
   }
   if (eigenvectors) {
     // Row-major device block -> column-major host n x nev (copy_to_host boundary).
@@ -671,6 +725,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
         eigenvectors[static_cast<size_t>(j) * n + i] = host[static_cast<size_t>(i) * nev + j];
   }
   st.iterations = static_cast<double>(it_done);
+  st.precise_grams = static_cast<double>(sm.precise_grams);
 }
 
 }  // namespace
@@ -703,6 +758,10 @@ extern "C" int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eig
       stats[5] = st.fp64_iterations;
       stats[6] = st.lower;
       stats[7] = st.upper;
+      stats[8] = st.filter_ms;
+      stats[9] = st.ortho_ms;
+      stats[10] = st.rr_ms;
+      stats[11] = st.precise_grams;
     }
   });
 }

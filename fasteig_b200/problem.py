@@ -148,7 +148,7 @@ class fasteig_problem:  # noqa: N801 - reference class name
         vals = np.zeros(nev)
         res = np.zeros(nev)
         vecs = np.zeros((nev, self.n())) if want_vectors else None  # column-major n x nev
-        stats = np.zeros(8)
+        stats = np.zeros(12)
         check(lib.fe_solve(self.A.handle, self.B.handle if self.B is not None else None,
                            text.encode(), vals.ctypes.data, res.ctypes.data,
                            vecs.ctypes.data if vecs is not None else None, stats.ctypes.data))
@@ -159,7 +159,9 @@ class fasteig_problem:  # noqa: N801 - reference class name
         self.stats = dict(iterations=int(stats[0]), status=int(stats[1]), seconds=float(stats[2]),
                           spmm_launches=int(stats[3]), fp32_iterations=int(stats[4]),
                           fp64_iterations=int(stats[5]), lower=float(stats[6]),
-                          upper=float(stats[7]))
+                          upper=float(stats[7]), filter_ms=float(stats[8]),
+                          ortho_ms=float(stats[9]), rr_ms=float(stats[10]),
+                          precise_grams=int(stats[11]))
         return self._status
 
     def eigenvalues(self) -> np.ndarray:

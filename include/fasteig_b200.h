@@ -214,8 +214,11 @@ int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ld
  * maxdim, maxblks, degree, which, solver, tol, seed, blksize) plus
  * extensions (precision=fp64|mixed, block=<cols>, bounds=reference|ritz).
  * Results: eigenvalues[nev], residual_norms[nev] (the reference's relative
- * residual), eigenvectors n-by-nev column-major (may be NULL), stats[8] (may
- * be NULL): iterations, status, solve seconds, SpMM launches, ...
+ * residual), eigenvectors n-by-nev column-major (may be NULL), stats[12] (may
+ * be NULL): iterations, status, solve seconds, SpMM launches, FP32 cycles, FP64
+ * cycles, spectral lower and upper bounds, device ms in filter, in
+ * orthogonalization, in Rayleigh-Ritz, and FP32 Cholesky passes redone with the
+ * FP64-accumulated Gram.
  * ------------------------------------------------------------------- */
 int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eigenvalues,
              double* residual_norms, double* eigenvectors, double* stats);
