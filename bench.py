@@ -51,7 +51,47 @@ def args_parse():
     p.add_argument("--amplification", type=float, default=1e6)
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison solve")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--kernel", default=None,
+                   choices=["cheb_step_f32", "cheb_step_f64", "gram_tf32x3", "rotate_tf32x3",
+                            "gram_f64", "rotate_f64"],
+                   help="run one kernel --launches times on the --side problem (profiling "
+                        "driver; prints per-launch CUDA-event times, no bench line)")
+    p.add_argument("--launches", type=int, default=4)
+    p.add_argument("--spmm-kernel", type=int, default=0,
+                   help="SpMM kernel selection passed to fe_set_spmm_kernel")
     return p.parse_args()
+
+
+def run_kernel(a):
+    """Profiling driver: the dominant kernels on the well problem of side --side."""
+    import torch
+    import fasteig_b200 as fe
+    from fasteig_b200 import ops
+    fe.lib.fe_set_spmm_kernel(a.spmm_kernel)
+    H = build_matrix(a)
+    dA = fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values)
+    n, b = H.n, a.block
+    dt = torch.float64 if a.kernel.endswith("f64") else torch.float32
+    X = torch.randn(n, b, device="cuda", dtype=dt)
+    Z = torch.randn(n, b, device="cuda", dtype=dt)
+    C = torch.randn(b, b, device="cuda", dtype=torch.float64)
+    fns = {"cheb_step_f32": lambda: ops.cheb_step(dA, X, Z, Z, 0.2, 0.1, -1.0),
+           "cheb_step_f64": lambda: ops.cheb_step(dA, X, Z, Z, 0.2, 0.1, -1.0),
+           "gram_tf32x3": lambda: ops.gram_tf32x3(X, Z),
+           "rotate_tf32x3": lambda: ops.rotate_tf32x3(X, C, Z),
+           "gram_f64": lambda: ops.gram(X, Z),
+           "rotate_f64": lambda: ops.rotate(X, C, Z)}
+    fn = fns[a.kernel]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.launches + 1)]
+    ev[0].record()
+    for i in range(a.launches):
+        fn()
+        ev[i + 1].record()
+    torch.cuda.synchronize()
+    ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(a.launches)]
+    print(json.dumps({"kernel": a.kernel, "n": n, "nnz": H.nnz, "cols": b,
+                      "ms_per_launch": ms, "device_status": ops.device_status()}))
+    return 0
 
 
 def dist_env():
@@ -253,6 +293,8 @@ def main():
     a = args_parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.kernel:
+        return run_kernel(a)
     import numpy as np
     import torch
 

@@ -45,46 +45,54 @@ struct Pack {
   T v[VEC];
 };
 
+// Vector types by total width: 16 bytes (float4 / double2), 8 bytes (float2 /
+// double), 4 bytes (float).
 template <typename T, int VEC>
-__device__ __forceinline__ Pack<T, VEC> load_pack(const T* p) {
+struct Raw;
+template <> struct Raw<float, 4> { using type = float4; };
+template <> struct Raw<float, 2> { using type = float2; };
+template <> struct Raw<float, 1> { using type = float; };
+template <> struct Raw<double, 2> { using type = double2; };
+template <> struct Raw<double, 1> { using type = double; };
+
+template <typename T, int VEC>
+__device__ __forceinline__ Pack<T, VEC> unpack(const typename Raw<T, VEC>::type& t) {
   Pack<T, VEC> r;
   if constexpr (VEC == 4) {
-    float4 t = __ldg(reinterpret_cast<const float4*>(p));
     r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
   } else if constexpr (VEC == 2) {
-    double2 t = __ldg(reinterpret_cast<const double2*>(p));
     r.v[0] = t.x; r.v[1] = t.y;
   } else {
-    r.v[0] = __ldg(p);
+    r.v[0] = t;
   }
   return r;
+}
+
+template <typename T, int VEC>
+__device__ __forceinline__ Pack<T, VEC> load_pack(const T* p) {
+  using R = typename Raw<T, VEC>::type;
+  return unpack<T, VEC>(__ldg(reinterpret_cast<const R*>(p)));
 }
 
 // Plain (coherent) load for blocks that may alias the output.
 template <typename T, int VEC>
 __device__ __forceinline__ Pack<T, VEC> load_pack_rw(const T* p) {
-  Pack<T, VEC> r;
-  if constexpr (VEC == 4) {
-    float4 t = *reinterpret_cast<const float4*>(p);
-    r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
-  } else if constexpr (VEC == 2) {
-    double2 t = *reinterpret_cast<const double2*>(p);
-    r.v[0] = t.x; r.v[1] = t.y;
-  } else {
-    r.v[0] = *p;
-  }
-  return r;
+  using R = typename Raw<T, VEC>::type;
+  return unpack<T, VEC>(*reinterpret_cast<const R*>(p));
 }
 
 template <typename T, int VEC>
 __device__ __forceinline__ void store_pack(T* p, const Pack<T, VEC>& r) {
+  using R = typename Raw<T, VEC>::type;
+  R t;
   if constexpr (VEC == 4) {
-    *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+    t.x = r.v[0]; t.y = r.v[1]; t.z = r.v[2]; t.w = r.v[3];
   } else if constexpr (VEC == 2) {
-    *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
+    t.x = r.v[0]; t.y = r.v[1];
   } else {
-    *p = r.v[0];
+    t = r.v[0];
   }
+  *reinterpret_cast<R*>(p) = t;
 }
 
 constexpr int kThreads = 256;
@@ -202,6 +210,222 @@ csr_spmm_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
       store_pack<T, VEC>(yrow + v * VEC, out);
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Row-batched register kernel: one warp per row for slabs of >= 32 vectors.
+//
+// The loop kernel above waits on a chain of dependent loads per row (rowptr ->
+// colind -> two neighbours per trip -> ... -> Z). Here the whole row is issued at
+// once: the neighbour rows of X (up to NZ nonzeros, all in registers) and the
+// Z row are loaded together, while the CSR metadata of the next row (colind and
+// values) and the row pointers of the row after it are prefetched. Each row then
+// costs about one memory round trip, and a warp keeps NZ*CPL 128-bit loads per
+// lane in flight. gamma is folded into the diagonal coefficient
+// (alpha*a_ii + gamma); a row without a stored diagonal loads its X row.
+// Columns are split into panels of at most 96 vectors (CPL <= 3).
+// ---------------------------------------------------------------------------
+template <typename T, int VEC, int CPL, int NZ>
+__global__ void __launch_bounds__(kThreads)
+csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
+                    const int32_t* __restrict__ colind, const T* __restrict__ vals,
+                    const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
+                    int64_t ldz, int ncols, int panel_vec, T alpha, T gamma, T beta,
+                    int use_gamma, int use_beta) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t tw = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
+  int64_t row = static_cast<int64_t>(blockIdx.x) * (kThreads / 32) + threadIdx.x / 32;
+  if (row >= nrows) return;
+  const int p0 = blockIdx.y * panel_vec * VEC;
+  const int nvec = min(panel_vec, (ncols - p0) / VEC);
+  const T* Xp = X + p0;
+
+  int s0 = __ldg(rowptr + row), e0 = __ldg(rowptr + row + 1);
+  int c_cur = 0;
+  T a_cur = T(0);
+  if (lane < min(e0 - s0, NZ)) {
+    c_cur = __ldg(colind + s0 + lane);
+    a_cur = __ldg(vals + s0 + lane);
+  }
+  int64_t nxt = row + tw;
+  int s1 = 0, e1 = 0;
+  if (nxt < nrows) {
+    s1 = __ldg(rowptr + nxt);
+    e1 = __ldg(rowptr + nxt + 1);
+  }
+  while (true) {
+    const int nnz = e0 - s0;
+    Pack<T, VEC> z[CPL];
+    if (use_beta) {
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) {
+        const int v = lane + 32 * q;
+        if (v < nvec) z[q] = load_pack_rw<T, VEC>(Z + row * ldz + p0 + v * VEC);
+      }
+    }
+    T acc[CPL][VEC];
+#pragma unroll
+    for (int q = 0; q < CPL; ++q)
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) acc[q][e] = T(0);
+    bool self_found = false;
+    // next-row metadata, prefetched under this row's loads
+    int c_n = 0;
+    T a_n = T(0);
+    int64_t nxt2 = nxt + tw;
+    int s2 = 0, e2 = 0;
+    if (nnz <= NZ) {
+      Pack<T, VEC> x[NZ][CPL];
+#pragma unroll
+      for (int t = 0; t < NZ; ++t) {
+        const int c = __shfl_sync(kFull, c_cur, t);
+        if (t < nnz) {
+          const T* xr = Xp + static_cast<int64_t>(c) * ldx;
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) {
+            const int v = lane + 32 * q;
+            if (v < nvec) x[t][q] = load_pack<T, VEC>(xr + v * VEC);
+          }
+        }
+      }
+      if (nxt < nrows && lane < min(e1 - s1, NZ)) {
+        c_n = __ldg(colind + s1 + lane);
+        a_n = __ldg(vals + s1 + lane);
+      }
+      if (nxt2 < nrows) {
+        s2 = __ldg(rowptr + nxt2);
+        e2 = __ldg(rowptr + nxt2 + 1);
+      }
+#pragma unroll
+      for (int t = 0; t < NZ; ++t) {
+        const int c = __shfl_sync(kFull, c_cur, t);
+        T coef = alpha * __shfl_sync(kFull, a_cur, t);
+        if (t < nnz) {
+          if (c == row) {
+            coef += gamma;
+            self_found = true;
+          }
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) {
+            const int v = lane + 32 * q;
+            if (v < nvec) {
+#pragma unroll
+              for (int e = 0; e < VEC; ++e) acc[q][e] = fma(coef, x[t][q].v[e], acc[q][e]);
+            }
+          }
+        }
+      }
+    } else {
+      // Long row: stream its nonzeros 32 at a time.
+      for (int base = s0; base < e0; base += 32) {
+        const int k = base + lane;
+        int c = 0;
+        T a = T(0);
+        if (k < e0) {
+          c = __ldg(colind + k);
+          a = __ldg(vals + k);
+        }
+        const int cnt = min(32, e0 - base);
+        for (int t = 0; t < cnt; ++t) {
+          const int c0 = __shfl_sync(kFull, c, t);
+          T coef = alpha * __shfl_sync(kFull, a, t);
+          if (c0 == row) {
+            coef += gamma;
+            self_found = true;
+          }
+          const T* xr = Xp + static_cast<int64_t>(c0) * ldx;
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) {
+            const int v = lane + 32 * q;
+            if (v < nvec) {
+              const Pack<T, VEC> p = load_pack<T, VEC>(xr + v * VEC);
+#pragma unroll
+              for (int e = 0; e < VEC; ++e) acc[q][e] = fma(coef, p.v[e], acc[q][e]);
+            }
+          }
+        }
+      }
+      if (nxt < nrows && lane < min(e1 - s1, NZ)) {
+        c_n = __ldg(colind + s1 + lane);
+        a_n = __ldg(vals + s1 + lane);
+      }
+      if (nxt2 < nrows) {
+        s2 = __ldg(rowptr + nxt2);
+        e2 = __ldg(rowptr + nxt2 + 1);
+      }
+    }
+    if (use_gamma && !self_found) {
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) {
+        const int v = lane + 32 * q;
+        if (v < nvec) {
+          const Pack<T, VEC> xr = load_pack<T, VEC>(Xp + row * ldx + v * VEC);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) acc[q][e] = fma(gamma, xr.v[e], acc[q][e]);
+        }
+      }
+    }
+    T* yr = Y + row * ldy + p0;
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) {
+      const int v = lane + 32 * q;
+      if (v < nvec) {
+        Pack<T, VEC> out;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e)
+          out.v[e] = use_beta ? fma(beta, z[q].v[e], acc[q][e]) : acc[q][e];
+        store_pack<T, VEC>(yr + v * VEC, out);
+      }
+    }
+    if (nxt >= nrows) break;
+    row = nxt;
+    nxt = nxt2;
+    s0 = s1;
+    e0 = e1;
+    s1 = s2;
+    e1 = e2;
+    c_cur = c_n;
+    a_cur = a_n;
+  }
+}
+
+template <typename T, int VEC>
+bool try_row_kernel(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, int64_t ldy,
+                    const T* Z, int64_t ldz, int ncols, T alpha, T gamma, T beta, bool ug, bool ub,
+                    cudaStream_t s, int max_cpl) {
+  constexpr int NZ = 7;
+  const int nvec = ncols / VEC;
+  if (nvec < 32 || ncols % VEC != 0 || A.max_row_nnz > NZ) return false;
+  const int panels = (nvec + 32 * max_cpl - 1) / (32 * max_cpl);
+  const int panel_vec = (nvec + panels - 1) / panels;
+  const int cpl = (panel_vec + 31) / 32;
+  // One warp per row, grid-stride over rows with exactly the resident CTAs.
+#define FE_ROW(CPL_)                                                                           \
+  do {                                                                                         \
+    auto kern = csr_spmm_row_kernel<T, VEC, CPL_, NZ>;                                         \
+    static int resident = 0;                                                                   \
+    if (resident == 0) {                                                                       \
+      FE_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, kThreads,   \
+                                                                  0));                         \
+      resident = std::max(resident, 1);                                                        \
+    }                                                                                          \
+    int64_t blocks = std::min<int64_t>((A.rows + 7) / 8,                                       \
+                                       static_cast<int64_t>(num_sms()) * resident);            \
+    blocks = std::max<int64_t>(blocks, 1);                                                     \
+    dim3 grid(static_cast<unsigned>(blocks), static_cast<unsigned>(panels));                   \
+    kern<<<grid, kThreads, 0, s>>>(A.rows, A.rowptr, A.colind, vals, X, ldx, Y, ldy, Z, ldz,   \
+                                   ncols, panel_vec, alpha, gamma, beta, ug ? 1 : 0,           \
+                                   ub ? 1 : 0);                                                \
+    check_launch("csr_spmm_row_kernel");                                                       \
+  } while (0)
+  if (cpl == 1) FE_ROW(1);
+  else if (cpl == 2) FE_ROW(2);
+  else if (cpl == 3) FE_ROW(3);
+  else if (cpl == 4) FE_ROW(4);
+  else FE_ROW(5);
+#undef FE_ROW
+  return true;
 }
 
 template <typename T, int VEC, int G, int CPL>
@@ -563,7 +787,9 @@ int read_spmm_status(bool clear) {
 }
 
 // Kernel selection for csr_spmm: "pipe" (bulk-copy pipelined) or "warp" (registers only).
-static int g_spmm_mode = 0;  // 0 = auto, 1 = force register kernel, 2 = prefer pipeline
+// 0 = row-batched kernel (panels <= 96 vectors) where it applies, 1 = loop kernel,
+// 2 = bulk-copy pipeline where it applies, 3 = row-batched with panels <= 64 vectors.
+static int g_spmm_mode = 0;
 void set_spmm_mode(int mode) { g_spmm_mode = mode; }
 
 // Shared entry used by the C ABI and the host solver.
@@ -587,9 +813,21 @@ void csr_spmm(const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T*
   const bool vec_ok = ncols % VEC == 0 && ldx % VEC == 0 && ldy % VEC == 0 && aligned16(X) &&
                       aligned16(Y) && (!ub || (ldz % VEC == 0 && aligned16(Z)));
   if (vec_ok) {
-    // The pipelined kernel needs 16-byte aligned row gathers (vec_ok) and rows
-    // that fit a stage; it pays off once a row slab is at least 64 bytes.
-    if (g_spmm_mode != 1 && ncols * static_cast<int64_t>(sizeof(T)) >= 64 &&
+    // Mode 0: the row-batched register kernel for slabs of >= 32 vectors and rows
+    // of <= 8 nonzeros; mode 2: the bulk-copy pipelined kernel (needs 16-byte
+    // aligned row gathers and rows that fit its stages).
+    // Mode 0 gives each lane 8-byte vectors (up to 5 per lane, so a 320-column
+    // FP32 slab needs no idle lanes and ~70 registers of loads in flight); mode 3
+    // uses 16-byte vectors with at most 2 per lane.
+    if (g_spmm_mode == 0 &&
+        try_row_kernel<T, 8 / sizeof(T)>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols),
+                                         T(alpha), T(gamma), T(beta), ug, ub, s, 5))
+      return;
+    if (g_spmm_mode == 3 &&
+        try_row_kernel<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
+                               T(gamma), T(beta), ug, ub, s, 2))
+      return;
+    if (g_spmm_mode == 2 && ncols * static_cast<int64_t>(sizeof(T)) >= 64 &&
         try_pipe<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                          T(gamma), T(beta), ug, ub, s))
       return;

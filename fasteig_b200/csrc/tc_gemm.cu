@@ -693,7 +693,7 @@ extern "C" int fe_device_status(int32_t* status, int32_t clear) {
 
 extern "C" int fe_set_spmm_kernel(int32_t mode) {
   return fe::guarded("fe_set_spmm_kernel", [&] {
-    FE_REQUIRE(mode >= 0 && mode <= 1, "mode must be 0 (auto) or 1 (register kernel)");
+    FE_REQUIRE(mode >= 0 && mode <= 3, "mode must be 0..3");
     fe::set_spmm_mode(mode);
   });
 }

@@ -150,9 +150,12 @@ int fe_rotate_tf32x3(const float* X, int64_t ldx, const double* C, int64_t ldc, 
 /* First failure code recorded by a bounded device-side wait of the tensor-core
  * or pipelined SpMM kernels (0 = none); clear != 0 resets it. */
 int fe_device_status(int32_t* status, int32_t clear);
-/* SpMM kernel selection for all later calls in the process: 0 = automatic
- * (bulk-copy pipelined kernel when the rows fit its stages, else the
- * register kernel), 1 = always the register kernel. */
+/* SpMM kernel selection for all later calls in the process (the numerics are
+ * the same; the choice only changes the memory schedule): 0 = default
+ * (row-batched register kernel for slabs of >= 32 128-bit vectors and rows of
+ * <= 7 nonzeros, else the loop kernel), 1 = loop kernel, 2 = bulk-copy
+ * pipelined kernel where it applies, 3 = row-batched kernel with narrower
+ * column panels. */
 int fe_set_spmm_kernel(int32_t mode);
 
 /* ---------------------------------------------------------------------
