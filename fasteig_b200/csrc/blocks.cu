@@ -14,6 +14,9 @@
 #include "fe_common.cuh"
 
 #include <algorithm>
+#include <climits>
+#include <mutex>
+#include <string>
 
 namespace fe {
 namespace {
@@ -104,13 +107,15 @@ struct GramPlan {
   size_t bytes;
 };
 
-GramPlan gram_plan(int64_t n, int64_t k, int64_t m) {
+// max_chunks caps the number of row chunks (so the partials fit a fixed scratch).
+GramPlan gram_plan(int64_t n, int64_t k, int64_t m, int64_t max_chunks = INT32_MAX) {
   GramPlan p{};
   p.tiles_k = static_cast<int>((k + kGT - 1) / kGT);
   p.tiles_m = static_cast<int>((m + kGT - 1) / kGT);
   const int64_t tiles = std::max<int64_t>(1, static_cast<int64_t>(p.tiles_k) * p.tiles_m);
   int64_t chunks = (kGramTargetCtas + tiles - 1) / tiles;
   chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, (n + 255) / 256));
+  chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, max_chunks));
   int64_t rpc = (n + chunks - 1) / chunks;
   rpc = ((rpc + kGK - 1) / kGK) * kGK;
   chunks = std::max<int64_t>(1, (n + rpc - 1) / rpc);
@@ -586,4 +591,79 @@ void fill_uniform(T* X, int64_t ld, int64_t n, int64_t m, uint64_t seed, cudaStr
 template void fill_uniform<double>(double*, int64_t, int64_t, int64_t, uint64_t, cudaStream_t);
 template void fill_uniform<float>(float*, int64_t, int64_t, int64_t, uint64_t, cudaStream_t);
 
+// --------------------------------------------- Gram without any allocation ----
+// Some callers cannot allocate device memory when they call us: a host program
+// that has already handed all device memory to its own pool, or code on a
+// latency-critical path where cudaMalloc (which can synchronize the device) is
+// not acceptable and no workspace was set aside. For them the FP64 Gram has a
+// variant whose split-K partial sums live in the fixed array below, which every
+// GPU that loads this library keeps for the life of the process.
+namespace {
+
+constexpr int64_t kStaticGramDoubles = int64_t(1) << 20;  // 8 MiB of FP64 partials
+constexpr int kMaxDevices = 64;
+
+__device__ __align__(256) double g_static_gram_scratch[kStaticGramDoubles];
+
+std::mutex g_static_gram_mutex;
+double* g_static_gram_ptr[kMaxDevices] = {};
+
+// Device address of the scratch on the current device. The symbol's name is only
+// a host-side stand-in, so the address is looked up once per device (with that
+// device current) and cached.
+double* static_gram_scratch() {
+  int dev = 0;
+  FE_CHECK_CUDA(cudaGetDevice(&dev));
+  FE_REQUIRE(dev >= 0 && dev < kMaxDevices, "static Gram scratch: device index out of range");
+  std::lock_guard<std::mutex> lock(g_static_gram_mutex);
+  if (!g_static_gram_ptr[dev]) {
+    void* p = nullptr;
+    FE_CHECK_CUDA(cudaGetSymbolAddress(&p, g_static_gram_scratch));
+    g_static_gram_ptr[dev] = static_cast<double*>(p);
+  }
+  return g_static_gram_ptr[dev];
+}
+
+}  // namespace
+
+int64_t static_gram_max_entries() { return kStaticGramDoubles; }
+
+void gram_f64_static(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t n,
+                     int64_t k, int64_t m, double* G, int64_t ldg, cudaStream_t s) {
+  FE_REQUIRE(n >= 0 && k >= 0 && m >= 0, "gram: negative dimension");
+  FE_REQUIRE(k * m <= kStaticGramDoubles,
+             "k*m = " + std::to_string(k * m) + " exceeds the static Gram scratch (k*m <= " +
+                 std::to_string(kStaticGramDoubles) + ")");
+  FE_REQUIRE(k <= 65535 * (int64_t)kGT && m <= 65535 * (int64_t)kGT, "gram: too many columns");
+  if (k == 0 || m == 0) return;
+  FE_REQUIRE(G && ldg >= k, "gram: invalid output");
+  double* scratch = static_gram_scratch();
+  if (n == 0) {
+    FE_CHECK_CUDA(cudaMemset2DAsync(G, ldg * sizeof(double), 0, k * sizeof(double), m, s));
+    return;
+  }
+  FE_REQUIRE(X && Y && ldx >= k && ldy >= m, "gram: invalid input block");
+  // As many row chunks as the scratch holds (each chunk's k x m partial is written
+  // in full by the partial kernel, so nothing needs clearing between calls).
+  const GramPlan p = gram_plan(n, k, m, std::max<int64_t>(1, kStaticGramDoubles / (k * m)));
+  dim3 grid(p.tiles_k, p.tiles_m, p.chunks);
+  gram_partial_kernel<double><<<grid, 256, 0, s>>>(X, ldx, Y, ldy, n, static_cast<int>(k),
+                                                   static_cast<int>(m), p.rows_per_chunk, scratch);
+  check_launch("gram_partial_kernel");
+  const int64_t total = k * m;
+  gram_reduce_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
+      scratch, p.chunks, static_cast<int>(k), static_cast<int>(m), G, ldg);
+  check_launch("gram_reduce_kernel");
+}
+
 }  // namespace fe
+
+extern "C" int fe_gram_f64_noalloc(const double* X, int64_t ldx, const double* Y, int64_t ldy,
+                                   int64_t n, int64_t k, int64_t m, double* G, int64_t ldg,
+                                   void* stream) {
+  return fe::guarded("fe_gram_f64_noalloc", [&] {
+    fe::gram_f64_static(X, ldx, Y, ldy, n, k, m, G, ldg, fe::as_stream(stream));
+  });
+}
+
+extern "C" int64_t fe_gram_f64_noalloc_max_entries(void) { return fe::static_gram_max_entries(); }

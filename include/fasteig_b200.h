@@ -117,6 +117,24 @@ int fe_gram_f32(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_
                 int64_t k, int64_t m, double* G, int64_t ldg, void* workspace,
                 size_t workspace_bytes, void* stream);
 
+/* FP64 Gram that allocates nothing (this entry point has no counterpart in the
+ * reference). For callers that cannot allocate device memory at call time —
+ * e.g. a program whose device memory is all owned by its own pool, or a
+ * latency-critical path that must not call cudaMalloc — the split-K partial
+ * sums go to a fixed 8 MiB array inside this library instead of a caller
+ * workspace; every GPU that loads the library keeps that array until the
+ * process exits. Same arguments, results and accuracy as fe_gram_f64; it
+ * requires k*m <= fe_gram_f64_noalloc_max_entries() (1,048,576) and returns
+ * FE_ERR_INVALID otherwise. The first call on a device looks up the array's
+ * device address with that device current; make that first call before any
+ * stream capture. All calls share the one array (each call overwrites the
+ * part it uses, nothing needs clearing): calls that can overlap on the GPU —
+ * on different streams, or from different host threads — race and must be
+ * serialized by the caller. */
+int fe_gram_f64_noalloc(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t n,
+                        int64_t k, int64_t m, double* G, int64_t ldg, void* stream);
+int64_t fe_gram_f64_noalloc_max_entries(void);
+
 /* Tensor-core Gram of FP32 blocks (tcgen05, 3xTF32 split products accumulated
  * in FP32 per row chunk, chunk partials summed in FP64): FP32-level accuracy
  * relative to |X|^T |Y|, for the mixed-precision path. Same shapes as
