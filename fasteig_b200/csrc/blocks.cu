@@ -24,33 +24,39 @@ namespace {
 // ---------------------------------------------------------------- Gram ----
 constexpr int kGT = 64;    // output tile (k and m)
 constexpr int kGK = 32;    // rows per smem stage
-constexpr int kGramTargetCtas = 592;  // about four CTAs per SM on 148 SMs
+constexpr int kGramThreads = 64;      // 8 x 8 threads, 8 x 8 outputs each
+// Row chunks are sized for about four waves of resident CTAs (five 2-warp CTAs per
+// SM at 190 registers per thread) on 148 SMs, so load latency of one CTA hides
+// behind the FMAs of the others.
+constexpr int kGramTargetCtas = 148 * 5 * 4;
 
+// 8x8 outputs per thread (rows ty + 8a, columns tx + 8b): 16 shared-memory loads
+// feed 64 FP64 FMAs, which matches the FP64 pipe to the shared-memory bandwidth.
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kGramThreads)
 gram_partial_kernel(const T* __restrict__ X, int64_t ldx, const T* __restrict__ Y, int64_t ldy,
                     int64_t n, int k, int m, int64_t rows_per_chunk,
                     double* __restrict__ partial) {
   __shared__ double Xs[kGK][kGT + 1];
   __shared__ double Ys[kGK][kGT + 1];
-  const int tx = threadIdx.x % 16;
-  const int ty = threadIdx.x / 16;
+  const int tx = threadIdx.x % 8;
+  const int ty = threadIdx.x / 8;
   const int i0 = blockIdx.x * kGT;
   const int j0 = blockIdx.y * kGT;
   const int64_t r_begin = static_cast<int64_t>(blockIdx.z) * rows_per_chunk;
   const int64_t r_end = min(n, r_begin + rows_per_chunk);
 
-  double acc[4][4];
+  double acc[8][8];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 8; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
 
   for (int64_t r0 = r_begin; r0 < r_end; r0 += kGK) {
-    // 32 rows x 64 columns per operand, 8 elements per thread, coalesced along columns.
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int idx = threadIdx.x + e * 256;
+    // 32 rows x 64 columns per operand, 32 elements per thread, coalesced along columns.
+#pragma unroll 8
+    for (int e = 0; e < (kGK * kGT) / kGramThreads; ++e) {
+      const int idx = threadIdx.x + e * kGramThreads;
       const int rr = idx / kGT;
       const int cc = idx % kGT;
       const int64_t r = r0 + rr;
@@ -63,27 +69,27 @@ gram_partial_kernel(const T* __restrict__ X, int64_t ldx, const T* __restrict__ 
       Ys[rr][cc] = yv;
     }
     __syncthreads();
-#pragma unroll 8
+#pragma unroll 4
     for (int rr = 0; rr < kGK; ++rr) {
-      double xv[4], yv[4];
+      double xv[8], yv[8];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) xv[a] = Xs[rr][ty + 16 * a];
+      for (int a = 0; a < 8; ++a) xv[a] = Xs[rr][ty + 8 * a];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) yv[b] = Ys[rr][tx + 16 * b];
+      for (int b = 0; b < 8; ++b) yv[b] = Ys[rr][tx + 8 * b];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(xv[a], yv[b], acc[a][b]);
+        for (int b = 0; b < 8; ++b) acc[a][b] = fma(xv[a], yv[b], acc[a][b]);
     }
     __syncthreads();
   }
   double* out = partial + static_cast<int64_t>(blockIdx.z) * k * m;
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int i = i0 + ty + 16 * a;
+  for (int a = 0; a < 8; ++a) {
+    const int i = i0 + ty + 8 * a;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int j = j0 + tx + 16 * b;
+    for (int b = 0; b < 8; ++b) {
+      const int j = j0 + tx + 8 * b;
       if (i < k && j < m) out[static_cast<int64_t>(j) * k + i] = acc[a][b];
     }
   }
@@ -128,29 +134,30 @@ GramPlan gram_plan(int64_t n, int64_t k, int64_t m, int64_t max_chunks = INT32_M
 // --------------------------------------------------------------- Rotation ----
 constexpr int kRT = 64;  // rows and output columns per tile
 constexpr int kRK = 32;  // inner (k) stage
+constexpr int kRotThreads = 64;  // 8 x 8 threads, 8 x 8 outputs each
 
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kRotThreads)
 rotate_kernel(const T* __restrict__ X, int64_t ldx, const double* __restrict__ C, int64_t ldc,
               T* __restrict__ Y, int64_t ldy, int64_t n, int k, int m, T alpha, T beta,
               int use_beta) {
   __shared__ T Xs[kRT][kRK + 1];
   __shared__ T Cs[kRK][kRT + 1];
-  const int tx = threadIdx.x % 16;
-  const int ty = threadIdx.x / 16;
+  const int tx = threadIdx.x % 8;
+  const int ty = threadIdx.x / 8;
   const int j0 = blockIdx.x * kRT;
   const int64_t r0 = static_cast<int64_t>(blockIdx.y) * kRT;
 
-  T acc[4][4];
+  T acc[8][8];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 8; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+    for (int b = 0; b < 8; ++b) acc[a][b] = T(0);
 
   for (int k0 = 0; k0 < k; k0 += kRK) {
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int idx = threadIdx.x + e * 256;
+#pragma unroll 8
+    for (int e = 0; e < (kRT * kRK) / kRotThreads; ++e) {
+      const int idx = threadIdx.x + e * kRotThreads;
       // X tile: 64 rows x 32 inner, coalesced along inner index.
       const int rr = idx / kRK;
       const int kk = idx % kRK;
@@ -164,27 +171,27 @@ rotate_kernel(const T* __restrict__ X, int64_t ldx, const double* __restrict__ C
                        : T(0);
     }
     __syncthreads();
-#pragma unroll 8
+#pragma unroll 4
     for (int kk = 0; kk < kRK; ++kk) {
-      T xv[4], cv[4];
+      T xv[8], cv[8];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) xv[a] = Xs[ty + 16 * a][kk];
+      for (int a = 0; a < 8; ++a) xv[a] = Xs[ty + 8 * a][kk];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) cv[b] = Cs[kk][tx + 16 * b];
+      for (int b = 0; b < 8; ++b) cv[b] = Cs[kk][tx + 8 * b];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(xv[a], cv[b], acc[a][b]);
+        for (int b = 0; b < 8; ++b) acc[a][b] = fma(xv[a], cv[b], acc[a][b]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int64_t r = r0 + ty + 16 * a;
+  for (int a = 0; a < 8; ++a) {
+    const int64_t r = r0 + ty + 8 * a;
     if (r >= n) continue;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int j = j0 + tx + 16 * b;
+    for (int b = 0; b < 8; ++b) {
+      const int j = j0 + tx + 8 * b;
       if (j < m) {
         T* y = Y + r * ldy + j;
         T v = alpha * acc[a][b];
@@ -326,7 +333,7 @@ void gram(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k
   const GramPlan p = gram_plan(n, k, m);
   FE_REQUIRE(ws && ws_bytes >= p.bytes, "gram: workspace too small");
   dim3 grid(p.tiles_k, p.tiles_m, p.chunks);
-  gram_partial_kernel<T><<<grid, 256, 0, s>>>(X, ldx, Y, ldy, n, static_cast<int>(k),
+  gram_partial_kernel<T><<<grid, kGramThreads, 0, s>>>(X, ldx, Y, ldy, n, static_cast<int>(k),
                                               static_cast<int>(m), p.rows_per_chunk,
                                               static_cast<double*>(ws));
   check_launch("gram_partial_kernel");
@@ -364,7 +371,7 @@ void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t
     const int64_t tiles = std::min<int64_t>(65535, row_tiles - base);
     dim3 grid(static_cast<unsigned>(col_tiles), static_cast<unsigned>(tiles));
     const int64_t r_off = base * kRT;
-    rotate_kernel<T><<<grid, 256, 0, s>>>(X + r_off * ldx, ldx, C, ldc, Y + r_off * ldy, ldy,
+    rotate_kernel<T><<<grid, kRotThreads, 0, s>>>(X + r_off * ldx, ldx, C, ldc, Y + r_off * ldy, ldy,
                                           n - r_off, static_cast<int>(k), static_cast<int>(m),
                                           T(alpha), T(beta), beta != 0.0 ? 1 : 0);
     check_launch("rotate_kernel");
@@ -647,7 +654,7 @@ void gram_f64_static(const double* X, int64_t ldx, const double* Y, int64_t ldy,
   // in full by the partial kernel, so nothing needs clearing between calls).
   const GramPlan p = gram_plan(n, k, m, std::max<int64_t>(1, kStaticGramDoubles / (k * m)));
   dim3 grid(p.tiles_k, p.tiles_m, p.chunks);
-  gram_partial_kernel<double><<<grid, 256, 0, s>>>(X, ldx, Y, ldy, n, static_cast<int>(k),
+  gram_partial_kernel<double><<<grid, kGramThreads, 0, s>>>(X, ldx, Y, ldy, n, static_cast<int>(k),
                                                    static_cast<int>(m), p.rows_per_chunk, scratch);
   check_launch("gram_partial_kernel");
   const int64_t total = k * m;

@@ -91,6 +91,100 @@ potrf_upper_kernel(double* G, int k, int64_t ldg, int32_t* info) {
   if (threadIdx.x == 0 && info) *info = failed;
 }
 
+// Blocked left-looking Cholesky (upper, G = R^T R) in one CTA of 32 warps, with
+// 32-column panels. For panel J (columns j0..j0+jb):
+//   1. G[J, c] -= R[0:j0, J]^T R[0:j0, c] for every c >= j0: one warp per column c,
+//      lane r owns row j0+r; R[0:j0, J] sits in shared memory, R[l, c] is a
+//      broadcast load. Only the upper triangle of the diagonal block is used.
+//   2. warp 0 factors the jb x jb diagonal block in registers/shared memory.
+//   3. R[J, c] = R_JJ^{-T} G[J, c] for c >= j0+jb: forward substitution with
+//      shuffles, one warp per column.
+// Dynamic shared memory: k*32 doubles (panel) + 32*33 doubles (diagonal block).
+constexpr int kPotrfNB = 32;
+
+__global__ void __launch_bounds__(1024)
+potrf_upper_blocked_kernel(double* G, int k, int64_t ldg, int32_t* info) {
+  extern __shared__ double psm[];
+  double* panel = psm;                      // [k][32]: panel[l * 32 + r] = R[l, j0 + r]
+  double* diag = psm + static_cast<size_t>(k) * kPotrfNB;  // [32][33]
+  __shared__ int failed;
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  const int nwarps = blockDim.x / 32;
+  if (threadIdx.x == 0) failed = 0;
+  __syncthreads();
+  auto g = [&](int r, int c) -> double& { return G[static_cast<int64_t>(c) * ldg + r]; };
+  for (int j0 = 0; j0 < k; j0 += kPotrfNB) {
+    const int jb = min(kPotrfNB, k - j0);
+    // stage R[0:j0, J] (already final) into shared memory
+    for (int idx = threadIdx.x; idx < j0 * kPotrfNB; idx += blockDim.x) {
+      const int l = idx / kPotrfNB;
+      const int r = idx % kPotrfNB;
+      panel[idx] = (r < jb) ? g(l, j0 + r) : 0.0;
+    }
+    __syncthreads();
+    // 1. update the panel row against the finished rows 0..j0-1
+    for (int c = j0 + warp; c < k; c += nwarps) {
+      if (lane < jb && j0 + lane <= c) {
+        double acc = 0.0;
+        for (int l = 0; l < j0; ++l) acc = fma(panel[l * kPotrfNB + lane], g(l, c), acc);
+        g(j0 + lane, c) -= acc;
+      }
+    }
+    __syncthreads();
+    // 2. factor the diagonal block (warp 0, column by column)
+    if (warp == 0) {
+      for (int c = 0; c < jb; ++c)
+        if (lane <= c) diag[lane * 33 + c] = g(j0 + lane, j0 + c);
+      __syncwarp();
+      for (int j = 0; j < jb; ++j) {
+        double d = diag[j * 33 + j];
+        const bool bad = !(d > 0.0) || !isfinite(d);
+        if (bad) {
+          if (lane == 0) failed = j0 + j + 1;
+          break;
+        }
+        const double r = sqrt(d);
+        __syncwarp();
+        if (lane == j) diag[j * 33 + j] = r;
+        if (lane > j && lane < jb) diag[j * 33 + lane] /= r;
+        __syncwarp();
+        // trailing update of the block's upper triangle: a = lane, columns c >= a
+        if (lane > j && lane < jb) {
+          const double rja = diag[j * 33 + lane];
+          for (int c = lane; c < jb; ++c) diag[lane * 33 + c] -= rja * diag[j * 33 + c];
+        }
+        __syncwarp();
+      }
+      __syncwarp();
+      if (!failed) {
+        for (int c = 0; c < jb; ++c)
+          if (lane <= c) g(j0 + lane, j0 + c) = diag[lane * 33 + c];
+      }
+    }
+    __syncthreads();
+    if (failed) break;
+    // 3. triangular solve for the rest of the panel row: R_JJ^T x = G[J, c]
+    for (int c = j0 + jb + warp; c < k; c += nwarps) {
+      double x = (lane < jb) ? g(j0 + lane, c) : 0.0;
+      for (int i = 0; i < jb; ++i) {
+        const double xi = __shfl_sync(0xffffffffu, x, i) / diag[i * 33 + i];
+        if (lane == i) x = xi;
+        if (lane > i && lane < jb) x -= diag[i * 33 + lane] * xi;
+      }
+      if (lane < jb) g(j0 + lane, c) = x;
+    }
+    __syncthreads();
+  }
+  // zero the strict lower triangle
+  for (int64_t idx = threadIdx.x; idx < static_cast<int64_t>(k) * k; idx += blockDim.x) {
+    const int r = static_cast<int>(idx % k);
+    const int c = static_cast<int>(idx / k);
+    if (r > c) g(r, c) = 0.0;
+  }
+  if (threadIdx.x == 0 && info) *info = failed;
+}
+
 // One warp per column c of Rinv: back substitution R x = e_c.
 __global__ void trinv_upper_kernel(const double* __restrict__ R, int64_t ldr,
                                    double* __restrict__ Rinv, int64_t ldi, int k) {
@@ -132,6 +226,18 @@ void potrf_upper(double* G, int64_t k, int64_t ldg, int32_t* info, cudaStream_t 
   FE_REQUIRE(k >= 0 && k <= 16384 && ldg >= k, "potrf_upper: invalid shape");
   if (k == 0) {
     if (info) FE_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int32_t), s));
+    return;
+  }
+  const size_t smem = (static_cast<size_t>(k) * kPotrfNB + 32 * 33) * sizeof(double);
+  if (smem <= 200 * 1024) {
+    static bool attr = false;
+    if (!attr) {
+      FE_CHECK_CUDA(cudaFuncSetAttribute(potrf_upper_blocked_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+      attr = true;
+    }
+    potrf_upper_blocked_kernel<<<1, 1024, smem, s>>>(G, static_cast<int>(k), ldg, info);
+    check_launch("potrf_upper_blocked_kernel");
     return;
   }
   potrf_upper_kernel<<<1, 1024, 0, s>>>(G, static_cast<int>(k), ldg, info);

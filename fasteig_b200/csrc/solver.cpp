@@ -478,8 +478,21 @@ struct ChebLoop {
       const double d = -(upper + cutoff) / (upper - cutoff);
       if (!std::isfinite(c) || !std::isfinite(d))
         throw Error(FE_ERR_NONFINITE, "ChebyshevSolver: invalid filter scaling.");
-      // The operator is sign*A: fold the sign into c.
-      filter(b.V.col(locked), b.V.ld, b.S.data(), b.S.ld, active, sign * c, d);
+      // The operator is sign*A: fold the sign into c. The active columns start at
+      // column `locked`; when that is not 16-byte aligned the filter runs on an
+      // aligned copy in S (with Q as its second buffer) so the SpMM keeps its
+      // vectorised path, and the result is copied back.
+      if ((locked * static_cast<int64_t>(sizeof(T))) % 16 == 0) {
+        filter(b.V.col(locked), b.V.ld, b.S.data(), b.S.ld, active, sign * c, d);
+      } else {
+        FE_CHECK_CUDA(cudaMemcpy2DAsync(b.S.data(), b.S.ld * sizeof(T), b.V.col(locked),
+                                        b.V.ld * sizeof(T), active * sizeof(T), n,
+                                        cudaMemcpyDeviceToDevice, s));
+        filter(b.S.data(), b.S.ld, b.Q.data(), b.Q.ld, active, sign * c, d);
+        FE_CHECK_CUDA(cudaMemcpy2DAsync(b.V.col(locked), b.V.ld * sizeof(T), b.S.data(),
+                                        b.S.ld * sizeof(T), active * sizeof(T), n,
+                                        cudaMemcpyDeviceToDevice, s));
+      }
       st.spmm_launches += static_cast<double>(degree);
     }
     ev.record(1, s);

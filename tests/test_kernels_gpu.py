@@ -267,7 +267,7 @@ def test_residual_norms(dtype, n, m):
     np.testing.assert_allclose(cn.cpu().numpy(), np.linalg.norm(X64, axis=0), rtol=1e-12)
 
 
-@pytest.mark.parametrize("k", [1, 2, 17, 64, 320])
+@pytest.mark.parametrize("k", [1, 2, 17, 33, 64, 100, 320, 500, 900])
 def test_potrf_and_trinv(k):
     from fasteig_b200 import ops
     rng = np.random.default_rng(k)
