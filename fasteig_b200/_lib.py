@@ -61,6 +61,7 @@ _SIGS = {
                                    vp]),
     "fe_device_status": (C.c_int, [C.POINTER(C.c_int32), C.c_int32]),
     "fe_set_spmm_kernel": (C.c_int, [C.c_int32]),
+    "fe_set_f64_gemm_kernel": (C.c_int, [C.c_int32]),
     "fe_gram_f64_noalloc": (C.c_int, [vp, i64, vp, i64, i64, i64, i64, vp, i64, vp]),
     "fe_gram_f64_noalloc_max_entries": (C.c_int64, []),
 }

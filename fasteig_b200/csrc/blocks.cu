@@ -17,6 +17,7 @@
 #include <climits>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 namespace fe {
 namespace {
@@ -95,15 +96,19 @@ gram_partial_kernel(const T* __restrict__ X, int64_t ldx, const T* __restrict__ 
   }
 }
 
+// With `symmetric` (k == m, only tiles on and above the diagonal computed) an
+// entry below the diagonal tiles reads its mirror (j, i).
 __global__ void gram_reduce_kernel(const double* __restrict__ partial, int chunks, int k, int m,
-                                   double* __restrict__ G, int64_t ldg) {
+                                   double* __restrict__ G, int64_t ldg, int symmetric) {
   const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t total = static_cast<int64_t>(k) * m;
   if (idx >= total) return;
   const int i = static_cast<int>(idx % k);
   const int j = static_cast<int>(idx / k);
+  const int64_t src =
+      (symmetric && i / kGT > j / kGT) ? static_cast<int64_t>(i) * k + j : idx;
   double s = 0.0;
-  for (int c = 0; c < chunks; ++c) s += partial[static_cast<int64_t>(c) * total + idx];
+  for (int c = 0; c < chunks; ++c) s += partial[static_cast<int64_t>(c) * total + src];
   G[static_cast<int64_t>(j) * ldg + i] = s;
 }
 
@@ -318,6 +323,32 @@ size_t gram_workspace_bytes(int64_t n, int64_t k, int64_t m) {
   return static_cast<size_t>(std::min(by_tiles, by_rows)) * sizeof(double);
 }
 
+// FP64 products: 0 = DMMA tensor-core kernels (dmma.cu), 1 = SIMT kernels.
+static int g_f64_gemm_mode = 0;
+
+void set_f64_gemm_mode(int mode) { g_f64_gemm_mode = mode; }
+
+// Split-K Gram partials for plan p; returns whether only the upper tiles were
+// computed (X and Y the same view), which the reduction then mirrors.
+template <typename T>
+bool launch_gram_partial(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k,
+                         int64_t m, const GramPlan& p, double* partial, cudaStream_t s) {
+  if constexpr (std::is_same_v<T, double>) {
+    if (g_f64_gemm_mode == 0) {
+      const bool sym = X == Y && ldx == ldy && k == m;
+      gram_partial_dmma(X, ldx, Y, ldy, n, static_cast<int>(k), static_cast<int>(m), p.tiles_k,
+                        p.tiles_m, p.chunks, p.rows_per_chunk, sym, partial, s);
+      return sym;
+    }
+  }
+  dim3 grid(p.tiles_k, p.tiles_m, p.chunks);
+  gram_partial_kernel<T><<<grid, kGramThreads, 0, s>>>(X, ldx, Y, ldy, n, static_cast<int>(k),
+                                                       static_cast<int>(m), p.rows_per_chunk,
+                                                       partial);
+  check_launch("gram_partial_kernel");
+  return false;
+}
+
 template <typename T>
 void gram(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k, int64_t m,
           double* G, int64_t ldg, void* ws, size_t ws_bytes, cudaStream_t s) {
@@ -332,14 +363,11 @@ void gram(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k
   FE_REQUIRE(X && Y && ldx >= k && ldy >= m, "gram: invalid input block");
   const GramPlan p = gram_plan(n, k, m);
   FE_REQUIRE(ws && ws_bytes >= p.bytes, "gram: workspace too small");
-  dim3 grid(p.tiles_k, p.tiles_m, p.chunks);
-  gram_partial_kernel<T><<<grid, kGramThreads, 0, s>>>(X, ldx, Y, ldy, n, static_cast<int>(k),
-                                              static_cast<int>(m), p.rows_per_chunk,
-                                              static_cast<double*>(ws));
-  check_launch("gram_partial_kernel");
+  const bool sym = launch_gram_partial(X, ldx, Y, ldy, n, k, m, p, static_cast<double*>(ws), s);
   const int64_t total = k * m;
   gram_reduce_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
-      static_cast<const double*>(ws), p.chunks, static_cast<int>(k), static_cast<int>(m), G, ldg);
+      static_cast<const double*>(ws), p.chunks, static_cast<int>(k), static_cast<int>(m), G, ldg,
+      sym ? 1 : 0);
   check_launch("gram_reduce_kernel");
 }
 
@@ -363,6 +391,12 @@ void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t
   FE_REQUIRE(X && C && ldx >= k && ldc >= k, "rotate: invalid input");
   FE_REQUIRE(!ranges_overlap(X, n, ldx, k, static_cast<const T*>(Y), n, ldy, m),
              "rotate: X and Y overlap");
+  if constexpr (std::is_same_v<T, double>) {
+    if (g_f64_gemm_mode == 0) {
+      rotate_dmma(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, s);
+      return;
+    }
+  }
   const int64_t row_tiles = (n + kRT - 1) / kRT;
   FE_REQUIRE(row_tiles <= 65535LL * 32768LL, "rotate: too many rows");
   const int64_t col_tiles = (m + kRT - 1) / kRT;
@@ -598,6 +632,112 @@ void fill_uniform(T* X, int64_t ld, int64_t n, int64_t m, uint64_t seed, cudaStr
 template void fill_uniform<double>(double*, int64_t, int64_t, int64_t, uint64_t, cudaStream_t);
 template void fill_uniform<float>(float*, int64_t, int64_t, int64_t, uint64_t, cudaStream_t);
 
+// ------------------------------------------------- small helper kernels ----
+namespace {
+
+// dst[:, j] = src[:, idx[j]] on row-major blocks (column gathers of residuals).
+template <typename T>
+__global__ void gather_columns_kernel(const T* __restrict__ src, int64_t lds,
+                                      const int32_t* __restrict__ idx, int m, T* __restrict__ dst,
+                                      int64_t ldd, int64_t n) {
+  const int64_t total = n * m;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = e / m;
+    const int j = static_cast<int>(e % m);
+    dst[r * ldd + j] = src[r * lds + idx[j]];
+  }
+}
+
+// Column-major small matrices: dst[:, j] = src[:, idx[j]] * (scale ? scale[j] : 1).
+__global__ void small_gather_scale_kernel(const double* __restrict__ src, int64_t lds, int rows,
+                                          const int32_t* __restrict__ idx,
+                                          const double* __restrict__ scale, int m,
+                                          double* __restrict__ dst, int64_t ldd) {
+  const int64_t total = static_cast<int64_t>(rows) * m;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % rows);
+    const int j = static_cast<int>(e / rows);
+    const double s = scale ? scale[j] : 1.0;
+    dst[static_cast<int64_t>(j) * ldd + i] = src[static_cast<int64_t>(idx[j]) * lds + i] * s;
+  }
+}
+
+// P[c, r] = P[r, c] for r < rows, c0 <= c < c0 + cols (column-major, ld).
+__global__ void mirror_block_kernel(double* P, int64_t ld, int rows, int c0, int cols) {
+  const int64_t total = static_cast<int64_t>(rows) * cols;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int r = static_cast<int>(e % rows);
+    const int c = c0 + static_cast<int>(e / rows);
+    P[static_cast<int64_t>(r) * ld + c] = P[static_cast<int64_t>(c) * ld + r];
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void gather_columns(const T* src, int64_t lds, const int32_t* idx, int64_t m, T* dst, int64_t ldd,
+                    int64_t n, cudaStream_t s) {
+  if (n <= 0 || m <= 0) return;
+  const int64_t blocks = std::min<int64_t>((n * m + 255) / 256, 148 * 32);
+  gather_columns_kernel<T><<<static_cast<unsigned>(blocks), 256, 0, s>>>(
+      src, lds, idx, static_cast<int>(m), dst, ldd, n);
+  check_launch("gather_columns_kernel");
+}
+template void gather_columns<double>(const double*, int64_t, const int32_t*, int64_t, double*,
+                                     int64_t, int64_t, cudaStream_t);
+template void gather_columns<float>(const float*, int64_t, const int32_t*, int64_t, float*,
+                                    int64_t, int64_t, cudaStream_t);
+
+void small_gather_scale(const double* src, int64_t lds, int64_t rows, const int32_t* idx,
+                        const double* scale, int64_t m, double* dst, int64_t ldd, cudaStream_t s) {
+  if (rows <= 0 || m <= 0) return;
+  const int64_t blocks = std::min<int64_t>((rows * m + 255) / 256, 1024);
+  small_gather_scale_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(
+      src, lds, static_cast<int>(rows), idx, scale, static_cast<int>(m), dst, ldd);
+  check_launch("small_gather_scale_kernel");
+}
+
+namespace {
+// Row-major (n x m, ld) -> column-major (n x m, leading dimension n), 32x32 tiles.
+__global__ void to_colmajor_kernel(const double* __restrict__ src, int64_t lds, int64_t n, int m,
+                                   double* __restrict__ dst) {
+  __shared__ double tile[32][33];
+  const int64_t r0 = static_cast<int64_t>(blockIdx.x) * 32;
+  const int c0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int64_t r = r0 + i;
+    const int c = c0 + threadIdx.x;
+    tile[i][threadIdx.x] = (r < n && c < m) ? src[r * lds + c] : 0.0;
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int c = c0 + j;
+    const int64_t r = r0 + threadIdx.x;
+    if (r < n && c < m) dst[static_cast<int64_t>(c) * n + r] = tile[threadIdx.x][j];
+  }
+}
+}  // namespace
+
+void to_colmajor(const double* src, int64_t lds, int64_t n, int64_t m, double* dst,
+                 cudaStream_t s) {
+  if (n <= 0 || m <= 0) return;
+  FE_REQUIRE((n + 31) / 32 <= 0x7fffffffLL && (m + 31) / 32 <= 65535, "to_colmajor: too large");
+  dim3 grid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>((m + 31) / 32));
+  to_colmajor_kernel<<<grid, dim3(32, 8), 0, s>>>(src, lds, n, static_cast<int>(m), dst);
+  check_launch("to_colmajor_kernel");
+}
+
+void mirror_block(double* P, int64_t ld, int64_t rows, int64_t c0, int64_t cols, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  const int64_t blocks = std::min<int64_t>((rows * cols + 255) / 256, 1024);
+  mirror_block_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(
+      P, ld, static_cast<int>(rows), static_cast<int>(c0), static_cast<int>(cols));
+  check_launch("mirror_block_kernel");
+}
+
 // --------------------------------------------- Gram without any allocation ----
 // Some callers cannot allocate device memory when they call us: a host program
 // that has already handed all device memory to its own pool, or code on a
@@ -653,13 +793,10 @@ void gram_f64_static(const double* X, int64_t ldx, const double* Y, int64_t ldy,
   // As many row chunks as the scratch holds (each chunk's k x m partial is written
   // in full by the partial kernel, so nothing needs clearing between calls).
   const GramPlan p = gram_plan(n, k, m, std::max<int64_t>(1, kStaticGramDoubles / (k * m)));
-  dim3 grid(p.tiles_k, p.tiles_m, p.chunks);
-  gram_partial_kernel<double><<<grid, kGramThreads, 0, s>>>(X, ldx, Y, ldy, n, static_cast<int>(k),
-                                                   static_cast<int>(m), p.rows_per_chunk, scratch);
-  check_launch("gram_partial_kernel");
+  const bool sym = launch_gram_partial(X, ldx, Y, ldy, n, k, m, p, scratch, s);
   const int64_t total = k * m;
   gram_reduce_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
-      scratch, p.chunks, static_cast<int>(k), static_cast<int>(m), G, ldg);
+      scratch, p.chunks, static_cast<int>(k), static_cast<int>(m), G, ldg, sym ? 1 : 0);
   check_launch("gram_reduce_kernel");
 }
 

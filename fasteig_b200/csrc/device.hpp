@@ -185,3 +185,14 @@ void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float*
                size_t ws_bytes, cudaStream_t s);
 int read_tc_status(bool clear);
 }  // namespace fe
+
+namespace fe {
+template <typename T>
+void gather_columns(const T* src, int64_t lds, const int32_t* idx, int64_t m, T* dst, int64_t ldd,
+                    int64_t n, cudaStream_t s);
+void small_gather_scale(const double* src, int64_t lds, int64_t rows, const int32_t* idx,
+                        const double* scale, int64_t m, double* dst, int64_t ldd, cudaStream_t s);
+void mirror_block(double* P, int64_t ld, int64_t rows, int64_t c0, int64_t cols, cudaStream_t s);
+void to_colmajor(const double* src, int64_t lds, int64_t n, int64_t m, double* dst,
+                 cudaStream_t s);
+}  // namespace fe

@@ -103,6 +103,14 @@ struct Csr {
 
 int num_sms();
 
+// FP64 tensor-core kernels (dmma.cu).
+void gram_partial_dmma(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t n,
+                       int k, int m, int tiles_k, int tiles_m, int chunks, int64_t rows_per_chunk,
+                       bool symmetric, double* partial, cudaStream_t s);
+void rotate_dmma(const double* X, int64_t ldx, const double* C, int64_t ldc, double* Y,
+                 int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
+                 cudaStream_t s);
+
 }  // namespace fe
 
 struct fe_csr {

@@ -741,6 +741,595 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   st.precise_grams = static_cast<double>(sm.precise_grams);
 }
 
+// ===========================================================================
+// Shared pieces of the block solvers (LOBPCG, Davidson) on FP64 blocks.
+// ===========================================================================
+
+// Relative residuals of the returned pairs, recomputed in FP64 on the device
+// (fasteig_problem::solve recomputes them for non-Krylov solvers,
+// src/fasteig_problem.cpp:419-422 -> src/fasteig_solver.cpp:89-129), and the
+// vectors to the host as column-major n x nev (transposed on the device).
+void finish_results(Context& ctx, SmallState& sm, const Csr& A, const Csr* B, const double* X,
+                    int64_t ldx, int64_t n, int64_t nev, const double* eigenvalues,
+                    double* residuals, double* eigenvectors) {
+  cudaStream_t s = ctx.stream;
+  Block<double> AX, BX;
+  AX.allocate(n, ldx);
+  csr_spmm<double>(A, X, ldx, AX.data(), AX.ld, nullptr, 0, nev, 1.0, 0.0, 0.0, s);
+  const double* MX = nullptr;
+  if (B) {
+    BX.allocate(n, ldx);
+    csr_spmm<double>(*B, X, ldx, BX.data(), BX.ld, nullptr, 0, nev, 1.0, 0.0, 0.0, s);
+    MX = BX.data();
+  }
+  FE_REQUIRE(AX.ld == ldx, "finish_results: leading dimension mismatch");
+  ctx.to_device(sm.W.as<double>(), eigenvalues, nev);
+  residual_norms<double>(AX.data(), X, MX, ldx, n, nev, sm.W.as<double>(), nullptr, 0,
+                         sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
+                         sm.rws.get(), sm.rws.bytes(), s, 1);
+  ctx.to_host(residuals, sm.rel.as<double>(), nev);
+  if (eigenvectors) {
+    DeviceBuffer cm(static_cast<size_t>(n) * nev * sizeof(double));
+    to_colmajor(X, ldx, n, nev, cm.as<double>(), s);
+    FE_CHECK_CUDA(cudaMemcpyAsync(eigenvectors, cm.get(), cm.bytes(), cudaMemcpyDeviceToHost, s));
+    ctx.sync();
+  }
+  ctx.sync();
+}
+
+// Reference selection order (lanczos_select_ritz_indices,
+// src/core/RitzExtraction.cpp:162-179; sort_indices, include/fasteig_solver.hpp:58-82).
+std::vector<int32_t> select_indices(const std::vector<double>& w, const std::string& which) {
+  const int m = static_cast<int>(w.size());
+  std::vector<int32_t> idx(m);
+  for (int i = 0; i < m; ++i) idx[i] = i;
+  if (which == "be") {
+    int pos = 0;
+    for (int i = 0; i < m / 2; ++i) {
+      idx[pos++] = m - 1 - i;
+      idx[pos++] = i;
+    }
+    if (m % 2 == 1) idx[pos] = m / 2;
+    return idx;
+  }
+  auto key = [&](int i) {
+    if (which == "sr") return w[i];
+    if (which == "lr") return -w[i];
+    if (which == "sm") return std::fabs(w[i]);
+    return -std::fabs(w[i]);  // lm
+  };
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return key(a) < key(b); });
+  return idx;
+}
+
+// Device Rayleigh-Ritz (extract_projected_ritz_pairs, src/core/RitzExtraction.cpp:65-141):
+// P (cols x cols, ld sm.cap, device) is destroyed. X = B C, AX = AB C, R = AX - X diag(l),
+// rel = ||r|| / ((1 + |l|) ||x||). C (cols x req, ld sm.cap) is left in `coef`.
+struct RitzResult {
+  std::vector<double> values, rel;
+};
+
+void ritz_extract(Context& ctx, SmallState& sm, ProjectedEig& eig, double* P, const double* Bm,
+                  const double* ABm, int64_t ld, int64_t n, int64_t cols, int64_t req,
+                  const std::string& which, double* X, double* AX, double* R, double* coef,
+                  DeviceBuffer& idx_dev, RitzResult& out) {
+  cudaStream_t s = ctx.stream;
+  symmetrize(P, cols, sm.cap, s);
+  eig.run(P, cols, sm.cap, sm.W.as<double>());
+  std::vector<double> w(cols);
+  int info = 0;
+  ctx.to_host(w.data(), sm.W.as<double>(), cols);
+  ctx.to_host(&info, eig.info(), 1);
+  ctx.sync();
+  if (info != 0) throw Error(FE_ERR_CUDA, "projected eigensolve failed.");
+  const std::vector<int32_t> idx = select_indices(w, which);
+  std::vector<int32_t> sel(idx.begin(), idx.begin() + req);
+  out.values.resize(req);
+  for (int64_t j = 0; j < req; ++j) out.values[j] = w[sel[j]];
+  idx_dev.resize(std::max<size_t>(sel.size() * sizeof(int32_t), 4));
+  ctx.to_device(idx_dev.as<int32_t>(), sel.data(), sel.size());
+  small_gather_scale(P, sm.cap, cols, idx_dev.as<int32_t>(), nullptr, req, coef, sm.cap, s);
+  rotate_block<double>(sm, Bm, ld, coef, X, ld, n, cols, req, 1.0, 0.0, s);
+  rotate_block<double>(sm, ABm, ld, coef, AX, ld, n, cols, req, 1.0, 0.0, s);
+  ctx.to_device(sm.W.as<double>(), out.values.data(), req);
+  residual_norms<double>(AX, X, nullptr, ld, n, req, sm.W.as<double>(), R, R ? ld : 0,
+                         sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
+                         sm.rws.get(), sm.rws.bytes(), s, 1);
+  out.rel.resize(req);
+  ctx.to_host(out.rel.data(), sm.rel.as<double>(), req);
+  ctx.sync();
+  for (int64_t j = 0; j < req; ++j)
+    if (!std::isfinite(out.values[j]) || !std::isfinite(out.rel[j]))
+      throw Error(FE_ERR_NONFINITE, "non-finite Ritz values or residuals.");
+}
+
+// Two-pass block Gram-Schmidt of src (n x b) against V[:, :k] into dst
+// (block_gram_schmidt, src/core/Orthogonalization.cpp:482-527). dst may be src.
+void block_gs(Context& ctx, SmallState& sm, const double* V, int64_t ld, int64_t k,
+              const double* src, double* dst, int64_t n, int64_t b) {
+  cudaStream_t s = ctx.stream;
+  if (dst != src)
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(dst, ld * sizeof(double), src, ld * sizeof(double),
+                                    b * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+  if (k == 0) return;
+  for (int pass = 0; pass < 2; ++pass) {
+    gram_block<double>(sm, V, ld, dst, ld, n, k, b, sm.G.as<double>(), s);
+    rotate_block<double>(sm, V, ld, sm.G.as<double>(), dst, ld, n, k, b, -1.0, 1.0, s);
+  }
+}
+
+// Orthonormal basis of the part of `src` outside V[:, :k], dropping numerically
+// dependent directions (orthonormalize_block, src/core/Orthogonalization.cpp:717-775).
+// Two passes of: column norms -> block Gram-Schmidt -> Gram -> eigen-decomposition
+// -> keep singular values above rank_tol * (largest column norm) -> rotate by
+// U Sigma^-1. The reference takes the SVD of the Householder R of the projected
+// block; the singular values and retained span are the same, computed here from the
+// FP64 Gram, which resolves singular values down to ~1e-8 of the largest, so
+// directions below that (and below rank_tol) are dropped. Returns the rank; the
+// result is in out[:, :rank].
+int64_t ortho_block(Context& ctx, SmallState& sm, ProjectedEig& eig, const double* V, int64_t ld,
+                    int64_t k, const double* src, int64_t b, double* out, double* tmp,
+                    int64_t n, DeviceBuffer& idx_dev, double rank_tol = 1e-12) {
+  cudaStream_t s = ctx.stream;
+  if (k >= n) return 0;
+  const double* cur = src;
+  int64_t cols = b;
+  int64_t rank = 0;
+  std::vector<double> norms, w, scale_v;
+  for (int pass = 0; pass < 2; ++pass) {
+    norms.resize(cols);
+    residual_norms<double>(nullptr, cur, nullptr, ld, n, cols, nullptr, nullptr, 0, nullptr,
+                           sm.xnorm.as<double>(), nullptr, sm.rws.get(), sm.rws.bytes(), s, 0);
+    ctx.to_host(norms.data(), sm.xnorm.as<double>(), cols);
+    ctx.sync();
+    double scale = 0.0;
+    for (double v : norms) {
+      if (!std::isfinite(v)) throw Error(FE_ERR_NONFINITE, "orthonormalize_block: non-finite column norms.");
+      scale = std::max(scale, v);
+    }
+    if (scale == 0.0) return 0;
+    block_gs(ctx, sm, V, ld, k, cur, tmp, n, cols);
+    double* G = sm.G.as<double>();
+    gram_block<double>(sm, tmp, ld, tmp, ld, n, cols, cols, G, s);
+    symmetrize(G, cols, sm.cap, s);
+    eig.run(G, cols, sm.cap, sm.W.as<double>());
+    w.resize(cols);
+    ctx.to_host(w.data(), sm.W.as<double>(), cols);
+    ctx.sync();
+    const double smax = std::sqrt(std::max(w[cols - 1], 0.0));
+    const int64_t capacity = std::min<int64_t>(cols, n - k);
+    const double cut = std::max(rank_tol * scale, 1e-7 * smax);
+    std::vector<int32_t> sel;
+    scale_v.clear();
+    for (int64_t i = cols - 1; i >= 0 && static_cast<int64_t>(sel.size()) < capacity; --i) {
+      const double sv = std::sqrt(std::max(w[i], 0.0));
+      if (!(sv > cut)) break;
+      sel.push_back(static_cast<int32_t>(i));
+      scale_v.push_back(1.0 / sv);
+    }
+    rank = static_cast<int64_t>(sel.size());
+    if (rank == 0) return 0;
+    const size_t dbl_off = ((rank * sizeof(int32_t) + 7) / 8) * 8;
+    idx_dev.resize(dbl_off + rank * sizeof(double));
+    int32_t* di = idx_dev.as<int32_t>();
+    double* ds = reinterpret_cast<double*>(idx_dev.as<uint8_t>() + dbl_off);
+    ctx.to_device(di, sel.data(), rank);
+    ctx.to_device(ds, scale_v.data(), rank);
+    small_gather_scale(G, sm.cap, cols, di, ds, rank, sm.Rinv.as<double>(), sm.cap, s);
+    rotate_block<double>(sm, tmp, ld, sm.Rinv.as<double>(), out, ld, n, cols, rank, 1.0, 0.0, s);
+    cur = out;
+    cols = rank;
+    ctx.sync();
+  }
+  return rank;
+}
+
+// Cholesky QR twice in place through `tmp` (stands in for the reference's
+// Householder QR of nearly orthonormal blocks: same span, orthonormal to FP64).
+void cholqr2_inplace(Context& ctx, SmallState& sm, double* X, double* tmp, int64_t ld, int64_t n,
+                     int64_t b, const char* what) {
+  FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, 4 * sizeof(int32_t), ctx.stream));
+  cholqr<double>(ctx, sm, X, ld, tmp, ld, n, b, 0);
+  cholqr<double>(ctx, sm, tmp, ld, X, ld, n, b, 1);
+  int32_t info[2] = {0, 0};
+  ctx.to_host(info, sm.info.as<int32_t>(), 2);
+  ctx.sync();
+  if (info[0] != 0 || info[1] != 0) throw Error(FE_ERR_NOT_SPD, std::string(what) + ": QR failed.");
+}
+
+void fill_initial_block(Context& ctx, double* X, int64_t ld, int64_t n, int64_t cols, unsigned seed,
+                        bool host_init) {
+  if (host_init) {
+    std::mt19937 rng(seed);
+    std::uniform_real_distribution<double> dist(-1.0, 1.0);
+    std::vector<double> host(static_cast<size_t>(n) * ld, 0.0);
+    for (int64_t j = 0; j < cols; ++j)
+      for (int64_t i = 0; i < n; ++i) host[static_cast<size_t>(i) * ld + j] = dist(rng);
+    ctx.to_device(X, host.data(), host.size());
+    ctx.sync();
+  } else {
+    fill_uniform<double>(X, ld, n, cols, seed, ctx.stream);
+  }
+}
+
+// LOBPCGSolver::solve (src/LOBPCGSolver.cpp:25-174): unpreconditioned LOBPCG with
+// block width nev, soft locking, basis [X W P] of at most min(n, 3 nev) columns.
+void lobpcg_solve(const Csr& A, const Options& opt, double* eigenvalues, double* residuals,
+                  double* eigenvectors, Stats& st) {
+  const int64_t n = A.rows, nev = opt.nev;
+  if (n <= 0 || nev <= 0 || nev > n || opt.maxiter <= 0)
+    throw Error(FE_ERR_INVALID, "LOBPCGSolver: require 0 < nev <= n and maxiter > 0.");
+  if (opt.which != "sr" && opt.which != "lr")
+    throw Error(FE_ERR_INVALID, "LOBPCGSolver: only SR and LR are supported.");
+  const double sign = opt.which == "lr" ? -1.0 : 1.0;
+  const double tol = opt.tol;
+  const int64_t cap = std::min<int64_t>(n, 3 * nev);
+  Context ctx;
+  cudaStream_t s = ctx.stream;
+  SmallState sm;
+  sm.allocate(n, cap, false);
+  ProjectedEig eig(ctx, cap);
+  Block<double> X, AX, R, Pd, S, AS, T1, T2, Wsrc;
+  for (Block<double>* b : {&X, &AX, &R, &Pd, &S, &AS, &T1, &T2, &Wsrc}) b->allocate(n, cap);
+  const int64_t ld = X.ld;
+  DeviceBuffer idx_dev(static_cast<size_t>(cap) * 16), coef(static_cast<size_t>(cap) * cap * sizeof(double));
+  fill_initial_block(ctx, X.data(), ld, n, nev, opt.seed_or_default(), opt.init == "host");
+  cholqr2_inplace(ctx, sm, X.data(), T1.data(), ld, n, nev, "LOBPCGSolver: initial");
+  csr_spmm<double>(A, X.data(), ld, AX.data(), ld, nullptr, 0, nev, sign, 0.0, 0.0, s);
+  st.spmm_launches += 1;
+  // Rayleigh-Ritz on span(X) (src/LOBPCGSolver.cpp:72-78).
+  FE_CHECK_CUDA(cudaMemcpy2DAsync(S.data(), ld * 8, X.data(), ld * 8, nev * 8, n,
+                                  cudaMemcpyDeviceToDevice, s));
+  FE_CHECK_CUDA(cudaMemcpy2DAsync(AS.data(), ld * 8, AX.data(), ld * 8, nev * 8, n,
+                                  cudaMemcpyDeviceToDevice, s));
+  gram_block<double>(sm, S.data(), ld, AS.data(), ld, n, nev, nev, sm.G.as<double>(), s);
+  RitzResult ritz;
+  ritz_extract(ctx, sm, eig, sm.G.as<double>(), S.data(), AS.data(), ld, n, nev, nev, "sr",
+               X.data(), AX.data(), R.data(), coef.as<double>(), idx_dev, ritz);
+  bool have_p = false;
+  int64_t it_done = 0;
+  for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
+    double worst = 0;
+    for (double v : ritz.rel) worst = std::max(worst, v);
+    if (worst <= tol) break;
+    std::vector<int32_t> active;
+    for (int64_t j = 0; j < nev; ++j)
+      if (ritz.rel[j] > tol) active.push_back(static_cast<int32_t>(j));
+    const int64_t na = static_cast<int64_t>(active.size());
+    DeviceBuffer act(na * sizeof(int32_t));
+    ctx.to_device(act.as<int32_t>(), active.data(), na);
+    gather_columns<double>(R.data(), ld, act.as<int32_t>(), na, Wsrc.data(), ld, n, s);
+    cholqr2_inplace(ctx, sm, X.data(), T1.data(), ld, n, nev, "LOBPCGSolver: Ritz-vector");
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(S.data(), ld * 8, X.data(), ld * 8, nev * 8, n,
+                                    cudaMemcpyDeviceToDevice, s));
+    int64_t cols = nev;
+    const int64_t rw = ortho_block(ctx, sm, eig, S.data(), ld, cols, Wsrc.data(), na, T1.data(),
+                                   T2.data(), n, idx_dev);
+    if (rw > 0) {
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(S.col(cols), ld * 8, T1.data(), ld * 8, rw * 8, n,
+                                      cudaMemcpyDeviceToDevice, s));
+      cols += rw;
+    }
+    if (have_p && cols < cap) {
+      gather_columns<double>(Pd.data(), ld, act.as<int32_t>(), na, Wsrc.data(), ld, n, s);
+      int64_t rp = ortho_block(ctx, sm, eig, S.data(), ld, cols, Wsrc.data(), na, T1.data(),
+                               T2.data(), n, idx_dev);
+      rp = std::min(rp, cap - cols);
+      if (rp > 0) {
+        FE_CHECK_CUDA(cudaMemcpy2DAsync(S.col(cols), ld * 8, T1.data(), ld * 8, rp * 8, n,
+                                        cudaMemcpyDeviceToDevice, s));
+        cols += rp;
+      }
+    }
+    // Rayleigh-Ritz in S = [X W P] with a fresh A*S (src/LOBPCGSolver.cpp:134-138).
+    csr_spmm<double>(A, S.data(), ld, AS.data(), ld, nullptr, 0, cols, sign, 0.0, 0.0, s);
+    st.spmm_launches += 1;
+    gram_block<double>(sm, S.data(), ld, AS.data(), ld, n, cols, cols, sm.G.as<double>(), s);
+    ritz_extract(ctx, sm, eig, sm.G.as<double>(), S.data(), AS.data(), ld, n, cols, nev, "sr",
+                 X.data(), AX.data(), R.data(), coef.as<double>(), idx_dev, ritz);
+    // P = S C with the X rows of C zeroed (src/LOBPCGSolver.cpp:147-150).
+    FE_CHECK_CUDA(cudaMemset2DAsync(coef.get(), cap * 8, 0, nev * 8, nev, s));
+    rotate_block<double>(sm, S.data(), ld, coef.as<double>(), Pd.data(), ld, n, cols, nev, 1.0, 0.0,
+                         s);
+    have_p = true;
+    it_done = iter + 1;
+    worst = 0;
+    for (double v : ritz.rel) worst = std::max(worst, v);
+    if (opt.verbosity >= 2)
+      std::fprintf(stderr, "[fe] lobpcg iter %lld cols %lld worst %.3e\n",
+                   static_cast<long long>(iter + 1), static_cast<long long>(cols), worst);
+    if (worst <= tol || cols == nev) break;
+  }
+  for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = sign * ritz.values[j];
+  finish_results(ctx, sm, A, nullptr, X.data(), ld, n, nev, eigenvalues, residuals, eigenvectors);
+  st.iterations = static_cast<double>(it_done);
+  st.fp64_iterations = static_cast<double>(it_done);
+}
+
+// DavidsonSolver::solve (src/DavidsonSolver.cpp:27-264): block Davidson with thick
+// restart, unpreconditioned residual corrections, locktol = min(1e-5, tol).
+void davidson_solve(const Csr& A, const Options& opt, double* eigenvalues, double* residuals,
+                    double* eigenvectors, Stats& st) {
+  const int64_t n = A.rows, nev = opt.nev;
+  if (n <= 0) throw Error(FE_ERR_INVALID, "DavidsonSolver: n must be > 0.");
+  if (nev <= 0 || nev > n) throw Error(FE_ERR_INVALID, "DavidsonSolver: nev must be in [1,n].");
+  if (opt.maxiter <= 0) throw Error(FE_ERR_INVALID, "DavidsonSolver: maxiter must be > 0.");
+  if (opt.maxblks < 1) throw Error(FE_ERR_INVALID, "DavidsonSolver: maxblks must be at least 1.");
+  const std::string which = opt.which;
+  if (which == "sai")
+    throw Error(FE_ERR_INVALID, "DavidsonSolver: SAI is not supported yet; use SR/LR/SM/LM/BE.");
+  if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
+    throw Error(FE_ERR_INVALID, "DavidsonSolver: invalid which option (use SR/LR/SM/LM/BE).");
+  const double tol = opt.tol;
+  const int64_t cap = std::min<int64_t>(n, opt.maxblks * nev);
+  Context ctx;
+  cudaStream_t s = ctx.stream;
+  SmallState sm;
+  sm.allocate(n, cap, false);
+  ProjectedEig eig(ctx, cap);
+  Block<double> V, AV, X, AX, R, Cb, ACb, T1;
+  for (Block<double>* b : {&V, &AV, &X, &AX, &R, &Cb, &ACb, &T1}) b->allocate(n, cap);
+  const int64_t ld = V.ld;
+  DeviceBuffer idx_dev(static_cast<size_t>(cap) * 16), coef(static_cast<size_t>(cap) * cap * sizeof(double));
+  DeviceBuffer proj(static_cast<size_t>(cap) * cap * sizeof(double));
+  double* Pm = proj.as<double>();
+  double* Pw = sm.G.as<double>();
+  auto extract = [&](int64_t cols, RitzResult& out) {
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(Pw, cap * 8, Pm, cap * 8, cols * 8, cols,
+                                    cudaMemcpyDeviceToDevice, s));
+    ritz_extract(ctx, sm, eig, Pw, V.data(), AV.data(), ld, n, cols, nev, which, X.data(),
+                 AX.data(), R.data(), coef.as<double>(), idx_dev, out);
+  };
+  // Initial block: random, Cholesky QR (src/DavidsonSolver.cpp:59-79).
+  fill_initial_block(ctx, X.data(), ld, n, nev, opt.seed_or_default(), opt.init == "host");
+  {
+    FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, 4 * sizeof(int32_t), s));
+    cholqr<double>(ctx, sm, X.data(), ld, V.data(), ld, n, nev, 0);
+    int32_t info = 0;
+    ctx.to_host(&info, sm.info.as<int32_t>(), 1);
+    ctx.sync();
+    if (info != 0) throw Error(FE_ERR_NOT_SPD, "DavidsonSolver: initial Cholesky QR failed.");
+  }
+  csr_spmm<double>(A, V.data(), ld, AV.data(), ld, nullptr, 0, nev, 1.0, 0.0, 0.0, s);
+  st.spmm_launches += 1;
+  gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, nev, nev, Pm, s);
+  RitzResult ritz;
+  extract(nev, ritz);
+  const double locktol = std::min(1.0e-5, tol);
+  int64_t it_done = 0;
+  for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
+    // Thick restart (src/DavidsonSolver.cpp:131-155).
+    cholqr2_inplace(ctx, sm, X.data(), T1.data(), ld, n, nev, "DavidsonSolver: restart");
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(V.data(), ld * 8, X.data(), ld * 8, nev * 8, n,
+                                    cudaMemcpyDeviceToDevice, s));
+    csr_spmm<double>(A, V.data(), ld, AV.data(), ld, nullptr, 0, nev, 1.0, 0.0, 0.0, s);
+    st.spmm_launches += 1;
+    FE_CHECK_CUDA(cudaMemset2DAsync(Pm, cap * 8, 0, cap * 8, cap, s));
+    gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, nev, nev, Pm, s);
+    int64_t cols = nev;
+    extract(cols, ritz);
+    for (int64_t blk = 1; blk < opt.maxblks; ++blk) {
+      std::vector<int32_t> active;
+      for (int64_t j = 0; j < nev; ++j)
+        if (ritz.rel[j] > locktol) active.push_back(static_cast<int32_t>(j));
+      const int64_t cc = static_cast<int64_t>(active.size());
+      if (cc == 0 || cols + cc > cap) break;
+      DeviceBuffer act(cc * sizeof(int32_t));
+      ctx.to_device(act.as<int32_t>(), active.data(), cc);
+      gather_columns<double>(R.data(), ld, act.as<int32_t>(), cc, Cb.data(), ld, n, s);
+      block_gs(ctx, sm, V.data(), ld, cols, Cb.data(), Cb.data(), n, cc);
+      cholqr2_inplace(ctx, sm, Cb.data(), T1.data(), ld, n, cc,
+                      "DavidsonSolver: correction-block");
+      csr_spmm<double>(A, Cb.data(), ld, ACb.data(), ld, nullptr, 0, cc, 1.0, 0.0, 0.0, s);
+      st.spmm_launches += 1;
+      // projected[:cols, cols:cols+cc] = V^T A C, mirrored; diagonal block C^T A C.
+      gram_block<double>(sm, V.data(), ld, ACb.data(), ld, n, cols, cc, Pm + cols * cap, s);
+      gram_block<double>(sm, Cb.data(), ld, ACb.data(), ld, n, cc, cc, Pm + cols * cap + cols, s);
+      mirror_block(Pm, cap, cols, cols, cc, s);
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(V.col(cols), ld * 8, Cb.data(), ld * 8, cc * 8, n,
+                                      cudaMemcpyDeviceToDevice, s));
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(AV.col(cols), ld * 8, ACb.data(), ld * 8, cc * 8, n,
+                                      cudaMemcpyDeviceToDevice, s));
+      cols += cc;
+      extract(cols, ritz);
+    }
+    it_done = iter + 1;
+    double worst = 0;
+    for (double v : ritz.rel) worst = std::max(worst, v);
+    if (opt.verbosity >= 2)
+      std::fprintf(stderr, "[fe] davidson iter %lld cols %lld worst %.3e\n",
+                   static_cast<long long>(iter + 1), static_cast<long long>(cols), worst);
+    if (!ritz.rel.empty() && worst < tol) break;
+  }
+  for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = ritz.values[j];
+  finish_results(ctx, sm, A, nullptr, X.data(), ld, n, nev, eigenvalues, residuals, eigenvectors);
+  st.iterations = static_cast<double>(it_done);
+  st.fp64_iterations = static_cast<double>(it_done);
+}
+
+// KrylovSchurSolver::solve (src/KrylovSchurSolver.cpp:28-160) for standard problems:
+// scalar Lanczos with two-pass classical reorthogonalization (KrylovSubspace,
+// src/core/KrylovSubspace.cpp:125-259) on the device, the m x m projected
+// eigenproblem on the host, Krylov-Schur restarts that keep the wanted Ritz
+// vectors and a dense coupling row (CpuLanczosWorkspace::prepare_krylov_schur_restart,
+// src/core/LanczosWorkspace.cpp:94-107), and final Ritz pairs evaluated on the
+// device (evaluate_ritz_pairs, src/core/RitzExtraction.cpp:34-63).
+void krylov_schur_solve(const Csr& A, const Options& opt, double* eigenvalues, double* residuals,
+                        double* eigenvectors, Stats& st) {
+  const int64_t n = A.rows, nev = opt.nev;
+  if (n <= 0) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: n must be > 0.");
+  if (nev <= 0 || nev > n) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: nev must be in [1,n].");
+  if (opt.maxiter <= 0) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: maxiter must be > 0.");
+  const std::string which = opt.which;
+  if (which == "sai")
+    throw Error(FE_ERR_UNSUPPORTED,
+                "KrylovSchurSolver: SAI needs a shift-invert factorization (out of scope here).");
+  if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
+    throw Error(FE_ERR_INVALID, "KrylovSchurSolver: invalid which option (use SR/LR/SM/LM/BE/SAI).");
+  const double tol = opt.tol;
+  const int64_t m = std::min<int64_t>(std::max<int64_t>({2 * nev, 20, opt.maxdim}), n);
+  const unsigned seed = opt.seed_or_default();
+  const bool host_init = opt.init == "host";
+  Context ctx;
+  cudaStream_t s = ctx.stream;
+  SmallState sm;
+  sm.allocate(n, m, false);
+  Block<double> V, Y;
+  V.allocate(n, m);
+  Y.allocate(n, m);
+  const int64_t ld = V.ld;
+  DeviceBuffer f(n * sizeof(double)), w(n * sizeof(double)), h(m * sizeof(double)),
+      hs(m * sizeof(double)), nrm(sizeof(double)), C(static_cast<size_t>(m) * m * sizeof(double));
+  DeviceBuffer gws(std::max<size_t>(gram_workspace_bytes(n, m, 1), 64));
+  DeviceBuffer rws(std::max<size_t>(residual_workspace_bytes(n, m), 64));
+  auto random_into = [&](double* dst, unsigned sd) {
+    if (host_init) {
+      std::mt19937 rng(sd);
+      std::uniform_real_distribution<double> dist(-1.0, 1.0);
+      std::vector<double> v(n);
+      for (auto& x : v) x = dist(rng);
+      ctx.to_device(dst, v.data(), n);
+    } else {
+      fill_uniform<double>(dst, 1, n, 1, sd, s);
+    }
+  };
+  auto norm = [&](const double* x) {
+    residual_norms<double>(nullptr, x, nullptr, 1, n, 1, nullptr, nullptr, 0, nullptr,
+                           nrm.as<double>(), nullptr, rws.get(), rws.bytes(), s, 0);
+    double r = 0;
+    ctx.to_host(&r, nrm.as<double>(), 1);
+    ctx.sync();
+    return r;
+  };
+  // f = src - V_k (V_k^T src), twice; returns the last coefficient (alpha).
+  auto orthogonalize = [&](int64_t k, const double* src) {
+    vec_axpby(n, 1.0, src, 1, 0.0, f.as<double>(), 1, s);
+    if (k == 0) return 0.0;
+    gram<double>(V.data(), ld, f.as<double>(), 1, n, k, 1, h.as<double>(), k, gws.get(),
+                 gws.bytes(), s);
+    rotate<double>(V.data(), ld, h.as<double>(), k, f.as<double>(), 1, n, k, 1, -1.0, 1.0, s);
+    gram<double>(V.data(), ld, f.as<double>(), 1, n, k, 1, hs.as<double>(), k, gws.get(),
+                 gws.bytes(), s);
+    rotate<double>(V.data(), ld, hs.as<double>(), k, f.as<double>(), 1, n, k, 1, -1.0, 1.0, s);
+    double a = 0, b = 0;
+    ctx.to_host(&a, h.as<double>() + k - 1, 1);
+    ctx.to_host(&b, hs.as<double>() + k - 1, 1);
+    ctx.sync();
+    return a + b;
+  };
+  std::vector<double> T(static_cast<size_t>(m) * m, 0.0);
+  auto t = [&](int64_t r, int64_t c) -> double& { return T[static_cast<size_t>(c) * m + r]; };
+  double beta_next = 0.0;
+  int64_t restart_row = -1;
+  random_into(f.as<double>(), seed);
+  auto expand = [&](int64_t begin) {
+    for (int64_t col = begin; col < m; ++col) {
+      bool restarted = false;
+      double beta = norm(f.as<double>());
+      if (!std::isfinite(beta))
+        throw Error(FE_ERR_NONFINITE, "core::KrylovSubspace: non-finite residual norm encountered.");
+      if (!(beta > std::numeric_limits<double>::epsilon())) {
+        DeviceBuffer cand(n * sizeof(double));
+        random_into(cand.as<double>(), seed + static_cast<unsigned>(col + 1));
+        orthogonalize(col, cand.as<double>());
+        restarted = true;
+        beta = norm(f.as<double>());
+        if (!(beta > std::numeric_limits<double>::epsilon()))
+          throw Error(FE_ERR_NONFINITE,
+                      "core::KrylovSubspace: breakdown, unable to generate new basis vector.");
+      }
+      vec_axpby(n, 1.0 / beta, f.as<double>(), 1, 0.0, V.col(col), ld, s);
+      csr_spmm<double>(A, V.col(col), ld, w.as<double>(), 1, nullptr, 0, 1, 1.0, 0.0, 0.0, s);
+      st.spmm_launches += 1;
+      const double alpha = orthogonalize(col + 1, w.as<double>());
+      beta_next = norm(f.as<double>());
+      if (!std::isfinite(beta_next))
+        throw Error(FE_ERR_NONFINITE, "core::KrylovSubspace: non-finite next residual norm encountered.");
+      const double rec_beta = restarted ? 0.0 : beta;
+      if (col != 0 && col != restart_row) {
+        t(col, col - 1) = rec_beta;
+        t(col - 1, col) = rec_beta;
+      }
+      t(col, col) = alpha;
+      if (col == restart_row) restart_row = -1;
+    }
+  };
+  expand(0);
+  std::unique_ptr<ProjectedEig> deig;
+  DeviceBuffer Td;
+  if (m > 96) {  // large projected matrices: cuSOLVER on the device
+    deig.reset(new ProjectedEig(ctx, m));
+    Td.resize(static_cast<size_t>(m) * m * sizeof(double));
+  }
+  for (int64_t iter = 1; iter <= opt.maxiter; ++iter) {
+    std::vector<double> lam, Z;
+    if (deig) {
+      ctx.to_device(Td.as<double>(), T.data(), T.size());
+      deig->run(Td.as<double>(), m, m, sm.W.as<double>());
+      lam.resize(m);
+      Z.resize(T.size());
+      ctx.to_host(lam.data(), sm.W.as<double>(), m);
+      ctx.to_host(Z.data(), Td.as<double>(), Z.size());
+      ctx.sync();
+    } else {
+      host_symmetric_eig(T, static_cast<int>(m), lam, Z);
+    }
+    const std::vector<int32_t> idx = select_indices(lam, which);
+    std::vector<double> lam_s(m), rel_s(m);
+    for (int64_t j = 0; j < m; ++j) {
+      lam_s[j] = lam[idx[j]];
+      rel_s[j] = std::fabs(beta_next * Z[static_cast<size_t>(idx[j]) * m + m - 1]) /
+                 (1.0 + std::fabs(lam_s[j]));
+    }
+    int64_t nconv = 0;
+    for (int64_t j = 0; j < nev; ++j) {
+      const double mag = std::fabs(lam_s[j]);
+      if (rel_s[j] * (1.0 + mag) < tol * mag) ++nconv;
+    }
+    const bool at_limit = (m == n) || (iter == opt.maxiter);
+    if (opt.verbosity >= 2)
+      std::fprintf(stderr, "[fe] krylov-schur restart %lld nconv %lld\n",
+                   static_cast<long long>(iter), static_cast<long long>(nconv));
+    if (nconv >= nev || at_limit) {
+      // evaluate_ritz_pairs: Y = V Csel, R = A Y - Y diag(l), rel = ||r|| / ((1+|l|) ||y||)
+      std::vector<double> Cs(static_cast<size_t>(m) * nev);
+      for (int64_t j = 0; j < nev; ++j)
+        std::memcpy(&Cs[static_cast<size_t>(j) * m], &Z[static_cast<size_t>(idx[j]) * m],
+                    m * sizeof(double));
+      ctx.to_device(C.as<double>(), Cs.data(), Cs.size());
+      rotate<double>(V.data(), ld, C.as<double>(), m, Y.data(), Y.ld, n, m, nev, 1.0, 0.0, s);
+      for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = lam_s[j];
+      finish_results(ctx, sm, A, nullptr, Y.data(), Y.ld, n, nev, eigenvalues, residuals,
+                     eigenvectors);
+      st.iterations = static_cast<double>(iter);
+      st.fp64_iterations = static_cast<double>(iter);
+      return;
+    }
+    const int64_t spare = (m - nev) / 2;
+    int64_t retained = nev + std::min(nconv, spare);
+    if (retained == 1 && m > 3) retained = m / 2;
+    // rotate_basis: V[:, :retained] = V * C_all[:, :retained]
+    std::vector<double> Cr(static_cast<size_t>(m) * retained);
+    for (int64_t j = 0; j < retained; ++j)
+      std::memcpy(&Cr[static_cast<size_t>(j) * m], &Z[static_cast<size_t>(idx[j]) * m],
+                  m * sizeof(double));
+    ctx.to_device(C.as<double>(), Cr.data(), Cr.size());
+    rotate<double>(V.data(), ld, C.as<double>(), m, Y.data(), Y.ld, n, m, retained, 1.0, 0.0, s);
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(V.data(), ld * 8, Y.data(), Y.ld * 8, retained * 8, n,
+                                    cudaMemcpyDeviceToDevice, s));
+    std::fill(T.begin(), T.end(), 0.0);
+    for (int64_t j = 0; j < retained; ++j) {
+      t(j, j) = lam_s[j];
+      const double coupling = beta_next * Z[static_cast<size_t>(idx[j]) * m + m - 1];
+      t(retained, j) = coupling;
+      t(j, retained) = coupling;
+    }
+    restart_row = retained;
+    expand(retained);
+  }
+  throw Error(FE_ERR_INVALID, "KrylovSchurSolver: unreachable solve termination.");
+}
+
 }  // namespace
 }  // namespace fe
 
@@ -757,6 +1346,17 @@ extern "C" int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eig
     if (opt.solver == "chebyshev") {
       FE_REQUIRE(B == nullptr, "ChebyshevSolver: generalized problems are not supported.");
       fe::chebyshev_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
+    } else if (opt.solver == "lobpcg") {
+      FE_REQUIRE(B == nullptr, "LOBPCGSolver: generalized problems are not supported.");
+      fe::lobpcg_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
+    } else if (opt.solver == "davidson") {
+      FE_REQUIRE(B == nullptr, "DavidsonSolver: generalized problems are not supported.");
+      fe::davidson_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
+    } else if (opt.solver == "krylovschur") {
+      FE_REQUIRE(B == nullptr,
+                 "KrylovSchurSolver: generalized problems need a B^{-1} factorization (out of "
+                 "scope on this backend).");
+      fe::krylov_schur_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
     } else {
       throw fe::Error(FE_ERR_UNSUPPORTED, "solver not available on this backend: " + opt.solver);
     }

@@ -35,6 +35,7 @@ namespace fe {
 
 int read_spmm_status(bool clear);
 void set_spmm_mode(int mode);
+void set_f64_gemm_mode(int mode);
 
 __device__ int g_tc_status = 0;  // 0 = ok, otherwise a code of the first failed wait
 
@@ -695,6 +696,13 @@ extern "C" int fe_set_spmm_kernel(int32_t mode) {
   return fe::guarded("fe_set_spmm_kernel", [&] {
     FE_REQUIRE(mode >= 0 && mode <= 3, "mode must be 0..3");
     fe::set_spmm_mode(mode);
+  });
+}
+
+extern "C" int fe_set_f64_gemm_kernel(int32_t mode) {
+  return fe::guarded("fe_set_f64_gemm_kernel", [&] {
+    FE_REQUIRE(mode >= 0 && mode <= 1, "mode must be 0 or 1");
+    fe::set_f64_gemm_mode(mode);
   });
 }
 

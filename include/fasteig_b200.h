@@ -175,6 +175,11 @@ int fe_device_status(int32_t* status, int32_t clear);
  * pipelined kernel where it applies, 3 = row-batched kernel with narrower
  * column panels. */
 int fe_set_spmm_kernel(int32_t mode);
+/* FP64 Gram / rotation kernel selection for all later calls in the process:
+ * 0 = default (FP64 tensor-core mma.sync.m8n8k4 kernels with a cp.async ring),
+ * 1 = SIMT FP64-FMA kernels. Both accumulate every output in FP64; results
+ * differ only in the order of the rounded additions. */
+int fe_set_f64_gemm_kernel(int32_t mode);
 
 /* ---------------------------------------------------------------------
  * Ritz residuals and column norms (replaces the copy + add_scaled_columns +

@@ -821,3 +821,223 @@ def select_reference(values, which: str, count: int, shift: float = 0.0):
 def eigenvalue_check(got, expected, atol: float = 1e-10, rtol: float = 1e-10):
     """compare() of tests/scripts/run_case.py:246-260: |got-exp| <= atol + rtol*|exp|."""
     return [abs(g - e) <= atol + rtol * abs(e) for g, e in zip(got, expected)]
+
+
+# --------------------------------------------------------------------------
+# Extension (not in the reference): generalized K u = l M u and Jacobi-
+# preconditioned LOBPCG / block Davidson. The reference's LOBPCGSolver and
+# DavidsonSolver are standard-only and unpreconditioned (src/LOBPCGSolver.cpp:25-174,
+# src/DavidsonSolver.cpp:27-264); these follow the same loop structure with every
+# inner product taken in the B metric (B-weighted Gram as in the reference's
+# weighted Cholesky QR, src/core/Orthogonalization.cpp:407-440), corrections
+# W = T R with T = diag(|K_ii|)^-1, and the relative residual of
+# evaluate_ritz_pairs with B (src/core/RitzExtraction.cpp:50-56):
+# ||K x - l M x|| / ((1 + |l|) ||M x||). The CUDA drivers execute the same steps.
+# --------------------------------------------------------------------------
+
+
+def jacobi_inverse_diagonal(A: Csr) -> np.ndarray:
+    """t_i = 1 / |A_ii| (1 where the diagonal entry is zero or absent)."""
+    d = np.abs(A.scipy().diagonal())
+    return np.where(d > 0.0, 1.0 / np.where(d > 0.0, d, 1.0), 1.0)
+
+
+def _b_apply(B: Optional[Csr], X: np.ndarray) -> np.ndarray:
+    return X.copy() if B is None else B.scipy() @ X
+
+
+def ortho_block_b(B: Optional[Csr], V: Optional[np.ndarray], BV: Optional[np.ndarray], k: int,
+                  source: np.ndarray, rank_tolerance: float = 1e-12):
+    """B-orthonormal basis of the part of `source` outside span(V[:, :k]) (V B-orthonormal,
+    BV = B V): two passes of B-norms -> two-pass block Gram-Schmidt in the B metric ->
+    B-Gram eigen-decomposition -> keep singular values above
+    max(rank_tolerance * largest B-norm, 1e-7 * largest singular value) -> rotate by
+    U S^-1 (orthonormalize_block, src/core/Orthogonalization.cpp:717-775, with the SVD of
+    the QR factor replaced by the B-Gram). Returns (Q, BQ) or (None, None)."""
+    n = source.shape[0]
+    if k >= n:
+        return None, None
+    cur = source
+    BQ = None
+    for _ in range(2):
+        Bc = _b_apply(B, cur)
+        bn = np.sqrt(np.maximum(np.sum(cur * Bc, axis=0), 0.0))
+        if not np.all(np.isfinite(bn)):
+            raise RuntimeError("orthonormalize_block: non-finite column norms.")
+        scale = bn.max()
+        if scale == 0.0:
+            return None, None
+        if k > 0:
+            for _g in range(2):
+                H = V[:, :k].T @ Bc
+                cur = cur - V[:, :k] @ H
+                Bc = Bc - BV[:, :k] @ H
+        G = cur.T @ Bc
+        G = 0.5 * (G + G.T)
+        w, U = np.linalg.eigh(G)
+        cols = cur.shape[1]
+        smax = math.sqrt(max(w[-1], 0.0))
+        cut = max(rank_tolerance * scale, 1e-7 * smax)
+        capacity = min(cols, n - k)
+        sel, inv = [], []
+        for i in range(cols - 1, -1, -1):
+            if len(sel) >= capacity:
+                break
+            sv = math.sqrt(max(w[i], 0.0))
+            if not sv > cut:
+                break
+            sel.append(i)
+            inv.append(1.0 / sv)
+        if not sel:
+            return None, None
+        C = U[:, sel] * np.asarray(inv)[None, :]
+        cur = cur @ C
+        BQ = Bc @ C
+    return cur, BQ
+
+
+def b_cholesky_qr(B: Optional[Csr], X: np.ndarray):
+    """Weighted Cholesky QR with a fresh BX (src/core/Orthogonalization.cpp:407-440):
+    returns (X R^-1, BX R^-1)."""
+    BX = _b_apply(B, X)
+    G = X.T @ BX
+    G = 0.5 * (G + G.T)
+    try:
+        L = np.linalg.cholesky(G)
+    except np.linalg.LinAlgError:
+        raise RuntimeError("weighted Cholesky QR failed.")
+    Rinv = np.linalg.inv(L.T)
+    return X @ Rinv, BX @ Rinv
+
+
+def _gen_ritz(S, AS, BS, cols, req, which):
+    P = S[:, :cols].T @ AS[:, :cols]
+    P = 0.5 * (P + P.T)
+    w, Z = np.linalg.eigh(P)
+    idx = select_ritz_indices(w, which)[:req]
+    vals = w[idx]
+    C = Z[:, idx]
+    X = S[:, :cols] @ C
+    AX = AS[:, :cols] @ C
+    BX = BS[:, :cols] @ C
+    R = AX - BX * vals[None, :]
+    rn = np.linalg.norm(R, axis=0)
+    bn = np.linalg.norm(BX, axis=0)
+    den = (1.0 + np.abs(vals)) * bn
+    rel = np.where(den > 0.0, rn / np.where(den > 0.0, den, 1.0), rn)
+    if not (np.all(np.isfinite(vals)) and np.all(np.isfinite(rel))):
+        raise RuntimeError("non-finite Ritz values or residuals.")
+    return vals, C, X, AX, BX, R, rel
+
+
+def lobpcg_gen_solve(A: Csr, nev: int, B: Optional[Csr] = None, precond: str = "none",
+                     block: int = 0, tol: float = 1e-8, maxiter: int = 1000, which: str = "sr",
+                     seed: int = 1) -> SolveResult:
+    """LOBPCG for K u = l M u (M = I when B is None) with optional Jacobi preconditioning
+    and a block of `block` >= nev vectors (convergence on the first nev), loop of
+    src/LOBPCGSolver.cpp:25-174 in the B metric; basis [X W P] of at most 3*block columns."""
+    n = A.rows
+    which = which.lower()
+    if n <= 0 or nev <= 0 or nev > n or maxiter <= 0:
+        raise ValueError("LOBPCGSolver: require 0 < nev <= n and maxiter > 0.")
+    if which not in ("sr", "lr"):
+        raise ValueError("LOBPCGSolver: only SR and LR are supported.")
+    b = min(n, max(nev, block))
+    sign = -1.0 if which == "lr" else 1.0
+    Hs = A.scipy()
+    H = (lambda X: sign * (Hs @ X))
+    t = jacobi_inverse_diagonal(A) if precond == "jacobi" else None
+    cap = min(n, 3 * b)
+    X0 = random_block(n, b, seed)
+    X, BX = ortho_block_b(B, None, None, 0, X0)
+    if X is None or X.shape[1] < b:
+        raise RuntimeError("LOBPCGSolver: initial block is rank deficient.")
+    AX = H(X)
+    vals, C, X, AX, BX, R, rel = _gen_ritz(X, AX, BX, b, b, "sr")
+    P = None
+    it_done = 0
+    for it in range(maxiter):
+        if rel[:nev].max() <= tol:
+            break
+        active = [j for j in range(b) if rel[j] > tol]
+        Wsrc = R[:, active]
+        if t is not None:
+            Wsrc = Wsrc * t[:, None]
+        X, BX = b_cholesky_qr(B, X)
+        S = np.zeros((n, cap))
+        BS = np.zeros((n, cap))
+        S[:, :b], BS[:, :b] = X, BX
+        cols = b
+        W, BW = ortho_block_b(B, S, BS, cols, Wsrc)
+        if W is not None:
+            r = min(W.shape[1], cap - cols)
+            S[:, cols:cols + r], BS[:, cols:cols + r] = W[:, :r], BW[:, :r]
+            cols += r
+        if P is not None and cols < cap:
+            Pq, BPq = ortho_block_b(B, S, BS, cols, P[:, active])
+            if Pq is not None:
+                r = min(Pq.shape[1], cap - cols)
+                S[:, cols:cols + r], BS[:, cols:cols + r] = Pq[:, :r], BPq[:, :r]
+                cols += r
+        AS = H(S[:, :cols])
+        vals, C, X, AX, BX, R, rel = _gen_ritz(S, AS, BS, cols, b, "sr")
+        Cp = C.copy()
+        Cp[:b, :] = 0.0
+        P = S[:, :cols] @ Cp
+        it_done = it + 1
+        if rel[:nev].max() <= tol or cols == b:
+            break
+    return SolveResult(sign * vals[:nev], X[:, :nev].copy(), rel[:nev].copy(), it_done)
+
+
+def davidson_gen_solve(A: Csr, nev: int, B: Optional[Csr] = None, precond: str = "none",
+                       tol: float = 1e-8, maxiter: int = 1000, which: str = "sr", seed: int = 1,
+                       maxblks: int = 10) -> SolveResult:
+    """Block Davidson for K u = l M u with thick restart and optional Jacobi-preconditioned
+    corrections (loop of src/DavidsonSolver.cpp:27-264, locktol = min(1e-5, tol), in the
+    B metric)."""
+    n = A.rows
+    which = which.lower()
+    if nev <= 0 or nev > n:
+        raise ValueError("DavidsonSolver: nev must be in [1,n].")
+    if which not in ("sr", "lr", "sm", "lm", "be"):
+        raise ValueError("DavidsonSolver: invalid which option (use SR/LR/SM/LM/BE).")
+    Hs = A.scipy()
+    H = (lambda X: Hs @ X)
+    t = jacobi_inverse_diagonal(A) if precond == "jacobi" else None
+    cap = min(n, maxblks * nev)
+    X0 = random_block(n, nev, seed)
+    X, BX = ortho_block_b(B, None, None, 0, X0)
+    if X is None or X.shape[1] < nev:
+        raise RuntimeError("DavidsonSolver: initial block is rank deficient.")
+    AX = H(X)
+    vals, C, X, AX, BX, R, rel = _gen_ritz(X, AX, BX, nev, nev, which)
+    locktol = min(1.0e-5, tol)
+    it_done = 0
+    for it in range(maxiter):
+        X, BX = b_cholesky_qr(B, X)
+        V = np.zeros((n, cap))
+        BV = np.zeros((n, cap))
+        AV = np.zeros((n, cap))
+        V[:, :nev], BV[:, :nev], AV[:, :nev] = X, BX, H(X)
+        cols = nev
+        vals, C, X, AX, BX, R, rel = _gen_ritz(V, AV, BV, cols, nev, which)
+        for _blk in range(1, maxblks):
+            active = [j for j in range(nev) if rel[j] > locktol]
+            cc = len(active)
+            if cc == 0 or cols + cc > cap:
+                break
+            Wsrc = R[:, active]
+            if t is not None:
+                Wsrc = Wsrc * t[:, None]
+            W, BW = ortho_block_b(B, V, BV, cols, Wsrc)
+            if W is None:
+                break
+            r = W.shape[1]
+            V[:, cols:cols + r], BV[:, cols:cols + r], AV[:, cols:cols + r] = W, BW, H(W)
+            cols += r
+            vals, C, X, AX, BX, R, rel = _gen_ritz(V, AV, BV, cols, nev, which)
+        it_done = it + 1
+        if rel.max() < tol:
+            break
+    return SolveResult(vals.copy(), X.copy(), rel.copy(), it_done)

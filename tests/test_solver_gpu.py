@@ -91,3 +91,54 @@ def test_chebyshev_ritz_bounds_matches_oracle(wells12):
               degree=12, block=16, bounds="ritz", amplification=1e300)
     np.testing.assert_allclose(p.eigenvalues(), ref.eigenvalues, rtol=1e-10, atol=1e-12)
     assert abs(p.last_iterations() - ref.iterations) <= 2
+
+
+@pytest.mark.parametrize("solver", ["LOBPCG", "Davidson"])
+def test_block_solvers_sio_sr5_known_answers(sio, spectra, solver):
+    from oracle import oracle as O
+    p = solve(sio, solver=solver, nev=5, which="SR", tol=1e-8, maxiter=2000, seed=1)
+    exp = spectra["SiO"]["lowest"][:5]
+    assert all(O.eigenvalue_check(p.eigenvalues(), exp)), (p.eigenvalues(), exp)
+    assert np.all(p.residual_norms() <= 1.01e-8), p.residual_norms()
+    final = O.residual_norms(sio, None, p.eigenvalues(), p.eigenvectors())
+    assert np.all(final <= 1.01e-8), final
+
+
+@pytest.mark.parametrize("which", ["sr", "lr"])
+def test_lobpcg_matches_oracle(wells12, which):
+    from oracle import oracle as O
+    ref = O.lobpcg_solve(wells12, 6, tol=1e-8, maxiter=500, which=which, seed=2)
+    p = solve(wells12, solver="LOBPCG", nev=6, which=which, tol=1e-8, maxiter=500, seed=2)
+    np.testing.assert_allclose(p.eigenvalues(), ref.eigenvalues, rtol=1e-10, atol=1e-12)
+    assert abs(p.last_iterations() - ref.iterations) <= 3, (p.last_iterations(), ref.iterations)
+    assert subspace_angle(p.eigenvectors(), ref.eigenvectors) < 1e-6
+
+
+@pytest.mark.parametrize("which", ["sr", "lr", "be", "lm"])
+def test_davidson_matches_oracle(wells12, which):
+    from oracle import oracle as O
+    ref = O.davidson_solve(wells12, 6, tol=1e-8, maxiter=300, which=which, seed=3, maxblks=6)
+    p = solve(wells12, solver="Davidson", nev=6, which=which, tol=1e-8, maxiter=300, seed=3,
+              maxblks=6)
+    np.testing.assert_allclose(p.eigenvalues(), ref.eigenvalues, rtol=1e-10, atol=1e-12)
+    assert abs(p.last_iterations() - ref.iterations) <= 3, (p.last_iterations(), ref.iterations)
+    assert np.all(p.residual_norms() <= 1.01e-8)
+
+
+def test_krylov_schur_sio_sr5_known_answers(sio, spectra):
+    from oracle import oracle as O
+    p = solve(sio, solver="KrylovSchur", nev=5, which="SR", tol=1e-8, maxiter=2000, seed=1,
+              maxdim=40)
+    exp = spectra["SiO"]["lowest"][:5]
+    assert all(O.eigenvalue_check(p.eigenvalues(), exp)), (p.eigenvalues(), exp)
+    assert np.all(p.residual_norms() <= 1e-8), p.residual_norms()
+
+
+@pytest.mark.parametrize("which", ["sr", "lr", "lm", "be"])
+def test_krylov_schur_matches_oracle(wells12, which):
+    from oracle import oracle as O
+    ref = O.krylov_schur_solve(wells12, 6, tol=1e-8, maxiter=300, which=which, seed=5, maxdim=24)
+    p = solve(wells12, solver="KrylovSchur", nev=6, which=which, tol=1e-8, maxiter=300, seed=5,
+              maxdim=24)
+    np.testing.assert_allclose(p.eigenvalues(), ref.eigenvalues, rtol=1e-10, atol=1e-12)
+    assert abs(p.last_iterations() - ref.iterations) <= 1, (p.last_iterations(), ref.iterations)
