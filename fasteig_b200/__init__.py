@@ -15,6 +15,7 @@ _LAZY = {
     "CsrMatrix": ".problem",
     "fasteig_options": ".problem",
     "fasteig_problem": ".problem",
+    "batch_krylov_schur": ".problem",
 }
 
 __all__ = sorted(_LAZY)

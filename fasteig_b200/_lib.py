@@ -62,6 +62,7 @@ _SIGS = {
     "fe_device_status": (C.c_int, [C.POINTER(C.c_int32), C.c_int32]),
     "fe_set_spmm_kernel": (C.c_int, [C.c_int32]),
     "fe_set_f64_gemm_kernel": (C.c_int, [C.c_int32]),
+    "fe_batch_krylov_schur": (C.c_int, [C.c_int32, vp, vp, C.c_char_p, vp, vp, vp, vp, vp, vp]),
     "fe_gram_f64_noalloc": (C.c_int, [vp, i64, vp, i64, i64, i64, i64, vp, i64, vp]),
     "fe_gram_f64_noalloc_max_entries": (C.c_int64, []),
 }

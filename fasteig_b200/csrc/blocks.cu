@@ -218,7 +218,8 @@ residual_partial_kernel(const T* __restrict__ AX, const T* __restrict__ X,
                         const T* __restrict__ BX, int64_t ld, int64_t n, int m,
                         const double* __restrict__ lambda, T* __restrict__ R, int64_t ldr,
                         int64_t rows_per_chunk, double* __restrict__ partial, int mode) {
-  // mode 0: norms of X only (column_norms); mode 1: residual.
+  // mode 0: norms of X (of BX when given) only; mode 1: residual; mode 2: B-norms
+  // sqrt(x . Bx) of the columns of X (BX required).
   __shared__ double red[2][8][kNormCols];
   const int lane = threadIdx.x % 32;
   const int warp = threadIdx.x / 32;
@@ -227,12 +228,16 @@ residual_partial_kernel(const T* __restrict__ AX, const T* __restrict__ X,
   const int64_t r_end = min(n, r_begin + rows_per_chunk);
   double sr = 0.0, sx = 0.0;
   if (j < m) {
-    const double lam = mode ? lambda[j] : 0.0;
+    const double lam = mode == 1 ? lambda[j] : 0.0;
     const T* M = BX ? BX : X;
     for (int64_t r = r_begin + warp; r < r_end; r += 8) {
       const double mx = static_cast<double>(M[r * ld + j]);
+      if (mode == 2) {  // B-inner products x . (Bx)
+        sx = fma(static_cast<double>(X[r * ld + j]), mx, sx);
+        continue;
+      }
       sx = fma(mx, mx, sx);
-      if (mode) {
+      if (mode == 1) {
         const T rv = static_cast<T>(static_cast<double>(AX[r * ld + j]) - lam * mx);
         if (R) R[r * ldr + j] = rv;
         const double rd = static_cast<double>(rv);
@@ -266,8 +271,8 @@ __global__ void residual_finish_kernel(const double* __restrict__ partial, int c
     b += partial[static_cast<int64_t>(c) * 2 * m + m + j];
   }
   const double rn = sqrt(a);
-  const double xn = sqrt(b);
-  if (mode == 0) {
+  const double xn = sqrt(fmax(b, 0.0));
+  if (mode != 1) {
     xnorm[j] = xn;
     return;
   }
@@ -432,7 +437,9 @@ void residual_norms(const T* AX, const T* X, const T* BX, int64_t ld, int64_t n,
   FE_REQUIRE(n >= 0 && m >= 0, "residual_norms: negative dimension");
   if (m == 0) return;
   FE_REQUIRE(X && ld >= m, "residual_norms: invalid block");
-  if (mode) FE_REQUIRE(AX && lambda, "residual_norms: missing AX or lambda");
+  FE_REQUIRE(mode >= 0 && mode <= 2, "residual_norms: invalid mode");
+  if (mode == 1) FE_REQUIRE(AX && lambda, "residual_norms: missing AX or lambda");
+  if (mode == 2) FE_REQUIRE(BX, "residual_norms: B-norms need BX");
   if (R) FE_REQUIRE(ldr >= m, "residual_norms: invalid R leading dimension");
   FE_REQUIRE(m <= 65535LL * kNormCols, "residual_norms: too many columns");
   const NormPlan p = norm_plan(std::max<int64_t>(n, 1), m);
@@ -639,13 +646,28 @@ namespace {
 template <typename T>
 __global__ void gather_columns_kernel(const T* __restrict__ src, int64_t lds,
                                       const int32_t* __restrict__ idx, int m, T* __restrict__ dst,
-                                      int64_t ldd, int64_t n) {
+                                      int64_t ldd, int64_t n, const double* __restrict__ row_scale) {
   const int64_t total = n * m;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t r = e / m;
     const int j = static_cast<int>(e % m);
-    dst[r * ldd + j] = src[r * lds + idx[j]];
+    const T v = src[r * lds + idx[j]];
+    dst[r * ldd + j] = row_scale ? static_cast<T>(row_scale[r] * static_cast<double>(v)) : v;
+  }
+}
+
+// t[r] = 1 / |A_rr| (1 where the diagonal entry is zero or absent): Jacobi.
+__global__ void jacobi_kernel(int64_t n, const int32_t* __restrict__ rowptr,
+                              const int32_t* __restrict__ colind, const double* __restrict__ val,
+                              double* __restrict__ t) {
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double d = 0.0;
+    for (int32_t p = rowptr[r]; p < rowptr[r + 1]; ++p)
+      if (colind[p] == r) d += val[p];
+    d = fabs(d);
+    t[r] = d > 0.0 ? 1.0 / d : 1.0;
   }
 }
 
@@ -679,17 +701,25 @@ __global__ void mirror_block_kernel(double* P, int64_t ld, int rows, int c0, int
 
 template <typename T>
 void gather_columns(const T* src, int64_t lds, const int32_t* idx, int64_t m, T* dst, int64_t ldd,
-                    int64_t n, cudaStream_t s) {
+                    int64_t n, cudaStream_t s, const double* row_scale) {
   if (n <= 0 || m <= 0) return;
   const int64_t blocks = std::min<int64_t>((n * m + 255) / 256, 148 * 32);
   gather_columns_kernel<T><<<static_cast<unsigned>(blocks), 256, 0, s>>>(
-      src, lds, idx, static_cast<int>(m), dst, ldd, n);
+      src, lds, idx, static_cast<int>(m), dst, ldd, n, row_scale);
   check_launch("gather_columns_kernel");
 }
 template void gather_columns<double>(const double*, int64_t, const int32_t*, int64_t, double*,
-                                     int64_t, int64_t, cudaStream_t);
+                                     int64_t, int64_t, cudaStream_t, const double*);
 template void gather_columns<float>(const float*, int64_t, const int32_t*, int64_t, float*,
-                                    int64_t, int64_t, cudaStream_t);
+                                    int64_t, int64_t, cudaStream_t, const double*);
+
+void jacobi_inverse_diagonal(const Csr& A, double* t, cudaStream_t s) {
+  if (A.rows <= 0) return;
+  const int64_t blocks = std::min<int64_t>((A.rows + 255) / 256, 148 * 16);
+  jacobi_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(A.rows, A.rowptr, A.colind,
+                                                             A.val64, t);
+  check_launch("jacobi_kernel");
+}
 
 void small_gather_scale(const double* src, int64_t lds, int64_t rows, const int32_t* idx,
                         const double* scale, int64_t m, double* dst, int64_t ldd, cudaStream_t s) {

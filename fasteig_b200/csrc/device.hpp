@@ -189,10 +189,46 @@ int read_tc_status(bool clear);
 namespace fe {
 template <typename T>
 void gather_columns(const T* src, int64_t lds, const int32_t* idx, int64_t m, T* dst, int64_t ldd,
-                    int64_t n, cudaStream_t s);
+                    int64_t n, cudaStream_t s, const double* row_scale = nullptr);
+void jacobi_inverse_diagonal(const Csr& A, double* t, cudaStream_t s);
 void small_gather_scale(const double* src, int64_t lds, int64_t rows, const int32_t* idx,
                         const double* scale, int64_t m, double* dst, int64_t ldd, cudaStream_t s);
 void mirror_block(double* P, int64_t ld, int64_t rows, int64_t c0, int64_t cols, cudaStream_t s);
 void to_colmajor(const double* src, int64_t lds, int64_t n, int64_t m, double* dst,
                  cudaStream_t s);
+}  // namespace fe
+
+namespace fe {
+// ---- batched Krylov-Schur (batch_ks.cu) -----------------------------------
+constexpr int kBatchMaxDim = 96;       // largest subspace dimension of the batched engine
+constexpr int kBatchChunkRows = 2048;  // rows per reduction chunk (never crosses problems)
+
+struct BatchLayout {
+  int32_t num_problems = 0, num_chunks = 0;
+  int64_t M = 0;  // leading dimension of the basis rows and of each T / Z / C
+  const int32_t* c_prob = nullptr;
+  const int64_t* c_row0 = nullptr;
+  const int32_t* c_rows = nullptr;
+  const int32_t* p_chunk0 = nullptr;
+  const int32_t* p_nchunks = nullptr;
+};
+
+struct BatchState {
+  int32_t *col = nullptr, *mdim = nullptr, *restart_row = nullptr, *active = nullptr,
+          *status = nullptr;
+  double *beta = nullptr, *inv = nullptr, *beta_next = nullptr, *T = nullptr, *part = nullptr,
+         *part1 = nullptr, *h1 = nullptr, *h2 = nullptr;
+};
+
+void bks_lanczos_step(const BatchLayout& L, const BatchState& S, const Csr& A, double* V,
+                      int64_t ldv, double* f, double* q, double* w, cudaStream_t s);
+void bks_jacobi(const BatchLayout& L, const double* T, const int32_t* mdim, const int32_t* todo,
+                int max_m, double* W, double* Z, cudaStream_t s);
+void bks_rotate(const BatchLayout& L, const double* V, int64_t ldv, const double* C,
+                const int32_t* mdim, const int32_t* keep, int max_m, int max_keep, double* dst,
+                int64_t ldd, cudaStream_t s);
+void bks_residuals(const BatchLayout& L, const int32_t* nev, const double* AY, const double* Y,
+                   int64_t ld, const double* lam, int ldl, double* part, double* rel,
+                   cudaStream_t s);
+void bks_offset_copy(const int32_t* src, int64_t count, int32_t add, int32_t* dst, cudaStream_t s);
 }  // namespace fe

@@ -69,6 +69,7 @@ struct Options {
   std::string init = "host";       // host (std::mt19937, bit-exact) | device
   double mixed_switch = 4.0e-6;    // FP32 -> FP64 switch when max residual <= this
   bool tensor_cores = true;        // FP32 Grams/rotations on tcgen05 (3xTF32)
+  std::string precond = "none";    // none | jacobi (LOBPCG / Davidson corrections W = T R)
 
   void parse(const char* text) {
     if (!text) return;
@@ -136,6 +137,11 @@ struct Options {
     else if (k == "init") init = lower(v);
     else if (k == "mixed_switch") mixed_switch = as_double(v);
     else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
+    else if (k == "precond") {
+      precond = lower(v);
+      if (precond != "none" && precond != "jacobi")
+        throw Error(FE_ERR_INVALID, "precond must be none or jacobi");
+    }
     else if (k == "print_every" || k == "logfile" || k == "output_format" || k == "gpu_backend" ||
              k == "shift" || k == "n") {
       // accepted for deck compatibility; no effect on this backend
@@ -812,7 +818,8 @@ struct RitzResult {
 void ritz_extract(Context& ctx, SmallState& sm, ProjectedEig& eig, double* P, const double* Bm,
                   const double* ABm, int64_t ld, int64_t n, int64_t cols, int64_t req,
                   const std::string& which, double* X, double* AX, double* R, double* coef,
-                  DeviceBuffer& idx_dev, RitzResult& out) {
+                  DeviceBuffer& idx_dev, RitzResult& out, const double* BBm = nullptr,
+                  double* BX = nullptr) {
   cudaStream_t s = ctx.stream;
   symmetrize(P, cols, sm.cap, s);
   eig.run(P, cols, sm.cap, sm.W.as<double>());
@@ -831,8 +838,9 @@ void ritz_extract(Context& ctx, SmallState& sm, ProjectedEig& eig, double* P, co
   small_gather_scale(P, sm.cap, cols, idx_dev.as<int32_t>(), nullptr, req, coef, sm.cap, s);
   rotate_block<double>(sm, Bm, ld, coef, X, ld, n, cols, req, 1.0, 0.0, s);
   rotate_block<double>(sm, ABm, ld, coef, AX, ld, n, cols, req, 1.0, 0.0, s);
+  if (BBm) rotate_block<double>(sm, BBm, ld, coef, BX, ld, n, cols, req, 1.0, 0.0, s);
   ctx.to_device(sm.W.as<double>(), out.values.data(), req);
-  residual_norms<double>(AX, X, nullptr, ld, n, req, sm.W.as<double>(), R, R ? ld : 0,
+  residual_norms<double>(AX, X, BBm ? BX : nullptr, ld, n, req, sm.W.as<double>(), R, R ? ld : 0,
                          sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
                          sm.rws.get(), sm.rws.bytes(), s, 1);
   out.rel.resize(req);
@@ -1147,6 +1155,323 @@ void davidson_solve(const Csr& A, const Options& opt, double* eigenvalues, doubl
   st.fp64_iterations = static_cast<double>(it_done);
 }
 
+// ===========================================================================
+// Extension: generalized K u = l M u and Jacobi-preconditioned LOBPCG / block
+// Davidson (the reference's solvers are standard-only and unpreconditioned,
+// src/LOBPCGSolver.cpp:25-174, src/DavidsonSolver.cpp:27-264). Same loops with
+// every inner product in the B metric (the weighted Gram of the reference's
+// weighted Cholesky QR, src/core/Orthogonalization.cpp:407-440), corrections
+// W = T R with T = diag(|K_ii|)^-1, and the relative residual of
+// evaluate_ritz_pairs with B (src/core/RitzExtraction.cpp:50-56). B absent means
+// M = I (B-blocks are then copies).
+// ===========================================================================
+struct GenBlockOps {
+  Context& ctx;
+  SmallState& sm;
+  ProjectedEig& eig;
+  const Csr& A;
+  const Csr* B;
+  double sign;
+  int64_t n, ld;
+  Stats& st;
+  DeviceBuffer idx_dev;
+
+  void bapply(const double* X, double* BX, int64_t cols) {
+    if (cols <= 0) return;
+    if (B) {
+      csr_spmm<double>(*B, X, ld, BX, ld, nullptr, 0, cols, 1.0, 0.0, 0.0, ctx.stream);
+      st.spmm_launches += 1;
+    } else {
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(BX, ld * 8, X, ld * 8, cols * 8, n,
+                                      cudaMemcpyDeviceToDevice, ctx.stream));
+    }
+  }
+  void happly(const double* X, double* AX, int64_t cols) {
+    if (cols <= 0) return;
+    csr_spmm<double>(A, X, ld, AX, ld, nullptr, 0, cols, sign, 0.0, 0.0, ctx.stream);
+    st.spmm_launches += 1;
+  }
+  void copy(double* dst, const double* src, int64_t cols) {
+    if (cols <= 0 || dst == src) return;
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(dst, ld * 8, src, ld * 8, cols * 8, n,
+                                    cudaMemcpyDeviceToDevice, ctx.stream));
+  }
+
+  // B-orthonormal basis of the part of src (cols columns) outside span(V[:, :k]),
+  // V B-orthonormal with BV = B V: two passes of B-norms -> two-pass block
+  // Gram-Schmidt in the B metric -> B-Gram eigen-decomposition -> keep singular
+  // values above max(rank_tol * largest B-norm, 1e-7 * largest) -> rotate by
+  // U S^-1 (orthonormalize_block, src/core/Orthogonalization.cpp:717-775, in the B
+  // metric). Writes out/Bout[:, :rank] (may alias src; tmp/tmpB are scratch).
+  int64_t ortho(const double* V, const double* BV, int64_t k, const double* src, int64_t cols,
+                double* out, double* Bout, double* tmp, double* tmpB, double rank_tol = 1e-12) {
+    cudaStream_t s = ctx.stream;
+    if (k >= n || cols <= 0) return 0;
+    const double* cur = src;
+    int64_t rank = 0;
+    std::vector<double> norms, w, inv;
+    for (int pass = 0; pass < 2; ++pass) {
+      bapply(cur, tmpB, cols);
+      residual_norms<double>(nullptr, cur, tmpB, ld, n, cols, nullptr, nullptr, 0, nullptr,
+                             sm.xnorm.as<double>(), nullptr, sm.rws.get(), sm.rws.bytes(), s, 2);
+      norms.resize(cols);
+      ctx.to_host(norms.data(), sm.xnorm.as<double>(), cols);
+      ctx.sync();
+      double scale = 0.0;
+      for (double v : norms) {
+        if (!std::isfinite(v))
+          throw Error(FE_ERR_NONFINITE, "orthonormalize_block: non-finite column norms.");
+        scale = std::max(scale, v);
+      }
+      if (scale == 0.0) return 0;
+      copy(tmp, cur, cols);
+      double* G = sm.G.as<double>();
+      if (k > 0) {
+        for (int g = 0; g < 2; ++g) {
+          gram_block<double>(sm, V, ld, tmpB, ld, n, k, cols, G, s);
+          rotate_block<double>(sm, V, ld, G, tmp, ld, n, k, cols, -1.0, 1.0, s);
+          rotate_block<double>(sm, BV, ld, G, tmpB, ld, n, k, cols, -1.0, 1.0, s);
+        }
+      }
+      gram_block<double>(sm, tmp, ld, tmpB, ld, n, cols, cols, G, s);
+      symmetrize(G, cols, sm.cap, s);
+      eig.run(G, cols, sm.cap, sm.W.as<double>());
+      w.resize(cols);
+      ctx.to_host(w.data(), sm.W.as<double>(), cols);
+      ctx.sync();
+      const double smax = std::sqrt(std::max(w[cols - 1], 0.0));
+      const int64_t capacity = std::min<int64_t>(cols, n - k);
+      const double cut = std::max(rank_tol * scale, 1e-7 * smax);
+      std::vector<int32_t> sel;
+      inv.clear();
+      for (int64_t i = cols - 1; i >= 0 && static_cast<int64_t>(sel.size()) < capacity; --i) {
+        const double sv = std::sqrt(std::max(w[i], 0.0));
+        if (!(sv > cut)) break;
+        sel.push_back(static_cast<int32_t>(i));
+        inv.push_back(1.0 / sv);
+      }
+      rank = static_cast<int64_t>(sel.size());
+      if (rank == 0) return 0;
+      const size_t dbl_off = ((rank * sizeof(int32_t) + 7) / 8) * 8;
+      idx_dev.resize(dbl_off + rank * sizeof(double));
+      int32_t* di = idx_dev.as<int32_t>();
+      double* ds = reinterpret_cast<double*>(idx_dev.as<uint8_t>() + dbl_off);
+      ctx.to_device(di, sel.data(), rank);
+      ctx.to_device(ds, inv.data(), rank);
+      small_gather_scale(G, sm.cap, cols, di, ds, rank, sm.Rinv.as<double>(), sm.cap, s);
+      rotate_block<double>(sm, tmp, ld, sm.Rinv.as<double>(), out, ld, n, cols, rank, 1.0, 0.0, s);
+      rotate_block<double>(sm, tmpB, ld, sm.Rinv.as<double>(), Bout, ld, n, cols, rank, 1.0, 0.0,
+                           s);
+      cur = out;
+      cols = rank;
+      ctx.sync();
+    }
+    return rank;
+  }
+
+  // Weighted Cholesky QR with a fresh BX: X <- X R^-1, BX <- B X R^-1 (through tmp/tmpB).
+  void bcholqr(double* X, double* BX, int64_t b, double* tmp, double* tmpB, const char* what) {
+    cudaStream_t s = ctx.stream;
+    bapply(X, BX, b);
+    double* G = sm.G.as<double>();
+    gram_block<double>(sm, X, ld, BX, ld, n, b, b, G, s);
+    symmetrize(G, b, sm.cap, s);
+    FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, sizeof(int32_t), s));
+    potrf_upper(G, b, sm.cap, sm.info.as<int32_t>(), s);
+    int32_t info = 0;
+    ctx.to_host(&info, sm.info.as<int32_t>(), 1);
+    ctx.sync();
+    if (info != 0) throw Error(FE_ERR_NOT_SPD, std::string(what) + ": weighted QR failed.");
+    trinv_upper(G, sm.cap, sm.Rinv.as<double>(), sm.cap, b, s);
+    rotate_block<double>(sm, X, ld, sm.Rinv.as<double>(), tmp, ld, n, b, b, 1.0, 0.0, s);
+    rotate_block<double>(sm, BX, ld, sm.Rinv.as<double>(), tmpB, ld, n, b, b, 1.0, 0.0, s);
+    copy(X, tmp, b);
+    copy(BX, tmpB, b);
+  }
+};
+
+void lobpcg_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* eigenvalues,
+                      double* residuals, double* eigenvectors, Stats& st) {
+  const int64_t n = A.rows, nev = opt.nev;
+  if (n <= 0 || nev <= 0 || nev > n || opt.maxiter <= 0)
+    throw Error(FE_ERR_INVALID, "LOBPCGSolver: require 0 < nev <= n and maxiter > 0.");
+  if (opt.which != "sr" && opt.which != "lr")
+    throw Error(FE_ERR_INVALID, "LOBPCGSolver: only SR and LR are supported.");
+  const int64_t b = std::min<int64_t>(n, std::max<int64_t>(nev, opt.block));
+  const double sign = opt.which == "lr" ? -1.0 : 1.0;
+  const double tol = opt.tol;
+  const int64_t cap = std::min<int64_t>(n, 3 * b);
+  Context ctx;
+  cudaStream_t s = ctx.stream;
+  SmallState sm;
+  sm.allocate(n, cap, false);
+  ProjectedEig eig(ctx, cap);
+  Block<double> X, AX, BX, R, Pd, S, AS, BS, T1, T2, Wsrc;
+  for (Block<double>* q : {&X, &AX, &BX, &R, &Pd, &S, &AS, &BS, &T1, &T2, &Wsrc})
+    q->allocate(n, cap);
+  const int64_t ld = X.ld;
+  GenBlockOps g{ctx, sm, eig, A, B, sign, n, ld, st, DeviceBuffer(64)};
+  DeviceBuffer tdiag, act(static_cast<size_t>(cap) * sizeof(int32_t) + 16),
+      coef(static_cast<size_t>(cap) * cap * sizeof(double));
+  const double* t = nullptr;
+  if (opt.precond == "jacobi") {
+    tdiag.resize(n * sizeof(double));
+    jacobi_inverse_diagonal(A, tdiag.as<double>(), s);
+    t = tdiag.as<double>();
+  }
+  fill_initial_block(ctx, X.data(), ld, n, b, opt.seed_or_default(), opt.init == "host");
+  if (g.ortho(nullptr, nullptr, 0, X.data(), b, X.data(), BX.data(), T1.data(), T2.data()) < b)
+    throw Error(FE_ERR_NOT_SPD, "LOBPCGSolver: initial block is rank deficient.");
+  g.happly(X.data(), AX.data(), b);
+  g.copy(S.data(), X.data(), b);
+  g.copy(AS.data(), AX.data(), b);
+  g.copy(BS.data(), BX.data(), b);
+  gram_block<double>(sm, S.data(), ld, AS.data(), ld, n, b, b, sm.G.as<double>(), s);
+  RitzResult ritz;
+  ritz_extract(ctx, sm, eig, sm.G.as<double>(), S.data(), AS.data(), ld, n, b, b, "sr", X.data(),
+               AX.data(), R.data(), coef.as<double>(), g.idx_dev, ritz, BS.data(), BX.data());
+  auto worst_nev = [&] {
+    double w = 0;
+    for (int64_t j = 0; j < nev; ++j) w = std::max(w, ritz.rel[j]);
+    return w;
+  };
+  bool have_p = false;
+  int64_t it_done = 0;
+  for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
+    if (worst_nev() <= tol) break;
+    std::vector<int32_t> active;
+    for (int64_t j = 0; j < b; ++j)
+      if (ritz.rel[j] > tol) active.push_back(static_cast<int32_t>(j));
+    const int64_t na = static_cast<int64_t>(active.size());
+    ctx.to_device(act.as<int32_t>(), active.data(), na);
+    gather_columns<double>(R.data(), ld, act.as<int32_t>(), na, Wsrc.data(), ld, n, s, t);
+    g.bcholqr(X.data(), BX.data(), b, T1.data(), T2.data(), "LOBPCGSolver: Ritz-vector");
+    g.copy(S.data(), X.data(), b);
+    g.copy(BS.data(), BX.data(), b);
+    int64_t cols = b;
+    int64_t rw = g.ortho(S.data(), BS.data(), cols, Wsrc.data(), na, S.col(cols), BS.col(cols),
+                         T1.data(), T2.data());
+    cols += std::min(rw, cap - cols);
+    if (have_p && cols < cap) {
+      gather_columns<double>(Pd.data(), ld, act.as<int32_t>(), na, Wsrc.data(), ld, n, s);
+      const int64_t rp = g.ortho(S.data(), BS.data(), cols, Wsrc.data(), na, S.col(cols),
+                                 BS.col(cols), T1.data(), T2.data());
+      cols += std::min(rp, cap - cols);
+    }
+    g.happly(S.data(), AS.data(), cols);
+    gram_block<double>(sm, S.data(), ld, AS.data(), ld, n, cols, cols, sm.G.as<double>(), s);
+    ritz_extract(ctx, sm, eig, sm.G.as<double>(), S.data(), AS.data(), ld, n, cols, b, "sr",
+                 X.data(), AX.data(), R.data(), coef.as<double>(), g.idx_dev, ritz, BS.data(),
+                 BX.data());
+    // P = S C with the X rows of C zeroed.
+    FE_CHECK_CUDA(cudaMemset2DAsync(coef.get(), cap * 8, 0, b * 8, b, s));
+    rotate_block<double>(sm, S.data(), ld, coef.as<double>(), Pd.data(), ld, n, cols, b, 1.0, 0.0,
+                         s);
+    have_p = true;
+    it_done = iter + 1;
+    if (opt.verbosity >= 2)
+      std::fprintf(stderr, "[fe] lobpcg-g iter %lld cols %lld worst %.3e\n",
+                   static_cast<long long>(iter + 1), static_cast<long long>(cols), worst_nev());
+    if (worst_nev() <= tol || cols == b) break;
+  }
+  for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = sign * ritz.values[j];
+  finish_results(ctx, sm, A, B, X.data(), ld, n, nev, eigenvalues, residuals, eigenvectors);
+  st.iterations = static_cast<double>(it_done);
+  st.fp64_iterations = static_cast<double>(it_done);
+}
+
+void davidson_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* eigenvalues,
+                        double* residuals, double* eigenvectors, Stats& st) {
+  const int64_t n = A.rows, nev = opt.nev;
+  if (n <= 0) throw Error(FE_ERR_INVALID, "DavidsonSolver: n must be > 0.");
+  if (nev <= 0 || nev > n) throw Error(FE_ERR_INVALID, "DavidsonSolver: nev must be in [1,n].");
+  if (opt.maxiter <= 0) throw Error(FE_ERR_INVALID, "DavidsonSolver: maxiter must be > 0.");
+  if (opt.maxblks < 1) throw Error(FE_ERR_INVALID, "DavidsonSolver: maxblks must be at least 1.");
+  const std::string which = opt.which;
+  if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
+    throw Error(FE_ERR_INVALID, "DavidsonSolver: invalid which option (use SR/LR/SM/LM/BE).");
+  const double tol = opt.tol;
+  const int64_t cap = std::min<int64_t>(n, opt.maxblks * nev);
+  Context ctx;
+  cudaStream_t s = ctx.stream;
+  SmallState sm;
+  sm.allocate(n, cap, false);
+  ProjectedEig eig(ctx, cap);
+  Block<double> V, AV, BV, X, AX, BX, R, T1, T2, Wsrc;
+  for (Block<double>* q : {&V, &AV, &BV, &X, &AX, &BX, &R, &T1, &T2, &Wsrc}) q->allocate(n, cap);
+  const int64_t ld = V.ld;
+  GenBlockOps g{ctx, sm, eig, A, B, 1.0, n, ld, st, DeviceBuffer(64)};
+  DeviceBuffer tdiag, act(static_cast<size_t>(cap) * sizeof(int32_t) + 16),
+      coef(static_cast<size_t>(cap) * cap * sizeof(double)),
+      proj(static_cast<size_t>(cap) * cap * sizeof(double));
+  const double* t = nullptr;
+  if (opt.precond == "jacobi") {
+    tdiag.resize(n * sizeof(double));
+    jacobi_inverse_diagonal(A, tdiag.as<double>(), s);
+    t = tdiag.as<double>();
+  }
+  double* Pm = proj.as<double>();
+  double* Pw = sm.G.as<double>();
+  RitzResult ritz;
+  auto extract = [&](int64_t cols) {
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(Pw, cap * 8, Pm, cap * 8, cols * 8, cols,
+                                    cudaMemcpyDeviceToDevice, s));
+    ritz_extract(ctx, sm, eig, Pw, V.data(), AV.data(), ld, n, cols, nev, which, X.data(),
+                 AX.data(), R.data(), coef.as<double>(), g.idx_dev, ritz, BV.data(), BX.data());
+  };
+  fill_initial_block(ctx, X.data(), ld, n, nev, opt.seed_or_default(), opt.init == "host");
+  if (g.ortho(nullptr, nullptr, 0, X.data(), nev, X.data(), BX.data(), T1.data(), T2.data()) < nev)
+    throw Error(FE_ERR_NOT_SPD, "DavidsonSolver: initial block is rank deficient.");
+  g.copy(V.data(), X.data(), nev);
+  g.copy(BV.data(), BX.data(), nev);
+  g.happly(V.data(), AV.data(), nev);
+  gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, nev, nev, Pm, s);
+  extract(nev);
+  const double locktol = std::min(1.0e-5, tol);
+  int64_t it_done = 0;
+  for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
+    g.bcholqr(X.data(), BX.data(), nev, T1.data(), T2.data(), "DavidsonSolver: restart");
+    g.copy(V.data(), X.data(), nev);
+    g.copy(BV.data(), BX.data(), nev);
+    g.happly(V.data(), AV.data(), nev);
+    FE_CHECK_CUDA(cudaMemset2DAsync(Pm, cap * 8, 0, cap * 8, cap, s));
+    gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, nev, nev, Pm, s);
+    int64_t cols = nev;
+    extract(cols);
+    for (int64_t blk = 1; blk < opt.maxblks; ++blk) {
+      std::vector<int32_t> active;
+      for (int64_t j = 0; j < nev; ++j)
+        if (ritz.rel[j] > locktol) active.push_back(static_cast<int32_t>(j));
+      const int64_t cc = static_cast<int64_t>(active.size());
+      if (cc == 0 || cols + cc > cap) break;
+      ctx.to_device(act.as<int32_t>(), active.data(), cc);
+      gather_columns<double>(R.data(), ld, act.as<int32_t>(), cc, Wsrc.data(), ld, n, s, t);
+      const int64_t r = g.ortho(V.data(), BV.data(), cols, Wsrc.data(), cc, V.col(cols),
+                                BV.col(cols), T1.data(), T2.data());
+      if (r == 0) break;
+      g.happly(V.col(cols), AV.col(cols), r);
+      // projected[:cols, cols:cols+r] = V^T A W, mirrored; diagonal block W^T A W.
+      gram_block<double>(sm, V.data(), ld, AV.col(cols), ld, n, cols, r, Pm + cols * cap, s);
+      gram_block<double>(sm, V.col(cols), ld, AV.col(cols), ld, n, r, r, Pm + cols * cap + cols,
+                         s);
+      mirror_block(Pm, cap, cols, cols, r, s);
+      cols += r;
+      extract(cols);
+    }
+    it_done = iter + 1;
+    double worst = 0;
+    for (double v : ritz.rel) worst = std::max(worst, v);
+    if (opt.verbosity >= 2)
+      std::fprintf(stderr, "[fe] davidson-g iter %lld cols %lld worst %.3e\n",
+                   static_cast<long long>(iter + 1), static_cast<long long>(cols), worst);
+    if (!ritz.rel.empty() && worst < tol) break;
+  }
+  for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = ritz.values[j];
+  finish_results(ctx, sm, A, B, X.data(), ld, n, nev, eigenvalues, residuals, eigenvectors);
+  st.iterations = static_cast<double>(it_done);
+  st.fp64_iterations = static_cast<double>(it_done);
+}
+
 // KrylovSchurSolver::solve (src/KrylovSchurSolver.cpp:28-160) for standard problems:
 // scalar Lanczos with two-pass classical reorthogonalization (KrylovSubspace,
 // src/core/KrylovSubspace.cpp:125-259) on the device, the m x m projected
@@ -1330,8 +1655,330 @@ void krylov_schur_solve(const Csr& A, const Options& opt, double* eigenvalues, d
   throw Error(FE_ERR_INVALID, "KrylovSchurSolver: unreachable solve termination.");
 }
 
+// ===========================================================================
+// Batched Krylov-Schur (extension): many independent standard problems, each
+// following KrylovSchurSolver::solve (src/KrylovSchurSolver.cpp:28-160) with the
+// Lanczos expansion of KrylovSubspace (src/core/KrylovSubspace.cpp:125-259), run
+// in lockstep on the grouped kernels of batch_ks.cu. One Lanczos step of the
+// whole batch is a captured CUDA graph; the host only acts once per restart
+// round (selection, convergence, restart bookkeeping), exactly as the single
+// solver does per problem.
+// ===========================================================================
+struct BatchStats {
+  double seconds = 0, rounds = 0, steps = 0, graph_launches = 0;
+};
+
+void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int64_t>& nevs,
+                        const Options& opt, double* eigenvalues, double* residuals,
+                        double* eigenvectors, int32_t* iterations, int32_t* status,
+                        BatchStats& bs) {
+  const int32_t P = static_cast<int32_t>(As.size());
+  if (P <= 0) throw Error(FE_ERR_INVALID, "batch: no problems.");
+  const std::string which = opt.which;
+  if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
+    throw Error(FE_ERR_INVALID, "KrylovSchurSolver: invalid which option (use SR/LR/SM/LM/BE/SAI).");
+  if (opt.maxiter <= 0) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: maxiter must be > 0.");
+  const double tol = opt.tol;
+  const int device = As[0]->device;
+  std::vector<int64_t> n(P), m(P), row0(P + 1, 0), nz0(P + 1, 0);
+  int max_m = 0, max_nev = 0;
+  int64_t max_row_nnz = 0;
+  for (int32_t p = 0; p < P; ++p) {
+    const Csr& A = *As[p];
+    FE_REQUIRE(A.device == device, "batch: all problems must live on one device.");
+    FE_REQUIRE(A.rows == A.cols && A.rows > 0, "batch: problems must be square and non-empty.");
+    n[p] = A.rows;
+    if (nevs[p] <= 0 || nevs[p] > n[p])
+      throw Error(FE_ERR_INVALID, "KrylovSchurSolver: nev must be in [1,n].");
+    m[p] = std::min<int64_t>(std::max<int64_t>({2 * nevs[p], 20, opt.maxdim}), n[p]);
+    FE_REQUIRE(m[p] <= kBatchMaxDim, "batch: subspace dimension above " +
+                                         std::to_string(kBatchMaxDim) +
+                                         " (use the single-problem solver).");
+    max_m = std::max<int>(max_m, static_cast<int>(m[p]));
+    max_nev = std::max<int>(max_nev, static_cast<int>(nevs[p]));
+    max_row_nnz = std::max(max_row_nnz, A.max_row_nnz);
+    row0[p + 1] = row0[p] + n[p];
+    nz0[p + 1] = nz0[p] + A.nnz;
+  }
+  const int64_t N = row0[P];
+  FE_REQUIRE(N < INT32_MAX && nz0[P] < INT32_MAX, "batch: more than 2^31 rows or nonzeros.");
+  const int64_t M = std::max<int64_t>(8, ((max_m + 7) / 8) * 8);
+  const int64_t ldy = std::max<int64_t>(8, ((max_nev + 7) / 8) * 8);
+  Context ctx;
+  cudaStream_t s = ctx.stream;
+  // Block-diagonal CSR of all problems.
+  DeviceBuffer rp((N + 1) * sizeof(int32_t)), ci(std::max<int64_t>(nz0[P], 1) * sizeof(int32_t)),
+      va(std::max<int64_t>(nz0[P], 1) * sizeof(double));
+  for (int32_t p = 0; p < P; ++p) {
+    const Csr& A = *As[p];
+    bks_offset_copy(A.rowptr, n[p], static_cast<int32_t>(nz0[p]), rp.as<int32_t>() + row0[p], s);
+    bks_offset_copy(A.colind, A.nnz, static_cast<int32_t>(row0[p]), ci.as<int32_t>() + nz0[p], s);
+    if (A.nnz > 0)
+      FE_CHECK_CUDA(cudaMemcpyAsync(va.as<double>() + nz0[p], A.val64, A.nnz * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, s));
+  }
+  {
+    const int32_t last = static_cast<int32_t>(nz0[P]);
+    ctx.to_device(rp.as<int32_t>() + N, &last, 1);
+  }
+  Csr Aall;
+  Aall.rows = Aall.cols = N;
+  Aall.nnz = nz0[P];
+  Aall.rowptr = rp.as<int32_t>();
+  Aall.colind = ci.as<int32_t>();
+  Aall.val64 = va.as<double>();
+  Aall.device = device;
+  Aall.max_row_nnz = max_row_nnz;
+  // Reduction chunks.
+  std::vector<int32_t> c_prob, c_rows, p_chunk0(P), p_nchunks(P);
+  std::vector<int64_t> c_row0;
+  for (int32_t p = 0; p < P; ++p) {
+    p_chunk0[p] = static_cast<int32_t>(c_prob.size());
+    for (int64_t r = 0; r < n[p]; r += kBatchChunkRows) {
+      c_prob.push_back(p);
+      c_row0.push_back(row0[p] + r);
+      c_rows.push_back(static_cast<int32_t>(std::min<int64_t>(kBatchChunkRows, n[p] - r)));
+    }
+    p_nchunks[p] = static_cast<int32_t>(c_prob.size()) - p_chunk0[p];
+  }
+  const int32_t NC = static_cast<int32_t>(c_prob.size());
+  DeviceBuffer d_cprob(NC * 4), d_crow0(NC * 8), d_crows(NC * 4), d_pc0(P * 4), d_pnc(P * 4);
+  ctx.to_device(d_cprob.as<int32_t>(), c_prob.data(), NC);
+  ctx.to_device(d_crow0.as<int64_t>(), c_row0.data(), NC);
+  ctx.to_device(d_crows.as<int32_t>(), c_rows.data(), NC);
+  ctx.to_device(d_pc0.as<int32_t>(), p_chunk0.data(), P);
+  ctx.to_device(d_pnc.as<int32_t>(), p_nchunks.data(), P);
+  BatchLayout L;
+  L.num_problems = P;
+  L.num_chunks = NC;
+  L.M = M;
+  L.c_prob = d_cprob.as<int32_t>();
+  L.c_row0 = d_crow0.as<int64_t>();
+  L.c_rows = d_crows.as<int32_t>();
+  L.p_chunk0 = d_pc0.as<int32_t>();
+  L.p_nchunks = d_pnc.as<int32_t>();
+  // Blocks and per-problem state.
+  DeviceBuffer V(static_cast<size_t>(N) * M * 8), f(N * 8), q(N * 8), w(N * 8);
+  DeviceBuffer d_col(P * 4), d_m(P * 4), d_rr(P * 4), d_act(P * 4), d_status(P * 4), d_beta(P * 8),
+      d_inv(P * 8), d_bn(P * 8), d_T(static_cast<size_t>(P) * M * M * 8),
+      d_part(static_cast<size_t>(NC) * M * 8), d_part1(NC * 8), d_h1(P * M * 8), d_h2(P * M * 8),
+      d_W(P * M * 8), d_Z(static_cast<size_t>(P) * M * M * 8), d_C(static_cast<size_t>(P) * M * M * 8),
+      d_todo(P * 4), d_keep(P * 4), d_keepY(P * 4);
+  BatchState S;
+  S.col = d_col.as<int32_t>();
+  S.mdim = d_m.as<int32_t>();
+  S.restart_row = d_rr.as<int32_t>();
+  S.active = d_act.as<int32_t>();
+  S.status = d_status.as<int32_t>();
+  S.beta = d_beta.as<double>();
+  S.inv = d_inv.as<double>();
+  S.beta_next = d_bn.as<double>();
+  S.T = d_T.as<double>();
+  S.part = d_part.as<double>();
+  S.part1 = d_part1.as<double>();
+  S.h1 = d_h1.as<double>();
+  S.h2 = d_h2.as<double>();
+  std::vector<int32_t> h_col(P, 0), h_m(P), h_rr(P, -1), h_act(P, 1), h_status(P, 0);
+  for (int32_t p = 0; p < P; ++p) h_m[p] = static_cast<int32_t>(m[p]);
+  std::vector<double> h_T(static_cast<size_t>(P) * M * M, 0.0);
+  auto upload_state = [&] {
+    ctx.to_device(S.col, h_col.data(), P);
+    ctx.to_device(S.restart_row, h_rr.data(), P);
+    ctx.to_device(S.active, h_act.data(), P);
+    ctx.to_device(S.T, h_T.data(), h_T.size());
+  };
+  ctx.to_device(S.mdim, h_m.data(), P);
+  ctx.to_device(S.status, h_status.data(), P);
+  upload_state();
+  // Starting vectors: each problem's own seeded draw (the single solver's
+  // random_into(f, seed)), so a problem starts identically alone or batched.
+  const unsigned seed = opt.seed_or_default();
+  if (opt.init == "host") {
+    std::vector<double> hf(N);
+    for (int32_t p = 0; p < P; ++p) {
+      std::mt19937 rng(seed);
+      std::uniform_real_distribution<double> dist(-1.0, 1.0);
+      for (int64_t i = 0; i < n[p]; ++i) hf[row0[p] + i] = dist(rng);
+    }
+    ctx.to_device(f.as<double>(), hf.data(), N);
+  } else {
+    for (int32_t p = 0; p < P; ++p) fill_uniform<double>(f.as<double>() + row0[p], 1, n[p], 1, seed, s);
+  }
+  FE_CHECK_CUDA(cudaMemsetAsync(V.get(), 0, V.bytes(), s));
+  ctx.sync();
+  // One Lanczos step of the whole batch as a CUDA graph.
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  FE_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  try {
+    bks_lanczos_step(L, S, Aall, V.as<double>(), M, f.as<double>(), q.as<double>(), w.as<double>(), s);
+  } catch (...) {
+    cudaStreamEndCapture(s, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  FE_CHECK_CUDA(cudaStreamEndCapture(s, &graph));
+  struct GraphGuard {
+    cudaGraph_t g;
+    cudaGraphExec_t* e;
+    ~GraphGuard() {
+      if (*e) cudaGraphExecDestroy(*e);
+      if (g) cudaGraphDestroy(g);
+    }
+  } guard{graph, &exec};
+  FE_CHECK_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<char> finished(P, 0);
+  std::vector<double> lam_final(static_cast<size_t>(P) * ldy, 0.0);
+  std::vector<int32_t> keep(P, 0), keepY(P, 0), todo(P, 0), nev32(P);
+  for (int32_t p = 0; p < P; ++p) nev32[p] = static_cast<int32_t>(nevs[p]);
+  std::vector<double> hW(static_cast<size_t>(P) * M), hZ(static_cast<size_t>(P) * M * M),
+      hC(static_cast<size_t>(P) * M * M, 0.0), hbn(P);
+  DeviceBuffer Y(static_cast<size_t>(N) * ldy * 8);
+  FE_CHECK_CUDA(cudaMemsetAsync(Y.get(), 0, Y.bytes(), s));
+  int64_t steps_needed = max_m;
+  for (int64_t iter = 1;; ++iter) {
+    for (int64_t k = 0; k < steps_needed; ++k) FE_CHECK_CUDA(cudaGraphLaunch(exec, s));
+    bs.steps += static_cast<double>(steps_needed);
+    bs.graph_launches += static_cast<double>(steps_needed);
+    bs.rounds += 1;
+    ctx.to_host(h_status.data(), S.status, P);
+    ctx.sync();
+    for (int32_t p = 0; p < P; ++p) {
+      if (finished[p]) continue;
+      if (h_status[p] == 2)
+        throw Error(FE_ERR_NONFINITE,
+                    "core::KrylovSubspace: breakdown in batched problem " + std::to_string(p) +
+                        " (solve it alone for the randomized restart).");
+      if (h_status[p] != 0)
+        throw Error(FE_ERR_NONFINITE, "core::KrylovSubspace: non-finite residual norm encountered.");
+      todo[p] = 1;
+    }
+    ctx.to_device(d_todo.as<int32_t>(), todo.data(), P);
+    bks_jacobi(L, S.T, S.mdim, d_todo.as<int32_t>(), max_m, d_W.as<double>(), d_Z.as<double>(), s);
+    ctx.to_host(hW.data(), d_W.as<double>(), hW.size());
+    ctx.to_host(hZ.data(), d_Z.as<double>(), hZ.size());
+    ctx.to_host(hbn.data(), S.beta_next, P);
+    ctx.sync();
+    int max_keep = 0, max_keepY = 0;
+    bool any_active = false;
+    for (int32_t p = 0; p < P; ++p) {
+      keep[p] = keepY[p] = 0;
+      h_act[p] = 0;
+      if (finished[p]) continue;
+      todo[p] = 0;
+      const int64_t mp = m[p], nev = nevs[p];
+      std::vector<double> lam(hW.begin() + static_cast<int64_t>(p) * M,
+                              hW.begin() + static_cast<int64_t>(p) * M + mp);
+      const double* Zp = hZ.data() + static_cast<size_t>(p) * M * M;
+      const std::vector<int32_t> idx = select_indices(lam, which);
+      std::vector<double> lam_s(mp), rel_s(mp);
+      for (int64_t j = 0; j < mp; ++j) {
+        lam_s[j] = lam[idx[j]];
+        rel_s[j] = std::fabs(hbn[p] * Zp[static_cast<size_t>(idx[j]) * M + mp - 1]) /
+                   (1.0 + std::fabs(lam_s[j]));
+      }
+      int64_t nconv = 0;
+      for (int64_t j = 0; j < nev; ++j) {
+        const double mag = std::fabs(lam_s[j]);
+        if (rel_s[j] * (1.0 + mag) < tol * mag) ++nconv;
+      }
+      const bool at_limit = (mp == n[p]) || (iter == opt.maxiter);
+      double* Cp = hC.data() + static_cast<size_t>(p) * M * M;
+      if (nconv >= nev || at_limit) {
+        for (int64_t j = 0; j < nev; ++j) {
+          std::memcpy(Cp + j * M, Zp + static_cast<size_t>(idx[j]) * M, mp * sizeof(double));
+          lam_final[static_cast<size_t>(p) * ldy + j] = lam_s[j];
+        }
+        keepY[p] = static_cast<int32_t>(nev);
+        max_keepY = std::max<int>(max_keepY, static_cast<int>(nev));
+        iterations[p] = static_cast<int32_t>(iter);
+        status[p] = 0;
+        finished[p] = 1;
+        continue;
+      }
+      const int64_t spare = (mp - nev) / 2;
+      int64_t retained = nev + std::min(nconv, spare);
+      if (retained == 1 && mp > 3) retained = mp / 2;
+      for (int64_t j = 0; j < retained; ++j)
+        std::memcpy(Cp + j * M, Zp + static_cast<size_t>(idx[j]) * M, mp * sizeof(double));
+      keep[p] = static_cast<int32_t>(retained);
+      max_keep = std::max<int>(max_keep, static_cast<int>(retained));
+      double* Tp = h_T.data() + static_cast<size_t>(p) * M * M;
+      std::fill(Tp, Tp + M * M, 0.0);
+      for (int64_t j = 0; j < retained; ++j) {
+        Tp[j + j * M] = lam_s[j];
+        const double coupling = hbn[p] * Zp[static_cast<size_t>(idx[j]) * M + mp - 1];
+        Tp[retained + j * M] = coupling;
+        Tp[j + retained * M] = coupling;
+      }
+      h_col[p] = static_cast<int32_t>(retained);
+      h_rr[p] = static_cast<int32_t>(retained);
+      h_act[p] = 1;
+      any_active = true;
+    }
+    ctx.to_device(d_C.as<double>(), hC.data(), hC.size());
+    ctx.to_device(d_keep.as<int32_t>(), keep.data(), P);
+    ctx.to_device(d_keepY.as<int32_t>(), keepY.data(), P);
+    // Finishing problems: Ritz vectors into Y; restarting problems: V[:, :retained] = V C.
+    bks_rotate(L, V.as<double>(), M, d_C.as<double>(), S.mdim, d_keepY.as<int32_t>(), max_m,
+               max_keepY, Y.as<double>(), ldy, s);
+    bks_rotate(L, V.as<double>(), M, d_C.as<double>(), S.mdim, d_keep.as<int32_t>(), max_m,
+               max_keep, V.as<double>(), M, s);
+    if (!any_active) break;
+    upload_state();
+    steps_needed = 0;
+    for (int32_t p = 0; p < P; ++p)
+      if (h_act[p]) steps_needed = std::max<int64_t>(steps_needed, m[p] - h_col[p]);
+  }
+  // Final Ritz residuals on the device (evaluate_ritz_pairs, src/core/RitzExtraction.cpp:34-63).
+  DeviceBuffer AY(static_cast<size_t>(N) * ldy * 8), d_lam(static_cast<size_t>(P) * ldy * 8),
+      d_rel(static_cast<size_t>(P) * ldy * 8), d_nev(P * 4),
+      d_rpart(static_cast<size_t>(NC) * 2 * ldy * 8);
+  ctx.to_device(d_lam.as<double>(), lam_final.data(), lam_final.size());
+  ctx.to_device(d_nev.as<int32_t>(), nev32.data(), P);
+  csr_spmm<double>(Aall, Y.as<double>(), ldy, AY.as<double>(), ldy, nullptr, 0, max_nev, 1.0, 0.0,
+                   0.0, s);
+  bks_residuals(L, d_nev.as<int32_t>(), AY.as<double>(), Y.as<double>(), ldy, d_lam.as<double>(),
+                static_cast<int>(ldy), d_rpart.as<double>(), d_rel.as<double>(), s);
+  std::vector<double> rel(static_cast<size_t>(P) * ldy);
+  ctx.to_host(rel.data(), d_rel.as<double>(), rel.size());
+  std::vector<double> hY;
+  if (eigenvectors) {
+    hY.resize(static_cast<size_t>(N) * ldy);
+    ctx.to_host(hY.data(), Y.as<double>(), hY.size());
+  }
+  ctx.sync();
+  bs.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  int64_t off = 0, voff = 0;
+  for (int32_t p = 0; p < P; ++p) {
+    for (int64_t j = 0; j < nevs[p]; ++j) {
+      eigenvalues[off + j] = lam_final[static_cast<size_t>(p) * ldy + j];
+      residuals[off + j] = rel[static_cast<size_t>(p) * ldy + j];
+      if (!std::isfinite(residuals[off + j]))
+        throw Error(FE_ERR_NONFINITE, "evaluate_ritz_pairs: invalid vector or non-finite residual.");
+    }
+    if (eigenvectors) {
+      for (int64_t j = 0; j < nevs[p]; ++j)
+        for (int64_t i = 0; i < n[p]; ++i)
+          eigenvectors[voff + j * n[p] + i] = hY[static_cast<size_t>(row0[p] + i) * ldy + j];
+      voff += n[p] * nevs[p];
+    }
+    off += nevs[p];
+  }
+}
+
 }  // namespace
 }  // namespace fe
+
+namespace {
+void check_pair(const fe::Csr& A, const fe::Csr& B) {
+  FE_REQUIRE(B.rows == A.rows && B.cols == A.cols,
+             "generalized problem: B must have the same shape as A.");
+  FE_REQUIRE(B.device == A.device, "generalized problem: A and B live on different devices.");
+}
+}  // namespace
 
 extern "C" int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eigenvalues,
                         double* residual_norms, double* eigenvectors, double* stats) {
@@ -1347,11 +1994,23 @@ extern "C" int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eig
       FE_REQUIRE(B == nullptr, "ChebyshevSolver: generalized problems are not supported.");
       fe::chebyshev_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
     } else if (opt.solver == "lobpcg") {
-      FE_REQUIRE(B == nullptr, "LOBPCGSolver: generalized problems are not supported.");
-      fe::lobpcg_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
+      // The reference's standard unpreconditioned LOBPCG unless the problem is
+      // generalized, preconditioned, or iterates more vectors than requested.
+      if (B || opt.precond != "none" || opt.block > opt.nev) {
+        if (B) check_pair(A->m, B->m);
+        fe::lobpcg_gen_solve(A->m, B ? &B->m : nullptr, opt, eigenvalues, residual_norms,
+                             eigenvectors, st);
+      } else {
+        fe::lobpcg_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
+      }
     } else if (opt.solver == "davidson") {
-      FE_REQUIRE(B == nullptr, "DavidsonSolver: generalized problems are not supported.");
-      fe::davidson_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
+      if (B || opt.precond != "none") {
+        if (B) check_pair(A->m, B->m);
+        fe::davidson_gen_solve(A->m, B ? &B->m : nullptr, opt, eigenvalues, residual_norms,
+                               eigenvectors, st);
+      } else {
+        fe::davidson_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
+      }
     } else if (opt.solver == "krylovschur") {
       FE_REQUIRE(B == nullptr,
                  "KrylovSchurSolver: generalized problems need a B^{-1} factorization (out of "
@@ -1375,6 +2034,34 @@ extern "C" int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eig
       stats[9] = st.ortho_ms;
       stats[10] = st.rr_ms;
       stats[11] = st.precise_grams;
+    }
+  });
+}
+
+extern "C" int fe_batch_krylov_schur(int32_t count, const fe_csr_t* A, const int64_t* nev,
+                                     const char* options, double* eigenvalues,
+                                     double* residual_norms, double* eigenvectors,
+                                     int32_t* iterations, int32_t* status, double* stats) {
+  return fe::guarded("fe_batch_krylov_schur", [&] {
+    FE_REQUIRE(count > 0 && A && nev, "null or empty batch");
+    FE_REQUIRE(eigenvalues && residual_norms && iterations && status, "null result arrays");
+    fe::Options opt;
+    opt.parse(options);
+    std::vector<const fe::Csr*> As(count);
+    std::vector<int64_t> nevs(nev, nev + count);
+    for (int32_t p = 0; p < count; ++p) {
+      FE_REQUIRE(A[p], "null CSR handle in batch");
+      As[p] = &A[p]->m;
+    }
+    FE_CHECK_CUDA(cudaSetDevice(As[0]->device));
+    fe::BatchStats bs;
+    fe::batch_krylov_schur(As, nevs, opt, eigenvalues, residual_norms, eigenvectors, iterations,
+                           status, bs);
+    if (stats) {
+      stats[0] = bs.seconds;
+      stats[1] = bs.rounds;
+      stats[2] = bs.steps;
+      stats[3] = bs.graph_launches;
     }
   });
 }

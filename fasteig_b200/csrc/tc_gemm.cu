@@ -54,6 +54,9 @@ constexpr int kABytes = kM * kKB * 4;   // 16 KB
 constexpr int kBBytes = kN * kKB * 4;   // 20 KB
 constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+// Rotation epilogue staging: 4 warps x 32 rows x (kN + 1) floats inside the stages.
+constexpr int kStageLd = kN + 1;
+static_assert(4 * 32 * kStageLd * 4 <= kStages * kStageBytes, "epilogue staging does not fit");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -454,16 +457,23 @@ rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
       fence_proxy_async();
       mbar_arrive(&sm.split[s]);
     }
-    if (mbar_wait(sm.accum, 0, 4)) {
-      tc_fence_after();
-      const int q = warp % 4;
-      const int64_t r = r0 + q * 32 + lane;
-      for (int c = 0; c < kN; c += 16) {
-        float v[16];
-        tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c, v);
-        if (r < n) {
+    // Epilogue: TMEM lane = tile row, column = output column. A 16-byte aligned Y
+    // is written straight from registers, four floats per store along each row.
+    // Otherwise (a column view such as V[:, locked:] at any offset) each warp
+    // stages its 32 rows x kN slice in the (now idle) pipeline shared memory and
+    // writes Y row by row with lanes on consecutive columns, so stores stay
+    // coalesced instead of one 4-byte store per row per lane.
+    if (vec_store) {
+      if (mbar_wait(sm.accum, 0, 4)) {
+        tc_fence_after();
+        const int q = warp % 4;
+        const int64_t r = r0 + q * 32 + lane;
+        for (int c = 0; c < kN; c += 16) {
+          float v[16];
+          tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c, v);
+          if (r >= n) continue;
           float* yr = Y + r * ldy + j0 + c;
-          if (vec_store && j0 + c + 16 <= m) {
+          if (j0 + c + 16 <= m) {
 #pragma unroll
             for (int e = 0; e < 16; e += 4) {
               float4 o = make_float4(alpha * v[e], alpha * v[e + 1], alpha * v[e + 2],
@@ -487,6 +497,28 @@ rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
               }
             }
           }
+        }
+      }
+    } else if (mbar_wait(sm.accum, 0, 4)) {
+      tc_fence_after();
+      const int q = warp % 4;
+      float* stage = reinterpret_cast<float*>(sm.base) + q * (32 * kStageLd);
+      for (int c = 0; c < kN; c += 16) {
+        float v[16];
+        tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c, v);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) stage[lane * kStageLd + c + e] = v[e];
+      }
+      __syncwarp();
+      const int jn = min(kN, m - j0);
+      for (int rr = 0; rr < 32; ++rr) {
+        const int64_t r = r0 + q * 32 + rr;
+        if (r >= n) break;
+        float* yr = Y + r * ldy + j0;
+        for (int c = lane; c < jn; c += 32) {
+          float o = alpha * stage[rr * kStageLd + c];
+          if (use_beta) o = fmaf(beta, yr[c], o);
+          yr[c] = o;
         }
       }
     }

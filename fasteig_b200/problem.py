@@ -19,7 +19,8 @@ from ._lib import check, lib
 _INT_KEYS = ("n", "nev", "maxiter", "maxdim", "maxblks", "degree", "blksize", "verbosity",
              "print_every", "block", "tensor_cores")
 _FLOAT_KEYS = ("tol", "shift", "amplification", "mixed_switch")
-_STR_KEYS = ("which", "solver", "precision", "bounds", "init", "logfile", "output_format")
+_STR_KEYS = ("which", "solver", "precision", "bounds", "init", "logfile", "output_format",
+             "precond")
 
 
 class fasteig_options:  # noqa: N801 - reference class name
@@ -178,3 +179,47 @@ class fasteig_problem:  # noqa: N801 - reference class name
 
     def last_iterations(self):
         return self._iters
+
+
+def batch_krylov_schur(problems, nevs, opts: Optional[fasteig_options] = None,
+                       want_vectors: bool = False):
+    """Solve many independent standard problems together with the batched
+    Krylov-Schur engine (``fe_batch_krylov_schur``). ``problems`` are device
+    ``CsrMatrix`` objects, ``nevs`` the wanted pair counts. Returns a list of dicts
+    (eigenvalues, residual_norms, eigenvectors or None, iterations, status) and the
+    batch stats (seconds, rounds, steps, graph_launches)."""
+    problems = list(problems)
+    nevs = np.ascontiguousarray(np.asarray(nevs, dtype=np.int64))
+    if len(problems) != nevs.size or not problems:
+        raise ValueError("one nev per problem is required")
+    opts = opts or fasteig_options()
+    text = opts.to_text()
+    count = len(problems)
+    handles = (C.c_void_p * count)(*[p.handle for p in problems])
+    total = int(nevs.sum())
+    vals = np.zeros(total)
+    res = np.zeros(total)
+    sizes = [p.rows * int(k) for p, k in zip(problems, nevs)]
+    vecs = np.zeros(sum(sizes)) if want_vectors else None
+    iters = np.zeros(count, dtype=np.int32)
+    status = np.zeros(count, dtype=np.int32)
+    stats = np.zeros(4)
+    check(lib.fe_batch_krylov_schur(count, C.cast(handles, C.c_void_p), nevs.ctypes.data,
+                                    text.encode(), vals.ctypes.data, res.ctypes.data,
+                                    vecs.ctypes.data if vecs is not None else None,
+                                    iters.ctypes.data, status.ctypes.data, stats.ctypes.data))
+    out, off, voff = [], 0, 0
+    for p, k, sz in zip(problems, nevs, sizes):
+        k = int(k)
+        ev = None
+        if vecs is not None:
+            ev = vecs[voff:voff + sz].reshape(k, p.rows).T
+            voff += sz
+        out.append(dict(eigenvalues=vals[off:off + k], residual_norms=res[off:off + k],
+                        eigenvectors=ev))
+        off += k
+    for d, it, st in zip(out, iters, status):
+        d["iterations"] = int(it)
+        d["status"] = int(st)
+    return out, dict(seconds=float(stats[0]), rounds=int(stats[1]), steps=int(stats[2]),
+                     graph_launches=int(stats[3]))

@@ -238,7 +238,10 @@ int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ld
  * build_csr_from_sparse_matrix produces) and options as "key=value" lines
  * with the reference's keys (src/fasteig_options.cpp:51-112: nev, maxiter,
  * maxdim, maxblks, degree, which, solver, tol, seed, blksize) plus
- * extensions (precision=fp64|mixed, block=<cols>, bounds=reference|ritz).
+ * extensions (precision=fp64|mixed, block=<cols>, bounds=reference|ritz,
+ * precond=none|jacobi, init=host|device). B != NULL makes the problem
+ * generalized (A x = l B x, B symmetric positive definite): LOBPCG and Davidson
+ * then work in the B metric (extension; the reference's are standard-only).
  * Results: eigenvalues[nev], residual_norms[nev] (the reference's relative
  * residual), eigenvectors n-by-nev column-major (may be NULL), stats[12] (may
  * be NULL): iterations, status, solve seconds, SpMM launches, FP32 cycles, FP64
@@ -248,6 +251,26 @@ int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ld
  * ------------------------------------------------------------------- */
 int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eigenvalues,
              double* residual_norms, double* eigenvectors, double* stats);
+
+/* ---------------------------------------------------------------------
+ * Batched Krylov-Schur (extension; the reference solves one problem per
+ * process with KrylovSchurSolver::solve, src/KrylovSchurSolver.cpp:28-160):
+ * `count` independent standard problems A[p] (all on one device) with nev[p]
+ * wanted pairs each, solved together in lockstep on grouped kernels, one CUDA
+ * graph per Lanczos step of the whole batch. Options as for fe_solve (which,
+ * tol, maxiter, maxdim, seed, init); subspace dimension per problem
+ * max(2 nev, 20, maxdim) capped at n and at 96. Each problem's arithmetic is
+ * independent of the rest of the batch, so its results are the same alone.
+ * Results concatenated in problem order: eigenvalues and residual_norms
+ * (sum of nev), eigenvectors (may be NULL) as consecutive n[p]-by-nev[p]
+ * column-major blocks, iterations[count] (restart cycles), status[count]
+ * (0 = converged or at maxiter), stats[4] (may be NULL): seconds, restart
+ * rounds, Lanczos steps, graph launches.
+ * ------------------------------------------------------------------- */
+int fe_batch_krylov_schur(int32_t count, const fe_csr_t* A, const int64_t* nev,
+                          const char* options, double* eigenvalues, double* residual_norms,
+                          double* eigenvectors, int32_t* iterations, int32_t* status,
+                          double* stats);
 
 #ifdef __cplusplus
 }

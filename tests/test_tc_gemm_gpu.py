@@ -81,3 +81,24 @@ def test_rotate_tf32x3_output_column_view():
     torch.cuda.synchronize()
     np.testing.assert_allclose(V[:, 13:40].double().cpu().numpy(), ref.cpu().numpy(),
                                rtol=0, atol=2e-5 * np.abs(ref.cpu().numpy()).max())
+
+
+@pytest.mark.parametrize("locked,sub", [(250, 320), (253, 320), (130, 320), (97, 300)])
+def test_rotate_tf32x3_deflation_update_in_place(locked, sub):
+    """The Chebyshev deflation update V[:, locked:] -= V[:, :locked] G inside one
+    320-wide slab: output column view at any offset (not 16-byte aligned)."""
+    from fasteig_b200 import ops
+    assert ops.device_status(clear=True) == 0
+    V = blk(20011, sub, 9, ld=320)
+    G = torch.randn(locked, sub - locked, dtype=torch.float64,
+                    generator=torch.Generator().manual_seed(3)).cuda() * 0.1
+    V64 = V.double().cpu().numpy()
+    ref = V64[:, locked:] - V64[:, :locked] @ G.cpu().numpy()
+    ops.rotate_tf32x3(V[:, :locked], G, V[:, locked:], -1.0, 1.0)
+    torch.cuda.synchronize()
+    assert ops.device_status() == 0
+    scale = np.abs(V64[:, :locked]) @ np.abs(G.cpu().numpy()) + np.abs(V64[:, locked:])
+    err = np.abs(V[:, locked:].double().cpu().numpy() - ref)
+    assert np.all(err <= (locked + 4) * 2.0 ** -22 * scale + 1e-30), (err / scale).max()
+    # untouched locked columns
+    assert np.array_equal(V[:, :locked].double().cpu().numpy(), V64[:, :locked])
