@@ -62,7 +62,12 @@ _SIGS = {
     "fe_device_status": (C.c_int, [C.POINTER(C.c_int32), C.c_int32]),
     "fe_set_spmm_kernel": (C.c_int, [C.c_int32]),
     "fe_set_f64_gemm_kernel": (C.c_int, [C.c_int32]),
+    "fe_csr_autotune": (C.c_int, [vp, i64, C.c_int32, vp, vp]),
     "fe_batch_krylov_schur": (C.c_int, [C.c_int32, vp, vp, C.c_char_p, vp, vp, vp, vp, vp, vp]),
+    "fe_server_create": (C.c_int, [C.c_int32, C.c_int32, i64, vp]),
+    "fe_server_submit": (C.c_int, [vp, vp, vp, C.c_char_p, vp]),
+    "fe_server_wait": (C.c_int, [vp, i64, C.c_double, vp, vp, vp]),
+    "fe_server_destroy": (C.c_int, [vp]),
     "fe_gram_f64_noalloc": (C.c_int, [vp, i64, vp, i64, i64, i64, i64, vp, i64, vp]),
     "fe_gram_f64_noalloc_max_entries": (C.c_int64, []),
 }

@@ -30,6 +30,24 @@ std::atomic<int64_t> g_launches{0};
 }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+cudaStream_t& alloc_stream() {
+  thread_local cudaStream_t s = nullptr;
+  return s;
+}
+
+void retain_pool_memory(int device) {
+  static std::mutex mu;
+  static bool done[64] = {};
+  if (device < 0 || device >= 64) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[device]) return;
+  cudaMemPool_t pool;
+  FE_CHECK_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t keep = UINT64_MAX;
+  FE_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  done[device] = true;
+}
+
 int num_sms() {
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 148;

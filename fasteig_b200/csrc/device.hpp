@@ -44,6 +44,15 @@ void trinv_upper(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_
 void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s);
 
 // ---- owning device buffer --------------------------------------------------
+// Stream on which this thread's DeviceBuffer allocations are ordered (set for the
+// lifetime of a solver Context). With a stream, buffers come from the device's
+// stream-ordered memory pool (cudaMallocAsync / cudaFreeAsync), which keeps the
+// memory of one solve for the next instead of mapping and unmapping tens of GB
+// per solve; without one, plain cudaMalloc / cudaFree.
+cudaStream_t& alloc_stream();
+// Keep freed pool memory reserved for this process (called once per device).
+void retain_pool_memory(int device);
+
 class DeviceBuffer {
  public:
   DeviceBuffer() = default;
@@ -51,17 +60,20 @@ class DeviceBuffer {
   ~DeviceBuffer() { release(); }
   DeviceBuffer(const DeviceBuffer&) = delete;
   DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-  DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), bytes_(o.bytes_) {
+  DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), bytes_(o.bytes_), s_(o.s_) {
     o.p_ = nullptr;
     o.bytes_ = 0;
+    o.s_ = nullptr;
   }
   DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
     if (this != &o) {
       release();
       p_ = o.p_;
       bytes_ = o.bytes_;
+      s_ = o.s_;
       o.p_ = nullptr;
       o.bytes_ = 0;
+      o.s_ = nullptr;
     }
     return *this;
   }
@@ -69,7 +81,8 @@ class DeviceBuffer {
     if (bytes <= bytes_ && p_) return;
     release();
     if (bytes == 0) return;
-    cudaError_t e = cudaMalloc(&p_, bytes);
+    s_ = alloc_stream();
+    cudaError_t e = s_ ? cudaMallocAsync(&p_, bytes, s_) : cudaMalloc(&p_, bytes);
     if (e != cudaSuccess) {
       p_ = nullptr;
       throw Error(FE_ERR_ALLOC, std::string("cudaMalloc(") + std::to_string(bytes) +
@@ -78,9 +91,13 @@ class DeviceBuffer {
     bytes_ = bytes;
   }
   void release() {
-    if (p_) cudaFree(p_);
+    if (p_) {
+      if (s_) cudaFreeAsync(p_, s_);
+      else cudaFree(p_);
+    }
     p_ = nullptr;
     bytes_ = 0;
+    s_ = nullptr;
   }
   void* get() const { return p_; }
   size_t bytes() const { return bytes_; }
@@ -92,6 +109,7 @@ class DeviceBuffer {
  private:
   void* p_ = nullptr;
   size_t bytes_ = 0;
+  cudaStream_t s_ = nullptr;  // allocation stream (pool) or null (cudaMalloc)
 };
 
 // Row-major n-by-cols block with leading dimension ld (padded to 8 elements so

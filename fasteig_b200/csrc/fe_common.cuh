@@ -99,6 +99,13 @@ struct Csr {
   float* val32 = nullptr;
   int device = 0;
   int64_t max_row_nnz = 0;
+  // SpMM kernel chosen by fe_csr_autotune per precision (0 FP64, 1 FP32) for up
+  // to four block widths; mode < 0 marks an empty entry.
+  struct Tuned {
+    int32_t ncols = 0;
+    int32_t mode = -1;
+  };
+  Tuned tuned[2][4];
 };
 
 int num_sms();

@@ -1,0 +1,220 @@
+// Request server (extension): a device-resident serving loop for eigenproblems
+// of uneven size. Requests are admitted in arrival order as soon as a worker slot
+// and enough of the device-memory budget are free (each request's blocks and
+// workspaces, bounded by solve_memory_bytes); every admitted solve runs on its
+// own stream with all of its state (subspace, Ritz values, locking) on the
+// device, so the work of concurrently admitted requests overlaps on the GPU and
+// requests that arrive while others run join as soon as memory frees up.
+//
+// The reference serves nothing: fasteig_problem::solve (src/fasteig_problem.cpp:
+// 340-437) is one blocking solve per call. Each request here runs exactly that
+// solve (the same code path as fe_solve), so its result does not depend on what
+// else is in flight.
+
+#include "device.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace fe {
+void solve_problem(const Csr& A, const Csr* B, const char* options, double* eigenvalues,
+                   double* residual_norms, double* eigenvectors, double* stats);
+size_t solve_memory_bytes(const Csr& A, const Csr* B, const char* options);
+int64_t options_nev(const char* options);
+}  // namespace fe
+
+struct fe_server {
+  using clock = std::chrono::steady_clock;
+  struct Request {
+    int64_t id = 0;
+    const fe::Csr* A = nullptr;
+    const fe::Csr* B = nullptr;
+    std::string options;
+    int64_t nev = 0;
+    size_t bytes = 0;
+    std::vector<double> eigenvalues, residuals, stats;
+    int state = 0;  // 0 queued, 1 running, 2 done
+    int rc = FE_OK;
+    std::string error;
+    clock::time_point t_submit, t_start, t_end;
+  };
+
+  int device = 0;
+  clock::time_point t_created = clock::now();
+  size_t budget = 0, in_use = 0;
+  int64_t next_id = 1;
+  int running = 0;
+  bool stopping = false;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request*> queue;
+  std::map<int64_t, std::unique_ptr<Request>> requests;
+  std::vector<std::thread> workers;
+
+  // Head-of-line admission: the oldest request starts when it fits the budget,
+  // or when nothing is running (a request larger than the budget still runs,
+  // alone).
+  bool can_admit() const {
+    if (queue.empty()) return false;
+    const Request* r = queue.front();
+    return running == 0 || in_use + r->bytes <= budget;
+  }
+
+  void worker_loop() {
+    cudaSetDevice(device);
+    while (true) {
+      Request* r = nullptr;
+      {
+        std::unique_lock<std::mutex> lock(mu);
+        cv_work.wait(lock, [&] { return stopping || can_admit(); });
+        if (stopping) return;
+        r = queue.front();
+        queue.pop_front();
+        in_use += r->bytes;
+        ++running;
+        r->state = 1;
+        r->t_start = clock::now();
+      }
+      const int rc = fe::guarded("fe_server request", [&] {
+        fe::solve_problem(*r->A, r->B, r->options.c_str(), r->eigenvalues.data(),
+                          r->residuals.data(), nullptr, r->stats.data());
+      });
+      {
+        std::lock_guard<std::mutex> lock(mu);
+        r->rc = rc;
+        if (rc != FE_OK) r->error = fe_last_error();
+        r->t_end = clock::now();
+        r->state = 2;
+        in_use -= r->bytes;
+        --running;
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();
+    }
+  }
+};
+
+extern "C" int fe_server_create(int32_t device, int32_t slots, int64_t memory_budget_bytes,
+                                fe_server_t* out) {
+  return fe::guarded("fe_server_create", [&] {
+    FE_REQUIRE(out, "null output handle");
+    FE_REQUIRE(slots >= 1 && slots <= 64, "slots must be in [1, 64]");
+    FE_CHECK_CUDA(cudaSetDevice(device));
+    auto srv = std::make_unique<fe_server>();
+    srv->device = device;
+    if (memory_budget_bytes > 0) {
+      srv->budget = static_cast<size_t>(memory_budget_bytes);
+    } else {
+      size_t free_b = 0, total_b = 0;
+      FE_CHECK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      srv->budget = free_b / 10 * 9;
+    }
+    for (int i = 0; i < slots; ++i) srv->workers.emplace_back([s = srv.get()] { s->worker_loop(); });
+    *out = srv.release();
+  });
+}
+
+extern "C" int fe_server_submit(fe_server_t srv, fe_csr_t A, fe_csr_t B, const char* options,
+                                int64_t* request_id) {
+  return fe::guarded("fe_server_submit", [&] {
+    FE_REQUIRE(srv && A && request_id, "null argument");
+    FE_REQUIRE(A->m.device == srv->device, "request operator lives on another device");
+    auto r = std::make_unique<fe_server::Request>();
+    r->A = &A->m;
+    r->B = B ? &B->m : nullptr;
+    r->options = options ? options : "";
+    r->bytes = fe::solve_memory_bytes(A->m, r->B, r->options.c_str());
+    // nev as the solve will parse it (unknown keys and bad values fail here, not
+    // in a worker).
+    r->nev = fe::options_nev(r->options.c_str());
+    FE_REQUIRE(r->nev >= 1 && r->nev <= A->m.rows, "nev must be in [1, n]");
+    r->eigenvalues.assign(r->nev, 0.0);
+    r->residuals.assign(r->nev, 0.0);
+    r->stats.assign(12, 0.0);
+    r->t_submit = fe_server::clock::now();
+    {
+      std::lock_guard<std::mutex> lock(srv->mu);
+      FE_REQUIRE(!srv->stopping, "server is shutting down");
+      r->id = srv->next_id++;
+      *request_id = r->id;
+      srv->queue.push_back(r.get());
+      srv->requests.emplace(r->id, std::move(r));
+    }
+    srv->cv_work.notify_one();
+  });
+}
+
+extern "C" int fe_server_wait(fe_server_t srv, int64_t request_id, double timeout_seconds,
+                              double* eigenvalues, double* residual_norms, double* stats) {
+  int solve_rc = FE_OK;
+  std::string solve_error;
+  const int rc = fe::guarded("fe_server_wait", [&] {
+    FE_REQUIRE(srv, "null server");
+    std::unique_ptr<fe_server::Request> r;
+    {
+      std::unique_lock<std::mutex> lock(srv->mu);
+      auto it = srv->requests.find(request_id);
+      FE_REQUIRE(it != srv->requests.end(), "unknown or already collected request id");
+      fe_server::Request* req = it->second.get();
+      auto done = [&] { return req->state == 2; };
+      if (timeout_seconds < 0) {
+        srv->cv_done.wait(lock, done);
+      } else if (!srv->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_seconds),
+                                        done)) {
+        throw fe::Error(FE_PENDING, "request still queued or running");
+      }
+      r = std::move(it->second);
+      srv->requests.erase(it);
+    }
+    if (eigenvalues) std::copy(r->eigenvalues.begin(), r->eigenvalues.end(), eigenvalues);
+    if (residual_norms) std::copy(r->residuals.begin(), r->residuals.end(), residual_norms);
+    if (stats) {
+      std::copy(r->stats.begin(), r->stats.end(), stats);
+      auto sec = [](fe_server::clock::time_point a, fe_server::clock::time_point b) {
+        return std::chrono::duration<double>(b - a).count();
+      };
+      stats[12] = sec(r->t_submit, r->t_start);  // queueing
+      stats[13] = sec(r->t_start, r->t_end);     // on the device
+      stats[14] = sec(r->t_submit, r->t_end);    // latency
+      stats[15] = static_cast<double>(r->bytes);
+      stats[16] = sec(srv->t_created, r->t_start);  // start, seconds since server creation
+      stats[17] = sec(srv->t_created, r->t_end);    // end
+    }
+    solve_rc = r->rc;
+    solve_error = r->error;
+  });
+  if (rc != FE_OK) return rc;
+  if (solve_rc != FE_OK) fe::set_last_error(solve_error);
+  return solve_rc;
+}
+
+extern "C" int fe_server_destroy(fe_server_t srv) {
+  return fe::guarded("fe_server_destroy", [&] {
+    if (!srv) return;
+    {
+      // Let admitted requests finish; queued ones are dropped (and reported so).
+      std::unique_lock<std::mutex> lock(srv->mu);
+      for (auto* r : srv->queue) {
+        r->state = 2;
+        r->rc = FE_ERR_INVALID;
+        r->error = "fe_server: server destroyed before the request ran";
+        r->t_start = r->t_end = fe_server::clock::now();
+      }
+      srv->queue.clear();
+      srv->cv_done.notify_all();
+      srv->cv_done.wait(lock, [&] { return srv->running == 0; });
+      srv->stopping = true;
+    }
+    srv->cv_work.notify_all();
+    for (auto& t : srv->workers) t.join();
+    delete srv;
+  });
+}

@@ -182,19 +182,31 @@ struct PhaseEvents {
   }
 };
 
+// One solve's stream and cuSOLVER handle. While it lives, this thread's
+// DeviceBuffers are allocated from the device's stream-ordered pool on its stream
+// (buffers declared after the Context are released before it).
 class Context {
  public:
   cudaStream_t stream = nullptr;
   cusolverDnHandle_t solver = nullptr;
   Context() {
+    int dev = 0;
+    FE_CHECK_CUDA(cudaGetDevice(&dev));
+    retain_pool_memory(dev);
     FE_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     FE_CHECK_SOLVER(cusolverDnCreate(&solver));
     FE_CHECK_SOLVER(cusolverDnSetStream(solver, stream));
+    prev_alloc_ = alloc_stream();
+    alloc_stream() = stream;
   }
   ~Context() {
+    alloc_stream() = prev_alloc_;
+    if (stream) cudaStreamSynchronize(stream);
     if (solver) cusolverDnDestroy(solver);
     if (stream) cudaStreamDestroy(stream);
   }
+  Context(const Context&) = delete;
+  Context& operator=(const Context&) = delete;
   void sync() { FE_CHECK_CUDA(cudaStreamSynchronize(stream)); }
   template <typename T>
   void to_host(T* dst, const T* src, size_t count) {
@@ -204,6 +216,9 @@ class Context {
   void to_device(T* dst, const T* src, size_t count) {
     FE_CHECK_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, stream));
   }
+
+ private:
+  cudaStream_t prev_alloc_ = nullptr;
 };
 
 // Host std::mt19937 draws in the reference's column-major order
@@ -591,6 +606,11 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   const bool host_init = opt.init == "host";
   const bool mixed = opt.precision == "mixed";
 
+  using clock = std::chrono::steady_clock;
+  const auto t_start = clock::now();
+  auto ms_since = [](clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(clock::now() - t).count();
+  };
   Context ctx;
   SmallState sm;
   sm.allocate(n, cap, mixed && opt.tensor_cores && tc_gemm_available());
@@ -627,6 +647,8 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     ctx.sync();
     if (info != 0) throw Error(FE_ERR_NOT_SPD, "ChebyshevSolver: initial Cholesky QR failed.");
   }
+  if (opt.verbosity >= 2)
+    std::fprintf(stderr, "[fe] setup (buffers, bounds, initial QR) %.1f ms\n", ms_since(t_start));
 
   int64_t locked = 0;
   int64_t sub = nev;
@@ -683,6 +705,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     const bool stalled = h >= 4 && worst > 0.7 * worst_history[h - 4];
     if (l32 && (worst <= std::max(opt.mixed_switch, tol) || stalled)) {
       worst_history.clear();
+      const auto t_switch = clock::now();
       // FP32 residual floor reached: continue on FP64 blocks.
       l64.reset(new ChebLoop<double>(ctx, A, opt, sm, eig, sign, lower, upper, false));
       l64->b.allocate(n, cap);
@@ -690,6 +713,8 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
                              ctx.stream);
       ctx.sync();
       l32.reset();
+      if (opt.verbosity >= 2)
+        std::fprintf(stderr, "[fe] FP32 -> FP64 switch %.1f ms\n", ms_since(t_switch));
       locked = 0;  // FP64 sweeps refine every pair to tol
       while (locked < nev && rel[locked] <= tol) ++locked;
     }
@@ -699,6 +724,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   // fasteig_problem::solve recomputes for non-Krylov solvers on the host
   // (src/fasteig_problem.cpp:419-422, src/fasteig_solver.cpp:89-129).
   for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = sign * W[j];
+  const auto t_finish = clock::now();
   {
     cudaStream_t s = ctx.stream;
     Block<double> Xf, AXf;
@@ -720,29 +746,20 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
                            sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
                            sm.rws.get(), sm.rws.bytes(), s, 1);
     ctx.to_host(residuals, sm.rel.as<double>(), nev);
-    ctx.sync();
-  }
-  if (eigenvectors) {
-    // Row-major device block -> column-major host n x nev (copy_to_host boundary).
-    std::vector<double> host(static_cast<size_t>(n) * nev);
-    if (l64) {
-      FE_CHECK_CUDA(cudaMemcpy2DAsync(host.data(), nev * sizeof(double), l64->b.V.data(),
-                                      l64->b.V.ld * sizeof(double), nev * sizeof(double), n,
-                                      cudaMemcpyDeviceToHost, ctx.stream));
-    } else {
-      Block<double> tmp;
-      tmp.allocate(n, nev);
-      convert<float, double>(l32->b.V.data(), l32->b.V.ld, tmp.data(), tmp.ld, n, nev, ctx.stream);
-      FE_CHECK_CUDA(cudaMemcpy2DAsync(host.data(), nev * sizeof(double), tmp.data(),
-                                      tmp.ld * sizeof(double), nev * sizeof(double), n,
-                                      cudaMemcpyDeviceToHost, ctx.stream));
+    if (eigenvectors) {
+      // Row-major device block -> column-major n x nev (the copy_to_host boundary),
+      // transposed on the device and copied straight into the caller's buffer.
+      AXf.buf.release();
+      DeviceBuffer cm(static_cast<size_t>(n) * nev * sizeof(double));
+      to_colmajor(Xp, ldx, n, nev, cm.as<double>(), s);
+      FE_CHECK_CUDA(cudaMemcpyAsync(eigenvectors, cm.get(), cm.bytes(), cudaMemcpyDeviceToHost, s));
       ctx.sync();
     }
     ctx.sync();
-    for (int64_t i = 0; i < n; ++i)
-      for (int64_t j = 0; j < nev; ++j)
-        eigenvectors[static_cast<size_t>(j) * n + i] = host[static_cast<size_t>(i) * nev + j];
   }
+  if (opt.verbosity >= 2)
+    std::fprintf(stderr, "[fe] finish (FP64 residual check%s) %.1f ms\n",
+                 eigenvectors ? ", vectors to host" : "", ms_since(t_finish));
   st.iterations = static_cast<double>(it_done);
   st.precise_grams = static_cast<double>(sm.precise_grams);
 }
@@ -1153,6 +1170,12 @@ void davidson_solve(const Csr& A, const Options& opt, double* eigenvalues, doubl
   finish_results(ctx, sm, A, nullptr, X.data(), ld, n, nev, eigenvalues, residuals, eigenvectors);
   st.iterations = static_cast<double>(it_done);
   st.fp64_iterations = static_cast<double>(it_done);
+}
+
+void check_pair(const Csr& A, const Csr& B) {
+  FE_REQUIRE(B.rows == A.rows && B.cols == A.cols,
+             "generalized problem: B must have the same shape as A.");
+  FE_REQUIRE(B.device == A.device, "generalized problem: A and B live on different devices.");
 }
 
 // ===========================================================================
@@ -1972,69 +1995,109 @@ void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int
 }  // namespace
 }  // namespace fe
 
-namespace {
-void check_pair(const fe::Csr& A, const fe::Csr& B) {
-  FE_REQUIRE(B.rows == A.rows && B.cols == A.cols,
-             "generalized problem: B must have the same shape as A.");
-  FE_REQUIRE(B.device == A.device, "generalized problem: A and B live on different devices.");
+namespace fe {
+
+// Solver dispatch of fasteig_problem::solve (src/fasteig_problem.cpp:340-437) on
+// device CSR operators; throws fe::Error. Shared by fe_solve and the request server.
+void solve_problem(const Csr& A, const Csr* B, const char* options, double* eigenvalues,
+                   double* residual_norms, double* eigenvectors, double* stats) {
+  FE_REQUIRE(eigenvalues && residual_norms, "null result arrays");
+  Options opt;
+  opt.parse(options);
+  Stats st;
+  const auto t0 = std::chrono::steady_clock::now();
+  FE_CHECK_CUDA(cudaSetDevice(A.device));
+  if (opt.solver == "chebyshev") {
+    FE_REQUIRE(B == nullptr, "ChebyshevSolver: generalized problems are not supported.");
+    chebyshev_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
+  } else if (opt.solver == "lobpcg") {
+    // The reference's standard unpreconditioned LOBPCG unless the problem is
+    // generalized, preconditioned, or iterates more vectors than requested.
+    if (B || opt.precond != "none" || opt.block > opt.nev) {
+      if (B) check_pair(A, *B);
+      lobpcg_gen_solve(A, B, opt, eigenvalues, residual_norms, eigenvectors, st);
+    } else {
+      lobpcg_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
+    }
+  } else if (opt.solver == "davidson") {
+    if (B || opt.precond != "none") {
+      if (B) check_pair(A, *B);
+      davidson_gen_solve(A, B, opt, eigenvalues, residual_norms, eigenvectors, st);
+    } else {
+      davidson_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
+    }
+  } else if (opt.solver == "krylovschur") {
+    FE_REQUIRE(B == nullptr,
+               "KrylovSchurSolver: generalized problems need a B^{-1} factorization (out of "
+               "scope on this backend).");
+    krylov_schur_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
+  } else {
+    throw Error(FE_ERR_UNSUPPORTED, "solver not available on this backend: " + opt.solver);
+  }
+  const auto t1 = std::chrono::steady_clock::now();
+  st.seconds = std::chrono::duration<double>(t1 - t0).count();
+  if (stats) {
+    stats[0] = st.iterations;
+    stats[1] = st.status;
+    stats[2] = st.seconds;
+    stats[3] = st.spmm_launches;
+    stats[4] = st.fp32_iterations;
+    stats[5] = st.fp64_iterations;
+    stats[6] = st.lower;
+    stats[7] = st.upper;
+    stats[8] = st.filter_ms;
+    stats[9] = st.ortho_ms;
+    stats[10] = st.rr_ms;
+    stats[11] = st.precise_grams;
+  }
 }
-}  // namespace
+
+// nev of an option string, validating every key as the solve will.
+int64_t options_nev(const char* options) {
+  Options opt;
+  opt.parse(options);
+  return opt.nev;
+}
+
+// Upper bound of the device memory one solve allocates (its blocks and
+// workspaces; the CSR operators are the caller's), for admission control.
+size_t solve_memory_bytes(const Csr& A, const Csr* B, const char* options) {
+  Options opt;
+  opt.parse(options);
+  const int64_t n = A.rows;
+  const int64_t nev = std::max<int64_t>(1, std::min<int64_t>(opt.nev, n));
+  auto ld = [](int64_t c) { return std::max<int64_t>(8, ((c + 7) / 8) * 8); };
+  double blocks = 0;  // n x ld doubles
+  int64_t cap = nev;
+  if (opt.solver == "chebyshev") {
+    cap = nev + std::min(nev, n - nev);
+    if (opt.block > 0) cap = std::max(nev, std::min(opt.block, n));
+    // FP64: 4 loop blocks + 2 initial; mixed adds 4 FP32 blocks (half size).
+    blocks = opt.precision == "mixed" ? 4 + 2 + 2 + 1 : 4 + 2 + 1;
+  } else if (opt.solver == "lobpcg") {
+    cap = std::min<int64_t>(n, 3 * std::max<int64_t>(nev, opt.block));
+    blocks = 12;
+  } else if (opt.solver == "davidson") {
+    cap = std::min<int64_t>(n, opt.maxblks * nev);
+    blocks = 11;
+  } else {
+    cap = std::min<int64_t>(std::max<int64_t>({2 * nev, 20, opt.maxdim}), n);
+    blocks = 3;
+  }
+  (void)B;
+  const double bytes = blocks * static_cast<double>(n) * ld(cap) * 8.0 +
+                       2.0 * static_cast<double>(cap) * cap * 8.0 * 8.0 + (64u << 20);
+  return static_cast<size_t>(bytes);
+}
+
+}  // namespace fe
 
 extern "C" int fe_solve(fe_csr_t A, fe_csr_t B, const char* options, double* eigenvalues,
                         double* residual_norms, double* eigenvectors, double* stats) {
   return fe::guarded("fe_solve", [&] {
     FE_REQUIRE(A, "null CSR handle");
-    FE_REQUIRE(eigenvalues && residual_norms, "null result arrays");
-    fe::Options opt;
-    opt.parse(options);
-    fe::Stats st;
-    const auto t0 = std::chrono::steady_clock::now();
-    FE_CHECK_CUDA(cudaSetDevice(A->m.device));
-    if (opt.solver == "chebyshev") {
-      FE_REQUIRE(B == nullptr, "ChebyshevSolver: generalized problems are not supported.");
-      fe::chebyshev_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
-    } else if (opt.solver == "lobpcg") {
-      // The reference's standard unpreconditioned LOBPCG unless the problem is
-      // generalized, preconditioned, or iterates more vectors than requested.
-      if (B || opt.precond != "none" || opt.block > opt.nev) {
-        if (B) check_pair(A->m, B->m);
-        fe::lobpcg_gen_solve(A->m, B ? &B->m : nullptr, opt, eigenvalues, residual_norms,
-                             eigenvectors, st);
-      } else {
-        fe::lobpcg_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
-      }
-    } else if (opt.solver == "davidson") {
-      if (B || opt.precond != "none") {
-        if (B) check_pair(A->m, B->m);
-        fe::davidson_gen_solve(A->m, B ? &B->m : nullptr, opt, eigenvalues, residual_norms,
-                               eigenvectors, st);
-      } else {
-        fe::davidson_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
-      }
-    } else if (opt.solver == "krylovschur") {
-      FE_REQUIRE(B == nullptr,
-                 "KrylovSchurSolver: generalized problems need a B^{-1} factorization (out of "
-                 "scope on this backend).");
-      fe::krylov_schur_solve(A->m, opt, eigenvalues, residual_norms, eigenvectors, st);
-    } else {
-      throw fe::Error(FE_ERR_UNSUPPORTED, "solver not available on this backend: " + opt.solver);
-    }
-    const auto t1 = std::chrono::steady_clock::now();
-    st.seconds = std::chrono::duration<double>(t1 - t0).count();
-    if (stats) {
-      stats[0] = st.iterations;
-      stats[1] = st.status;
-      stats[2] = st.seconds;
-      stats[3] = st.spmm_launches;
-      stats[4] = st.fp32_iterations;
-      stats[5] = st.fp64_iterations;
-      stats[6] = st.lower;
-      stats[7] = st.upper;
-      stats[8] = st.filter_ms;
-      stats[9] = st.ortho_ms;
-      stats[10] = st.rr_ms;
-      stats[11] = st.precise_grams;
-    }
+    fe::solve_problem(A->m, B ? &B->m : nullptr, options, eigenvalues, residual_norms,
+                      eigenvectors, stats);
   });
 }
 

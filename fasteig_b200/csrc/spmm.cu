@@ -22,6 +22,9 @@
 
 #include "fe_common.cuh"
 
+#include <cmath>
+#include <mutex>
+
 #include <algorithm>
 
 namespace fe {
@@ -792,10 +795,47 @@ int read_spmm_status(bool clear) {
 static int g_spmm_mode = 0;
 void set_spmm_mode(int mode) { g_spmm_mode = mode; }
 
+template <typename T>
+void fill_uniform(T* X, int64_t ld, int64_t n, int64_t m, uint64_t seed, cudaStream_t s);
+
+// Kernel choice for a call: an explicit process-wide mode (1..3) wins; under the
+// default mode a width tuned on this operator by fe_csr_autotune (within a factor
+// of two of ncols) picks the kernel.
+std::mutex g_tune_mutex;
+
+int tuned_mode(const Csr& A, int precision, int64_t ncols) {
+  if (g_spmm_mode != 0) return g_spmm_mode;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  int best = -1;
+  double best_d = 1.0;
+  for (const auto& e : A.tuned[precision]) {
+    if (e.mode < 0 || e.ncols <= 0) continue;
+    const double d = std::fabs(std::log2(static_cast<double>(ncols) / e.ncols));
+    if (d <= best_d) {
+      best_d = d;
+      best = e.mode;
+    }
+  }
+  return best >= 0 ? best : 0;
+}
+
+template <typename T>
+void csr_spmm_mode(int mode, const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
+                   int64_t ldz, int64_t ncols, double alpha, double gamma, double beta,
+                   cudaStream_t s);
+
 // Shared entry used by the C ABI and the host solver.
 template <typename T>
 void csr_spmm(const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T* Z, int64_t ldz,
               int64_t ncols, double alpha, double gamma, double beta, cudaStream_t s) {
+  csr_spmm_mode<T>(tuned_mode(A, sizeof(T) == 4 ? 1 : 0, ncols), A, X, ldx, Y, ldy, Z, ldz, ncols,
+                   alpha, gamma, beta, s);
+}
+
+template <typename T>
+void csr_spmm_mode(int mode, const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
+                   int64_t ldz, int64_t ncols, double alpha, double gamma, double beta,
+                   cudaStream_t s) {
   FE_REQUIRE(ncols >= 0 && ncols <= 0x7fffffff, "csr_spmm: invalid column count");
   if (ncols == 0 || A.rows == 0) return;
   FE_REQUIRE(X && Y, "csr_spmm: null block pointer");
@@ -819,15 +859,15 @@ void csr_spmm(const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T*
     // Mode 0 gives each lane 8-byte vectors (up to 5 per lane, so a 320-column
     // FP32 slab needs no idle lanes and ~70 registers of loads in flight); mode 3
     // uses 16-byte vectors with at most 2 per lane.
-    if (g_spmm_mode == 0 &&
+    if (mode == 0 &&
         try_row_kernel<T, 8 / sizeof(T)>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols),
                                          T(alpha), T(gamma), T(beta), ug, ub, s, 5))
       return;
-    if (g_spmm_mode == 3 &&
+    if (mode == 3 &&
         try_row_kernel<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                                T(gamma), T(beta), ug, ub, s, 2))
       return;
-    if (g_spmm_mode == 2 && ncols * static_cast<int64_t>(sizeof(T)) >= 64 &&
+    if (mode == 2 && ncols * static_cast<int64_t>(sizeof(T)) >= 64 &&
         try_pipe<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                          T(gamma), T(beta), ug, ub, s))
       return;
@@ -842,6 +882,71 @@ void csr_spmm(const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T*
 template void csr_spmm<double>(const Csr&, const double*, int64_t, double*, int64_t,
                                const double*, int64_t, int64_t, double, double, double,
                                cudaStream_t);
+
+// Time every SpMM kernel on this operator for an n x ncols block in the Chebyshev
+// step form (Y = a A X + g X + b Z, the filter's inner loop) and record the fastest
+// in the operator's table. Returns the chosen mode.
+template <typename T>
+int autotune_spmm(Csr& A, int64_t ncols, cudaStream_t s) {
+  FE_REQUIRE(ncols >= 1 && A.rows == A.cols, "autotune: invalid block width");
+  const int64_t ld = ((ncols + 7) / 8) * 8;
+  const size_t bytes = static_cast<size_t>(A.rows) * ld * sizeof(T);
+  void *x = nullptr, *y = nullptr, *z = nullptr;
+  FE_CHECK_CUDA(cudaMallocAsync(&x, bytes, s));
+  FE_CHECK_CUDA(cudaMallocAsync(&y, bytes, s));
+  FE_CHECK_CUDA(cudaMallocAsync(&z, bytes, s));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int best = 0;
+  auto cleanup = [&] {
+    cudaFreeAsync(x, s);
+    cudaFreeAsync(y, s);
+    cudaFreeAsync(z, s);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  try {
+    fill_uniform<T>(static_cast<T*>(x), ld, A.rows, ld, 11, s);
+    fill_uniform<T>(static_cast<T*>(z), ld, A.rows, ld, 12, s);
+    FE_CHECK_CUDA(cudaEventCreate(&e0));
+    FE_CHECK_CUDA(cudaEventCreate(&e1));
+    float best_ms = 0.0f;
+    for (int mode : {0, 3, 2, 1}) {
+      auto run = [&] {
+        csr_spmm_mode<T>(mode, A, static_cast<const T*>(x), ld, static_cast<T*>(y), ld,
+                         static_cast<const T*>(z), ld, ncols, 0.25, 0.1, -1.0, s);
+      };
+      run();  // warm-up (module load, caches)
+      FE_CHECK_CUDA(cudaEventRecord(e0, s));
+      for (int r = 0; r < 3; ++r) run();
+      FE_CHECK_CUDA(cudaEventRecord(e1, s));
+      FE_CHECK_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.0f;
+      FE_CHECK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (mode == 0 || ms < best_ms) {
+        best_ms = ms;
+        best = mode;
+      }
+    }
+  } catch (...) {
+    cleanup();
+    throw;
+  }
+  cleanup();
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  auto& table = A.tuned[sizeof(T) == 4 ? 1 : 0];
+  int slot = -1;
+  for (int i = 0; i < 4 && slot < 0; ++i)
+    if (table[i].ncols == ncols || table[i].mode < 0) slot = i;
+  if (slot < 0) {
+    for (int i = 0; i < 3; ++i) table[i] = table[i + 1];
+    slot = 3;
+  }
+  table[slot].ncols = static_cast<int32_t>(ncols);
+  table[slot].mode = best;
+  return best;
+}
+template int autotune_spmm<double>(Csr&, int64_t, cudaStream_t);
+template int autotune_spmm<float>(Csr&, int64_t, cudaStream_t);
 template void csr_spmm<float>(const Csr&, const float*, int64_t, float*, int64_t, const float*,
                               int64_t, int64_t, double, double, double, cudaStream_t);
 
@@ -926,5 +1031,17 @@ extern "C" int fe_cheb_filter_f32(fe_csr_t A, float* X, float* scratch, int64_t 
   return guarded("fe_cheb_filter_f32", [&] {
     FE_REQUIRE(A, "null CSR handle");
     fe::cheb_filter<float>(A->m, X, scratch, ld, ncols, degree, c, d, fe::as_stream(stream));
+  });
+}
+
+extern "C" int fe_csr_autotune(fe_csr_t A, int64_t ncols, int32_t precision, void* stream,
+                               int32_t* mode) {
+  return fe::guarded("fe_csr_autotune", [&] {
+    FE_REQUIRE(A, "null CSR handle");
+    FE_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
+    FE_CHECK_CUDA(cudaSetDevice(A->m.device));
+    const int m = precision == 0 ? fe::autotune_spmm<double>(A->m, ncols, fe::as_stream(stream))
+                                 : fe::autotune_spmm<float>(A->m, ncols, fe::as_stream(stream));
+    if (mode) *mode = m;
   });
 }

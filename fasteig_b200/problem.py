@@ -107,6 +107,14 @@ class CsrMatrix:
     def nnz(self) -> int:
         return int(self.values.size)
 
+    def autotune(self, ncols: int, precision: str = "fp32") -> int:
+        """Pick the fastest SpMM kernel for n x ncols blocks on this operator
+        (``fe_csr_autotune``); returns the chosen kernel mode."""
+        mode = C.c_int32()
+        check(lib.fe_csr_autotune(self.handle, int(ncols), 1 if precision == "fp32" else 0, None,
+                                  C.byref(mode)))
+        return int(mode.value)
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             lib.fe_csr_destroy(self.handle)
@@ -139,7 +147,11 @@ class fasteig_problem:  # noqa: N801 - reference class name
     def is_generalized(self) -> bool:
         return self.B is not None
 
-    def solve(self, opts: Optional[fasteig_options] = None, want_vectors: bool = True) -> int:
+    def solve(self, opts: Optional[fasteig_options] = None, want_vectors: bool = True,
+              vectors_out: Optional[np.ndarray] = None) -> int:
+        """Run the solver. ``vectors_out`` (optional) is a caller-owned C-contiguous
+        float64 array of shape (nev, n) (column-major n x nev), e.g. a view of pinned
+        host memory, that receives the eigenvectors directly."""
         opts = opts or fasteig_options(self.n())
         opts.validate()
         text = opts.to_text()
@@ -148,7 +160,13 @@ class fasteig_problem:  # noqa: N801 - reference class name
         nev = opts.nev()
         vals = np.zeros(nev)
         res = np.zeros(nev)
-        vecs = np.zeros((nev, self.n())) if want_vectors else None  # column-major n x nev
+        if vectors_out is not None:
+            if (vectors_out.dtype != np.float64 or vectors_out.shape != (nev, self.n())
+                    or not vectors_out.flags["C_CONTIGUOUS"]):
+                raise ValueError("vectors_out must be a C-contiguous float64 (nev, n) array")
+            vecs = vectors_out
+        else:
+            vecs = np.empty((nev, self.n())) if want_vectors else None  # column-major n x nev
         stats = np.zeros(12)
         check(lib.fe_solve(self.A.handle, self.B.handle if self.B is not None else None,
                            text.encode(), vals.ctypes.data, res.ctypes.data,
@@ -223,3 +241,66 @@ def batch_krylov_schur(problems, nevs, opts: Optional[fasteig_options] = None,
         d["status"] = int(st)
     return out, dict(seconds=float(stats[0]), rounds=int(stats[1]), steps=int(stats[2]),
                      graph_launches=int(stats[3]))
+
+
+class Server:
+    """Request server over ``fe_server_*``: requests (operator + options) are
+    admitted as worker slots and device memory free up, run concurrently on their
+    own streams, and are collected with ``wait``. Keep each request's CsrMatrix
+    alive until it is collected."""
+
+    PENDING = 1
+
+    def __init__(self, slots: int = 4, memory_budget_bytes: int = 0, device: int = 0):
+        h = C.c_void_p()
+        check(lib.fe_server_create(int(device), int(slots), int(memory_budget_bytes), C.byref(h)))
+        self.handle = h
+        self._nev = {}
+        self._keep = {}
+
+    def submit(self, A: CsrMatrix, opts: fasteig_options, B: Optional[CsrMatrix] = None,
+               solver: Optional[str] = None) -> int:
+        opts.validate()
+        text = opts.to_text()
+        if solver is not None:
+            text += f"\nsolver={solver}"
+        rid = C.c_int64()
+        check(lib.fe_server_submit(self.handle, A.handle, B.handle if B is not None else None,
+                                   text.encode(), C.byref(rid)))
+        self._nev[rid.value] = opts.nev()
+        self._keep[rid.value] = (A, B)
+        return rid.value
+
+    def wait(self, request_id: int, timeout: float = -1.0):
+        """Result dict, or None if the request is still pending after ``timeout`` s."""
+        nev = self._nev[request_id]
+        vals, res, stats = np.zeros(nev), np.zeros(nev), np.zeros(18)
+        rc = lib.fe_server_wait(self.handle, int(request_id), float(timeout), vals.ctypes.data,
+                                res.ctypes.data, stats.ctypes.data)
+        if rc == self.PENDING:
+            return None
+        self._nev.pop(request_id)
+        self._keep.pop(request_id)
+        check(rc)
+        return dict(eigenvalues=vals, residual_norms=res, iterations=int(stats[0]),
+                    status=int(stats[1]), solve_seconds=float(stats[2]),
+                    queued_s=float(stats[12]), running_s=float(stats[13]),
+                    latency_s=float(stats[14]), admitted_bytes=int(stats[15]),
+                    start_s=float(stats[16]), end_s=float(stats[17]))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            check(lib.fe_server_destroy(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -37,6 +37,7 @@ extern "C" {
 #define FE_ERR_NONFINITE -4   /* non-finite Ritz data / residuals */
 #define FE_ERR_ALLOC -5       /* device allocation failure */
 #define FE_ERR_UNSUPPORTED -6 /* option not supported by this backend */
+#define FE_PENDING 1          /* fe_server_wait: request not finished within the timeout */
 
 typedef struct fe_csr* fe_csr_t;
 
@@ -175,6 +176,13 @@ int fe_device_status(int32_t* status, int32_t clear);
  * pipelined kernel where it applies, 3 = row-batched kernel with narrower
  * column panels. */
 int fe_set_spmm_kernel(int32_t mode);
+/* SpMM autotuner: times every SpMM kernel on operator A for an n-by-ncols block
+ * in the Chebyshev-step form (precision 0 = FP64, 1 = FP32) on `stream` and
+ * records the fastest on the handle (up to four widths per precision); later
+ * SpMMs of that precision within a factor of two of a tuned width use it while
+ * the process-wide mode is the default 0. Writes the chosen mode to *mode (may
+ * be NULL). Not to be called while solves on the same handle are running. */
+int fe_csr_autotune(fe_csr_t A, int64_t ncols, int32_t precision, void* stream, int32_t* mode);
 /* FP64 Gram / rotation kernel selection for all later calls in the process:
  * 0 = default (FP64 tensor-core mma.sync.m8n8k4 kernels with a cp.async ring),
  * 1 = SIMT FP64-FMA kernels. Both accumulate every output in FP64; results
@@ -271,6 +279,35 @@ int fe_batch_krylov_schur(int32_t count, const fe_csr_t* A, const int64_t* nev,
                           const char* options, double* eigenvalues, double* residual_norms,
                           double* eigenvectors, int32_t* iterations, int32_t* status,
                           double* stats);
+
+/* ---------------------------------------------------------------------
+ * Request server (extension; the reference's fasteig_problem::solve,
+ * src/fasteig_problem.cpp:340-437, is one blocking solve per call).
+ * A server owns `slots` worker threads on `device`. Submitted requests are
+ * admitted in arrival order as soon as a slot is free and the request's device
+ * memory bound (its blocks and workspaces) fits the budget
+ * (memory_budget_bytes, or 90 % of the free memory at creation when <= 0); a
+ * request larger than the budget runs alone. Each admitted request runs the
+ * fe_solve path on its own stream, so concurrent requests overlap on the GPU
+ * and each result is the one fe_solve gives alone. The caller keeps A (and B)
+ * alive until the request is collected.
+ *   fe_server_submit: options as for fe_solve; returns a request id.
+ *   fe_server_wait: blocks (timeout < 0) or up to timeout seconds; FE_PENDING
+ *     if still queued or running, else the solve's status. On completion
+ *     writes eigenvalues[nev], residual_norms[nev] and stats[18] (the 12
+ *     fe_solve stats, then seconds queued, seconds running, latency from
+ *     submission, admitted memory bytes, start and end in seconds since the
+ *     server was created) and forgets the request.
+ *   fe_server_destroy: finishes running requests, drops queued ones.
+ * ------------------------------------------------------------------- */
+typedef struct fe_server* fe_server_t;
+int fe_server_create(int32_t device, int32_t slots, int64_t memory_budget_bytes,
+                     fe_server_t* out);
+int fe_server_submit(fe_server_t server, fe_csr_t A, fe_csr_t B, const char* options,
+                     int64_t* request_id);
+int fe_server_wait(fe_server_t server, int64_t request_id, double timeout_seconds,
+                   double* eigenvalues, double* residual_norms, double* stats);
+int fe_server_destroy(fe_server_t server);
 
 #ifdef __cplusplus
 }

@@ -289,3 +289,26 @@ def test_potrf_reports_rank_loss_on_device():
     _, info = ops.potrf_upper(torch.from_numpy(G).cuda())
     torch.cuda.synchronize()
     assert int(info.item()) == 2
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_autotuned_spmm_matches_oracle(dtype):
+    """fe_csr_autotune records the fastest kernel for a block width; SpMMs of that
+    width then use it and keep the componentwise bound."""
+    from fasteig_b200 import matrices as M
+    from fasteig_b200 import ops
+    from oracle import oracle as O
+    H = M.laplacian_wells(20, wells=4, seed=5)
+    A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
+    dA = dev_csr(A)
+    mode = dA.autotune(96, "fp32" if dtype == torch.float32 else "fp64")
+    assert mode in (0, 1, 2, 3)
+    X = block(H.n, 96, dtype, 41)
+    Y = torch.zeros_like(X)
+    X64 = X.double().cpu().numpy()
+    ops.spmm(dA, X, Y, -0.5, 0.0)
+    torch.cuda.synchronize()
+    ref = -0.5 * (A.scipy() @ X64)
+    scale = 0.5 * (absA(A) @ np.abs(X64))
+    tol = 1e-13 if dtype == torch.float64 else 4e-6
+    assert np.all(np.abs(Y.double().cpu().numpy() - ref) <= tol * scale + 1e-300)
