@@ -142,13 +142,13 @@ def run_batch_ks(a):
         assert o.set(k, v), k
     for _ in range(max(0, a.warmup)):
         fe.batch_krylov_schur(dev, nevs, o)
-    times, conv, rounds = [], 0, 0
+    times, conv, rounds, steps = [], 0, 0, 0
     for _ in range(a.steps):
         t = time.perf_counter()
         out, st = fe.batch_krylov_schur(dev, nevs, o)
         times.append(time.perf_counter() - t)
         conv = sum(int((r["residual_norms"] <= a.tol).sum()) for r in out)
-        rounds = st["rounds"]
+        rounds, steps = st["rounds"], st["steps"]
     sec = sum(times) / len(times)
     n_total = sum(H.n for H, _ in probs)
     line = {"metric": METRIC, "value": round(conv / sec, 3), "unit": UNIT, "n_gpus": 1,
@@ -159,7 +159,7 @@ def run_batch_ks(a):
                        "problems": a.batch_count, "rows_total": n_total,
                        "pairs_requested": int(sum(nevs)), "tol": a.tol,
                        "solver": "KrylovSchur (batched lockstep, graph per Lanczos step)"},
-            "converged_pairs": conv, "restart_rounds": rounds,
+            "converged_pairs": conv, "restart_rounds": rounds, "lanczos_steps": steps,
             "latency_s": {"p50": sorted(times)[len(times) // 2], "max": max(times)},
             "csr_upload_s": round(upload_s, 2)}
     print(json.dumps(line), flush=True)
@@ -177,10 +177,13 @@ def run_generalized(a):
     K, Mm = M.stiffness_mass_27pt(side, seed=0)
     dK = fe.CsrMatrix(K.n, K.rowptr, K.colind, K.values)
     dM = fe.CsrMatrix(Mm.n, Mm.rowptr, Mm.colind, Mm.values)
-    for solver in ("LOBPCG", "Davidson"):
+    # Both solvers iterate a block of 96 vectors for the 64 wanted pairs: the extra
+    # vectors cut the iteration count several-fold on this pair (LOBPCG 2,885 -> 184
+    # iterations); Davidson keeps up to 4 such blocks in its basis.
+    for solver, extra in (("LOBPCG", dict(block=96)), ("Davidson", dict(block=96, maxblks=4))):
         o = fe.fasteig_options()
-        for k, v in dict(solver=solver, nev=64, which="SR", tol=a.tol, maxiter=3000, seed=1,
-                         precond="jacobi", maxblks=4, init="device").items():
+        for k, v in dict(dict(solver=solver, nev=64, which="SR", tol=a.tol, maxiter=3000, seed=1,
+                              precond="jacobi", init="device"), **extra).items():
             assert o.set(k, v), k
         p = fe.fasteig_problem(dK, dM, solver=solver)
         p.solve(o, want_vectors=False)
@@ -190,9 +193,9 @@ def run_generalized(a):
                           "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": round(sec * 1e3, 1),
                           "higher_is_better": True, "dtype": "f64", "data": "synthetic",
                           "impl": "b200",
-                          "config": {"workload": f"generalized_27pt_{side}cube_{solver.lower()}",
-                                     "n": K.n, "nnz_K": K.nnz, "nev": 64, "tol": a.tol,
-                                     "precond": "jacobi", "maxblks": 4},
+                          "config": dict({"workload": f"generalized_27pt_{side}cube_{solver.lower()}",
+                                          "n": K.n, "nnz_K": K.nnz, "nev": 64, "tol": a.tol,
+                                          "precond": "jacobi"}, **extra),
                           "converged_pairs": conv, "iterations": p.last_iterations(),
                           "spmm_launches": p.stats["spmm_launches"]}), flush=True)
     return 0
@@ -229,7 +232,8 @@ def run_serving(a):
             kv.update(degree=16, bounds="ritz", amplification=1e6, maxiter=300,
                       precision="mixed" if tol >= 1e-6 else "fp64")
         else:
-            kv.update(maxiter=400)
+            # a block a quarter wider than nev: far fewer iterations for the last pairs
+            kv.update(maxiter=600, block=min(H.n, nev + max(4, nev // 4)))
         for key, v in kv.items():
             assert o.set(key, v), key
         return A, o, nev, tol, H.n, st, solver
@@ -553,13 +557,19 @@ def main():
         rp_h, ci_h = pin(H.rowptr.astype(np.int32)), pin(H.colind.astype(np.int32))
         va_h = pin(H.values.astype(np.float64))
         vec_h = torch.empty((a.nev, H.n), dtype=torch.float64).pin_memory().numpy()
+
+        def e2e_step():
+            dA2 = fe.CsrMatrix(H.n, rp_h, ci_h, va_h)
+            p2 = fe.fasteig_problem(dA2, solver="Chebyshev")
+            p2.solve(opts, vectors_out=vec_h)
+            dA2.close()
+            return p2
+
+        e2e_step()  # warm-up of the host-buffer path (first touch of pool and pinned memory)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        dA2 = fe.CsrMatrix(H.n, rp_h, ci_h, va_h)
-        p2 = fe.fasteig_problem(dA2, solver="Chebyshev")
-        p2.solve(opts, vectors_out=vec_h)
+        p2 = e2e_step()
         t_e2e = time.perf_counter() - t0
-        dA2.close()
         e2e_pairs = int((p2.residual_norms() <= a.tol).sum())
         h2d = rp_h.nbytes + ci_h.nbytes + va_h.nbytes
         d2h = 8 * a.nev * (H.n + 2)

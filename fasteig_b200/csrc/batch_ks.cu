@@ -143,11 +143,65 @@ __global__ void bks_dots_finish_kernel(BatchLayout L, BatchState S, const double
   }
 }
 
-// dst[r] = src[r] - V[r, :col+1] h_p (active problems; dst may be src).
-__global__ void __launch_bounds__(kBT) bks_update_kernel(BatchLayout L, BatchState S,
-                                                         const double* __restrict__ V, int64_t ldv,
-                                                         const double* __restrict__ h,
-                                                         const double* src, double* dst) {
+// First Gram-Schmidt update fused with the second pass's reduction:
+// f[r] = w[r] - V[r, :col+1] h1_p, and part[c * M + j] = sum over chunk rows of V[r, j] f[r].
+__global__ void __launch_bounds__(kBT) bks_update_dots_kernel(BatchLayout L, BatchState S,
+                                                              const double* __restrict__ V,
+                                                              int64_t ldv,
+                                                              const double* __restrict__ h,
+                                                              const double* __restrict__ src,
+                                                              double* __restrict__ dst,
+                                                              double* __restrict__ part) {
+  __shared__ double red[kBT / 32][kBatchMaxDim];
+  const int c = blockIdx.x;
+  const int p = L.c_prob[c];
+  if (!S.active[p]) return;
+  const int ncols = S.col[p] + 1;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  double hr[kLaneCols], acc[kLaneCols];
+#pragma unroll
+  for (int t = 0; t < kLaneCols; ++t) {
+    const int j = lane + 32 * t;
+    hr[t] = j < ncols ? h[static_cast<int64_t>(p) * L.M + j] : 0.0;
+    acc[t] = 0.0;
+  }
+  const int64_t r0 = L.c_row0[c];
+  const int rows = L.c_rows[c];
+  for (int i = warp; i < rows; i += kBT / 32) {
+    const int64_t r = r0 + i;
+    const double* vr = V + r * ldv;
+    double v[kLaneCols];
+    double s = 0.0;
+#pragma unroll
+    for (int t = 0; t < kLaneCols; ++t) {
+      const int j = lane + 32 * t;
+      v[t] = j < ncols ? vr[j] : 0.0;
+      s = fma(v[t], hr[t], s);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double fr = src[r] - s;
+    if (lane == 0) dst[r] = fr;
+#pragma unroll
+    for (int t = 0; t < kLaneCols; ++t) acc[t] = fma(v[t], fr, acc[t]);
+  }
+#pragma unroll
+  for (int t = 0; t < kLaneCols; ++t) red[warp][lane + 32 * t] = acc[t];
+  __syncthreads();
+  for (int j = threadIdx.x; j < ncols; j += kBT) {
+    double sum = 0.0;
+    for (int w = 0; w < kBT / 32; ++w) sum += red[w][j];
+    part[static_cast<int64_t>(c) * L.M + j] = sum;
+  }
+}
+
+// Second Gram-Schmidt update fused with the norm: f[r] -= V[r, :col+1] h2_p and
+// part1[c] = sum over chunk rows of f[r]^2.
+__global__ void __launch_bounds__(kBT) bks_update_sumsq_kernel(BatchLayout L, BatchState S,
+                                                               const double* __restrict__ V,
+                                                               int64_t ldv,
+                                                               const double* __restrict__ h,
+                                                               double* __restrict__ f) {
+  __shared__ double red[kBT / 32];
   const int c = blockIdx.x;
   const int p = L.c_prob[c];
   if (!S.active[p]) return;
@@ -161,6 +215,7 @@ __global__ void __launch_bounds__(kBT) bks_update_kernel(BatchLayout L, BatchSta
   }
   const int64_t r0 = L.c_row0[c];
   const int rows = L.c_rows[c];
+  double acc = 0.0;
   for (int i = warp; i < rows; i += kBT / 32) {
     const int64_t r = r0 + i;
     const double* vr = V + r * ldv;
@@ -171,7 +226,18 @@ __global__ void __launch_bounds__(kBT) bks_update_kernel(BatchLayout L, BatchSta
       if (j < ncols) s = fma(vr[j], hr[t], s);
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) dst[r] = src[r] - s;
+    const double fr = f[r] - s;
+    if (lane == 0) {
+      f[r] = fr;
+      acc = fma(fr, fr, acc);
+    }
+  }
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sum = 0.0;
+    for (int w = 0; w < kBT / 32; ++w) sum += red[w];
+    S.part1[c] = sum;
   }
 }
 
@@ -210,7 +276,8 @@ __global__ void __launch_bounds__(kBT) bks_jacobi_kernel(BatchLayout L, const do
                                                          const int32_t* __restrict__ mdim,
                                                          const int32_t* __restrict__ todo,
                                                          double* __restrict__ W,
-                                                         double* __restrict__ Z) {
+                                                         double* __restrict__ Z,
+                                                         double* __restrict__ Zlast) {
   extern __shared__ double sh[];
   const int p = blockIdx.x;
   if (!todo[p]) return;
@@ -310,7 +377,48 @@ __global__ void __launch_bounds__(kBT) bks_jacobi_kernel(BatchLayout L, const do
       if (dj < di || (dj == di && j < i)) ++rank;
     }
     W[p * M + rank] = di;
+    Zlast[p * M + rank] = Q[(m - 1) + i * ld];
     for (int r = 0; r < m; ++r) Z[p * M * M + r + static_cast<int64_t>(rank) * M] = Q[r + i * ld];
+  }
+}
+
+// Restart bookkeeping on the device, one CTA per problem: rotation coefficients
+// C_p[:, j] = Z_p[:, idx_p[j]] for j < max(keep, keepY), and for restarting
+// problems (keep > 0) the new projected matrix T_p: diag(lam_s[:keep]) with the
+// coupling row/column at index keep (CpuLanczosWorkspace::prepare_krylov_schur_restart,
+// src/core/LanczosWorkspace.cpp:94-107).
+__global__ void __launch_bounds__(kBT) bks_restart_kernel(BatchLayout L,
+                                                          const int32_t* __restrict__ mdim,
+                                                          const int32_t* __restrict__ idx,
+                                                          const int32_t* __restrict__ keep,
+                                                          const int32_t* __restrict__ keepY,
+                                                          const double* __restrict__ diag,
+                                                          const double* __restrict__ coup,
+                                                          const double* __restrict__ Z,
+                                                          double* __restrict__ C,
+                                                          double* __restrict__ T) {
+  const int p = blockIdx.x;
+  const int kp = keep[p], ky = keepY[p];
+  const int kc = max(kp, ky);
+  if (kc <= 0) return;
+  const int m = mdim[p];
+  const int64_t M = L.M;
+  const double* Zp = Z + p * M * M;
+  double* Cp = C + p * M * M;
+  const int32_t* ip = idx + p * M;
+  for (int e = threadIdx.x; e < m * kc; e += kBT) {
+    const int i = e % m, j = e / m;
+    Cp[i + j * M] = Zp[i + static_cast<int64_t>(ip[j]) * M];
+  }
+  if (kp > 0) {
+    double* Tp = T + p * M * M;
+    for (int e = threadIdx.x; e < M * M; e += kBT) Tp[e] = 0.0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < kp; j += kBT) {
+      Tp[j + j * M] = diag[p * M + j];
+      Tp[kp + j * M] = coup[p * M + j];
+      Tp[j + kp * M] = coup[p * M + j];
+    }
   }
 }
 
@@ -453,8 +561,7 @@ void bks_lanczos_step(const BatchLayout& L, const BatchState& S, const Csr& A, d
                       int64_t ldv, double* f, double* q, double* w, cudaStream_t s) {
   const unsigned pc = static_cast<unsigned>(L.num_chunks);
   const unsigned pp = static_cast<unsigned>((L.num_problems + 127) / 128);
-  bks_sumsq_kernel<<<pc, kBT, 0, s>>>(L, f, S.part1);
-  check_launch("bks_sumsq_kernel");
+  // part1 holds the chunk sums of f^2 on entry (bks_init_norm or the previous step).
   bks_begin_kernel<<<pp, 128, 0, s>>>(L, S);
   check_launch("bks_begin_kernel");
   bks_store_kernel<<<pc, kBT, 0, s>>>(L, S, f, q, V, ldv);
@@ -464,18 +571,19 @@ void bks_lanczos_step(const BatchLayout& L, const BatchState& S, const Csr& A, d
   check_launch("bks_dots_kernel");
   bks_dots_finish_kernel<<<static_cast<unsigned>(L.num_problems), 128, 0, s>>>(L, S, S.part, S.h1);
   check_launch("bks_dots_finish_kernel");
-  bks_update_kernel<<<pc, kBT, 0, s>>>(L, S, V, ldv, S.h1, w, f);
-  check_launch("bks_update_kernel");
-  bks_dots_kernel<<<pc, kBT, 0, s>>>(L, S, V, ldv, f, S.part);
-  check_launch("bks_dots_kernel");
+  bks_update_dots_kernel<<<pc, kBT, 0, s>>>(L, S, V, ldv, S.h1, w, f, S.part);
+  check_launch("bks_update_dots_kernel");
   bks_dots_finish_kernel<<<static_cast<unsigned>(L.num_problems), 128, 0, s>>>(L, S, S.part, S.h2);
   check_launch("bks_dots_finish_kernel");
-  bks_update_kernel<<<pc, kBT, 0, s>>>(L, S, V, ldv, S.h2, f, f);
-  check_launch("bks_update_kernel");
-  bks_sumsq_kernel<<<pc, kBT, 0, s>>>(L, f, S.part1);
-  check_launch("bks_sumsq_kernel");
+  bks_update_sumsq_kernel<<<pc, kBT, 0, s>>>(L, S, V, ldv, S.h2, f);
+  check_launch("bks_update_sumsq_kernel");
   bks_end_kernel<<<pp, 128, 0, s>>>(L, S);
   check_launch("bks_end_kernel");
+}
+
+void bks_init_norm(const BatchLayout& L, const BatchState& S, const double* f, cudaStream_t s) {
+  bks_sumsq_kernel<<<static_cast<unsigned>(L.num_chunks), kBT, 0, s>>>(L, f, S.part1);
+  check_launch("bks_sumsq_kernel");
 }
 
 size_t bks_jacobi_smem(int m) {
@@ -484,12 +592,21 @@ size_t bks_jacobi_smem(int m) {
 }
 
 void bks_jacobi(const BatchLayout& L, const double* T, const int32_t* mdim, const int32_t* todo,
-                int max_m, double* W, double* Z, cudaStream_t s) {
+                int max_m, double* W, double* Z, double* Zlast, cudaStream_t s) {
   const size_t smem = bks_jacobi_smem(max_m);
   FE_CHECK_CUDA(cudaFuncSetAttribute(bks_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
-  bks_jacobi_kernel<<<static_cast<unsigned>(L.num_problems), kBT, smem, s>>>(L, T, mdim, todo, W, Z);
+  bks_jacobi_kernel<<<static_cast<unsigned>(L.num_problems), kBT, smem, s>>>(L, T, mdim, todo, W, Z,
+                                                                          Zlast);
   check_launch("bks_jacobi_kernel");
+}
+
+void bks_restart(const BatchLayout& L, const int32_t* mdim, const int32_t* idx,
+                 const int32_t* keep, const int32_t* keepY, const double* diag,
+                 const double* coup, const double* Z, double* C, double* T, cudaStream_t s) {
+  bks_restart_kernel<<<static_cast<unsigned>(L.num_problems), kBT, 0, s>>>(L, mdim, idx, keep, keepY,
+                                                                        diag, coup, Z, C, T);
+  check_launch("bks_restart_kernel");
 }
 
 void bks_rotate(const BatchLayout& L, const double* V, int64_t ldv, const double* C,

@@ -383,7 +383,7 @@ template void gram<float>(const float*, int64_t, const float*, int64_t, int64_t,
 
 template <typename T>
 void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t ldy, int64_t n,
-            int64_t k, int64_t m, double alpha, double beta, cudaStream_t s) {
+            int64_t k, int64_t m, double alpha, double beta, cudaStream_t s, bool upper_tri) {
   FE_REQUIRE(n >= 0 && k >= 0 && m >= 0, "rotate: negative dimension");
   if (n == 0 || m == 0) return;
   FE_REQUIRE(Y && ldy >= m, "rotate: invalid output block");
@@ -398,7 +398,7 @@ void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t
              "rotate: X and Y overlap");
   if constexpr (std::is_same_v<T, double>) {
     if (g_f64_gemm_mode == 0) {
-      rotate_dmma(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, s);
+      rotate_dmma(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, s, upper_tri);
       return;
     }
   }
@@ -418,9 +418,9 @@ void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t
 }
 
 template void rotate<double>(const double*, int64_t, const double*, int64_t, double*, int64_t,
-                             int64_t, int64_t, int64_t, double, double, cudaStream_t);
+                             int64_t, int64_t, int64_t, double, double, cudaStream_t, bool);
 template void rotate<float>(const float*, int64_t, const double*, int64_t, float*, int64_t,
-                            int64_t, int64_t, int64_t, double, double, cudaStream_t);
+                            int64_t, int64_t, int64_t, double, double, cudaStream_t, bool);
 
 // Bound valid for every call with n' <= n and m' <= m (chunks never exceed the
 // target count nor one per 64 rows).
@@ -517,7 +517,8 @@ extern "C" int fe_rotate_f64(const double* X, int64_t ldx, const double* C, int6
                              double* Y, int64_t ldy, int64_t n, int64_t k, int64_t m,
                              double alpha, double beta, void* stream) {
   return guarded("fe_rotate_f64", [&] {
-    fe::rotate<double>(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, fe::as_stream(stream));
+    fe::rotate<double>(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, fe::as_stream(stream),
+                       false);
   });
 }
 
@@ -525,7 +526,8 @@ extern "C" int fe_rotate_f32(const float* X, int64_t ldx, const double* C, int64
                              int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha,
                              double beta, void* stream) {
   return guarded("fe_rotate_f32", [&] {
-    fe::rotate<float>(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, fe::as_stream(stream));
+    fe::rotate<float>(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, fe::as_stream(stream),
+                      false);
   });
 }
 

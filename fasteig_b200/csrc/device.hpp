@@ -28,9 +28,12 @@ size_t gram_workspace_bytes(int64_t n, int64_t k, int64_t m);
 template <typename T>
 void gram(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k, int64_t m,
           double* G, int64_t ldg, void* ws, size_t ws_bytes, cudaStream_t s);
+// upper_tri: C is upper triangular (zero below its diagonal), so the products of
+// its zero rows may be skipped.
 template <typename T>
 void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t ldy, int64_t n,
-            int64_t k, int64_t m, double alpha, double beta, cudaStream_t s);
+            int64_t k, int64_t m, double alpha, double beta, cudaStream_t s,
+            bool upper_tri = false);
 size_t residual_workspace_bytes(int64_t n, int64_t m);
 template <typename T>
 void residual_norms(const T* AX, const T* X, const T* BX, int64_t ld, int64_t n, int64_t m,
@@ -200,7 +203,7 @@ void gram_tc(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n
 size_t tc_rotate_workspace_bytes(int64_t k, int64_t m);
 void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float* Y, int64_t ldy,
                int64_t n, int64_t k, int64_t m, double alpha, double beta, void* ws,
-               size_t ws_bytes, cudaStream_t s);
+               size_t ws_bytes, cudaStream_t s, bool upper_tri = false);
 int read_tc_status(bool clear);
 }  // namespace fe
 
@@ -240,8 +243,12 @@ struct BatchState {
 
 void bks_lanczos_step(const BatchLayout& L, const BatchState& S, const Csr& A, double* V,
                       int64_t ldv, double* f, double* q, double* w, cudaStream_t s);
+void bks_init_norm(const BatchLayout& L, const BatchState& S, const double* f, cudaStream_t s);
 void bks_jacobi(const BatchLayout& L, const double* T, const int32_t* mdim, const int32_t* todo,
-                int max_m, double* W, double* Z, cudaStream_t s);
+                int max_m, double* W, double* Z, double* Zlast, cudaStream_t s);
+void bks_restart(const BatchLayout& L, const int32_t* mdim, const int32_t* idx,
+                 const int32_t* keep, const int32_t* keepY, const double* diag,
+                 const double* coup, const double* Z, double* C, double* T, cudaStream_t s);
 void bks_rotate(const BatchLayout& L, const double* V, int64_t ldv, const double* C,
                 const int32_t* mdim, const int32_t* keep, int max_m, int max_keep, double* dst,
                 int64_t ldd, cudaStream_t s);

@@ -172,7 +172,7 @@ template <int VEC>
 __global__ void __launch_bounds__(kRThreads)
 rotate_dmma_kernel(const double* __restrict__ X, int64_t ldx, const double* __restrict__ C,
                    int64_t ldc, double* __restrict__ Y, int64_t ldy, int64_t n, int k, int m,
-                   double alpha, double beta, int use_beta) {
+                   double alpha, double beta, int use_beta, int upper_tri) {
   extern __shared__ double smem[];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -181,7 +181,10 @@ rotate_dmma_kernel(const double* __restrict__ X, int64_t ldx, const double* __re
   const int wc = (warp >> 2) * 32;
   const int j0 = blockIdx.x * kRCols;
   const int64_t r0 = static_cast<int64_t>(blockIdx.y) * kRRows;
-  const int stages = (k + kRK - 1) / kRK;
+  // Upper-triangular C (CholQR's R^-1): rows k >= j0 + kRCols are zero for this
+  // tile's columns, so those stages are skipped.
+  const int k_eff = upper_tri ? min(k, j0 + kRCols) : k;
+  const int stages = (k_eff + kRK - 1) / kRK;
 
   auto xs = [&](int buf) { return smem + static_cast<size_t>(buf) * kRStage; };
   auto cs = [&](int buf) { return xs(buf) + kRRows * kRXLd; };
@@ -289,7 +292,7 @@ void gram_partial_dmma(const double* X, int64_t ldx, const double* Y, int64_t ld
 
 void rotate_dmma(const double* X, int64_t ldx, const double* C, int64_t ldc, double* Y,
                  int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
-                 cudaStream_t s) {
+                 cudaStream_t s, bool upper_tri) {
   const bool vec2 = aligned16(X) && ldx % 2 == 0 && k % 2 == 0;
   const int64_t row_tiles = (n + kRRows - 1) / kRRows;
   const int64_t col_tiles = (m + kRCols - 1) / kRCols;
@@ -303,7 +306,7 @@ void rotate_dmma(const double* X, int64_t ldx, const double* C, int64_t ldc, dou
     const int64_t r_off = base * kRRows;
     kern<<<grid, kRThreads, kRSmem, s>>>(X + r_off * ldx, ldx, C, ldc, Y + r_off * ldy, ldy,
                                          n - r_off, static_cast<int>(k), static_cast<int>(m),
-                                         alpha, beta, beta != 0.0 ? 1 : 0);
+                                         alpha, beta, beta != 0.0 ? 1 : 0, upper_tri ? 1 : 0);
     check_launch("rotate_dmma_kernel");
   }
 }

@@ -116,7 +116,7 @@ void gram_partial_dmma(const double* X, int64_t ldx, const double* Y, int64_t ld
                        bool symmetric, double* partial, cudaStream_t s);
 void rotate_dmma(const double* X, int64_t ldx, const double* C, int64_t ldc, double* Y,
                  int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
-                 cudaStream_t s);
+                 cudaStream_t s, bool upper_tri = false);
 
 }  // namespace fe
 

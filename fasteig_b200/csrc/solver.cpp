@@ -424,14 +424,16 @@ void gram_block(SmallState& sm, const T* X, int64_t ldx, const T* Y, int64_t ldy
 // Y = alpha X C + beta Y (C: FP64 column-major with leading dimension cap).
 template <typename T>
 void rotate_block(SmallState& sm, const T* X, int64_t ldx, const double* C, T* Y, int64_t ldy,
-                  int64_t n, int64_t k, int64_t m, double alpha, double beta, cudaStream_t s) {
+                  int64_t n, int64_t k, int64_t m, double alpha, double beta, cudaStream_t s,
+                  bool upper_tri = false) {
   if constexpr (sizeof(T) == 4) {
     if (sm.tensor_cores && tc_ok(X, ldx) && n >= 128) {
-      rotate_tc(X, ldx, C, sm.cap, Y, ldy, n, k, m, alpha, beta, sm.cws.get(), sm.cws.bytes(), s);
+      rotate_tc(X, ldx, C, sm.cap, Y, ldy, n, k, m, alpha, beta, sm.cws.get(), sm.cws.bytes(), s,
+                upper_tri);
       return;
     }
   }
-  rotate<T>(X, ldx, C, sm.cap, Y, ldy, n, k, m, alpha, beta, s);
+  rotate<T>(X, ldx, C, sm.cap, Y, ldy, n, k, m, alpha, beta, s, upper_tri);
 }
 
 // Cholesky QR of src (n x k) into dst: G = src^T src, R = chol(G), dst = src R^{-1}
@@ -457,7 +459,8 @@ void cholqr(Context& ctx, SmallState& sm, const T* src, int64_t lds, T* dst, int
     }
   }
   trinv_upper(G, sm.cap, sm.Rinv.as<double>(), sm.cap, k, s);
-  rotate_block<T>(sm, src, lds, sm.Rinv.as<double>(), dst, ldd, n, k, k, 1.0, 0.0, s);
+  rotate_block<T>(sm, src, lds, sm.Rinv.as<double>(), dst, ldd, n, k, k, 1.0, 0.0, s,
+                  /*upper_tri=*/true);
 }
 
 // Filter scaling (src/ChebyshevSolver.cpp:231-239) for a damped interval [cutoff, upper]
@@ -491,6 +494,22 @@ struct ChebLoop {
                std::vector<double>& rel, int32_t* info_host, Stats& st) {
     cudaStream_t s = ctx.stream;
     const int64_t active = sub - locked;
+    // The filter's SpMM and the deflation's tensor-core rotation want a block that
+    // starts 16-byte aligned and spans whole 16-byte vectors. When V's active
+    // columns [locked, sub) do not, they are staged in S, padded with zero columns
+    // to a whole number of vectors (the padding never mixes into real columns),
+    // filtered and deflated there, and copied back.
+    const int64_t vw = 16 / static_cast<int64_t>(sizeof(T));
+    const bool in_place = locked % vw == 0 && active % vw == 0;
+    const int64_t act_pad = ((active + vw - 1) / vw) * vw;
+    auto stage_active = [&] {
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(b.S.data(), b.S.ld * sizeof(T), b.V.col(locked),
+                                      b.V.ld * sizeof(T), active * sizeof(T), n,
+                                      cudaMemcpyDeviceToDevice, s));
+      if (act_pad > active)
+        FE_CHECK_CUDA(cudaMemset2DAsync(b.S.col(active), b.S.ld * sizeof(T), 0,
+                                        (act_pad - active) * sizeof(T), n, s));
+    };
     FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, 4 * sizeof(int32_t), s));
     ev.record(0, s);
     // 1. Filter Y = T_degree(c*op + d*I) X_active, in place on V's active columns.
@@ -499,33 +518,34 @@ struct ChebLoop {
       const double d = -(upper + cutoff) / (upper - cutoff);
       if (!std::isfinite(c) || !std::isfinite(d))
         throw Error(FE_ERR_NONFINITE, "ChebyshevSolver: invalid filter scaling.");
-      // The operator is sign*A: fold the sign into c. The active columns start at
-      // column `locked`; when that is not 16-byte aligned the filter runs on an
-      // aligned copy in S (with Q as its second buffer) so the SpMM keeps its
-      // vectorised path, and the result is copied back.
-      if ((locked * static_cast<int64_t>(sizeof(T))) % 16 == 0) {
+      // The operator is sign*A: fold the sign into c.
+      if (in_place) {
         filter(b.V.col(locked), b.V.ld, b.S.data(), b.S.ld, active, sign * c, d);
       } else {
-        FE_CHECK_CUDA(cudaMemcpy2DAsync(b.S.data(), b.S.ld * sizeof(T), b.V.col(locked),
-                                        b.V.ld * sizeof(T), active * sizeof(T), n,
-                                        cudaMemcpyDeviceToDevice, s));
-        filter(b.S.data(), b.S.ld, b.Q.data(), b.Q.ld, active, sign * c, d);
-        FE_CHECK_CUDA(cudaMemcpy2DAsync(b.V.col(locked), b.V.ld * sizeof(T), b.S.data(),
-                                        b.S.ld * sizeof(T), active * sizeof(T), n,
-                                        cudaMemcpyDeviceToDevice, s));
+        stage_active();
+        filter(b.S.data(), b.S.ld, b.Q.data(), b.Q.ld, act_pad, sign * c, d);
       }
       st.spmm_launches += static_cast<double>(degree);
+    } else if (!in_place) {
+      stage_active();
     }
     ev.record(1, s);
     // 2. Deflate against locked vectors with two-pass block Gram-Schmidt
-    // (block_gram_schmidt, src/core/Orthogonalization.cpp:482-527).
+    // (block_gram_schmidt, src/core/Orthogonalization.cpp:482-527), on the
+    // aligned block (V's active columns, or their staged copy in S).
+    T* Y = in_place ? b.V.col(locked) : b.S.data();
+    const int64_t ldy = in_place ? b.V.ld : b.S.ld;
     if (locked > 0) {
       for (int pass = 0; pass < 2; ++pass) {
-        gram_block<T>(sm, b.V.data(), b.V.ld, b.V.col(locked), b.V.ld, n, locked, active,
-                      sm.G.as<double>(), s);
-        rotate_block<T>(sm, b.V.data(), b.V.ld, sm.G.as<double>(), b.V.col(locked), b.V.ld, n,
-                        locked, active, -1.0, 1.0, s);
+        gram_block<T>(sm, b.V.data(), b.V.ld, Y, ldy, n, locked, active, sm.G.as<double>(), s);
+        rotate_block<T>(sm, b.V.data(), b.V.ld, sm.G.as<double>(), Y, ldy, n, locked, active, -1.0,
+                        1.0, s);
       }
+    }
+    if (!in_place) {
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(b.V.col(locked), b.V.ld * sizeof(T), b.S.data(),
+                                      b.S.ld * sizeof(T), active * sizeof(T), n,
+                                      cudaMemcpyDeviceToDevice, s));
     }
     // 3. Cholesky QR of the current subspace (CholQR2 on FP32 blocks).
     if (cholqr2) {
@@ -625,6 +645,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   std::unique_ptr<ChebLoop<double>> l64;
   // Initial block and its Cholesky QR (src/ChebyshevSolver.cpp:94-107).
   {
+    FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, 4 * sizeof(int32_t), ctx.stream));
     Block<double> V0;
     V0.allocate(n, cap);
     if (host_init) random_block_host<double>(ctx, V0, cap, seed);
@@ -632,20 +653,22 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     if (mixed) {
       l32.reset(new ChebLoop<float>(ctx, A, opt, sm, eig, sign, lower, upper, true));
       l32->b.allocate(n, cap);
-      // QR in FP64 then round the orthonormal block to FP32.
-      Block<double> Q0;
-      Q0.allocate(n, cap);
-      cholqr<double>(ctx, sm, V0.data(), V0.ld, Q0.data(), Q0.ld, n, cap, 0);
-      convert<double, float>(Q0.data(), Q0.ld, l32->b.V.data(), l32->b.V.ld, n, cap, ctx.stream);
+      // A random block is well conditioned: round it to FP32 and orthonormalize
+      // with CholQR2 on the FP32 (tensor-core) path.
+      convert<double, float>(V0.data(), V0.ld, l32->b.S.data(), l32->b.S.ld, n, cap, ctx.stream);
+      V0.buf.release();
+      cholqr<float>(ctx, sm, l32->b.S.data(), l32->b.S.ld, l32->b.Q.data(), l32->b.Q.ld, n, cap, 0);
+      cholqr<float>(ctx, sm, l32->b.Q.data(), l32->b.Q.ld, l32->b.V.data(), l32->b.V.ld, n, cap, 1);
     } else {
       l64.reset(new ChebLoop<double>(ctx, A, opt, sm, eig, sign, lower, upper, false));
       l64->b.allocate(n, cap);
       cholqr<double>(ctx, sm, V0.data(), V0.ld, l64->b.V.data(), l64->b.V.ld, n, cap, 0);
     }
-    int32_t info = 0;
-    ctx.to_host(&info, sm.info.as<int32_t>(), 1);
+    int32_t info[2] = {0, 0};
+    ctx.to_host(info, sm.info.as<int32_t>(), 2);
     ctx.sync();
-    if (info != 0) throw Error(FE_ERR_NOT_SPD, "ChebyshevSolver: initial Cholesky QR failed.");
+    if (info[0] != 0 || info[1] != 0)
+      throw Error(FE_ERR_NOT_SPD, "ChebyshevSolver: initial Cholesky QR failed.");
   }
   if (opt.verbosity >= 2)
     std::fprintf(stderr, "[fe] setup (buffers, bounds, initial QR) %.1f ms\n", ms_since(t_start));
@@ -1414,7 +1437,9 @@ void davidson_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* 
   if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
     throw Error(FE_ERR_INVALID, "DavidsonSolver: invalid which option (use SR/LR/SM/LM/BE).");
   const double tol = opt.tol;
-  const int64_t cap = std::min<int64_t>(n, opt.maxblks * nev);
+  // Block of b >= nev Ritz vectors; convergence is judged on the first nev.
+  const int64_t bw = std::min<int64_t>(n, std::max<int64_t>(nev, opt.block));
+  const int64_t cap = std::min<int64_t>(n, opt.maxblks * bw);
   Context ctx;
   cudaStream_t s = ctx.stream;
   SmallState sm;
@@ -1439,31 +1464,31 @@ void davidson_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* 
   auto extract = [&](int64_t cols) {
     FE_CHECK_CUDA(cudaMemcpy2DAsync(Pw, cap * 8, Pm, cap * 8, cols * 8, cols,
                                     cudaMemcpyDeviceToDevice, s));
-    ritz_extract(ctx, sm, eig, Pw, V.data(), AV.data(), ld, n, cols, nev, which, X.data(),
+    ritz_extract(ctx, sm, eig, Pw, V.data(), AV.data(), ld, n, cols, bw, which, X.data(),
                  AX.data(), R.data(), coef.as<double>(), g.idx_dev, ritz, BV.data(), BX.data());
   };
-  fill_initial_block(ctx, X.data(), ld, n, nev, opt.seed_or_default(), opt.init == "host");
-  if (g.ortho(nullptr, nullptr, 0, X.data(), nev, X.data(), BX.data(), T1.data(), T2.data()) < nev)
+  fill_initial_block(ctx, X.data(), ld, n, bw, opt.seed_or_default(), opt.init == "host");
+  if (g.ortho(nullptr, nullptr, 0, X.data(), bw, X.data(), BX.data(), T1.data(), T2.data()) < bw)
     throw Error(FE_ERR_NOT_SPD, "DavidsonSolver: initial block is rank deficient.");
-  g.copy(V.data(), X.data(), nev);
-  g.copy(BV.data(), BX.data(), nev);
-  g.happly(V.data(), AV.data(), nev);
-  gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, nev, nev, Pm, s);
-  extract(nev);
+  g.copy(V.data(), X.data(), bw);
+  g.copy(BV.data(), BX.data(), bw);
+  g.happly(V.data(), AV.data(), bw);
+  gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, bw, bw, Pm, s);
+  extract(bw);
   const double locktol = std::min(1.0e-5, tol);
   int64_t it_done = 0;
   for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
-    g.bcholqr(X.data(), BX.data(), nev, T1.data(), T2.data(), "DavidsonSolver: restart");
-    g.copy(V.data(), X.data(), nev);
-    g.copy(BV.data(), BX.data(), nev);
-    g.happly(V.data(), AV.data(), nev);
+    g.bcholqr(X.data(), BX.data(), bw, T1.data(), T2.data(), "DavidsonSolver: restart");
+    g.copy(V.data(), X.data(), bw);
+    g.copy(BV.data(), BX.data(), bw);
+    g.happly(V.data(), AV.data(), bw);
     FE_CHECK_CUDA(cudaMemset2DAsync(Pm, cap * 8, 0, cap * 8, cap, s));
-    gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, nev, nev, Pm, s);
-    int64_t cols = nev;
+    gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, bw, bw, Pm, s);
+    int64_t cols = bw;
     extract(cols);
     for (int64_t blk = 1; blk < opt.maxblks; ++blk) {
       std::vector<int32_t> active;
-      for (int64_t j = 0; j < nev; ++j)
+      for (int64_t j = 0; j < bw; ++j)
         if (ritz.rel[j] > locktol) active.push_back(static_cast<int32_t>(j));
       const int64_t cc = static_cast<int64_t>(active.size());
       if (cc == 0 || cols + cc > cap) break;
@@ -1483,7 +1508,7 @@ void davidson_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* 
     }
     it_done = iter + 1;
     double worst = 0;
-    for (double v : ritz.rel) worst = std::max(worst, v);
+    for (int64_t j = 0; j < nev; ++j) worst = std::max(worst, ritz.rel[j]);
     if (opt.verbosity >= 2)
       std::fprintf(stderr, "[fe] davidson-g iter %lld cols %lld worst %.3e\n",
                    static_cast<long long>(iter + 1), static_cast<long long>(cols), worst);
@@ -1786,7 +1811,8 @@ void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int
       d_inv(P * 8), d_bn(P * 8), d_T(static_cast<size_t>(P) * M * M * 8),
       d_part(static_cast<size_t>(NC) * M * 8), d_part1(NC * 8), d_h1(P * M * 8), d_h2(P * M * 8),
       d_W(P * M * 8), d_Z(static_cast<size_t>(P) * M * M * 8), d_C(static_cast<size_t>(P) * M * M * 8),
-      d_todo(P * 4), d_keep(P * 4), d_keepY(P * 4);
+      d_todo(P * 4), d_keep(P * 4), d_keepY(P * 4), d_Zl(P * M * 8), d_idx(P * M * 4),
+      d_diag(P * M * 8), d_coup(P * M * 8);
   BatchState S;
   S.col = d_col.as<int32_t>();
   S.mdim = d_m.as<int32_t>();
@@ -1803,15 +1829,14 @@ void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int
   S.h2 = d_h2.as<double>();
   std::vector<int32_t> h_col(P, 0), h_m(P), h_rr(P, -1), h_act(P, 1), h_status(P, 0);
   for (int32_t p = 0; p < P; ++p) h_m[p] = static_cast<int32_t>(m[p]);
-  std::vector<double> h_T(static_cast<size_t>(P) * M * M, 0.0);
   auto upload_state = [&] {
     ctx.to_device(S.col, h_col.data(), P);
     ctx.to_device(S.restart_row, h_rr.data(), P);
     ctx.to_device(S.active, h_act.data(), P);
-    ctx.to_device(S.T, h_T.data(), h_T.size());
   };
   ctx.to_device(S.mdim, h_m.data(), P);
   ctx.to_device(S.status, h_status.data(), P);
+  FE_CHECK_CUDA(cudaMemsetAsync(S.T, 0, d_T.bytes(), s));
   upload_state();
   // Starting vectors: each problem's own seeded draw (the single solver's
   // random_into(f, seed)), so a problem starts identically alone or batched.
@@ -1828,6 +1853,7 @@ void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int
     for (int32_t p = 0; p < P; ++p) fill_uniform<double>(f.as<double>() + row0[p], 1, n[p], 1, seed, s);
   }
   FE_CHECK_CUDA(cudaMemsetAsync(V.get(), 0, V.bytes(), s));
+  bks_init_norm(L, S, f.as<double>(), s);
   ctx.sync();
   // One Lanczos step of the whole batch as a CUDA graph.
   cudaGraph_t graph = nullptr;
@@ -1856,8 +1882,9 @@ void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int
   std::vector<double> lam_final(static_cast<size_t>(P) * ldy, 0.0);
   std::vector<int32_t> keep(P, 0), keepY(P, 0), todo(P, 0), nev32(P);
   for (int32_t p = 0; p < P; ++p) nev32[p] = static_cast<int32_t>(nevs[p]);
-  std::vector<double> hW(static_cast<size_t>(P) * M), hZ(static_cast<size_t>(P) * M * M),
-      hC(static_cast<size_t>(P) * M * M, 0.0), hbn(P);
+  std::vector<double> hW(static_cast<size_t>(P) * M), hZl(static_cast<size_t>(P) * M),
+      hdiag(static_cast<size_t>(P) * M, 0.0), hcoup(static_cast<size_t>(P) * M, 0.0), hbn(P);
+  std::vector<int32_t> hidx(static_cast<size_t>(P) * M, 0);
   DeviceBuffer Y(static_cast<size_t>(N) * ldy * 8);
   FE_CHECK_CUDA(cudaMemsetAsync(Y.get(), 0, Y.bytes(), s));
   int64_t steps_needed = max_m;
@@ -1879,9 +1906,10 @@ void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int
       todo[p] = 1;
     }
     ctx.to_device(d_todo.as<int32_t>(), todo.data(), P);
-    bks_jacobi(L, S.T, S.mdim, d_todo.as<int32_t>(), max_m, d_W.as<double>(), d_Z.as<double>(), s);
+    bks_jacobi(L, S.T, S.mdim, d_todo.as<int32_t>(), max_m, d_W.as<double>(), d_Z.as<double>(),
+               d_Zl.as<double>(), s);
     ctx.to_host(hW.data(), d_W.as<double>(), hW.size());
-    ctx.to_host(hZ.data(), d_Z.as<double>(), hZ.size());
+    ctx.to_host(hZl.data(), d_Zl.as<double>(), hZl.size());
     ctx.to_host(hbn.data(), S.beta_next, P);
     ctx.sync();
     int max_keep = 0, max_keepY = 0;
@@ -1894,13 +1922,13 @@ void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int
       const int64_t mp = m[p], nev = nevs[p];
       std::vector<double> lam(hW.begin() + static_cast<int64_t>(p) * M,
                               hW.begin() + static_cast<int64_t>(p) * M + mp);
-      const double* Zp = hZ.data() + static_cast<size_t>(p) * M * M;
+      const double* Zl = hZl.data() + static_cast<size_t>(p) * M;  // last row of Z_p
       const std::vector<int32_t> idx = select_indices(lam, which);
+      std::copy(idx.begin(), idx.end(), hidx.begin() + static_cast<size_t>(p) * M);
       std::vector<double> lam_s(mp), rel_s(mp);
       for (int64_t j = 0; j < mp; ++j) {
         lam_s[j] = lam[idx[j]];
-        rel_s[j] = std::fabs(hbn[p] * Zp[static_cast<size_t>(idx[j]) * M + mp - 1]) /
-                   (1.0 + std::fabs(lam_s[j]));
+        rel_s[j] = std::fabs(hbn[p] * Zl[idx[j]]) / (1.0 + std::fabs(lam_s[j]));
       }
       int64_t nconv = 0;
       for (int64_t j = 0; j < nev; ++j) {
@@ -1908,12 +1936,8 @@ void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int
         if (rel_s[j] * (1.0 + mag) < tol * mag) ++nconv;
       }
       const bool at_limit = (mp == n[p]) || (iter == opt.maxiter);
-      double* Cp = hC.data() + static_cast<size_t>(p) * M * M;
       if (nconv >= nev || at_limit) {
-        for (int64_t j = 0; j < nev; ++j) {
-          std::memcpy(Cp + j * M, Zp + static_cast<size_t>(idx[j]) * M, mp * sizeof(double));
-          lam_final[static_cast<size_t>(p) * ldy + j] = lam_s[j];
-        }
+        for (int64_t j = 0; j < nev; ++j) lam_final[static_cast<size_t>(p) * ldy + j] = lam_s[j];
         keepY[p] = static_cast<int32_t>(nev);
         max_keepY = std::max<int>(max_keepY, static_cast<int>(nev));
         iterations[p] = static_cast<int32_t>(iter);
@@ -1924,27 +1948,27 @@ void batch_krylov_schur(const std::vector<const Csr*>& As, const std::vector<int
       const int64_t spare = (mp - nev) / 2;
       int64_t retained = nev + std::min(nconv, spare);
       if (retained == 1 && mp > 3) retained = mp / 2;
-      for (int64_t j = 0; j < retained; ++j)
-        std::memcpy(Cp + j * M, Zp + static_cast<size_t>(idx[j]) * M, mp * sizeof(double));
       keep[p] = static_cast<int32_t>(retained);
       max_keep = std::max<int>(max_keep, static_cast<int>(retained));
-      double* Tp = h_T.data() + static_cast<size_t>(p) * M * M;
-      std::fill(Tp, Tp + M * M, 0.0);
       for (int64_t j = 0; j < retained; ++j) {
-        Tp[j + j * M] = lam_s[j];
-        const double coupling = hbn[p] * Zp[static_cast<size_t>(idx[j]) * M + mp - 1];
-        Tp[retained + j * M] = coupling;
-        Tp[j + retained * M] = coupling;
+        hdiag[static_cast<size_t>(p) * M + j] = lam_s[j];
+        hcoup[static_cast<size_t>(p) * M + j] = hbn[p] * Zl[idx[j]];
       }
       h_col[p] = static_cast<int32_t>(retained);
       h_rr[p] = static_cast<int32_t>(retained);
       h_act[p] = 1;
       any_active = true;
     }
-    ctx.to_device(d_C.as<double>(), hC.data(), hC.size());
+    ctx.to_device(d_idx.as<int32_t>(), hidx.data(), hidx.size());
     ctx.to_device(d_keep.as<int32_t>(), keep.data(), P);
     ctx.to_device(d_keepY.as<int32_t>(), keepY.data(), P);
-    // Finishing problems: Ritz vectors into Y; restarting problems: V[:, :retained] = V C.
+    ctx.to_device(d_diag.as<double>(), hdiag.data(), hdiag.size());
+    ctx.to_device(d_coup.as<double>(), hcoup.data(), hcoup.size());
+    // Coefficients and the restarted T on the device; then finishing problems'
+    // Ritz vectors into Y and restarting problems' V[:, :retained] = V C.
+    bks_restart(L, S.mdim, d_idx.as<int32_t>(), d_keep.as<int32_t>(), d_keepY.as<int32_t>(),
+                d_diag.as<double>(), d_coup.as<double>(), d_Z.as<double>(), d_C.as<double>(), S.T,
+                s);
     bks_rotate(L, V.as<double>(), M, d_C.as<double>(), S.mdim, d_keepY.as<int32_t>(), max_m,
                max_keepY, Y.as<double>(), ldy, s);
     bks_rotate(L, V.as<double>(), M, d_C.as<double>(), S.mdim, d_keep.as<int32_t>(), max_m,
@@ -2020,7 +2044,7 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
       lobpcg_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
     }
   } else if (opt.solver == "davidson") {
-    if (B || opt.precond != "none") {
+    if (B || opt.precond != "none" || opt.block > opt.nev) {
       if (B) check_pair(A, *B);
       davidson_gen_solve(A, B, opt, eigenvalues, residual_norms, eigenvectors, st);
     } else {
@@ -2078,7 +2102,7 @@ size_t solve_memory_bytes(const Csr& A, const Csr* B, const char* options) {
     cap = std::min<int64_t>(n, 3 * std::max<int64_t>(nev, opt.block));
     blocks = 12;
   } else if (opt.solver == "davidson") {
-    cap = std::min<int64_t>(n, opt.maxblks * nev);
+    cap = std::min<int64_t>(n, opt.maxblks * std::max<int64_t>(nev, opt.block));
     blocks = 11;
   } else {
     cap = std::min<int64_t>(std::max<int64_t>({2 * nev, 20, opt.maxdim}), n);

@@ -422,14 +422,17 @@ __global__ void __launch_bounds__(kThreads, 1)
 rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmCh,
                  const __grid_constant__ CUtensorMap tmCl, int64_t n, int k, int m, int m_tiles,
                  float* __restrict__ Y, int64_t ldy, float alpha, float beta, int use_beta,
-                 int vec_store) {
+                 int vec_store, int upper_tri) {
   extern __shared__ uint8_t dyn_smem[];
   const Smem sm = carve(dyn_smem);
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   const int j0 = static_cast<int>(blockIdx.x % m_tiles) * kN;
   const int64_t r0 = static_cast<int64_t>(blockIdx.x / m_tiles) * kM;
-  const int nkb = (k + kKB - 1) / kKB;
+  // With an upper-triangular C (CholQR's R^-1), rows k >= j0 + kN of C are zero for
+  // this tile's columns: those K blocks contribute exact zeros and are skipped.
+  const int k_eff = upper_tri ? min(k, j0 + kN) : k;
+  const int nkb = (k_eff + kKB - 1) / kKB;
 
   prologue(sm, warp);
   const uint32_t tmem = *sm.tmem_slot;
@@ -670,7 +673,7 @@ size_t tc_rotate_workspace_bytes(int64_t k, int64_t m) {
 // Y = alpha X C + beta Y (FP32 blocks, 3xTF32 tensor cores).
 void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float* Y, int64_t ldy,
                int64_t n, int64_t k, int64_t m, double alpha, double beta, void* ws,
-               size_t ws_bytes, cudaStream_t s) {
+               size_t ws_bytes, cudaStream_t s, bool upper_tri) {
   FE_REQUIRE(n > 0 && k > 0 && m > 0, "rotate_tc: invalid shape");
   FE_REQUIRE(n < (int64_t(1) << 31), "rotate_tc: too many rows for 32-bit TMA coordinates");
   FE_REQUIRE((reinterpret_cast<uintptr_t>(X) & 15u) == 0, "rotate_tc: X not 16-byte aligned");
@@ -699,7 +702,7 @@ void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float*
                                                       static_cast<int>(m_tiles), Y, ldy,
                                                       static_cast<float>(alpha),
                                                       static_cast<float>(beta), beta != 0.0,
-                                                      vec ? 1 : 0);
+                                                      vec ? 1 : 0, upper_tri ? 1 : 0);
   check_launch("rotate_tc_kernel");
 }
 
@@ -769,6 +772,6 @@ extern "C" int fe_rotate_tf32x3(const float* X, int64_t ldx, const double* C, in
     FE_REQUIRE(!fe::ranges_overlap(X, n, ldx, k, static_cast<const float*>(Y), n, ldy, m),
                "X and Y overlap");
     fe::rotate_tc(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, workspace, workspace_bytes,
-                  fe::as_stream(stream));
+                  fe::as_stream(stream), false);
   });
 }

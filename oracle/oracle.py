@@ -992,10 +992,10 @@ def lobpcg_gen_solve(A: Csr, nev: int, B: Optional[Csr] = None, precond: str = "
 
 def davidson_gen_solve(A: Csr, nev: int, B: Optional[Csr] = None, precond: str = "none",
                        tol: float = 1e-8, maxiter: int = 1000, which: str = "sr", seed: int = 1,
-                       maxblks: int = 10) -> SolveResult:
+                       maxblks: int = 10, block: int = 0) -> SolveResult:
     """Block Davidson for K u = l M u with thick restart and optional Jacobi-preconditioned
     corrections (loop of src/DavidsonSolver.cpp:27-264, locktol = min(1e-5, tol), in the
-    B metric)."""
+    B metric), on a block of max(nev, block) Ritz vectors (convergence on the first nev)."""
     n = A.rows
     which = which.lower()
     if nev <= 0 or nev > n:
@@ -1005,13 +1005,14 @@ def davidson_gen_solve(A: Csr, nev: int, B: Optional[Csr] = None, precond: str =
     Hs = A.scipy()
     H = (lambda X: Hs @ X)
     t = jacobi_inverse_diagonal(A) if precond == "jacobi" else None
-    cap = min(n, maxblks * nev)
-    X0 = random_block(n, nev, seed)
+    b = min(n, max(nev, block))
+    cap = min(n, maxblks * b)
+    X0 = random_block(n, b, seed)
     X, BX = ortho_block_b(B, None, None, 0, X0)
-    if X is None or X.shape[1] < nev:
+    if X is None or X.shape[1] < b:
         raise RuntimeError("DavidsonSolver: initial block is rank deficient.")
     AX = H(X)
-    vals, C, X, AX, BX, R, rel = _gen_ritz(X, AX, BX, nev, nev, which)
+    vals, C, X, AX, BX, R, rel = _gen_ritz(X, AX, BX, b, b, which)
     locktol = min(1.0e-5, tol)
     it_done = 0
     for it in range(maxiter):
@@ -1019,11 +1020,11 @@ def davidson_gen_solve(A: Csr, nev: int, B: Optional[Csr] = None, precond: str =
         V = np.zeros((n, cap))
         BV = np.zeros((n, cap))
         AV = np.zeros((n, cap))
-        V[:, :nev], BV[:, :nev], AV[:, :nev] = X, BX, H(X)
-        cols = nev
-        vals, C, X, AX, BX, R, rel = _gen_ritz(V, AV, BV, cols, nev, which)
+        V[:, :b], BV[:, :b], AV[:, :b] = X, BX, H(X)
+        cols = b
+        vals, C, X, AX, BX, R, rel = _gen_ritz(V, AV, BV, cols, b, which)
         for _blk in range(1, maxblks):
-            active = [j for j in range(nev) if rel[j] > locktol]
+            active = [j for j in range(b) if rel[j] > locktol]
             cc = len(active)
             if cc == 0 or cols + cc > cap:
                 break
@@ -1036,8 +1037,8 @@ def davidson_gen_solve(A: Csr, nev: int, B: Optional[Csr] = None, precond: str =
             r = W.shape[1]
             V[:, cols:cols + r], BV[:, cols:cols + r], AV[:, cols:cols + r] = W, BW, H(W)
             cols += r
-            vals, C, X, AX, BX, R, rel = _gen_ritz(V, AV, BV, cols, nev, which)
+            vals, C, X, AX, BX, R, rel = _gen_ritz(V, AV, BV, cols, b, which)
         it_done = it + 1
-        if rel.max() < tol:
+        if rel[:nev].max() < tol:
             break
-    return SolveResult(vals.copy(), X.copy(), rel.copy(), it_done)
+    return SolveResult(vals[:nev].copy(), X[:, :nev].copy(), rel[:nev].copy(), it_done)

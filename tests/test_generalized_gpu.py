@@ -128,3 +128,25 @@ def test_generalized_rejects_shape_mismatch(km8):
     opts.set("solver", "LOBPCG")
     with pytest.raises(Exception, match="same shape"):
         fasteig_problem(dK, dB, solver="LOBPCG").solve(opts)
+
+
+@pytest.mark.parametrize("generalized", [False, True])
+def test_davidson_block_larger_than_nev(km8, wells_small, generalized):
+    """Davidson on a block of 12 Ritz vectors for 8 requested pairs (Jacobi corrections),
+    standard and generalized, against the oracle and dense eigh."""
+    import scipy.linalg as sl
+    from oracle import oracle as O
+    if generalized:
+        A, Bm = km8
+        dense = sl.eigh(A.scipy().toarray(), Bm.scipy().toarray(), eigvals_only=True)
+    else:
+        (A, dense), Bm = wells_small, None
+    ref = O.davidson_gen_solve(A, 8, B=Bm, precond="jacobi", block=12, tol=1e-8, maxiter=500,
+                               seed=4, maxblks=4)
+    p = solve(A, Bm, solver="Davidson", nev=8, which="SR", tol=1e-8, maxiter=500, seed=4,
+              precond="jacobi", block=12, maxblks=4)
+    np.testing.assert_allclose(p.eigenvalues(), ref.eigenvalues, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(p.eigenvalues(), dense[:8], rtol=1e-10, atol=1e-12)
+    assert abs(p.last_iterations() - ref.iterations) <= max(3, 0.1 * ref.iterations)
+    final = O.residual_norms(A, Bm, p.eigenvalues(), p.eigenvectors())
+    assert np.all(final <= 1.01e-8), final
