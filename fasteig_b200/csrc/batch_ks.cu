@@ -93,6 +93,27 @@ __global__ void __launch_bounds__(kBT) bks_store_kernel(BatchLayout L, BatchStat
   }
 }
 
+// w = A q on the rows of active problems only (one thread per row, the block-diagonal
+// CSR's global column indices); chunks of finished or waiting problems exit at once.
+__global__ void __launch_bounds__(kBT) bks_spmv_kernel(BatchLayout L, BatchState S,
+                                                       const int32_t* __restrict__ rowptr,
+                                                       const int32_t* __restrict__ colind,
+                                                       const double* __restrict__ val,
+                                                       const double* __restrict__ q,
+                                                       double* __restrict__ w) {
+  const int c = blockIdx.x;
+  const int p = L.c_prob[c];
+  if (!S.active[p]) return;
+  const int64_t r0 = L.c_row0[c];
+  const int rows = L.c_rows[c];
+  for (int i = threadIdx.x; i < rows; i += kBT) {
+    const int64_t r = r0 + i;
+    double acc = 0.0;
+    for (int32_t e = rowptr[r]; e < rowptr[r + 1]; ++e) acc = fma(val[e], q[colind[e]], acc);
+    w[r] = acc;
+  }
+}
+
 // part[c * M + j] = sum over chunk rows of V[r, j] x[r], j <= col (active problems).
 __global__ void __launch_bounds__(kBT) bks_dots_kernel(BatchLayout L, BatchState S,
                                                        const double* __restrict__ V, int64_t ldv,
@@ -566,7 +587,8 @@ void bks_lanczos_step(const BatchLayout& L, const BatchState& S, const Csr& A, d
   check_launch("bks_begin_kernel");
   bks_store_kernel<<<pc, kBT, 0, s>>>(L, S, f, q, V, ldv);
   check_launch("bks_store_kernel");
-  csr_spmm<double>(A, q, 1, w, 1, nullptr, 0, 1, 1.0, 0.0, 0.0, s);
+  bks_spmv_kernel<<<pc, kBT, 0, s>>>(L, S, A.rowptr, A.colind, A.val64, q, w);
+  check_launch("bks_spmv_kernel");
   bks_dots_kernel<<<pc, kBT, 0, s>>>(L, S, V, ldv, w, S.part);
   check_launch("bks_dots_kernel");
   bks_dots_finish_kernel<<<static_cast<unsigned>(L.num_problems), 128, 0, s>>>(L, S, S.part, S.h1);

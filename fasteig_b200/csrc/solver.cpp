@@ -417,6 +417,16 @@ void gram_block(SmallState& sm, const T* X, int64_t ldx, const T* Y, int64_t ldy
       gram_tc(X, ldx, Y, ldy, n, k, m, G, sm.cap, sm.gws.get(), sm.gws.bytes(), s);
       return;
     }
+    if (precise && X == Y && ldx == ldy && n >= 128) {
+      // The FP64-accumulated Gram of an FP32 block: widen it once (FP32 values are
+      // exact in FP64) and take the FP64 tensor-core Gram, upper tiles only.
+      Block<double> wide;
+      wide.allocate(n, k);
+      convert<float, double>(X, ldx, wide.data(), wide.ld, n, k, s);
+      gram<double>(wide.data(), wide.ld, wide.data(), wide.ld, n, k, k, G, sm.cap, sm.gws.get(),
+                   sm.gws.bytes(), s);
+      return;
+    }
   }
   gram<T>(X, ldx, Y, ldy, n, k, m, G, sm.cap, sm.gws.get(), sm.gws.bytes(), s);
 }
@@ -1520,15 +1530,79 @@ void davidson_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* 
   st.fp64_iterations = static_cast<double>(it_done);
 }
 
-// KrylovSchurSolver::solve (src/KrylovSchurSolver.cpp:28-160) for standard problems:
-// scalar Lanczos with two-pass classical reorthogonalization (KrylovSubspace,
-// src/core/KrylovSubspace.cpp:125-259) on the device, the m x m projected
-// eigenproblem on the host, Krylov-Schur restarts that keep the wanted Ritz
-// vectors and a dense coupling row (CpuLanczosWorkspace::prepare_krylov_schur_restart,
-// src/core/LanczosWorkspace.cpp:94-107), and final Ritz pairs evaluated on the
-// device (evaluate_ritz_pairs, src/core/RitzExtraction.cpp:34-63).
-void krylov_schur_solve(const Csr& A, const Options& opt, double* eigenvalues, double* residuals,
-                        double* eigenvectors, Stats& st) {
+// Solves B x = b on the device by conjugate gradients with the Jacobi
+// preconditioner, to ||r|| <= 1e-14 ||b|| (at most 1000 iterations). Stands in for
+// the reference's sparse factorization of B in the generalized Krylov-Schur
+// operator B^-1 A (src/gpu/CudaShiftInvertOperator.cpp uses cuDSS): B is the
+// symmetric positive definite mass matrix, and its inverse is applied to the
+// tolerance of the FP64 path, so the Lanczos recurrence sees B^-1 A to ~1e-14.
+struct MassSolver {
+  Context& ctx;
+  const Csr& B;
+  int64_t n;
+  DeviceBuffer t, r, z, p, q, out, ws, idx0;
+  int64_t iterations = 0;
+  MassSolver(Context& c, const Csr& b)
+      : ctx(c), B(b), n(b.rows), t(n * 8), r(n * 8), z(n * 8), p(n * 8), q(n * 8), out(8),
+        ws(std::max<size_t>(residual_workspace_bytes(b.rows, 1), 64)), idx0(16) {
+    jacobi_inverse_diagonal(B, t.as<double>(), ctx.stream);
+    const int32_t zero = 0;
+    ctx.to_device(idx0.as<int32_t>(), &zero, 1);
+  }
+  // sqrt(x . y) for x . y >= 0 (the B-norm kernel with y in place of B x).
+  double dot_pos(const double* x, const double* y) {
+    residual_norms<double>(nullptr, x, y, 1, n, 1, nullptr, nullptr, 0, nullptr, out.as<double>(),
+                           nullptr, ws.get(), ws.bytes(), ctx.stream, 2);
+    double v = 0;
+    ctx.to_host(&v, out.as<double>(), 1);
+    ctx.sync();
+    return v * v;
+  }
+  void precondition(const double* src, double* dst) {
+    gather_columns<double>(src, 1, idx0.as<int32_t>(), 1, dst, 1, n, ctx.stream, t.as<double>());
+  }
+  // x = B^-1 b (x and b distinct device vectors).
+  void solve(const double* b, double* x) {
+    cudaStream_t s = ctx.stream;
+    FE_CHECK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+    FE_CHECK_CUDA(cudaMemcpyAsync(r.get(), b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    const double bnorm2 = dot_pos(b, b);
+    if (bnorm2 == 0.0) return;
+    precondition(r.as<double>(), z.as<double>());
+    FE_CHECK_CUDA(cudaMemcpyAsync(p.get(), z.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    double rz = dot_pos(r.as<double>(), z.as<double>());
+    for (int it = 0; it < 1000; ++it) {
+      csr_spmm<double>(B, p.as<double>(), 1, q.as<double>(), 1, nullptr, 0, 1, 1.0, 0.0, 0.0, s);
+      const double pq = dot_pos(p.as<double>(), q.as<double>());
+      if (!(pq > 0.0) || !std::isfinite(pq))
+        throw Error(FE_ERR_NONFINITE, "B must be positive definite (invalid B-norm).");
+      const double alpha = rz / pq;
+      vec_axpby(n, alpha, p.as<double>(), 1, 1.0, x, 1, s);
+      vec_axpby(n, -alpha, q.as<double>(), 1, 1.0, r.as<double>(), 1, s);
+      ++iterations;
+      if (dot_pos(r.as<double>(), r.as<double>()) <= 1e-28 * bnorm2) return;
+      precondition(r.as<double>(), z.as<double>());
+      const double rz_new = dot_pos(r.as<double>(), z.as<double>());
+      vec_axpby(n, 1.0, z.as<double>(), 1, rz_new / rz, p.as<double>(), 1, s);
+      rz = rz_new;
+    }
+    throw Error(FE_ERR_NONFINITE, "KrylovSchurSolver: mass-matrix solve did not converge.");
+  }
+};
+
+// KrylovSchurSolver::solve (src/KrylovSchurSolver.cpp:28-160): scalar Lanczos with
+// two-pass classical reorthogonalization (KrylovSubspace, src/core/KrylovSubspace.cpp:
+// 125-259) on the device, the m x m projected eigenproblem on the host, Krylov-Schur
+// restarts that keep the wanted Ritz vectors and a dense coupling row
+// (CpuLanczosWorkspace::prepare_krylov_schur_restart, src/core/LanczosWorkspace.cpp:94-107),
+// and final Ritz pairs evaluated on the device (evaluate_ritz_pairs,
+// src/core/RitzExtraction.cpp:34-63). With B the recurrence runs in the B inner
+// product on the operator B^-1 A (B-norms of KrylovSubspace::residual_norm,
+// src/core/KrylovSubspace.cpp:162-178; Gram-Schmidt weighted by BV), converged pairs are
+// verified by their true residual ||A y - l B y|| / ((1+|l|) ||B y||) and the status is 1
+// when they are not (src/KrylovSchurSolver.cpp:136-140).
+void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* eigenvalues,
+                        double* residuals, double* eigenvectors, Stats& st) {
   const int64_t n = A.rows, nev = opt.nev;
   if (n <= 0) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: n must be > 0.");
   if (nev <= 0 || nev > n) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: nev must be in [1,n].");
@@ -1547,12 +1621,20 @@ void krylov_schur_solve(const Csr& A, const Options& opt, double* eigenvalues, d
   cudaStream_t s = ctx.stream;
   SmallState sm;
   sm.allocate(n, m, false);
-  Block<double> V, Y;
+  Block<double> V, Y, BV;
   V.allocate(n, m);
   Y.allocate(n, m);
+  if (B) BV.allocate(n, m);
   const int64_t ld = V.ld;
   DeviceBuffer f(n * sizeof(double)), w(n * sizeof(double)), h(m * sizeof(double)),
       hs(m * sizeof(double)), nrm(sizeof(double)), C(static_cast<size_t>(m) * m * sizeof(double));
+  DeviceBuffer bf, aw;
+  std::unique_ptr<MassSolver> mass;
+  if (B) {
+    bf.resize(n * sizeof(double));
+    aw.resize(n * sizeof(double));
+    mass.reset(new MassSolver(ctx, *B));
+  }
   DeviceBuffer gws(std::max<size_t>(gram_workspace_bytes(n, m, 1), 64));
   DeviceBuffer rws(std::max<size_t>(residual_workspace_bytes(n, m), 64));
   auto random_into = [&](double* dst, unsigned sd) {
@@ -1566,23 +1648,31 @@ void krylov_schur_solve(const Csr& A, const Options& opt, double* eigenvalues, d
       fill_uniform<double>(dst, 1, n, 1, sd, s);
     }
   };
+  // ||x|| (standard) or the B-norm sqrt(x . Bx) with Bx kept in bf (generalized).
   auto norm = [&](const double* x) {
-    residual_norms<double>(nullptr, x, nullptr, 1, n, 1, nullptr, nullptr, 0, nullptr,
-                           nrm.as<double>(), nullptr, rws.get(), rws.bytes(), s, 0);
+    if (B) {
+      csr_spmm<double>(*B, x, 1, bf.as<double>(), 1, nullptr, 0, 1, 1.0, 0.0, 0.0, s);
+      st.spmm_launches += 1;
+      residual_norms<double>(nullptr, x, bf.as<double>(), 1, n, 1, nullptr, nullptr, 0, nullptr,
+                             nrm.as<double>(), nullptr, rws.get(), rws.bytes(), s, 2);
+    } else {
+      residual_norms<double>(nullptr, x, nullptr, 1, n, 1, nullptr, nullptr, 0, nullptr,
+                             nrm.as<double>(), nullptr, rws.get(), rws.bytes(), s, 0);
+    }
     double r = 0;
     ctx.to_host(&r, nrm.as<double>(), 1);
     ctx.sync();
     return r;
   };
-  // f = src - V_k (V_k^T src), twice; returns the last coefficient (alpha).
+  // f = src - V_k (W_k^T src), twice (W = BV with B, else V); returns the last coefficient.
+  const double* W = B ? BV.data() : V.data();
   auto orthogonalize = [&](int64_t k, const double* src) {
     vec_axpby(n, 1.0, src, 1, 0.0, f.as<double>(), 1, s);
     if (k == 0) return 0.0;
-    gram<double>(V.data(), ld, f.as<double>(), 1, n, k, 1, h.as<double>(), k, gws.get(),
-                 gws.bytes(), s);
+    gram<double>(W, ld, f.as<double>(), 1, n, k, 1, h.as<double>(), k, gws.get(), gws.bytes(), s);
     rotate<double>(V.data(), ld, h.as<double>(), k, f.as<double>(), 1, n, k, 1, -1.0, 1.0, s);
-    gram<double>(V.data(), ld, f.as<double>(), 1, n, k, 1, hs.as<double>(), k, gws.get(),
-                 gws.bytes(), s);
+    gram<double>(W, ld, f.as<double>(), 1, n, k, 1, hs.as<double>(), k, gws.get(), gws.bytes(),
+                 s);
     rotate<double>(V.data(), ld, hs.as<double>(), k, f.as<double>(), 1, n, k, 1, -1.0, 1.0, s);
     double a = 0, b = 0;
     ctx.to_host(&a, h.as<double>() + k - 1, 1);
@@ -1612,7 +1702,13 @@ void krylov_schur_solve(const Csr& A, const Options& opt, double* eigenvalues, d
                       "core::KrylovSubspace: breakdown, unable to generate new basis vector.");
       }
       vec_axpby(n, 1.0 / beta, f.as<double>(), 1, 0.0, V.col(col), ld, s);
-      csr_spmm<double>(A, V.col(col), ld, w.as<double>(), 1, nullptr, 0, 1, 1.0, 0.0, 0.0, s);
+      if (B) vec_axpby(n, 1.0 / beta, bf.as<double>(), 1, 0.0, BV.col(col), ld, s);
+      if (B) {
+        csr_spmm<double>(A, V.col(col), ld, aw.as<double>(), 1, nullptr, 0, 1, 1.0, 0.0, 0.0, s);
+        mass->solve(aw.as<double>(), w.as<double>());
+      } else {
+        csr_spmm<double>(A, V.col(col), ld, w.as<double>(), 1, nullptr, 0, 1, 1.0, 0.0, 0.0, s);
+      }
       st.spmm_launches += 1;
       const double alpha = orthogonalize(col + 1, w.as<double>());
       beta_next = norm(f.as<double>());
@@ -1657,31 +1753,44 @@ void krylov_schur_solve(const Csr& A, const Options& opt, double* eigenvalues, d
     int64_t nconv = 0;
     for (int64_t j = 0; j < nev; ++j) {
       const double mag = std::fabs(lam_s[j]);
-      if (rel_s[j] * (1.0 + mag) < tol * mag) ++nconv;
+      const bool ok = B ? rel_s[j] <= tol : rel_s[j] * (1.0 + mag) < tol * mag;
+      if (ok) ++nconv;
     }
     const bool at_limit = (m == n) || (iter == opt.maxiter);
     if (opt.verbosity >= 2)
       std::fprintf(stderr, "[fe] krylov-schur restart %lld nconv %lld\n",
                    static_cast<long long>(iter), static_cast<long long>(nconv));
     if (nconv >= nev || at_limit) {
-      // evaluate_ritz_pairs: Y = V Csel, R = A Y - Y diag(l), rel = ||r|| / ((1+|l|) ||y||)
+      // evaluate_ritz_pairs: Y = V Csel, R = A Y - B Y diag(l), rel = ||r|| / ((1+|l|) ||B y||)
       std::vector<double> Cs(static_cast<size_t>(m) * nev);
       for (int64_t j = 0; j < nev; ++j)
         std::memcpy(&Cs[static_cast<size_t>(j) * m], &Z[static_cast<size_t>(idx[j]) * m],
                     m * sizeof(double));
       ctx.to_device(C.as<double>(), Cs.data(), Cs.size());
       rotate<double>(V.data(), ld, C.as<double>(), m, Y.data(), Y.ld, n, m, nev, 1.0, 0.0, s);
-      for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = lam_s[j];
-      finish_results(ctx, sm, A, nullptr, Y.data(), Y.ld, n, nev, eigenvalues, residuals,
-                     eigenvectors);
-      st.iterations = static_cast<double>(iter);
-      st.fp64_iterations = static_cast<double>(iter);
-      return;
+      std::vector<double> vals(lam_s.begin(), lam_s.begin() + nev), res(nev);
+      std::vector<double> vecs;
+      if (eigenvectors) vecs.resize(static_cast<size_t>(n) * nev);
+      finish_results(ctx, sm, A, B, Y.data(), Y.ld, n, nev, vals.data(), res.data(),
+                     eigenvectors ? vecs.data() : nullptr);
+      bool verified = true;
+      for (double r : res) verified = verified && r <= tol;
+      if (!B || verified || at_limit) {
+        for (int64_t j = 0; j < nev; ++j) {
+          eigenvalues[j] = vals[j];
+          residuals[j] = res[j];
+        }
+        if (eigenvectors) std::memcpy(eigenvectors, vecs.data(), vecs.size() * sizeof(double));
+        st.status = (B && !verified) ? 1 : 0;
+        st.iterations = static_cast<double>(iter);
+        st.fp64_iterations = static_cast<double>(iter);
+        return;
+      }
     }
     const int64_t spare = (m - nev) / 2;
     int64_t retained = nev + std::min(nconv, spare);
     if (retained == 1 && m > 3) retained = m / 2;
-    // rotate_basis: V[:, :retained] = V * C_all[:, :retained]
+    // rotate_basis: V[:, :retained] = V * C_all[:, :retained] (and BV alike)
     std::vector<double> Cr(static_cast<size_t>(m) * retained);
     for (int64_t j = 0; j < retained; ++j)
       std::memcpy(&Cr[static_cast<size_t>(j) * m], &Z[static_cast<size_t>(idx[j]) * m],
@@ -1690,6 +1799,12 @@ void krylov_schur_solve(const Csr& A, const Options& opt, double* eigenvalues, d
     rotate<double>(V.data(), ld, C.as<double>(), m, Y.data(), Y.ld, n, m, retained, 1.0, 0.0, s);
     FE_CHECK_CUDA(cudaMemcpy2DAsync(V.data(), ld * 8, Y.data(), Y.ld * 8, retained * 8, n,
                                     cudaMemcpyDeviceToDevice, s));
+    if (B) {
+      rotate<double>(BV.data(), ld, C.as<double>(), m, Y.data(), Y.ld, n, m, retained, 1.0, 0.0,
+                     s);
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(BV.data(), ld * 8, Y.data(), Y.ld * 8, retained * 8, n,
+                                      cudaMemcpyDeviceToDevice, s));
+    }
     std::fill(T.begin(), T.end(), 0.0);
     for (int64_t j = 0; j < retained; ++j) {
       t(j, j) = lam_s[j];
@@ -2051,10 +2166,8 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
       davidson_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
     }
   } else if (opt.solver == "krylovschur") {
-    FE_REQUIRE(B == nullptr,
-               "KrylovSchurSolver: generalized problems need a B^{-1} factorization (out of "
-               "scope on this backend).");
-    krylov_schur_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
+    if (B) check_pair(A, *B);
+    krylov_schur_solve(A, B, opt, eigenvalues, residual_norms, eigenvectors, st);
   } else {
     throw Error(FE_ERR_UNSUPPORTED, "solver not available on this backend: " + opt.solver);
   }

@@ -249,7 +249,10 @@ int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ld
  * extensions (precision=fp64|mixed, block=<cols>, bounds=reference|ritz,
  * precond=none|jacobi, init=host|device). B != NULL makes the problem
  * generalized (A x = l B x, B symmetric positive definite): LOBPCG and Davidson
- * then work in the B metric (extension; the reference's are standard-only).
+ * then work in the B metric (extension; the reference's are standard-only), and
+ * Krylov-Schur runs the reference's B-metric Lanczos on B^-1 A with B^-1
+ * applied by conjugate gradients to 1e-14 (the reference factorizes B with
+ * cuDSS); its status is 1 when the returned pairs miss tol.
  * Results: eigenvalues[nev], residual_norms[nev] (the reference's relative
  * residual), eigenvectors n-by-nev column-major (may be NULL), stats[12] (may
  * be NULL): iterations, status, solve seconds, SpMM launches, FP32 cycles, FP64

@@ -150,3 +150,34 @@ def test_davidson_block_larger_than_nev(km8, wells_small, generalized):
     assert abs(p.last_iterations() - ref.iterations) <= max(3, 0.1 * ref.iterations)
     final = O.residual_norms(A, Bm, p.eigenvalues(), p.eigenvectors())
     assert np.all(final <= 1.01e-8), final
+
+
+@pytest.mark.parametrize("which", ["sr", "lr", "be"])
+def test_krylov_schur_generalized_matches_oracle(km8, dense_km8, which):
+    """B-metric Krylov-Schur on B^-1 A (the mass-matrix solve by device CG to 1e-14
+    stands in for the reference's factorization) against the oracle, which applies B^-1
+    with a sparse LU, and dense eigh(K, M)."""
+    from oracle import oracle as O
+    K, Mm = km8
+    ref = O.krylov_schur_solve(K, 6, tol=1e-8, maxiter=300, which=which, seed=5, maxdim=24, B=Mm)
+    p = solve(K, Mm, solver="KrylovSchur", nev=6, which=which, tol=1e-8, maxiter=300, seed=5,
+              maxdim=24)
+    np.testing.assert_allclose(p.eigenvalues(), ref.eigenvalues, rtol=1e-10, atol=1e-12)
+    assert abs(p.last_iterations() - ref.iterations) <= 1, (p.last_iterations(), ref.iterations)
+    assert p.status() == ref.status
+    exp = O.select_reference(dense_km8, which, 6)
+    # dense eigh carries ~1e-13 |K| absolute error of its own
+    np.testing.assert_allclose(np.sort(p.eigenvalues()), np.sort(exp), rtol=1e-10, atol=1e-11)
+    final = O.residual_norms(K, Mm, p.eigenvalues(), p.eigenvectors())
+    np.testing.assert_allclose(p.residual_norms(), final, rtol=1e-6, atol=1e-15)
+
+
+def test_krylov_schur_generalized_kuumuu_known_answers(kuumuu, spectra):
+    from oracle import oracle as O
+    K, Mm = kuumuu
+    p = solve(K, Mm, solver="KrylovSchur", nev=5, which="SR", tol=1e-8, maxiter=2000, seed=1,
+              maxdim=40)
+    exp = spectra["KuuMuu"]["lowest"][:5]
+    assert all(O.eigenvalue_check(p.eigenvalues(), exp)), (p.eigenvalues(), exp)
+    assert p.status() == 0
+    assert np.all(p.residual_norms() <= 1e-8), p.residual_norms()
