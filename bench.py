@@ -609,6 +609,9 @@ def main():
             "data": "synthetic", "impl": "b200",
             "config": config_dict(a, {"parallelism": f"replicas x{world}"}),
             "converged_pairs": converged, "latency_s": {"p50": lat[len(lat) // 2], "max": lat[-1]},
+            "solve_seconds": [round(s["seconds"], 3) for s in per_solve],
+            "phase_ms": [[round(s["filter_ms"]), round(s["ortho_ms"]), round(s["rr_ms"])]
+                         for s in per_solve],
             "cycles": [s["iterations"] for s in per_solve],
             "fp32_cycles": [s["fp32_iterations"] for s in per_solve],
             "gpu_launches": int(launches), "clocks": clocks}

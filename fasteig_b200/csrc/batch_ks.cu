@@ -21,7 +21,11 @@
 
 #include "device.hpp"
 
+#include <algorithm>
 #include <cfloat>
+#include <memory>
+#include <string>
+#include <vector>
 
 namespace fe {
 namespace {
@@ -661,3 +665,115 @@ void bks_offset_copy(const int32_t* src, int64_t count, int32_t add, int32_t* ds
 }
 
 }  // namespace fe
+
+// ---------------------------------------------------------------------------
+// C ABI: the batch engine's building blocks on their own.
+// ---------------------------------------------------------------------------
+
+// Block-diagonal operator of `count` CSR handles (rows and columns offset by the
+// preceding parts): one SpMM over it is a grouped SpMM of all parts.
+extern "C" int fe_csr_block_diag(int32_t count, const fe_csr_t* parts, fe_csr_t* out) {
+  return fe::guarded("fe_csr_block_diag", [&] {
+    FE_REQUIRE(count > 0 && parts && out, "null or empty part list");
+    *out = nullptr;
+    int64_t rows = 0, cols = 0, nnz = 0, maxnz = 0;
+    const int device = parts[0] ? parts[0]->m.device : 0;
+    for (int32_t p = 0; p < count; ++p) {
+      FE_REQUIRE(parts[p], "null CSR handle in part list");
+      FE_REQUIRE(parts[p]->m.device == device, "parts live on different devices");
+      rows += parts[p]->m.rows;
+      cols += parts[p]->m.cols;
+      nnz += parts[p]->m.nnz;
+      maxnz = std::max(maxnz, parts[p]->m.max_row_nnz);
+    }
+    FE_REQUIRE(rows < 0x7fffffffLL && cols < 0x7fffffffLL && nnz <= 0x7fffffffLL,
+               "block-diagonal operator exceeds int32 indexing");
+    FE_CHECK_CUDA(cudaSetDevice(device));
+    auto h = std::make_unique<fe_csr>();
+    fe::Csr& A = h->m;
+    A.rows = rows;
+    A.cols = cols;
+    A.nnz = nnz;
+    A.device = device;
+    A.max_row_nnz = maxnz;
+    auto fail = [&] {
+      cudaFree(A.rowptr);
+      cudaFree(A.colind);
+      cudaFree(A.val64);
+      cudaFree(A.val32);
+    };
+    try {
+      FE_CHECK_CUDA(cudaMalloc(&A.rowptr, (rows + 1) * sizeof(int32_t)));
+      FE_CHECK_CUDA(cudaMalloc(&A.colind, std::max<int64_t>(nnz, 1) * sizeof(int32_t)));
+      FE_CHECK_CUDA(cudaMalloc(&A.val64, std::max<int64_t>(nnz, 1) * sizeof(double)));
+      FE_CHECK_CUDA(cudaMalloc(&A.val32, std::max<int64_t>(nnz, 1) * sizeof(float)));
+      int64_t r0 = 0, c0 = 0, z0 = 0;
+      for (int32_t p = 0; p < count; ++p) {
+        const fe::Csr& P = parts[p]->m;
+        fe::bks_offset_copy(P.rowptr, P.rows, static_cast<int32_t>(z0), A.rowptr + r0, nullptr);
+        fe::bks_offset_copy(P.colind, P.nnz, static_cast<int32_t>(c0), A.colind + z0, nullptr);
+        if (P.nnz > 0) {
+          FE_CHECK_CUDA(cudaMemcpyAsync(A.val64 + z0, P.val64, P.nnz * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, nullptr));
+          FE_CHECK_CUDA(cudaMemcpyAsync(A.val32 + z0, P.val32, P.nnz * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, nullptr));
+        }
+        r0 += P.rows;
+        c0 += P.cols;
+        z0 += P.nnz;
+      }
+      const int32_t last = static_cast<int32_t>(nnz);
+      FE_CHECK_CUDA(cudaMemcpy(A.rowptr + rows, &last, sizeof(int32_t), cudaMemcpyHostToDevice));
+      FE_CHECK_CUDA(cudaStreamSynchronize(nullptr));
+    } catch (...) {
+      fail();
+      throw;
+    }
+    *out = h.release();
+  });
+}
+
+// Batched symmetric eigensolver (parallel cyclic Jacobi, one CTA per matrix) for
+// small FP64 matrices, sizes m[p] <= 96 (host array), stored column-major with
+// leading dimension lda at A + p*lda*lda on the device. Writes ascending
+// eigenvalues to W + p*lda and eigenvectors to Z + p*lda*lda.
+extern "C" int fe_syevd_batched_f64(int32_t count, const int32_t* m, const double* A, int64_t lda,
+                                    double* W, double* Z, void* stream) {
+  return fe::guarded("fe_syevd_batched_f64", [&] {
+    FE_REQUIRE(count >= 0 && m, "invalid batch");
+    if (count == 0) return;
+    FE_REQUIRE(A && W && Z, "null matrix pointer");
+    int max_m = 1;
+    for (int32_t p = 0; p < count; ++p) {
+      FE_REQUIRE(m[p] >= 1 && m[p] <= fe::kBatchMaxDim,
+                 "matrix size must be in [1, " + std::to_string(fe::kBatchMaxDim) + "]");
+      FE_REQUIRE(m[p] <= lda, "lda smaller than a matrix size");
+      max_m = std::max<int>(max_m, m[p]);
+    }
+    cudaStream_t s = fe::as_stream(stream);
+    void *dm = nullptr, *dtodo = nullptr, *dzl = nullptr;
+    FE_CHECK_CUDA(cudaMallocAsync(&dm, count * sizeof(int32_t), s));
+    FE_CHECK_CUDA(cudaMallocAsync(&dtodo, count * sizeof(int32_t), s));
+    FE_CHECK_CUDA(cudaMallocAsync(&dzl, static_cast<size_t>(count) * lda * sizeof(double), s));
+    std::vector<int32_t> ones(count, 1);
+    try {
+      FE_CHECK_CUDA(cudaMemcpyAsync(dm, m, count * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+      FE_CHECK_CUDA(cudaMemcpyAsync(dtodo, ones.data(), count * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, s));
+      fe::BatchLayout L;
+      L.num_problems = count;
+      L.M = lda;
+      fe::bks_jacobi(L, A, static_cast<int32_t*>(dm), static_cast<int32_t*>(dtodo), max_m, W, Z,
+                     static_cast<double*>(dzl), s);
+      FE_CHECK_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+      cudaFreeAsync(dm, s);
+      cudaFreeAsync(dtodo, s);
+      cudaFreeAsync(dzl, s);
+      throw;
+    }
+    cudaFreeAsync(dm, s);
+    cudaFreeAsync(dtodo, s);
+    cudaFreeAsync(dzl, s);
+  });
+}

@@ -315,6 +315,86 @@ __global__ void convert_kernel(const S* __restrict__ src, int64_t lds, D* __rest
   }
 }
 
+// ------------------------------------------------ tall-skinny GEMV ----
+// The Lanczos recurrences multiply an n x k basis (k up to a few dozen) by one
+// vector: y = V^T x and x -= V h. A warp takes a row, its lanes the columns, so
+// each basis row is read once, coalesced; partial sums per row chunk are reduced
+// in a fixed order (deterministic).
+constexpr int kGemvMaxCols = 128;
+constexpr int kGemvLaneCols = kGemvMaxCols / 32;
+constexpr int kGemvThreads = 256;
+constexpr int kGemvTargetChunks = 148 * 8;
+
+template <typename T>
+__global__ void __launch_bounds__(kGemvThreads)
+gemv_t_partial_kernel(const T* __restrict__ V, int64_t ldv, const T* __restrict__ x, int64_t incx,
+                      int64_t n, int k, int64_t rows_per_chunk, double* __restrict__ part) {
+  __shared__ double red[kGemvThreads / 32][kGemvMaxCols];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int64_t r_begin = static_cast<int64_t>(blockIdx.x) * rows_per_chunk;
+  const int64_t r_end = min(n, r_begin + rows_per_chunk);
+  double acc[kGemvLaneCols];
+#pragma unroll
+  for (int t = 0; t < kGemvLaneCols; ++t) acc[t] = 0.0;
+  for (int64_t r = r_begin + warp; r < r_end; r += kGemvThreads / 32) {
+    const double xv = static_cast<double>(x[r * incx]);
+    const T* vr = V + r * ldv;
+#pragma unroll
+    for (int t = 0; t < kGemvLaneCols; ++t) {
+      const int j = lane + 32 * t;
+      if (j < k) acc[t] = fma(static_cast<double>(vr[j]), xv, acc[t]);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < kGemvLaneCols; ++t) red[warp][lane + 32 * t] = acc[t];
+  __syncthreads();
+  for (int j = threadIdx.x; j < k; j += kGemvThreads) {
+    double sum = 0.0;
+    for (int w = 0; w < kGemvThreads / 32; ++w) sum += red[w][j];
+    part[static_cast<int64_t>(blockIdx.x) * k + j] = sum;
+  }
+}
+
+__global__ void gemv_t_reduce_kernel(const double* __restrict__ part, int chunks, int k,
+                                     double* __restrict__ y) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= k) return;
+  double sum = 0.0;
+  for (int c = 0; c < chunks; ++c) sum += part[static_cast<int64_t>(c) * k + j];
+  y[j] = sum;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kGemvThreads)
+gemv_n_kernel(const T* __restrict__ V, int64_t ldv, const double* __restrict__ h, int k,
+              T* y, int64_t incy, int64_t n, double alpha, double beta, int use_beta) {
+  const int lane = threadIdx.x % 32;
+  double hr[kGemvLaneCols];
+#pragma unroll
+  for (int t = 0; t < kGemvLaneCols; ++t) {
+    const int j = lane + 32 * t;
+    hr[t] = j < k ? h[j] : 0.0;
+  }
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (kGemvThreads / 32);
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * (kGemvThreads / 32) + threadIdx.x / 32;
+       r < n; r += warps) {
+    const T* vr = V + r * ldv;
+    double sum = 0.0;
+#pragma unroll
+    for (int t = 0; t < kGemvLaneCols; ++t) {
+      const int j = lane + 32 * t;
+      if (j < k) sum = fma(static_cast<double>(vr[j]), hr[t], sum);
+    }
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) {
+      T* yr = y + r * incy;
+      double v = alpha * sum;
+      if (use_beta) v = fma(beta, static_cast<double>(*yr), v);
+      *yr = static_cast<T>(v);
+    }
+  }
+}
+
 }  // namespace
 
 // Workspace that suffices for every call with n' <= n, k' <= k, m' <= m, so a
@@ -366,6 +446,22 @@ void gram(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k
     return;
   }
   FE_REQUIRE(X && Y && ldx >= k && ldy >= m, "gram: invalid input block");
+  if (m == 1 && k <= kGemvMaxCols) {
+    // Basis-times-vector shape (Lanczos): G[:, 0] = X^T y by the GEMV kernels.
+    const int64_t chunks =
+        std::max<int64_t>(1, std::min<int64_t>(kGemvTargetChunks, (n + 255) / 256));
+    const int64_t rpc = (n + chunks - 1) / chunks;
+    const int64_t nchunks = (n + rpc - 1) / rpc;
+    FE_REQUIRE(ws && ws_bytes >= static_cast<size_t>(nchunks) * k * sizeof(double),
+               "gram: workspace too small");
+    gemv_t_partial_kernel<T><<<static_cast<unsigned>(nchunks), kGemvThreads, 0, s>>>(
+        X, ldx, Y, ldy, n, static_cast<int>(k), rpc, static_cast<double*>(ws));
+    check_launch("gemv_t_partial_kernel");
+    gemv_t_reduce_kernel<<<static_cast<unsigned>((k + 127) / 128), 128, 0, s>>>(
+        static_cast<const double*>(ws), static_cast<int>(nchunks), static_cast<int>(k), G);
+    check_launch("gemv_t_reduce_kernel");
+    return;
+  }
   const GramPlan p = gram_plan(n, k, m);
   FE_REQUIRE(ws && ws_bytes >= p.bytes, "gram: workspace too small");
   const bool sym = launch_gram_partial(X, ldx, Y, ldy, n, k, m, p, static_cast<double*>(ws), s);
@@ -396,6 +492,14 @@ void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t
   FE_REQUIRE(X && C && ldx >= k && ldc >= k, "rotate: invalid input");
   FE_REQUIRE(!ranges_overlap(X, n, ldx, k, static_cast<const T*>(Y), n, ldy, m),
              "rotate: X and Y overlap");
+  if (m == 1 && k <= kGemvMaxCols) {
+    // Basis-times-vector shape (Lanczos): y = alpha X c + beta y by the GEMV kernel.
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, 148 * 16));
+    gemv_n_kernel<T><<<static_cast<unsigned>(blocks), kGemvThreads, 0, s>>>(
+        X, ldx, C, static_cast<int>(k), Y, ldy, n, alpha, beta, beta != 0.0 ? 1 : 0);
+    check_launch("gemv_n_kernel");
+    return;
+  }
   if constexpr (std::is_same_v<T, double>) {
     if (g_f64_gemm_mode == 0) {
       rotate_dmma(X, ldx, C, ldc, Y, ldy, n, k, m, alpha, beta, s, upper_tri);

@@ -12,6 +12,7 @@
 #include "fe_common.cuh"
 
 #include <atomic>
+#include <map>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -46,6 +47,96 @@ void retain_pool_memory(int device) {
   uint64_t keep = UINT64_MAX;
   FE_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
   done[device] = true;
+}
+
+// ---- cache of large solve buffers --------------------------------------------
+// A solve allocates a handful of multi-GB blocks whose sizes repeat from one solve
+// of a configuration to the next. They are kept after release and handed back to
+// a request of the same (2 MiB-rounded) size on the same device: the release
+// records an event on its stream and the next user's stream waits on it, so reuse
+// is stream-ordered. A failed allocation first returns the cached blocks to the
+// device and retries.
+namespace {
+struct CachedBlock {
+  void* ptr;
+  cudaEvent_t ready;
+};
+std::mutex g_cache_mutex;
+std::map<std::pair<int, size_t>, std::vector<CachedBlock>> g_cache;
+
+size_t round_block(size_t bytes) {
+  const size_t g = size_t(2) << 20;
+  return (bytes + g - 1) / g * g;
+}
+
+void trim_cache(int device) {
+  std::vector<CachedBlock> drop;
+  {
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    for (auto it = g_cache.begin(); it != g_cache.end();) {
+      if (it->first.first == device) {
+        drop.insert(drop.end(), it->second.begin(), it->second.end());
+        it = g_cache.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+  for (auto& b : drop) {
+    cudaEventSynchronize(b.ready);
+    cudaEventDestroy(b.ready);
+    cudaFree(b.ptr);
+  }
+}
+}  // namespace
+
+void* big_alloc(size_t bytes, cudaStream_t s, size_t* granted) {
+  int dev = 0;
+  FE_CHECK_CUDA(cudaGetDevice(&dev));
+  const size_t want = round_block(bytes);
+  *granted = want;
+  {
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    auto it = g_cache.find({dev, want});
+    if (it != g_cache.end() && !it->second.empty()) {
+      CachedBlock b = it->second.back();
+      it->second.pop_back();
+      cudaError_t e = cudaStreamWaitEvent(s, b.ready, 0);
+      cudaEventDestroy(b.ready);
+      if (e != cudaSuccess) {
+        cudaFree(b.ptr);
+        FE_CHECK_CUDA(e);
+      }
+      return b.ptr;
+    }
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    trim_cache(dev);
+    e = cudaMalloc(&p, want);
+  }
+  if (e != cudaSuccess) {
+    throw Error(FE_ERR_ALLOC, std::string("cudaMalloc(") + std::to_string(want) +
+                                  ") failed: " + cudaGetErrorString(e));
+  }
+  return p;
+}
+
+void big_free(void* p, size_t granted, cudaStream_t s) {
+  int dev = 0;
+  cudaEvent_t ev = nullptr;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventRecord(ev, s) != cudaSuccess) {
+    if (ev) cudaEventDestroy(ev);
+    cudaStreamSynchronize(s);
+    cudaFree(p);
+    return;
+  }
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  g_cache[{dev, granted}].push_back({p, ev});
 }
 
 int num_sms() {
@@ -282,6 +373,9 @@ void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s) {
   check_launch("symmetrize_kernel");
 }
 
+template <typename S, typename D>
+void convert(const S* src, int64_t lds, D* dst, int64_t ldd, int64_t n, int64_t m, cudaStream_t s);
+
 // ------------------------------------------------------------------ CSR ----
 Csr* csr_create(int64_t rows, int64_t cols, int64_t nnz, const int32_t* rowptr,
                 const int32_t* colind, const double* values) {
@@ -316,8 +410,9 @@ Csr* csr_create(int64_t rows, int64_t cols, int64_t nnz, const int32_t* rowptr,
     if (nnz > 0) {
       FE_CHECK_CUDA(cudaMemcpy(A->colind, colind, nnz * sizeof(int32_t), cudaMemcpyHostToDevice));
       FE_CHECK_CUDA(cudaMemcpy(A->val64, values, nnz * sizeof(double), cudaMemcpyHostToDevice));
-      std::vector<float> v32(values, values + nnz);
-      FE_CHECK_CUDA(cudaMemcpy(A->val32, v32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice));
+      // FP32 copy of the values, rounded on the device
+      convert<double, float>(A->val64, 1, A->val32, 1, nnz, 1, nullptr);
+      FE_CHECK_CUDA(cudaStreamSynchronize(nullptr));
     }
   } catch (...) {
     cudaFree(A->rowptr);

@@ -55,6 +55,10 @@ void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s);
 cudaStream_t& alloc_stream();
 // Keep freed pool memory reserved for this process (called once per device).
 void retain_pool_memory(int device);
+// Large blocks (>= 64 MiB) of a solve: exact-size reuse across solves (see dense.cu).
+void* big_alloc(size_t bytes, cudaStream_t s, size_t* granted);
+void big_free(void* p, size_t granted, cudaStream_t s);
+constexpr size_t kBigBlockBytes = size_t(64) << 20;
 
 class DeviceBuffer {
  public:
@@ -63,9 +67,11 @@ class DeviceBuffer {
   ~DeviceBuffer() { release(); }
   DeviceBuffer(const DeviceBuffer&) = delete;
   DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-  DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), bytes_(o.bytes_), s_(o.s_) {
+  DeviceBuffer(DeviceBuffer&& o) noexcept
+      : p_(o.p_), bytes_(o.bytes_), granted_(o.granted_), s_(o.s_) {
     o.p_ = nullptr;
     o.bytes_ = 0;
+    o.granted_ = 0;
     o.s_ = nullptr;
   }
   DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
@@ -73,9 +79,11 @@ class DeviceBuffer {
       release();
       p_ = o.p_;
       bytes_ = o.bytes_;
+      granted_ = o.granted_;
       s_ = o.s_;
       o.p_ = nullptr;
       o.bytes_ = 0;
+      o.granted_ = 0;
       o.s_ = nullptr;
     }
     return *this;
@@ -85,6 +93,11 @@ class DeviceBuffer {
     release();
     if (bytes == 0) return;
     s_ = alloc_stream();
+    if (s_ && bytes >= kBigBlockBytes) {
+      p_ = big_alloc(bytes, s_, &granted_);
+      bytes_ = bytes;
+      return;
+    }
     cudaError_t e = s_ ? cudaMallocAsync(&p_, bytes, s_) : cudaMalloc(&p_, bytes);
     if (e != cudaSuccess) {
       p_ = nullptr;
@@ -95,11 +108,13 @@ class DeviceBuffer {
   }
   void release() {
     if (p_) {
-      if (s_) cudaFreeAsync(p_, s_);
+      if (granted_) big_free(p_, granted_, s_);
+      else if (s_) cudaFreeAsync(p_, s_);
       else cudaFree(p_);
     }
     p_ = nullptr;
     bytes_ = 0;
+    granted_ = 0;
     s_ = nullptr;
   }
   void* get() const { return p_; }
@@ -112,7 +127,8 @@ class DeviceBuffer {
  private:
   void* p_ = nullptr;
   size_t bytes_ = 0;
-  cudaStream_t s_ = nullptr;  // allocation stream (pool) or null (cudaMalloc)
+  size_t granted_ = 0;        // size of a cached large block (0: pool or plain allocation)
+  cudaStream_t s_ = nullptr;  // allocation stream (pool / cache) or null (cudaMalloc)
 };
 
 // Row-major n-by-cols block with leading dimension ld (padded to 8 elements so

@@ -24,6 +24,7 @@
 #include <limits>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <sstream>
 
@@ -185,25 +186,58 @@ struct PhaseEvents {
 // One solve's stream and cuSOLVER handle. While it lives, this thread's
 // DeviceBuffers are allocated from the device's stream-ordered pool on its stream
 // (buffers declared after the Context are released before it).
+// Streams and cuSOLVER handles are kept for reuse (per device, shared by all
+// threads): creating and destroying them per solve cost up to half a second
+// (the handle's own buffers are released with synchronizing frees).
+struct ContextResources {
+  int device;
+  cudaStream_t stream;
+  cusolverDnHandle_t solver;
+};
+std::mutex g_ctx_mutex;
+std::vector<ContextResources> g_ctx_free;
+
 class Context {
  public:
   cudaStream_t stream = nullptr;
   cusolverDnHandle_t solver = nullptr;
   Context() {
-    int dev = 0;
-    FE_CHECK_CUDA(cudaGetDevice(&dev));
-    retain_pool_memory(dev);
-    FE_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    FE_CHECK_SOLVER(cusolverDnCreate(&solver));
-    FE_CHECK_SOLVER(cusolverDnSetStream(solver, stream));
+    FE_CHECK_CUDA(cudaGetDevice(&device_));
+    retain_pool_memory(device_);
+    {
+      std::lock_guard<std::mutex> lock(g_ctx_mutex);
+      for (size_t i = 0; i < g_ctx_free.size(); ++i) {
+        if (g_ctx_free[i].device == device_) {
+          stream = g_ctx_free[i].stream;
+          solver = g_ctx_free[i].solver;
+          g_ctx_free.erase(g_ctx_free.begin() + static_cast<std::ptrdiff_t>(i));
+          break;
+        }
+      }
+    }
+    if (!stream) {
+      FE_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+      cusolverStatus_t st = cusolverDnCreate(&solver);
+      if (st == CUSOLVER_STATUS_SUCCESS) st = cusolverDnSetStream(solver, stream);
+      if (st != CUSOLVER_STATUS_SUCCESS) {
+        if (solver) cusolverDnDestroy(solver);
+        cudaStreamDestroy(stream);
+        throw Error(FE_ERR_CUDA, "cusolverDnCreate failed");
+      }
+    }
     prev_alloc_ = alloc_stream();
     alloc_stream() = stream;
   }
   ~Context() {
     alloc_stream() = prev_alloc_;
-    if (stream) cudaStreamSynchronize(stream);
-    if (solver) cusolverDnDestroy(solver);
-    if (stream) cudaStreamDestroy(stream);
+    if (!stream) return;
+    if (cudaStreamSynchronize(stream) == cudaSuccess) {
+      std::lock_guard<std::mutex> lock(g_ctx_mutex);
+      g_ctx_free.push_back({device_, stream, solver});
+    } else {
+      if (solver) cusolverDnDestroy(solver);
+      cudaStreamDestroy(stream);
+    }
   }
   Context(const Context&) = delete;
   Context& operator=(const Context&) = delete;
@@ -219,6 +253,7 @@ class Context {
 
  private:
   cudaStream_t prev_alloc_ = nullptr;
+  int device_ = 0;
 };
 
 // Host std::mt19937 draws in the reference's column-major order
@@ -642,14 +677,19 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     return std::chrono::duration<double, std::milli>(clock::now() - t).count();
   };
   Context ctx;
+  if (opt.verbosity >= 2)
+    std::fprintf(stderr, "[fe] context %.1f ms\n", ms_since(t_start));
   SmallState sm;
   sm.allocate(n, cap, mixed && opt.tensor_cores && tc_gemm_available());
   ProjectedEig eig(ctx, cap);
 
   double lower = 0, upper = 0;
+  const auto t_bounds = clock::now();
   lanczos_bounds(ctx, A, sign, seed, host_init, lower, upper);
   st.lower = lower;
   st.upper = upper;
+  if (opt.verbosity >= 2)
+    std::fprintf(stderr, "[fe] Lanczos bounds %.1f ms\n", ms_since(t_bounds));
 
   std::unique_ptr<ChebLoop<float>> l32;
   std::unique_ptr<ChebLoop<double>> l64;
@@ -689,6 +729,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   std::vector<double> W, rel, worst_history;
   int64_t it_done = 0;
   const double tol = opt.tol;
+  const auto t_loop = clock::now();
   for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
     // Damped interval [cutoff, upper]: the reference fixes the cutoff where the
     // filter amplifies `lower` by 1e3. bounds=ritz (after the first cycle) damps
@@ -757,6 +798,8 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   // fasteig_problem::solve recomputes for non-Krylov solvers on the host
   // (src/fasteig_problem.cpp:419-422, src/fasteig_solver.cpp:89-129).
   for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = sign * W[j];
+  if (opt.verbosity >= 2)
+    std::fprintf(stderr, "[fe] filter cycles (wall) %.1f ms\n", ms_since(t_loop));
   const auto t_finish = clock::now();
   {
     cudaStream_t s = ctx.stream;
@@ -2173,6 +2216,8 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
   }
   const auto t1 = std::chrono::steady_clock::now();
   st.seconds = std::chrono::duration<double>(t1 - t0).count();
+  if (opt.verbosity >= 2)
+    std::fprintf(stderr, "[fe] solve total (incl. buffer release) %.1f ms\n", st.seconds * 1e3);
   if (stats) {
     stats[0] = st.iterations;
     stats[1] = st.status;

@@ -39,6 +39,10 @@ void set_f64_gemm_mode(int mode);
 
 __device__ int g_tc_status = 0;  // 0 = ok, otherwise a code of the first failed wait
 
+// Aligned 3xTF32 rotations on the persistent kernel (1) or one CTA per tile (0).
+static int g_rotate_persistent = 1;
+void set_rotate_persistent(int on) { g_rotate_persistent = on; }
+
 namespace {
 
 constexpr int kM = 128;           // MMA M (TMEM lanes)
@@ -529,6 +533,199 @@ rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
   epilogue_dealloc(sm, warp, tmem);
 }
 
+// Persistent variant for 16-byte aligned outputs: one CTA per SM loops over
+// tiles (column tile fastest); the operand ring continues across tiles and the
+// accumulator alternates between two TMEM buffers, so four dedicated epilogue
+// warps drain tile i while the producer, split and MMA warps already run tile
+// i+1 (no per-tile prologue, pipeline fill or exposed epilogue). Warps: 0 TMA
+// producer, 1 MMA issuer, 2-5 hi/lo split, 6-9 epilogue.
+constexpr int kPersistThreads = 320;
+constexpr uint32_t kPersistTmemCols = 512;
+constexpr uint32_t kAccStride = 256;  // TMEM columns between the two accumulators
+
+__global__ void __launch_bounds__(kPersistThreads, 1)
+rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
+                            const __grid_constant__ CUtensorMap tmCh,
+                            const __grid_constant__ CUtensorMap tmCl, int64_t n, int k, int m,
+                            int m_tiles, int64_t total_tiles, float* __restrict__ Y, int64_t ldy,
+                            float alpha, float beta, int use_beta, int upper_tri) {
+  extern __shared__ uint8_t dyn_smem[];
+  const Smem sm = carve(dyn_smem);
+  // Accumulator full (MMA -> epilogue) and empty (epilogue -> MMA) barriers, after
+  // the TMEM address slot.
+  uint64_t* accf = reinterpret_cast<uint64_t*>(sm.tmem_slot + 2);
+  uint64_t* acce = accf + 2;
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+      mbar_init(&sm.split[s], kSplitThreads);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(sm.tmem_slot)),
+                 "r"(kPersistTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *sm.tmem_slot;
+  const int nkb_full = (k + kKB - 1) / kKB;
+  auto tile_nkb = [&](int j0) {
+    return upper_tri ? (min(k, j0 + kN) + kKB - 1) / kKB : nkb_full;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t g = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; ok && t < total_tiles; t += gridDim.x) {
+        const int j0 = static_cast<int>(t % m_tiles) * kN;
+        const int r0 = static_cast<int>((t / m_tiles) * kM);
+        const int nkb = tile_nkb(j0);
+        for (int kb = 0; kb < nkb; ++kb, ++g) {
+          const int s = static_cast<int>(g % kStages);
+          const uint32_t ph = (g / kStages) & 1u;
+          if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&sm.full[s], kABytes + 2 * kBBytes);
+          tma_load_2d(sm.a_hi(s), &tmX, kb * kKB, r0, &sm.full[s]);
+          tma_load_2d(sm.b_hi(s), &tmCh, kb * kKB, j0, &sm.full[s]);
+          tma_load_2d(sm.b_lo(s), &tmCl, kb * kKB, j0, &sm.full[s]);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_tf32(false, false);
+      uint32_t g = 0;
+      int lt = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; ok && t < total_tiles; t += gridDim.x, ++lt) {
+        const int j0 = static_cast<int>(t % m_tiles) * kN;
+        const int nkb = tile_nkb(j0);
+        const int b = lt & 1;
+        if (lt >= 2 && !mbar_wait(&acce[b], static_cast<uint32_t>((lt >> 1) - 1) & 1u, 5)) break;
+        tc_fence_after();
+        const uint32_t acc_tmem = tmem + static_cast<uint32_t>(b) * kAccStride;
+        for (int kb = 0; kb < nkb; ++kb, ++g) {
+          const int s = static_cast<int>(g % kStages);
+          const uint32_t ph = (g / kStages) & 1u;
+          if (!mbar_wait(&sm.split[s], ph, 3)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t ah = smem_u32(sm.a_hi(s)), al = smem_u32(sm.a_lo(s));
+          const uint32_t bh = smem_u32(sm.b_hi(s)), bl = smem_u32(sm.b_lo(s));
+#pragma unroll
+          for (int kk = 0; kk < kKB / 8; ++kk) {
+            const uint32_t off = kk * 32u;
+            const uint64_t dah = smem_desc(ah + off, 16u, 1024u, kLayoutSW128);
+            const uint64_t dal = smem_desc(al + off, 16u, 1024u, kLayoutSW128);
+            const uint64_t dbh = smem_desc(bh + off, 16u, 1024u, kLayoutSW128);
+            const uint64_t dbl = smem_desc(bl + off, 16u, 1024u, kLayoutSW128);
+            const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+            umma_tf32(acc_tmem, dah, dbh, idesc, acc);
+            umma_tf32(acc_tmem, dah, dbl, idesc, 1u);
+            umma_tf32(acc_tmem, dal, dbh, idesc, 1u);
+          }
+          umma_commit(&sm.empty[s]);
+        }
+        if (!ok) break;
+        umma_commit(&accf[b]);
+      }
+    }
+    __syncwarp();
+  } else if (warp < 6) {
+    const int tid = threadIdx.x - 64;
+    uint32_t g = 0;
+    bool ok = true;
+    for (int64_t t = blockIdx.x; ok && t < total_tiles; t += gridDim.x) {
+      const int j0 = static_cast<int>(t % m_tiles) * kN;
+      const int nkb = tile_nkb(j0);
+      for (int kb = 0; kb < nkb; ++kb, ++g) {
+        const int s = static_cast<int>(g % kStages);
+        const uint32_t ph = (g / kStages) & 1u;
+        if (!mbar_wait(&sm.full[s], ph, 2)) {
+          ok = false;
+          break;
+        }
+        split_tile(sm.a_hi(s), sm.a_lo(s), kABytes / 16, tid);
+        fence_proxy_async();
+        mbar_arrive(&sm.split[s]);
+      }
+    }
+  } else {
+    const int q = warp % 4;
+    int lt = 0;
+    for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x, ++lt) {
+      const int j0 = static_cast<int>(t % m_tiles) * kN;
+      const int64_t r0 = (t / m_tiles) * kM;
+      const int b = lt & 1;
+      if (!mbar_wait(&accf[b], static_cast<uint32_t>(lt >> 1) & 1u, 4)) break;
+      tc_fence_after();
+      const int64_t r = r0 + q * 32 + lane;
+      const uint32_t base = tmem + static_cast<uint32_t>(b) * kAccStride +
+                            (static_cast<uint32_t>(q * 32) << 16);
+      for (int c = 0; c < kN; c += 16) {
+        float v[16];
+        tmem_ld16(base + c, v);
+        if (r >= n) continue;
+        float* yr = Y + r * ldy + j0 + c;
+        if (j0 + c + 16 <= m) {
+#pragma unroll
+          for (int e = 0; e < 16; e += 4) {
+            float4 o = make_float4(alpha * v[e], alpha * v[e + 1], alpha * v[e + 2],
+                                   alpha * v[e + 3]);
+            if (use_beta) {
+              const float4 y = *reinterpret_cast<const float4*>(yr + e);
+              o.x = fmaf(beta, y.x, o.x);
+              o.y = fmaf(beta, y.y, o.y);
+              o.z = fmaf(beta, y.z, o.z);
+              o.w = fmaf(beta, y.w, o.w);
+            }
+            *reinterpret_cast<float4*>(yr + e) = o;
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            if (j0 + c + e < m) {
+              float out = alpha * v[e];
+              if (use_beta) out = fmaf(beta, yr[e], out);
+              yr[e] = out;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[b]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kPersistTmemCols)
+                 : "memory");
+  }
+}
+
 // C (k x m FP64 column-major) -> Ch, Cl (m_pad x k_pad FP32 row-major = C^T, K-major),
 // zero-padded.
 __global__ void rotate_prep_kernel(const double* __restrict__ C, int64_t ldc, int k, int m,
@@ -696,6 +893,22 @@ void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float*
   const int64_t m_tiles = m_pad / kN;
   FE_REQUIRE(row_tiles * m_tiles <= 2147483647LL, "rotate_tc: too many tiles");
   const bool vec = (reinterpret_cast<uintptr_t>(Y) & 15u) == 0 && ldy % 4 == 0;
+  const int64_t total_tiles = row_tiles * m_tiles;
+  if (vec && g_rotate_persistent) {
+    static std::once_flag once_p;
+    std::call_once(once_p, [] {
+      FE_CHECK_CUDA(cudaFuncSetAttribute(rotate_tc_persistent_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kSmemBytes));
+    });
+    const int64_t ctas = std::min<int64_t>(total_tiles, num_sms());
+    rotate_tc_persistent_kernel<<<static_cast<unsigned>(ctas), kPersistThreads, kSmemBytes, s>>>(
+        mx, mh, ml, n, static_cast<int>(k), static_cast<int>(m), static_cast<int>(m_tiles),
+        total_tiles, Y, ldy, static_cast<float>(alpha), static_cast<float>(beta), beta != 0.0,
+        upper_tri ? 1 : 0);
+    check_launch("rotate_tc_persistent_kernel");
+    return;
+  }
   dim3 grid(static_cast<unsigned>(row_tiles * m_tiles));
   rotate_tc_kernel<<<grid, kThreads, kSmemBytes, s>>>(mx, mh, ml, n, static_cast<int>(k),
                                                       static_cast<int>(m),
@@ -731,6 +944,13 @@ extern "C" int fe_set_spmm_kernel(int32_t mode) {
   return fe::guarded("fe_set_spmm_kernel", [&] {
     FE_REQUIRE(mode >= 0 && mode <= 3, "mode must be 0..3");
     fe::set_spmm_mode(mode);
+  });
+}
+
+extern "C" int fe_set_tc_rotate_kernel(int32_t mode) {
+  return fe::guarded("fe_set_tc_rotate_kernel", [&] {
+    FE_REQUIRE(mode >= 0 && mode <= 1, "mode must be 0 or 1");
+    fe::set_rotate_persistent(mode == 0 ? 1 : 0);
   });
 }
 

@@ -10,6 +10,8 @@ from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
+
 import torch
 
 from ._lib import check, lib
@@ -174,3 +176,19 @@ def device_status(clear: bool = False) -> int:
     v = C.c_int32()
     check(lib.fe_device_status(C.byref(v), 1 if clear else 0))
     return int(v.value)
+
+
+def syevd_batched(A: torch.Tensor, sizes) -> tuple:
+    """Eigen-decomposition of a batch of small symmetric FP64 matrices
+    (``fe_syevd_batched_f64``). A: CUDA float64 (count, lda, lda); matrix p occupies
+    its leading sizes[p] x sizes[p] block. Returns (W, Z) with W[p, :m] ascending and
+    Z[p, :m, :m] holding the eigenvectors as columns."""
+    assert A.is_cuda and A.dtype == torch.float64 and A.dim() == 3 and A.is_contiguous()
+    count, lda, _ = A.shape
+    m = np.ascontiguousarray(np.asarray(sizes, dtype=np.int32))
+    W = torch.zeros((count, lda), dtype=torch.float64, device=A.device)
+    Zc = torch.zeros((count, lda, lda), dtype=torch.float64, device=A.device)
+    # A is symmetric, so its row-major and column-major storage agree.
+    check(lib.fe_syevd_batched_f64(count, m.ctypes.data, A.data_ptr(), lda, W.data_ptr(),
+                                   Zc.data_ptr(), _stream()))
+    return W, Zc.transpose(1, 2)  # column-major storage -> Z[p][i, j] = component i of vector j

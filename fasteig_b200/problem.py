@@ -105,7 +105,26 @@ class CsrMatrix:
 
     @property
     def nnz(self) -> int:
-        return int(self.values.size)
+        if self.values is not None:
+            return int(self.values.size)
+        z = C.c_int64()
+        check(lib.fe_csr_info(self.handle, None, None, C.byref(z)))
+        return int(z.value)
+
+    @classmethod
+    def block_diag(cls, parts) -> "CsrMatrix":
+        """Block-diagonal operator of device CSR parts (``fe_csr_block_diag``): an SpMM
+        on it is the grouped SpMM of all parts."""
+        parts = list(parts)
+        handles = (C.c_void_p * len(parts))(*[p.handle for p in parts])
+        h = C.c_void_p()
+        check(lib.fe_csr_block_diag(len(parts), C.cast(handles, C.c_void_p), C.byref(h)))
+        obj = cls.__new__(cls)
+        obj.handle = h
+        obj.rowptr = obj.colind = obj.values = None
+        obj.rows = sum(p.rows for p in parts)
+        obj.cols = sum(p.cols for p in parts)
+        return obj
 
     def autotune(self, ncols: int, precision: str = "fp32") -> int:
         """Pick the fastest SpMM kernel for n x ncols blocks on this operator

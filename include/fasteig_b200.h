@@ -188,6 +188,11 @@ int fe_csr_autotune(fe_csr_t A, int64_t ncols, int32_t precision, void* stream, 
  * 1 = SIMT FP64-FMA kernels. Both accumulate every output in FP64; results
  * differ only in the order of the rounded additions. */
 int fe_set_f64_gemm_kernel(int32_t mode);
+/* 3xTF32 rotation kernel for 16-byte aligned outputs, for all later calls:
+ * 0 = default (persistent kernel, one CTA per SM looping over tiles with two
+ * TMEM accumulators), 1 = one CTA per tile. Same arithmetic; unaligned outputs
+ * always use the one-CTA-per-tile kernel with its staged epilogue. */
+int fe_set_tc_rotate_kernel(int32_t mode);
 
 /* ---------------------------------------------------------------------
  * Ritz residuals and column norms (replaces the copy + add_scaled_columns +
@@ -282,6 +287,21 @@ int fe_batch_krylov_schur(int32_t count, const fe_csr_t* A, const int64_t* nev,
                           const char* options, double* eigenvalues, double* residual_norms,
                           double* eigenvectors, int32_t* iterations, int32_t* status,
                           double* stats);
+
+/* Block-diagonal operator of `count` CSR handles on one device (part p's rows and
+ * columns follow those of parts 0..p-1); an SpMM on it is the grouped SpMM of
+ * all parts in one launch (the reference applies one operator per process).
+ * The result is a new handle (release with fe_csr_destroy); parts stay valid. */
+int fe_csr_block_diag(int32_t count, const fe_csr_t* parts, fe_csr_t* out);
+
+/* Batched symmetric eigensolver for `count` small FP64 matrices (replaces one
+ * Dsyevd per projected matrix, src/gpu/CudaLanczosWorkspace.cpp:155): sizes
+ * m[count] (host array, each in [1, 96]), matrix p column-major at
+ * A + p*lda*lda on the device (lda >= max m); ascending eigenvalues to
+ * W + p*lda, eigenvectors to Z + p*lda*lda. Parallel cyclic Jacobi, one CTA per
+ * matrix; returns after the stream has finished. */
+int fe_syevd_batched_f64(int32_t count, const int32_t* m, const double* A, int64_t lda,
+                         double* W, double* Z, void* stream);
 
 /* ---------------------------------------------------------------------
  * Request server (extension; the reference's fasteig_problem::solve,

@@ -312,3 +312,73 @@ def test_autotuned_spmm_matches_oracle(dtype):
     scale = 0.5 * (absA(A) @ np.abs(X64))
     tol = 1e-13 if dtype == torch.float64 else 4e-6
     assert np.all(np.abs(Y.double().cpu().numpy() - ref) <= tol * scale + 1e-300)
+
+
+def test_batched_syevd_matches_numpy():
+    """fe_syevd_batched_f64: eigenvalues within 1e-12 |A| of numpy's, eigenvectors
+    orthonormal and satisfying A z = l z to 1e-12 |A|, for sizes 1..96 in one call."""
+    from fasteig_b200 import ops
+    sizes = [1, 2, 5, 17, 20, 33, 64, 95, 96]
+    lda = 96
+    rng = np.random.default_rng(3)
+    A = np.zeros((len(sizes), lda, lda))
+    for p, m in enumerate(sizes):
+        B = rng.standard_normal((m, m))
+        A[p, :m, :m] = B + B.T
+    W, Z = ops.syevd_batched(torch.from_numpy(A).cuda(), sizes)
+    W, Z = W.cpu().numpy(), Z.cpu().numpy()
+    for p, m in enumerate(sizes):
+        a = A[p, :m, :m]
+        scale = np.abs(a).max() * m
+        ref = np.linalg.eigvalsh(a)
+        assert np.all(np.abs(W[p, :m] - ref) <= 1e-12 * scale), p
+        z = Z[p, :m, :m]
+        assert np.abs(z.T @ z - np.eye(m)).max() <= 1e-12 * m
+        assert np.abs(a @ z - z * W[p, :m]).max() <= 1e-12 * scale
+
+
+def test_block_diag_grouped_spmm():
+    """An SpMM on fe_csr_block_diag(parts) equals each part's SpMM on its rows."""
+    from fasteig_b200 import CsrMatrix, ops
+    from oracle import oracle as O
+    parts = [rand_sym_csr(n, 0.02, 10 + i) for i, n in enumerate([300, 1, 517, 64])]
+    dev = [dev_csr(A) for A in parts]
+    G = CsrMatrix.block_diag(dev)
+    assert G.rows == sum(A.rows for A in parts) and G.nnz == sum(A.values.size for A in parts)
+    X = block(G.rows, 40, torch.float64, 7)
+    Y = torch.zeros_like(X)
+    ops.spmm(G, X, Y, 1.0, 0.0)
+    torch.cuda.synchronize()
+    X64, Y64 = X.cpu().numpy(), Y.cpu().numpy()
+    r0 = 0
+    for A in parts:
+        ref = A.scipy() @ X64[r0:r0 + A.rows]
+        scale = absA(A) @ np.abs(X64[r0:r0 + A.rows])
+        assert np.all(np.abs(Y64[r0:r0 + A.rows] - ref) <= 1e-13 * scale + 1e-300)
+        r0 += A.rows
+    G.close()
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("n,k", [(1, 1), (300, 20), (70001, 97), (2049, 128)])
+def test_basis_times_vector_products(dtype, n, k):
+    """Lanczos-shaped products (m = 1: V^T x and y = a V c + b y, the vector a
+    strided column) keep the Gram and rotation bounds."""
+    from fasteig_b200 import ops
+    V = block(n, k, dtype, 51, ld=k + 3)
+    Xw = block(n, 2, dtype, 52, ld=5)
+    x = Xw[:, 1:2]
+    V64, x64 = V.double().cpu().numpy(), x.double().cpu().numpy()
+    G = ops.gram(V, x).cpu().numpy()
+    ref = V64.T @ x64
+    assert np.all(np.abs(G - ref) <= 1e-13 * (np.abs(V64).T @ np.abs(x64)) + 1e-300)
+    c = torch.randn(k, 1, dtype=torch.float64, generator=torch.Generator().manual_seed(1)).cuda()
+    c64 = c.cpu().numpy()
+    if dtype == torch.float32:
+        c64 = c64.astype(np.float32).astype(np.float64)
+    y0 = x.double().cpu().numpy()
+    ops.rotate(V, c, x, -1.0, 1.0)
+    got = x.double().cpu().numpy()
+    ref = y0 - V64 @ c64
+    tol = 1e-13 if dtype == torch.float64 else (k + 2) * 2.0 ** -22
+    assert np.all(np.abs(got - ref) <= tol * (np.abs(V64) @ np.abs(c64) + np.abs(y0)) + 1e-300)

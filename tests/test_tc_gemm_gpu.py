@@ -102,3 +102,41 @@ def test_rotate_tf32x3_deflation_update_in_place(locked, sub):
     assert np.all(err <= (locked + 4) * 2.0 ** -22 * scale + 1e-30), (err / scale).max()
     # untouched locked columns
     assert np.array_equal(V[:, :locked].double().cpu().numpy(), V64[:, :locked])
+
+
+@pytest.fixture(params=[0, 1], ids=["persistent", "per_tile"])
+def rotate_kernel(request):
+    import fasteig_b200 as fe
+    assert fe.lib.fe_set_tc_rotate_kernel(request.param) == 0
+    yield request.param
+    assert fe.lib.fe_set_tc_rotate_kernel(0) == 0
+
+
+@pytest.mark.parametrize("n,k,m", [(128, 8, 8), (20000, 256, 320), (70001, 320, 320),
+                                   (33333, 320, 200), (131072, 64, 160)])
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.0, 1.0)])
+def test_rotate_tf32x3_both_kernels(rotate_kernel, n, k, m, alpha, beta):
+    """The persistent (several tiles per CTA, alternating TMEM accumulators) and the
+    one-CTA-per-tile rotation give the same product within the 3xTF32 bound, and the
+    persistent one is bit-identical to the per-tile one (same MMAs, same order)."""
+    import fasteig_b200 as fe
+    from fasteig_b200 import ops
+    assert ops.device_status(clear=True) == 0
+    X = blk(n, k, 15, ld=((k + 3) // 4) * 4)
+    Y = blk(n, m, 16)
+    Y0 = Y.clone()
+    Cm = torch.randn(k, m, dtype=torch.float64, generator=torch.Generator().manual_seed(2)).cuda()
+    X64, Y64, C64 = X.double().cpu().numpy(), Y.double().cpu().numpy(), Cm.cpu().numpy()
+    ref = alpha * X64 @ C64 + (beta * Y64 if beta else 0.0)
+    ops.rotate_tf32x3(X, Cm, Y, alpha, beta)
+    torch.cuda.synchronize()
+    assert ops.device_status() == 0
+    scale = np.abs(X64) @ np.abs(C64) + (abs(beta) * np.abs(Y64) if beta else 0.0)
+    err = np.abs(Y.double().cpu().numpy() - ref)
+    assert np.all(err <= (k + 4) * 2.0 ** -22 * scale + 1e-30), (err / scale).max()
+    other = 1 - rotate_kernel
+    assert fe.lib.fe_set_tc_rotate_kernel(other) == 0
+    Y2 = Y0.clone()
+    ops.rotate_tf32x3(X, Cm, Y2, alpha, beta)
+    torch.cuda.synchronize()
+    assert torch.equal(Y, Y2)
