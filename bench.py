@@ -380,7 +380,11 @@ def solve_opts(a, precision, seed):
     return o
 
 
-def roofline_cheb_step(a, H, dA, peak, launches=20):
+SPMM_KERNEL_NAMES = {0: "csr_spmm_row_kernel<float,2,5,7>", 1: "csr_spmm_kernel<float,4,32,*>",
+                     2: "csr_spmm_pipe_kernel<float,4,*>", 3: "csr_spmm_row_kernel<float,4,2,7>"}
+
+
+def roofline_cheb_step(a, H, dA, peak, launches=20, mode=0):
     """Time the dominant kernel (fused FP32 Chebyshev step, 320 columns) with CUDA
     events on the stream it is launched on; achieved = algorithmic bytes / time."""
     import torch
@@ -402,7 +406,8 @@ def roofline_cheb_step(a, H, dA, peak, launches=20):
     achieved = algo / (ms * 1e-3) / 1e9
     del X, Z
     torch.cuda.empty_cache()
-    return {"kernel": "csr_spmm_row_kernel<float,2,5,7> (fused Chebyshev step, FP32, 320 cols)",
+    return {"kernel": SPMM_KERNEL_NAMES.get(mode, "csr_spmm") + " (fused Chebyshev step, FP32, "
+                      f"{a.block} cols)",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
             "algorithmic_bytes": algo, "ms_per_launch": round(ms, 4)}
@@ -506,6 +511,8 @@ def main():
 
     H = build_matrix(a)
     dA = fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values)
+    # The SpMM kernel for this operator and block width is picked by measurement.
+    tuned = {"fp32": dA.autotune(a.block, "fp32"), "fp64": dA.autotune(a.block, "fp64")}
     seed = 1 + rank
     opts = solve_opts(a, "mixed", seed)
 
@@ -598,7 +605,7 @@ def main():
                     "cycles": runs[-1].stats["iterations"], "converged": c64}
             extra["fp64_plain"] = fp64
             extra["mixed_vs_fp64"] = round((value / world) / fp64["value"], 3) if fp64["value"] else None
-        extra["roofline"] = roofline_cheb_step(a, H, dA, peak)
+        extra["roofline"] = roofline_cheb_step(a, H, dA, peak, mode=tuned["fp32"])
         extra["roofline"]["peak_kind"] = f"{peak_kind} hbm_gbs (burst copy)"
         if world == 1 and not a.no_cpu:
             cycles = fp64["cycles"] if fp64 else REFERENCE_CYCLES
@@ -607,7 +614,8 @@ def main():
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(elapsed / a.steps * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic", "impl": "b200",
-            "config": config_dict(a, {"parallelism": f"replicas x{world}"}),
+            "config": config_dict(a, {"parallelism": f"replicas x{world}",
+                                      "spmm_kernel_autotuned": tuned}),
             "converged_pairs": converged, "latency_s": {"p50": lat[len(lat) // 2], "max": lat[-1]},
             "solve_seconds": [round(s["seconds"], 3) for s in per_solve],
             "phase_ms": [[round(s["filter_ms"]), round(s["ortho_ms"]), round(s["rr_ms"])]

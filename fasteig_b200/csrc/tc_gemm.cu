@@ -323,7 +323,7 @@ __device__ void mma_loop(const Smem& sm, uint32_t tmem, int nkb, uint32_t idesc)
 __global__ void __launch_bounds__(kThreads, 1)
 gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmY,
                int64_t n, int k, int m, int sx, int sy, int k_tiles, int64_t rows_per_chunk,
-               float* __restrict__ partial) {
+               float* __restrict__ partial, int symmetric) {
   extern __shared__ uint8_t dyn_smem[];
   const Smem sm = carve(dyn_smem);
   const int warp = threadIdx.x / 32;
@@ -332,6 +332,8 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   const int tj = blockIdx.x / k_tiles;
   const int i0 = ti * kM;   // tile origin in shifted (tensor-map) column space of X
   const int j0 = tj * kN;
+  // X^T X: a tile wholly below the diagonal is the transpose of a computed one.
+  if (symmetric && i0 >= j0 + kN) return;
   const int64_t r_begin = static_cast<int64_t>(blockIdx.y) * rows_per_chunk;
   const int64_t r_end = min(n, r_begin + rows_per_chunk);
   const int nkb = static_cast<int>((r_end - r_begin + kKB - 1) / kKB);
@@ -408,14 +410,20 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   epilogue_dealloc(sm, warp, tmem);
 }
 
+// With `symmetric` (X^T X: k == m, equal column shift `shift`), entries of tiles
+// that lie wholly below the diagonal were not computed and read their mirror.
 __global__ void gram_tc_reduce(const float* __restrict__ partial, int chunks, int k, int m,
-                               double* __restrict__ G, int64_t ldg) {
+                               double* __restrict__ G, int64_t ldg, int symmetric, int shift) {
   const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t total = static_cast<int64_t>(k) * m;
   if (idx >= total) return;
+  const int i = static_cast<int>(idx % k), j = static_cast<int>(idx / k);
+  int64_t src = idx;
+  if (symmetric && ((i + shift) / kM) * kM >= ((j + shift) / kN) * kN + kN)
+    src = static_cast<int64_t>(i) * k + j;
   double s = 0.0;
-  for (int c = 0; c < chunks; ++c) s += static_cast<double>(partial[c * total + idx]);
-  G[(idx / k) * ldg + (idx % k)] = s;
+  for (int c = 0; c < chunks; ++c) s += static_cast<double>(partial[c * total + src]);
+  G[static_cast<int64_t>(j) * ldg + i] = s;
 }
 
 // --------------------------------------------------------------- Rotation ----
@@ -849,14 +857,17 @@ void gram_tc(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n
   const CUtensorMap my = make_map(Ya, m + sy, n, ldy, 32, kKB, true);
   static std::once_flag once;
   std::call_once(once, [] { set_smem_attr(reinterpret_cast<const void*>(gram_tc_kernel)); });
+  const bool sym = X == Y && ldx == ldy && k == m;
   dim3 grid(p.k_tiles * p.m_tiles, p.chunks);
   gram_tc_kernel<<<grid, kThreads, kSmemBytes, s>>>(mx, my, n, static_cast<int>(k),
                                                     static_cast<int>(m), sx, sy, p.k_tiles,
-                                                    p.rows_per_chunk, static_cast<float*>(ws));
+                                                    p.rows_per_chunk, static_cast<float*>(ws),
+                                                    sym ? 1 : 0);
   check_launch("gram_tc_kernel");
   const int64_t total = k * m;
   gram_tc_reduce<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
-      static_cast<const float*>(ws), p.chunks, static_cast<int>(k), static_cast<int>(m), G, ldg);
+      static_cast<const float*>(ws), p.chunks, static_cast<int>(k), static_cast<int>(m), G, ldg,
+      sym ? 1 : 0, sx);
   check_launch("gram_tc_reduce");
 }
 

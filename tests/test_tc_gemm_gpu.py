@@ -140,3 +140,24 @@ def test_rotate_tf32x3_both_kernels(rotate_kernel, n, k, m, alpha, beta):
     ops.rotate_tf32x3(X, Cm, Y2, alpha, beta)
     torch.cuda.synchronize()
     assert torch.equal(Y, Y2)
+
+
+@pytest.mark.parametrize("n,k,off", [(5000, 320, 0), (33333, 300, 1), (4096, 400, 3), (777, 130, 2)])
+def test_gram_tf32x3_symmetric_mirrored_tiles(n, k, off):
+    """X^T X skips the tiles wholly below the diagonal and mirrors them in the FP64
+    reduction: the mirrored entries equal their transposes and every entry keeps the
+    split-TF32 bound, also for a column view that does not start on a 16-byte boundary."""
+    from fasteig_b200 import ops
+    assert ops.device_status(clear=True) == 0
+    V = blk(n, k + off, 21, ld=((k + off + 3) // 4) * 4)
+    X = V[:, off:off + k]
+    G = ops.gram_tf32x3(X, X).cpu().numpy()
+    torch.cuda.synchronize()
+    assert ops.device_status() == 0
+    X64 = X.double().cpu().numpy()
+    ref = X64.T @ X64
+    scale = np.abs(X64).T @ np.abs(X64)
+    assert np.all(np.abs(G - ref) <= 4e-6 * scale + 1e-30), (np.abs(G - ref) / scale).max()
+    i, j = np.indices(G.shape)
+    mirrored = ((i + off) // 128) * 128 >= ((j + off) // 160) * 160 + 160
+    assert np.array_equal(G[mirrored], G.T[mirrored])
