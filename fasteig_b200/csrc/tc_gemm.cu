@@ -50,6 +50,10 @@ constexpr int kN = 160;           // MMA N (columns per CTA tile)
 constexpr int kKB = 32;           // FP32 elements per 128-byte swizzle row
 constexpr int kStages = 3;
 constexpr int kThreads = 192;     // 6 warps
+// The Gram splits both operands (36 KB per K stage against the rotation's 16 KB),
+// so it runs 8 splitting warps.
+constexpr int kGramSplitThreads = 256;
+constexpr int kGramThreads = 64 + kGramSplitThreads;
 constexpr int kSplitThreads = 128;
 constexpr uint32_t kTmemCols = 256;
 
@@ -191,21 +195,43 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
   return r;
 }
 
-// Split n_vec16 16-byte chunks of raw FP32 data in place into hi, and into lo.
+__device__ __forceinline__ void split4(const float4& v, float4& hi, float4& lw) {
+  hi.x = __uint_as_float(tf32_rna(v.x));
+  hi.y = __uint_as_float(tf32_rna(v.y));
+  hi.z = __uint_as_float(tf32_rna(v.z));
+  hi.w = __uint_as_float(tf32_rna(v.w));
+  lw.x = __uint_as_float(tf32_rna(v.x - hi.x));
+  lw.y = __uint_as_float(tf32_rna(v.y - hi.y));
+  lw.z = __uint_as_float(tf32_rna(v.z - hi.z));
+  lw.w = __uint_as_float(tf32_rna(v.w - hi.w));
+}
+
+// Split n_vec16 16-byte chunks of raw FP32 data in place into hi, and into lo
+// (NT splitting threads, this one `tid`).
+template <int NT = kSplitThreads>
 __device__ __forceinline__ void split_tile(float* raw_hi, float* lo, int n_vec16, int tid) {
   float4* h = reinterpret_cast<float4*>(raw_hi);
   float4* l = reinterpret_cast<float4*>(lo);
-  for (int i = tid; i < n_vec16; i += kSplitThreads) {
-    float4 v = h[i];
+  for (int i = tid; i < n_vec16; i += NT) {
     float4 hi, lw;
-    hi.x = __uint_as_float(tf32_rna(v.x));
-    hi.y = __uint_as_float(tf32_rna(v.y));
-    hi.z = __uint_as_float(tf32_rna(v.z));
-    hi.w = __uint_as_float(tf32_rna(v.w));
-    lw.x = __uint_as_float(tf32_rna(v.x - hi.x));
-    lw.y = __uint_as_float(tf32_rna(v.y - hi.y));
-    lw.z = __uint_as_float(tf32_rna(v.z - hi.z));
-    lw.w = __uint_as_float(tf32_rna(v.w - hi.w));
+    split4(h[i], hi, lw);
+    h[i] = hi;
+    l[i] = lw;
+  }
+}
+
+// As split_tile, for the last K stage of a Gram row chunk: the data are TMA boxes
+// of 32 rows of 128 bytes (the 128-byte swizzle permutes 16-byte chunks within a
+// row only), and rows whose index within their box is >= `valid` lie past the
+// chunk's end; they are written as zeros so they do not enter this chunk's sum.
+template <int NT = kSplitThreads>
+__device__ __forceinline__ void split_tile_rows(float* raw_hi, float* lo, int n_vec16, int tid,
+                                                int valid) {
+  float4* h = reinterpret_cast<float4*>(raw_hi);
+  float4* l = reinterpret_cast<float4*>(lo);
+  for (int i = tid; i < n_vec16; i += NT) {
+    float4 hi = make_float4(0.f, 0.f, 0.f, 0.f), lw = hi;
+    if (((i >> 3) & 31) < valid) split4(h[i], hi, lw);
     h[i] = hi;
     l[i] = lw;
   }
@@ -245,12 +271,13 @@ __device__ __forceinline__ Smem carve(uint8_t* dyn) {
 }
 
 // Common prologue: barrier init (thread 0) and TMEM allocation (warp 1).
-__device__ __forceinline__ void prologue(const Smem& sm, int warp) {
+__device__ __forceinline__ void prologue(const Smem& sm, int warp,
+                                         int split_warps = kSplitThreads / 32) {
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&sm.full[s], 1);
       mbar_init(&sm.empty[s], 1);
-      mbar_init(&sm.split[s], kSplitThreads);
+      mbar_init(&sm.split[s], split_warps);
     }
     mbar_init(sm.accum, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -319,8 +346,9 @@ __device__ void mma_loop(const Smem& sm, uint32_t tmem, int nkb, uint32_t idesc)
 // grid.x = k_tiles * m_tiles (k tile fastest), grid.y = row chunks.
 // A = X^T (MN-major: 4 boxes of 32 columns x 32 rows), B = Y (MN-major, 5 boxes).
 // X and Y tensor maps start at columns aligned down to 16 bytes; sx/sy are the
-// column shifts of the caller's views (outputs are re-indexed).
-__global__ void __launch_bounds__(kThreads, 1)
+// column shifts of the caller's views (outputs are re-indexed). Warps: 0 TMA
+// producer, 1 MMA issuer, 2-9 hi/lo split, then epilogue.
+__global__ void __launch_bounds__(kGramThreads, 1)
 gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmY,
                int64_t n, int k, int m, int sx, int sy, int k_tiles, int64_t rows_per_chunk,
                float* __restrict__ partial, int symmetric) {
@@ -338,7 +366,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   const int64_t r_end = min(n, r_begin + rows_per_chunk);
   const int nkb = static_cast<int>((r_end - r_begin + kKB - 1) / kKB);
 
-  prologue(sm, warp);
+  prologue(sm, warp, kGramSplitThreads / 32);
   const uint32_t tmem = *sm.tmem_slot;
 
   if (warp == 0 && lane == 0) {
@@ -360,41 +388,36 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     __syncwarp();
   } else if (warp >= 2) {
     const int tid = threadIdx.x - 64;
-    // Rows past r_end inside the last block belong to the next chunk: zero them
-    // in the split so they do not enter this chunk's sum.
+    // Rows past r_end inside the last block belong to the next chunk: the split
+    // writes them as zeros, so they do not enter this chunk's sum.
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % kStages;
       const uint32_t ph = (kb / kStages) & 1u;
-      if (!mbar_wait(&sm.full[s], ph, 2)) break;
+      if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2))) break;
       const int64_t y = r_begin + static_cast<int64_t>(kb) * kKB;
       const int64_t left = r_end - y;
       const int valid = left < kKB ? static_cast<int>(left) : kKB;
-      if (valid < kKB) {
-        // Row r of a box sits at byte r*128 (swizzle permutes 16-byte chunks
-        // within the row only), so zeroing whole 128-byte rows is layout-safe.
-        for (int idx = tid; idx < (kM / 32 + kN / 32) * (kKB - valid) * 32; idx += kSplitThreads) {
-          const int box = idx / ((kKB - valid) * 32);
-          const int rem = idx % ((kKB - valid) * 32);
-          const int row = valid + rem / 32;
-          const int e = rem % 32;
-          float* bp = box < kM / 32 ? sm.a_hi(s) + box * (32 * kKB)
-                                    : sm.b_hi(s) + (box - kM / 32) * (32 * kKB);
-          bp[row * 32 + e] = 0.0f;
-        }
-        asm volatile("bar.sync 1, 128;" ::: "memory");
+      if (valid == kKB) {
+        split_tile<kGramSplitThreads>(sm.a_hi(s), sm.a_lo(s), kABytes / 16, tid);
+        split_tile<kGramSplitThreads>(sm.b_hi(s), sm.b_lo(s), kBBytes / 16, tid);
+      } else {
+        split_tile_rows<kGramSplitThreads>(sm.a_hi(s), sm.a_lo(s), kABytes / 16, tid, valid);
+        split_tile_rows<kGramSplitThreads>(sm.b_hi(s), sm.b_lo(s), kBBytes / 16, tid, valid);
       }
-      split_tile(sm.a_hi(s), sm.a_lo(s), kABytes / 16, tid);
-      split_tile(sm.b_hi(s), sm.b_lo(s), kBBytes / 16, tid);
       fence_proxy_async();
-      mbar_arrive(&sm.split[s]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.split[s]);
     }
-    // Epilogue: TMEM lane = output row i (within the k tile), column = j.
+    // Epilogue: TMEM lane = output row i (within the k tile), column = j. A warp
+    // reads the TMEM lane quarter warp % 4; warps 2-5 take columns [0, kN/2),
+    // warps 6-9 the rest.
     if (mbar_wait(sm.accum, 0, 4)) {
       tc_fence_after();
       const int q = warp % 4;
+      const int c0 = ((warp - 2) / 4) * (kN / 2);
       const int i = i0 + q * 32 + lane - sx;  // caller's column index in X
       float* out = partial + static_cast<int64_t>(blockIdx.y) * k * m;
-      for (int c = 0; c < kN; c += 16) {
+      for (int c = c0; c < c0 + kN / 2; c += 16) {
         float v[16];
         tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c, v);
         if (i >= 0 && i < k) {
@@ -467,10 +490,11 @@ rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % kStages;
       const uint32_t ph = (kb / kStages) & 1u;
-      if (!mbar_wait(&sm.full[s], ph, 2)) break;
+      if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2))) break;
       split_tile(sm.a_hi(s), sm.a_lo(s), kABytes / 16, tid);
       fence_proxy_async();
-      mbar_arrive(&sm.split[s]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.split[s]);
     }
     // Epilogue: TMEM lane = tile row, column = output column. A 16-byte aligned Y
     // is written straight from registers, four floats per store along each row.
@@ -569,7 +593,7 @@ rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&sm.full[s], 1);
       mbar_init(&sm.empty[s], 1);
-      mbar_init(&sm.split[s], kSplitThreads);
+      mbar_init(&sm.split[s], kSplitThreads / 32);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf[b], 1);
@@ -668,13 +692,14 @@ rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
       for (int kb = 0; kb < nkb; ++kb, ++g) {
         const int s = static_cast<int>(g % kStages);
         const uint32_t ph = (g / kStages) & 1u;
-        if (!mbar_wait(&sm.full[s], ph, 2)) {
+        if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2))) {
           ok = false;
           break;
         }
         split_tile(sm.a_hi(s), sm.a_lo(s), kABytes / 16, tid);
         fence_proxy_async();
-        mbar_arrive(&sm.split[s]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.split[s]);
       }
     }
   } else {
@@ -859,7 +884,7 @@ void gram_tc(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n
   std::call_once(once, [] { set_smem_attr(reinterpret_cast<const void*>(gram_tc_kernel)); });
   const bool sym = X == Y && ldx == ldy && k == m;
   dim3 grid(p.k_tiles * p.m_tiles, p.chunks);
-  gram_tc_kernel<<<grid, kThreads, kSmemBytes, s>>>(mx, my, n, static_cast<int>(k),
+  gram_tc_kernel<<<grid, kGramThreads, kSmemBytes, s>>>(mx, my, n, static_cast<int>(k),
                                                     static_cast<int>(m), sx, sy, p.k_tiles,
                                                     p.rows_per_chunk, static_cast<float*>(ws),
                                                     sym ? 1 : 0);

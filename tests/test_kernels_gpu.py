@@ -85,8 +85,9 @@ def register_kernel():
 @pytest.mark.parametrize("stencil", ["star1", "star2", "box"])
 @pytest.mark.parametrize("b", [16, 40, 320, 1000])
 def test_pipelined_and_register_spmm_agree_on_stencils(dtype, stencil, b):
-    """Bulk-copy pipelined kernel (7/13/27-point rows) vs the register kernel vs
-    the oracle, including multi-panel widths and the fused Chebyshev epilogue."""
+    """Every SpMM kernel (row-batched with 8- and 16-byte lanes, loop, bulk-copy
+    pipelined; 7/13/27-point rows) vs the oracle, including multi-panel and ragged
+    panel widths and the fused Chebyshev epilogue."""
     import fasteig_b200 as fe
     from fasteig_b200 import matrices as M, ops
     from oracle import oracle as O
@@ -101,7 +102,7 @@ def test_pipelined_and_register_spmm_agree_on_stencils(dtype, stencil, b):
     Xn, Zn = X.double().cpu().numpy(), Z.double().cpu().numpy()
     ref = 0.7 * (A.scipy() @ Xn) - 0.2 * Xn - Zn
     outs = []
-    for mode in (0, 1):
+    for mode in (0, 1, 2, 3):
         assert fe.lib.fe_set_spmm_kernel(mode) == 0
         Zc = Z.clone()
         ops.cheb_step(dA, X, Zc, Zc, 0.7, -0.2, -1.0)
@@ -110,6 +111,53 @@ def test_pipelined_and_register_spmm_agree_on_stencils(dtype, stencil, b):
     assert fe.lib.fe_set_spmm_kernel(0) == 0
     assert ops.device_status(clear=True) == 0
     scale = 0.7 * (absA(A) @ np.abs(Xn)) + 0.2 * np.abs(Xn) + np.abs(Zn)
+    tol = 1e-13 if dtype == torch.float64 else 4e-6
+    for got in outs:
+        assert np.all(np.abs(got - ref) <= tol * scale + 1e-300)
+
+
+def short_row_csr(n, max_nnz, seed):
+    """Square CSR with 0..max_nnz random distinct columns per row (some rows
+    empty, most without a stored diagonal)."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(seed)
+    rows, cols = [], []
+    for r in range(n):
+        k = int(rng.integers(0, max_nnz + 1))
+        c = rng.choice(n, size=min(k, n), replace=False)
+        rows.extend([r] * c.size)
+        cols.extend(c.tolist())
+    rows, cols = np.array(rows, dtype=np.int64), np.array(cols, dtype=np.int64)
+    return O.csr_from_triplets(n, rows, cols, rng.standard_normal(rows.size), False)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("n,b", [(1, 16), (300, 16), (2000, 40), (5000, 320), (1200, 1000)])
+@pytest.mark.parametrize("alpha,gamma,beta", [(1.0, 0.0, 0.0), (0.7, -0.2, -1.0), (-1.3, 0.4, 0.5)])
+def test_pipelined_spmm_rows_without_diagonal(dtype, n, b, alpha, gamma, beta):
+    """Bulk-copy pipelined kernel (mode 2) and the default kernel on rows of 0..7
+    nonzeros, most without a stored diagonal (the gamma term then reads the row's
+    own X row), some empty: oracle parity."""
+    import fasteig_b200 as fe
+    from fasteig_b200 import ops
+    A = short_row_csr(n, 7, seed=n + b)
+    dA = dev_csr(A)
+    X = block(n, b, dtype, 1)
+    Z = block(n, b, dtype, 2)
+    Xn, Zn = X.double().cpu().numpy(), Z.double().cpu().numpy()
+    ref = alpha * (A.scipy() @ Xn) + gamma * Xn + beta * Zn
+    outs = []
+    try:
+        for mode in (2, 0):
+            assert fe.lib.fe_set_spmm_kernel(mode) == 0
+            Y = torch.full_like(X, float("nan"))
+            ops.cheb_step(dA, X, Z, Y, alpha, gamma, beta)
+            torch.cuda.synchronize()
+            outs.append(Y.double().cpu().numpy())
+    finally:
+        assert fe.lib.fe_set_spmm_kernel(0) == 0
+    assert ops.device_status(clear=True) == 0
+    scale = abs(alpha) * (absA(A) @ np.abs(Xn)) + abs(gamma) * np.abs(Xn) + abs(beta) * np.abs(Zn)
     tol = 1e-13 if dtype == torch.float64 else 4e-6
     for got in outs:
         assert np.all(np.abs(got - ref) <= tol * scale + 1e-300)
