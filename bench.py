@@ -49,6 +49,11 @@ def args_parse():
     p.add_argument("--tol", type=float, default=1e-8)
     p.add_argument("--maxiter", type=int, default=300)
     p.add_argument("--amplification", type=float, default=1e6)
+    p.add_argument("--locking", default="hard", choices=["soft", "hard"],
+                   help="Chebyshev locking: soft (the reference: QR and Rayleigh-Ritz over the "
+                        "whole subspace) or hard (over the active block only)")
+    p.add_argument("--mixed-switch", type=float, default=1e-6,
+                   help="FP32 locking threshold and FP32 -> FP64 switch of the mixed path")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison solve")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--kernel", default=None,
@@ -295,6 +300,7 @@ def config_dict(a, extra=None):
          "matrix": f"3D 7-point Dirichlet Laplacian {a.side}^3 + {a.wells} Gaussian wells (seeded)",
          "solver": "Chebyshev", "nev": a.nev, "block": a.block, "degree": a.degree,
          "tol": a.tol, "bounds": "ritz", "amplification_cap": a.amplification,
+         "locking": a.locking, "mixed_switch": a.mixed_switch,
          "precision": "mixed (FP32 filter/SpMM/rotation, FP64-accumulated Gram, FP64 "
                       "Cholesky/eig/residual, FP64 final sweeps)",
          "init": "device", "l2": "blocks (n x 320) >> 126 MB L2; no flush needed"}
@@ -370,12 +376,13 @@ def build_matrix(a):
     return M.laplacian_wells(a.side, wells=a.wells, seed=0)
 
 
-def solve_opts(a, precision, seed):
+def solve_opts(a, precision, seed, locking=None):
     import fasteig_b200 as fe
     o = fe.fasteig_options()
     for k, v in dict(solver="Chebyshev", nev=a.nev, which="SR", tol=a.tol, maxiter=a.maxiter,
                      seed=seed, degree=a.degree, block=a.block, bounds="ritz",
-                     amplification=a.amplification, precision=precision, init="device").items():
+                     amplification=a.amplification, precision=precision, init="device",
+                     locking=locking or a.locking, mixed_switch=a.mixed_switch).items():
         assert o.set(k, v), k
     return o
 
@@ -470,7 +477,9 @@ def run_reference(a):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": config_dict(a, {"precision": "fp64 (CPU restatement)"}),
+            "config": config_dict(a, {"precision": "fp64 (CPU restatement)",
+                                      "locking": "soft (the reference's)",
+                                      "mixed_switch": None}),
             "cpu_baseline": {k: vals[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     line["cpu_baseline"]["value"] = v
@@ -594,17 +603,27 @@ def main():
         del p2, vec_h, rp_h, ci_h, va_h
         fp64 = None
         if not a.no_fp64:
-            # Plain FP64 path of this build, warmed up like the mixed path (one
-            # untimed solve), then the mean of two solves.
-            o64 = solve_opts(a, "fp64", seed)
-            solve_once(o64)
-            runs = [solve_once(o64) for _ in range(2)]
-            sec64 = sum(p.stats["seconds"] for p in runs) / len(runs)
-            c64 = int((runs[-1].residual_norms() <= a.tol).sum())
-            fp64 = {"value": round(c64 / sec64, 4), "unit": UNIT, "seconds": round(sec64, 3),
-                    "cycles": runs[-1].stats["iterations"], "converged": c64}
+            # FP64 paths of this build, each warmed up like the mixed path (one
+            # untimed solve), then the mean of two solves: "plain" is the
+            # reference's algorithm (soft locking) in FP64; the second uses every
+            # option of the mixed run except the precision.
+            def fp64_run(locking):
+                o64 = solve_opts(a, "fp64", seed, locking=locking)
+                solve_once(o64)
+                runs = [solve_once(o64) for _ in range(2)]
+                sec64 = sum(p.stats["seconds"] for p in runs) / len(runs)
+                c64 = int((runs[-1].residual_norms() <= a.tol).sum())
+                return {"value": round(c64 / sec64, 4), "unit": UNIT, "seconds": round(sec64, 3),
+                        "cycles": runs[-1].stats["iterations"], "converged": c64,
+                        "locking": locking}
+            fp64 = fp64_run("soft")
             extra["fp64_plain"] = fp64
             extra["mixed_vs_fp64"] = round((value / world) / fp64["value"], 3) if fp64["value"] else None
+            if a.locking != "soft":
+                same = fp64_run(a.locking)
+                extra["fp64_same_options"] = same
+                extra["mixed_vs_fp64_same_options"] = (
+                    round((value / world) / same["value"], 3) if same["value"] else None)
         extra["roofline"] = roofline_cheb_step(a, H, dA, peak, mode=tuned["fp32"])
         extra["roofline"]["peak_kind"] = f"{peak_kind} hbm_gbs (burst copy)"
         if world == 1 and not a.no_cpu:

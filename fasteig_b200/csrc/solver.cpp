@@ -71,6 +71,7 @@ struct Options {
   double mixed_switch = 4.0e-6;    // FP32 -> FP64 switch when max residual <= this
   bool tensor_cores = true;        // FP32 Grams/rotations on tcgen05 (3xTF32)
   std::string precond = "none";    // none | jacobi (LOBPCG / Davidson corrections W = T R)
+  std::string locking = "soft";    // Chebyshev: soft (reference) | hard
 
   void parse(const char* text) {
     if (!text) return;
@@ -138,7 +139,11 @@ struct Options {
     else if (k == "init") init = lower(v);
     else if (k == "mixed_switch") mixed_switch = as_double(v);
     else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
-    else if (k == "precond") {
+    else if (k == "locking") {
+      locking = lower(v);
+      if (locking != "soft" && locking != "hard")
+        throw Error(FE_ERR_INVALID, "locking must be soft or hard");
+    } else if (k == "precond") {
       precond = lower(v);
       if (precond != "none" && precond != "jacobi")
         throw Error(FE_ERR_INVALID, "precond must be none or jacobi");
@@ -526,12 +531,13 @@ struct ChebLoop {
   int64_t n, nev, cap, degree;
   double sign, lower, upper;
   bool cholqr2;
+  bool hard;  // hard locking: the locked prefix is final, QR and Rayleigh-Ritz see the rest
   PhaseEvents ev;
 
   ChebLoop(Context& c, const Csr& a, const Options& o, SmallState& s, ProjectedEig& e, double sg,
            double lo, double up, bool two_pass)
       : ctx(c), A(a), opt(o), sm(s), eig(e), n(a.rows), nev(o.nev), degree(o.degree), sign(sg),
-        lower(lo), upper(up), cholqr2(two_pass) {}
+        lower(lo), upper(up), cholqr2(two_pass), hard(o.locking == "hard") {}
 
   // One filter + deflation + QR + Rayleigh-Ritz cycle (src/ChebyshevSolver.cpp:151-184).
   // On return the host holds the Ritz values W[0:sub], residuals rel[0:sub] and info.
@@ -587,6 +593,10 @@ struct ChebLoop {
                         1.0, s);
       }
     }
+    if (hard) {
+      iterate_active(locked, sub, Y, ldy, W, rel, info_host, st);
+      return;
+    }
     if (!in_place) {
       FE_CHECK_CUDA(cudaMemcpy2DAsync(b.V.col(locked), b.V.ld * sizeof(T), b.S.data(),
                                       b.S.ld * sizeof(T), active * sizeof(T), n,
@@ -622,6 +632,60 @@ struct ChebLoop {
     rel.assign(sub, 0.0);  // guard columns: residuals not formed
     ctx.to_host(W.data(), sm.W.as<double>(), sub);
     ctx.to_host(rel.data(), sm.rel.as<double>(), nres);
+    ctx.to_host(info_host, sm.info.as<int32_t>(), 2);
+    ctx.to_host(info_host + 2, eig.info(), 1);
+    ev.record(3, s);
+    ctx.sync();
+    ev.accumulate(st);
+  }
+
+  // Steps 3-4 under hard locking. The locked prefix V[:, :locked] holds final
+  // Ritz vectors; the filtered block Y (active columns, deflated against the
+  // prefix, 16-byte aligned: V's own columns or the staging copy in S) is
+  // orthonormalized and Rayleigh-Ritz projected on its own, so the QR and the
+  // projection cost n*active^2 instead of n*sub^2 once most pairs have locked. The
+  // prefix's Ritz values and residuals stay as they were when they locked; only
+  // W[locked:sub] and rel[locked:nev] are renewed.
+  void iterate_active(int64_t locked, int64_t sub, const T* Y, int64_t ldy,
+                      std::vector<double>& W, std::vector<double>& rel, int32_t* info_host,
+                      Stats& st) {
+    cudaStream_t s = ctx.stream;
+    const int64_t active = sub - locked;
+    if (cholqr2) {
+      cholqr<T>(ctx, sm, Y, ldy, b.AQ.data(), b.AQ.ld, n, active, 0);
+      cholqr<T>(ctx, sm, b.AQ.data(), b.AQ.ld, b.Q.data(), b.Q.ld, n, active, 1);
+    } else {
+      cholqr<T>(ctx, sm, Y, ldy, b.Q.data(), b.Q.ld, n, active, 0);
+    }
+    ev.record(2, s);
+    csr_spmm<T>(A, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, nullptr, 0, active, sign, 0.0, 0.0,
+                s);
+    st.spmm_launches += 1;
+    double* P = sm.G.as<double>();
+    gram_block<T>(sm, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, n, active, active, P, s);
+    symmetrize(P, active, sm.cap, s);
+    eig.run(P, active, sm.cap, sm.W.as<double>());
+    // Ritz vectors of the active block into S (aligned), residuals of its wanted
+    // pairs (indices locked..nev-1), then into V[:, locked:sub].
+    rotate_block<T>(sm, b.Q.data(), b.Q.ld, P, b.S.data(), b.S.ld, n, active, active, 1.0, 0.0,
+                    s);
+    const int64_t nw = nev - locked;
+    const int64_t vw = 16 / static_cast<int64_t>(sizeof(T));
+    const int64_t nw_pad = std::min(((nw + vw - 1) / vw) * vw, b.S.ld);  // whole vectors
+    csr_spmm<T>(A, b.S.data(), b.S.ld, b.AQ.data(), b.AQ.ld, nullptr, 0, nw_pad, sign, 0.0, 0.0,
+                s);
+    st.spmm_launches += 1;
+    residual_norms<T>(b.AQ.data(), b.S.data(), nullptr, b.S.ld, n, nw, sm.W.as<double>(), nullptr,
+                      0, sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
+                      sm.rws.get(), sm.rws.bytes(), s, 1);
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(b.V.col(locked), b.V.ld * sizeof(T), b.S.data(),
+                                    b.S.ld * sizeof(T), active * sizeof(T), n,
+                                    cudaMemcpyDeviceToDevice, s));
+    W.resize(sub);
+    rel.resize(sub, 0.0);
+    std::fill(rel.begin() + nev, rel.end(), 0.0);  // guard columns: residuals not formed
+    ctx.to_host(W.data() + locked, sm.W.as<double>(), active);
+    ctx.to_host(rel.data() + locked, sm.rel.as<double>(), nw);
     ctx.to_host(info_host, sm.info.as<int32_t>(), 2);
     ctx.to_host(info_host + 2, eig.info(), 1);
     ev.record(3, s);
@@ -766,7 +830,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     // residuals cannot reach tol, pairs lock at the FP32 floor (mixed_switch) so
     // the spare columns still enter the subspace as the prefix converges.
     const double lock_tol = l32 ? std::max(tol, opt.mixed_switch) : tol;
-    locked = 0;
+    if (opt.locking != "hard") locked = 0;  // soft: recheck the whole prefix (reference)
     while (locked < nev && rel[locked] <= lock_tol) ++locked;
     sub = std::max(sub, nev + std::min(locked, cap - nev));
     it_done = iter + 1;
@@ -803,6 +867,19 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   // returned vectors on the device: ||A x - l x|| / ((1 + |l|) ||x||), which
   // fasteig_problem::solve recomputes for non-Krylov solvers on the host
   // (src/fasteig_problem.cpp:419-422, src/fasteig_solver.cpp:89-129).
+  // Hard locking can leave a locked pair above a Ritz value found later (an
+  // eigenvalue that entered the subspace after the prefix locked); such pairs are
+  // returned in ascending order, as the reference's whole-subspace Rayleigh-Ritz
+  // returns them.
+  std::vector<int32_t> order;
+  if (opt.locking == "hard" && !std::is_sorted(W.begin(), W.begin() + nev)) {
+    order.resize(nev);
+    for (int64_t j = 0; j < nev; ++j) order[j] = static_cast<int32_t>(j);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return W[a] < W[b]; });
+    std::vector<double> Ws(nev);
+    for (int64_t j = 0; j < nev; ++j) Ws[j] = W[order[j]];
+    std::copy(Ws.begin(), Ws.end(), W.begin());
+  }
   for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = sign * W[j];
   if (opt.verbosity >= 2)
     std::fprintf(stderr, "[fe] filter cycles (wall) %.1f ms\n", ms_since(t_loop));
@@ -820,6 +897,16 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
       convert<float, double>(l32->b.V.data(), l32->b.V.ld, Xf.data(), Xf.ld, n, nev, s);
       Xp = Xf.data();
       ldx = Xf.ld;
+    }
+    Block<double> Xs;
+    if (!order.empty()) {
+      Xs.allocate(n, cap);
+      DeviceBuffer idx(static_cast<size_t>(nev) * sizeof(int32_t));
+      ctx.to_device(idx.as<int32_t>(), order.data(), nev);
+      gather_columns<double>(Xp, ldx, idx.as<int32_t>(), nev, Xs.data(), Xs.ld, n, s);
+      ctx.sync();
+      Xp = Xs.data();
+      ldx = Xs.ld;
     }
     AXf.allocate(n, cap);  // same leading dimension as the vector block
     csr_spmm<double>(A, Xp, ldx, AXf.data(), AXf.ld, nullptr, 0, nev, 1.0, 0.0, 0.0, s);

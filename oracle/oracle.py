@@ -548,7 +548,8 @@ def chebyshev_filter_window(H_apply, X: np.ndarray, degree: int, cutoff: float,
 def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
                     maxiter: int = 1000, which: str = "sr", seed: int = 1,
                     block: Optional[int] = None, record_history: bool = False,
-                    bounds: str = "reference", amplification: float = math.inf) -> SolveResult:
+                    bounds: str = "reference", amplification: float = math.inf,
+                    locking: str = "soft") -> SolveResult:
     """ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221).
 
     ``block`` overrides the subspace capacity ``nev + min(nev, n - nev)``
@@ -557,7 +558,12 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
     after each Rayleigh-Ritz the damped interval is [theta_max, upper], where
     theta_max is the largest Ritz value of the subspace (Zhou & Saad, 2007), and
     the cutoff is lowered where needed so that the filter's amplification at
-    the Lanczos lower bound stays within ``amplification``."""
+    the Lanczos lower bound stays within ``amplification``.
+    ``locking="hard"`` is the hard-locking extension (not in the reference, which
+    rechecks the whole prefix after a Rayleigh-Ritz over the whole subspace,
+    src/ChebyshevSolver.cpp:160-192): locked pairs are final, and the QR and the
+    Rayleigh-Ritz act on the deflated active block only; pairs are returned in
+    ascending order."""
     n = A.rows
     which = which.lower()
     if n <= 0 or nev <= 0 or nev > n:
@@ -582,7 +588,8 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
     for it in range(maxiter):
         active = subspace_cols - locked
         if bounds == "ritz" and ritz is not None:
-            cutoff = float(ritz.values[subspace_cols_prev - 1])
+            cutoff = float(ritz.values[-1] if locking == "hard"
+                           else ritz.values[subspace_cols_prev - 1])
             if math.isfinite(amplification):
                 xl = math.cosh(math.acosh(amplification) / degree)
                 cutoff = min(cutoff, (2.0 * lower + upper * (xl - 1.0)) / (1.0 + xl))
@@ -594,6 +601,32 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
         if locked > 0:
             _, filtered, _ = block_gram_schmidt(vectors, locked, filtered)
         vectors[:, locked:locked + active] = filtered
+        if locking == "hard":
+            info, basis, _ = cholesky_qr(filtered)
+            if info != 0:
+                raise RuntimeError("ChebyshevSolver: Cholesky QR failed during filtering.")
+            op_basis = H_apply(basis)
+            ritz_a = extract_projected_ritz_pairs(basis.T @ op_basis, basis, op_basis, active,
+                                                  active, "sr")
+            if ritz is None:
+                vals, rels = np.zeros(capacity), np.zeros(capacity)
+            vals[locked:subspace_cols] = ritz_a.values
+            rels[locked:subspace_cols] = ritz_a.relative_residuals
+            if not (np.all(np.isfinite(ritz_a.values)) and
+                    np.all(np.isfinite(ritz_a.relative_residuals))):
+                raise RuntimeError("ChebyshevSolver: non-finite Ritz values or residuals.")
+            vectors[:, locked:subspace_cols] = ritz_a.vectors
+            ritz = ritz_a
+            subspace_cols_prev = subspace_cols
+            while locked < nev and rels[locked] <= tol:
+                locked += 1
+            subspace_cols = max(subspace_cols, nev + min(locked, capacity - nev))
+            it_done = it + 1
+            if record_history:
+                history.append((sign * vals[:nev].copy(), rels[:nev].copy()))
+            if rels[:nev].max() <= tol:
+                break
+            continue
         basis = vectors[:, :subspace_cols].copy()
         info, basis, _ = cholesky_qr(basis)
         if info != 0:
@@ -615,6 +648,10 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
             history.append((sign * ritz.values[:nev].copy(), ritz.relative_residuals[:nev].copy()))
         if ritz.relative_residuals[:nev].max() <= tol:
             break
+    if locking == "hard":
+        order = np.argsort(vals[:nev], kind="stable")
+        return SolveResult(sign * vals[:nev][order], vectors[:, :nev][:, order].copy(),
+                           rels[:nev][order].copy(), it_done, 0, history)
     return SolveResult(sign * ritz.values[:nev], ritz.vectors[:, :nev].copy(),
                        ritz.relative_residuals[:nev].copy(), it_done, 0, history)
 

@@ -101,3 +101,22 @@ def test_spmm_restatement_matches_literal_loop():
     Y2 = Y.copy()
     O.csr_apply_block(A, X, 0, 5, Y2, 0.7, -0.3)
     np.testing.assert_allclose(Y2, lit, rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.parametrize("which", ["sr", "lr"])
+def test_chebyshev_hard_locking_extension_against_dense(which):
+    """Hard-locking extension of the oracle's Chebyshev solver (QR and Rayleigh-Ritz
+    on the active block only): eigenvalues equal the dense spectrum, true residuals
+    reach tol, pairs come back in order."""
+    from fasteig_b200 import matrices as M
+    H = M.laplacian_wells(12, wells=8, seed=2)
+    A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
+    dense = np.linalg.eigvalsh(A.scipy().toarray())
+    exp = dense[:24] if which == "sr" else dense[::-1][:24]
+    res = O.chebyshev_solve(A, 24, degree=16, tol=1e-8, maxiter=300, seed=1, block=32,
+                            bounds="ritz", amplification=1e6, locking="hard", which=which)
+    np.testing.assert_allclose(res.eigenvalues, exp, rtol=1e-10, atol=1e-10)
+    assert np.all(O.residual_norms(A, None, res.eigenvalues, res.eigenvectors) <= 1.01e-8)
+    soft = O.chebyshev_solve(A, 24, degree=16, tol=1e-8, maxiter=300, seed=1, block=32,
+                             bounds="ritz", amplification=1e6, which=which)
+    assert res.iterations <= soft.iterations + 1

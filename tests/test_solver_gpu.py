@@ -83,6 +83,29 @@ def test_chebyshev_ritz_bounds_block_against_dense(wells12, precision):
         assert p.stats["fp32_iterations"] > 0
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("nev,blk,which", [(24, 32, "sr"), (23, 30, "sr"), (21, 27, "lr")])
+def test_chebyshev_hard_locking_against_dense_and_oracle(wells12, precision, nev, blk, which):
+    """locking=hard (QR and Rayleigh-Ritz on the active block only), aligned and
+    unaligned active blocks: dense eigenvalues, FP64 residuals <= tol, ascending
+    order, and (FP64) the oracle's hard-locking iteration count within 2."""
+    from oracle import oracle as O
+    kw = dict(degree=16, block=blk, bounds="ritz", amplification=1e6)
+    p = solve(wells12, solver="Chebyshev", nev=nev, which=which, tol=1e-8, maxiter=300, seed=1,
+              precision=precision, locking="hard", **kw)
+    dense = np.linalg.eigvalsh(wells12.scipy().toarray())
+    exp = dense[:nev] if which == "sr" else dense[::-1][:nev]
+    assert np.all(p.residual_norms() <= 1e-8), p.residual_norms()
+    np.testing.assert_allclose(p.eigenvalues(), exp, rtol=1e-10, atol=1e-10)
+    final = O.residual_norms(wells12, None, p.eigenvalues(), p.eigenvectors())
+    assert np.all(final <= 1.01e-8)
+    if precision == "fp64":
+        ref = O.chebyshev_solve(wells12, nev, tol=1e-8, maxiter=300, which=which, seed=1,
+                                locking="hard", **kw)
+        assert abs(p.last_iterations() - ref.iterations) <= 2, (p.last_iterations(),
+                                                                 ref.iterations)
+
+
 def test_chebyshev_ritz_bounds_matches_oracle(wells12):
     from oracle import oracle as O
     ref = O.chebyshev_solve(wells12, 12, degree=12, tol=1e-8, maxiter=300, seed=4, block=16,
