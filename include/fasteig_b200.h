@@ -252,7 +252,10 @@ int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ld
  * with the reference's keys (src/fasteig_options.cpp:51-112: nev, maxiter,
  * maxdim, maxblks, degree, which, solver, tol, seed, blksize) plus
  * extensions (precision=fp64|mixed, block=<cols>, bounds=reference|ritz,
- * precond=none|jacobi, init=host|device). B != NULL makes the problem
+ * precond=none|jacobi, init=host|device, mixed_switch=<FP32 floor>,
+ * locking=soft|hard: Chebyshev soft locking is the reference's, hard locking
+ * keeps locked pairs final and orthonormalizes and projects only the active
+ * block). B != NULL makes the problem
  * generalized (A x = l B x, B symmetric positive definite): LOBPCG and Davidson
  * then work in the B metric (extension; the reference's are standard-only), and
  * Krylov-Schur runs the reference's B-metric Lanczos on B^-1 A with B^-1
