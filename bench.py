@@ -234,8 +234,12 @@ def run_serving(a):
         o = fe.fasteig_options(H.n)
         kv = dict(solver=solver, nev=nev, which="SR", tol=tol, seed=1 + k, init="device")
         if solver == "Chebyshev":
+            # mixed precision with hard locking; for tol 1e-8 the FP32 pairs lock at
+            # 1e-6 before the FP64 cycles (the default 4e-6 floor where tol is 1e-6)
             kv.update(degree=16, bounds="ritz", amplification=1e6, maxiter=300,
-                      precision="mixed" if tol >= 1e-6 else "fp64")
+                      precision="mixed", locking="hard")
+            if tol < 1e-6:
+                kv.update(mixed_switch=1e-6)
         else:
             # a block a quarter wider than nev: far fewer iterations for the last pairs
             kv.update(maxiter=600, block=min(H.n, nev + max(4, nev // 4)))
