@@ -395,6 +395,66 @@ gemv_n_kernel(const T* __restrict__ V, int64_t ldv, const double* __restrict__ h
   }
 }
 
+// Narrow bases (k <= K <= 32, the Lanczos bound estimate and Krylov-Schur bases
+// of a few dozen columns): a lane takes a whole row and keeps the K column sums
+// in registers, so a warp covers 32 rows per pass instead of one, and the rows'
+// loads of a pass are independent. Column sums are reduced across lanes with a
+// fixed shuffle tree, then across the CTA's warps in order: deterministic.
+template <typename T, int K>
+__global__ void __launch_bounds__(kGemvThreads)
+gemv_t_rows_kernel(const T* __restrict__ V, int64_t ldv, const T* __restrict__ x, int64_t incx,
+                   int64_t n, int k, int64_t rows_per_chunk, double* __restrict__ part) {
+  __shared__ double red[kGemvThreads / 32][K];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int64_t r_begin = static_cast<int64_t>(blockIdx.x) * rows_per_chunk;
+  const int64_t r_end = min(n, r_begin + rows_per_chunk);
+  double acc[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) acc[j] = 0.0;
+  for (int64_t r = r_begin + threadIdx.x; r < r_end; r += kGemvThreads) {
+    const double xv = static_cast<double>(x[r * incx]);
+    const T* vr = V + r * ldv;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+      if (j < k) acc[j] = fma(static_cast<double>(vr[j]), xv, acc[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    double v = acc[j];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][j] = v;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < k; j += kGemvThreads) {
+    double sum = 0.0;
+    for (int w = 0; w < kGemvThreads / 32; ++w) sum += red[w][j];
+    part[static_cast<int64_t>(blockIdx.x) * k + j] = sum;
+  }
+}
+
+// y = alpha * V h + beta * y for narrow V, a lane per row (coalesced y).
+template <typename T, int K>
+__global__ void __launch_bounds__(kGemvThreads)
+gemv_n_rows_kernel(const T* __restrict__ V, int64_t ldv, const double* __restrict__ h, int k,
+                   T* y, int64_t incy, int64_t n, double alpha, double beta, int use_beta) {
+  double hr[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) hr[j] = j < k ? h[j] : 0.0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * kGemvThreads;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * kGemvThreads + threadIdx.x; r < n;
+       r += stride) {
+    const T* vr = V + r * ldv;
+    double sum = 0.0;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+      if (j < k) sum = fma(static_cast<double>(vr[j]), hr[j], sum);
+    T* yr = y + r * incy;
+    double v = alpha * sum;
+    if (use_beta) v = fma(beta, static_cast<double>(*yr), v);
+    *yr = static_cast<T>(v);
+  }
+}
+
 }  // namespace
 
 // Workspace that suffices for every call with n' <= n, k' <= k, m' <= m, so a
@@ -454,8 +514,18 @@ void gram(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k
     const int64_t nchunks = (n + rpc - 1) / rpc;
     FE_REQUIRE(ws && ws_bytes >= static_cast<size_t>(nchunks) * k * sizeof(double),
                "gram: workspace too small");
-    gemv_t_partial_kernel<T><<<static_cast<unsigned>(nchunks), kGemvThreads, 0, s>>>(
-        X, ldx, Y, ldy, n, static_cast<int>(k), rpc, static_cast<double*>(ws));
+    double* part = static_cast<double*>(ws);
+    const int ki = static_cast<int>(k);
+    const unsigned grid = static_cast<unsigned>(nchunks);
+    if (k <= 8) {
+      gemv_t_rows_kernel<T, 8><<<grid, kGemvThreads, 0, s>>>(X, ldx, Y, ldy, n, ki, rpc, part);
+    } else if (k <= 16) {
+      gemv_t_rows_kernel<T, 16><<<grid, kGemvThreads, 0, s>>>(X, ldx, Y, ldy, n, ki, rpc, part);
+    } else if (k <= 32) {
+      gemv_t_rows_kernel<T, 32><<<grid, kGemvThreads, 0, s>>>(X, ldx, Y, ldy, n, ki, rpc, part);
+    } else {
+      gemv_t_partial_kernel<T><<<grid, kGemvThreads, 0, s>>>(X, ldx, Y, ldy, n, ki, rpc, part);
+    }
     check_launch("gemv_t_partial_kernel");
     gemv_t_reduce_kernel<<<static_cast<unsigned>((k + 127) / 128), 128, 0, s>>>(
         static_cast<const double*>(ws), static_cast<int>(nchunks), static_cast<int>(k), G);
@@ -494,9 +564,25 @@ void rotate(const T* X, int64_t ldx, const double* C, int64_t ldc, T* Y, int64_t
              "rotate: X and Y overlap");
   if (m == 1 && k <= kGemvMaxCols) {
     // Basis-times-vector shape (Lanczos): y = alpha X c + beta y by the GEMV kernel.
-    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, 148 * 16));
-    gemv_n_kernel<T><<<static_cast<unsigned>(blocks), kGemvThreads, 0, s>>>(
-        X, ldx, C, static_cast<int>(k), Y, ldy, n, alpha, beta, beta != 0.0 ? 1 : 0);
+    const int ki = static_cast<int>(k);
+    const int ub = beta != 0.0 ? 1 : 0;
+    if (k <= 32) {
+      const unsigned blocks = static_cast<unsigned>(
+          std::max<int64_t>(1, std::min<int64_t>((n + kGemvThreads - 1) / kGemvThreads, 148 * 8)));
+      if (k <= 8)
+        gemv_n_rows_kernel<T, 8><<<blocks, kGemvThreads, 0, s>>>(X, ldx, C, ki, Y, ldy, n, alpha,
+                                                                 beta, ub);
+      else if (k <= 16)
+        gemv_n_rows_kernel<T, 16><<<blocks, kGemvThreads, 0, s>>>(X, ldx, C, ki, Y, ldy, n, alpha,
+                                                                  beta, ub);
+      else
+        gemv_n_rows_kernel<T, 32><<<blocks, kGemvThreads, 0, s>>>(X, ldx, C, ki, Y, ldy, n, alpha,
+                                                                  beta, ub);
+    } else {
+      const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, 148 * 16));
+      gemv_n_kernel<T><<<static_cast<unsigned>(blocks), kGemvThreads, 0, s>>>(
+          X, ldx, C, ki, Y, ldy, n, alpha, beta, ub);
+    }
     check_launch("gemv_n_kernel");
     return;
   }
@@ -732,6 +818,32 @@ void vec_axpby(int64_t n, double a, const double* x, int64_t incx, double b, dou
   const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 16);
   vec_axpby_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(n, a, x, incx, b, y, incy);
   check_launch("vec_axpby_kernel");
+}
+
+// y[i*incy] = x[i] / *nrm with the divisor read on the device (a Lanczos basis
+// vector from the residual and its norm, with no host round trip).
+__global__ void scale_by_inv_kernel(int64_t n, const double* __restrict__ x,
+                                    const double* __restrict__ nrm, double* __restrict__ y,
+                                    int64_t incy) {
+  const double inv = 1.0 / *nrm;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    y[i * incy] = x[i] * inv;
+}
+
+__global__ void sum2_kernel(const double* a, const double* b, double* out) { *out = *a + *b; }
+
+void scale_by_inv(int64_t n, const double* x, const double* nrm, double* y, int64_t incy,
+                  cudaStream_t s) {
+  if (n <= 0) return;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 16);
+  scale_by_inv_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(n, x, nrm, y, incy);
+  check_launch("scale_by_inv_kernel");
+}
+
+void sum2(const double* a, const double* b, double* out, cudaStream_t s) {
+  sum2_kernel<<<1, 1, 0, s>>>(a, b, out);
+  check_launch("sum2_kernel");
 }
 
 template <typename T>

@@ -207,6 +207,10 @@ inline void host_symmetric_eig(std::vector<double> A, int m, std::vector<double>
 namespace fe {
 void vec_axpby(int64_t n, double a, const double* x, int64_t incx, double b, double* y,
                int64_t incy, cudaStream_t s);
+// y[i*incy] = x[i] / *nrm (divisor on the device); *out = *a + *b (one thread).
+void scale_by_inv(int64_t n, const double* x, const double* nrm, double* y, int64_t incy,
+                  cudaStream_t s);
+void sum2(const double* a, const double* b, double* out, cudaStream_t s);
 template <typename T>
 void fill_uniform(T* X, int64_t ld, int64_t n, int64_t m, uint64_t seed, cudaStream_t s);
 }  // namespace fe

@@ -327,39 +327,92 @@ void lanczos_bounds(Context& ctx, const Csr& A, double sign, unsigned seed, bool
     return a + b;
   };
   double beta_next = 0.0;
-  for (int64_t it = 0; it < steps; ++it) {
-    bool restarted = false;
-    double beta = norm(f.as<double>());
-    if (!std::isfinite(beta)) throw Error(FE_ERR_NONFINITE, "Lanczos: non-finite residual norm");
-    if (!(beta > std::numeric_limits<double>::epsilon())) {
-      // restart_residual (src/core/KrylovSubspace.cpp:251-259)
-      DeviceBuffer cand(n * sizeof(double));
-      if (host_init) {
-        std::mt19937 rng(seed + static_cast<unsigned>(it + 1));
-        std::uniform_real_distribution<double> dist(-1.0, 1.0);
-        std::vector<double> v(n);
-        for (auto& x : v) x = dist(rng);
-        ctx.to_device(cand.as<double>(), v.data(), n);
-      } else {
-        fill_uniform<double>(cand.as<double>(), 1, n, 1, seed + it + 1, s);
+  bool fast_done = false;
+  // Fast path: the whole recurrence is queued with its scalars (norms, alpha)
+  // kept on the device and read once at the end, instead of three host round
+  // trips per step. A breakdown (a residual norm at rounding level, where the
+  // reference restarts from a fresh random vector) is detected afterwards; the
+  // recurrence is then redone step by step below from the same start vector.
+  {
+    DeviceBuffer f0(n * sizeof(double)), alphas(steps * sizeof(double)),
+        betas((steps + 1) * sizeof(double));
+    vec_axpby(n, 1.0, f.as<double>(), 1, 0.0, f0.as<double>(), 1, s);
+    auto dnorm = [&](const double* x, double* out) {
+      residual_norms<double>(nullptr, x, nullptr, 1, n, 1, nullptr, nullptr, 0, nullptr, out,
+                             nullptr, ws.get(), ws.bytes(), s, 0);
+    };
+    for (int64_t it = 0; it < steps; ++it) {
+      dnorm(f.as<double>(), betas.as<double>() + it);
+      scale_by_inv(n, f.as<double>(), betas.as<double>() + it, V + it, ld, s);
+      csr_spmm<double>(A, V + it, ld, w.as<double>(), 1, nullptr, 0, 1, sign, 0.0, 0.0, s);
+      const int64_t k = it + 1;
+      vec_axpby(n, 1.0, w.as<double>(), 1, 0.0, f.as<double>(), 1, s);
+      gram<double>(V, ld, f.as<double>(), 1, n, k, 1, h.as<double>(), k, ws.get(), ws.bytes(), s);
+      rotate<double>(V, ld, h.as<double>(), k, f.as<double>(), 1, n, k, 1, -1.0, 1.0, s);
+      gram<double>(V, ld, f.as<double>(), 1, n, k, 1, hs.as<double>(), k, ws.get(), ws.bytes(),
+                   s);
+      rotate<double>(V, ld, hs.as<double>(), k, f.as<double>(), 1, n, k, 1, -1.0, 1.0, s);
+      sum2(h.as<double>() + k - 1, hs.as<double>() + k - 1, alphas.as<double>() + it, s);
+    }
+    dnorm(f.as<double>(), betas.as<double>() + steps);
+    std::vector<double> al(steps), be(steps + 1);
+    ctx.to_host(al.data(), alphas.as<double>(), steps);
+    ctx.to_host(be.data(), betas.as<double>(), steps + 1);
+    ctx.sync();
+    bool ok = true;
+    for (int64_t it = 0; it < steps; ++it)
+      ok = ok && std::isfinite(al[it]) && std::isfinite(be[it]) &&
+           be[it] > std::numeric_limits<double>::epsilon();
+    ok = ok && std::isfinite(be[steps]);
+    if (ok) {
+      for (int64_t it = 0; it < steps; ++it) {
+        if (it != 0) {
+          T[static_cast<size_t>(it - 1) * steps + it] = be[it];
+          T[static_cast<size_t>(it) * steps + it - 1] = be[it];
+        }
+        T[static_cast<size_t>(it) * steps + it] = al[it];
       }
-      orthogonalize(it, cand.as<double>());
-      restarted = true;
-      beta = norm(f.as<double>());
-      if (!(beta > std::numeric_limits<double>::epsilon()))
-        throw Error(FE_ERR_NONFINITE, "Lanczos: breakdown, unable to generate new basis vector.");
+      beta_next = be[steps];
+      fast_done = true;
+    } else {
+      vec_axpby(n, 1.0, f0.as<double>(), 1, 0.0, f.as<double>(), 1, s);
     }
-    vec_axpby(n, 1.0 / beta, f.as<double>(), 1, 0.0, V + it, ld, s);
-    csr_spmm<double>(A, V + it, ld, w.as<double>(), 1, nullptr, 0, 1, sign, 0.0, 0.0, s);
-    const double alpha = orthogonalize(it + 1, w.as<double>());
-    beta_next = norm(f.as<double>());
-    if (!std::isfinite(beta_next)) throw Error(FE_ERR_NONFINITE, "Lanczos: non-finite norm");
-    const double rec_beta = restarted ? 0.0 : beta;
-    if (it != 0) {
-      T[static_cast<size_t>(it - 1) * steps + it] = rec_beta;
-      T[static_cast<size_t>(it) * steps + it - 1] = rec_beta;
+  }
+  if (!fast_done) {
+    for (int64_t it = 0; it < steps; ++it) {
+      bool restarted = false;
+      double beta = norm(f.as<double>());
+      if (!std::isfinite(beta)) throw Error(FE_ERR_NONFINITE, "Lanczos: non-finite residual norm");
+      if (!(beta > std::numeric_limits<double>::epsilon())) {
+        // restart_residual (src/core/KrylovSubspace.cpp:251-259)
+        DeviceBuffer cand(n * sizeof(double));
+        if (host_init) {
+          std::mt19937 rng(seed + static_cast<unsigned>(it + 1));
+          std::uniform_real_distribution<double> dist(-1.0, 1.0);
+          std::vector<double> v(n);
+          for (auto& x : v) x = dist(rng);
+          ctx.to_device(cand.as<double>(), v.data(), n);
+        } else {
+          fill_uniform<double>(cand.as<double>(), 1, n, 1, seed + it + 1, s);
+        }
+        orthogonalize(it, cand.as<double>());
+        restarted = true;
+        beta = norm(f.as<double>());
+        if (!(beta > std::numeric_limits<double>::epsilon()))
+          throw Error(FE_ERR_NONFINITE, "Lanczos: breakdown, unable to generate new basis vector.");
+      }
+      vec_axpby(n, 1.0 / beta, f.as<double>(), 1, 0.0, V + it, ld, s);
+      csr_spmm<double>(A, V + it, ld, w.as<double>(), 1, nullptr, 0, 1, sign, 0.0, 0.0, s);
+      const double alpha = orthogonalize(it + 1, w.as<double>());
+      beta_next = norm(f.as<double>());
+      if (!std::isfinite(beta_next)) throw Error(FE_ERR_NONFINITE, "Lanczos: non-finite norm");
+      const double rec_beta = restarted ? 0.0 : beta;
+      if (it != 0) {
+        T[static_cast<size_t>(it - 1) * steps + it] = rec_beta;
+        T[static_cast<size_t>(it) * steps + it - 1] = rec_beta;
+      }
+      T[static_cast<size_t>(it) * steps + it] = alpha;
     }
-    T[static_cast<size_t>(it) * steps + it] = alpha;
   }
   std::vector<double> lam, Z;
   host_symmetric_eig(T, static_cast<int>(steps), lam, Z);

@@ -408,7 +408,8 @@ def test_block_diag_grouped_spmm():
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
-@pytest.mark.parametrize("n,k", [(1, 1), (300, 20), (70001, 97), (2049, 128)])
+@pytest.mark.parametrize("n,k", [(1, 1), (300, 20), (70001, 8), (5000, 9), (100003, 16), (777, 31), (40000, 32),
+                                 (70001, 97), (2049, 128)])
 def test_basis_times_vector_products(dtype, n, k):
     """Lanczos-shaped products (m = 1: V^T x and y = a V c + b y, the vector a
     strided column) keep the Gram and rotation bounds."""
