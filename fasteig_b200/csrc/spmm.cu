@@ -234,7 +234,7 @@ csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
                     const int32_t* __restrict__ colind, const T* __restrict__ vals,
                     const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
                     int64_t ldz, int ncols, int panel_vec, T alpha, T gamma, T beta,
-                    int use_gamma, int use_beta) {
+                    int use_gamma, int use_beta, int prefetch_z) {
   constexpr unsigned kFull = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t tw = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
@@ -265,6 +265,16 @@ csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
       for (int q = 0; q < CPL; ++q) {
         const int v = lane + 32 * q;
         if (v < nvec) z[q] = load_pack_rw<T, VEC>(Z + row * ldz + p0 + v * VEC);
+      }
+      // Z rows stream from DRAM: with prefetch_z, start this warp's next Z row
+      // toward L2 now (one 128-byte line per lane, addresses inside the row), so
+      // its loads there meet L2 rather than DRAM latency (pays off for the FP64
+      // panels, not for one FP32 panel: a per-operator autotune choice).
+      if (prefetch_z && nxt < nrows) {
+        const int bytes = nvec * VEC * static_cast<int>(sizeof(T));
+        if (lane * 128 < bytes)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(
+              reinterpret_cast<const char*>(Z + nxt * ldz + p0) + lane * 128));
       }
     }
     T acc[CPL][VEC];
@@ -396,7 +406,7 @@ csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
 template <typename T, int VEC>
 bool try_row_kernel(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, int64_t ldy,
                     const T* Z, int64_t ldz, int ncols, T alpha, T gamma, T beta, bool ug, bool ub,
-                    cudaStream_t s, int max_cpl) {
+                    cudaStream_t s, int max_cpl, bool prefetch_z = false) {
   constexpr int NZ = 7;
   const int nvec = ncols / VEC;
   if (nvec < 32 || ncols % VEC != 0 || A.max_row_nnz > NZ) return false;
@@ -419,7 +429,7 @@ bool try_row_kernel(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, 
     dim3 grid(static_cast<unsigned>(blocks), static_cast<unsigned>(panels));                   \
     kern<<<grid, kThreads, 0, s>>>(A.rows, A.rowptr, A.colind, vals, X, ldx, Y, ldy, Z, ldz,   \
                                    ncols, panel_vec, alpha, gamma, beta, ug ? 1 : 0,           \
-                                   ub ? 1 : 0);                                                \
+                                   ub ? 1 : 0, prefetch_z ? 1 : 0);                            \
     check_launch("csr_spmm_row_kernel");                                                       \
   } while (0)
   if (cpl == 1) FE_ROW(1);
@@ -791,7 +801,8 @@ int read_spmm_status(bool clear) {
 
 // Kernel selection for csr_spmm: "pipe" (bulk-copy pipelined) or "warp" (registers only).
 // 0 = row-batched kernel (panels <= 96 vectors) where it applies, 1 = loop kernel,
-// 2 = bulk-copy pipeline where it applies, 3 = row-batched with panels <= 64 vectors.
+// 2 = bulk-copy pipeline where it applies, 3 = row-batched with panels <= 64 vectors,
+// 4 = mode 0 with the next Z row prefetched into L2.
 static int g_spmm_mode = 0;
 void set_spmm_mode(int mode) { g_spmm_mode = mode; }
 
@@ -867,6 +878,11 @@ void csr_spmm_mode(int mode, const Csr& A, const T* X, int64_t ldx, T* Y, int64_
         try_row_kernel<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                                T(gamma), T(beta), ug, ub, s, 2))
       return;
+    // Mode 4: mode 0 with the next row's Z row prefetched into L2.
+    if (mode == 4 &&
+        try_row_kernel<T, 8 / sizeof(T)>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols),
+                                         T(alpha), T(gamma), T(beta), ug, ub, s, 5, true))
+      return;
     if (mode == 2 && ncols * static_cast<int64_t>(sizeof(T)) >= 64 &&
         try_pipe<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                          T(gamma), T(beta), ug, ub, s))
@@ -910,7 +926,7 @@ int autotune_spmm(Csr& A, int64_t ncols, cudaStream_t s) {
     FE_CHECK_CUDA(cudaEventCreate(&e0));
     FE_CHECK_CUDA(cudaEventCreate(&e1));
     float best_ms = 0.0f;
-    for (int mode : {0, 3, 2, 1}) {
+    for (int mode : {0, 3, 2, 1, 4}) {
       auto run = [&] {
         csr_spmm_mode<T>(mode, A, static_cast<const T*>(x), ld, static_cast<T*>(y), ld,
                          static_cast<const T*>(z), ld, ncols, 0.25, 0.1, -1.0, s);

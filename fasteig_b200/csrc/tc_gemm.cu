@@ -978,7 +978,7 @@ extern "C" int fe_device_status(int32_t* status, int32_t clear) {
 
 extern "C" int fe_set_spmm_kernel(int32_t mode) {
   return fe::guarded("fe_set_spmm_kernel", [&] {
-    FE_REQUIRE(mode >= 0 && mode <= 3, "mode must be 0..3");
+    FE_REQUIRE(mode >= 0 && mode <= 4, "mode must be 0..4");
     fe::set_spmm_mode(mode);
   });
 }

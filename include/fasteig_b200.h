@@ -174,7 +174,7 @@ int fe_device_status(int32_t* status, int32_t clear);
  * (row-batched register kernel for slabs of >= 32 128-bit vectors and rows of
  * <= 7 nonzeros, else the loop kernel), 1 = loop kernel, 2 = bulk-copy
  * pipelined kernel where it applies, 3 = row-batched kernel with narrower
- * column panels. */
+ * column panels, 4 = mode 0 with each warp's next Z row prefetched into L2. */
 int fe_set_spmm_kernel(int32_t mode);
 /* SpMM autotuner: times every SpMM kernel on operator A for an n-by-ncols block
  * in the Chebyshev-step form (precision 0 = FP64, 1 = FP32) on `stream` and

@@ -85,8 +85,8 @@ def register_kernel():
 @pytest.mark.parametrize("stencil", ["star1", "star2", "box"])
 @pytest.mark.parametrize("b", [16, 40, 320, 1000])
 def test_pipelined_and_register_spmm_agree_on_stencils(dtype, stencil, b):
-    """Every SpMM kernel (row-batched with 8- and 16-byte lanes, loop, bulk-copy
-    pipelined; 7/13/27-point rows) vs the oracle, including multi-panel and ragged
+    """Every SpMM kernel (row-batched with 8- and 16-byte lanes, with and without
+    the Z prefetch, loop, bulk-copy pipelined; 7/13/27-point rows) vs the oracle, including multi-panel and ragged
     panel widths and the fused Chebyshev epilogue."""
     import fasteig_b200 as fe
     from fasteig_b200 import matrices as M, ops
@@ -102,7 +102,7 @@ def test_pipelined_and_register_spmm_agree_on_stencils(dtype, stencil, b):
     Xn, Zn = X.double().cpu().numpy(), Z.double().cpu().numpy()
     ref = 0.7 * (A.scipy() @ Xn) - 0.2 * Xn - Zn
     outs = []
-    for mode in (0, 1, 2, 3):
+    for mode in (0, 1, 2, 3, 4):
         assert fe.lib.fe_set_spmm_kernel(mode) == 0
         Zc = Z.clone()
         ops.cheb_step(dA, X, Zc, Zc, 0.7, -0.2, -1.0)
@@ -148,7 +148,7 @@ def test_pipelined_spmm_rows_without_diagonal(dtype, n, b, alpha, gamma, beta):
     ref = alpha * (A.scipy() @ Xn) + gamma * Xn + beta * Zn
     outs = []
     try:
-        for mode in (2, 0):
+        for mode in (2, 0, 4):
             assert fe.lib.fe_set_spmm_kernel(mode) == 0
             Y = torch.full_like(X, float("nan"))
             ops.cheb_step(dA, X, Z, Y, alpha, gamma, beta)
