@@ -275,6 +275,14 @@ csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
         if (lane * 128 < bytes)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(
               reinterpret_cast<const char*>(Z + nxt * ldz + p0) + lane * 128));
+        // The next row's farthest neighbour, guessed by translating this row's
+        // (exact for a translation-invariant stencil; a wrong guess only wastes
+        // the prefetch): the X row a banded operator touches first.
+        const int cl = __shfl_sync(kFull, c_cur, min(nnz, NZ) - 1);
+        const int64_t cg = cl + (nxt - row);
+        if (nnz > 0 && cg >= 0 && cg < nrows && lane >= 16 && (lane - 16) * 128 < bytes)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(
+              reinterpret_cast<const char*>(Xp + cg * ldx) + (lane - 16) * 128));
       }
     }
     T acc[CPL][VEC];
@@ -429,7 +437,7 @@ bool try_row_kernel(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, 
     dim3 grid(static_cast<unsigned>(blocks), static_cast<unsigned>(panels));                   \
     kern<<<grid, kThreads, 0, s>>>(A.rows, A.rowptr, A.colind, vals, X, ldx, Y, ldy, Z, ldz,   \
                                    ncols, panel_vec, alpha, gamma, beta, ug ? 1 : 0,           \
-                                   ub ? 1 : 0, prefetch_z ? 1 : 0);                            \
+                                   ub ? 1 : 0, prefetch_z && A.rows == A.cols ? 1 : 0);        \
     check_launch("csr_spmm_row_kernel");                                                       \
   } while (0)
   if (cpl == 1) FE_ROW(1);
