@@ -1054,11 +1054,12 @@ struct RitzResult {
   std::vector<double> values, rel;
 };
 
-void ritz_extract(Context& ctx, SmallState& sm, ProjectedEig& eig, double* P, const double* Bm,
-                  const double* ABm, int64_t ld, int64_t n, int64_t cols, int64_t req,
-                  const std::string& which, double* X, double* AX, double* R, double* coef,
-                  DeviceBuffer& idx_dev, RitzResult& out, const double* BBm = nullptr,
-                  double* BX = nullptr) {
+template <typename T>
+void ritz_extract(Context& ctx, SmallState& sm, ProjectedEig& eig, double* P, const T* Bm,
+                  const T* ABm, int64_t ld, int64_t n, int64_t cols, int64_t req,
+                  const std::string& which, T* X, T* AX, T* R, double* coef,
+                  DeviceBuffer& idx_dev, RitzResult& out, const T* BBm = nullptr,
+                  T* BX = nullptr) {
   cudaStream_t s = ctx.stream;
   symmetrize(P, cols, sm.cap, s);
   eig.run(P, cols, sm.cap, sm.W.as<double>());
@@ -1075,11 +1076,11 @@ void ritz_extract(Context& ctx, SmallState& sm, ProjectedEig& eig, double* P, co
   idx_dev.resize(std::max<size_t>(sel.size() * sizeof(int32_t), 4));
   ctx.to_device(idx_dev.as<int32_t>(), sel.data(), sel.size());
   small_gather_scale(P, sm.cap, cols, idx_dev.as<int32_t>(), nullptr, req, coef, sm.cap, s);
-  rotate_block<double>(sm, Bm, ld, coef, X, ld, n, cols, req, 1.0, 0.0, s);
-  rotate_block<double>(sm, ABm, ld, coef, AX, ld, n, cols, req, 1.0, 0.0, s);
-  if (BBm) rotate_block<double>(sm, BBm, ld, coef, BX, ld, n, cols, req, 1.0, 0.0, s);
+  rotate_block<T>(sm, Bm, ld, coef, X, ld, n, cols, req, 1.0, 0.0, s);
+  rotate_block<T>(sm, ABm, ld, coef, AX, ld, n, cols, req, 1.0, 0.0, s);
+  if (BBm) rotate_block<T>(sm, BBm, ld, coef, BX, ld, n, cols, req, 1.0, 0.0, s);
   ctx.to_device(sm.W.as<double>(), out.values.data(), req);
-  residual_norms<double>(AX, X, BBm ? BX : nullptr, ld, n, req, sm.W.as<double>(), R, R ? ld : 0,
+  residual_norms<T>(AX, X, BBm ? BX : nullptr, ld, n, req, sm.W.as<double>(), R, R ? ld : 0,
                          sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
                          sm.rws.get(), sm.rws.bytes(), s, 1);
   out.rel.resize(req);
@@ -1410,7 +1411,8 @@ void check_pair(const Csr& A, const Csr& B) {
 // evaluate_ritz_pairs with B (src/core/RitzExtraction.cpp:50-56). B absent means
 // M = I (B-blocks are then copies).
 // ===========================================================================
-struct GenBlockOps {
+template <typename T>
+struct GenBlockOpsT {
   Context& ctx;
   SmallState& sm;
   ProjectedEig& eig;
@@ -1420,25 +1422,28 @@ struct GenBlockOps {
   int64_t n, ld;
   Stats& st;
   DeviceBuffer idx_dev;
+  // Singular values of an orthonormalization below this fraction of the largest
+  // are dropped as noise: about sqrt(unit roundoff) of the block's precision.
+  static constexpr double kRankFloor = sizeof(T) == 4 ? 1e-3 : 1e-7;
 
-  void bapply(const double* X, double* BX, int64_t cols) {
+  void bapply(const T* X, T* BX, int64_t cols) {
     if (cols <= 0) return;
     if (B) {
-      csr_spmm<double>(*B, X, ld, BX, ld, nullptr, 0, cols, 1.0, 0.0, 0.0, ctx.stream);
+      csr_spmm<T>(*B, X, ld, BX, ld, nullptr, 0, cols, 1.0, 0.0, 0.0, ctx.stream);
       st.spmm_launches += 1;
     } else {
-      FE_CHECK_CUDA(cudaMemcpy2DAsync(BX, ld * 8, X, ld * 8, cols * 8, n,
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(BX, ld * sizeof(T), X, ld * sizeof(T), cols * sizeof(T), n,
                                       cudaMemcpyDeviceToDevice, ctx.stream));
     }
   }
-  void happly(const double* X, double* AX, int64_t cols) {
+  void happly(const T* X, T* AX, int64_t cols) {
     if (cols <= 0) return;
-    csr_spmm<double>(A, X, ld, AX, ld, nullptr, 0, cols, sign, 0.0, 0.0, ctx.stream);
+    csr_spmm<T>(A, X, ld, AX, ld, nullptr, 0, cols, sign, 0.0, 0.0, ctx.stream);
     st.spmm_launches += 1;
   }
-  void copy(double* dst, const double* src, int64_t cols) {
+  void copy(T* dst, const T* src, int64_t cols) {
     if (cols <= 0 || dst == src) return;
-    FE_CHECK_CUDA(cudaMemcpy2DAsync(dst, ld * 8, src, ld * 8, cols * 8, n,
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(dst, ld * sizeof(T), src, ld * sizeof(T), cols * sizeof(T), n,
                                     cudaMemcpyDeviceToDevice, ctx.stream));
   }
 
@@ -1448,16 +1453,16 @@ struct GenBlockOps {
   // values above max(rank_tol * largest B-norm, 1e-7 * largest) -> rotate by
   // U S^-1 (orthonormalize_block, src/core/Orthogonalization.cpp:717-775, in the B
   // metric). Writes out/Bout[:, :rank] (may alias src; tmp/tmpB are scratch).
-  int64_t ortho(const double* V, const double* BV, int64_t k, const double* src, int64_t cols,
-                double* out, double* Bout, double* tmp, double* tmpB, double rank_tol = 1e-12) {
+  int64_t ortho(const T* V, const T* BV, int64_t k, const T* src, int64_t cols, T* out, T* Bout,
+                T* tmp, T* tmpB, double rank_tol = 1e-12) {
     cudaStream_t s = ctx.stream;
     if (k >= n || cols <= 0) return 0;
-    const double* cur = src;
+    const T* cur = src;
     int64_t rank = 0;
     std::vector<double> norms, w, inv;
     for (int pass = 0; pass < 2; ++pass) {
       bapply(cur, tmpB, cols);
-      residual_norms<double>(nullptr, cur, tmpB, ld, n, cols, nullptr, nullptr, 0, nullptr,
+      residual_norms<T>(nullptr, cur, tmpB, ld, n, cols, nullptr, nullptr, 0, nullptr,
                              sm.xnorm.as<double>(), nullptr, sm.rws.get(), sm.rws.bytes(), s, 2);
       norms.resize(cols);
       ctx.to_host(norms.data(), sm.xnorm.as<double>(), cols);
@@ -1473,12 +1478,12 @@ struct GenBlockOps {
       double* G = sm.G.as<double>();
       if (k > 0) {
         for (int g = 0; g < 2; ++g) {
-          gram_block<double>(sm, V, ld, tmpB, ld, n, k, cols, G, s);
-          rotate_block<double>(sm, V, ld, G, tmp, ld, n, k, cols, -1.0, 1.0, s);
-          rotate_block<double>(sm, BV, ld, G, tmpB, ld, n, k, cols, -1.0, 1.0, s);
+          gram_block<T>(sm, V, ld, tmpB, ld, n, k, cols, G, s);
+          rotate_block<T>(sm, V, ld, G, tmp, ld, n, k, cols, -1.0, 1.0, s);
+          rotate_block<T>(sm, BV, ld, G, tmpB, ld, n, k, cols, -1.0, 1.0, s);
         }
       }
-      gram_block<double>(sm, tmp, ld, tmpB, ld, n, cols, cols, G, s);
+      gram_block<T>(sm, tmp, ld, tmpB, ld, n, cols, cols, G, s);
       symmetrize(G, cols, sm.cap, s);
       eig.run(G, cols, sm.cap, sm.W.as<double>());
       w.resize(cols);
@@ -1486,7 +1491,7 @@ struct GenBlockOps {
       ctx.sync();
       const double smax = std::sqrt(std::max(w[cols - 1], 0.0));
       const int64_t capacity = std::min<int64_t>(cols, n - k);
-      const double cut = std::max(rank_tol * scale, 1e-7 * smax);
+      const double cut = std::max(rank_tol * scale, kRankFloor * smax);
       std::vector<int32_t> sel;
       inv.clear();
       for (int64_t i = cols - 1; i >= 0 && static_cast<int64_t>(sel.size()) < capacity; --i) {
@@ -1504,9 +1509,8 @@ struct GenBlockOps {
       ctx.to_device(di, sel.data(), rank);
       ctx.to_device(ds, inv.data(), rank);
       small_gather_scale(G, sm.cap, cols, di, ds, rank, sm.Rinv.as<double>(), sm.cap, s);
-      rotate_block<double>(sm, tmp, ld, sm.Rinv.as<double>(), out, ld, n, cols, rank, 1.0, 0.0, s);
-      rotate_block<double>(sm, tmpB, ld, sm.Rinv.as<double>(), Bout, ld, n, cols, rank, 1.0, 0.0,
-                           s);
+      rotate_block<T>(sm, tmp, ld, sm.Rinv.as<double>(), out, ld, n, cols, rank, 1.0, 0.0, s);
+      rotate_block<T>(sm, tmpB, ld, sm.Rinv.as<double>(), Bout, ld, n, cols, rank, 1.0, 0.0, s);
       cur = out;
       cols = rank;
       ctx.sync();
@@ -1515,11 +1519,11 @@ struct GenBlockOps {
   }
 
   // Weighted Cholesky QR with a fresh BX: X <- X R^-1, BX <- B X R^-1 (through tmp/tmpB).
-  void bcholqr(double* X, double* BX, int64_t b, double* tmp, double* tmpB, const char* what) {
+  void bcholqr(T* X, T* BX, int64_t b, T* tmp, T* tmpB, const char* what) {
     cudaStream_t s = ctx.stream;
     bapply(X, BX, b);
     double* G = sm.G.as<double>();
-    gram_block<double>(sm, X, ld, BX, ld, n, b, b, G, s);
+    gram_block<T>(sm, X, ld, BX, ld, n, b, b, G, s);
     symmetrize(G, b, sm.cap, s);
     FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, sizeof(int32_t), s));
     potrf_upper(G, b, sm.cap, sm.info.as<int32_t>(), s);
@@ -1528,13 +1532,110 @@ struct GenBlockOps {
     ctx.sync();
     if (info != 0) throw Error(FE_ERR_NOT_SPD, std::string(what) + ": weighted QR failed.");
     trinv_upper(G, sm.cap, sm.Rinv.as<double>(), sm.cap, b, s);
-    rotate_block<double>(sm, X, ld, sm.Rinv.as<double>(), tmp, ld, n, b, b, 1.0, 0.0, s);
-    rotate_block<double>(sm, BX, ld, sm.Rinv.as<double>(), tmpB, ld, n, b, b, 1.0, 0.0, s);
+    rotate_block<T>(sm, X, ld, sm.Rinv.as<double>(), tmp, ld, n, b, b, 1.0, 0.0, s);
+    rotate_block<T>(sm, BX, ld, sm.Rinv.as<double>(), tmpB, ld, n, b, b, 1.0, 0.0, s);
     copy(X, tmp, b);
     copy(BX, tmpB, b);
   }
 };
+using GenBlockOps = GenBlockOpsT<double>;
 
+// Device blocks of one precision phase of the generalized LOBPCG.
+template <typename T>
+struct LobpcgBlocks {
+  Block<T> X, AX, BX, R, Pd, S, AS, BS, T1, T2, Wsrc;
+  void allocate(int64_t n, int64_t cap) {
+    for (Block<T>* q : {&X, &AX, &BX, &R, &Pd, &S, &AS, &BS, &T1, &T2, &Wsrc}) q->allocate(n, cap);
+  }
+};
+
+// One precision phase of the generalized LOBPCG (LOBPCGSolver::solve,
+// src/LOBPCGSolver.cpp:25-174, in the B metric with an optional Jacobi
+// preconditioner t): B-orthonormalize the start block X[:, :b], Rayleigh-Ritz,
+// then iterate until every wanted pair's residual is <= lock_tol (pairs at or
+// below it leave the correction block W), maxiter, or, with stop_at_floor (the
+// FP32 phase), a worst residual below 1e-3 that has not halved over fifteen
+// iterations (far from convergence the worst pair of a LOBPCG block can sit still
+// for a while before the block converges; near the FP32 floor it creeps).
+template <typename T>
+void lobpcg_gen_phase(Context& ctx, SmallState& sm, ProjectedEig& eig, const Csr& A,
+                      const Csr* B, const Options& opt, double sign, int64_t b, int64_t cap,
+                      const double* t, LobpcgBlocks<T>& L, RitzResult& ritz, int64_t& it_done,
+                      double lock_tol, bool stop_at_floor, DeviceBuffer& act, DeviceBuffer& coef,
+                      Stats& st) {
+  cudaStream_t s = ctx.stream;
+  const int64_t n = A.rows, nev = opt.nev, ld = L.X.ld;
+  GenBlockOpsT<T> g{ctx, sm, eig, A, B, sign, n, ld, st, DeviceBuffer(64)};
+  if (g.ortho(nullptr, nullptr, 0, L.X.data(), b, L.X.data(), L.BX.data(), L.T1.data(),
+              L.T2.data()) < b)
+    throw Error(FE_ERR_NOT_SPD, "LOBPCGSolver: initial block is rank deficient.");
+  g.happly(L.X.data(), L.AX.data(), b);
+  g.copy(L.S.data(), L.X.data(), b);
+  g.copy(L.AS.data(), L.AX.data(), b);
+  g.copy(L.BS.data(), L.BX.data(), b);
+  gram_block<T>(sm, L.S.data(), ld, L.AS.data(), ld, n, b, b, sm.G.as<double>(), s);
+  ritz_extract<T>(ctx, sm, eig, sm.G.as<double>(), L.S.data(), L.AS.data(), ld, n, b, b, "sr",
+                  L.X.data(), L.AX.data(), L.R.data(), coef.as<double>(), g.idx_dev, ritz,
+                  L.BS.data(), L.BX.data());
+  auto worst_nev = [&] {
+    double w = 0;
+    for (int64_t j = 0; j < nev; ++j) w = std::max(w, ritz.rel[j]);
+    return w;
+  };
+  std::vector<double> history;
+  bool have_p = false;
+  while (it_done < opt.maxiter) {
+    const double worst = worst_nev();
+    if (worst <= lock_tol) break;
+    if (stop_at_floor && worst <= 1e-3) {
+      history.push_back(worst);
+      const size_t h = history.size();
+      if (h > 15 && worst > 0.5 * history[h - 16]) break;
+    }
+    std::vector<int32_t> active;
+    for (int64_t j = 0; j < b; ++j)
+      if (ritz.rel[j] > lock_tol) active.push_back(static_cast<int32_t>(j));
+    const int64_t na = static_cast<int64_t>(active.size());
+    ctx.to_device(act.as<int32_t>(), active.data(), na);
+    gather_columns<T>(L.R.data(), ld, act.as<int32_t>(), na, L.Wsrc.data(), ld, n, s, t);
+    g.bcholqr(L.X.data(), L.BX.data(), b, L.T1.data(), L.T2.data(), "LOBPCGSolver: Ritz-vector");
+    g.copy(L.S.data(), L.X.data(), b);
+    g.copy(L.BS.data(), L.BX.data(), b);
+    int64_t cols = b;
+    const int64_t rw = g.ortho(L.S.data(), L.BS.data(), cols, L.Wsrc.data(), na, L.S.col(cols),
+                               L.BS.col(cols), L.T1.data(), L.T2.data());
+    cols += std::min(rw, cap - cols);
+    if (have_p && cols < cap) {
+      gather_columns<T>(L.Pd.data(), ld, act.as<int32_t>(), na, L.Wsrc.data(), ld, n, s);
+      const int64_t rp = g.ortho(L.S.data(), L.BS.data(), cols, L.Wsrc.data(), na, L.S.col(cols),
+                                 L.BS.col(cols), L.T1.data(), L.T2.data());
+      cols += std::min(rp, cap - cols);
+    }
+    g.happly(L.S.data(), L.AS.data(), cols);
+    gram_block<T>(sm, L.S.data(), ld, L.AS.data(), ld, n, cols, cols, sm.G.as<double>(), s);
+    ritz_extract<T>(ctx, sm, eig, sm.G.as<double>(), L.S.data(), L.AS.data(), ld, n, cols, b, "sr",
+                    L.X.data(), L.AX.data(), L.R.data(), coef.as<double>(), g.idx_dev, ritz,
+                    L.BS.data(), L.BX.data());
+    // P = S C with the X rows of C zeroed.
+    FE_CHECK_CUDA(cudaMemset2DAsync(coef.get(), cap * 8, 0, b * 8, b, s));
+    rotate_block<T>(sm, L.S.data(), ld, coef.as<double>(), L.Pd.data(), ld, n, cols, b, 1.0, 0.0,
+                    s);
+    have_p = true;
+    ++it_done;
+    if (opt.verbosity >= 2)
+      std::fprintf(stderr, "[fe] lobpcg-g %s iter %lld cols %lld worst %.3e\n",
+                   sizeof(T) == 4 ? "fp32" : "fp64", static_cast<long long>(it_done),
+                   static_cast<long long>(cols), worst_nev());
+    if (worst_nev() <= lock_tol || cols == b) break;
+  }
+}
+
+// Generalized / preconditioned / wide-block LOBPCG. precision=mixed runs the
+// iteration on FP32 blocks (FP32 SpMMs, split-TF32 Grams and rotations, FP64
+// projected problems) until the wanted pairs reach the FP32 floor (mixed_switch)
+// or stall there, then restarts from those Ritz vectors on FP64 blocks to tol
+// (carrying the FP32 search directions P over measured slower: 78 vs 66 FP64
+// iterations on the 80^3 pair).
 void lobpcg_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* eigenvalues,
                       double* residuals, double* eigenvectors, Stats& st) {
   const int64_t n = A.rows, nev = opt.nev;
@@ -1542,20 +1643,18 @@ void lobpcg_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* ei
     throw Error(FE_ERR_INVALID, "LOBPCGSolver: require 0 < nev <= n and maxiter > 0.");
   if (opt.which != "sr" && opt.which != "lr")
     throw Error(FE_ERR_INVALID, "LOBPCGSolver: only SR and LR are supported.");
+  FE_REQUIRE(opt.precision == "fp64" || opt.precision == "mixed",
+             "precision must be fp64 or mixed");
   const int64_t b = std::min<int64_t>(n, std::max<int64_t>(nev, opt.block));
   const double sign = opt.which == "lr" ? -1.0 : 1.0;
   const double tol = opt.tol;
   const int64_t cap = std::min<int64_t>(n, 3 * b);
+  const bool mixed = opt.precision == "mixed";
   Context ctx;
   cudaStream_t s = ctx.stream;
   SmallState sm;
-  sm.allocate(n, cap, false);
+  sm.allocate(n, cap, mixed && opt.tensor_cores && tc_gemm_available());
   ProjectedEig eig(ctx, cap);
-  Block<double> X, AX, BX, R, Pd, S, AS, BS, T1, T2, Wsrc;
-  for (Block<double>* q : {&X, &AX, &BX, &R, &Pd, &S, &AS, &BS, &T1, &T2, &Wsrc})
-    q->allocate(n, cap);
-  const int64_t ld = X.ld;
-  GenBlockOps g{ctx, sm, eig, A, B, sign, n, ld, st, DeviceBuffer(64)};
   DeviceBuffer tdiag, act(static_cast<size_t>(cap) * sizeof(int32_t) + 16),
       coef(static_cast<size_t>(cap) * cap * sizeof(double));
   const double* t = nullptr;
@@ -1564,65 +1663,36 @@ void lobpcg_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* ei
     jacobi_inverse_diagonal(A, tdiag.as<double>(), s);
     t = tdiag.as<double>();
   }
-  fill_initial_block(ctx, X.data(), ld, n, b, opt.seed_or_default(), opt.init == "host");
-  if (g.ortho(nullptr, nullptr, 0, X.data(), b, X.data(), BX.data(), T1.data(), T2.data()) < b)
-    throw Error(FE_ERR_NOT_SPD, "LOBPCGSolver: initial block is rank deficient.");
-  g.happly(X.data(), AX.data(), b);
-  g.copy(S.data(), X.data(), b);
-  g.copy(AS.data(), AX.data(), b);
-  g.copy(BS.data(), BX.data(), b);
-  gram_block<double>(sm, S.data(), ld, AS.data(), ld, n, b, b, sm.G.as<double>(), s);
   RitzResult ritz;
-  ritz_extract(ctx, sm, eig, sm.G.as<double>(), S.data(), AS.data(), ld, n, b, b, "sr", X.data(),
-               AX.data(), R.data(), coef.as<double>(), g.idx_dev, ritz, BS.data(), BX.data());
-  auto worst_nev = [&] {
-    double w = 0;
-    for (int64_t j = 0; j < nev; ++j) w = std::max(w, ritz.rel[j]);
-    return w;
-  };
-  bool have_p = false;
   int64_t it_done = 0;
-  for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
-    if (worst_nev() <= tol) break;
-    std::vector<int32_t> active;
-    for (int64_t j = 0; j < b; ++j)
-      if (ritz.rel[j] > tol) active.push_back(static_cast<int32_t>(j));
-    const int64_t na = static_cast<int64_t>(active.size());
-    ctx.to_device(act.as<int32_t>(), active.data(), na);
-    gather_columns<double>(R.data(), ld, act.as<int32_t>(), na, Wsrc.data(), ld, n, s, t);
-    g.bcholqr(X.data(), BX.data(), b, T1.data(), T2.data(), "LOBPCGSolver: Ritz-vector");
-    g.copy(S.data(), X.data(), b);
-    g.copy(BS.data(), BX.data(), b);
-    int64_t cols = b;
-    int64_t rw = g.ortho(S.data(), BS.data(), cols, Wsrc.data(), na, S.col(cols), BS.col(cols),
-                         T1.data(), T2.data());
-    cols += std::min(rw, cap - cols);
-    if (have_p && cols < cap) {
-      gather_columns<double>(Pd.data(), ld, act.as<int32_t>(), na, Wsrc.data(), ld, n, s);
-      const int64_t rp = g.ortho(S.data(), BS.data(), cols, Wsrc.data(), na, S.col(cols),
-                                 BS.col(cols), T1.data(), T2.data());
-      cols += std::min(rp, cap - cols);
+  LobpcgBlocks<double> D;
+  if (mixed) {
+    LobpcgBlocks<float> F;
+    F.allocate(n, cap);
+    {
+      Block<double> X0;
+      X0.allocate(n, b);
+      fill_initial_block(ctx, X0.data(), X0.ld, n, b, opt.seed_or_default(), opt.init == "host");
+      convert<double, float>(X0.data(), X0.ld, F.X.data(), F.X.ld, n, b, s);
+      ctx.sync();
     }
-    g.happly(S.data(), AS.data(), cols);
-    gram_block<double>(sm, S.data(), ld, AS.data(), ld, n, cols, cols, sm.G.as<double>(), s);
-    ritz_extract(ctx, sm, eig, sm.G.as<double>(), S.data(), AS.data(), ld, n, cols, b, "sr",
-                 X.data(), AX.data(), R.data(), coef.as<double>(), g.idx_dev, ritz, BS.data(),
-                 BX.data());
-    // P = S C with the X rows of C zeroed.
-    FE_CHECK_CUDA(cudaMemset2DAsync(coef.get(), cap * 8, 0, b * 8, b, s));
-    rotate_block<double>(sm, S.data(), ld, coef.as<double>(), Pd.data(), ld, n, cols, b, 1.0, 0.0,
-                         s);
-    have_p = true;
-    it_done = iter + 1;
-    if (opt.verbosity >= 2)
-      std::fprintf(stderr, "[fe] lobpcg-g iter %lld cols %lld worst %.3e\n",
-                   static_cast<long long>(iter + 1), static_cast<long long>(cols), worst_nev());
-    if (worst_nev() <= tol || cols == b) break;
+    lobpcg_gen_phase<float>(ctx, sm, eig, A, B, opt, sign, b, cap, t, F, ritz, it_done,
+                            std::max(tol, opt.mixed_switch), true, act, coef, st);
+    st.fp32_iterations = static_cast<double>(it_done);
+    D.allocate(n, cap);
+    convert<float, double>(F.X.data(), F.X.ld, D.X.data(), D.X.ld, n, b, s);
+    ctx.sync();
+  } else {
+    D.allocate(n, cap);
+    fill_initial_block(ctx, D.X.data(), D.X.ld, n, b, opt.seed_or_default(), opt.init == "host");
   }
+  const int64_t it64 = it_done;
+  lobpcg_gen_phase<double>(ctx, sm, eig, A, B, opt, sign, b, cap, t, D, ritz, it_done, tol, false,
+                           act, coef, st);
   for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = sign * ritz.values[j];
-  finish_results(ctx, sm, A, B, X.data(), ld, n, nev, eigenvalues, residuals, eigenvectors);
+  finish_results(ctx, sm, A, B, D.X.data(), D.X.ld, n, nev, eigenvalues, residuals, eigenvectors);
   st.iterations = static_cast<double>(it_done);
-  st.fp64_iterations = static_cast<double>(it_done);
+  st.fp64_iterations = static_cast<double>(it_done - it64);
 }
 
 void davidson_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* eigenvalues,
@@ -2341,7 +2411,7 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
   } else if (opt.solver == "lobpcg") {
     // The reference's standard unpreconditioned LOBPCG unless the problem is
     // generalized, preconditioned, or iterates more vectors than requested.
-    if (B || opt.precond != "none" || opt.block > opt.nev) {
+    if (B || opt.precond != "none" || opt.block > opt.nev || opt.precision == "mixed") {
       if (B) check_pair(A, *B);
       lobpcg_gen_solve(A, B, opt, eigenvalues, residual_norms, eigenvectors, st);
     } else {

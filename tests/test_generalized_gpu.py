@@ -62,6 +62,37 @@ def test_lobpcg_generalized_matches_oracle_and_dense(km8, dense_km8, precond):
 
 
 @pytest.mark.parametrize("precond", ["none", "jacobi"])
+@pytest.mark.parametrize("which,nev,block", [("sr", 8, 8), ("sr", 13, 18), ("lr", 8, 12)])
+def test_lobpcg_generalized_mixed_precision_against_dense(km8, dense_km8, precond, which, nev,
+                                                          block):
+    """precision=mixed: FP32 phase (FP32 SpMMs, split-TF32 Grams and rotations) to the
+    FP32 floor, then FP64 iterations to tol from its Ritz vectors. Eigenvalues equal the
+    dense generalized spectrum, residuals recomputed by the oracle reach tol, and both
+    phases ran."""
+    from oracle import oracle as O
+    K, Mm = km8
+    p = solve(K, Mm, solver="LOBPCG", nev=nev, which=which, tol=1e-8, maxiter=800, seed=1,
+              precond=precond, block=block, precision="mixed")
+    exp = dense_km8[:nev] if which == "sr" else dense_km8[::-1][:nev]
+    np.testing.assert_allclose(p.eigenvalues(), exp, rtol=1e-10, atol=1e-12)
+    assert np.all(p.residual_norms() <= 1.01e-8)
+    final = O.residual_norms(K, Mm, p.eigenvalues(), p.eigenvectors())
+    assert np.all(final <= 1.01e-8), final
+    assert p.stats["fp32_iterations"] > 0 and p.stats["fp64_iterations"] > 0, p.stats
+
+
+def test_lobpcg_standard_mixed_precision_against_dense(wells_small):
+    """precision=mixed on a standard problem (routed to the generalized loop with B = I)."""
+    from oracle import oracle as O
+    A, dense = wells_small
+    p = solve(A, None, solver="LOBPCG", nev=10, which="SR", tol=1e-8, maxiter=800, seed=2,
+              block=14, precision="mixed")
+    np.testing.assert_allclose(p.eigenvalues(), dense[:10], rtol=1e-10, atol=1e-12)
+    final = O.residual_norms(A, None, p.eigenvalues(), p.eigenvectors())
+    assert np.all(final <= 1.01e-8), final
+
+
+@pytest.mark.parametrize("precond", ["none", "jacobi"])
 @pytest.mark.parametrize("which", ["sr", "lr"])
 def test_davidson_generalized_matches_oracle_and_dense(km8, dense_km8, precond, which):
     from oracle import oracle as O
