@@ -187,7 +187,8 @@ def run_generalized(a):
     # iterations); Davidson keeps up to 4 such blocks in its basis.
     for solver, extra in (("LOBPCG", dict(block=96)),
                           ("LOBPCG", dict(block=96, precision="mixed")),
-                          ("Davidson", dict(block=96, maxblks=4))):
+                          ("Davidson", dict(block=96, maxblks=4)),
+                          ("Davidson", dict(block=96, maxblks=4, precision="mixed"))):
         o = fe.fasteig_options()
         for k, v in dict(dict(solver=solver, nev=64, which="SR", tol=a.tol, maxiter=3000, seed=1,
                               precond="jacobi", init="device"), **extra).items():

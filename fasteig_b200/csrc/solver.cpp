@@ -1695,6 +1695,98 @@ void lobpcg_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* ei
   st.fp64_iterations = static_cast<double>(it_done - it64);
 }
 
+template <typename T>
+struct DavidsonBlocks {
+  Block<T> V, AV, BV, X, AX, BX, R, T1, T2, Wsrc;
+  void allocate(int64_t n, int64_t cap) {
+    for (Block<T>* q : {&V, &AV, &BV, &X, &AX, &BX, &R, &T1, &T2, &Wsrc}) q->allocate(n, cap);
+  }
+};
+
+// One precision phase of the generalized block Davidson (DavidsonSolver::solve,
+// src/DavidsonSolver.cpp:27-264, in the B metric with an optional Jacobi
+// preconditioner t): restart from X[:, :bw], expand the basis by up to maxblks - 1
+// blocks of corrections, Rayleigh-Ritz after each. Stops when the wanted pairs are
+// below `stop_tol`, at maxiter, or, with stop_at_floor (the FP32 phase), when a
+// worst residual below 1e-3 has not halved over eight restarts. Corrections are
+// formed for pairs above `active_tol`.
+template <typename T>
+void davidson_gen_phase(Context& ctx, SmallState& sm, ProjectedEig& eig, const Csr& A,
+                        const Csr* B, const Options& opt, int64_t bw, int64_t cap,
+                        const double* t, DavidsonBlocks<T>& L, RitzResult& ritz,
+                        int64_t& it_done, double stop_tol, double active_tol, bool stop_at_floor,
+                        DeviceBuffer& act, DeviceBuffer& coef, DeviceBuffer& proj, Stats& st) {
+  cudaStream_t s = ctx.stream;
+  const int64_t n = A.rows, nev = opt.nev, ld = L.V.ld;
+  const std::string which = opt.which;
+  GenBlockOpsT<T> g{ctx, sm, eig, A, B, 1.0, n, ld, st, DeviceBuffer(64)};
+  double* Pm = proj.as<double>();
+  double* Pw = sm.G.as<double>();
+  auto extract = [&](int64_t cols) {
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(Pw, cap * 8, Pm, cap * 8, cols * 8, cols,
+                                    cudaMemcpyDeviceToDevice, s));
+    ritz_extract<T>(ctx, sm, eig, Pw, L.V.data(), L.AV.data(), ld, n, cols, bw, which,
+                    L.X.data(), L.AX.data(), L.R.data(), coef.as<double>(), g.idx_dev, ritz,
+                    L.BV.data(), L.BX.data());
+  };
+  if (g.ortho(nullptr, nullptr, 0, L.X.data(), bw, L.X.data(), L.BX.data(), L.T1.data(),
+              L.T2.data()) < bw)
+    throw Error(FE_ERR_NOT_SPD, "DavidsonSolver: initial block is rank deficient.");
+  g.copy(L.V.data(), L.X.data(), bw);
+  g.copy(L.BV.data(), L.BX.data(), bw);
+  g.happly(L.V.data(), L.AV.data(), bw);
+  gram_block<T>(sm, L.V.data(), ld, L.AV.data(), ld, n, bw, bw, Pm, s);
+  extract(bw);
+  std::vector<double> history;
+  while (it_done < opt.maxiter) {
+    g.bcholqr(L.X.data(), L.BX.data(), bw, L.T1.data(), L.T2.data(), "DavidsonSolver: restart");
+    g.copy(L.V.data(), L.X.data(), bw);
+    g.copy(L.BV.data(), L.BX.data(), bw);
+    g.happly(L.V.data(), L.AV.data(), bw);
+    FE_CHECK_CUDA(cudaMemset2DAsync(Pm, cap * 8, 0, cap * 8, cap, s));
+    gram_block<T>(sm, L.V.data(), ld, L.AV.data(), ld, n, bw, bw, Pm, s);
+    int64_t cols = bw;
+    extract(cols);
+    for (int64_t blk = 1; blk < opt.maxblks; ++blk) {
+      std::vector<int32_t> active;
+      for (int64_t j = 0; j < bw; ++j)
+        if (ritz.rel[j] > active_tol) active.push_back(static_cast<int32_t>(j));
+      const int64_t cc = static_cast<int64_t>(active.size());
+      if (cc == 0 || cols + cc > cap) break;
+      ctx.to_device(act.as<int32_t>(), active.data(), cc);
+      gather_columns<T>(L.R.data(), ld, act.as<int32_t>(), cc, L.Wsrc.data(), ld, n, s, t);
+      const int64_t r = g.ortho(L.V.data(), L.BV.data(), cols, L.Wsrc.data(), cc, L.V.col(cols),
+                                L.BV.col(cols), L.T1.data(), L.T2.data());
+      if (r == 0) break;
+      g.happly(L.V.col(cols), L.AV.col(cols), r);
+      // projected[:cols, cols:cols+r] = V^T A W, mirrored; diagonal block W^T A W.
+      gram_block<T>(sm, L.V.data(), ld, L.AV.col(cols), ld, n, cols, r, Pm + cols * cap, s);
+      gram_block<T>(sm, L.V.col(cols), ld, L.AV.col(cols), ld, n, r, r, Pm + cols * cap + cols,
+                    s);
+      mirror_block(Pm, cap, cols, cols, r, s);
+      cols += r;
+      extract(cols);
+    }
+    ++it_done;
+    double worst = 0;
+    for (int64_t j = 0; j < nev; ++j) worst = std::max(worst, ritz.rel[j]);
+    if (opt.verbosity >= 2)
+      std::fprintf(stderr, "[fe] davidson-g %s iter %lld cols %lld worst %.3e\n",
+                   sizeof(T) == 4 ? "fp32" : "fp64", static_cast<long long>(it_done),
+                   static_cast<long long>(cols), worst);
+    if (!ritz.rel.empty() && worst < stop_tol) break;
+    if (stop_at_floor && worst <= 1e-3) {
+      history.push_back(worst);
+      const size_t h = history.size();
+      if (h > 8 && worst > 0.5 * history[h - 9]) break;
+    }
+  }
+}
+
+// Generalized / preconditioned / wide-block Davidson. precision=mixed runs the
+// restarts on FP32 blocks (FP32 SpMMs, split-TF32 Grams and rotations, FP64
+// projected problems) until the wanted pairs reach the FP32 floor (mixed_switch)
+// or stall there, then restarts from those Ritz vectors on FP64 blocks to tol.
 void davidson_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* eigenvalues,
                         double* residuals, double* eigenvectors, Stats& st) {
   const int64_t n = A.rows, nev = opt.nev;
@@ -1705,19 +1797,18 @@ void davidson_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* 
   const std::string which = opt.which;
   if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
     throw Error(FE_ERR_INVALID, "DavidsonSolver: invalid which option (use SR/LR/SM/LM/BE).");
+  FE_REQUIRE(opt.precision == "fp64" || opt.precision == "mixed",
+             "precision must be fp64 or mixed");
   const double tol = opt.tol;
+  const bool mixed = opt.precision == "mixed";
   // Block of b >= nev Ritz vectors; convergence is judged on the first nev.
   const int64_t bw = std::min<int64_t>(n, std::max<int64_t>(nev, opt.block));
   const int64_t cap = std::min<int64_t>(n, opt.maxblks * bw);
   Context ctx;
   cudaStream_t s = ctx.stream;
   SmallState sm;
-  sm.allocate(n, cap, false);
+  sm.allocate(n, cap, mixed && opt.tensor_cores && tc_gemm_available());
   ProjectedEig eig(ctx, cap);
-  Block<double> V, AV, BV, X, AX, BX, R, T1, T2, Wsrc;
-  for (Block<double>* q : {&V, &AV, &BV, &X, &AX, &BX, &R, &T1, &T2, &Wsrc}) q->allocate(n, cap);
-  const int64_t ld = V.ld;
-  GenBlockOps g{ctx, sm, eig, A, B, 1.0, n, ld, st, DeviceBuffer(64)};
   DeviceBuffer tdiag, act(static_cast<size_t>(cap) * sizeof(int32_t) + 16),
       coef(static_cast<size_t>(cap) * cap * sizeof(double)),
       proj(static_cast<size_t>(cap) * cap * sizeof(double));
@@ -1727,66 +1818,37 @@ void davidson_gen_solve(const Csr& A, const Csr* B, const Options& opt, double* 
     jacobi_inverse_diagonal(A, tdiag.as<double>(), s);
     t = tdiag.as<double>();
   }
-  double* Pm = proj.as<double>();
-  double* Pw = sm.G.as<double>();
   RitzResult ritz;
-  auto extract = [&](int64_t cols) {
-    FE_CHECK_CUDA(cudaMemcpy2DAsync(Pw, cap * 8, Pm, cap * 8, cols * 8, cols,
-                                    cudaMemcpyDeviceToDevice, s));
-    ritz_extract(ctx, sm, eig, Pw, V.data(), AV.data(), ld, n, cols, bw, which, X.data(),
-                 AX.data(), R.data(), coef.as<double>(), g.idx_dev, ritz, BV.data(), BX.data());
-  };
-  fill_initial_block(ctx, X.data(), ld, n, bw, opt.seed_or_default(), opt.init == "host");
-  if (g.ortho(nullptr, nullptr, 0, X.data(), bw, X.data(), BX.data(), T1.data(), T2.data()) < bw)
-    throw Error(FE_ERR_NOT_SPD, "DavidsonSolver: initial block is rank deficient.");
-  g.copy(V.data(), X.data(), bw);
-  g.copy(BV.data(), BX.data(), bw);
-  g.happly(V.data(), AV.data(), bw);
-  gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, bw, bw, Pm, s);
-  extract(bw);
-  const double locktol = std::min(1.0e-5, tol);
   int64_t it_done = 0;
-  for (int64_t iter = 0; iter < opt.maxiter; ++iter) {
-    g.bcholqr(X.data(), BX.data(), bw, T1.data(), T2.data(), "DavidsonSolver: restart");
-    g.copy(V.data(), X.data(), bw);
-    g.copy(BV.data(), BX.data(), bw);
-    g.happly(V.data(), AV.data(), bw);
-    FE_CHECK_CUDA(cudaMemset2DAsync(Pm, cap * 8, 0, cap * 8, cap, s));
-    gram_block<double>(sm, V.data(), ld, AV.data(), ld, n, bw, bw, Pm, s);
-    int64_t cols = bw;
-    extract(cols);
-    for (int64_t blk = 1; blk < opt.maxblks; ++blk) {
-      std::vector<int32_t> active;
-      for (int64_t j = 0; j < bw; ++j)
-        if (ritz.rel[j] > locktol) active.push_back(static_cast<int32_t>(j));
-      const int64_t cc = static_cast<int64_t>(active.size());
-      if (cc == 0 || cols + cc > cap) break;
-      ctx.to_device(act.as<int32_t>(), active.data(), cc);
-      gather_columns<double>(R.data(), ld, act.as<int32_t>(), cc, Wsrc.data(), ld, n, s, t);
-      const int64_t r = g.ortho(V.data(), BV.data(), cols, Wsrc.data(), cc, V.col(cols),
-                                BV.col(cols), T1.data(), T2.data());
-      if (r == 0) break;
-      g.happly(V.col(cols), AV.col(cols), r);
-      // projected[:cols, cols:cols+r] = V^T A W, mirrored; diagonal block W^T A W.
-      gram_block<double>(sm, V.data(), ld, AV.col(cols), ld, n, cols, r, Pm + cols * cap, s);
-      gram_block<double>(sm, V.col(cols), ld, AV.col(cols), ld, n, r, r, Pm + cols * cap + cols,
-                         s);
-      mirror_block(Pm, cap, cols, cols, r, s);
-      cols += r;
-      extract(cols);
+  DavidsonBlocks<double> D;
+  if (mixed) {
+    DavidsonBlocks<float> F;
+    F.allocate(n, cap);
+    {
+      Block<double> X0;
+      X0.allocate(n, bw);
+      fill_initial_block(ctx, X0.data(), X0.ld, n, bw, opt.seed_or_default(), opt.init == "host");
+      convert<double, float>(X0.data(), X0.ld, F.X.data(), F.X.ld, n, bw, s);
+      ctx.sync();
     }
-    it_done = iter + 1;
-    double worst = 0;
-    for (int64_t j = 0; j < nev; ++j) worst = std::max(worst, ritz.rel[j]);
-    if (opt.verbosity >= 2)
-      std::fprintf(stderr, "[fe] davidson-g iter %lld cols %lld worst %.3e\n",
-                   static_cast<long long>(iter + 1), static_cast<long long>(cols), worst);
-    if (!ritz.rel.empty() && worst < tol) break;
+    const double floor32 = std::max(tol, opt.mixed_switch);
+    davidson_gen_phase<float>(ctx, sm, eig, A, B, opt, bw, cap, t, F, ritz, it_done, floor32,
+                              floor32, true, act, coef, proj, st);
+    st.fp32_iterations = static_cast<double>(it_done);
+    D.allocate(n, cap);
+    convert<float, double>(F.X.data(), F.X.ld, D.X.data(), D.X.ld, n, bw, s);
+    ctx.sync();
+  } else {
+    D.allocate(n, cap);
+    fill_initial_block(ctx, D.X.data(), D.X.ld, n, bw, opt.seed_or_default(), opt.init == "host");
   }
+  const int64_t it64 = it_done;
+  davidson_gen_phase<double>(ctx, sm, eig, A, B, opt, bw, cap, t, D, ritz, it_done, tol,
+                             std::min(1.0e-5, tol), false, act, coef, proj, st);
   for (int64_t j = 0; j < nev; ++j) eigenvalues[j] = ritz.values[j];
-  finish_results(ctx, sm, A, B, X.data(), ld, n, nev, eigenvalues, residuals, eigenvectors);
+  finish_results(ctx, sm, A, B, D.X.data(), D.X.ld, n, nev, eigenvalues, residuals, eigenvectors);
   st.iterations = static_cast<double>(it_done);
-  st.fp64_iterations = static_cast<double>(it_done);
+  st.fp64_iterations = static_cast<double>(it_done - it64);
 }
 
 // Solves B x = b on the device by conjugate gradients with the Jacobi
@@ -2418,7 +2480,7 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
       lobpcg_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
     }
   } else if (opt.solver == "davidson") {
-    if (B || opt.precond != "none" || opt.block > opt.nev) {
+    if (B || opt.precond != "none" || opt.block > opt.nev || opt.precision == "mixed") {
       if (B) check_pair(A, *B);
       davidson_gen_solve(A, B, opt, eigenvalues, residual_norms, eigenvectors, st);
     } else {

@@ -81,6 +81,23 @@ def test_lobpcg_generalized_mixed_precision_against_dense(km8, dense_km8, precon
     assert p.stats["fp32_iterations"] > 0 and p.stats["fp64_iterations"] > 0, p.stats
 
 
+@pytest.mark.parametrize("precond", ["none", "jacobi"])
+@pytest.mark.parametrize("which,nev,block", [("sr", 8, 8), ("lr", 7, 12)])
+def test_davidson_generalized_mixed_precision_against_dense(km8, dense_km8, precond, which,
+                                                            nev, block):
+    """Davidson with precision=mixed: FP32 restarts to the FP32 floor, then FP64 to tol;
+    dense generalized eigenvalues, oracle-recomputed residuals <= tol, both phases ran."""
+    from oracle import oracle as O
+    K, Mm = km8
+    p = solve(K, Mm, solver="Davidson", nev=nev, which=which, tol=1e-8, maxiter=800, seed=1,
+              precond=precond, block=block, maxblks=4, precision="mixed")
+    exp = dense_km8[:nev] if which == "sr" else dense_km8[::-1][:nev]
+    np.testing.assert_allclose(p.eigenvalues(), exp, rtol=1e-10, atol=1e-12)
+    final = O.residual_norms(K, Mm, p.eigenvalues(), p.eigenvectors())
+    assert np.all(final <= 1.01e-8), final
+    assert p.stats["fp32_iterations"] > 0 and p.stats["fp64_iterations"] > 0, p.stats
+
+
 def test_lobpcg_standard_mixed_precision_against_dense(wells_small):
     """precision=mixed on a standard problem (routed to the generalized loop with B = I)."""
     from oracle import oracle as O
