@@ -73,3 +73,17 @@ def test_workspace_queries_are_host_only():
     assert fe.lib.fe_gram_workspace_bytes(2097152, 320, 320) > 0
     assert fe.lib.fe_gram_workspace_bytes(0, 3, 3) == 0
     assert fe.lib.fe_residual_workspace_bytes(1000, 17) >= 2 * 17 * 8
+
+
+def test_extension_options_reach_the_option_text():
+    """Extension keys (locking, precision, mixed_switch) are accepted and passed to
+    fe_solve's option text; unknown keys are refused like the reference's set()."""
+    import fasteig_b200 as fe
+    o = fe.fasteig_options(100)
+    for k, v in (("solver", "Chebyshev"), ("locking", "hard"), ("precision", "mixed"),
+                 ("mixed_switch", 1e-6)):
+        assert o.set(k, v), k
+    text = o.to_text()
+    for frag in ("locking=hard", "precision=mixed", "mixed_switch=1e-06"):
+        assert frag in text, (frag, text)
+    assert not o.set("no_such_option", 1)
