@@ -304,6 +304,20 @@ def dist_env():
     return rank, world, local
 
 
+def whole_job(seconds, count, world, device="cuda"):
+    """Whole-job figure of N replicas: the slowest rank's seconds and the sum of the
+    ranks' counts (every rank must call it, in the same order)."""
+    if world <= 1:
+        return float(seconds), int(count)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(seconds)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(count)], device=device, dtype=torch.float64)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(c.item())
+
+
 def config_dict(a, extra=None):
     d = {"workload": "chebyshev_wells_128cube" if a.side == 128 else f"chebyshev_wells_{a.side}cube",
          "n": a.side ** 3, "nnz": a.side ** 3 + 6 * (a.side - 1) * a.side ** 2,
@@ -565,57 +579,54 @@ def main():
     clocks = clocks_sampler_stop(proc, fh, clk_path, local)
     elapsed = start.elapsed_time(end) / 1e3
     converged = sum(int((p.residual_norms() <= a.tol).sum()) for p in results)
-    if world > 1:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        c = torch.tensor([converged], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(c, op=torch.distributed.ReduceOp.SUM)
-        elapsed, converged = float(t.item()), int(c.item())
+    elapsed, converged = whole_job(elapsed, converged, world)
     value = converged / elapsed
     per_solve = [p.stats for p in results]
     lat = sorted(s["seconds"] for s in per_solve)
 
     extra = {}
     peak, peak_kind = measured_peaks()
+    # End to end through the C ABI with host buffers, on every rank: CSR upload
+    # from pinned host arrays, solve, eigenvalues/residuals/eigenvectors back into
+    # pinned host memory, all inside the timed region (the pinned buffers are
+    # allocated before it, as a serving process would keep them). The whole-job
+    # figure is the sum of the ranks' pairs over the slowest rank's time.
+    pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory().numpy()
+    rp_h, ci_h = pin(H.rowptr.astype(np.int32)), pin(H.colind.astype(np.int32))
+    va_h = pin(H.values.astype(np.float64))
+    vec_h = torch.empty((a.nev, H.n), dtype=torch.float64).pin_memory().numpy()
+
+    parts = {}
+
+    def e2e_step():
+        t = time.perf_counter()
+        dA2 = fe.CsrMatrix(H.n, rp_h, ci_h, va_h)
+        t1 = time.perf_counter()
+        parts["csr_upload_s"] = t1 - t
+        p2 = fe.fasteig_problem(dA2, solver="Chebyshev")
+        p2.solve(opts, vectors_out=vec_h)
+        t2 = time.perf_counter()
+        parts["solve_call_s"] = t2 - t1
+        parts["solve_s"] = p2.stats["seconds"]
+        dA2.close()
+        parts["csr_release_s"] = time.perf_counter() - t2
+        return p2
+
+    e2e_step()  # warm-up of the host-buffer path (first touch of pool and pinned memory)
+    barrier()
+    t0 = time.perf_counter()
+    p2 = e2e_step()
+    t_e2e = time.perf_counter() - t0
+    e2e_pairs = int((p2.residual_norms() <= a.tol).sum())
+    t_e2e, e2e_pairs = whole_job(t_e2e, e2e_pairs, world)
+    h2d = world * (rp_h.nbytes + ci_h.nbytes + va_h.nbytes)
+    d2h = world * 8 * a.nev * (H.n + 2)
+    extra["e2e"] = {"value": round(e2e_pairs / t_e2e, 4), "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "seconds": round(t_e2e, 3),
+                    "parts_s": {k: round(v, 3) for k, v in parts.items()}}
+    del p2, vec_h, rp_h, ci_h, va_h
     if rank == 0:
-        # End to end through the C ABI with host buffers: CSR upload from pinned host
-        # arrays, solve, eigenvalues/residuals/eigenvectors back into pinned host
-        # memory, all inside the timed region (the pinned buffers are allocated
-        # before it, as a serving process would keep them).
-        pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory().numpy()
-        rp_h, ci_h = pin(H.rowptr.astype(np.int32)), pin(H.colind.astype(np.int32))
-        va_h = pin(H.values.astype(np.float64))
-        vec_h = torch.empty((a.nev, H.n), dtype=torch.float64).pin_memory().numpy()
-
-        parts = {}
-
-        def e2e_step():
-            t = time.perf_counter()
-            dA2 = fe.CsrMatrix(H.n, rp_h, ci_h, va_h)
-            t1 = time.perf_counter()
-            parts["csr_upload_s"] = t1 - t
-            p2 = fe.fasteig_problem(dA2, solver="Chebyshev")
-            p2.solve(opts, vectors_out=vec_h)
-            t2 = time.perf_counter()
-            parts["solve_call_s"] = t2 - t1
-            parts["solve_s"] = p2.stats["seconds"]
-            dA2.close()
-            parts["csr_release_s"] = time.perf_counter() - t2
-            return p2
-
-        e2e_step()  # warm-up of the host-buffer path (first touch of pool and pinned memory)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        p2 = e2e_step()
-        t_e2e = time.perf_counter() - t0
-        e2e_pairs = int((p2.residual_norms() <= a.tol).sum())
-        h2d = rp_h.nbytes + ci_h.nbytes + va_h.nbytes
-        d2h = 8 * a.nev * (H.n + 2)
-        extra["e2e"] = {"value": round(e2e_pairs / t_e2e, 4), "unit": UNIT,
-                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                        "seconds": round(t_e2e, 3),
-                        "parts_s": {k: round(v, 3) for k, v in parts.items()}}
-        del p2, vec_h, rp_h, ci_h, va_h
         fp64 = None
         if not a.no_fp64:
             # FP64 paths of this build, each warmed up like the mixed path (one
