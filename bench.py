@@ -11,9 +11,10 @@ relative residual <= 1e-8, or maxiter) of the same seeded input, already
 resident in HBM. Under torchrun every rank solves its own replica (the solve
 is one GPU's work; no data-path collective), so `scaling` is "weak" and `value`
 is the total converged pairs of all ranks / the max over ranks of the elapsed
-time. `--impl reference` times the CPU restatement of the reference path (the
-reference's Eigen build is unavailable: Eigen is not installed) on the host
-cores, rank 0 only.
+time. `--impl reference` runs the oracle (the FP64 CPU restatement of the
+reference's Chebyshev loop; the reference's own Eigen build is unavailable:
+Eigen is not installed) on the host cores, rank 0 only, one filter cycle of a
+real solve per step.
 """
 from __future__ import annotations
 
@@ -54,6 +55,9 @@ def args_parse():
                         "whole subspace) or hard (over the active block only)")
     p.add_argument("--mixed-switch", type=float, default=1e-6,
                    help="FP32 locking threshold and FP32 -> FP64 switch of the mixed path")
+    p.add_argument("--tail-degree", type=int, default=0,
+                   help="mixed: filter degree of the FP64 cycles after the switch (0 = --degree)")
+    p.add_argument("--verbosity", type=int, default=0, help="solver log level (2: per cycle)")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison solve")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--kernel", default=None,
@@ -318,19 +322,16 @@ def whole_job(seconds, count, world, device="cuda"):
     return float(t.item()), int(c.item())
 
 
-def config_dict(a, extra=None):
-    d = {"workload": "chebyshev_wells_128cube" if a.side == 128 else f"chebyshev_wells_{a.side}cube",
-         "n": a.side ** 3, "nnz": a.side ** 3 + 6 * (a.side - 1) * a.side ** 2,
-         "matrix": f"3D 7-point Dirichlet Laplacian {a.side}^3 + {a.wells} Gaussian wells (seeded)",
-         "solver": "Chebyshev", "nev": a.nev, "block": a.block, "degree": a.degree,
-         "tol": a.tol, "bounds": "ritz", "amplification_cap": a.amplification,
-         "locking": a.locking, "mixed_switch": a.mixed_switch,
-         "precision": "mixed (FP32 filter/SpMM/rotation, FP64-accumulated Gram, FP64 "
-                      "Cholesky/eig/residual, FP64 final sweeps)",
-         "init": "device", "l2": "blocks (n x 320) >> 126 MB L2; no flush needed"}
-    if extra:
-        d.update(extra)
-    return d
+def config_dict(a):
+    """The workload both arms run (the b200 arm's implementation choices are reported
+    beside it, under "impl_config")."""
+    return {"workload": "chebyshev_wells_128cube" if a.side == 128 else f"chebyshev_wells_{a.side}cube",
+            "n": a.side ** 3, "nnz": a.side ** 3 + 6 * (a.side - 1) * a.side ** 2,
+            "matrix": f"3D 7-point Dirichlet Laplacian {a.side}^3 + {a.wells} Gaussian wells (seeded)",
+            "solver": "Chebyshev", "nev": a.nev, "block": a.block, "degree": a.degree,
+            "tol": a.tol, "bounds": "ritz", "amplification_cap": a.amplification,
+            "locking": a.locking,
+            "l2": "blocks (n x 320) >> 126 MB L2; no flush needed"}
 
 
 def clocks_sampler_start(path):
@@ -408,6 +409,10 @@ def solve_opts(a, precision, seed, locking=None):
                      amplification=a.amplification, precision=precision, init="device",
                      locking=locking or a.locking, mixed_switch=a.mixed_switch).items():
         assert o.set(k, v), k
+    if a.tail_degree > 0 and precision == "mixed":
+        assert o.set("tail_degree", a.tail_degree)
+    if a.verbosity:
+        assert o.set("verbosity", a.verbosity)
     return o
 
 
@@ -445,76 +450,116 @@ def roofline_cheb_step(a, H, dA, peak, launches=20, mode=0):
             "algorithmic_bytes": algo, "ms_per_launch": round(ms, 4)}
 
 
-def cpu_sample(a, H, iterations):
-    """Oracle (FP64 NumPy/SciPy restatement of the reference's CPU path) timed on the
-    host cores on a bounded sample of the same workload: one SpMM on a 32-column
-    slice of the n x 320 block (scaled x10, x17 per cycle: 16 filter steps + the
-    Rayleigh-Ritz apply) and one full-width Gram and rotation (x2 Gram, x3 rotation
-    per cycle), extrapolated to the GPU run's cycle count."""
-    import numpy as np
+def oracle_cycles(a, H, seed=1):
+    """The oracle's FP64 Chebyshev loop on this workload with the b200 arm's options
+    (block, degree, tol, bounds=ritz, amplification cap, locking), one filter cycle
+    per next(); the operator runs on every host core (oracle/cpu.py)."""
+    from oracle import cpu
     from oracle import oracle as O
     A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
-    S = A.scipy()
-    rng = np.random.default_rng(0)
-    Xs = rng.standard_normal((H.n, 32))
+    ops = cpu.ThreadedChebyshevOps(A, 1.0)
+    gen = O.chebyshev_cycles(A, a.nev, degree=a.degree, tol=a.tol, maxiter=a.maxiter, which="sr",
+                             seed=seed, block=a.block, bounds="ritz",
+                             amplification=a.amplification, locking=a.locking, ops=ops)
+    return gen, ops
+
+
+def cpu_sample(a, H, cycles):
+    """cpu_baseline of the b200 line: the oracle's set-up (random block, Cholesky QR,
+    Lanczos bounds) and first filter cycle on this workload, timed on the host cores,
+    extrapolated to `cycles` cycles (the FP64 cycle count of this run's own GPU
+    FP64 solve with the same options)."""
+    import numpy as np  # noqa: F401
+    gen, ops = oracle_cycles(a, H)
     t = time.perf_counter()
-    _ = S @ Xs
-    t_spmm32 = time.perf_counter() - t
-    X = rng.standard_normal((H.n, a.block))
-    t = time.perf_counter()
-    G = X.T @ X
-    t_gram = time.perf_counter() - t
-    C = rng.standard_normal((a.block, a.block))
-    t = time.perf_counter()
-    _ = X @ C
-    t_rot = time.perf_counter() - t
-    t = time.perf_counter()
-    np.linalg.eigh(0.5 * (G + G.T))
-    t_eig = time.perf_counter() - t
-    per_cycle = 17 * t_spmm32 * (a.block / 32) + 2 * t_gram + 3 * t_rot + t_eig
-    total = per_cycle * iterations
-    return {"value": round(a.nev / total, 4), "unit": UNIT, "cores": os.cpu_count(),
+    prog = next(gen)
+    first = time.perf_counter() - t
+    per_solve = first * cycles
+    return {"value": round(a.nev / per_solve, 5), "unit": UNIT, "cores": ops.threads,
             "kind": "port",
-            "sample": (f"oracle FP64: 1 SpMM of {H.n}x32 ({t_spmm32:.2f}s, scipy, 1 thread as the "
-                       f"reference's Eigen SpMM), 1 Gram {H.n}x{a.block} ({t_gram:.2f}s) and 1 "
-                       f"rotation ({t_rot:.2f}s, NumPy BLAS, all cores), eig {a.block} "
-                       f"({t_eig:.3f}s); cycle = 17 SpMM(320) + 2 Gram + 3 rotation + eig = "
-                       f"{per_cycle:.1f}s, x {iterations} cycles (GPU FP64 run) = {total:.0f}s "
-                       f"per solve"),
-            "seconds_per_cycle": round(per_cycle, 3)}
+            "sample": (f"oracle FP64 Chebyshev loop (CPU restatement of src/ChebyshevSolver.cpp:"
+                       f"67-221, same options as this line) on this {H.n}-row matrix: set-up + "
+                       f"first filter cycle ({prog.filtered_cols} columns, degree {a.degree}) "
+                       f"measured at {first:.1f} s on {ops.threads} threads, x {cycles} cycles "
+                       f"(the GPU FP64 same-options solve) = {per_solve:.0f} s per solve "
+                       f"(extrapolated; later cycles filter fewer columns)"),
+            "measured_s": round(first, 3), "cycles_assumed": cycles}
 
 
 def run_reference(a):
+    """Reference arm: the oracle's FP64 Chebyshev solve of this workload on the host
+    cores, one filter cycle per step (the first step also runs the set-up). A solve
+    that ends before the last step is followed by a new solve. value = the
+    converged pairs of the first complete solve / the seconds its cycles took
+    (measured); if no solve completes within the steps, the solve time is
+    extrapolated from the cycles done and the line says so."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
+    import numpy as np
     H = build_matrix(a)
-    # Cycle count of the FP64 path on this workload (measured with the GPU FP64
-    # path, same algorithm); the CPU restatement needs the same number of cycles.
-    iters = int(os.environ.get("FE_CPU_CYCLES", "0")) or REFERENCE_CYCLES
-    vals = []
-    for i in range(a.warmup + a.steps):
-        r = cpu_sample(a, H, iters)
-        if i >= a.warmup:
-            vals.append(r)
-    v = sum(r["value"] for r in vals) / len(vals)
-    ms = a.nev / v * 1e3
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": config_dict(a, {"precision": "fp64 (CPU restatement)",
-                                      "locking": "soft (the reference's)",
-                                      "mixed_switch": None}),
-            "cpu_baseline": {k: vals[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    line["cpu_baseline"]["value"] = v
+    gen, ops = oracle_cycles(a, H)
+    # Warm-up steps: one threaded filter step over an n x block block each (first
+    # touch of the block memory, thread pool start-up); no solve cycles.
+    Xw = np.ones((H.n, a.block))
+    Yw = np.empty_like(Xw)
+    for _ in range(a.warmup):
+        ops.step(Xw, None, Yw, 1.0, 0.0, 0.0)
+    del Xw, Yw
+    steps, first_solve, done_solve = [], [], None
+    solve_idx = 0
+    t_all = time.perf_counter()
+    for _ in range(a.steps):
+        t = time.perf_counter()
+        prog = next(gen)
+        dt = time.perf_counter() - t
+        steps.append(dt)
+        if solve_idx == 0:
+            first_solve.append(dt)
+        if prog.result is not None:
+            if solve_idx == 0:
+                done_solve = prog.result
+            solve_idx += 1
+            gen, _ = oracle_cycles(a, H, seed=1 + solve_idx)
+    elapsed = time.perf_counter() - t_all
+    if done_solve is not None:
+        sec = sum(first_solve)
+        conv = int((done_solve.residual_norms <= a.tol).sum())
+        value = conv / sec
+        how = (f"measured: first solve converged {conv}/{a.nev} pairs in {done_solve.iterations} "
+               f"cycles, {sec:.1f} s")
+        cycles = done_solve.iterations
+    else:
+        done = len(first_solve)
+        cycles = max(done, FP64_CYCLES_SAME_OPTIONS)
+        sec = sum(first_solve) * cycles / done
+        value = a.nev / sec
+        how = (f"extrapolated: {done} of about {cycles} cycles done in {sum(first_solve):.1f} s "
+               f"(cycle count of the GPU FP64 solve with the same options)")
+    line = {"metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(elapsed / a.steps * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference", "config": config_dict(a),
+            "impl_config": {"precision": "fp64 (oracle: CPU restatement of the reference loop)",
+                            "init": "std::mt19937 block (the reference's Executor)",
+                            "threads": ops.threads},
+            "solve_seconds": round(sec, 3), "cycles_per_solve": cycles,
+            "step_seconds": [round(x, 2) for x in steps],
+            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": ops.threads,
+                             "kind": "port",
+                             "sample": (f"oracle FP64 Chebyshev loop on the {H.n}-row matrix, one "
+                                        f"filter cycle of a real solve per step on {ops.threads} "
+                                        f"threads; {how}")},
+            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-# Filter cycles the plain FP64 path needs on the 128^3 well problem (measured on
-# the GPU FP64 run of this same configuration: 14 cycles, seed 1).
-REFERENCE_CYCLES = 14
+# Filter cycles of this repository's plain FP64 GPU solve of the 128^3 well problem
+# with the bench options (hard locking, bounds=ritz): 14 (B200, seed 1). Used only to
+# extrapolate a reference-arm run too short to finish one solve.
+FP64_CYCLES_SAME_OPTIONS = 14
 
 
 def main():
@@ -589,16 +634,17 @@ def main():
     # End to end through the C ABI with host buffers, on every rank: CSR upload
     # from pinned host arrays, solve, eigenvalues/residuals/eigenvectors back into
     # pinned host memory, all inside the timed region (the pinned buffers are
-    # allocated before it, as a serving process would keep them). The whole-job
-    # figure is the sum of the ranks' pairs over the slowest rank's time.
+    # allocated before it, as a serving process would keep them). One untimed
+    # warm-up, then E2E_REPEATS timed repeats: the median is the figure, min/max the
+    # spread. The whole-job figure is the sum of the ranks' pairs over the slowest
+    # rank's time.
     pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory().numpy()
     rp_h, ci_h = pin(H.rowptr.astype(np.int32)), pin(H.colind.astype(np.int32))
     va_h = pin(H.values.astype(np.float64))
     vec_h = torch.empty((a.nev, H.n), dtype=torch.float64).pin_memory().numpy()
 
-    parts = {}
-
     def e2e_step():
+        parts = {}
         t = time.perf_counter()
         dA2 = fe.CsrMatrix(H.n, rp_h, ci_h, va_h)
         t1 = time.perf_counter()
@@ -607,60 +653,77 @@ def main():
         p2.solve(opts, vectors_out=vec_h)
         t2 = time.perf_counter()
         parts["solve_call_s"] = t2 - t1
-        parts["solve_s"] = p2.stats["seconds"]
         dA2.close()
         parts["csr_release_s"] = time.perf_counter() - t2
-        return p2
+        return p2, parts, time.perf_counter() - t
 
     e2e_step()  # warm-up of the host-buffer path (first touch of pool and pinned memory)
-    barrier()
-    t0 = time.perf_counter()
-    p2 = e2e_step()
-    t_e2e = time.perf_counter() - t0
+    runs = []
+    for _ in range(E2E_REPEATS):
+        barrier()
+        runs.append(e2e_step())
+    secs = sorted(r[2] for r in runs)
+    med = secs[len(secs) // 2]
+    p2, parts, _ = min(runs, key=lambda r: abs(r[2] - med))
     e2e_pairs = int((p2.residual_norms() <= a.tol).sum())
-    t_e2e, e2e_pairs = whole_job(t_e2e, e2e_pairs, world)
+    t_e2e, e2e_pairs = whole_job(med, e2e_pairs, world)
     h2d = world * (rp_h.nbytes + ci_h.nbytes + va_h.nbytes)
     d2h = world * 8 * a.nev * (H.n + 2)
     extra["e2e"] = {"value": round(e2e_pairs / t_e2e, 4), "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "seconds": round(t_e2e, 3),
-                    "parts_s": {k: round(v, 3) for k, v in parts.items()}}
-    del p2, vec_h, rp_h, ci_h, va_h
+                    "seconds_median": round(t_e2e, 4), "repeats": E2E_REPEATS,
+                    "seconds_min_max": [round(secs[0], 4), round(secs[-1], 4)],
+                    "parts_s_of_median_run": {k: round(v, 4) for k, v in parts.items()}}
+    mixed_vals = runs[-1][0].eigenvalues().copy()  # the run whose vectors are in vec_h
+    del rp_h, ci_h, va_h
     if rank == 0:
-        fp64 = None
+        fp64 = same = None
         if not a.no_fp64:
             # FP64 paths of this build, each warmed up like the mixed path (one
             # untimed solve), then the mean of two solves: "plain" is the
             # reference's algorithm (soft locking) in FP64; the second uses every
             # option of the mixed run except the precision.
-            def fp64_run(locking):
+            def fp64_run(locking, vectors_out=None):
                 o64 = solve_opts(a, "fp64", seed, locking=locking)
                 solve_once(o64)
-                runs = [solve_once(o64) for _ in range(2)]
-                sec64 = sum(p.stats["seconds"] for p in runs) / len(runs)
-                c64 = int((runs[-1].residual_norms() <= a.tol).sum())
-                return {"value": round(c64 / sec64, 4), "unit": UNIT, "seconds": round(sec64, 3),
-                        "cycles": runs[-1].stats["iterations"], "converged": c64,
-                        "locking": locking}
+                runs64 = [solve_once(o64) for _ in range(2)]
+                sec64 = sum(p.stats["seconds"] for p in runs64) / len(runs64)
+                c64 = int((runs64[-1].residual_norms() <= a.tol).sum())
+                out = {"value": round(c64 / sec64, 4), "unit": UNIT, "seconds": round(sec64, 3),
+                       "cycles": runs64[-1].stats["iterations"], "converged": c64,
+                       "locking": locking}
+                if vectors_out is not None:
+                    pv = fe.fasteig_problem(dA, solver="Chebyshev")
+                    pv.solve(o64, vectors_out=vectors_out)
+                    out["_eigenvalues"] = pv.eigenvalues().copy()
+                return out
             fp64 = fp64_run("soft")
             extra["fp64_plain"] = fp64
             extra["mixed_vs_fp64"] = round((value / world) / fp64["value"], 3) if fp64["value"] else None
             if a.locking != "soft":
-                same = fp64_run(a.locking)
-                extra["fp64_same_options"] = same
+                vec64 = torch.empty((a.nev, H.n), dtype=torch.float64).pin_memory().numpy()
+                same = fp64_run(a.locking, vectors_out=vec64)
+                extra["fp64_same_options"] = {k: v for k, v in same.items() if not k.startswith("_")}
                 extra["mixed_vs_fp64_same_options"] = (
                     round((value / world) / same["value"], 3) if same["value"] else None)
+                extra["accuracy_vs_fp64"] = accuracy_vs_fp64(dA, mixed_vals, vec_h,
+                                                             same["_eigenvalues"], vec64)
+                del vec64
         extra["roofline"] = roofline_cheb_step(a, H, dA, peak, mode=tuned["fp32"])
         extra["roofline"]["peak_kind"] = f"{peak_kind} hbm_gbs (burst copy)"
         if world == 1 and not a.no_cpu:
-            cycles = fp64["cycles"] if fp64 else REFERENCE_CYCLES
+            cycles = (same or fp64 or {}).get("cycles") or FP64_CYCLES_SAME_OPTIONS
             extra["cpu_baseline"] = cpu_sample(a, H, cycles)
+    del vec_h
     line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(elapsed / a.steps * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-            "data": "synthetic", "impl": "b200",
-            "config": config_dict(a, {"parallelism": f"replicas x{world}",
-                                      "spmm_kernel_autotuned": tuned}),
+            "data": "synthetic", "impl": "b200", "config": config_dict(a),
+            "impl_config": {"precision": "mixed (FP32 filter/SpMM/rotation, FP64-accumulated "
+                                         "Gram, FP64 Cholesky/eig/residual, FP64 final sweeps)",
+                            "mixed_switch": a.mixed_switch, "tail_degree": a.tail_degree or a.degree,
+                            "init": "device counter RNG",
+                            "parallelism": f"replicas x{world}", "spmm_kernel_autotuned": tuned},
             "converged_pairs": converged, "latency_s": {"p50": lat[len(lat) // 2], "max": lat[-1]},
             "solve_seconds": [round(s["seconds"], 3) for s in per_solve],
             "phase_ms": [[round(s["filter_ms"]), round(s["ortho_ms"]), round(s["rr_ms"])]
@@ -675,6 +738,45 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+E2E_REPEATS = 5
+
+
+def accuracy_vs_fp64(dA, lam_m, vec_m, lam_f, vec_f):
+    """The mixed result against this build's plain FP64 path (same options, same
+    seed): max relative eigenvalue difference, the largest principal angle between the
+    two nev-dimensional eigenvector subspaces, and the mixed pairs' residuals in both
+    definitions, ||Ax - lx|| / ((1 + |l|) ||x||) (the reference's) and
+    ||Ax - lx|| / (|l| ||x||), recomputed in FP64 from the returned vectors."""
+    import numpy as np
+    import torch
+    from fasteig_b200 import ops
+    lam_m = np.asarray(lam_m)
+    lam_f = np.asarray(lam_f)
+    out = {"eig_rel_err_max": float(np.max(np.abs(lam_m - lam_f) / np.abs(lam_f)))}
+    Xm = torch.from_numpy(vec_m).cuda().T.contiguous()  # n x nev row-major
+    Xf = torch.from_numpy(vec_f).cuda().T.contiguous()
+    qm, _ = torch.linalg.qr(Xm)
+    qf, _ = torch.linalg.qr(Xf)
+    D = qm - qf @ (qf.T @ qm)  # (I - Qf Qf^T) Qm: its 2-norm is sin of the largest angle
+    sin_max = float(torch.linalg.eigvalsh(D.T @ D).max().clamp_min(0.0).sqrt())
+    out["subspace_angle_max_rad"] = float(np.arcsin(min(1.0, sin_max)))
+    del qm, qf, D, Xf
+    AX = torch.empty_like(Xm)
+    ops.spmm(dA, Xm, AX, 1.0, 0.0)
+    lam = torch.from_numpy(lam_m).cuda()
+    rn = torch.linalg.vector_norm(AX - Xm * lam[None, :], dim=0)
+    xn = torch.linalg.vector_norm(Xm, dim=0)
+    ref_def = (rn / ((1.0 + lam.abs()) * xn)).cpu().numpy()
+    base_def = (rn / (lam.abs() * xn)).cpu().numpy()
+    out["residual_ref_def_max"] = float(ref_def.max())
+    out["residual_abs_lambda_def_max"] = float(base_def.max())
+    out["pairs_le_tol_ref_def"] = int((ref_def <= 1e-8).sum())
+    out["pairs_le_tol_abs_lambda_def"] = int((base_def <= 1e-8).sum())
+    del Xm, AX
+    torch.cuda.empty_cache()
+    return out
 
 
 if __name__ == "__main__":

@@ -72,6 +72,7 @@ struct Options {
   bool tensor_cores = true;        // FP32 Grams/rotations on tcgen05 (3xTF32)
   std::string precond = "none";    // none | jacobi (LOBPCG / Davidson corrections W = T R)
   std::string locking = "soft";    // Chebyshev: soft (reference) | hard
+  int64_t tail_degree = 0;         // Chebyshev mixed: filter degree of the FP64 cycles (0 = degree)
 
   void parse(const char* text) {
     if (!text) return;
@@ -139,6 +140,7 @@ struct Options {
     else if (k == "init") init = lower(v);
     else if (k == "mixed_switch") mixed_switch = as_double(v);
     else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
+    else if (k == "tail_degree") tail_degree = as_int(v);
     else if (k == "locking") {
       locking = lower(v);
       if (locking != "soft" && locking != "hard")
@@ -858,13 +860,15 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     // filter amplifies `lower` by 1e3. bounds=ritz (after the first cycle) damps
     // from the largest Ritz value of the last Rayleigh-Ritz instead, lowered if
     // needed so that the amplification at `lower` stays within the cap.
-    double cutoff = reference_cutoff(lower, upper, opt.degree, 1.0e3);
+    const int64_t deg_now = l32 ? opt.degree : (l64 ? l64->degree : opt.degree);
+    double cutoff = reference_cutoff(lower, upper, deg_now, 1.0e3);
     if (opt.bounds == "ritz" && sub_prev > 0) {
       cutoff = std::min(W[sub_prev - 1],
-                        reference_cutoff(lower, upper, opt.degree, opt.amplification));
+                        reference_cutoff(lower, upper, deg_now, opt.amplification));
     }
     if (upper == lower) cutoff = upper;  // collapsed spectrum: no filtering
     int32_t info[3] = {0, 0, 0};
+    const auto t_cycle = clock::now();
     if (l32) {
       l32->iterate(locked, sub, cutoff, W, rel, info, st);
       st.fp32_iterations += 1;
@@ -890,9 +894,12 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     double worst = 0.0;
     for (int64_t j = 0; j < nev; ++j) worst = std::max(worst, rel[j]);
     if (opt.verbosity >= 2) {
-      std::fprintf(stderr, "[fe] iter %lld %s sub %lld locked %lld worst %.3e cutoff %.6g\n",
+      std::fprintf(stderr,
+                   "[fe] iter %lld %s deg %lld sub %lld locked %lld worst %.3e cutoff %.6g "
+                   "%.2f ms\n",
                    static_cast<long long>(iter + 1), l32 ? "fp32" : "fp64",
-                   static_cast<long long>(sub_prev), static_cast<long long>(locked), worst, cutoff);
+                   static_cast<long long>(deg_now), static_cast<long long>(sub_prev),
+                   static_cast<long long>(locked), worst, cutoff, ms_since(t_cycle));
     }
     if (worst <= tol) break;
     worst_history.push_back(worst);
@@ -905,6 +912,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
       const auto t_switch = clock::now();
       // FP32 residual floor reached: continue on FP64 blocks.
       l64.reset(new ChebLoop<double>(ctx, A, opt, sm, eig, sign, lower, upper, false));
+      if (opt.tail_degree > 0) l64->degree = opt.tail_degree;
       l64->b.allocate(n, cap);
       convert<float, double>(l32->b.V.data(), l32->b.V.ld, l64->b.V.data(), l64->b.V.ld, n, cap,
                              ctx.stream);

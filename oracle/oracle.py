@@ -32,6 +32,7 @@ from dataclasses import dataclass, field
 from typing import Optional
 
 import numpy as np
+import scipy.linalg as sla
 import scipy.sparse as sp
 
 EPS = np.finfo(np.float64).eps
@@ -198,7 +199,10 @@ def cholesky_qr(X: np.ndarray, gram: Optional[np.ndarray] = None):
     except np.linalg.LinAlgError:
         return -1, None, None
     R = L.T
-    Q = np.linalg.solve(R.T, X.T).T  # X * R^{-1}
+    # Q = X * R^{-1}, with R^{-1} from the triangular solve against the identity
+    # (src/core/Orthogonalization.cpp:54-55).
+    Rinv = sla.solve_triangular(R, np.eye(R.shape[0]), lower=False, check_finite=False)
+    Q = X @ Rinv
     return 0, Q, R
 
 
@@ -315,8 +319,10 @@ class RitzPairs:
 
 def extract_projected_ritz_pairs(projected: np.ndarray, basis: np.ndarray,
                                  operator_basis: np.ndarray, active: int, requested: int,
-                                 which: str) -> RitzPairs:
-    """extract_projected_ritz_pairs (src/core/RitzExtraction.cpp:65-141)."""
+                                 which: str, norms=None) -> RitzPairs:
+    """extract_projected_ritz_pairs (src/core/RitzExtraction.cpp:65-141). ``norms``
+    (optional) returns (||AXr - Xr diag(vals)||, ||Xr||) per column without forming
+    the residual block, which is then not returned."""
     m = active
     P = projected[:m, :m]
     P = 0.5 * (P + P.T)
@@ -326,9 +332,13 @@ def extract_projected_ritz_pairs(projected: np.ndarray, basis: np.ndarray,
     C = Z[:, idx]
     Xr = basis[:, :m] @ C
     AXr = operator_basis[:, :m] @ C
-    Rs = AXr - Xr * vals[None, :]
-    rn = np.linalg.norm(Rs, axis=0)
-    xn = np.linalg.norm(Xr, axis=0)
+    if norms is not None:
+        Rs = None
+        rn, xn = norms(AXr, Xr, vals)
+    else:
+        Rs = AXr - Xr * vals[None, :]
+        rn = np.linalg.norm(Rs, axis=0)
+        xn = np.linalg.norm(Xr, axis=0)
     den = (1.0 + np.abs(vals)) * xn
     rel = np.where(den > 0.0, rn / np.where(den > 0.0, den, 1.0), rn)
     return RitzPairs(vals, rel, C, Xr, AXr, Rs)
@@ -545,12 +555,57 @@ def chebyshev_filter_window(H_apply, X: np.ndarray, degree: int, cutoff: float,
     return cur
 
 
+class NumpyChebyshevOps:
+    """Operator applications of the Chebyshev loop with SciPy/NumPy (the parity path)."""
+
+    def __init__(self, A: Csr, sign: float):
+        self.Hs = A.scipy()
+        self.sign = sign
+
+    def apply(self, X: np.ndarray) -> np.ndarray:
+        return self.sign * (self.Hs @ X)
+
+    def filter(self, X: np.ndarray, degree: int, lower: float, upper: float) -> np.ndarray:
+        return chebyshev_filter(self.apply, X, degree, lower, upper)
+
+    def filter_window(self, X: np.ndarray, degree: int, cutoff: float, upper: float) -> np.ndarray:
+        return chebyshev_filter_window(self.apply, X, degree, cutoff, upper)
+
+
+@dataclass
+class ChebyshevProgress:
+    """State after one cycle of chebyshev_cycles."""
+    iteration: int = 0
+    locked: int = 0
+    filtered_cols: int = 0
+    worst: float = math.inf
+    converged: bool = False
+    result: Optional[SolveResult] = None
+
+
 def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
                     maxiter: int = 1000, which: str = "sr", seed: int = 1,
                     block: Optional[int] = None, record_history: bool = False,
                     bounds: str = "reference", amplification: float = math.inf,
-                    locking: str = "soft") -> SolveResult:
-    """ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221).
+                    locking: str = "soft", ops=None) -> SolveResult:
+    """ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221); runs
+    chebyshev_cycles to the end and returns its result."""
+    prog = None
+    for prog in chebyshev_cycles(A, nev, degree, tol, maxiter, which, seed, block,
+                                 record_history, bounds, amplification, locking, ops):
+        pass
+    return prog.result
+
+
+def chebyshev_cycles(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
+                     maxiter: int = 1000, which: str = "sr", seed: int = 1,
+                     block: Optional[int] = None, record_history: bool = False,
+                     bounds: str = "reference", amplification: float = math.inf,
+                     locking: str = "soft", ops=None):
+    """ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221), one filter cycle per
+    ``next()``: the first call also runs the set-up (random block, Cholesky QR,
+    Lanczos bounds). Yields a ChebyshevProgress after every cycle; the last one
+    carries the SolveResult.
 
     ``block`` overrides the subspace capacity ``nev + min(nev, n - nev)``
     (src/ChebyshevSolver.cpp:94); None keeps the reference behaviour.
@@ -563,7 +618,9 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
     rechecks the whole prefix after a Rayleigh-Ritz over the whole subspace,
     src/ChebyshevSolver.cpp:160-192): locked pairs are final, and the QR and the
     Rayleigh-Ritz act on the deflated active block only; pairs are returned in
-    ascending order."""
+    ascending order.
+    ``ops`` applies the operator (NumpyChebyshevOps by default; oracle/cpu.py has a
+    threaded host version with the same arithmetic for timing at full size)."""
     n = A.rows
     which = which.lower()
     if n <= 0 or nev <= 0 or nev > n:
@@ -571,20 +628,23 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
     if which not in ("sr", "lr"):
         raise ValueError("ChebyshevSolver: only SR and LR are supported.")
     sign = -1.0 if which == "lr" else 1.0
-    Hs = A.scipy()
-    H_apply = (lambda X: sign * (Hs @ X))
+    if ops is None:
+        ops = NumpyChebyshevOps(A, sign)
+    H_apply = ops.apply
+    norms = getattr(ops, "residual_norms", None)
     capacity = nev + min(nev, n - nev) if block is None else max(nev, min(block, n))
     vectors = random_block(n, capacity, seed)
     info, vectors, _ = cholesky_qr(vectors)
     if info != 0:
         raise RuntimeError("ChebyshevSolver: initial Cholesky QR failed.")
-    lower, upper = estimate_bounds(lambda v: sign * (Hs @ v), n, seed)
+    lower, upper = estimate_bounds(lambda v: H_apply(v), n, seed)
 
     locked = 0
     subspace_cols = nev
     ritz = None
     it_done = 0
     history = []
+    prog = ChebyshevProgress()
     for it in range(maxiter):
         active = subspace_cols - locked
         if bounds == "ritz" and ritz is not None:
@@ -593,21 +653,22 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
             if math.isfinite(amplification):
                 xl = math.cosh(math.acosh(amplification) / degree)
                 cutoff = min(cutoff, (2.0 * lower + upper * (xl - 1.0)) / (1.0 + xl))
-            filtered = chebyshev_filter_window(H_apply, vectors[:, locked:locked + active].copy(),
-                                               degree, cutoff, upper)
+            filtered = ops.filter_window(vectors[:, locked:locked + active].copy(), degree,
+                                         cutoff, upper)
         else:
-            filtered = chebyshev_filter(H_apply, vectors[:, locked:locked + active].copy(),
-                                        degree, lower, upper)
+            filtered = ops.filter(vectors[:, locked:locked + active].copy(), degree, lower, upper)
         if locked > 0:
             _, filtered, _ = block_gram_schmidt(vectors, locked, filtered)
         vectors[:, locked:locked + active] = filtered
+        prog.filtered_cols = active
         if locking == "hard":
             info, basis, _ = cholesky_qr(filtered)
             if info != 0:
                 raise RuntimeError("ChebyshevSolver: Cholesky QR failed during filtering.")
             op_basis = H_apply(basis)
             ritz_a = extract_projected_ritz_pairs(basis.T @ op_basis, basis, op_basis, active,
-                                                  active, "sr")
+                                                  active, "sr", norms)
+            del basis, op_basis
             if ritz is None:
                 vals, rels = np.zeros(capacity), np.zeros(capacity)
             vals[locked:subspace_cols] = ritz_a.values
@@ -616,7 +677,9 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
                     np.all(np.isfinite(ritz_a.relative_residuals))):
                 raise RuntimeError("ChebyshevSolver: non-finite Ritz values or residuals.")
             vectors[:, locked:subspace_cols] = ritz_a.vectors
-            ritz = ritz_a
+            ritz = RitzPairs(ritz_a.values, ritz_a.relative_residuals, ritz_a.coefficients,
+                             None, None, None)
+            del ritz_a
             subspace_cols_prev = subspace_cols
             while locked < nev and rels[locked] <= tol:
                 locked += 1
@@ -624,8 +687,11 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
             it_done = it + 1
             if record_history:
                 history.append((sign * vals[:nev].copy(), rels[:nev].copy()))
+            prog.iteration, prog.locked, prog.worst = it_done, locked, float(rels[:nev].max())
             if rels[:nev].max() <= tol:
+                prog.converged = True
                 break
+            yield prog
             continue
         basis = vectors[:, :subspace_cols].copy()
         info, basis, _ = cholesky_qr(basis)
@@ -634,7 +700,7 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
         op_basis = H_apply(basis)
         projected = basis.T @ op_basis
         ritz = extract_projected_ritz_pairs(projected, basis, op_basis, subspace_cols,
-                                            subspace_cols, "sr")
+                                            subspace_cols, "sr", norms)
         if not (np.all(np.isfinite(ritz.values)) and np.all(np.isfinite(ritz.relative_residuals))):
             raise RuntimeError("ChebyshevSolver: non-finite Ritz values or residuals.")
         vectors[:, :subspace_cols] = ritz.vectors
@@ -646,14 +712,20 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
         it_done = it + 1
         if record_history:
             history.append((sign * ritz.values[:nev].copy(), ritz.relative_residuals[:nev].copy()))
+        prog.iteration, prog.locked = it_done, locked
+        prog.worst = float(ritz.relative_residuals[:nev].max())
         if ritz.relative_residuals[:nev].max() <= tol:
+            prog.converged = True
             break
+        yield prog
     if locking == "hard":
         order = np.argsort(vals[:nev], kind="stable")
-        return SolveResult(sign * vals[:nev][order], vectors[:, :nev][:, order].copy(),
-                           rels[:nev][order].copy(), it_done, 0, history)
-    return SolveResult(sign * ritz.values[:nev], ritz.vectors[:, :nev].copy(),
-                       ritz.relative_residuals[:nev].copy(), it_done, 0, history)
+        prog.result = SolveResult(sign * vals[:nev][order], vectors[:, :nev][:, order].copy(),
+                                  rels[:nev][order].copy(), it_done, 0, history)
+    else:
+        prog.result = SolveResult(sign * ritz.values[:nev], ritz.vectors[:, :nev].copy(),
+                                  ritz.relative_residuals[:nev].copy(), it_done, 0, history)
+    yield prog
 
 
 def lobpcg_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,

@@ -7,7 +7,7 @@ Reads (read-only) the reference's own test inputs and known answers:
 and runs the g++ build of oracle/rng_golden.cpp for std::mt19937 known answers.
 
 Writes tests/golden/{SiO.npz, KuuMuu.npz, spectra.json, mt19937.json}.
-Usage: python tests/golden/make_fixtures.py [/path/to/reference]
+Usage: python tests/golden/make_fixtures.py /path/to/fasteig-checkout
 """
 from __future__ import annotations
 
@@ -21,7 +21,6 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
 
 
 def read_triangle(path: Path):
@@ -45,6 +44,9 @@ def spectrum(path: Path):
 
 
 def main():
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py /path/to/fasteig-checkout")
+    REF = Path(sys.argv[1])
     mats = REF / "examples" / "Sparse_Matrices"
     n, sym, r, c, v = read_triangle(mats / "SiO.mtx")
     np.savez_compressed(HERE / "SiO.npz", n=n, symmetric=sym == "symmetric", row=r, col=c, val=v)
@@ -58,7 +60,7 @@ def main():
                "KuuMuu": {"n": len(kuu), "lowest": kuu[:40], "highest": kuu[-40:]}}
     (HERE / "spectra.json").write_text(json.dumps(spectra, indent=1))
     subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True, capture_output=True)
-    exe = ROOT / "oracle" / "_build" / "rng_golden"
+    exe = ROOT / "oracle" / "_bin" / "rng_golden"
     rng = {}
     for seed in (1, 2, 7, 12345, 4294967295):
         out = subprocess.run([str(exe), str(seed), "64"], check=True, capture_output=True, text=True)
