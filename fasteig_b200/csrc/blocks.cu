@@ -1003,15 +1003,27 @@ __device__ __align__(256) double g_static_gram_scratch[kStaticGramDoubles];
 std::mutex g_static_gram_mutex;
 double* g_static_gram_ptr[kMaxDevices] = {};
 
+// True when p is still device memory of device dev (false after cudaDeviceReset
+// has torn down the context the address came from).
+bool device_address_valid(const void* p, int dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();  // clear the failed query
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
 // Device address of the scratch on the current device. The symbol's name is only
 // a host-side stand-in, so the address is looked up once per device (with that
-// device current) and cached.
+// device current) and cached; a cached address that no longer belongs to the
+// device (its context was reset) is looked up again.
 double* static_gram_scratch() {
   int dev = 0;
   FE_CHECK_CUDA(cudaGetDevice(&dev));
   FE_REQUIRE(dev >= 0 && dev < kMaxDevices, "static Gram scratch: device index out of range");
   std::lock_guard<std::mutex> lock(g_static_gram_mutex);
-  if (!g_static_gram_ptr[dev]) {
+  if (!g_static_gram_ptr[dev] || !device_address_valid(g_static_gram_ptr[dev], dev)) {
     void* p = nullptr;
     FE_CHECK_CUDA(cudaGetSymbolAddress(&p, g_static_gram_scratch));
     g_static_gram_ptr[dev] = static_cast<double*>(p);

@@ -128,7 +128,10 @@ int fe_gram_f32(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_
  * requires k*m <= fe_gram_f64_noalloc_max_entries() (1,048,576) and returns
  * FE_ERR_INVALID otherwise. The first call on a device looks up the array's
  * device address with that device current; make that first call before any
- * stream capture. All calls share the one array (each call overwrites the
+ * stream capture. The address belongs to the device's primary context (the one
+ * the CUDA runtime uses); it is looked up again after cudaDeviceReset, and a
+ * caller that makes a different context current through the driver API must not
+ * call this entry point. All calls share the one array (each call overwrites the
  * part it uses, nothing needs clearing): calls that can overlap on the GPU —
  * on different streams, or from different host threads — race and must be
  * serialized by the caller. */
@@ -193,6 +196,28 @@ int fe_set_f64_gemm_kernel(int32_t mode);
  * TMEM accumulators), 1 = one CTA per tile. Same arithmetic; unaligned outputs
  * always use the one-CTA-per-tile kernel with its staged epilogue. */
 int fe_set_tc_rotate_kernel(int32_t mode);
+
+/* ---------------------------------------------------------------------
+ * One Lanczos step on the device (replaces KrylovSubspace::build_one,
+ * src/core/KrylovSubspace.cpp:125-131, for a standard problem: its
+ * normalize_residual_into_basis, apply_operator_to_basis_column, two-pass
+ * orthogonalize_operator_result and residual_norm, and the T entries that
+ * CudaLanczosKernels.cu:11-22 records):
+ *     beta = *fnorm;  V[:, j] = f / beta;  w = A V[:, j];
+ *     h = V_j^T w, w -= V_j h;  h2 = V_j^T w, w -= V_j h2  (V_j = V[:, 0..j]);
+ *     T[j, j] = h[j] + h2[j];  T[j, j-1] = T[j-1, j] = beta (j > 0);
+ *     f = w;  *fnorm = ||f||.
+ * V is an n-by-m row-major device block (ldv >= m), f an n-vector, fnorm one
+ * device double (||f|| on entry, the new ||f|| on exit), T m-by-m FP64
+ * column-major (ldt >= m). All scalars stay on the device, so steps can be
+ * queued (or graph-captured) back to back. A breakdown (*fnorm == 0) is the
+ * caller's to handle (the reference restarts with a random vector,
+ * normalize_or_restart). Workspace from fe_lanczos_workspace_bytes(n, m).
+ * ------------------------------------------------------------------- */
+size_t fe_lanczos_workspace_bytes(int64_t n, int64_t m);
+int fe_lanczos_step(fe_csr_t A, double* V, int64_t ldv, int64_t m, int64_t j, double* f,
+                    double* fnorm, double* T, int64_t ldt, void* workspace,
+                    size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------
  * Ritz residuals and column norms (replaces the copy + add_scaled_columns +

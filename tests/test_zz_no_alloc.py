@@ -56,6 +56,23 @@ def test_noalloc_gram_matches_allocating_gram_twice(n, k, m):
         assert np.all(np.abs(G0 - G1) <= 1e-13 * scale), call
 
 
+def test_noalloc_gram_at_its_exact_capacity():
+    """k * m equal to the scratch size: one row chunk fills the whole array, where the
+    allocating Gram splits the same rows over several chunks."""
+    import fasteig_b200 as fe
+    assert fe.lib.fe_gram_f64_noalloc_max_entries() == 1024 * 1024
+    g = torch.Generator().manual_seed(11)
+    n = 60000
+    for call in range(2):
+        X = torch.randn(n, 1024, generator=g, dtype=torch.float64).cuda()
+        Y = X if call == 0 else torch.randn(n, 1024, generator=g, dtype=torch.float64).cuda()
+        G0 = _gram_noalloc(X, Y).cpu().numpy()
+        G1 = _gram_allocating(X, Y).cpu().numpy()
+        torch.cuda.synchronize()
+        scale = np.abs(X.cpu().numpy()).T @ np.abs(Y.cpu().numpy())
+        assert np.all(np.abs(G0 - G1) <= 1e-13 * scale), call
+
+
 def test_noalloc_gram_rejects_sizes_beyond_its_scratch():
     import fasteig_b200 as fe
     cap = fe.lib.fe_gram_f64_noalloc_max_entries()
