@@ -28,6 +28,8 @@ _SIGS = {
     "fe_launch_count": (C.c_int64, []),
     "fe_csr_create": (C.c_int, [i64, i64, i64, vp, vp, vp, C.POINTER(vp)]),
     "fe_csr_destroy": (C.c_int, [vp]),
+    "fe_csr_create_from_triplets": (C.c_int, [i64, i64, vp, vp, vp, i32, C.POINTER(vp)]),
+    "fe_csr_create_from_matrix_market": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
     "fe_csr_info": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]),
     "fe_csr_copy_to_host": (C.c_int, [vp, vp, vp, vp]),
     "fe_spmm_csr_f64": (C.c_int, [vp, vp, i64, vp, i64, i64, f64, f64, vp]),

@@ -112,6 +112,51 @@ class CsrMatrix:
         return int(z.value)
 
     @classmethod
+    def _from_handle(cls, h) -> "CsrMatrix":
+        obj = cls.__new__(cls)
+        obj.handle = h
+        obj.rowptr = obj.colind = obj.values = None
+        r, c = C.c_int64(), C.c_int64()
+        check(lib.fe_csr_info(h, C.byref(r), C.byref(c), None))
+        obj.rows, obj.cols = int(r.value), int(c.value)
+        return obj
+
+    @classmethod
+    def from_triplets(cls, n: int, rows, cols, values, expand: str = "none") -> "CsrMatrix":
+        """Device CSR built on the GPU from 0-based triplets (``fe_csr_create_from_triplets``):
+        duplicates summed in input order, ``expand`` = "none", "symmetric" (one triangle
+        given) or "skew", as fasteig_problem::build_sparse_matrix_from_triplets followed by
+        build_csr_from_sparse_matrix (src/fasteig_problem.cpp:474-607)."""
+        codes = {"none": 0, "symmetric": 1, "skew": 2}
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        c = np.ascontiguousarray(cols, dtype=np.int32)
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        if not (r.size == c.size == v.size):
+            raise ValueError("Triplet arrays inconsistent with nnz.")
+        h = C.c_void_p()
+        check(lib.fe_csr_create_from_triplets(int(n), int(v.size), r.ctypes.data, c.ctypes.data,
+                                              v.ctypes.data, codes[expand], C.byref(h)))
+        return cls._from_handle(h)
+
+    @classmethod
+    def from_matrix_market(cls, path) -> "CsrMatrix":
+        """MatrixMarket coordinate file read on the host and built on the GPU
+        (``fe_csr_create_from_matrix_market``; symmetric files expand their triangle)."""
+        h = C.c_void_p()
+        check(lib.fe_csr_create_from_matrix_market(str(path).encode(), C.byref(h)))
+        return cls._from_handle(h)
+
+    def to_host(self):
+        """(rowptr, colind, values) of the stored matrix (CsrMatrix::copy_to_host)."""
+        z = C.c_int64()
+        check(lib.fe_csr_info(self.handle, None, None, C.byref(z)))
+        rp = np.zeros(self.rows + 1, dtype=np.int32)
+        ci = np.zeros(max(int(z.value), 1), dtype=np.int32)
+        va = np.zeros(max(int(z.value), 1), dtype=np.float64)
+        check(lib.fe_csr_copy_to_host(self.handle, rp.ctypes.data, ci.ctypes.data, va.ctypes.data))
+        return rp, ci[:int(z.value)], va[:int(z.value)]
+
+    @classmethod
     def block_diag(cls, parts) -> "CsrMatrix":
         """Block-diagonal operator of device CSR parts (``fe_csr_block_diag``): an SpMM
         on it is the grouped SpMM of all parts."""

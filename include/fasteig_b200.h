@@ -64,6 +64,26 @@ int fe_csr_info(fe_csr_t csr, int64_t* rows, int64_t* cols, int64_t* nnz);
  * include/core/CsrMatrix.hpp:35). Arrays must hold rows+1 / nnz / nnz items. */
 int fe_csr_copy_to_host(fe_csr_t csr, int32_t* rowptr, int32_t* colind, double* values);
 
+/* CSR built on the device from triplets (replaces the host Eigen path
+ * fasteig_problem::build_sparse_matrix_from_triplets, src/fasteig_problem.cpp:474-506,
+ * followed by build_csr_from_sparse_matrix, :554-607). rows/cols/values are `count`
+ * 0-based host triplets of an n-by-n matrix; duplicates are summed left to right in
+ * input order (Eigen's setFromTriplets); expand = 0 keeps the matrix as given,
+ * 1 adds the mirror (c, r, v) of every off-diagonal entry (a symmetric matrix
+ * stored as one triangle), 2 adds (c, r, -v) (skew); positions that then hold two
+ * values keep their sum. Rows come out sorted by column, explicit zeros are kept,
+ * and the result is bit-identical to the reference's. Index errors give the
+ * reference's messages ("Triplet index out of bounds.", "Invalid matrix
+ * dimension n <= 0."). */
+int fe_csr_create_from_triplets(int64_t n, int64_t count, const int32_t* rows,
+                                const int32_t* cols, const double* values, int32_t expand,
+                                fe_csr_t* out);
+/* MatrixMarket coordinate file (real, integer or pattern; general, symmetric or
+ * skew-symmetric; 1-based entries, as src/mmio.cpp reads them) parsed on the host
+ * into triplets and built on the device as fe_csr_create_from_triplets does
+ * (symmetric files expand their stored triangle). */
+int fe_csr_create_from_matrix_market(const char* path, fe_csr_t* out);
+
 /* ---------------------------------------------------------------------
  * Block SpMM (replaces LinearOperator::apply_block of a CSR matrix,
  * include/core/LinearOperator.hpp:32-37; GPU: CudaCsrMatrix::apply_block,

@@ -113,27 +113,50 @@ def validate_csr(A: Csr) -> None:
         raise ValueError("CsrMatrixData: column index out of range.")
 
 
-def csr_from_triplets(n: int, rows, cols, vals, expand_symmetric: bool) -> Csr:
-    """Symmetric expansion and duplicate summation of a triangle.
+def csr_from_triplets(n: int, rows, cols, vals, expand_symmetric: bool,
+                      expand_skew: bool = False) -> Csr:
+    """Duplicate summation and symmetric expansion of triplets.
 
-    fasteig_problem::build_sparse_matrix_from_triplets (src/fasteig_problem.cpp:474-506)
-    and build_csr_from_sparse_matrix (src/fasteig_problem.cpp:554-607): every
-    off-diagonal (r,c,v) also contributes (c,r,v); duplicates are summed; rows
-    are sorted by column (Eigen row-major compressed storage).
+    fasteig_problem::build_sparse_matrix_from_triplets (src/fasteig_problem.cpp:474-506):
+    Eigen's setFromTriplets sums duplicates left to right in input order. Then
+    build_csr_from_sparse_matrix (src/fasteig_problem.cpp:554-607): every stored
+    off-diagonal (r,c,v) of the merged matrix also contributes (c,r,v) (or -v when
+    ``expand_skew``), positions holding two values keep their sum, rows are sorted by
+    column (Eigen row-major compressed storage), explicit zeros are kept.
     """
     rows = np.asarray(rows, dtype=np.int64)
     cols = np.asarray(cols, dtype=np.int64)
     vals = np.asarray(vals, dtype=np.float64)
-    if expand_symmetric:
-        off = rows != cols
-        rows, cols, vals = (np.concatenate([rows, cols[off]]),
-                            np.concatenate([cols, rows[off]]),
-                            np.concatenate([vals, vals[off]]))
-    m = sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
-    m.sum_duplicates()
-    m.sort_indices()
-    return Csr(n, n, m.indptr.astype(np.int32), m.indices.astype(np.int32),
-               m.data.astype(np.float64))
+    if n <= 0:
+        raise ValueError("Invalid matrix dimension n <= 0.")
+    if rows.size and (rows.min() < 0 or cols.min() < 0 or rows.max() >= n or cols.max() >= n):
+        raise ValueError("Triplet index out of bounds.")
+
+    def merge(r, c, v):
+        key = r * n + c
+        order = np.argsort(key, kind="stable")  # equal keys stay in input order
+        key, v = key[order], v[order]
+        if key.size == 0:
+            return key // n, key % n, v
+        starts = np.flatnonzero(np.r_[True, key[1:] != key[:-1]])
+        lengths = np.diff(np.r_[starts, key.size])
+        acc = v[starts].copy()
+        for t in range(1, int(lengths.max())):  # left-to-right sums (collapseDuplicates)
+            more = lengths > t
+            acc[more] = acc[more] + v[starts[more] + t]
+        uk = key[starts]
+        return uk // n, uk % n, acc
+
+    r1, c1, v1 = merge(rows, cols, vals)
+    if expand_symmetric or expand_skew:
+        off = r1 != c1
+        sign = -1.0 if expand_skew else 1.0
+        r1, c1, v1 = merge(np.concatenate([r1, c1[off]]), np.concatenate([c1, r1[off]]),
+                           np.concatenate([v1, sign * v1[off]]))
+    rowptr = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(rowptr, r1 + 1, 1)
+    rowptr = np.cumsum(rowptr)
+    return Csr(n, n, rowptr.astype(np.int32), c1.astype(np.int32), v1.astype(np.float64))
 
 
 def read_mtx(path) -> Csr:
