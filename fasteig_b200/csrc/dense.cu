@@ -31,6 +31,32 @@ std::atomic<int64_t> g_launches{0};
 }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+namespace {
+thread_local int* tl_status_word = nullptr;
+}
+int* current_status_word() { return tl_status_word; }
+void set_status_word(int* word) { tl_status_word = word; }
+
+int* thread_status_word() {
+  constexpr int kDevices = 64;
+  thread_local int* words[kDevices] = {};
+  int dev = 0;
+  FE_CHECK_CUDA(cudaGetDevice(&dev));
+  FE_REQUIRE(dev >= 0 && dev < kDevices, "device index out of range");
+  int*& w = words[dev];
+  if (w) {
+    // Still this device's memory? (not after cudaDeviceReset)
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, w) != cudaSuccess || a.type != cudaMemoryTypeDevice ||
+        a.device != dev) {
+      (void)cudaGetLastError();
+      w = nullptr;
+    }
+  }
+  if (!w) FE_CHECK_CUDA(cudaMalloc(&w, sizeof(int)));
+  return w;
+}
+
 cudaStream_t& alloc_stream() {
   thread_local cudaStream_t s = nullptr;
   return s;

@@ -110,6 +110,23 @@ struct Csr {
 
 int num_sms();
 
+// Device status word that kernels launched from this host thread record a
+// timed-out bounded wait in: the one a solve installed for its duration
+// (StatusScope), or null for the library's default word (fe_device_status).
+int* current_status_word();
+void set_status_word(int* word);
+struct StatusScope {
+  int* prev;
+  explicit StatusScope(int* word) : prev(current_status_word()) { set_status_word(word); }
+  ~StatusScope() { set_status_word(prev); }
+  StatusScope(const StatusScope&) = delete;
+  StatusScope& operator=(const StatusScope&) = delete;
+};
+void launch_wait_probe(int* status, long long limit_cycles, int code, cudaStream_t s);
+// A status word owned by the calling host thread on the current device (allocated
+// on first use and kept; solves on one thread run one at a time).
+int* thread_status_word();
+
 // FP64 tensor-core kernels (dmma.cu).
 void gram_partial_dmma(const double* X, int64_t ldx, const double* Y, int64_t ldy, int64_t n,
                        int k, int m, int tiles_k, int tiles_m, int chunks, int64_t rows_per_chunk,

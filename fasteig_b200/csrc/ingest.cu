@@ -27,8 +27,6 @@
 
 namespace fe {
 
-void count_launch();
-
 namespace {
 
 constexpr int kThreads = 256;
@@ -122,14 +120,12 @@ void exclusive_scan(const T* in, int64_t n, int64_t* out, cudaStream_t s) {
   const int64_t items = n + 1;  // item n reads as zero
   const int64_t blocks = (items + 1023) / 1024;
   Tmp<int64_t> sums(blocks);
-  count_launch();
   scan_block_kernel<T><<<static_cast<unsigned>(blocks), 1024, 0, s>>>(in, n, items, out, sums.p);
   check_launch("scan_block_kernel");
   if (blocks > 1) {
     Tmp<int64_t> offs(blocks + 1);
     exclusive_scan<int64_t>(sums.p, blocks, offs.p, s);
-    count_launch();
-    scan_add_kernel<<<static_cast<unsigned>(blocks), 1024, 0, s>>>(out, items, offs.p);
+      scan_add_kernel<<<static_cast<unsigned>(blocks), 1024, 0, s>>>(out, items, offs.p);
     check_launch("scan_add_kernel");
     FE_CHECK_CUDA(cudaStreamSynchronize(s));  // before `offs` is freed
   }
@@ -311,7 +307,6 @@ Csr* csr_from_triplets(int64_t n, int64_t count, const int32_t* rows, const int3
   FE_CHECK_CUDA(cudaMemsetAsync(cnt.p, 0, n * sizeof(int32_t), s));
   FE_CHECK_CUDA(cudaMemsetAsync(fill.p, 0, n * sizeof(int32_t), s));
   FE_CHECK_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int32_t), s));
-  count_launch();
   check_and_count_kernel<<<grid_for(count), kThreads, 0, s>>>(n, count, r.p, c.p, cnt.p, bad.p);
   check_launch("check_and_count_kernel");
   int32_t bad_h = 0;
@@ -324,11 +319,9 @@ Csr* csr_from_triplets(int64_t n, int64_t count, const int32_t* rows, const int3
   Tmp<int32_t> bcol(count), mcnt(n);
   Tmp<int64_t> bidx(count);
   Tmp<double> mval(count);
-  count_launch();
   scatter_kernel<<<grid_for(count), kThreads, 0, s>>>(count, r.p, c.p, start.p, fill.p, bcol.p,
                                                       bidx.p);
   check_launch("scatter_kernel");
-  count_launch();
   sort_merge_kernel<<<grid_for(n), kThreads, 0, s>>>(n, start.p, bcol.p, bidx.p, v.p, mval.p,
                                                      mcnt.p);
   check_launch("sort_merge_kernel");
@@ -347,21 +340,17 @@ Csr* csr_from_triplets(int64_t n, int64_t count, const int32_t* rows, const int3
   if (expand) {
     FE_CHECK_CUDA(cudaMemsetAsync(ecnt.p, 0, n * sizeof(int32_t), s));
     FE_CHECK_CUDA(cudaMemsetAsync(efill.p, 0, n * sizeof(int32_t), s));
-    count_launch();
-    mirror_count_kernel<<<grid_for(n), kThreads, 0, s>>>(n, start.p, mcnt.p, bcol.p, ecnt.p);
+      mirror_count_kernel<<<grid_for(n), kThreads, 0, s>>>(n, start.p, mcnt.p, bcol.p, ecnt.p);
     check_launch("mirror_count_kernel");
-    count_launch();
-    add_counts_kernel<<<grid_for(n), kThreads, 0, s>>>(n, mcnt.p, ecnt.p);
+      add_counts_kernel<<<grid_for(n), kThreads, 0, s>>>(n, mcnt.p, ecnt.p);
     check_launch("add_counts_kernel");
     exclusive_scan(ecnt.p, n, fstart.p, s);
-    count_launch();
-    expand_scatter_kernel<<<grid_for(n), kThreads, 0, s>>>(n, start.p, mcnt.p, bcol.p, mval.p,
+      expand_scatter_kernel<<<grid_for(n), kThreads, 0, s>>>(n, start.p, mcnt.p, bcol.p, mval.p,
                                                            fstart.p, efill.p,
                                                            expand == 2 ? -1.0 : 1.0, fcol.p,
                                                            fval.p);
     check_launch("expand_scatter_kernel");
-    count_launch();
-    expand_merge_kernel<<<grid_for(n), kThreads, 0, s>>>(n, fstart.p, fcol.p, fval.p, fcnt.p);
+      expand_merge_kernel<<<grid_for(n), kThreads, 0, s>>>(n, fstart.p, fcol.p, fval.p, fcnt.p);
     check_launch("expand_merge_kernel");
     fin_cnt = fcnt.p;
     fin_start = fstart.p;
@@ -384,18 +373,15 @@ Csr* csr_from_triplets(int64_t n, int64_t count, const int32_t* rows, const int3
     FE_CHECK_CUDA(cudaMalloc(&A->colind, std::max<int64_t>(nnz, 1) * sizeof(int32_t)));
     FE_CHECK_CUDA(cudaMalloc(&A->val64, std::max<int64_t>(nnz, 1) * sizeof(double)));
     FE_CHECK_CUDA(cudaMalloc(&A->val32, std::max<int64_t>(nnz, 1) * sizeof(float)));
-    count_launch();
-    compact_kernel<<<grid_for(n), kThreads, 0, s>>>(n, fin_start, fin_cnt, rp64.p, fin_col,
+      compact_kernel<<<grid_for(n), kThreads, 0, s>>>(n, fin_start, fin_cnt, rp64.p, fin_col,
                                                     fin_val, A->colind, A->val64);
     check_launch("compact_kernel");
-    count_launch();
-    narrow_kernel<<<grid_for(n + 1), kThreads, 0, s>>>(rp64.p, n + 1, A->rowptr);
+      narrow_kernel<<<grid_for(n + 1), kThreads, 0, s>>>(rp64.p, n + 1, A->rowptr);
     check_launch("narrow_kernel");
     if (nnz > 0) convert<double, float>(A->val64, 1, A->val32, 1, nnz, 1, s);
     Tmp<int> mx(1);
     FE_CHECK_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
-    count_launch();
-    row_max_kernel<<<grid_for(n), kThreads, 0, s>>>(n, rp64.p, mx.p);
+      row_max_kernel<<<grid_for(n), kThreads, 0, s>>>(n, rp64.p, mx.p);
     check_launch("row_max_kernel");
     int mx_h = 0;
     FE_CHECK_CUDA(cudaMemcpyAsync(&mx_h, mx.p, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -73,6 +73,7 @@ struct Options {
   std::string precond = "none";    // none | jacobi (LOBPCG / Davidson corrections W = T R)
   std::string locking = "soft";    // Chebyshev: soft (reference) | hard
   int64_t tail_degree = 0;         // Chebyshev mixed: filter degree of the FP64 cycles (0 = degree)
+  int64_t inject_wait_timeout = 0;  // test hook: status code of a forced bounded-wait timeout
 
   void parse(const char* text) {
     if (!text) return;
@@ -141,6 +142,7 @@ struct Options {
     else if (k == "mixed_switch") mixed_switch = as_double(v);
     else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
     else if (k == "tail_degree") tail_degree = as_int(v);
+    else if (k == "inject_wait_timeout") inject_wait_timeout = as_int(v);
     else if (k == "locking") {
       locking = lower(v);
       if (locking != "soft" && locking != "hard")
@@ -2475,6 +2477,20 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
   Stats st;
   const auto t0 = std::chrono::steady_clock::now();
   FE_CHECK_CUDA(cudaSetDevice(A.device));
+  // This solve's own device status word: a bounded wait that runs out in one of its
+  // kernels is reported here, to this solve, and not to whichever solve reads the
+  // library's default word next.
+  int32_t* status_word = thread_status_word();
+  FE_CHECK_CUDA(cudaMemset(status_word, 0, sizeof(int32_t)));
+  StatusScope status_scope(status_word);
+  if (opt.inject_wait_timeout != 0) {
+    // Test hook: a probe kernel whose bounded wait runs out (about a millisecond of
+    // SM clock on an mbarrier nothing arrives on) records the code in this solve's
+    // word, as a real timeout in a solve kernel would.
+    launch_wait_probe(status_word, 2000000LL, static_cast<int>(opt.inject_wait_timeout),
+                      nullptr);
+    FE_CHECK_CUDA(cudaStreamSynchronize(nullptr));
+  }
   if (opt.solver == "chebyshev") {
     FE_REQUIRE(B == nullptr, "ChebyshevSolver: generalized problems are not supported.");
     chebyshev_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
@@ -2500,6 +2516,11 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
   } else {
     throw Error(FE_ERR_UNSUPPORTED, "solver not available on this backend: " + opt.solver);
   }
+  int32_t word = 0;
+  FE_CHECK_CUDA(cudaMemcpy(&word, status_word, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (word != 0)
+    throw Error(FE_ERR_CUDA, "device wait timed out in a solve kernel (status code " +
+                                 std::to_string(word) + "); results discarded");
   const auto t1 = std::chrono::steady_clock::now();
   st.seconds = std::chrono::duration<double>(t1 - t0).count();
   if (opt.verbosity >= 2)

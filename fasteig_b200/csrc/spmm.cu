@@ -534,14 +534,14 @@ __device__ __forceinline__ bool pipe_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait (about two seconds of SM clock); records `code` on timeout.
-__device__ __forceinline__ bool pipe_wait(uint64_t* bar, uint32_t parity, int code) {
+__device__ __forceinline__ bool pipe_wait(uint64_t* bar, uint32_t parity, int code, int* status) {
   if (pipe_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (true) {
     for (int i = 0; i < 64; ++i)
       if (pipe_try_wait(bar, parity)) return true;
     if (clock64() - t0 > 4000000000LL) {
-      atomicCAS(&g_spmm_status, 0, code);
+      atomicCAS(status ? status : &g_spmm_status, 0, code);
       return false;
     }
   }
@@ -590,7 +590,7 @@ csr_spmm_pipe_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
                      const int32_t* __restrict__ colind, const T* __restrict__ vals,
                      const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
                      int64_t ldz, int ncols, int panel_cols, int slots, T alpha, T gamma, T beta,
-                     int use_gamma, int use_beta) {
+                     int use_gamma, int use_beta, int* status) {
   extern __shared__ __align__(128) uint8_t pipe_smem[];
   const PipeLayout<T> L = pipe_layout<T>(pipe_smem);
   const int warp = threadIdx.x / 32;
@@ -657,7 +657,7 @@ csr_spmm_pipe_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
     if (r >= nrows) break;
     const int s = static_cast<int>(i % kPipeDepth);
     const uint32_t parity = static_cast<uint32_t>((i / kPipeDepth) & 1);
-    if (!pipe_wait(&bars[s], parity, 11)) {
+    if (!pipe_wait(&bars[s], parity, 11, status)) {
       ok = false;
       break;
     }
@@ -745,7 +745,7 @@ csr_spmm_pipe_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
   }
   if (!ok) {
     // Let copies already issued for this warp land before the CTA exits.
-    for (int s = 0; s < kPipeDepth; ++s) pipe_wait(&bars[s], 0, 12);
+    for (int s = 0; s < kPipeDepth; ++s) pipe_wait(&bars[s], 0, 12, status);
   }
 }
 
@@ -779,7 +779,7 @@ bool try_pipe(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, int64_
     }                                                                                          \
     kern<<<grid, kPipeWarps * 32, smem, s>>>(A.rows, A.rowptr, A.colind, vals, X, ldx, Y, ldy, \
                                              Z, ldz, ncols, panel, slots, alpha, gamma, beta,  \
-                                             ug ? 1 : 0, ub ? 1 : 0);                          \
+                                             ug ? 1 : 0, ub ? 1 : 0, current_status_word());  \
     check_launch("csr_spmm_pipe_kernel");                                                      \
   } while (0)
   switch (cpl) {

@@ -96,18 +96,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: about two seconds of SM clock, then record `code` and give up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int code) {
+// Bounded wait: `limit` SM clocks (about two seconds by default), then record `code`
+// in the launch's status word and give up.
+__device__ __forceinline__ bool mbar_wait_limit(uint64_t* bar, uint32_t parity, int code,
+                                                int* status, long long limit) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (true) {
     for (int i = 0; i < 64; ++i)
       if (mbar_try_wait(bar, parity)) return true;
-    if (clock64() - t0 > 4000000000LL) {
-      atomicCAS(&g_tc_status, 0, code);
+    if (clock64() - t0 > limit) {
+      atomicCAS(status, 0, code);
       return false;
     }
   }
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int code, int* status) {
+  return mbar_wait_limit(bar, parity, code, status, 4000000000LL);
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
@@ -244,6 +250,7 @@ struct Smem {
   uint64_t* split;
   uint64_t* accum;
   uint32_t* tmem_slot;
+  int* status;  // the launch's status word (a solve's own, or the library default)
   __device__ float* a_hi(int s) const { return reinterpret_cast<float*>(base + s * kStageBytes); }
   __device__ float* a_lo(int s) const {
     return reinterpret_cast<float*>(base + s * kStageBytes + kABytes);
@@ -256,8 +263,9 @@ struct Smem {
   }
 };
 
-__device__ __forceinline__ Smem carve(uint8_t* dyn) {
+__device__ __forceinline__ Smem carve(uint8_t* dyn, int* status) {
   Smem s;
+  s.status = status ? status : &g_tc_status;
   uintptr_t p = reinterpret_cast<uintptr_t>(dyn);
   p = (p + 1023) & ~uintptr_t(1023);
   s.base = reinterpret_cast<uint8_t*>(p);
@@ -321,7 +329,7 @@ __device__ void mma_loop(const Smem& sm, uint32_t tmem, int nkb, uint32_t idesc)
   for (int kb = 0; kb < nkb; ++kb) {
     const int s = kb % kStages;
     const uint32_t ph = (kb / kStages) & 1u;
-    if (!mbar_wait(&sm.split[s], ph, 3)) return;
+    if (!mbar_wait(&sm.split[s], ph, 3, sm.status)) return;
     tc_fence_after();
     const uint32_t ah = smem_u32(sm.a_hi(s)), al = smem_u32(sm.a_lo(s));
     const uint32_t bh = smem_u32(sm.b_hi(s)), bl = smem_u32(sm.b_lo(s));
@@ -351,9 +359,9 @@ __device__ void mma_loop(const Smem& sm, uint32_t tmem, int nkb, uint32_t idesc)
 __global__ void __launch_bounds__(kGramThreads, 1)
 gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmY,
                int64_t n, int k, int m, int sx, int sy, int k_tiles, int64_t rows_per_chunk,
-               float* __restrict__ partial, int symmetric) {
+               float* __restrict__ partial, int symmetric, int* status) {
   extern __shared__ uint8_t dyn_smem[];
-  const Smem sm = carve(dyn_smem);
+  const Smem sm = carve(dyn_smem, status);
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   const int ti = blockIdx.x % k_tiles;
@@ -373,7 +381,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % kStages;
       const uint32_t ph = (kb / kStages) & 1u;
-      if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1)) break;
+      if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1, sm.status)) break;
       mbar_expect_tx(&sm.full[s], kABytes + kBBytes);
       const int y = static_cast<int>(r_begin + static_cast<int64_t>(kb) * kKB);
 #pragma unroll
@@ -393,7 +401,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % kStages;
       const uint32_t ph = (kb / kStages) & 1u;
-      if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2))) break;
+      if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2, sm.status))) break;
       const int64_t y = r_begin + static_cast<int64_t>(kb) * kKB;
       const int64_t left = r_end - y;
       const int valid = left < kKB ? static_cast<int>(left) : kKB;
@@ -411,7 +419,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     // Epilogue: TMEM lane = output row i (within the k tile), column = j. A warp
     // reads the TMEM lane quarter warp % 4; warps 2-5 take columns [0, kN/2),
     // warps 6-9 the rest.
-    if (mbar_wait(sm.accum, 0, 4)) {
+    if (mbar_wait(sm.accum, 0, 4, sm.status)) {
       tc_fence_after();
       const int q = warp % 4;
       const int c0 = ((warp - 2) / 4) * (kN / 2);
@@ -457,9 +465,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmCh,
                  const __grid_constant__ CUtensorMap tmCl, int64_t n, int k, int m, int m_tiles,
                  float* __restrict__ Y, int64_t ldy, float alpha, float beta, int use_beta,
-                 int vec_store, int upper_tri) {
+                 int vec_store, int upper_tri, int* status) {
   extern __shared__ uint8_t dyn_smem[];
-  const Smem sm = carve(dyn_smem);
+  const Smem sm = carve(dyn_smem, status);
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   const int j0 = static_cast<int>(blockIdx.x % m_tiles) * kN;
@@ -476,7 +484,7 @@ rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % kStages;
       const uint32_t ph = (kb / kStages) & 1u;
-      if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1)) break;
+      if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1, sm.status)) break;
       mbar_expect_tx(&sm.full[s], kABytes + 2 * kBBytes);
       tma_load_2d(sm.a_hi(s), &tmX, kb * kKB, static_cast<int>(r0), &sm.full[s]);
       tma_load_2d(sm.b_hi(s), &tmCh, kb * kKB, j0, &sm.full[s]);
@@ -490,7 +498,7 @@ rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % kStages;
       const uint32_t ph = (kb / kStages) & 1u;
-      if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2))) break;
+      if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2, sm.status))) break;
       split_tile(sm.a_hi(s), sm.a_lo(s), kABytes / 16, tid);
       fence_proxy_async();
       __syncwarp();
@@ -503,7 +511,7 @@ rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
     // writes Y row by row with lanes on consecutive columns, so stores stay
     // coalesced instead of one 4-byte store per row per lane.
     if (vec_store) {
-      if (mbar_wait(sm.accum, 0, 4)) {
+      if (mbar_wait(sm.accum, 0, 4, sm.status)) {
         tc_fence_after();
         const int q = warp % 4;
         const int64_t r = r0 + q * 32 + lane;
@@ -538,7 +546,7 @@ rotate_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
           }
         }
       }
-    } else if (mbar_wait(sm.accum, 0, 4)) {
+    } else if (mbar_wait(sm.accum, 0, 4, sm.status)) {
       tc_fence_after();
       const int q = warp % 4;
       float* stage = reinterpret_cast<float*>(sm.base) + q * (32 * kStageLd);
@@ -580,9 +588,10 @@ rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
                             const __grid_constant__ CUtensorMap tmCh,
                             const __grid_constant__ CUtensorMap tmCl, int64_t n, int k, int m,
                             int m_tiles, int64_t total_tiles, float* __restrict__ Y, int64_t ldy,
-                            float alpha, float beta, int use_beta, int upper_tri) {
+                            float alpha, float beta, int use_beta, int upper_tri,
+                            int* status) {
   extern __shared__ uint8_t dyn_smem[];
-  const Smem sm = carve(dyn_smem);
+  const Smem sm = carve(dyn_smem, status);
   // Accumulator full (MMA -> epilogue) and empty (epilogue -> MMA) barriers, after
   // the TMEM address slot.
   uint64_t* accf = reinterpret_cast<uint64_t*>(sm.tmem_slot + 2);
@@ -629,7 +638,7 @@ rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
         for (int kb = 0; kb < nkb; ++kb, ++g) {
           const int s = static_cast<int>(g % kStages);
           const uint32_t ph = (g / kStages) & 1u;
-          if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1)) {
+          if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1, sm.status)) {
             ok = false;
             break;
           }
@@ -650,13 +659,13 @@ rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
         const int j0 = static_cast<int>(t % m_tiles) * kN;
         const int nkb = tile_nkb(j0);
         const int b = lt & 1;
-        if (lt >= 2 && !mbar_wait(&acce[b], static_cast<uint32_t>((lt >> 1) - 1) & 1u, 5)) break;
+        if (lt >= 2 && !mbar_wait(&acce[b], static_cast<uint32_t>((lt >> 1) - 1) & 1u, 5, sm.status)) break;
         tc_fence_after();
         const uint32_t acc_tmem = tmem + static_cast<uint32_t>(b) * kAccStride;
         for (int kb = 0; kb < nkb; ++kb, ++g) {
           const int s = static_cast<int>(g % kStages);
           const uint32_t ph = (g / kStages) & 1u;
-          if (!mbar_wait(&sm.split[s], ph, 3)) {
+          if (!mbar_wait(&sm.split[s], ph, 3, sm.status)) {
             ok = false;
             break;
           }
@@ -692,7 +701,7 @@ rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
       for (int kb = 0; kb < nkb; ++kb, ++g) {
         const int s = static_cast<int>(g % kStages);
         const uint32_t ph = (g / kStages) & 1u;
-        if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2))) {
+        if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2, sm.status))) {
           ok = false;
           break;
         }
@@ -709,7 +718,7 @@ rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
       const int j0 = static_cast<int>(t % m_tiles) * kN;
       const int64_t r0 = (t / m_tiles) * kM;
       const int b = lt & 1;
-      if (!mbar_wait(&accf[b], static_cast<uint32_t>(lt >> 1) & 1u, 4)) break;
+      if (!mbar_wait(&accf[b], static_cast<uint32_t>(lt >> 1) & 1u, 4, sm.status)) break;
       tc_fence_after();
       const int64_t r = r0 + q * 32 + lane;
       const uint32_t base = tmem + static_cast<uint32_t>(b) * kAccStride +
@@ -761,6 +770,22 @@ rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
 
 // C (k x m FP64 column-major) -> Ch, Cl (m_pad x k_pad FP32 row-major = C^T, K-major),
 // zero-padded.
+
+// Test probe of the bounded wait: one warp waits on an mbarrier that nothing
+// arrives on, for `limit` SM clocks, then records `code` in `status` (or the
+// library's default word) and returns. No copies are in flight, so the timeout
+// path leaves nothing behind.
+__global__ void wait_probe_kernel(int* status, long long limit, int code) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_wait_limit(&bar, 0, code, status ? status : &g_tc_status, limit);
+  __syncthreads();
+}
+
 __global__ void rotate_prep_kernel(const double* __restrict__ C, int64_t ldc, int k, int m,
                                    int k_pad, int m_pad, float* __restrict__ Ch,
                                    float* __restrict__ Cl) {
@@ -887,7 +912,7 @@ void gram_tc(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n
   gram_tc_kernel<<<grid, kGramThreads, kSmemBytes, s>>>(mx, my, n, static_cast<int>(k),
                                                     static_cast<int>(m), sx, sy, p.k_tiles,
                                                     p.rows_per_chunk, static_cast<float*>(ws),
-                                                    sym ? 1 : 0);
+                                                    sym ? 1 : 0, current_status_word());
   check_launch("gram_tc_kernel");
   const int64_t total = k * m;
   gram_tc_reduce<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
@@ -941,7 +966,7 @@ void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float*
     rotate_tc_persistent_kernel<<<static_cast<unsigned>(ctas), kPersistThreads, kSmemBytes, s>>>(
         mx, mh, ml, n, static_cast<int>(k), static_cast<int>(m), static_cast<int>(m_tiles),
         total_tiles, Y, ldy, static_cast<float>(alpha), static_cast<float>(beta), beta != 0.0,
-        upper_tri ? 1 : 0);
+        upper_tri ? 1 : 0, current_status_word());
     check_launch("rotate_tc_persistent_kernel");
     return;
   }
@@ -951,8 +976,14 @@ void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float*
                                                       static_cast<int>(m_tiles), Y, ldy,
                                                       static_cast<float>(alpha),
                                                       static_cast<float>(beta), beta != 0.0,
-                                                      vec ? 1 : 0, upper_tri ? 1 : 0);
+                                                      vec ? 1 : 0, upper_tri ? 1 : 0,
+                                                      current_status_word());
   check_launch("rotate_tc_kernel");
+}
+
+void launch_wait_probe(int* status, long long limit_cycles, int code, cudaStream_t s) {
+  wait_probe_kernel<<<1, 32, 0, s>>>(status, limit_cycles, code);
+  check_launch("wait_probe_kernel");
 }
 
 int read_tc_status(bool clear) {
@@ -966,6 +997,14 @@ int read_tc_status(bool clear) {
 }
 
 }  // namespace fe
+
+extern "C" int fe_selftest_wait_timeout(int64_t limit_cycles, int32_t code, void* stream) {
+  return fe::guarded("fe_selftest_wait_timeout", [&] {
+    FE_REQUIRE(code != 0, "code must be nonzero");
+    FE_REQUIRE(limit_cycles >= 0 && limit_cycles <= 4000000000LL, "limit out of range");
+    fe::launch_wait_probe(nullptr, limit_cycles, code, fe::as_stream(stream));
+  });
+}
 
 extern "C" int fe_device_status(int32_t* status, int32_t clear) {
   return fe::guarded("fe_device_status", [&] {

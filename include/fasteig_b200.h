@@ -190,8 +190,17 @@ int fe_rotate_tf32x3(const float* X, int64_t ldx, const double* C, int64_t ldc, 
                      int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
                      void* workspace, size_t workspace_bytes, void* stream);
 /* First failure code recorded by a bounded device-side wait of the tensor-core
- * or pipelined SpMM kernels (0 = none); clear != 0 resets it. */
+ * or pipelined SpMM kernels launched outside a solve (0 = none); clear != 0
+ * resets it. Kernels launched by a solve record in that solve's own word. */
 int fe_device_status(int32_t* status, int32_t clear);
+/* Self-test of the bounded-wait failure path (this entry point has no counterpart
+ * in the reference): launches one warp that waits on an mbarrier nothing arrives
+ * on for limit_cycles SM clocks, then records `code` in the library's default
+ * status word (read by fe_device_status) and returns. No copies are in flight and
+ * the context stays usable. Solves (fe_solve, the server) record timeouts in a
+ * status word of their own and fail with FE_ERR_CUDA instead; the fe_solve option
+ * inject_wait_timeout=<code> runs the same probe on a solve's word (test hook). */
+int fe_selftest_wait_timeout(int64_t limit_cycles, int32_t code, void* stream);
 /* SpMM kernel selection for all later calls in the process (the numerics are
  * the same; the choice only changes the memory schedule): 0 = default
  * (row-batched register kernel for slabs of >= 32 128-bit vectors and rows of
