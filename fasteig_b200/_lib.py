@@ -39,6 +39,8 @@ _SIGS = {
     "fe_cheb_filter_f64": (C.c_int, [vp, vp, vp, i64, i64, i32, f64, f64, vp]),
     "fe_cheb_filter_f32": (C.c_int, [vp, vp, vp, i64, i64, i32, f64, f64, vp]),
     "fe_gram_workspace_bytes": (sz, [i64, i64, i64]),
+    "fe_syevd_f64_workspace_bytes": (sz, [i64]),
+    "fe_syevd_f64": (C.c_int, [vp, i64, i64, vp, vp, vp, sz, vp]),
     "fe_selftest_wait_timeout": (C.c_int, [i64, i32, vp]),
     "fe_lanczos_workspace_bytes": (sz, [i64, i64]),
     "fe_lanczos_step": (C.c_int, [vp, vp, i64, i64, i64, vp, vp, vp, i64, vp, sz, vp]),

@@ -733,10 +733,11 @@ extern "C" int fe_csr_block_diag(int32_t count, const fe_csr_t* parts, fe_csr_t*
   });
 }
 
-// Batched symmetric eigensolver (parallel cyclic Jacobi, one CTA per matrix) for
-// small FP64 matrices, sizes m[p] <= 96 (host array), stored column-major with
-// leading dimension lda at A + p*lda*lda on the device. Writes ascending
-// eigenvalues to W + p*lda and eigenvectors to Z + p*lda*lda.
+// Batched symmetric eigensolver for small FP64 matrices, sizes m[p] (host array),
+// stored column-major with leading dimension lda at A + p*lda*lda on the device.
+// Writes ascending eigenvalues to W + p*lda and eigenvectors to Z + p*lda*lda.
+// Batches whose matrices are all <= 96 run the parallel cyclic Jacobi kernel (one
+// CTA per matrix, in shared memory); larger ones the tridiagonal path of syevd.cu.
 extern "C" int fe_syevd_batched_f64(int32_t count, const int32_t* m, const double* A, int64_t lda,
                                     double* W, double* Z, void* stream) {
   return fe::guarded("fe_syevd_batched_f64", [&] {
@@ -745,12 +746,22 @@ extern "C" int fe_syevd_batched_f64(int32_t count, const int32_t* m, const doubl
     FE_REQUIRE(A && W && Z, "null matrix pointer");
     int max_m = 1;
     for (int32_t p = 0; p < count; ++p) {
-      FE_REQUIRE(m[p] >= 1 && m[p] <= fe::kBatchMaxDim,
-                 "matrix size must be in [1, " + std::to_string(fe::kBatchMaxDim) + "]");
+      FE_REQUIRE(m[p] >= 1 && m[p] <= 8192, "matrix size must be in [1, 8192]");
       FE_REQUIRE(m[p] <= lda, "lda smaller than a matrix size");
       max_m = std::max<int>(max_m, m[p]);
     }
     cudaStream_t s = fe::as_stream(stream);
+    if (max_m > fe::kBatchMaxDim) {
+      // A is input only: decompose a copy (the tridiagonal path overwrites it).
+      const size_t mats = static_cast<size_t>(count) * lda * lda * sizeof(double);
+      fe::DeviceBuffer copy(mats), info(static_cast<size_t>(count) * sizeof(int32_t)),
+          ws(fe::syevd_workspace_bytes(count, lda));
+      FE_CHECK_CUDA(cudaMemcpyAsync(copy.get(), A, mats, cudaMemcpyDeviceToDevice, s));
+      fe::syevd_batched(count, m, copy.as<double>(), lda, W, Z, info.as<int32_t>(), ws.get(),
+                        ws.bytes(), s);
+      FE_CHECK_CUDA(cudaStreamSynchronize(s));
+      return;
+    }
     void *dm = nullptr, *dtodo = nullptr, *dzl = nullptr;
     FE_CHECK_CUDA(cudaMallocAsync(&dm, count * sizeof(int32_t), s));
     FE_CHECK_CUDA(cudaMallocAsync(&dtodo, count * sizeof(int32_t), s));

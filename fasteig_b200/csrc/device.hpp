@@ -45,6 +45,17 @@ void potrf_upper(double* G, int64_t k, int64_t ldg, int32_t* info, cudaStream_t 
 void trinv_upper(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
                  cudaStream_t s);
 void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s);
+// Device symmetric eigensolver (syevd.cu): A (k x k, lda, column-major) is replaced
+// by its eigenvectors, W gets the ascending eigenvalues, *info (device) is nonzero
+// for non-finite input.
+size_t syevd_single_workspace_bytes(int64_t k);
+void syevd_single(double* A, int64_t lda, int64_t k, double* W, int32_t* info, void* ws,
+                  size_t ws_bytes, cudaStream_t s);
+// Batched form: `count` matrices A + p*lda*lda of sizes m_host[p] <= lda; eigenvalues
+// to W + p*lda, eigenvectors to Z + p*lda*lda; A is overwritten by reflectors.
+size_t syevd_workspace_bytes(int count, int64_t lda);
+void syevd_batched(int count, const int32_t* m_host, double* A, int64_t lda, double* W,
+                   double* Z, int32_t* info, void* ws, size_t ws_bytes, cudaStream_t s);
 
 // ---- owning device buffer --------------------------------------------------
 // Stream on which this thread's DeviceBuffer allocations are ordered (set for the

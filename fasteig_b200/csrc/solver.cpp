@@ -16,7 +16,6 @@
 // switches the block to FP64 for the final sweeps once the FP32 residual floor
 // is reached.
 
-#include <cusolverDn.h>
 
 #include <chrono>
 #include <cstdio>
@@ -32,15 +31,6 @@
 
 namespace fe {
 namespace {
-
-#define FE_CHECK_SOLVER(call)                                                               \
-  do {                                                                                      \
-    cusolverStatus_t st_ = (call);                                                          \
-    if (st_ != CUSOLVER_STATUS_SUCCESS) {                                                   \
-      throw ::fe::Error(FE_ERR_CUDA, std::string(#call) + " failed: status " +              \
-                                         std::to_string(static_cast<int>(st_)));            \
-    }                                                                                       \
-  } while (0)
 
 std::string lower(std::string s) {
   for (auto& c : s) c = static_cast<char>(std::tolower(static_cast<unsigned char>(c)));
@@ -192,16 +182,13 @@ struct PhaseEvents {
   }
 };
 
-// One solve's stream and cuSOLVER handle. While it lives, this thread's
-// DeviceBuffers are allocated from the device's stream-ordered pool on its stream
-// (buffers declared after the Context are released before it).
-// Streams and cuSOLVER handles are kept for reuse (per device, shared by all
-// threads): creating and destroying them per solve cost up to half a second
-// (the handle's own buffers are released with synchronizing frees).
+// One solve's stream. While it lives, this thread's DeviceBuffers are allocated
+// from the device's stream-ordered pool on its stream (buffers declared after the
+// Context are released before it). Streams are kept for reuse (per device, shared by
+// all threads).
 struct ContextResources {
   int device;
   cudaStream_t stream;
-  cusolverDnHandle_t solver;
 };
 std::mutex g_ctx_mutex;
 std::vector<ContextResources> g_ctx_free;
@@ -209,7 +196,6 @@ std::vector<ContextResources> g_ctx_free;
 class Context {
  public:
   cudaStream_t stream = nullptr;
-  cusolverDnHandle_t solver = nullptr;
   Context() {
     FE_CHECK_CUDA(cudaGetDevice(&device_));
     retain_pool_memory(device_);
@@ -218,22 +204,12 @@ class Context {
       for (size_t i = 0; i < g_ctx_free.size(); ++i) {
         if (g_ctx_free[i].device == device_) {
           stream = g_ctx_free[i].stream;
-          solver = g_ctx_free[i].solver;
           g_ctx_free.erase(g_ctx_free.begin() + static_cast<std::ptrdiff_t>(i));
           break;
         }
       }
     }
-    if (!stream) {
-      FE_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-      cusolverStatus_t st = cusolverDnCreate(&solver);
-      if (st == CUSOLVER_STATUS_SUCCESS) st = cusolverDnSetStream(solver, stream);
-      if (st != CUSOLVER_STATUS_SUCCESS) {
-        if (solver) cusolverDnDestroy(solver);
-        cudaStreamDestroy(stream);
-        throw Error(FE_ERR_CUDA, "cusolverDnCreate failed");
-      }
-    }
+    if (!stream) FE_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     prev_alloc_ = alloc_stream();
     alloc_stream() = stream;
   }
@@ -242,9 +218,8 @@ class Context {
     if (!stream) return;
     if (cudaStreamSynchronize(stream) == cudaSuccess) {
       std::lock_guard<std::mutex> lock(g_ctx_mutex);
-      g_ctx_free.push_back({device_, stream, solver});
+      g_ctx_free.push_back({device_, stream});
     } else {
-      if (solver) cusolverDnDestroy(solver);
       cudaStreamDestroy(stream);
     }
   }
@@ -433,25 +408,19 @@ void lanczos_bounds(Context& ctx, const Csr& A, double sign, unsigned seed, bool
   upper_out = up;
 }
 
-// cusolverDnDsyevd on the device for the projected k-by-k matrix.
+// Device eigensolver for the projected k-by-k matrix (syevd.cu): replaces the
+// reference's Dsyevd (src/gpu/CudaLanczosWorkspace.cpp:155-157) and host Eigen
+// SelfAdjointEigenSolver (src/core/RitzExtraction.cpp:104).
 class ProjectedEig {
  public:
   ProjectedEig(Context& ctx, int64_t cap) : ctx_(ctx), cap_(cap) {
-    DeviceBuffer P(static_cast<size_t>(cap) * cap * sizeof(double)), W(cap * sizeof(double));
-    int lwork = 0;
-    FE_CHECK_SOLVER(cusolverDnDsyevd_bufferSize(ctx.solver, CUSOLVER_EIG_MODE_VECTOR,
-                                                CUBLAS_FILL_MODE_UPPER, static_cast<int>(cap),
-                                                P.as<double>(), static_cast<int>(cap),
-                                                W.as<double>(), &lwork));
-    work_.resize(static_cast<size_t>(std::max(lwork, 1)) * sizeof(double));
-    lwork_ = lwork;
+    work_.resize(syevd_single_workspace_bytes(cap));
     info_.resize(sizeof(int));
   }
   // P (k-by-k, ldp) is overwritten by eigenvectors; W gets ascending eigenvalues.
   void run(double* P, int64_t k, int64_t ldp, double* W) {
-    FE_CHECK_SOLVER(cusolverDnDsyevd(ctx_.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,
-                                     static_cast<int>(k), P, static_cast<int>(ldp), W,
-                                     work_.as<double>(), lwork_, info_.as<int>()));
+    FE_REQUIRE(k <= cap_, "projected eigensolve larger than its capacity");
+    syevd_single(P, ldp, k, W, info_.as<int32_t>(), work_.get(), work_.bytes(), ctx_.stream);
   }
   int* info() const { return info_.as<int>(); }
 
@@ -459,7 +428,6 @@ class ProjectedEig {
   Context& ctx_;
   int64_t cap_;
   DeviceBuffer work_, info_;
-  int lwork_ = 0;
 };
 
 // Per-precision block set of the Chebyshev iteration.

@@ -45,8 +45,7 @@ typedef struct fe_csr* fe_csr_t;
 const char* fe_version(void);
 const char* fe_last_error(void);
 int fe_device_count(int* count);
-/* Kernel launches issued by this library since it was loaded (all threads);
- * library calls made on its behalf (cuSOLVER) are not counted. */
+/* Kernel launches issued by this library since it was loaded (all threads). */
 int64_t fe_launch_count(void);
 
 /* ---------------------------------------------------------------------
@@ -351,12 +350,27 @@ int fe_batch_krylov_schur(int32_t count, const fe_csr_t* A, const int64_t* nev,
  * The result is a new handle (release with fe_csr_destroy); parts stay valid. */
 int fe_csr_block_diag(int32_t count, const fe_csr_t* parts, fe_csr_t* out);
 
+/* Symmetric eigensolver for one small dense FP64 matrix on the device (replaces
+ * the projected-matrix Dsyevd of src/gpu/CudaLanczosWorkspace.cpp:155-157 and the
+ * host SelfAdjointEigenSolver of src/core/RitzExtraction.cpp:104): A (k-by-k,
+ * column-major, lda >= k) is replaced by its orthonormal eigenvectors, W[k] gets
+ * the eigenvalues in ascending order, *info (device int) is 0, or 1 for
+ * non-finite input. Householder tridiagonalization in one CTA, bisection for the
+ * eigenvalues, inverse iteration (clusters re-orthogonalized) for the vectors,
+ * back-transformation; k <= 8192. Asynchronous on `stream`; workspace from
+ * fe_syevd_f64_workspace_bytes(k). */
+size_t fe_syevd_f64_workspace_bytes(int64_t k);
+int fe_syevd_f64(double* A, int64_t lda, int64_t k, double* W, int32_t* info, void* workspace,
+                 size_t workspace_bytes, void* stream);
+
 /* Batched symmetric eigensolver for `count` small FP64 matrices (replaces one
  * Dsyevd per projected matrix, src/gpu/CudaLanczosWorkspace.cpp:155): sizes
- * m[count] (host array, each in [1, 96]), matrix p column-major at
- * A + p*lda*lda on the device (lda >= max m); ascending eigenvalues to
- * W + p*lda, eigenvectors to Z + p*lda*lda. Parallel cyclic Jacobi, one CTA per
- * matrix; returns after the stream has finished. */
+ * m[count] (host array, each in [1, 8192]), matrix p column-major at
+ * A + p*lda*lda on the device (lda >= max m; A is not modified); ascending
+ * eigenvalues to W + p*lda, eigenvectors to Z + p*lda*lda. Batches of matrices
+ * up to 96 run a parallel cyclic Jacobi kernel (one CTA per matrix), larger ones
+ * the tridiagonal path of fe_syevd_f64 (one CTA per matrix per stage); returns
+ * after the stream has finished. */
 int fe_syevd_batched_f64(int32_t count, const int32_t* m, const double* A, int64_t lda,
                          double* W, double* Z, void* stream);
 
