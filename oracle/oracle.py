@@ -59,8 +59,22 @@ def random_block(rows: int, cols: int, seed: int = 1) -> np.ndarray:
     """Executor::create_random_multivector (src/core/Executor.cpp:44-62)."""
     if rows <= 0 or cols <= 0:
         raise ValueError("Executor::create_random_multivector: dimensions must be positive.")
-    v = mt19937_uniform(rows * cols, seed)
-    return v.reshape(cols, rows).T.copy()  # column-major fill
+    # Column-major fill: column j takes draws [j*rows, (j+1)*rows) of one stream,
+    # generated a column at a time (large blocks need no multi-GB temporaries).
+    # (lo + hi * 2^32) is formed exactly as a 64-bit integer; its conversion to
+    # double rounds once, as the double sum in generate_canonical does.
+    bg = np.random.MT19937(0)
+    bg._legacy_seeding(int(seed) & 0xFFFFFFFF)
+    colmajor = np.empty((cols, rows))
+    below_one = np.nextafter(1.0, 0.0)
+    for j in range(cols):
+        raw = bg.random_raw(2 * rows)
+        canon = ((raw[1::2] << np.uint64(32)) | raw[0::2]).astype(np.float64)
+        canon *= 1.0 / 18446744073709551616.0
+        np.minimum(canon, below_one, out=canon)
+        np.multiply(canon, 2.0, out=colmajor[j])
+        colmajor[j] -= 1.0
+    return np.ascontiguousarray(colmajor.T)
 
 
 def random_vector(size: int, seed: int = 1) -> np.ndarray:

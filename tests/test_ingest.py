@@ -105,7 +105,7 @@ def test_device_ingest_matrix_market_files(tmp_path):
         with open(path, "w") as f:
             f.write(f"%%MatrixMarket matrix coordinate real {sym}\n% comment\n{n} {n} {r.size}\n")
             for i, j, x in zip(r, c, v):
-                f.write(f"{i + 1} {j + 1} {x!r}\n")
+                f.write(f"{i + 1} {j + 1} {float(x)!r}\n")
         ref = O.csr_from_triplets(n, r, c, v, exp_sym, expand_skew=exp_skew)
         _same(fe.CsrMatrix.from_matrix_market(path), ref)
     path = tmp_path / "pattern.mtx"
