@@ -390,6 +390,97 @@ void trinv_upper(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_
   check_launch("trinv_upper_kernel");
 }
 
+// C = alpha op(A) B + beta C for small column-major FP64 matrices (projected
+// k-by-k algebra): op(A) = A (m x kk) or A^T (A stored kk x m). 32 x 32 output tiles,
+// the kk dimension staged through shared memory in 32-wide slabs.
+__global__ void small_gemm_kernel(int trans_a, int m, int n, int kk, double alpha,
+                                  const double* __restrict__ A, int64_t lda,
+                                  const double* __restrict__ B, int64_t ldb, double beta,
+                                  double* __restrict__ C, int64_t ldc) {
+  __shared__ double As[32][33];
+  __shared__ double Bs[32][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8 threads, 4 rows each
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k0 = 0; k0 < kk; k0 += 32) {
+    for (int q = ty; q < 32; q += 8) {
+      // As[i][l] = op(A)(r0 + i, k0 + l); Bs[l][j] = B(k0 + l, c0 + j)
+      const int i = tx, l = q;
+      double a = 0.0;
+      if (r0 + i < m && k0 + l < kk)
+        a = trans_a ? A[static_cast<int64_t>(r0 + i) * lda + (k0 + l)]
+                    : A[static_cast<int64_t>(k0 + l) * lda + (r0 + i)];
+      As[i][l] = a;
+      double b = 0.0;
+      if (k0 + tx < kk && c0 + q < n) b = B[static_cast<int64_t>(c0 + q) * ldb + (k0 + tx)];
+      Bs[tx][q] = b;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int l = 0; l < 32; ++l) {
+      const double a = As[tx][l];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fma(a, Bs[l][ty + 8 * q], acc[q]);
+    }
+    __syncthreads();
+  }
+  const int i = r0 + tx;
+  if (i >= m) return;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int j = c0 + ty + 8 * q;
+    if (j < n) {
+      double* c = C + static_cast<int64_t>(j) * ldc + i;
+      *c = (beta == 0.0) ? alpha * acc[q] : fma(alpha, acc[q], beta * *c);
+    }
+  }
+}
+
+// d[j] = 1 / sqrt(G[j, j]) (1 where the diagonal is not positive).
+__global__ void inv_sqrt_diag_kernel(const double* __restrict__ G, int k, int64_t ldg,
+                                     double* __restrict__ d) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= k) return;
+  const double g = G[static_cast<int64_t>(j) * ldg + j];
+  d[j] = g > 0.0 ? 1.0 / sqrt(g) : 1.0;
+}
+
+// M[i, j] *= d[i] * d[j] (cols_scaled) or M[i, j] *= d[i] (rows only).
+__global__ void diag_scale_kernel(double* __restrict__ M, int rows, int cols, int64_t ldm,
+                                  const double* __restrict__ d, int both) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<int64_t>(rows) * cols) return;
+  const int i = static_cast<int>(idx % rows), j = static_cast<int>(idx / rows);
+  double* x = M + static_cast<int64_t>(j) * ldm + i;
+  *x *= both ? d[i] * d[j] : d[i];
+}
+
+void small_gemm(bool trans_a, int64_t m, int64_t n, int64_t kk, double alpha, const double* A,
+                int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
+                cudaStream_t s) {
+  if (m <= 0 || n <= 0) return;
+  dim3 grid(static_cast<unsigned>((m + 31) / 32), static_cast<unsigned>((n + 31) / 32));
+  small_gemm_kernel<<<grid, dim3(32, 8), 0, s>>>(trans_a ? 1 : 0, static_cast<int>(m),
+                                                 static_cast<int>(n), static_cast<int>(kk), alpha,
+                                                 A, lda, B, ldb, beta, C, ldc);
+  check_launch("small_gemm_kernel");
+}
+
+void inv_sqrt_diag(const double* G, int64_t k, int64_t ldg, double* d, cudaStream_t s) {
+  inv_sqrt_diag_kernel<<<static_cast<unsigned>((k + 127) / 128), 128, 0, s>>>(
+      G, static_cast<int>(k), ldg, d);
+  check_launch("inv_sqrt_diag_kernel");
+}
+
+void diag_scale(double* M, int64_t rows, int64_t cols, int64_t ldm, const double* d, bool both,
+                cudaStream_t s) {
+  const int64_t total = rows * cols;
+  if (total <= 0) return;
+  diag_scale_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
+      M, static_cast<int>(rows), static_cast<int>(cols), ldm, d, both ? 1 : 0);
+  check_launch("diag_scale_kernel");
+}
+
 void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s) {
   FE_REQUIRE(k >= 0 && ldp >= k, "symmetrize: invalid shape");
   if (k == 0) return;

@@ -45,6 +45,14 @@ void potrf_upper(double* G, int64_t k, int64_t ldg, int32_t* info, cudaStream_t 
 void trinv_upper(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
                  cudaStream_t s);
 void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s);
+// Small column-major FP64 products: C = alpha op(A) B + beta C, op(A) = A or A^T.
+void small_gemm(bool trans_a, int64_t m, int64_t n, int64_t kk, double alpha, const double* A,
+                int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
+                cudaStream_t s);
+// d[j] = 1/sqrt(G[j,j]); M <- D M D (both) or D M (rows only).
+void inv_sqrt_diag(const double* G, int64_t k, int64_t ldg, double* d, cudaStream_t s);
+void diag_scale(double* M, int64_t rows, int64_t cols, int64_t ldm, const double* d, bool both,
+                cudaStream_t s);
 // Device symmetric eigensolver (syevd.cu): A (k x k, lda, column-major) is replaced
 // by its eigenvectors, W gets the ascending eigenvalues, *info (device) is nonzero
 // for non-finite input.

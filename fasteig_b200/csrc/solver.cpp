@@ -64,6 +64,10 @@ struct Options {
   std::string locking = "soft";    // Chebyshev: soft (reference) | hard
   int64_t tail_degree = 0;         // Chebyshev mixed: filter degree of the FP64 cycles (0 = degree)
   int64_t inject_wait_timeout = 0;  // test hook: status code of a forced bounded-wait timeout
+  // Chebyshev hard locking: Rayleigh-Ritz with the Cholesky QR rotation folded in
+  // ("fused", the default of precision=mixed) or Cholesky QR then Rayleigh-Ritz as
+  // the reference orders them ("cholqr", the default of precision=fp64).
+  std::string rr = "";
 
   void parse(const char* text) {
     if (!text) return;
@@ -133,6 +137,10 @@ struct Options {
     else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
     else if (k == "tail_degree") tail_degree = as_int(v);
     else if (k == "inject_wait_timeout") inject_wait_timeout = as_int(v);
+    else if (k == "rr") {
+      rr = lower(v);
+      if (rr != "fused" && rr != "cholqr") throw Error(FE_ERR_INVALID, "rr must be fused or cholqr");
+    }
     else if (k == "locking") {
       locking = lower(v);
       if (locking != "soft" && locking != "hard")
@@ -447,6 +455,7 @@ struct ChebBlocks {
 
 struct SmallState {
   DeviceBuffer G, Rinv, W, rel, rnorm, xnorm, info, gws, rws, cws;
+  DeviceBuffer Gk, Tmp, dscale;  // fused Rayleigh-Ritz: Gram, product scratch, scaling
   int64_t cap = 0;
   bool tensor_cores = false;  // FP32 Grams/rotations on tcgen05 (3xTF32)
   int64_t precise_grams = 0;  // FP32 Cholesky passes redone with the FP64-accumulated Gram
@@ -455,6 +464,9 @@ struct SmallState {
     tensor_cores = tc;
     G.resize(static_cast<size_t>(c) * c * sizeof(double));
     Rinv.resize(static_cast<size_t>(c) * c * sizeof(double));
+    Gk.resize(static_cast<size_t>(c) * c * sizeof(double));
+    Tmp.resize(static_cast<size_t>(c) * c * sizeof(double));
+    dscale.resize(c * sizeof(double));
     W.resize(c * sizeof(double));
     rel.resize(c * sizeof(double));
     rnorm.resize(c * sizeof(double));
@@ -538,6 +550,64 @@ void cholqr(Context& ctx, SmallState& sm, const T* src, int64_t lds, T* dst, int
                   /*upper_tri=*/true);
 }
 
+// Rayleigh-Ritz on the span of a block Y (n x k, columns independent but not
+// orthonormal) as the generalized problem (Y^T A Y) c = theta (Y^T Y) c: with
+// D = diag(Y^T Y)^{-1/2} and D Y^T Y D = R^T R, P = R^{-T} D (Y^T A Y) D R^{-1} = Z Theta Z^T
+// and the Ritz vectors are X = Y (D R^{-1} Z). This is the reference's Cholesky QR of Y
+// followed by its Rayleigh-Ritz (src/core/Orthogonalization.cpp:185-246,
+// src/core/RitzExtraction.cpp:65-141) with the QR's rotation folded into the Ritz
+// rotation: one n x k x k product instead of two. AY receives op*Y; P = sm.G holds Z
+// and sm.W the ascending Ritz values on return. Returns false (nothing written to X)
+// when the scaled Gram is not positive definite, so the caller can take the
+// Cholesky QR path instead.
+template <typename T>
+bool fused_rr(Context& ctx, SmallState& sm, ProjectedEig& eig, const Csr& A, double sign,
+              const T* Y, int64_t ldy, T* AY, int64_t lday, T* X, int64_t ldx, int64_t n, int64_t k,
+              Stats& st) {
+  cudaStream_t s = ctx.stream;
+  const int64_t ld = sm.cap;
+  double* G = sm.Gk.as<double>();
+  double* H = sm.G.as<double>();
+  double* d = sm.dscale.as<double>();
+  int32_t* info = sm.info.as<int32_t>() + 3;
+  csr_spmm<T>(A, Y, ldy, AY, lday, nullptr, 0, k, sign, 0.0, 0.0, s);
+  st.spmm_launches += 1;
+  gram_block<T>(sm, Y, ldy, Y, ldy, n, k, k, G, s);
+  gram_block<T>(sm, Y, ldy, AY, lday, n, k, k, H, s);
+  auto factor = [&] {
+    FE_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int32_t), s));
+    inv_sqrt_diag(G, k, ld, d, s);
+    diag_scale(G, k, k, ld, d, true, s);
+    potrf_upper(G, k, ld, info, s);
+    int32_t h = 0;
+    ctx.to_host(&h, info, 1);
+    ctx.sync();
+    return h == 0;
+  };
+  if (!factor()) {
+    if (sizeof(T) == 4 && sm.tensor_cores) {
+      // FP32 blocks: retry once with the FP64-accumulated Gram.
+      sm.precise_grams += 1;
+      gram_block<T>(sm, Y, ldy, Y, ldy, n, k, k, G, s, /*precise=*/true);
+      if (!factor()) return false;
+    } else {
+      return false;
+    }
+  }
+  diag_scale(H, k, k, ld, d, true, s);
+  double* Rinv = sm.Rinv.as<double>();
+  double* Tm = sm.Tmp.as<double>();
+  trinv_upper(G, ld, Rinv, ld, k, s);
+  small_gemm(false, k, k, k, 1.0, H, ld, Rinv, ld, 0.0, Tm, ld, s);    // H R^-1
+  small_gemm(true, k, k, k, 1.0, Rinv, ld, Tm, ld, 0.0, H, ld, s);     // R^-T H R^-1
+  symmetrize(H, k, ld, s);
+  eig.run(H, k, ld, sm.W.as<double>());
+  small_gemm(false, k, k, k, 1.0, Rinv, ld, H, ld, 0.0, Tm, ld, s);    // R^-1 Z
+  diag_scale(Tm, k, k, ld, d, false, s);                                // D R^-1 Z
+  rotate_block<T>(sm, Y, ldy, Tm, X, ldx, n, k, k, 1.0, 0.0, s);
+  return true;
+}
+
 // Filter scaling (src/ChebyshevSolver.cpp:231-239) for a damped interval [cutoff, upper]
 // where the amplification at `lower` is `amp` (the reference: amp = 1e3).
 double reference_cutoff(double lower, double upper, int64_t degree, double amp) {
@@ -557,6 +627,7 @@ struct ChebLoop {
   double sign, lower, upper;
   bool cholqr2;
   bool hard;  // hard locking: the locked prefix is final, QR and Rayleigh-Ritz see the rest
+  bool fused = false;  // Rayleigh-Ritz with the (second) Cholesky QR pass folded in
   PhaseEvents ev;
 
   ChebLoop(Context& c, const Csr& a, const Options& o, SmallState& s, ProjectedEig& e, double sg,
@@ -676,24 +747,49 @@ struct ChebLoop {
                       Stats& st) {
     cudaStream_t s = ctx.stream;
     const int64_t active = sub - locked;
-    if (cholqr2) {
+    bool done = false;
+    if (fused) {
+      // FP32 blocks: one Cholesky QR pass, its second pass folded into the
+      // Rayleigh-Ritz; FP64 blocks (the mixed path's FP64 cycles, whose filtered
+      // columns are near-orthogonal once scaled): the Rayleigh-Ritz directly.
+      const T* Yq = Y;
+      int64_t ldq = ldy;
+      if (cholqr2) {
+        cholqr<T>(ctx, sm, Y, ldy, b.Q.data(), b.Q.ld, n, active, 0);
+        Yq = b.Q.data();
+        ldq = b.Q.ld;
+      }
+      ev.record(2, s);
+      done = fused_rr<T>(ctx, sm, eig, A, sign, Yq, ldq, b.AQ.data(), b.AQ.ld, b.S.data(),
+                         b.S.ld, n, active, st);
+      if (!done && cholqr2) {  // fall back to the second Cholesky QR pass
+        cholqr<T>(ctx, sm, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, n, active, 1);
+        FE_CHECK_CUDA(cudaMemcpy2DAsync(b.Q.data(), b.Q.ld * sizeof(T), b.AQ.data(),
+                                        b.AQ.ld * sizeof(T), active * sizeof(T), n,
+                                        cudaMemcpyDeviceToDevice, s));
+      } else if (!done) {
+        cholqr<T>(ctx, sm, Y, ldy, b.Q.data(), b.Q.ld, n, active, 0);
+      }
+    } else if (cholqr2) {
       cholqr<T>(ctx, sm, Y, ldy, b.AQ.data(), b.AQ.ld, n, active, 0);
       cholqr<T>(ctx, sm, b.AQ.data(), b.AQ.ld, b.Q.data(), b.Q.ld, n, active, 1);
     } else {
       cholqr<T>(ctx, sm, Y, ldy, b.Q.data(), b.Q.ld, n, active, 0);
     }
-    ev.record(2, s);
-    csr_spmm<T>(A, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, nullptr, 0, active, sign, 0.0, 0.0,
-                s);
-    st.spmm_launches += 1;
-    double* P = sm.G.as<double>();
-    gram_block<T>(sm, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, n, active, active, P, s);
-    symmetrize(P, active, sm.cap, s);
-    eig.run(P, active, sm.cap, sm.W.as<double>());
-    // Ritz vectors of the active block into S (aligned), residuals of its wanted
-    // pairs (indices locked..nev-1), then into V[:, locked:sub].
-    rotate_block<T>(sm, b.Q.data(), b.Q.ld, P, b.S.data(), b.S.ld, n, active, active, 1.0, 0.0,
-                    s);
+    if (!done) {
+      if (!fused) ev.record(2, s);
+      csr_spmm<T>(A, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, nullptr, 0, active, sign, 0.0,
+                  0.0, s);
+      st.spmm_launches += 1;
+      double* P = sm.G.as<double>();
+      gram_block<T>(sm, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, n, active, active, P, s);
+      symmetrize(P, active, sm.cap, s);
+      eig.run(P, active, sm.cap, sm.W.as<double>());
+      // Ritz vectors of the active block into S (aligned), residuals of its wanted
+      // pairs (indices locked..nev-1), then into V[:, locked:sub].
+      rotate_block<T>(sm, b.Q.data(), b.Q.ld, P, b.S.data(), b.S.ld, n, active, active, 1.0, 0.0,
+                      s);
+    }
     const int64_t nw = nev - locked;
     const int64_t vw = 16 / static_cast<int64_t>(sizeof(T));
     const int64_t nw_pad = std::min(((nw + vw - 1) / vw) * vw, b.S.ld);  // whole vectors
@@ -765,6 +861,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   if (opt.block > 0) cap = std::max(nev, std::min(opt.block, n));
   const bool host_init = opt.init == "host";
   const bool mixed = opt.precision == "mixed";
+  const bool fused_rr_on = opt.rr.empty() ? mixed : opt.rr == "fused";
 
   using clock = std::chrono::steady_clock;
   const auto t_start = clock::now();
@@ -797,6 +894,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     else fill_uniform<double>(V0.data(), V0.ld, n, cap, seed, ctx.stream);
     if (mixed) {
       l32.reset(new ChebLoop<float>(ctx, A, opt, sm, eig, sign, lower, upper, true));
+      l32->fused = fused_rr_on;
       l32->b.allocate(n, cap);
       // A random block is well conditioned: round it to FP32 and orthonormalize
       // with CholQR2 on the FP32 (tensor-core) path.
@@ -806,6 +904,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
       cholqr<float>(ctx, sm, l32->b.Q.data(), l32->b.Q.ld, l32->b.V.data(), l32->b.V.ld, n, cap, 1);
     } else {
       l64.reset(new ChebLoop<double>(ctx, A, opt, sm, eig, sign, lower, upper, false));
+      l64->fused = fused_rr_on;
       l64->b.allocate(n, cap);
       cholqr<double>(ctx, sm, V0.data(), V0.ld, l64->b.V.data(), l64->b.V.ld, n, cap, 0);
     }
@@ -882,6 +981,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
       const auto t_switch = clock::now();
       // FP32 residual floor reached: continue on FP64 blocks.
       l64.reset(new ChebLoop<double>(ctx, A, opt, sm, eig, sign, lower, upper, false));
+      l64->fused = fused_rr_on;
       if (opt.tail_degree > 0) l64->degree = opt.tail_degree;
       l64->b.allocate(n, cap);
       convert<float, double>(l32->b.V.data(), l32->b.V.ld, l64->b.V.data(), l64->b.V.ld, n, cap,
