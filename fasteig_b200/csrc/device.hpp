@@ -21,6 +21,18 @@ namespace fe {
 template <typename T>
 void csr_spmm(const Csr& A, const T* X, int64_t ldx, T* Y, int64_t ldy, const T* Z, int64_t ldz,
               int64_t ncols, double alpha, double gamma, double beta, cudaStream_t s);
+// Refined filter pieces (spmm.cu): the FP32 Chebyshev step with a correction term
+// R diag(delta), and the elementwise start (R32 = R64 - X diag(theta), Z1 = c R32) and
+// finish (X = X diag(t) + Z) of the correction recurrence.
+void csr_spmm_corr_f32(const Csr& A, const float* X, int64_t ldx, float* Y, int64_t ldy,
+                       const float* Z, int64_t ldz, const float* R, int64_t ldr,
+                       const float* delta, int64_t ncols, double alpha, double gamma, double beta,
+                       cudaStream_t s);
+void refine_start(int64_t n, int64_t ncols, const double* R64, int64_t ld64, const double* X,
+                  int64_t ldx, const double* theta, double c, float* R32, float* Z1,
+                  int64_t ld32, cudaStream_t s);
+void refine_finish(int64_t n, int64_t ncols, const double* t, const float* Z, int64_t ld32,
+                   double* X, int64_t ldx, cudaStream_t s);
 template <typename T>
 void cheb_filter(const Csr& A, T* X, T* scratch, int64_t ld, int64_t ncols, int degree, double c,
                  double d, cudaStream_t s);

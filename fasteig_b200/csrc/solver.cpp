@@ -12,9 +12,9 @@
 // Chebyshev follows ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221).
 // Precision: "fp64" runs every block in FP64 (the plain path); "mixed" runs the
 // filter, SpMMs and rotations on FP32 blocks with FP64-accumulated Grams, FP64
-// Cholesky (two passes: CholQR2) and an FP64 projected eigensolve, then
-// switches the block to FP64 for the final sweeps once the FP32 residual floor
-// is reached.
+// Cholesky and an FP64 projected eigensolve, then switches the block to FP64 for
+// the final sweeps once the FP32 residual floor is reached; those sweeps filter
+// through an FP32 correction recurrence that keeps FP64 accuracy (refined_filter).
 
 
 #include <chrono>
@@ -26,6 +26,7 @@
 #include <mutex>
 #include <random>
 #include <sstream>
+#include <type_traits>
 
 #include "device.hpp"
 
@@ -68,6 +69,9 @@ struct Options {
   // ("fused", the default of precision=mixed) or Cholesky QR then Rayleigh-Ritz as
   // the reference orders them ("cholqr", the default of precision=fp64).
   std::string rr = "";
+  // Chebyshev mixed: filter of the FP64 cycles, "refined" (FP32 correction recurrence,
+  // FP64 accuracy) or "fp64" (FP64 SpMMs).
+  std::string tail_filter = "refined";
 
   void parse(const char* text) {
     if (!text) return;
@@ -137,7 +141,11 @@ struct Options {
     else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
     else if (k == "tail_degree") tail_degree = as_int(v);
     else if (k == "inject_wait_timeout") inject_wait_timeout = as_int(v);
-    else if (k == "rr") {
+    else if (k == "tail_filter") {
+      tail_filter = lower(v);
+      if (tail_filter != "refined" && tail_filter != "fp64")
+        throw Error(FE_ERR_INVALID, "tail_filter must be refined or fp64");
+    } else if (k == "rr") {
       rr = lower(v);
       if (rr != "fused" && rr != "cholqr") throw Error(FE_ERR_INVALID, "rr must be fused or cholqr");
     }
@@ -628,6 +636,11 @@ struct ChebLoop {
   bool cholqr2;
   bool hard;  // hard locking: the locked prefix is final, QR and Rayleigh-Ritz see the rest
   bool fused = false;  // Rayleigh-Ritz with the (second) Cholesky QR pass folded in
+  // FP64 cycles of the mixed path: filter through the FP32 correction recurrence
+  // (refined_filter) when every active column has a Ritz value from the last cycle.
+  bool refine = false;
+  bool theta_ready = false;
+  Block<float> r32, z0, z1;  // refined-filter blocks (allocated on first use)
   PhaseEvents ev;
 
   ChebLoop(Context& c, const Csr& a, const Options& o, SmallState& s, ProjectedEig& e, double sg,
@@ -666,11 +679,27 @@ struct ChebLoop {
       if (!std::isfinite(c) || !std::isfinite(d))
         throw Error(FE_ERR_NONFINITE, "ChebyshevSolver: invalid filter scaling.");
       // The operator is sign*A: fold the sign into c.
-      if (in_place) {
-        filter(b.V.col(locked), b.V.ld, b.S.data(), b.S.ld, active, sign * c, d);
-      } else {
-        stage_active();
-        filter(b.S.data(), b.S.ld, b.Q.data(), b.Q.ld, act_pad, sign * c, d);
+      bool refined = false;
+      if constexpr (std::is_same_v<T, double>) {
+        if (refine && theta_ready) {
+          std::vector<double> theta(static_cast<size_t>(act_pad), 0.0);
+          for (int64_t j = 0; j < active; ++j) theta[j] = W[locked + j];
+          if (in_place) {
+            refined_filter(b.V.col(locked), b.V.ld, active, c, d, theta);
+          } else {
+            stage_active();
+            refined_filter(b.S.data(), b.S.ld, act_pad, c, d, theta);
+          }
+          refined = true;
+        }
+      }
+      if (!refined) {
+        if (in_place) {
+          filter(b.V.col(locked), b.V.ld, b.S.data(), b.S.ld, active, sign * c, d);
+        } else {
+          stage_active();
+          filter(b.S.data(), b.S.ld, b.Q.data(), b.Q.ld, act_pad, sign * c, d);
+        }
       }
       st.spmm_launches += static_cast<double>(degree);
     } else if (!in_place) {
@@ -760,8 +789,17 @@ struct ChebLoop {
         ldq = b.Q.ld;
       }
       ev.record(2, s);
-      done = fused_rr<T>(ctx, sm, eig, A, sign, Yq, ldq, b.AQ.data(), b.AQ.ld, b.S.data(),
-                         b.S.ld, n, active, st);
+      // The Ritz vectors go to S, or to Q (then copied to S) when Y is staged in S.
+      const bool y_in_s = Yq == b.S.data();
+      T* Xo = y_in_s ? b.Q.data() : b.S.data();
+      const int64_t ldxo = y_in_s ? b.Q.ld : b.S.ld;
+      done = fused_rr<T>(ctx, sm, eig, A, sign, Yq, ldq, b.AQ.data(), b.AQ.ld, Xo, ldxo, n,
+                         active, st);
+      if (done && y_in_s) {
+        FE_CHECK_CUDA(cudaMemcpy2DAsync(b.S.data(), b.S.ld * sizeof(T), b.Q.data(),
+                                        b.Q.ld * sizeof(T), active * sizeof(T), n,
+                                        cudaMemcpyDeviceToDevice, s));
+      }
       if (!done && cholqr2) {  // fall back to the second Cholesky QR pass
         cholqr<T>(ctx, sm, b.Q.data(), b.Q.ld, b.AQ.data(), b.AQ.ld, n, active, 1);
         FE_CHECK_CUDA(cudaMemcpy2DAsync(b.Q.data(), b.Q.ld * sizeof(T), b.AQ.data(),
@@ -814,6 +852,66 @@ struct ChebLoop {
     ev.accumulate(st);
   }
 
+  // Chebyshev filter of FP64 columns X whose Ritz values theta are known, computed to
+  // FP64 accuracy with FP32 SpMMs. With L = c op + d and t_k = T_k(L(theta_j)), the
+  // filtered column is y_m = T_m(L) x = t_m x + z_m where z_k = y_k - t_k x obeys
+  //   z_0 = 0, z_1 = c r, z_{k+1} = 2 L z_k - z_{k-1} + 2 c t_k r,  r = (op - theta) x,
+  // the three-term recurrence of the filter (src/ChebyshevSolver.cpp:243-256) with one
+  // extra term. r is formed once in FP64 and rounded to FP32; for a column near an
+  // eigenvector z is small against t_m x, so the FP32 rounding of the recurrence stays
+  // small against z and the result carries FP64-level accuracy, where an FP32 filter of
+  // x itself would carry FP32-level error relative to y.
+  void refined_filter(double* X, int64_t ldx, int64_t cols, double c, double d,
+                      const std::vector<double>& theta) {
+    cudaStream_t s = ctx.stream;
+    if (!r32.data()) {
+      r32.allocate(n, b.V.ld);
+      z0.allocate(n, b.V.ld);
+      z1.allocate(n, b.V.ld);
+    }
+    const int64_t cols4 = (cols + 3) / 4 * 4;  // 16-byte rows for the FP32 steps
+    const int64_t m = degree;
+    std::vector<float> delta(static_cast<size_t>(std::max<int64_t>(m - 1, 1)) * cols4, 0.0f);
+    std::vector<double> tm(static_cast<size_t>(cols), 1.0);
+    for (int64_t j = 0; j < cols; ++j) {
+      const double x = c * theta[j] + d;
+      double tprev = 1.0, tcur = x;
+      for (int64_t k = 1; k < m; ++k) {
+        delta[static_cast<size_t>(k - 1) * cols4 + j] = static_cast<float>(2.0 * c * tcur);
+        const double tn = 2.0 * x * tcur - tprev;
+        tprev = tcur;
+        tcur = tn;
+      }
+      tm[j] = tcur;
+    }
+    DeviceBuffer d_delta(delta.size() * sizeof(float)), d_tm(tm.size() * sizeof(double)),
+        d_theta(theta.size() * sizeof(double));
+    ctx.to_device(d_delta.as<float>(), delta.data(), delta.size());
+    ctx.to_device(d_tm.as<double>(), tm.data(), tm.size());
+    ctx.to_device(d_theta.as<double>(), theta.data(), theta.size());
+    const int64_t ld32 = r32.ld;
+    if (cols4 > cols) {
+      FE_CHECK_CUDA(cudaMemset2DAsync(r32.col(cols), ld32 * sizeof(float), 0,
+                                      (cols4 - cols) * sizeof(float), n, s));
+      FE_CHECK_CUDA(cudaMemset2DAsync(z1.col(cols), ld32 * sizeof(float), 0,
+                                      (cols4 - cols) * sizeof(float), n, s));
+    }
+    // r = op x - theta x (FP64 product, rounded once to FP32); z_1 = c r.
+    csr_spmm<double>(A, X, ldx, b.AQ.data(), b.AQ.ld, nullptr, 0, cols, sign, 0.0, 0.0, s);
+    refine_start(n, cols, b.AQ.data(), b.AQ.ld, X, ldx, d_theta.as<double>(), c, r32.data(),
+                 z1.data(), ld32, s);
+    float* prev = z0.data();
+    float* cur = z1.data();
+    for (int64_t k = 1; k < m; ++k) {
+      csr_spmm_corr_f32(A, cur, ld32, prev, ld32, prev, ld32, r32.data(), ld32,
+                        d_delta.as<float>() + (k - 1) * cols4, cols4, 2.0 * c * sign, 2.0 * d,
+                        k == 1 ? 0.0 : -1.0, s);
+      std::swap(prev, cur);
+    }
+    refine_finish(n, cols, d_tm.as<double>(), cur, ld32, X, ldx, s);
+    ctx.sync();  // the host tables are released on return
+  }
+
   void filter(T* X, int64_t ldx, T* Sc, int64_t lds, int64_t cols, double c, double d) {
     cudaStream_t s = ctx.stream;
     // Y1 = c*A*Y0 + d*Y0 into scratch; Y_k = 2c*A*Y_{k-1} + 2d*Y_{k-1} - Y_{k-2} in place.
@@ -862,6 +960,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
   const bool host_init = opt.init == "host";
   const bool mixed = opt.precision == "mixed";
   const bool fused_rr_on = opt.rr.empty() ? mixed : opt.rr == "fused";
+  const bool refine_on = mixed && opt.tail_filter == "refined";
 
   using clock = std::chrono::steady_clock;
   const auto t_start = clock::now();
@@ -942,6 +1041,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
       l32->iterate(locked, sub, cutoff, W, rel, info, st);
       st.fp32_iterations += 1;
     } else {
+      l64->theta_ready = sub_prev >= sub;  // every active column has a Ritz value
       l64->iterate(locked, sub, cutoff, W, rel, info, st);
       st.fp64_iterations += 1;
     }
@@ -982,6 +1082,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
       // FP32 residual floor reached: continue on FP64 blocks.
       l64.reset(new ChebLoop<double>(ctx, A, opt, sm, eig, sign, lower, upper, false));
       l64->fused = fused_rr_on;
+      l64->refine = refine_on;
       if (opt.tail_degree > 0) l64->degree = opt.tail_degree;
       l64->b.allocate(n, cap);
       convert<float, double>(l32->b.V.data(), l32->b.V.ld, l64->b.V.data(), l64->b.V.ld, n, cap,

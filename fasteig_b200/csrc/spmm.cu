@@ -228,13 +228,15 @@ csr_spmm_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
 // (alpha*a_ii + gamma); a row without a stored diagonal loads its X row.
 // Columns are split into panels of at most 96 vectors (CPL <= 3).
 // ---------------------------------------------------------------------------
-template <typename T, int VEC, int CPL, int NZ>
-__global__ void __launch_bounds__(kThreads)
-csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
-                    const int32_t* __restrict__ colind, const T* __restrict__ vals,
-                    const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
-                    int64_t ldz, int ncols, int panel_vec, T alpha, T gamma, T beta,
-                    int use_gamma, int use_beta, int prefetch_z) {
+// With CORR, every output also gains delta[j] * R[row, j] (the correction term of the
+// refined filter, see csr_spmm_corr).
+template <typename T, int VEC, int CPL, int NZ, bool CORR>
+__device__ __forceinline__ void csr_spmm_row_body(
+    int64_t nrows, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind,
+    const T* __restrict__ vals, const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy,
+    const T* Z, int64_t ldz, int ncols, int panel_vec, T alpha, T gamma, T beta, int use_gamma,
+    int use_beta, int prefetch_z, const T* __restrict__ R, int64_t ldr,
+    const T* __restrict__ delta) {
   constexpr unsigned kFull = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t tw = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
@@ -260,6 +262,14 @@ csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
   while (true) {
     const int nnz = e0 - s0;
     Pack<T, VEC> z[CPL];
+    Pack<T, VEC> rc[CPL];
+    if constexpr (CORR) {
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) {
+        const int v = lane + 32 * q;
+        if (v < nvec) rc[q] = load_pack_rw<T, VEC>(R + row * ldr + p0 + v * VEC);
+      }
+    }
     if (use_beta) {
 #pragma unroll
       for (int q = 0; q < CPL; ++q) {
@@ -396,6 +406,11 @@ csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
 #pragma unroll
         for (int e = 0; e < VEC; ++e)
           out.v[e] = use_beta ? fma(beta, z[q].v[e], acc[q][e]) : acc[q][e];
+        if constexpr (CORR) {
+          const Pack<T, VEC> dl = load_pack<T, VEC>(delta + p0 + v * VEC);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) out.v[e] = fma(dl.v[e], rc[q].v[e], out.v[e]);
+        }
         store_pack<T, VEC>(yr + v * VEC, out);
       }
     }
@@ -409,6 +424,34 @@ csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
     c_cur = c_n;
     a_cur = a_n;
   }
+}
+
+template <typename T, int VEC, int CPL, int NZ>
+__global__ void __launch_bounds__(kThreads)
+csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
+                    const int32_t* __restrict__ colind, const T* __restrict__ vals,
+                    const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
+                    int64_t ldz, int ncols, int panel_vec, T alpha, T gamma, T beta,
+                    int use_gamma, int use_beta, int prefetch_z) {
+  csr_spmm_row_body<T, VEC, CPL, NZ, false>(nrows, rowptr, colind, vals, X, ldx, Y, ldy, Z, ldz,
+                                            ncols, panel_vec, alpha, gamma, beta, use_gamma,
+                                            use_beta, prefetch_z, nullptr, 0, nullptr);
+}
+
+// The row kernel with the correction term delta[j] * R[row, j] added to every output
+// (the refined filter's recurrence, csr_spmm_corr_f32); register use bounded for two
+// CTAs per SM.
+template <typename T, int VEC, int CPL, int NZ>
+__global__ void __launch_bounds__(kThreads, 2)
+csr_spmm_row_corr_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
+                         const int32_t* __restrict__ colind, const T* __restrict__ vals,
+                         const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
+                         int64_t ldz, int ncols, int panel_vec, T alpha, T gamma, T beta,
+                         int use_gamma, int use_beta, const T* __restrict__ R, int64_t ldr,
+                         const T* __restrict__ delta) {
+  csr_spmm_row_body<T, VEC, CPL, NZ, true>(nrows, rowptr, colind, vals, X, ldx, Y, ldy, Z, ldz,
+                                           ncols, panel_vec, alpha, gamma, beta, use_gamma,
+                                           use_beta, 0, R, ldr, delta);
 }
 
 template <typename T, int VEC>
@@ -447,6 +490,54 @@ bool try_row_kernel(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, 
   else FE_ROW(5);
 #undef FE_ROW
   return true;
+}
+
+// Y[:, j] += delta[j] * R[:, j] (the correction term where the row kernel does not
+// apply).
+__global__ void col_scaled_add_kernel(int64_t n, int ncols, const float* __restrict__ R,
+                                      int64_t ldr, const float* __restrict__ delta,
+                                      float* __restrict__ Y, int64_t ldy) {
+  const int64_t total = n * ncols;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx / ncols;
+    const int j = static_cast<int>(idx % ncols);
+    Y[i * ldy + j] = fmaf(delta[j], R[i * ldr + j], Y[i * ldy + j]);
+  }
+}
+
+// Start of the refined filter: R32 = float(R64 - theta_j X) and Z1 = c * R32.
+__global__ void refine_start_kernel(int64_t n, int ncols, const double* __restrict__ R64,
+                                    int64_t ld64, const double* __restrict__ X, int64_t ldx,
+                                    const double* __restrict__ theta, double c,
+                                    float* __restrict__ R32, float* __restrict__ Z1,
+                                    int64_t ld32) {
+  const int64_t total = n * ncols;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx / ncols;
+    const int j = static_cast<int>(idx % ncols);
+    const double r = R64[i * ld64 + j] - theta[j] * X[i * ldx + j];
+    R32[i * ld32 + j] = static_cast<float>(r);
+    Z1[i * ld32 + j] = static_cast<float>(c * r);
+  }
+}
+
+// End of the refined filter: X = t_j X + Z (FP64).
+__global__ void refine_finish_kernel(int64_t n, int ncols, const double* __restrict__ t,
+                                     const float* __restrict__ Z, int64_t ld32,
+                                     double* __restrict__ X, int64_t ldx) {
+  const int64_t total = n * ncols;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx / ncols;
+    const int j = static_cast<int>(idx % ncols);
+    X[i * ldx + j] = fma(t[j], X[i * ldx + j], static_cast<double>(Z[i * ld32 + j]));
+  }
+}
+
+inline unsigned elementwise_grid(int64_t total) {
+  return static_cast<unsigned>(std::min<int64_t>((total + 255) / 256, int64_t(148) * 32));
 }
 
 template <typename T, int VEC, int G, int CPL>
@@ -973,6 +1064,80 @@ template int autotune_spmm<double>(Csr&, int64_t, cudaStream_t);
 template int autotune_spmm<float>(Csr&, int64_t, cudaStream_t);
 template void csr_spmm<float>(const Csr&, const float*, int64_t, float*, int64_t, const float*,
                               int64_t, int64_t, double, double, double, cudaStream_t);
+
+// Y = alpha A X + gamma X + beta Z + R diag(delta) on FP32 blocks: the Chebyshev step
+// of the refined filter's correction recurrence (see refined_filter in the solver).
+// The row-batched kernel carries the extra term in its store; where that kernel does
+// not apply, the step is followed by a separate column-scaled add.
+void csr_spmm_corr_f32(const Csr& A, const float* X, int64_t ldx, float* Y, int64_t ldy,
+                       const float* Z, int64_t ldz, const float* R, int64_t ldr,
+                       const float* delta, int64_t ncols, double alpha, double gamma, double beta,
+                       cudaStream_t s) {
+  if (ncols == 0 || A.rows == 0) return;
+  FE_REQUIRE(R && delta && ldr >= ncols, "csr_spmm_corr: invalid correction block");
+  constexpr int VEC = 2;  // 8-byte lanes, as the default row kernel
+  constexpr int NZ = 7;
+  const bool ub = beta != 0.0;
+  const int nvec = static_cast<int>(ncols / VEC);
+  const bool ok = ncols % 4 == 0 && ldx % 4 == 0 && ldy % 4 == 0 && ldr % 4 == 0 &&
+                  aligned16(X) && aligned16(Y) && aligned16(R) && aligned16(delta) &&
+                  (!ub || (ldz % 4 == 0 && aligned16(Z))) && nvec >= 32 && A.max_row_nnz <= NZ &&
+                  !ranges_overlap(X, A.cols, ldx, ncols, static_cast<const float*>(Y), A.rows,
+                                  ldy, ncols);
+  if (!ok) {
+    csr_spmm<float>(A, X, ldx, Y, ldy, Z, ldz, ncols, alpha, gamma, beta, s);
+    col_scaled_add_kernel<<<elementwise_grid(A.rows * ncols), 256, 0, s>>>(
+        A.rows, static_cast<int>(ncols), R, ldr, delta, Y, ldy);
+    check_launch("col_scaled_add_kernel");
+    return;
+  }
+  const int max_cpl = 5;
+  const int panels = (nvec + 32 * max_cpl - 1) / (32 * max_cpl);
+  const int panel_vec = (nvec + panels - 1) / panels;
+  const int cpl = (panel_vec + 31) / 32;
+#define FE_ROWC(CPL_)                                                                          \
+  do {                                                                                         \
+    auto kern = csr_spmm_row_corr_kernel<float, VEC, CPL_, NZ>;                                \
+    static int resident = 0;                                                                   \
+    if (resident == 0) {                                                                       \
+      FE_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, kThreads,   \
+                                                                  0));                         \
+      resident = std::max(resident, 1);                                                        \
+    }                                                                                          \
+    int64_t blocks = std::min<int64_t>((A.rows + 7) / 8,                                       \
+                                       static_cast<int64_t>(num_sms()) * resident);            \
+    blocks = std::max<int64_t>(blocks, 1);                                                     \
+    dim3 grid(static_cast<unsigned>(blocks), static_cast<unsigned>(panels));                   \
+    kern<<<grid, kThreads, 0, s>>>(A.rows, A.rowptr, A.colind, A.val32, X, ldx, Y, ldy, Z, ldz, \
+                                   static_cast<int>(ncols), panel_vec, static_cast<float>(alpha), \
+                                   static_cast<float>(gamma), static_cast<float>(beta),        \
+                                   gamma != 0.0 ? 1 : 0, ub ? 1 : 0, R, ldr, delta);           \
+    check_launch("csr_spmm_row_corr_kernel");                                                  \
+  } while (0)
+  if (cpl == 1) FE_ROWC(1);
+  else if (cpl == 2) FE_ROWC(2);
+  else if (cpl == 3) FE_ROWC(3);
+  else if (cpl == 4) FE_ROWC(4);
+  else FE_ROWC(5);
+#undef FE_ROWC
+}
+
+void refine_start(int64_t n, int64_t ncols, const double* R64, int64_t ld64, const double* X,
+                  int64_t ldx, const double* theta, double c, float* R32, float* Z1,
+                  int64_t ld32, cudaStream_t s) {
+  if (n <= 0 || ncols <= 0) return;
+  refine_start_kernel<<<elementwise_grid(n * ncols), 256, 0, s>>>(
+      n, static_cast<int>(ncols), R64, ld64, X, ldx, theta, c, R32, Z1, ld32);
+  check_launch("refine_start_kernel");
+}
+
+void refine_finish(int64_t n, int64_t ncols, const double* t, const float* Z, int64_t ld32,
+                   double* X, int64_t ldx, cudaStream_t s) {
+  if (n <= 0 || ncols <= 0) return;
+  refine_finish_kernel<<<elementwise_grid(n * ncols), 256, 0, s>>>(
+      n, static_cast<int>(ncols), t, Z, ld32, X, ldx);
+  check_launch("refine_finish_kernel");
+}
 
 // In-place filter of degree `degree`: X <- T_degree(c*A + d*I) X, scratch holds Y_{k-1}.
 template <typename T>

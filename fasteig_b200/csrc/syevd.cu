@@ -121,24 +121,27 @@ sytrd_kernel(const int32_t* __restrict__ msz, double* __restrict__ A, int64_t ld
     }
     __syncthreads();
     if (t == 0.0) continue;
-    // p = tau A22 v  (thread per row; column-major loads are coalesced over rows)
-    part = 0.0;
-    for (int i = tid; i < m; i += blockDim.x) {
+    // p = tau A22 v. A22 is symmetric, so p_i is column i of A22 (contiguous in
+    // column-major storage) dotted with v: one warp per column, lanes along it.
+    const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
+    for (int i = warp; i < m; i += nwarps) {
+      const double* col = M + (o + 1 + i) * ldm + (o + 1);
       double acc = 0.0;
-      const double* col = M + (o + 1) * ldm + (o + 1 + i);
-      for (int l = 0; l < m; ++l) acc = fma(col[l * ldm], v[l], acc);
-      acc *= t;
-      w[i] = acc;
-      part += acc * v[i];
+      for (int l = lane; l < m; l += 32) acc = fma(col[l], v[l], acc);
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (lane == 0) w[i] = t * acc;
     }
+    __syncthreads();
+    part = 0.0;
+    for (int i = tid; i < m; i += blockDim.x) part += w[i] * v[i];
     const double K = 0.5 * t * block_sum(part, red);
     for (int i = tid; i < m; i += blockDim.x) w[i] = w[i] - K * v[i];
     __syncthreads();
-    // A22 -= v w^T + w v^T
-    for (int i = tid; i < m; i += blockDim.x) {
-      const double vi = v[i], wi = w[i];
-      double* col = M + (o + 1) * ldm + (o + 1 + i);
-      for (int l = 0; l < m; ++l) col[l * ldm] -= vi * w[l] + wi * v[l];
+    // A22 -= v w^T + w v^T: one warp per column, lanes along it.
+    for (int l = warp; l < m; l += nwarps) {
+      double* col = M + (o + 1 + l) * ldm + (o + 1);
+      const double vl = v[l], wl = w[l];
+      for (int i = lane; i < m; i += 32) col[i] -= v[i] * wl + w[i] * vl;
     }
     __syncthreads();
   }
@@ -160,11 +163,16 @@ __device__ __forceinline__ void gershgorin(const double* d, const double* e, int
   gl = 1e308;
   gu = -1e308;
   double emax = 0.0;
+  bool finite = true;
   for (int i = 0; i < k; ++i) {
+    finite = finite && isfinite(d[i]) && (i + 1 >= k || isfinite(e[i]));
     const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < k ? fabs(e[i]) : 0.0);
     gl = fmin(gl, d[i] - r);
     gu = fmax(gu, d[i] + r);
     if (i + 1 < k) emax = fmax(emax, e[i] * e[i]);
+  }
+  if (!finite) {  // fmin/fmax drop NaN: report non-finite data through the bounds
+    gl = gu = nan("");
   }
   tnorm = fmax(fabs(gl), fabs(gu));
   pivmin = kTiny * fmax(1.0, emax);

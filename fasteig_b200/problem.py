@@ -20,7 +20,7 @@ _INT_KEYS = ("n", "nev", "maxiter", "maxdim", "maxblks", "degree", "blksize", "v
              "print_every", "block", "tensor_cores", "tail_degree", "inject_wait_timeout")
 _FLOAT_KEYS = ("tol", "shift", "amplification", "mixed_switch")
 _STR_KEYS = ("which", "solver", "precision", "bounds", "init", "logfile", "output_format",
-             "precond", "locking", "rr")
+             "precond", "locking", "rr", "tail_filter")
 
 
 class fasteig_options:  # noqa: N801 - reference class name
