@@ -2226,7 +2226,7 @@ void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* 
   expand(0);
   std::unique_ptr<ProjectedEig> deig;
   DeviceBuffer Td;
-  if (m > 96) {  // large projected matrices: cuSOLVER on the device
+  if (m > 96) {  // large projected matrices: the device eigensolver
     deig.reset(new ProjectedEig(ctx, m));
     Td.resize(static_cast<size_t>(m) * m * sizeof(double));
   }
@@ -2316,6 +2316,371 @@ void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* 
     expand(retained);
   }
   throw Error(FE_ERR_INVALID, "KrylovSchurSolver: unreachable solve termination.");
+}
+
+// ===========================================================================
+// Block Krylov-Schur: BlockKrylovSchurSolver::solve (src/BlockKrylovSchurSolver.cpp:26-215)
+// for standard problems, on the device block kernels: the BlockKrylovSubspace
+// expansion (src/core/KrylovSubspace.cpp:261-437: block SpMM, two-pass block
+// Gram-Schmidt, complete_block_qr of the residual block), the block-tridiagonal
+// projection (src/core/LanczosWorkspace.cpp:42-73), residual estimates from the last
+// coupling block (src/core/RitzExtraction.cpp:272-380), and the thick block restart
+// (src/core/LanczosWorkspace.cpp:109-135). Large blocks stay on the device; the
+// projected matrix and the b x b couplings are small host arrays, as in the reference.
+// ===========================================================================
+void block_krylov_schur_solve(const Csr& A, const Options& opt, double* eigenvalues,
+                              double* residuals, double* eigenvectors, Stats& st) {
+  const int64_t n = A.rows, nev = opt.nev, b = opt.blksize;
+  const std::string which = opt.which;
+  if (n <= 0) throw Error(FE_ERR_INVALID, "BlockKrylovSchurSolver: n must be > 0.");
+  if (nev <= 0 || nev > n)
+    throw Error(FE_ERR_INVALID, "BlockKrylovSchurSolver: nev must be in [1,n].");
+  if (opt.maxiter <= 0) throw Error(FE_ERR_INVALID, "BlockKrylovSchurSolver: maxiter must be > 0.");
+  if (which == "sai")
+    throw Error(FE_ERR_UNSUPPORTED,
+                "BlockKrylovSchurSolver: SAI needs a shift-invert factorization (out of scope here).");
+  if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
+    throw Error(FE_ERR_INVALID, "BlockKrylovSchurSolver: invalid which option.");
+  if (b <= 0 || b > n) throw Error(FE_ERR_INVALID, "BlockKrylovSchurSolver: blksize must be in [1,n].");
+  const int64_t requested_dim = opt.maxdim > 0 ? opt.maxdim : std::max<int64_t>(2 * nev, 20);
+  const int64_t block_count = requested_dim >= n ? 1 + (n - 1) / b : requested_dim / b;
+  const int64_t cycle_dim = std::min(n, block_count * b);
+  const int64_t wanted_blocks = 1 + (nev - 1) / b;
+  if (cycle_dim < n && block_count <= wanted_blocks)
+    throw Error(FE_ERR_INVALID,
+                "BlockKrylovSchurSolver: maxdim must accommodate ceil(nev/blksize) retained blocks "
+                "plus at least one expansion block (or the full matrix dimension).");
+  const int64_t pdim = (block_count + 1) * b;  // projection dimension
+  const int64_t retained_blocks = cycle_dim == n ? 0 : std::max(wanted_blocks, block_count / 2);
+  const int64_t retained_dim = retained_blocks * b;
+  const int64_t snapshot_count = std::max(nev, retained_dim);
+  const unsigned seed = opt.seed_or_default();
+  const bool host_init = opt.init == "host";
+  Context ctx;
+  cudaStream_t s = ctx.stream;
+  SmallState sm;
+  sm.allocate(n, pdim, false);
+  Block<double> V, Z, Rb, Qb, Y, one, best;
+  V.allocate(n, pdim);
+  Z.allocate(n, b);
+  Rb.allocate(n, b);
+  Qb.allocate(n, b);
+  Y.allocate(n, std::max<int64_t>(snapshot_count, b));
+  one.allocate(n, 1);
+  best.allocate(n, 1);
+  const int64_t ld = V.ld;
+  DeviceBuffer hdev(static_cast<size_t>(pdim) * b * sizeof(double)),
+      h2dev(static_cast<size_t>(pdim) * b * sizeof(double)), nrm(sizeof(double)),
+      Cd(static_cast<size_t>(pdim) * pdim * sizeof(double));
+  FE_CHECK_CUDA(cudaMemsetAsync(V.data(), 0, static_cast<size_t>(n) * ld * sizeof(double), s));
+  auto host_random = [&](double* dst, int64_t ldd, int64_t cols, unsigned sd) {
+    // Executor::create_random_multivector / create_random_vector (src/core/Executor.cpp:20-62)
+    std::mt19937 rng(sd);
+    std::uniform_real_distribution<double> dist(-1.0, 1.0);
+    std::vector<double> host(static_cast<size_t>(n) * ldd, 0.0);
+    for (int64_t j = 0; j < cols; ++j)
+      for (int64_t i = 0; i < n; ++i) host[static_cast<size_t>(i) * ldd + j] = dist(rng);
+    ctx.to_device(dst, host.data(), host.size());
+    ctx.sync();
+  };
+  auto vnorm = [&](const double* x, int64_t incx) {
+    residual_norms<double>(nullptr, x, nullptr, incx, n, 1, nullptr, nullptr, 0, nullptr,
+                           nrm.as<double>(), nullptr, sm.rws.get(), sm.rws.bytes(), s, 0);
+    double r = 0;
+    ctx.to_host(&r, nrm.as<double>(), 1);
+    ctx.sync();
+    return r;
+  };
+  // Two-pass classical Gram-Schmidt of the column x (stride ldx) against W[:, :k].
+  auto cgs2 = [&](const double* W, int64_t ldw, int64_t k, double* x, int64_t ldx) {
+    if (k == 0) return;
+    for (int pass = 0; pass < 2; ++pass) {
+      gram<double>(W, ldw, x, ldx, n, k, 1, hdev.as<double>(), k, sm.gws.get(), sm.gws.bytes(), s);
+      rotate<double>(W, ldw, hdev.as<double>(), k, x, ldx, n, k, 1, -1.0, 1.0, s);
+    }
+  };
+  // complete_block_qr (src/core/Orthogonalization.cpp:609-715) of src (n x b) against
+  // V[:, :active] into Q (n x b); R (b x b, column-major host) gets the coupling.
+  auto complete_block_qr = [&](int64_t active, const double* src, int64_t lds, double* Q,
+                               int64_t ldq, unsigned sd, double reference_norm,
+                               std::vector<double>& R) {
+    const int64_t capacity = std::min(b, n - active);
+    const double threshold = 64.0 * std::numeric_limits<double>::epsilon() * reference_norm;
+    R.assign(static_cast<size_t>(b) * b, 0.0);
+    if (capacity == b) {
+      double* G = sm.G.as<double>();
+      int32_t* info = sm.info.as<int32_t>();
+      FE_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int32_t), s));
+      gram<double>(src, lds, src, lds, n, b, b, G, pdim, sm.gws.get(), sm.gws.bytes(), s);
+      potrf_upper(G, b, pdim, info, s);
+      int32_t h = 0;
+      std::vector<double> Rh(static_cast<size_t>(pdim) * b);
+      ctx.to_host(&h, info, 1);
+      ctx.to_host(Rh.data(), G, Rh.size());
+      ctx.sync();
+      if (h == 0) {
+        trinv_upper(G, pdim, sm.Rinv.as<double>(), pdim, b, s);
+        rotate<double>(src, lds, sm.Rinv.as<double>(), pdim, Q, ldq, n, b, b, 1.0, 0.0, s,
+                       /*upper_tri=*/true);
+        std::vector<double> g(static_cast<size_t>(b) * b), c(static_cast<size_t>(std::max<int64_t>(active, 1)) * b);
+        gram<double>(Q, ldq, Q, ldq, n, b, b, hdev.as<double>(), b, sm.gws.get(), sm.gws.bytes(), s);
+        ctx.to_host(g.data(), hdev.as<double>(), g.size());
+        if (active > 0) {
+          gram<double>(V.data(), ld, Q, ldq, n, active, b, h2dev.as<double>(), active,
+                       sm.gws.get(), sm.gws.bytes(), s);
+          ctx.to_host(c.data(), h2dev.as<double>(), static_cast<size_t>(active) * b);
+        }
+        ctx.sync();
+        double mind = std::numeric_limits<double>::infinity(), gerr = 0.0, cerr = 0.0;
+        bool finite = true;
+        for (int64_t j = 0; j < b; ++j) {
+          for (int64_t i = 0; i <= j; ++i) {
+            const double r = Rh[static_cast<size_t>(j) * pdim + i];
+            finite = finite && std::isfinite(r);
+            R[static_cast<size_t>(j) * b + i] = r;
+          }
+          mind = std::min(mind, std::fabs(R[static_cast<size_t>(j) * b + j]));
+          for (int64_t i = 0; i < b; ++i) {
+            const double v = g[static_cast<size_t>(j) * b + i] - (i == j ? 1.0 : 0.0);
+            finite = finite && std::isfinite(v);
+            gerr += v * v;
+          }
+        }
+        for (int64_t e = 0; e < active * b; ++e) {
+          finite = finite && std::isfinite(c[e]);
+          cerr += c[e] * c[e];
+        }
+        if (finite && mind > threshold && std::sqrt(gerr) < 1e-10 && std::sqrt(cerr) < 1e-10)
+          return false;
+      }
+    }
+    // Rank loss: two-pass projection column by column, filling missing directions.
+    bool replenished = false;
+    FE_CHECK_CUDA(cudaMemset2DAsync(Q, ldq * sizeof(double), 0, b * sizeof(double), n, s));
+    for (int64_t j = 0; j < capacity; ++j) {
+      double length = 0.0, original_scale = 0.0;
+      bool have = false;
+      for (int64_t col = 0; col < b; ++col) {
+        FE_CHECK_CUDA(cudaMemcpy2DAsync(one.data(), one.ld * sizeof(double), src + col,
+                                        lds * sizeof(double), sizeof(double), n,
+                                        cudaMemcpyDeviceToDevice, s));
+        original_scale = std::max(original_scale, vnorm(one.data(), one.ld));
+        cgs2(V.data(), ld, active, one.data(), one.ld);
+        cgs2(Q, ldq, j, one.data(), one.ld);
+        const double cn = vnorm(one.data(), one.ld);
+        if (cn > length) {
+          length = cn;
+          have = true;
+          FE_CHECK_CUDA(cudaMemcpy2DAsync(best.data(), best.ld * sizeof(double), one.data(),
+                                          one.ld * sizeof(double), sizeof(double), n,
+                                          cudaMemcpyDeviceToDevice, s));
+        }
+      }
+      const double cutoff = std::max(threshold, 1e-12 * original_scale);
+      if (have && length > cutoff) {
+        FE_CHECK_CUDA(cudaMemcpy2DAsync(one.data(), one.ld * sizeof(double), best.data(),
+                                        best.ld * sizeof(double), sizeof(double), n,
+                                        cudaMemcpyDeviceToDevice, s));
+        length = vnorm(one.data(), one.ld);
+      }
+      if (!(length > cutoff)) {
+        replenished = true;
+        length = 0.0;
+        for (unsigned attempt = 0; attempt < 4; ++attempt) {
+          host_random(one.data(), one.ld, 1, sd + 17u * static_cast<unsigned>(j + 1) + attempt);
+          const double rn = vnorm(one.data(), one.ld);
+          cgs2(V.data(), ld, active, one.data(), one.ld);
+          cgs2(Q, ldq, j, one.data(), one.ld);
+          length = vnorm(one.data(), one.ld);
+          if (length > 1e-12 * rn) break;
+          length = 0.0;
+        }
+        if (length == 0.0)
+          throw Error(FE_ERR_NONFINITE, "complete_block_qr: unable to complete the basis.");
+      }
+      vec_axpby(n, 1.0 / length, one.data(), one.ld, 0.0, Q + j, ldq, s);
+    }
+    gram<double>(Q, ldq, src, lds, n, b, b, hdev.as<double>(), b, sm.gws.get(), sm.gws.bytes(), s);
+    ctx.to_host(R.data(), hdev.as<double>(), R.size());
+    ctx.sync();
+    for (int64_t j = 0; j < b; ++j) {
+      double c2 = 0.0;
+      for (int64_t i = 0; i < b; ++i) c2 += R[static_cast<size_t>(j) * b + i] * R[static_cast<size_t>(j) * b + i];
+      if (std::sqrt(c2) <= threshold)
+        for (int64_t i = 0; i < b; ++i) R[static_cast<size_t>(j) * b + i] = 0.0;
+    }
+    return replenished;
+  };
+
+  std::vector<double> T(static_cast<size_t>(pdim) * pdim, 0.0), beta(static_cast<size_t>(b) * b, 0.0);
+  auto t = [&](int64_t r, int64_t c) -> double& { return T[static_cast<size_t>(c) * pdim + r]; };
+  // initialize_basis_block: the seeded block, completed to an orthonormal block.
+  {
+    if (host_init) host_random(Z.data(), Z.ld, b, seed);
+    else fill_uniform<double>(Z.data(), Z.ld, n, b, seed, s);
+    std::vector<double> R0;
+    complete_block_qr(0, Z.data(), Z.ld, V.data(), ld, seed, 0.0, R0);
+  }
+  auto expand = [&](int64_t first_block) {
+    for (int64_t blk = first_block; blk < block_count; ++blk) {
+      csr_spmm<double>(A, V.col(blk * b), ld, Z.data(), Z.ld, nullptr, 0, b, 1.0, 0.0, 0.0, s);
+      st.spmm_launches += 1;
+      const int64_t active = std::min(n, (blk + 1) * b);
+      // block_gram_schmidt (src/core/Orthogonalization.cpp:482-527): two passes.
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(Rb.data(), Rb.ld * sizeof(double), Z.data(),
+                                      Z.ld * sizeof(double), b * sizeof(double), n,
+                                      cudaMemcpyDeviceToDevice, s));
+      std::vector<double> H(static_cast<size_t>(active) * b, 0.0), H2(H.size());
+      gram<double>(V.data(), ld, Rb.data(), Rb.ld, n, active, b, hdev.as<double>(), active,
+                   sm.gws.get(), sm.gws.bytes(), s);
+      rotate<double>(V.data(), ld, hdev.as<double>(), active, Rb.data(), Rb.ld, n, active, b, -1.0,
+                     1.0, s);
+      gram<double>(V.data(), ld, Rb.data(), Rb.ld, n, active, b, h2dev.as<double>(), active,
+                   sm.gws.get(), sm.gws.bytes(), s);
+      rotate<double>(V.data(), ld, h2dev.as<double>(), active, Rb.data(), Rb.ld, n, active, b,
+                     -1.0, 1.0, s);
+      ctx.to_host(H.data(), hdev.as<double>(), H.size());
+      ctx.to_host(H2.data(), h2dev.as<double>(), H2.size());
+      // ||column norms of Z|| for the rank threshold of the residual QR
+      std::vector<double> zn(b);
+      residual_norms<double>(nullptr, Z.data(), nullptr, Z.ld, n, b, nullptr, nullptr, 0, nullptr,
+                             sm.xnorm.as<double>(), nullptr, sm.rws.get(), sm.rws.bytes(), s, 0);
+      ctx.to_host(zn.data(), sm.xnorm.as<double>(), b);
+      ctx.sync();
+      double scale = 0.0;
+      for (double x : zn) scale += x * x;
+      scale = std::sqrt(scale);
+      const int64_t width = 1 + (active - 1) % b;
+      const int64_t row = blk * b, nrow = (blk + 1) * b;
+      for (int64_t c = 0; c < b; ++c)
+        for (int64_t r = 0; r < b; ++r) t(row + r, row + c) = 0.0;
+      for (int64_t c = 0; c < width; ++c)
+        for (int64_t r = 0; r < width; ++r) {
+          const size_t e = static_cast<size_t>(c) * active + (active - width + r);
+          t(row + r, row + c) = H[e] + H2[e];
+        }
+      std::vector<double> R;
+      complete_block_qr(std::min(nrow, n), Rb.data(), Rb.ld, V.col(nrow), ld,
+                        seed + static_cast<unsigned>(nrow), scale, R);
+      for (int64_t c = 0; c < b; ++c)
+        for (int64_t r = 0; r < b; ++r) {
+          const double v = R[static_cast<size_t>(c) * b + r];
+          t(nrow + r, row + c) = v;
+          t(row + c, nrow + r) = v;
+        }
+      beta = R;
+    }
+  };
+  expand(0);
+  std::unique_ptr<ProjectedEig> deig;
+  DeviceBuffer Td;
+  if (cycle_dim > 96) {
+    deig.reset(new ProjectedEig(ctx, cycle_dim));
+    Td.resize(static_cast<size_t>(cycle_dim) * cycle_dim * sizeof(double));
+  }
+  const int64_t m = cycle_dim;
+  for (int64_t iter = 1; iter <= opt.maxiter; ++iter) {
+    std::vector<double> Tm(static_cast<size_t>(m) * m), lam, Zm;
+    for (int64_t c = 0; c < m; ++c)
+      for (int64_t r = 0; r < m; ++r) Tm[static_cast<size_t>(c) * m + r] = t(r, c);
+    if (deig) {
+      ctx.to_device(Td.as<double>(), Tm.data(), Tm.size());
+      deig->run(Td.as<double>(), m, m, sm.W.as<double>());
+      lam.resize(m);
+      Zm.resize(Tm.size());
+      ctx.to_host(lam.data(), sm.W.as<double>(), m);
+      ctx.to_host(Zm.data(), Td.as<double>(), Zm.size());
+      ctx.sync();
+    } else {
+      host_symmetric_eig(Tm, static_cast<int>(m), lam, Zm);
+    }
+    const std::vector<int32_t> idx = select_indices(lam, which);
+    const int64_t cnt = std::min(snapshot_count, m);
+    const int64_t tail = 1 + (m - 1) % b;
+    std::vector<double> lam_s(cnt), rel_s(cnt);
+    for (int64_t j = 0; j < cnt; ++j) {
+      lam_s[j] = lam[idx[j]];
+      // || beta * y_last ||, y_last = the eigenvector's last `tail` rows (zero padded)
+      double a2 = 0.0;
+      for (int64_t r = 0; r < b; ++r) {
+        double acc = 0.0;
+        for (int64_t c = 0; c < tail; ++c)
+          acc += beta[static_cast<size_t>(c) * b + r] *
+                 Zm[static_cast<size_t>(idx[j]) * m + (m - tail + c)];
+        a2 += acc * acc;
+      }
+      rel_s[j] = std::sqrt(a2) / (1.0 + std::fabs(lam_s[j]));
+    }
+    const int64_t k = std::min(nev, cnt);
+    double worst = 0.0;
+    for (int64_t j = 0; j < k; ++j) worst = std::max(worst, rel_s[j]);
+    bool converged = k > 0 && worst < opt.tol;
+    const bool at_limit = iter == opt.maxiter || cycle_dim == n;
+    if (opt.verbosity >= 2)
+      std::fprintf(stderr, "[fe] block krylov-schur restart %lld worst %.3e\n",
+                   static_cast<long long>(iter), worst);
+    if (converged || at_limit) {
+      std::vector<double> Cs(static_cast<size_t>(m) * k);
+      for (int64_t j = 0; j < k; ++j)
+        std::memcpy(&Cs[static_cast<size_t>(j) * m], &Zm[static_cast<size_t>(idx[j]) * m],
+                    m * sizeof(double));
+      ctx.to_device(Cd.as<double>(), Cs.data(), Cs.size());
+      rotate<double>(V.data(), ld, Cd.as<double>(), m, Y.data(), Y.ld, n, m, k, 1.0, 0.0, s);
+      std::vector<double> vals(lam_s.begin(), lam_s.begin() + k), res(k);
+      std::vector<double> vecs;
+      if (eigenvectors) vecs.resize(static_cast<size_t>(n) * k);
+      finish_results(ctx, sm, A, nullptr, Y.data(), Y.ld, n, k, vals.data(), res.data(),
+                     eigenvectors ? vecs.data() : nullptr);
+      converged = true;
+      for (double r : res) converged = converged && r <= opt.tol;
+      if (converged || at_limit) {
+        for (int64_t j = 0; j < k; ++j) {
+          eigenvalues[j] = vals[j];
+          residuals[j] = res[j];
+        }
+        if (eigenvectors) std::memcpy(eigenvectors, vecs.data(), vecs.size() * sizeof(double));
+        st.status = converged ? 0 : 1;
+        st.iterations = static_cast<double>(iter);
+        st.fp64_iterations = static_cast<double>(iter);
+        return;
+      }
+    }
+    // Thick block restart: V = [V C_keep, Q_residual], T = [diag(theta), F^T; F, .],
+    // F = beta * C_keep(last b rows).
+    std::vector<double> Cr(static_cast<size_t>(m) * retained_dim), F(static_cast<size_t>(b) * retained_dim);
+    for (int64_t j = 0; j < retained_dim; ++j) {
+      std::memcpy(&Cr[static_cast<size_t>(j) * m], &Zm[static_cast<size_t>(idx[j]) * m],
+                  m * sizeof(double));
+      for (int64_t r = 0; r < b; ++r) {
+        double acc = 0.0;
+        for (int64_t c = 0; c < b; ++c)
+          acc += beta[static_cast<size_t>(c) * b + r] * Cr[static_cast<size_t>(j) * m + (m - b + c)];
+        F[static_cast<size_t>(j) * b + r] = acc;
+      }
+    }
+    ctx.to_device(Cd.as<double>(), Cr.data(), Cr.size());
+    rotate<double>(V.data(), ld, Cd.as<double>(), m, Y.data(), Y.ld, n, m, retained_dim, 1.0, 0.0,
+                   s);
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(Qb.data(), Qb.ld * sizeof(double), V.col(block_count * b),
+                                    ld * sizeof(double), b * sizeof(double), n,
+                                    cudaMemcpyDeviceToDevice, s));
+    FE_CHECK_CUDA(cudaMemsetAsync(V.data(), 0, static_cast<size_t>(n) * ld * sizeof(double), s));
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(V.data(), ld * sizeof(double), Y.data(), Y.ld * sizeof(double),
+                                    retained_dim * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(V.col(retained_dim), ld * sizeof(double), Qb.data(),
+                                    Qb.ld * sizeof(double), b * sizeof(double), n,
+                                    cudaMemcpyDeviceToDevice, s));
+    std::fill(T.begin(), T.end(), 0.0);
+    for (int64_t j = 0; j < retained_dim; ++j) {
+      t(j, j) = lam_s[j];
+      for (int64_t r = 0; r < b; ++r) {
+        t(retained_dim + r, j) = F[static_cast<size_t>(j) * b + r];
+        t(j, retained_dim + r) = F[static_cast<size_t>(j) * b + r];
+      }
+    }
+    expand(retained_blocks);
+  }
+  throw Error(FE_ERR_INVALID, "BlockKrylovSchurSolver: unreachable solve termination.");
 }
 
 // ===========================================================================
@@ -2679,6 +3044,10 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
     } else {
       davidson_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
     }
+  } else if (opt.solver == "blockkrylovschur") {
+    FE_REQUIRE(B == nullptr,
+               "BlockKrylovSchurSolver: generalized problems are not supported on this backend.");
+    block_krylov_schur_solve(A, opt, eigenvalues, residual_norms, eigenvectors, st);
   } else if (opt.solver == "krylovschur") {
     if (B) check_pair(A, *B);
     krylov_schur_solve(A, B, opt, eigenvalues, residual_norms, eigenvectors, st);
@@ -2738,6 +3107,10 @@ size_t solve_memory_bytes(const Csr& A, const Csr* B, const char* options) {
   } else if (opt.solver == "davidson") {
     cap = std::min<int64_t>(n, opt.maxblks * std::max<int64_t>(nev, opt.block));
     blocks = 11;
+  } else if (opt.solver == "blockkrylovschur") {
+    const int64_t b = std::max<int64_t>(1, opt.blksize);
+    cap = std::min<int64_t>(opt.maxdim > 0 ? opt.maxdim : std::max<int64_t>(2 * nev, 20), n) + b;
+    blocks = 2 + 5.0 * static_cast<double>(b) / static_cast<double>(cap);
   } else {
     cap = std::min<int64_t>(std::max<int64_t>({2 * nev, 20, opt.maxdim}), n);
     blocks = 3;

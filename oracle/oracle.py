@@ -940,6 +940,165 @@ def krylov_schur_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
     raise RuntimeError("KrylovSchurSolver: unreachable solve termination.")
 
 
+def _cgs2(V: np.ndarray, k: int, src: np.ndarray) -> np.ndarray:
+    """Two-pass classical Gram-Schmidt of one vector against V[:, :k]
+    (CpuMultiVector::orthogonalize_active_columns, src/core/MultiVector.cpp:153-185)."""
+    if k == 0:
+        return src.copy()
+    Vk = V[:, :k]
+    r = src - Vk @ (Vk.T @ src)
+    return r - Vk @ (Vk.T @ r)
+
+
+def complete_block_qr(basis: np.ndarray, active_cols: int, source: np.ndarray, seed: int,
+                      reference_norm: float):
+    """complete_block_qr (src/core/Orthogonalization.cpp:609-715), standard inner product.
+    Returns (replenished, Q, R)."""
+    n, b = source.shape
+    capacity = min(b, n - active_cols)
+    threshold = 64.0 * EPS * reference_norm
+    if capacity == b:
+        info, Q, R = cholesky_qr(source.copy())
+        if info == 0:
+            gram = Q.T @ Q
+            cross = basis[:, :active_cols].T @ Q
+            if (np.all(np.isfinite(R)) and np.abs(np.diag(R)).min() > threshold and
+                    np.all(np.isfinite(gram)) and np.all(np.isfinite(cross)) and
+                    np.linalg.norm(gram - np.eye(b)) < 1e-10 and np.linalg.norm(cross) < 1e-10):
+                return False, Q, R
+    replenished = False
+    Q = np.zeros((n, b))
+
+    def project(v, j):
+        return _cgs2(Q, j, _cgs2(basis, active_cols, v))
+
+    for j in range(capacity):
+        length, original_scale, best = 0.0, 0.0, None
+        for col in range(b):
+            v = source[:, col].copy()
+            original_scale = max(original_scale, float(np.linalg.norm(v)))
+            v = project(v, j)
+            cn = float(np.linalg.norm(v))
+            if cn > length:
+                length, best = cn, v.copy()
+        cutoff = max(threshold, 1e-12 * original_scale)
+        if length > cutoff:
+            v = best
+            length = float(np.linalg.norm(v))
+        if not (length > cutoff):
+            replenished = True
+            length = 0.0
+            for attempt in range(4):
+                v = random_vector(n, seed + 17 * (j + 1) + attempt)
+                rn = float(np.linalg.norm(v))
+                v = project(v, j)
+                length = float(np.linalg.norm(v))
+                if length > 1e-12 * rn:
+                    break
+                length = 0.0
+            if length == 0.0:
+                raise RuntimeError("complete_block_qr: unable to complete the basis.")
+        Q[:, j] = v / length
+    R = Q.T @ source
+    R[:, np.linalg.norm(R, axis=0) <= threshold] = 0.0
+    return replenished, Q, R
+
+
+def block_krylov_schur_solve(A: Csr, nev: int, blksize: int, tol: float = 1e-8,
+                             maxiter: int = 1000, which: str = "sr", seed: int = 1,
+                             maxdim: int = 0) -> SolveResult:
+    """BlockKrylovSchurSolver::solve (src/BlockKrylovSchurSolver.cpp:26-215) for standard
+    problems: BlockKrylovSubspace expansion (src/core/KrylovSubspace.cpp:261-437: block
+    apply, two-pass block Gram-Schmidt, complete_block_qr of the residual block),
+    block-tridiagonal projection (src/core/LanczosWorkspace.cpp:42-73), Ritz residual
+    estimates from the coupling block (src/core/RitzExtraction.cpp:272-380) and the thick
+    block restart (src/core/LanczosWorkspace.cpp:109-135)."""
+    n = A.rows
+    which = which.lower()
+    if n <= 0:
+        raise ValueError("BlockKrylovSchurSolver: n must be > 0.")
+    if nev <= 0 or nev > n:
+        raise ValueError("BlockKrylovSchurSolver: nev must be in [1,n].")
+    if maxiter <= 0:
+        raise ValueError("BlockKrylovSchurSolver: maxiter must be > 0.")
+    if which not in ("sr", "lr", "sm", "lm", "be"):
+        raise ValueError("BlockKrylovSchurSolver: invalid which option.")
+    b = int(blksize)
+    if b <= 0 or b > n:
+        raise ValueError("BlockKrylovSchurSolver: blksize must be in [1,n].")
+    requested_dim = maxdim if maxdim > 0 else max(2 * nev, 20)
+    block_count = (1 + (n - 1) // b) if requested_dim >= n else requested_dim // b
+    cycle_dim = min(n, block_count * b)
+    wanted_blocks = 1 + (nev - 1) // b
+    if cycle_dim < n and block_count <= wanted_blocks:
+        raise ValueError("BlockKrylovSchurSolver: maxdim must accommodate ceil(nev/blksize) "
+                         "retained blocks plus at least one expansion block (or the full "
+                         "matrix dimension).")
+    projection_dim = (block_count + 1) * b
+    retained_blocks = 0 if cycle_dim == n else max(wanted_blocks, block_count // 2)
+    retained_dim = retained_blocks * b
+    snapshot_count = max(nev, retained_dim)
+    Hs = A.scipy()
+    basis = np.zeros((n, projection_dim))
+    _, Q0, _ = complete_block_qr(basis, 0, random_block(n, b, seed), seed, 0.0)
+    basis[:, :b] = Q0
+    T = np.zeros((projection_dim, projection_dim))
+    beta = np.zeros((b, b))
+
+    def expand(first_block):
+        nonlocal beta
+        for block in range(first_block, block_count):
+            Z = Hs @ basis[:, block * b:(block + 1) * b]
+            active = min(n, (block + 1) * b)
+            _, Rres, H = block_gram_schmidt(basis, active, Z)
+            width = 1 + (active - 1) % b
+            diag = np.zeros((b, b))
+            diag[:width, :width] = H[H.shape[0] - width:, :width]
+            scale = float(np.linalg.norm(np.linalg.norm(Z, axis=0)))
+            _, Qn, coupling = complete_block_qr(basis, min((block + 1) * b, n), Rres,
+                                                seed + (block + 1) * b, scale)
+            basis[:, (block + 1) * b:(block + 2) * b] = Qn
+            row, nrow = block * b, (block + 1) * b
+            T[row:row + b, row:row + b] = diag
+            T[nrow:nrow + b, row:row + b] = coupling
+            T[row:row + b, nrow:nrow + b] = coupling.T
+            beta = coupling
+
+    expand(0)
+    for iteration in range(1, maxiter + 1):
+        m = cycle_dim
+        w, Z = np.linalg.eigh(T[:m, :m])
+        tail = 1 + (m - 1) % b
+        last = np.zeros((b, m))
+        last[:tail] = Z[m - tail:, :]
+        idx = select_ritz_indices(w, which)
+        cnt = min(snapshot_count, m)
+        lam_all = w[idx[:cnt]]
+        rel_all = np.linalg.norm(beta @ last[:, idx[:cnt]], axis=0) / (1.0 + np.abs(lam_all))
+        C_all = Z[:, idx[:cnt]]
+        k = min(nev, cnt)
+        converged = k > 0 and rel_all[:k].max() < tol
+        at_limit = iteration == maxiter or cycle_dim == n
+        if converged or at_limit:
+            Y, res = evaluate_ritz_pairs(A, None, basis, cycle_dim, lam_all[:k], C_all[:, :k])
+            converged = bool(np.all(res <= tol))
+            if converged or at_limit:
+                return SolveResult(lam_all[:k].copy(), Y, res, iteration, 0 if converged else 1)
+        Cr = C_all[:, :retained_dim]
+        restart_coupling = beta @ Cr[m - b:, :]
+        ritz_block = basis[:, :cycle_dim] @ Cr
+        resid_block = basis[:, block_count * b:block_count * b + b].copy()
+        basis[:] = 0.0
+        basis[:, :retained_dim] = ritz_block
+        basis[:, retained_dim:retained_dim + b] = resid_block
+        T[:] = 0.0
+        T[:retained_dim, :retained_dim] = np.diag(lam_all[:retained_dim])
+        T[retained_dim:retained_dim + b, :retained_dim] = restart_coupling
+        T[:retained_dim, retained_dim:retained_dim + b] = restart_coupling.T
+        expand(retained_blocks)
+    raise RuntimeError("BlockKrylovSchurSolver: unreachable solve termination.")
+
+
 # --------------------------------------------------------------------------
 # Reference spectra: tests/scripts/ref_eigs.py (parse) and run_case.py (select)
 # --------------------------------------------------------------------------
