@@ -10,8 +10,8 @@
 //      p = tau A22 v, w = p - (tau/2)(p.v) v, A22 -= v w^T + w v^T (both triangles
 //      kept). The trailing matrix moves into shared memory once it fits. The
 //      reflectors stay in A's strictly lower part for step 4.
-//   2. stebz: every eigenvalue of the tridiagonal by bisection on its Sturm count,
-//      one thread per eigenvalue index (ascending order by construction).
+//   2. stebz: every eigenvalue of the tridiagonal by multisection on its Sturm
+//      count, one warp per eigenvalue index (ascending order by construction).
 //   3. stein: eigenvectors of the tridiagonal by inverse iteration (LU of T - lambda
 //      I with partial pivoting, tiny pivots replaced by eps*||T||, three solves from
 //      a hashed start vector), one warp per cluster of eigenvalues closer than
@@ -195,36 +195,48 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* e, int
   return cnt;
 }
 
-// Eigenvalue i of tridiagonal p by bisection; info[p] = 1 for non-finite data.
+// Eigenvalue i of tridiagonal p by multisection, one warp per eigenvalue: each round
+// the 32 lanes take Sturm counts at 32 interior points of [lo, hi] and the interval
+// shrinks to the sub-interval where the count passes i (5 bits per round instead of
+// bisection's 1). info[p] = 1 for non-finite data.
 __global__ void stebz_kernel(const int32_t* __restrict__ msz, const double* __restrict__ d,
                              const double* __restrict__ e, int64_t vec_stride,
                              double* __restrict__ W, int64_t ldw, double* __restrict__ tnorm_out,
                              int32_t* __restrict__ info) {
   const int p = blockIdx.y;
   const int k = msz[p];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
   if (i >= k) return;
   const double* dp = d + p * vec_stride;
   const double* ep = e + p * vec_stride;
   double gl, gu, tnorm, pivmin;
   gershgorin(dp, ep, k, gl, gu, tnorm, pivmin);
   if (!isfinite(gl) || !isfinite(gu)) {
-    if (i == 0) {
+    if (i == 0 && lane == 0) {
       info[p] = 1;
       tnorm_out[p] = 1.0;
     }
-    W[p * ldw + i] = nan("");
+    if (lane == 0) W[p * ldw + i] = nan("");
     return;
   }
-  if (i == 0) tnorm_out[p] = tnorm;
+  if (i == 0 && lane == 0) tnorm_out[p] = tnorm;
   double lo = gl, hi = gu;
-  for (int it = 0; it < 128; ++it) {
-    const double mid = 0.5 * (lo + hi);
-    if (hi - lo <= 2.0 * kEps * fmax(fabs(lo), fabs(hi)) + pivmin || mid == lo || mid == hi) break;
-    if (sturm_count(dp, ep, k, mid, pivmin) > i) hi = mid;
-    else lo = mid;
+  for (int round = 0; round < 64; ++round) {
+    if (hi - lo <= 2.0 * kEps * fmax(fabs(lo), fabs(hi)) + pivmin) break;
+    const double x = lo + (hi - lo) * (static_cast<double>(lane + 1) / 33.0);
+    const bool above = sturm_count(dp, ep, k, x, pivmin) > i;
+    const unsigned mask = __ballot_sync(0xffffffffu, above);
+    const int first = mask ? __ffs(mask) - 1 : 32;
+    const double x_first = __shfl_sync(0xffffffffu, x, first < 32 ? first : 31);
+    const double x_prev = __shfl_sync(0xffffffffu, x, first > 0 ? first - 1 : 0);
+    const double nlo = first == 0 ? lo : x_prev;
+    const double nhi = first < 32 ? x_first : hi;
+    if (nlo == lo && nhi == hi) break;  // no representable progress
+    lo = nlo;
+    hi = nhi;
   }
-  W[p * ldw + i] = 0.5 * (lo + hi);
+  if (lane == 0) W[p * ldw + i] = 0.5 * (lo + hi);
 }
 
 __device__ __forceinline__ double hash_uniform(uint64_t a, uint64_t b) {
@@ -451,8 +463,8 @@ void syevd_batched(int count, const int32_t* m_host, double* A, int64_t lda, dou
   sytrd_kernel<<<count, kTrdThreads, smem, s>>>(w.msz, A, lda, w.d, w.e, w.tau, w.vec_stride, kmax,
                                                 tile_cap);
   check_launch("sytrd_kernel");
-  stebz_kernel<<<dim3((kmax + 127) / 128, count), 128, 0, s>>>(w.msz, w.d, w.e, w.vec_stride, W,
-                                                                lda, w.tnorm, info);
+  stebz_kernel<<<dim3((kmax + 3) / 4, count), 128, 0, s>>>(w.msz, w.d, w.e, w.vec_stride, W, lda,
+                                                            w.tnorm, info);
   check_launch("stebz_kernel");
   FE_CHECK_CUDA(cudaMemsetAsync(Z, 0, sizeof(double) * count * lda * lda, s));
   stein_kernel<<<dim3((kmax + 3) / 4, count), 128, 0, s>>>(w.msz, w.d, w.e, w.vec_stride, W, lda,
