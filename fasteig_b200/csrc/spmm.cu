@@ -982,6 +982,17 @@ void csr_spmm_mode(int mode, const Csr& A, const T* X, int64_t ldx, T* Y, int64_
         try_row_kernel<T, 8 / sizeof(T)>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols),
                                          T(alpha), T(gamma), T(beta), ug, ub, s, 5, true))
       return;
+    // Mode 5: 16-byte vectors, up to 3 per lane (a 320-column FP32 slab in one panel);
+    // mode 6: 8-byte vectors, up to 3 per lane (a 320-column FP32 slab in two panels,
+    // fewer registers per warp).
+    if (mode == 5 &&
+        try_row_kernel<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
+                               T(gamma), T(beta), ug, ub, s, 3))
+      return;
+    if (mode == 6 &&
+        try_row_kernel<T, 8 / sizeof(T)>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols),
+                                         T(alpha), T(gamma), T(beta), ug, ub, s, 3))
+      return;
     if (mode == 2 && ncols * static_cast<int64_t>(sizeof(T)) >= 64 &&
         try_pipe<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                          T(gamma), T(beta), ug, ub, s))
@@ -1025,7 +1036,7 @@ int autotune_spmm(Csr& A, int64_t ncols, cudaStream_t s) {
     FE_CHECK_CUDA(cudaEventCreate(&e0));
     FE_CHECK_CUDA(cudaEventCreate(&e1));
     float best_ms = 0.0f;
-    for (int mode : {0, 3, 2, 1, 4}) {
+    for (int mode : {0, 3, 2, 1, 4, 5, 6}) {
       auto run = [&] {
         csr_spmm_mode<T>(mode, A, static_cast<const T*>(x), ld, static_cast<T*>(y), ld,
                          static_cast<const T*>(z), ld, ncols, 0.25, 0.1, -1.0, s);

@@ -1017,7 +1017,7 @@ extern "C" int fe_device_status(int32_t* status, int32_t clear) {
 
 extern "C" int fe_set_spmm_kernel(int32_t mode) {
   return fe::guarded("fe_set_spmm_kernel", [&] {
-    FE_REQUIRE(mode >= 0 && mode <= 4, "mode must be 0..4");
+    FE_REQUIRE(mode >= 0 && mode <= 6, "mode must be 0..6");
     fe::set_spmm_mode(mode);
   });
 }

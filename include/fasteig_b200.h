@@ -205,7 +205,9 @@ int fe_selftest_wait_timeout(int64_t limit_cycles, int32_t code, void* stream);
  * (row-batched register kernel for slabs of >= 32 128-bit vectors and rows of
  * <= 7 nonzeros, else the loop kernel), 1 = loop kernel, 2 = bulk-copy
  * pipelined kernel where it applies, 3 = row-batched kernel with narrower
- * column panels, 4 = mode 0 with each warp's next Z row prefetched into L2. */
+ * column panels, 4 = mode 0 with each warp's next Z row prefetched into L2,
+ * 5 = row-batched kernel with 16-byte lanes and up to 3 per lane, 6 = row-batched
+ * kernel with 8-byte lanes and up to 3 per lane. */
 int fe_set_spmm_kernel(int32_t mode);
 /* SpMM autotuner: times every SpMM kernel on operator A for an n-by-ncols block
  * in the Chebyshev-step form (precision 0 = FP64, 1 = FP32) on `stream` and
