@@ -855,11 +855,19 @@ struct TcGramPlan {
   size_t bytes;
 };
 
-TcGramPlan tc_gram_plan(int64_t n, int64_t kx, int64_t my, int64_t k, int64_t m) {
+// Row chunks: as many as make the CTAs that compute (the output tiles, less those
+// wholly below the diagonal of a symmetric Gram) fill two whole waves of one CTA per
+// SM, so every SM gets equal work, the per-CTA prologue and partial tile are paid a few
+// hundred times rather than thousands, and no tail wave runs half empty; at least four
+// K stages per chunk.
+TcGramPlan tc_gram_plan(int64_t n, int64_t kx, int64_t my, int64_t k, int64_t m,
+                        int64_t active_tiles) {
   TcGramPlan p{};
   p.k_tiles = static_cast<int>((kx + kM - 1) / kM);
   p.m_tiles = static_cast<int>((my + kN - 1) / kN);
-  int64_t chunks = std::min<int64_t>(kGramTcTargetChunks, (n + 4 * kKB - 1) / (4 * kKB));
+  const int64_t tiles = std::max<int64_t>(1, active_tiles);
+  int64_t chunks = std::max<int64_t>(1, (2 * static_cast<int64_t>(num_sms())) / tiles);
+  chunks = std::min<int64_t>({chunks, kGramTcTargetChunks, (n + 4 * kKB - 1) / (4 * kKB)});
   chunks = std::max<int64_t>(chunks, 1);
   int64_t rpc = (n + chunks - 1) / chunks;
   rpc = ((rpc + kKB - 1) / kKB) * kKB;
@@ -901,13 +909,20 @@ void gram_tc(const float* X, int64_t ldx, const float* Y, int64_t ldy, int64_t n
   const int sy = static_cast<int>((reinterpret_cast<uintptr_t>(Y) & 15u) / 4);
   const float* Xa = X - sx;
   const float* Ya = Y - sy;
-  const TcGramPlan p = tc_gram_plan(n, k + sx, m + sy, k, m);
+  const bool sym = X == Y && ldx == ldy && k == m;
+  int64_t active_tiles = 0;
+  {
+    const int64_t kt = (k + sx + kM - 1) / kM, mt = (m + sy + kN - 1) / kN;
+    for (int64_t ti = 0; ti < kt; ++ti)
+      for (int64_t tj = 0; tj < mt; ++tj)
+        if (!(sym && ti * kM >= tj * kN + kN)) ++active_tiles;
+  }
+  const TcGramPlan p = tc_gram_plan(n, k + sx, m + sy, k, m, active_tiles);
   FE_REQUIRE(ws && ws_bytes >= p.bytes, "gram_tc: workspace too small");
   const CUtensorMap mx = make_map(Xa, k + sx, n, ldx, 32, kKB, true);
   const CUtensorMap my = make_map(Ya, m + sy, n, ldy, 32, kKB, true);
   static std::once_flag once;
   std::call_once(once, [] { set_smem_attr(reinterpret_cast<const void*>(gram_tc_kernel)); });
-  const bool sym = X == Y && ldx == ldy && k == m;
   dim3 grid(p.k_tiles * p.m_tiles, p.chunks);
   gram_tc_kernel<<<grid, kGramThreads, kSmemBytes, s>>>(mx, my, n, static_cast<int>(k),
                                                     static_cast<int>(m), sx, sy, p.k_tiles,
