@@ -419,7 +419,8 @@ def solve_opts(a, precision, seed, locking=None):
 SPMM_KERNEL_NAMES = {0: "csr_spmm_row_kernel<float,2,5,7>", 1: "csr_spmm_kernel<float,4,32,*>",
                      2: "csr_spmm_pipe_kernel<float,4,*>", 3: "csr_spmm_row_kernel<float,4,2,7>",
                      4: "csr_spmm_row_kernel<float,2,5,7> (Z prefetched to L2)",
-                     5: "csr_spmm_row_kernel<float,4,3,7>", 6: "csr_spmm_row_kernel<float,2,3,7>"}
+                     5: "csr_spmm_row_kernel<float,4,3,7>", 6: "csr_spmm_row_kernel<float,2,3,7>",
+                     7: "csr_spmm_row_cg_kernel<float,2,5,7>"}
 
 
 def roofline_cheb_step(a, H, dA, peak, launches=20, mode=0):

@@ -68,6 +68,7 @@ _SIGS = {
                                    vp]),
     "fe_device_status": (C.c_int, [C.POINTER(C.c_int32), C.c_int32]),
     "fe_set_spmm_kernel": (C.c_int, [C.c_int32]),
+    "fe_set_cheb_wave_kernel": (C.c_int, [C.c_int32]),
     "fe_set_f64_gemm_kernel": (C.c_int, [C.c_int32]),
     "fe_set_tc_rotate_kernel": (C.c_int, [C.c_int32]),
     "fe_csr_autotune": (C.c_int, [vp, i64, C.c_int32, vp, vp]),

@@ -36,6 +36,15 @@ void refine_finish(int64_t n, int64_t ncols, const double* t, const float* Z, in
 template <typename T>
 void cheb_filter(const Csr& A, T* X, T* scratch, int64_t ld, int64_t ncols, int degree, double c,
                  double d, cudaStream_t s);
+// The filter in launches of several steps each (the result in X, Sc scratch); false
+// (nothing launched) where it does not apply. `sync` holds wave_sync_bytes(A.rows).
+size_t wave_sync_bytes(int64_t nrows);
+void set_wave_mode(int mode);
+int64_t csr_bandwidth(const Csr& A, cudaStream_t s);
+template <typename T>
+bool cheb_filter_wave(const Csr& A, T* X, int64_t ldx, T* Sc, int64_t lds, int64_t ncols,
+                      int degree, double c, double d, void* sync, size_t sync_bytes,
+                      cudaStream_t s);
 size_t gram_workspace_bytes(int64_t n, int64_t k, int64_t m);
 template <typename T>
 void gram(const T* X, int64_t ldx, const T* Y, int64_t ldy, int64_t n, int64_t k, int64_t m,

@@ -99,6 +99,9 @@ struct Csr {
   float* val32 = nullptr;
   int device = 0;
   int64_t max_row_nnz = 0;
+  // max |column - row| over the stored entries, measured on first use by the
+  // multi-step filter (-1: not measured yet)
+  mutable int64_t bandwidth = -1;
   // SpMM kernel chosen by fe_csr_autotune per precision (0 FP64, 1 FP32) for up
   // to four block widths; mode < 0 marks an empty entry.
   struct Tuned {

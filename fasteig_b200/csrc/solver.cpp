@@ -641,6 +641,7 @@ struct ChebLoop {
   bool refine = false;
   bool theta_ready = false;
   Block<float> r32, z0, z1;  // refined-filter blocks (allocated on first use)
+  DeviceBuffer wave_sync;    // multi-step filter's tickets and flags (allocated on first use)
   PhaseEvents ev;
 
   ChebLoop(Context& c, const Csr& a, const Options& o, SmallState& s, ProjectedEig& e, double sg,
@@ -914,6 +915,14 @@ struct ChebLoop {
 
   void filter(T* X, int64_t ldx, T* Sc, int64_t lds, int64_t cols, double c, double d) {
     cudaStream_t s = ctx.stream;
+    // Several filter steps per launch where the operator allows it (cheb_filter_wave).
+    if (degree >= 2) {
+      const size_t need = wave_sync_bytes(n);
+      if (wave_sync.bytes() < need) wave_sync.resize(need);
+      if (cheb_filter_wave<T>(A, X, ldx, Sc, lds, cols, static_cast<int>(degree), c, d,
+                              wave_sync.get(), wave_sync.bytes(), s))
+        return;
+    }
     // Y1 = c*A*Y0 + d*Y0 into scratch; Y_k = 2c*A*Y_{k-1} + 2d*Y_{k-1} - Y_{k-2} in place.
     csr_spmm<T>(A, X, ldx, Sc, lds, nullptr, 0, cols, c, d, 0.0, s);
     T* prev = X;
@@ -1028,11 +1037,14 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     // filter amplifies `lower` by 1e3. bounds=ritz (after the first cycle) damps
     // from the largest Ritz value of the last Rayleigh-Ritz instead, lowered if
     // needed so that the amplification at `lower` stays within the cap.
+    // The interval is set by the configured degree in every phase: a different
+    // degree for the FP64 cycles (tail_degree) changes how strongly the same
+    // interval is filtered, not where it lies.
     const int64_t deg_now = l32 ? opt.degree : (l64 ? l64->degree : opt.degree);
-    double cutoff = reference_cutoff(lower, upper, deg_now, 1.0e3);
+    double cutoff = reference_cutoff(lower, upper, opt.degree, 1.0e3);
     if (opt.bounds == "ritz" && sub_prev > 0) {
       cutoff = std::min(W[sub_prev - 1],
-                        reference_cutoff(lower, upper, deg_now, opt.amplification));
+                        reference_cutoff(lower, upper, opt.degree, opt.amplification));
     }
     if (upper == lower) cutoff = upper;  // collapsed spectrum: no filtering
     int32_t info[3] = {0, 0, 0};

@@ -77,6 +77,13 @@ __device__ __forceinline__ Pack<T, VEC> load_pack(const T* p) {
   return unpack<T, VEC>(__ldg(reinterpret_cast<const R*>(p)));
 }
 
+// Load bypassing L1 (cached in L2 only), for blocks other SMs rewrite during a launch.
+template <typename T, int VEC>
+__device__ __forceinline__ Pack<T, VEC> load_pack_cg(const T* p) {
+  using R = typename Raw<T, VEC>::type;
+  return unpack<T, VEC>(__ldcg(reinterpret_cast<const R*>(p)));
+}
+
 // Plain (coherent) load for blocks that may alias the output.
 template <typename T, int VEC>
 __device__ __forceinline__ Pack<T, VEC> load_pack_rw(const T* p) {
@@ -215,6 +222,9 @@ csr_spmm_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
   }
 }
 
+// Library-default status word of the SpMM kernels' bounded waits (fe_device_status).
+__device__ int g_spmm_status = 0;
+
 // ---------------------------------------------------------------------------
 // Row-batched register kernel: one warp per row for slabs of >= 32 vectors.
 //
@@ -230,18 +240,133 @@ csr_spmm_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
 // ---------------------------------------------------------------------------
 // With CORR, every output also gains delta[j] * R[row, j] (the correction term of the
 // refined filter, see csr_spmm_corr).
-template <typename T, int VEC, int CPL, int NZ, bool CORR>
+//
+// With WAVE != 0, the warp takes the rows wave_row0, wave_row0 + wave_stride, ... below
+// wave_end instead of a grid stride, and X and Z are read with
+// coherent loads (WAVE 1: ld.global.cg, L2 only, so no L1 line can hold a stale
+// copy; WAVE 2: plain loads; WAVE 3: the read-only path, for launches that run one
+// step): the multi-step filter (cheb_wave_kernel) reads blocks that other CTAs of the
+// same launch wrote.
+// Cross-level link of the multi-step filter (cheb_wave_kernel): the level this warp
+// runs waits, before each row, until the previous level has finished every row up
+// to `reach` past it, and reports each finished row. Rows are counted per block of
+// 2^block_shift rows.
+struct WaveLink {
+  const int* prev_done;  // finished-row counts of the previous level (null: no wait)
+  int* own_done;         // this level's counts
+  int64_t reach;         // operator bandwidth
+  int64_t nrows;
+  int block_shift;
+  const int* abort_flag;
+  int* status;
+  long long max_polls;
+  int64_t* known;  // this warp's count of leading blocks known complete (shared memory)
+};
+
+constexpr int kWaveTimeoutCode = 13;
+
+__device__ __forceinline__ int ld_acquire_s32(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Returns false if the wait timed out or the launch was aborted (the warp stops).
+__device__ __forceinline__ bool wave_wait(const WaveLink& L, int64_t row) {
+  const int lane = threadIdx.x & 31;
+  const int64_t need_row = min(L.nrows - 1, row + L.reach);
+  const int64_t need = need_row >> L.block_shift;  // blocks [0, need] must be complete
+  int64_t known = *L.known;
+  if (known > need) return true;
+  const int64_t nblocks = ((L.nrows - 1) >> L.block_shift) + 1;
+  const int64_t brows = int64_t(1) << L.block_shift;
+  long long polls = 0;
+  while (true) {
+    const int64_t b = known + lane;
+    int f = 1;
+    if (b < nblocks) {
+      const int64_t full = min(brows, L.nrows - b * brows);
+      f = ld_acquire_s32(L.prev_done + b) == full;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, f != 0);
+    known += m == 0xffffffffu ? 32 : __ffs(~m) - 1;
+    if (known > need) break;
+    if (m != 0xffffffffu) {
+      int halt = 0;
+      if (lane == 0) {
+        halt = *reinterpret_cast<const volatile int*>(L.abort_flag) != 0;
+        if (!halt && ++polls > L.max_polls) {
+          atomicCAS(L.status ? L.status : &g_spmm_status, 0, kWaveTimeoutCode);
+          atomicExch(const_cast<int*>(L.abort_flag), 1);
+          halt = 1;
+        }
+      }
+      if (__shfl_sync(0xffffffffu, halt, 0)) return false;
+      __nanosleep(64);
+    }
+  }
+  if (lane == 0) *L.known = known;
+  __syncwarp();
+  return true;
+}
+
+// Finished rows are reported kWaveBatch at a time: one fence per batch (a fence waits
+// for the warp's stores to drain, which stalls a latency-bound warp), then relaxed
+// increments of the batch's block counters. `pending` holds the batch's rows.
+constexpr int kWaveBatch = 4;
+
+__device__ __forceinline__ void wave_flush(const WaveLink& L, const int64_t (&pending)[kWaveBatch],
+                                           int count) {
+  __syncwarp();  // every lane's stores precede the fence below
+  if ((threadIdx.x & 31) == 0 && count > 0) {
+    __threadfence();
+#pragma unroll
+    for (int i = 0; i < kWaveBatch; ++i)
+      if (i < count)
+        asm volatile("red.relaxed.gpu.global.add.s32 [%0], 1;" ::"l"(
+                         L.own_done + (pending[i] >> L.block_shift))
+                     : "memory");
+  }
+}
+
+__device__ __forceinline__ void wave_done(const WaveLink& L, int64_t row,
+                                          int64_t (&pending)[kWaveBatch], int& count) {
+  if (!L.own_done) return;  // the last level of a launch: nobody waits on it
+#pragma unroll
+  for (int i = 0; i < kWaveBatch; ++i)
+    if (i == count) pending[i] = row;
+  if (++count == kWaveBatch) {
+    wave_flush(L, pending, count);
+    count = 0;
+  }
+}
+
+// X loads of the row body: WAVE 0 and 3 = read-only path (X not written during the
+// launch), 1 = L2 only (ld.global.cg), 2 = plain coherent loads.
+template <typename T, int VEC, int WAVE>
+__device__ __forceinline__ Pack<T, VEC> body_load_x(const T* p) {
+  if constexpr (WAVE == 1) return load_pack_cg<T, VEC>(p);
+  else if constexpr (WAVE == 2) return load_pack_rw<T, VEC>(p);
+  else return load_pack<T, VEC>(p);
+}
+
+template <typename T, int VEC, int CPL, int NZ, bool CORR, int WAVE = 0, int XL = -1>
 __device__ __forceinline__ void csr_spmm_row_body(
     int64_t nrows, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind,
-    const T* __restrict__ vals, const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy,
+    const T* __restrict__ vals, const T* X, int64_t ldx, T* Y, int64_t ldy,
     const T* Z, int64_t ldz, int ncols, int panel_vec, T alpha, T gamma, T beta, int use_gamma,
     int use_beta, int prefetch_z, const T* __restrict__ R, int64_t ldr,
-    const T* __restrict__ delta) {
+    const T* __restrict__ delta, int64_t wave_row0 = 0, int64_t wave_end = 0,
+    int64_t wave_stride = 1, const WaveLink* link = nullptr) {
   constexpr unsigned kFull = 0xffffffffu;
+  // load kind of X and Z: XL if given, else by the wave mode (see body_load_x)
+  constexpr int XLK = XL >= 0 ? XL : WAVE;
   const int lane = threadIdx.x & 31;
-  const int64_t tw = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
-  int64_t row = static_cast<int64_t>(blockIdx.x) * (kThreads / 32) + threadIdx.x / 32;
-  if (row >= nrows) return;
+  const int64_t tw = WAVE != 0 ? wave_stride : static_cast<int64_t>(gridDim.x) * (kThreads / 32);
+  int64_t row = WAVE != 0 ? wave_row0
+                          : static_cast<int64_t>(blockIdx.x) * (kThreads / 32) + threadIdx.x / 32;
+  const int64_t row_end = WAVE != 0 ? wave_end : nrows;
+  if (row >= row_end) return;
   const int p0 = blockIdx.y * panel_vec * VEC;
   const int nvec = min(panel_vec, (ncols - p0) / VEC);
   const T* Xp = X + p0;
@@ -255,11 +380,26 @@ __device__ __forceinline__ void csr_spmm_row_body(
   }
   int64_t nxt = row + tw;
   int s1 = 0, e1 = 0;
-  if (nxt < nrows) {
+  if (nxt < row_end) {
     s1 = __ldg(rowptr + nxt);
     e1 = __ldg(rowptr + nxt + 1);
   }
+  int64_t pending[kWaveBatch];
+  int npending = 0;
   while (true) {
+    if constexpr (WAVE != 0) {
+      if (link->prev_done) {
+        const int64_t need = min(link->nrows - 1, row + link->reach) >> link->block_shift;
+        if (*link->known <= need) {
+          // about to wait: report this warp's finished rows first
+          if (link->own_done && npending > 0) {
+            wave_flush(*link, pending, npending);
+            npending = 0;
+          }
+          if (!wave_wait(*link, row)) return;
+        }
+      }
+    }
     const int nnz = e0 - s0;
     Pack<T, VEC> z[CPL];
     Pack<T, VEC> rc[CPL];
@@ -274,13 +414,15 @@ __device__ __forceinline__ void csr_spmm_row_body(
 #pragma unroll
       for (int q = 0; q < CPL; ++q) {
         const int v = lane + 32 * q;
-        if (v < nvec) z[q] = load_pack_rw<T, VEC>(Z + row * ldz + p0 + v * VEC);
+        if (v < nvec)
+          z[q] = XLK == 1 ? load_pack_cg<T, VEC>(Z + row * ldz + p0 + v * VEC)
+                          : load_pack_rw<T, VEC>(Z + row * ldz + p0 + v * VEC);
       }
       // Z rows stream from DRAM: with prefetch_z, start this warp's next Z row
       // toward L2 now (one 128-byte line per lane, addresses inside the row), so
       // its loads there meet L2 rather than DRAM latency (pays off for the FP64
       // panels, not for one FP32 panel: a per-operator autotune choice).
-      if (prefetch_z && nxt < nrows) {
+      if (prefetch_z && nxt < row_end) {
         const int bytes = nvec * VEC * static_cast<int>(sizeof(T));
         if (lane * 128 < bytes)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(
@@ -316,15 +458,15 @@ __device__ __forceinline__ void csr_spmm_row_body(
 #pragma unroll
           for (int q = 0; q < CPL; ++q) {
             const int v = lane + 32 * q;
-            if (v < nvec) x[t][q] = load_pack<T, VEC>(xr + v * VEC);
+            if (v < nvec) x[t][q] = body_load_x<T, VEC, XLK>(xr + v * VEC);
           }
         }
       }
-      if (nxt < nrows && lane < min(e1 - s1, NZ)) {
+      if (nxt < row_end && lane < min(e1 - s1, NZ)) {
         c_n = __ldg(colind + s1 + lane);
         a_n = __ldg(vals + s1 + lane);
       }
-      if (nxt2 < nrows) {
+      if (nxt2 < row_end) {
         s2 = __ldg(rowptr + nxt2);
         e2 = __ldg(rowptr + nxt2 + 1);
       }
@@ -370,18 +512,18 @@ __device__ __forceinline__ void csr_spmm_row_body(
           for (int q = 0; q < CPL; ++q) {
             const int v = lane + 32 * q;
             if (v < nvec) {
-              const Pack<T, VEC> p = load_pack<T, VEC>(xr + v * VEC);
+              const Pack<T, VEC> p = body_load_x<T, VEC, XLK>(xr + v * VEC);
 #pragma unroll
               for (int e = 0; e < VEC; ++e) acc[q][e] = fma(coef, p.v[e], acc[q][e]);
             }
           }
         }
       }
-      if (nxt < nrows && lane < min(e1 - s1, NZ)) {
+      if (nxt < row_end && lane < min(e1 - s1, NZ)) {
         c_n = __ldg(colind + s1 + lane);
         a_n = __ldg(vals + s1 + lane);
       }
-      if (nxt2 < nrows) {
+      if (nxt2 < row_end) {
         s2 = __ldg(rowptr + nxt2);
         e2 = __ldg(rowptr + nxt2 + 1);
       }
@@ -391,7 +533,7 @@ __device__ __forceinline__ void csr_spmm_row_body(
       for (int q = 0; q < CPL; ++q) {
         const int v = lane + 32 * q;
         if (v < nvec) {
-          const Pack<T, VEC> xr = load_pack<T, VEC>(Xp + row * ldx + v * VEC);
+          const Pack<T, VEC> xr = body_load_x<T, VEC, XLK>(Xp + row * ldx + v * VEC);
 #pragma unroll
           for (int e = 0; e < VEC; ++e) acc[q][e] = fma(gamma, xr.v[e], acc[q][e]);
         }
@@ -414,7 +556,8 @@ __device__ __forceinline__ void csr_spmm_row_body(
         store_pack<T, VEC>(yr + v * VEC, out);
       }
     }
-    if (nxt >= nrows) break;
+    if constexpr (WAVE != 0) wave_done(*link, row, pending, npending);
+    if (nxt >= row_end) break;
     row = nxt;
     nxt = nxt2;
     s0 = s1;
@@ -423,6 +566,9 @@ __device__ __forceinline__ void csr_spmm_row_body(
     e1 = e2;
     c_cur = c_n;
     a_cur = a_n;
+  }
+  if constexpr (WAVE != 0) {
+    if (link->own_done) wave_flush(*link, pending, npending);
   }
 }
 
@@ -436,6 +582,21 @@ csr_spmm_row_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
   csr_spmm_row_body<T, VEC, CPL, NZ, false>(nrows, rowptr, colind, vals, X, ldx, Y, ldy, Z, ldz,
                                             ncols, panel_vec, alpha, gamma, beta, use_gamma,
                                             use_beta, prefetch_z, nullptr, 0, nullptr);
+}
+
+// The row kernel with X and Z read through L2 only (ld.global.cg): gathers whose
+// neighbour rows see little L1 reuse skip the L1 allocation (SpMM mode 7).
+template <typename T, int VEC, int CPL, int NZ>
+__global__ void __launch_bounds__(kThreads)
+csr_spmm_row_cg_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
+                       const int32_t* __restrict__ colind, const T* __restrict__ vals,
+                       const T* __restrict__ X, int64_t ldx, T* Y, int64_t ldy, const T* Z,
+                       int64_t ldz, int ncols, int panel_vec, T alpha, T gamma, T beta,
+                       int use_gamma, int use_beta, int prefetch_z) {
+  csr_spmm_row_body<T, VEC, CPL, NZ, false, 0, 1>(nrows, rowptr, colind, vals, X, ldx, Y, ldy, Z,
+                                                  ldz, ncols, panel_vec, alpha, gamma, beta,
+                                                  use_gamma, use_beta, prefetch_z, nullptr, 0,
+                                                  nullptr);
 }
 
 // The row kernel with the correction term delta[j] * R[row, j] added to every output
@@ -454,10 +615,91 @@ csr_spmm_row_corr_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
                                            use_beta, 0, R, ldr, delta);
 }
 
+// ---------------------------------------------------------------------------
+// Multi-step Chebyshev filter in one launch (levels trailing each other over rows).
+//
+// Step k of the filter writes Y_k = alpha_k A Y_{k-1} + gamma_k Y_{k-1} + beta_k Y_{k-2}
+// into the buffer that held Y_{k-2} (buf[k & 1]; buf[0] holds the input block). Row r
+// of Y_k needs the rows of Y_{k-1} within the operator's bandwidth bw of r. One
+// launch runs `levels` consecutive steps: the warps of the grid are dealt round-robin
+// to the levels, and the warps of a level sweep the rows exactly as the single-step
+// row kernel does (warp j of the level: rows j, j + W, j + 2W, ..., W the level's
+// warps), so each level's rows in flight stay within a narrow band. Before each row,
+// a warp of level k waits until level k - 1 has finished every row up to bw past it
+// (finished rows are counted per block of 1024 rows with release increments and read
+// with acquire loads), so level k runs about bw rows behind level k - 1 and gathers
+// rows of Y_{k-1} written a moment before, from L2. A launch of S steps therefore
+// reads two blocks from DRAM and writes S, where S single steps read 2 S and write S.
+// In-place overwrites are safe: level k overwrites row r of Y_{k-2} only after level
+// k - 1, the last reader of those rows near r, has passed r + bw. The first level
+// never waits and every level waits only on the one before, so with all warps
+// resident (a cooperative launch) the schedule cannot deadlock; every wait is
+// bounded (timeout: status code 13 and an abort flag that stops every waiting warp).
+// The arithmetic of every row is that of the single-step row kernel (bit-identical
+// results). Blocks are read with ld.global.cg (L2 only): rows are rewritten by other
+// SMs during the launch, and no L1 line may hold a stale copy.
+constexpr int kWaveMaxLevels = 8;
+constexpr int kWaveBlockShift = 10;  // 1024 rows per completion counter
+
+template <typename T>
+struct WaveParams {
+  int64_t nrows;
+  const int32_t* rowptr;
+  const int32_t* colind;
+  const T* vals;
+  T* buf[2];
+  int64_t ld[2];
+  int ncols, panel_vec;
+  int levels;   // steps in this launch
+  int first_k;  // filter step of level 0 (1-based)
+  T alpha[kWaveMaxLevels], gamma[kWaveMaxLevels], beta[kWaveMaxLevels];
+  int64_t reach;  // operator bandwidth (rows)
+  int* done;      // levels x blocks finished-row counters
+  int64_t nblocks;
+  int* abort_flag;
+  int* status;
+  long long max_polls;
+};
+
+template <typename T, int VEC, int CPL, int NZ, int LOADS>
+__global__ void __launch_bounds__(kThreads, 2)
+cheb_wave_kernel(const __grid_constant__ WaveParams<T> P) {
+  static_assert(LOADS >= 1 && LOADS <= 3, "the multi-step kernel sweeps rows per level");
+  __shared__ int64_t s_known[kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) s_known[warp] = 0;
+  __syncwarp();
+  const int64_t gw = static_cast<int64_t>(blockIdx.x) * (kThreads / 32) + warp;
+  const int64_t nw = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
+  const int lev = static_cast<int>(gw % P.levels);
+  const int64_t j = gw / P.levels;
+  const int64_t wl = (nw - lev + P.levels - 1) / P.levels;  // warps of this level
+  WaveLink L;
+  L.prev_done = lev > 0 ? P.done + static_cast<int64_t>(lev - 1) * P.nblocks : nullptr;
+  L.own_done = lev + 1 < P.levels ? P.done + static_cast<int64_t>(lev) * P.nblocks : nullptr;
+  L.reach = P.reach;
+  L.nrows = P.nrows;
+  L.block_shift = kWaveBlockShift;
+  L.abort_flag = P.abort_flag;
+  L.status = P.status;
+  L.max_polls = P.max_polls;
+  L.known = &s_known[warp];
+  const int k = P.first_k + lev;
+  T* out = P.buf[k & 1];
+  const int64_t ldo = P.ld[k & 1];
+  const T* cur = P.buf[(k - 1) & 1];
+  const int64_t ldc = P.ld[(k - 1) & 1];
+  const T be = P.beta[lev];
+  csr_spmm_row_body<T, VEC, CPL, NZ, false, LOADS>(
+      P.nrows, P.rowptr, P.colind, P.vals, cur, ldc, out, ldo, out, ldo, P.ncols, P.panel_vec,
+      P.alpha[lev], P.gamma[lev], be, 1, be != T(0) ? 1 : 0, 0, nullptr, 0, nullptr, j, P.nrows,
+      wl, &L);
+}
+
 template <typename T, int VEC>
 bool try_row_kernel(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, int64_t ldy,
                     const T* Z, int64_t ldz, int ncols, T alpha, T gamma, T beta, bool ug, bool ub,
-                    cudaStream_t s, int max_cpl, bool prefetch_z = false) {
+                    cudaStream_t s, int max_cpl, bool prefetch_z = false, bool cg = false) {
   constexpr int NZ = 7;
   const int nvec = ncols / VEC;
   if (nvec < 32 || ncols % VEC != 0 || A.max_row_nnz > NZ) return false;
@@ -467,8 +709,10 @@ bool try_row_kernel(const Csr& A, const T* vals, const T* X, int64_t ldx, T* Y, 
   // One warp per row, grid-stride over rows with exactly the resident CTAs.
 #define FE_ROW(CPL_)                                                                           \
   do {                                                                                         \
-    auto kern = csr_spmm_row_kernel<T, VEC, CPL_, NZ>;                                         \
-    static int resident = 0;                                                                   \
+    auto kern = cg ? csr_spmm_row_cg_kernel<T, VEC, CPL_, NZ>                                  \
+                   : csr_spmm_row_kernel<T, VEC, CPL_, NZ>;                                    \
+    static int resident_by_kind[2] = {0, 0};                                                   \
+    int& resident = resident_by_kind[cg ? 1 : 0];                                              \
     if (resident == 0) {                                                                       \
       FE_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, kThreads,   \
                                                                   0));                         \
@@ -595,8 +839,6 @@ constexpr int kPipeWarps = 8;
 constexpr int kPipeDepth = 2;
 constexpr int kPipeMaxSlots = 32;
 constexpr int kPipeStageBytes = 10240;  // per warp and stage: slots * row bytes
-
-__device__ int g_spmm_status = 0;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -993,6 +1235,11 @@ void csr_spmm_mode(int mode, const Csr& A, const T* X, int64_t ldx, T* Y, int64_
         try_row_kernel<T, 8 / sizeof(T)>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols),
                                          T(alpha), T(gamma), T(beta), ug, ub, s, 3))
       return;
+    // Mode 7: mode 0 with X and Z read through L2 only.
+    if (mode == 7 &&
+        try_row_kernel<T, 8 / sizeof(T)>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols),
+                                         T(alpha), T(gamma), T(beta), ug, ub, s, 5, false, true))
+      return;
     if (mode == 2 && ncols * static_cast<int64_t>(sizeof(T)) >= 64 &&
         try_pipe<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                          T(gamma), T(beta), ug, ub, s))
@@ -1036,7 +1283,7 @@ int autotune_spmm(Csr& A, int64_t ncols, cudaStream_t s) {
     FE_CHECK_CUDA(cudaEventCreate(&e0));
     FE_CHECK_CUDA(cudaEventCreate(&e1));
     float best_ms = 0.0f;
-    for (int mode : {0, 3, 2, 1, 4, 5, 6}) {
+    for (int mode : {0, 3, 2, 1, 4, 5, 6, 7}) {
       auto run = [&] {
         csr_spmm_mode<T>(mode, A, static_cast<const T*>(x), ld, static_cast<T*>(y), ld,
                          static_cast<const T*>(z), ld, ncols, 0.25, 0.1, -1.0, s);
@@ -1151,10 +1398,226 @@ void refine_finish(int64_t n, int64_t ncols, const double* t, const float* Z, in
 }
 
 // In-place filter of degree `degree`: X <- T_degree(c*A + d*I) X, scratch holds Y_{k-1}.
+// ---- multi-step filter host side ------------------------------------------
+__global__ void csr_bandwidth_kernel(int64_t nrows, const int32_t* __restrict__ rowptr,
+                                     const int32_t* __restrict__ colind,
+                                     unsigned long long* __restrict__ out) {
+  unsigned long long mx = 0;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < nrows;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) {
+      const int64_t dist = colind[e] >= r ? colind[e] - r : r - colind[e];
+      mx = max(mx, static_cast<unsigned long long>(dist));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0 && mx > 0) atomicMax(out, mx);
+}
+
+int64_t csr_bandwidth(const Csr& A, cudaStream_t s) {
+  if (A.bandwidth >= 0) return A.bandwidth;
+  unsigned long long* d = nullptr;
+  FE_CHECK_CUDA(cudaMallocAsync(&d, sizeof(unsigned long long), s));
+  FE_CHECK_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
+  if (A.rows > 0) {
+    csr_bandwidth_kernel<<<elementwise_grid(A.rows), 256, 0, s>>>(A.rows, A.rowptr, A.colind, d);
+    check_launch("csr_bandwidth_kernel");
+  }
+  unsigned long long h = 0;
+  FE_CHECK_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
+  FE_CHECK_CUDA(cudaFreeAsync(d, s));
+  FE_CHECK_CUDA(cudaStreamSynchronize(s));
+  A.bandwidth = static_cast<int64_t>(h);
+  return A.bandwidth;
+}
+
+// 0 = off (default), 1 = on where it applies; 2..8 = that many steps per launch
+// whatever the L2 window; 9 = one step per launch through the multi-step kernel;
+// 12..18 = 2..8 steps per launch with plain (L1-cached) coherent loads; 100 P + S =
+// P column panels (1, 2 or 4) of S steps per launch.
+static int g_wave_mode = 0;
+void set_wave_mode(int mode) { g_wave_mode = mode; }
+
+size_t wave_sync_bytes(int64_t nrows) {
+  const int64_t nblocks = ((std::max<int64_t>(nrows, 1) - 1) >> kWaveBlockShift) + 1;
+  return 16 + sizeof(int) * static_cast<size_t>(kWaveMaxLevels) * nblocks;
+}
+
+template <typename T, int VEC, int CPL, int LOADS>
+void launch_wave_coop(dim3 g, const WaveParams<T>& P, cudaStream_t s) {
+  WaveParams<T> arg = P;
+  void* args[] = {&arg};
+  FE_CHECK_CUDA(cudaLaunchCooperativeKernel(
+      reinterpret_cast<const void*>(cheb_wave_kernel<T, VEC, CPL, 7, LOADS>), g, dim3(kThreads),
+      args, 0, s));
+}
+
+template <typename T, int VEC, int LOADS>
+void launch_wave(int cpl, dim3 g, const WaveParams<T>& P, cudaStream_t s) {
+  switch (cpl) {
+    case 1: launch_wave_coop<T, VEC, 1, LOADS>(g, P, s); break;
+    case 2: launch_wave_coop<T, VEC, 2, LOADS>(g, P, s); break;
+    case 3: launch_wave_coop<T, VEC, 3, LOADS>(g, P, s); break;
+    case 4: launch_wave_coop<T, VEC, 4, LOADS>(g, P, s); break;
+    default: launch_wave_coop<T, VEC, 5, LOADS>(g, P, s); break;
+  }
+}
+
+template <typename T, int CPL>
+int wave_resident() {
+  static int resident = 0;  // per instantiation; the same on every B200
+  if (resident == 0) {
+    FE_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &resident, cheb_wave_kernel<T, 8 / sizeof(T), CPL, 7, 1>, kThreads, 0));
+    resident = std::max(resident, 1);
+  }
+  return resident;
+}
+
+template <typename T>
+int wave_resident_for(int cpl) {
+  switch (cpl) {
+    case 1: return wave_resident<T, 1>();
+    case 2: return wave_resident<T, 2>();
+    case 3: return wave_resident<T, 3>();
+    case 4: return wave_resident<T, 4>();
+    default: return wave_resident<T, 5>();
+  }
+}
+
+// The filter Y_degree = T_degree(c A + d I) X (X and Sc as in cheb_filter; the result
+// lands in X) in launches of several steps each, over column panels where a panel's
+// window of 2 bw rows per level must fit in L2. Returns false, having launched
+// nothing, where the multi-step kernel does not apply (not square, rows longer than
+// 7, blocks not made of 8-byte vectors, or no panel split whose window fits about
+// 75% of L2 with at least two levels); the caller then runs one step per launch.
+template <typename T>
+bool cheb_filter_wave(const Csr& A, T* X, int64_t ldx, T* Sc, int64_t lds, int64_t ncols,
+                      int degree, double c, double d, void* sync, size_t sync_bytes,
+                      cudaStream_t s) {
+  constexpr int VEC = 8 / sizeof(T);
+  const int mode = g_wave_mode;
+  if (mode == 0 || degree < 2 || A.rows != A.cols || A.rows < 4096 || A.max_row_nnz > 7 ||
+      A.max_row_nnz < 1)
+    return false;
+  if (!sync || sync_bytes < wave_sync_bytes(A.rows)) return false;
+  if (ncols % VEC != 0 || ldx % VEC != 0 || lds % VEC != 0 || !aligned16(X) || !aligned16(Sc))
+    return false;
+  if (ranges_overlap(X, A.rows, ldx, ncols, static_cast<const T*>(Sc), A.rows, lds, ncols))
+    return false;
+  const int64_t bw = csr_bandwidth(A, s);
+  int dev = 0, l2 = 0;
+  FE_CHECK_CUDA(cudaGetDevice(&dev));
+  FE_CHECK_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+  const double budget = 0.75 * static_cast<double>(l2);
+  // Candidate splits: P panels of ncols / P columns (16-byte aligned panel starts,
+  // 32..160 vectors each); S levels with (S + 1) windows of 2 bw rows in L2. Cost per
+  // step in bytes: the CSR once per panel plus (2 + S) / S passes over the blocks.
+  int panels = 0, levels = 0, loads = 1;
+  double best = 0.0;
+  const double csr_bytes = static_cast<double>(A.nnz) * (4.0 + sizeof(T));
+  const double block_bytes = static_cast<double>(A.rows) * ncols * sizeof(T);
+  const int force_p = mode >= 100 ? mode / 100 : 0;
+  for (int P : {1, 2, 4}) {
+    if (ncols % P != 0 || (force_p && P != force_p)) continue;
+    const int64_t pc = ncols / P;
+    const int64_t pv = pc / VEC;
+    if (pc % VEC != 0 || pv < 32 || pv > 160 || (P > 1 && (pc * sizeof(T)) % 16 != 0)) continue;
+    const double window = 2.0 * static_cast<double>(bw) * pc * sizeof(T);
+    int S = 0;
+    if (mode >= 100) S = std::min(mode % 100, degree);
+    else if (mode >= 2 && mode <= 8) S = std::min(mode, degree);
+    else if (mode >= 12 && mode <= 18) S = std::min(mode - 10, degree);
+    else if (mode == 9) S = 1;
+    else
+      for (int t = std::min(kWaveMaxLevels, degree); t >= 2 && S == 0; --t)
+        if ((t + 1) * window <= budget) S = t;
+    if (S == 0) continue;
+    const double cost = P * csr_bytes + block_bytes * (2.0 + S) / S;
+    if (panels == 0 || cost < best) {
+      best = cost;
+      panels = P;
+      levels = S;
+    }
+    if (mode >= 2) break;  // forced schedules take the fewest panels that fit
+  }
+  if (panels == 0 || levels < 1) return false;
+  if (mode >= 12 && mode <= 18) loads = 2;
+  if (mode == 9) loads = 3;
+  const int64_t pc = ncols / panels;
+  const int64_t pv = pc / VEC;
+  const int cpl = static_cast<int>((pv + 31) / 32);
+  const int64_t grid = static_cast<int64_t>(num_sms()) * wave_resident_for<T>(cpl);
+  const int64_t nblocks = ((A.rows - 1) >> kWaveBlockShift) + 1;
+  int* status = current_status_word();
+  char* base = static_cast<char*>(sync);
+  for (int p = 0; p < panels; ++p) {
+    for (int k0 = 1; k0 <= degree; k0 += levels) {
+      const int lv = std::min(levels, degree - k0 + 1);
+      WaveParams<T> P{};
+      P.nrows = A.rows;
+      P.rowptr = A.rowptr;
+      P.colind = A.colind;
+      if constexpr (sizeof(T) == 8) P.vals = A.val64; else P.vals = A.val32;
+      P.buf[0] = X + p * pc;
+      P.buf[1] = Sc + p * pc;
+      P.ld[0] = ldx;
+      P.ld[1] = lds;
+      P.ncols = static_cast<int>(pc);
+      P.panel_vec = static_cast<int>(pv);
+      P.levels = lv;
+      P.first_k = k0;
+      for (int l = 0; l < lv; ++l) {
+        const bool first = k0 + l == 1;
+        P.alpha[l] = static_cast<T>(first ? c : 2.0 * c);
+        P.gamma[l] = static_cast<T>(first ? d : 2.0 * d);
+        P.beta[l] = static_cast<T>(first ? 0.0 : -1.0);
+      }
+      P.reach = bw;
+      P.abort_flag = reinterpret_cast<int*>(base);
+      P.done = reinterpret_cast<int*>(base + 16);
+      P.nblocks = nblocks;
+      P.status = status;
+      P.max_polls = 1LL << 22;
+      FE_CHECK_CUDA(cudaMemsetAsync(sync, 0, 16 + sizeof(int) * lv * nblocks, s));
+      const dim3 g(static_cast<unsigned>(grid), 1);
+      if (loads == 1) launch_wave<T, VEC, 1>(cpl, g, P, s);
+      else if (loads == 2) launch_wave<T, VEC, 2>(cpl, g, P, s);
+      else launch_wave<T, VEC, 3>(cpl, g, P, s);
+      check_launch("cheb_wave_kernel");
+    }
+  }
+  if (degree % 2 == 1) {  // Y_degree is in buf[1]
+    FE_CHECK_CUDA(cudaMemcpy2DAsync(X, ldx * sizeof(T), Sc, lds * sizeof(T), ncols * sizeof(T),
+                                    A.rows, cudaMemcpyDeviceToDevice, s));
+  }
+  return true;
+}
+
+template bool cheb_filter_wave<float>(const Csr&, float*, int64_t, float*, int64_t, int64_t, int,
+                                      double, double, void*, size_t, cudaStream_t);
+template bool cheb_filter_wave<double>(const Csr&, double*, int64_t, double*, int64_t, int64_t,
+                                       int, double, double, void*, size_t, cudaStream_t);
+
 template <typename T>
 void cheb_filter(const Csr& A, T* X, T* scratch, int64_t ld, int64_t ncols, int degree, double c,
                  double d, cudaStream_t s) {
   FE_REQUIRE(degree >= 1, "cheb_filter: degree must be >= 1");
+  if (degree >= 2 && g_wave_mode != 0 && A.rows == A.cols) {
+    // several steps per launch where the operator's bandwidth allows it
+    const size_t bytes = wave_sync_bytes(A.rows);
+    void* sync = nullptr;
+    FE_CHECK_CUDA(cudaMallocAsync(&sync, bytes, s));
+    bool done = false;
+    try {
+      done = cheb_filter_wave<T>(A, X, ld, scratch, ld, ncols, degree, c, d, sync, bytes, s);
+    } catch (...) {
+      cudaFreeAsync(sync, s);
+      throw;
+    }
+    FE_CHECK_CUDA(cudaFreeAsync(sync, s));
+    if (done) return;
+  }
   // Y1 = c*A*Y0 + d*Y0 into scratch; then Y_k overwrites Y_{k-2} in place.
   csr_spmm<T>(A, X, ld, scratch, ld, nullptr, 0, ncols, c, d, 0.0, s);
   T* prev = X;       // Y_{k-2}

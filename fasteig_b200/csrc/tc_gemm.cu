@@ -35,6 +35,7 @@ namespace fe {
 
 int read_spmm_status(bool clear);
 void set_spmm_mode(int mode);
+void set_wave_mode(int mode);
 void set_f64_gemm_mode(int mode);
 
 __device__ int g_tc_status = 0;  // 0 = ok, otherwise a code of the first failed wait
@@ -1032,8 +1033,18 @@ extern "C" int fe_device_status(int32_t* status, int32_t clear) {
 
 extern "C" int fe_set_spmm_kernel(int32_t mode) {
   return fe::guarded("fe_set_spmm_kernel", [&] {
-    FE_REQUIRE(mode >= 0 && mode <= 6, "mode must be 0..6");
+    FE_REQUIRE(mode >= 0 && mode <= 7, "mode must be 0..7");
     fe::set_spmm_mode(mode);
+  });
+}
+
+extern "C" int fe_set_cheb_wave_kernel(int32_t mode) {
+  return fe::guarded("fe_set_cheb_wave_kernel", [&] {
+    const bool panels = mode >= 100 && (mode / 100 == 1 || mode / 100 == 2 || mode / 100 == 4) &&
+                        mode % 100 >= 1 && mode % 100 <= 8;
+    FE_REQUIRE((mode >= 0 && mode <= 9) || (mode >= 12 && mode <= 18) || panels,
+               "mode must be 0..9, 12..18 or 100 P + S (P in 1, 2, 4; S in 1..8)");
+    fe::set_wave_mode(mode);
   });
 }
 

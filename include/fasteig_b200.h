@@ -207,8 +207,25 @@ int fe_selftest_wait_timeout(int64_t limit_cycles, int32_t code, void* stream);
  * pipelined kernel where it applies, 3 = row-batched kernel with narrower
  * column panels, 4 = mode 0 with each warp's next Z row prefetched into L2,
  * 5 = row-batched kernel with 16-byte lanes and up to 3 per lane, 6 = row-batched
- * kernel with 8-byte lanes and up to 3 per lane. */
+ * kernel with 8-byte lanes and up to 3 per lane, 7 = mode 0 with X and Z read
+ * through L2 only (ld.global.cg). */
 int fe_set_spmm_kernel(int32_t mode);
+/* Chebyshev filter schedule for all later filters in the process (fe_cheb_filter_*
+ * and the Chebyshev solver; the numerics are the same bit for bit): 0 = default,
+ * one SpMM launch per step; 1 = several filter steps per launch (levels of warps, each level one step, each
+ * trailing the previous one by the operator's bandwidth so the block it gathers is
+ * still in L2) where the operator is square with at least 4096 rows of <= 7 entries,
+ * the block splits into 1, 2 or 4 column panels of 32..160 8-byte vectors and a
+ * panel's window of 2 x bandwidth rows per level fits about 75% of L2 for at least
+ * two levels (measured slower than one step per launch on B200 for the 128^3
+ * well operator: the steps are bound by gather latency, not by DRAM bytes).
+ * For measurements: 2..8 = that many
+ * steps per launch whatever the L2 window, 9 = one step per launch through the
+ * multi-step kernel, 12..18 = 2..8 steps per launch with L1-cached coherent loads,
+ * 100 P + S = P column panels (1, 2 or 4) of S steps (1..8) per launch.
+ * A timed-out wait in the multi-step kernel records status 13 (see
+ * fe_device_status). */
+int fe_set_cheb_wave_kernel(int32_t mode);
 /* SpMM autotuner: times every SpMM kernel on operator A for an n-by-ncols block
  * in the Chebyshev-step form (precision 0 = FP64, 1 = FP32) on `stream` and
  * records the fastest on the handle (up to four widths per precision); later

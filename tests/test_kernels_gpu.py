@@ -102,7 +102,7 @@ def test_pipelined_and_register_spmm_agree_on_stencils(dtype, stencil, b):
     Xn, Zn = X.double().cpu().numpy(), Z.double().cpu().numpy()
     ref = 0.7 * (A.scipy() @ Xn) - 0.2 * Xn - Zn
     outs = []
-    for mode in (0, 1, 2, 3, 4, 5, 6):
+    for mode in (0, 1, 2, 3, 4, 5, 6, 7):
         assert fe.lib.fe_set_spmm_kernel(mode) == 0
         Zc = Z.clone()
         ops.cheb_step(dA, X, Zc, Zc, 0.7, -0.2, -1.0)
@@ -148,7 +148,7 @@ def test_pipelined_spmm_rows_without_diagonal(dtype, n, b, alpha, gamma, beta):
     ref = alpha * (A.scipy() @ Xn) + gamma * Xn + beta * Zn
     outs = []
     try:
-        for mode in (2, 0, 4, 5, 6):
+        for mode in (2, 0, 4, 5, 6, 7):
             assert fe.lib.fe_set_spmm_kernel(mode) == 0
             Y = torch.full_like(X, float("nan"))
             ops.cheb_step(dA, X, Z, Y, alpha, gamma, beta)
