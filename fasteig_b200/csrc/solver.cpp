@@ -64,6 +64,7 @@ struct Options {
   std::string precond = "none";    // none | jacobi (LOBPCG / Davidson corrections W = T R)
   std::string locking = "soft";    // Chebyshev: soft (reference) | hard
   int64_t tail_degree = 0;         // Chebyshev mixed: filter degree of the FP64 cycles (0 = degree)
+  int64_t tail_guard = 0;          // Chebyshev mixed: columns past nev in the FP64 cycles (0 = all)
   int64_t inject_wait_timeout = 0;  // test hook: status code of a forced bounded-wait timeout
   // Chebyshev hard locking: Rayleigh-Ritz with the Cholesky QR rotation folded in
   // ("fused", the default of precision=mixed) or Cholesky QR then Rayleigh-Ritz as
@@ -140,6 +141,10 @@ struct Options {
     else if (k == "mixed_switch") mixed_switch = as_double(v);
     else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
     else if (k == "tail_degree") tail_degree = as_int(v);
+    else if (k == "tail_guard") {
+      tail_guard = as_int(v);
+      if (tail_guard < 0) throw Error(FE_ERR_INVALID, "tail_guard must be >= 0");
+    }
     else if (k == "inject_wait_timeout") inject_wait_timeout = as_int(v);
     else if (k == "tail_filter") {
       tail_filter = lower(v);
@@ -1071,6 +1076,9 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
     if (opt.locking != "hard") locked = 0;  // soft: recheck the whole prefix (reference)
     while (locked < nev && rel[locked] <= lock_tol) ++locked;
     sub = std::max(sub, nev + std::min(locked, cap - nev));
+    // FP64 cycles of the mixed path with tail_guard: the subspace keeps that many
+    // columns past nev (the FP32 phase has brought every wanted pair to its floor).
+    if (l64 && opt.tail_guard > 0) sub = std::min(sub, nev + opt.tail_guard);
     it_done = iter + 1;
     double worst = 0.0;
     for (int64_t j = 0; j < nev; ++j) worst = std::max(worst, rel[j]);
@@ -1105,6 +1113,7 @@ void chebyshev_solve(const Csr& A, const Options& opt, double* eigenvalues, doub
         std::fprintf(stderr, "[fe] FP32 -> FP64 switch %.1f ms\n", ms_since(t_switch));
       locked = 0;  // FP64 sweeps refine every pair to tol
       while (locked < nev && rel[locked] <= tol) ++locked;
+      if (opt.tail_guard > 0) sub = std::min(sub, nev + opt.tail_guard);
     }
   }
   // Results: eigenvalues (sign restored) and the FP64 residual check of the

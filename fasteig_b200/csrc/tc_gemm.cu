@@ -97,6 +97,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Non-blocking test of a phase (try_wait may suspend the thread for a while first).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Bounded wait: `limit` SM clocks (about two seconds by default), then record `code`
 // in the launch's status word and give up.
 __device__ __forceinline__ bool mbar_wait_limit(uint64_t* bar, uint32_t parity, int code,
@@ -196,6 +209,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+
 __device__ __forceinline__ uint32_t tf32_rna(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -251,6 +277,8 @@ struct Smem {
   uint64_t* split;
   uint64_t* accum;
   uint32_t* tmem_slot;
+  uint64_t* sub_full;   // Gram: a sub-chunk accumulator is complete (2, by buffer)
+  uint64_t* sub_empty;  // Gram: a sub-chunk accumulator has been drained (2)
   int* status;  // the launch's status word (a solve's own, or the library default)
   __device__ float* a_hi(int s) const { return reinterpret_cast<float*>(base + s * kStageBytes); }
   __device__ float* a_lo(int s) const {
@@ -276,12 +304,15 @@ __device__ __forceinline__ Smem carve(uint8_t* dyn, int* status) {
   s.split = bars + 2 * kStages;
   s.accum = bars + 3 * kStages;
   s.tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * kStages + 1);
+  s.sub_full = bars + 3 * kStages + 2;
+  s.sub_empty = bars + 3 * kStages + 4;
   return s;
 }
 
 // Common prologue: barrier init (thread 0) and TMEM allocation (warp 1).
 __device__ __forceinline__ void prologue(const Smem& sm, int warp,
-                                         int split_warps = kSplitThreads / 32) {
+                                         int split_warps = kSplitThreads / 32,
+                                         uint32_t tmem_cols = kTmemCols) {
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&sm.full[s], 1);
@@ -289,13 +320,17 @@ __device__ __forceinline__ void prologue(const Smem& sm, int warp,
       mbar_init(&sm.split[s], split_warps);
     }
     mbar_init(sm.accum, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&sm.sub_full[b], 1);
+      mbar_init(&sm.sub_empty[b], split_warps);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     fence_proxy_async();
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(sm.tmem_slot)),
-                 "r"(kTmemCols)
+                 "r"(tmem_cols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -304,13 +339,14 @@ __device__ __forceinline__ void prologue(const Smem& sm, int warp,
   tc_fence_after();
 }
 
-__device__ __forceinline__ void epilogue_dealloc(const Smem& sm, int warp, uint32_t tmem) {
+__device__ __forceinline__ void epilogue_dealloc(const Smem& sm, int warp, uint32_t tmem,
+                                                 uint32_t tmem_cols = kTmemCols) {
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(kTmemCols)
+                 "r"(tmem_cols)
                  : "memory");
   }
 }
@@ -351,6 +387,49 @@ __device__ void mma_loop(const Smem& sm, uint32_t tmem, int nkb, uint32_t idesc)
   umma_commit(sm.accum);
 }
 
+// Gram MMA loop: the row chunk runs as sub-chunks of kGramSubStages K stages, each
+// accumulated from zero into one of two TMEM buffers (columns 0 and 256, alternating);
+// sub_full[b] fires when a sub-chunk's products are complete, and buffer b is reused
+// only after the split warps have drained it (sub_empty[b]).
+constexpr int kGramSubStages = 8;  // 256 rows
+constexpr uint32_t kGramTmemCols = 512;
+
+__device__ void mma_loop_gram(const Smem& sm, uint32_t tmem, int nkb, uint32_t idesc) {
+  const uint32_t lbo = 4096u, sbo = 512u, layout = kLayoutSW128Base32;  // MN-major operands
+  for (int kb = 0; kb < nkb; ++kb) {
+    const int s = kb % kStages;
+    const uint32_t ph = (kb / kStages) & 1u;
+    const int sub = kb / kGramSubStages;
+    const int buf = sub & 1;
+    const bool first = kb % kGramSubStages == 0;
+    if (first && sub >= 2) {
+      if (!mbar_wait(&sm.sub_empty[buf], static_cast<uint32_t>((sub >> 1) - 1) & 1u, 5,
+                     sm.status))
+        return;
+      tc_fence_after();
+    }
+    if (!mbar_wait(&sm.split[s], ph, 3, sm.status)) return;
+    tc_fence_after();
+    const uint32_t d = tmem + static_cast<uint32_t>(buf) * 256u;
+    const uint32_t ah = smem_u32(sm.a_hi(s)), al = smem_u32(sm.a_lo(s));
+    const uint32_t bh = smem_u32(sm.b_hi(s)), bl = smem_u32(sm.b_lo(s));
+#pragma unroll
+    for (int k = 0; k < kKB / 8; ++k) {
+      const uint32_t off = k * 1024u;
+      const uint64_t dah = smem_desc(ah + off, lbo, sbo, layout);
+      const uint64_t dal = smem_desc(al + off, lbo, sbo, layout);
+      const uint64_t dbh = smem_desc(bh + off, lbo, sbo, layout);
+      const uint64_t dbl = smem_desc(bl + off, lbo, sbo, layout);
+      const uint32_t acc = (!first || k > 0) ? 1u : 0u;
+      umma_tf32(d, dah, dbh, idesc, acc);
+      umma_tf32(d, dah, dbl, idesc, 1u);
+      umma_tf32(d, dal, dbh, idesc, 1u);
+    }
+    umma_commit(&sm.empty[s]);
+    if ((kb + 1) % kGramSubStages == 0 || kb + 1 == nkb) umma_commit(&sm.sub_full[buf]);
+  }
+}
+
 // ------------------------------------------------------------------ Gram ----
 // grid.x = k_tiles * m_tiles (k tile fastest), grid.y = row chunks.
 // A = X^T (MN-major: 4 boxes of 32 columns x 32 rows), B = Y (MN-major, 5 boxes).
@@ -375,7 +454,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   const int64_t r_end = min(n, r_begin + rows_per_chunk);
   const int nkb = static_cast<int>((r_end - r_begin + kKB - 1) / kKB);
 
-  prologue(sm, warp, kGramSplitThreads / 32);
+  prologue(sm, warp, kGramSplitThreads / 32, kGramTmemCols);
   const uint32_t tmem = *sm.tmem_slot;
 
   if (warp == 0 && lane == 0) {
@@ -393,16 +472,73 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         tma_load_2d(sm.b_hi(s) + c * (32 * kKB), &tmY, j0 + 32 * c, y, &sm.full[s]);
     }
   } else if (warp == 1) {
-    if (lane == 0) mma_loop<true>(sm, tmem, nkb, idesc_tf32(true, true));
+    if (lane == 0) mma_loop_gram(sm, tmem, nkb, idesc_tf32(true, true));
     __syncwarp();
   } else if (warp >= 2) {
     const int tid = threadIdx.x - 64;
+    // TMEM: the MMA's sub-chunk buffers at columns [0, kN) and [256, 256 + kN); the
+    // running sum at [160, 240) and [416, 496) (this warp's half of the columns).
+    // Each split warp owns TMEM lanes 32 (warp % 4) .. + 31 and half of the columns,
+    // and drains completed sub-chunks into the running sum in FP32 registers
+    // (round to nearest): the tensor-core accumulator's own rounding error then
+    // grows with the 256 rows of a sub-chunk instead of the whole chunk.
+    const int q = warp % 4;
+    const int c0 = ((warp - 2) / 4) * (kN / 2);
+    const uint32_t lane_base = tmem + (static_cast<uint32_t>(q * 32) << 16);
+    auto t2col = [](int c) -> uint32_t {
+      return c < kN / 2 ? 160u + static_cast<uint32_t>(c) : 336u + static_cast<uint32_t>(c);
+    };
+    const int nsub = (nkb + kGramSubStages - 1) / kGramSubStages;
+    int drained = 0;
+    bool failed = false;
+    auto drain = [&](int j) {
+      const uint32_t src = lane_base + static_cast<uint32_t>(j & 1) * 256u;
+      for (int c = c0; c < c0 + kN / 2; c += 16) {
+        float v[16];
+        tmem_ld16(src + c, v);
+        if (j > 0) {
+          float t[16];
+          tmem_ld16(lane_base + t2col(c), t);
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] += t[e];
+        }
+        tmem_st16(lane_base + t2col(c), v);
+      }
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.sub_empty[j & 1]);
+    };
+    // Drain the next sub-chunk if its products are complete (decided for the whole
+    // warp: tcgen05 loads and stores are warp-collective).
+    auto try_drain = [&]() {
+      if (drained >= nsub) return;
+      // every lane observes the phase (acquire) before the warp reads TMEM
+      if (__all_sync(0xffffffffu,
+                     mbar_test_wait(&sm.sub_full[drained & 1], (drained >> 1) & 1))) {
+        tc_fence_after();
+        drain(drained);
+        ++drained;
+      }
+    };
     // Rows past r_end inside the last block belong to the next chunk: the split
     // writes them as zeros, so they do not enter this chunk's sum.
-    for (int kb = 0; kb < nkb; ++kb) {
+    for (int kb = 0; kb < nkb && !failed; ++kb) {
       const int s = kb % kStages;
       const uint32_t ph = (kb / kStages) & 1u;
-      if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2, sm.status))) break;
+      // wait for the stage's operands, draining finished sub-chunks meanwhile (the
+      // MMA may be waiting for a drain before it frees this stage's buffers)
+      const long long t0 = clock64();
+      while (true) {
+        if (__all_sync(0xffffffffu, mbar_try_wait(&sm.full[s], ph))) break;
+        try_drain();
+        if (clock64() - t0 > 4000000000LL) {
+          if (lane == 0) atomicCAS(sm.status, 0, 2);
+          failed = true;
+          break;
+        }
+      }
+      if (failed) break;
       const int64_t y = r_begin + static_cast<int64_t>(kb) * kKB;
       const int64_t left = r_end - y;
       const int valid = left < kKB ? static_cast<int>(left) : kKB;
@@ -416,19 +552,27 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       fence_proxy_async();
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.split[s]);
+      try_drain();
     }
-    // Epilogue: TMEM lane = output row i (within the k tile), column = j. A warp
-    // reads the TMEM lane quarter warp % 4; warps 2-5 take columns [0, kN/2),
-    // warps 6-9 the rest.
-    if (mbar_wait(sm.accum, 0, 4, sm.status)) {
+    while (!failed && drained < nsub) {
+      if (!__all_sync(0xffffffffu,
+                      mbar_wait(&sm.sub_full[drained & 1], (drained >> 1) & 1, 4, sm.status))) {
+        failed = true;
+        break;
+      }
       tc_fence_after();
-      const int q = warp % 4;
-      const int c0 = ((warp - 2) / 4) * (kN / 2);
+      drain(drained);
+      ++drained;
+    }
+    // Epilogue: TMEM lane = output row i (within the k tile), column = j, from the
+    // running sum.
+    if (!failed) {
+      tc_fence_after();
       const int i = i0 + q * 32 + lane - sx;  // caller's column index in X
       float* out = partial + static_cast<int64_t>(blockIdx.y) * k * m;
       for (int c = c0; c < c0 + kN / 2; c += 16) {
         float v[16];
-        tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + c, v);
+        tmem_ld16(lane_base + t2col(c), v);
         if (i >= 0 && i < k) {
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
@@ -439,7 +583,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       }
     }
   }
-  epilogue_dealloc(sm, warp, tmem);
+  epilogue_dealloc(sm, warp, tmem, kGramTmemCols);
 }
 
 // With `symmetric` (X^T X: k == m, equal column shift `shift`), entries of tiles

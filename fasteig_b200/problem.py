@@ -17,7 +17,8 @@ import numpy as np
 from ._lib import check, lib
 
 _INT_KEYS = ("n", "nev", "maxiter", "maxdim", "maxblks", "degree", "blksize", "verbosity",
-             "print_every", "block", "tensor_cores", "tail_degree", "inject_wait_timeout")
+             "print_every", "block", "tensor_cores", "tail_degree", "tail_guard",
+             "inject_wait_timeout")
 _FLOAT_KEYS = ("tol", "shift", "amplification", "mixed_switch")
 _STR_KEYS = ("which", "solver", "precision", "bounds", "init", "logfile", "output_format",
              "precond", "locking", "rr", "tail_filter")

@@ -327,7 +327,9 @@ int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ld
  * precond=none|jacobi, init=host|device, mixed_switch=<FP32 floor>,
  * locking=soft|hard: Chebyshev soft locking is the reference's, hard locking
  * keeps locked pairs final and orthonormalizes and projects only the active
- * block). B != NULL makes the problem
+ * block; for precision=mixed also tail_degree=<filter degree of the FP64 cycles>,
+ * tail_guard=<columns past nev kept in the FP64 cycles>, tail_filter=refined|fp64,
+ * rr=fused|cholqr). B != NULL makes the problem
  * generalized (A x = l B x, B symmetric positive definite): LOBPCG and Davidson
  * then work in the B metric (extension; the reference's are standard-only), and
  * Krylov-Schur runs the reference's B-metric Lanczos on B^-1 A with B^-1
