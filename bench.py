@@ -62,7 +62,7 @@ def args_parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--kernel", default=None,
                    choices=["cheb_step_f32", "cheb_step_f64", "gram_tf32x3", "rotate_tf32x3",
-                            "gram_f64", "rotate_f64"],
+                            "gram_f64", "rotate_f64", "syevd_f64"],
                    help="run one kernel --launches times on the --side problem (profiling "
                         "driver; prints per-launch CUDA-event times, no bench line)")
     p.add_argument("--launches", type=int, default=4)
@@ -89,6 +89,8 @@ def run_kernel(a):
     import fasteig_b200 as fe
     from fasteig_b200 import ops
     fe.lib.fe_set_spmm_kernel(a.spmm_kernel)
+    if a.kernel == "syevd_f64":
+        return run_syevd(a)
     H = build_matrix(a)
     dA = fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values)
     n, b = H.n, a.block
@@ -115,17 +117,67 @@ def run_kernel(a):
     return 0
 
 
+def run_syevd(a):
+    """Profiling driver: fe_syevd_f64 on a --block x --block Gaussian symmetric matrix,
+    --launches timed calls after 3 warm-ups; eigenvalue error against numpy."""
+    import numpy as np
+    import torch
+    import fasteig_b200 as fe
+    k = a.block
+    rng = np.random.default_rng(0)
+    M = rng.standard_normal((k, k))
+    A = M + M.T
+    dA0 = torch.from_numpy(A).cuda()
+    dA = dA0.clone()
+    W = torch.zeros(k, dtype=torch.float64, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    need = fe.lib.fe_syevd_f64_workspace_bytes(k)
+    ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+
+    def call():
+        dA.copy_(dA0)
+        assert fe.lib.fe_syevd_f64(dA.data_ptr(), k, k, W.data_ptr(), info.data_ptr(),
+                                   ws.data_ptr(), need, st) == 0
+    for _ in range(3):
+        call()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.launches + 1)]
+    ev[0].record()
+    for i in range(a.launches):
+        call()
+        ev[i + 1].record()
+    torch.cuda.synchronize()
+    ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(a.launches)]
+    err = float(np.abs(W.cpu().numpy() - np.linalg.eigvalsh(A)).max() / np.abs(A).sum(1).max())
+    print(json.dumps({"kernel": a.kernel, "k": k, "ms_per_call": ms, "eig_err_over_norm": err,
+                      "info": int(info.item())}))
+    return 0
+
+
+def autotune_widths(a, dA):
+    """The SpMM kernel for this operator, picked by measurement at the block width and
+    at the narrower widths the filter runs on once pairs lock."""
+    widths = sorted({a.block, max(32, a.block // 2), max(32, a.block // 4)}, reverse=True)
+    return {prec: {str(w): dA.autotune(w, prec) for w in widths} for prec in ("fp32", "fp64")}
+
+
 def run_solve_only(a):
-    """Profiling driver: one solve of the workload (no warm-up, no bench line)."""
+    """Profiling driver: one solve of the workload (no warm-up, no bench line), with
+    the SpMM autotune done first as in the bench line; the solve is bracketed by
+    cudaProfilerStart/Stop (ncu --profile-from-start off captures the solve alone)."""
     import torch
     import fasteig_b200 as fe
     torch.cuda.set_device(0)
     H = build_matrix(a)
     dA = fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values)
+    autotune_widths(a, dA)
     p = fe.fasteig_problem(dA, solver="Chebyshev")
+    torch.cuda.synchronize()
     l0 = fe.lib.fe_launch_count()
+    torch.cuda.cudart().cudaProfilerStart()
     p.solve(solve_opts(a, a.solve_only, 1))
     torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
     conv = int((p.residual_norms() <= a.tol).sum())
     print(json.dumps({"solve": a.solve_only, "converged": conv,
                       "launches": int(fe.lib.fe_launch_count() - l0), "stats": p.stats}))
@@ -596,10 +648,7 @@ def main():
 
     H = build_matrix(a)
     dA = fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values)
-    # The SpMM kernel for this operator is picked by measurement at the block width
-    # and at the narrower widths the filter runs on once pairs lock.
-    widths = sorted({a.block, max(32, a.block // 2), max(32, a.block // 4)}, reverse=True)
-    tuned = {prec: {str(w): dA.autotune(w, prec) for w in widths} for prec in ("fp32", "fp64")}
+    tuned = autotune_widths(a, dA)
     seed = 1 + rank
     opts = solve_opts(a, "mixed", seed)
 

@@ -1244,6 +1244,19 @@ void csr_spmm_mode(int mode, const Csr& A, const T* X, int64_t ldx, T* Y, int64_
         try_pipe<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                          T(gamma), T(beta), ug, ub, s))
       return;
+  }
+  // Where the selected kernel does not apply (too few 16-byte vectors for modes 3 and
+  // 5, a block without 16-byte alignment or whole 16-byte rows), the row kernel with
+  // 8-byte lanes runs before the loop kernels (mode 1 asks for the loop kernel).
+  constexpr int V8 = 8 / sizeof(T);
+  auto aligned8 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; };
+  const bool vec8_ok = ncols % V8 == 0 && ldx % V8 == 0 && ldy % V8 == 0 && aligned8(X) &&
+                       aligned8(Y) && (!ub || (ldz % V8 == 0 && aligned8(Z)));
+  if (mode != 1 && vec8_ok &&
+      try_row_kernel<T, V8>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
+                            T(gamma), T(beta), ug, ub, s, 5, false, mode == 7))
+    return;
+  if (vec_ok) {
     dispatch_vec<T, VEC>(A, vals, X, ldx, Y, ldy, Z, ldz, static_cast<int>(ncols), T(alpha),
                          T(gamma), T(beta), ug, ub, s);
   } else {
