@@ -782,7 +782,9 @@ struct ChebLoop {
                       Stats& st) {
     cudaStream_t s = ctx.stream;
     const int64_t active = sub - locked;
+    const int64_t vw = 16 / static_cast<int64_t>(sizeof(T));
     bool done = false;
+    bool ritz_in_v = false;  // the Ritz vectors were written to V[:, locked:] directly
     if (fused) {
       // FP32 blocks: one Cholesky QR pass, its second pass folded into the
       // Rayleigh-Ritz; FP64 blocks (the mixed path's FP64 cycles, whose filtered
@@ -795,13 +797,17 @@ struct ChebLoop {
         ldq = b.Q.ld;
       }
       ev.record(2, s);
-      // The Ritz vectors go to S, or to Q (then copied to S) when Y is staged in S.
+      // The Ritz vectors go to S, or to Q (then copied to S) when Y is staged in S; or,
+      // when the first QR pass moved the block into Q and V's active columns are
+      // 16-byte aligned, straight into V[:, locked:] (no copy back afterwards).
       const bool y_in_s = Yq == b.S.data();
-      T* Xo = y_in_s ? b.Q.data() : b.S.data();
-      const int64_t ldxo = y_in_s ? b.Q.ld : b.S.ld;
+      ritz_in_v = Yq == b.Q.data() && aligned16(b.V.col(locked)) && b.V.ld % vw == 0;
+      T* Xo = ritz_in_v ? b.V.col(locked) : (y_in_s ? b.Q.data() : b.S.data());
+      const int64_t ldxo = ritz_in_v ? b.V.ld : (y_in_s ? b.Q.ld : b.S.ld);
       done = fused_rr<T>(ctx, sm, eig, A, sign, Yq, ldq, b.AQ.data(), b.AQ.ld, Xo, ldxo, n,
                          active, st);
-      if (done && y_in_s) {
+      if (!done) ritz_in_v = false;
+      if (done && y_in_s && !ritz_in_v) {
         FE_CHECK_CUDA(cudaMemcpy2DAsync(b.S.data(), b.S.ld * sizeof(T), b.Q.data(),
                                         b.Q.ld * sizeof(T), active * sizeof(T), n,
                                         cudaMemcpyDeviceToDevice, s));
@@ -835,17 +841,20 @@ struct ChebLoop {
                       s);
     }
     const int64_t nw = nev - locked;
-    const int64_t vw = 16 / static_cast<int64_t>(sizeof(T));
-    const int64_t nw_pad = std::min(((nw + vw - 1) / vw) * vw, b.S.ld);  // whole vectors
-    csr_spmm<T>(A, b.S.data(), b.S.ld, b.AQ.data(), b.AQ.ld, nullptr, 0, nw_pad, sign, 0.0, 0.0,
-                s);
+    const T* Xr = ritz_in_v ? b.V.col(locked) : b.S.data();  // the Ritz vectors
+    const int64_t ldr = ritz_in_v ? b.V.ld : b.S.ld;
+    const int64_t room = ritz_in_v ? b.V.ld - locked : b.S.ld;
+    const int64_t nw_pad = std::min(((nw + vw - 1) / vw) * vw, room);  // whole vectors
+    csr_spmm<T>(A, Xr, ldr, b.AQ.data(), b.AQ.ld, nullptr, 0, nw_pad, sign, 0.0, 0.0, s);
     st.spmm_launches += 1;
-    residual_norms<T>(b.AQ.data(), b.S.data(), nullptr, b.S.ld, n, nw, sm.W.as<double>(), nullptr,
-                      0, sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
+    residual_norms<T>(b.AQ.data(), Xr, nullptr, ldr, n, nw, sm.W.as<double>(), nullptr, 0,
+                      sm.rnorm.as<double>(), sm.xnorm.as<double>(), sm.rel.as<double>(),
                       sm.rws.get(), sm.rws.bytes(), s, 1);
-    FE_CHECK_CUDA(cudaMemcpy2DAsync(b.V.col(locked), b.V.ld * sizeof(T), b.S.data(),
-                                    b.S.ld * sizeof(T), active * sizeof(T), n,
-                                    cudaMemcpyDeviceToDevice, s));
+    if (!ritz_in_v) {
+      FE_CHECK_CUDA(cudaMemcpy2DAsync(b.V.col(locked), b.V.ld * sizeof(T), b.S.data(),
+                                      b.S.ld * sizeof(T), active * sizeof(T), n,
+                                      cudaMemcpyDeviceToDevice, s));
+    }
     W.resize(sub);
     rel.resize(sub, 0.0);
     std::fill(rel.begin() + nev, rel.end(), 0.0);  // guard columns: residuals not formed
