@@ -41,7 +41,7 @@ void set_f64_gemm_mode(int mode);
 __device__ int g_tc_status = 0;  // 0 = ok, otherwise a code of the first failed wait
 
 // Aligned 3xTF32 rotations on the persistent kernel (1) or one CTA per tile (0).
-static int g_rotate_persistent = 1;
+static int g_rotate_persistent = 2;  // 2: TMEM A operand, 1: shared-memory split, 0: per tile
 void set_rotate_persistent(int on) { g_rotate_persistent = on; }
 
 namespace {
@@ -188,6 +188,18 @@ __device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t adesc, uint6
       : "memory");
 }
 
+// The same MMA with A read from tensor memory (row i of A in TMEM lane i, one FP32/TF32
+// element per 32-bit column, K consecutive columns), B from shared memory.
+__device__ __forceinline__ void umma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
+                                             uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -219,6 +231,20 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
       "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
       "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
       "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+
+// 32 consecutive TMEM columns of this thread's lane (warp-collective).
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+      "%28, %29, %30, %31, %32};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]),
+      "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]),
+      "r"(r[29]), "r"(r[30]), "r"(r[31])
       : "memory");
 }
 
@@ -920,6 +946,247 @@ rotate_tc_persistent_kernel(const __grid_constant__ CUtensorMap tmX,
 // arrives on, for `limit` SM clocks, then records `code` in `status` (or the
 // library's default word) and returns. No copies are in flight, so the timeout
 // path leaves nothing behind.
+// Persistent rotation with X split once in registers and fed to the MMA from tensor
+// memory: the split warps read each raw X row of a stage from shared memory (row r of
+// the tile = TMEM lane r, one thread per row), round it to hi = rna(x), lo = rna(x - hi)
+// and store both into one of two TMEM A slots (32 columns each, in the columns the two
+// accumulators leave free), so the MMAs read only C's hi/lo tiles from shared memory.
+// Per K stage this moves 132 KB through shared memory where the split in place moves
+// 212 KB; the MMAs, their order and so the results are those of
+// rotate_tc_persistent_kernel, bit for bit.
+// Three A slots (one per pipeline stage), hi and lo 32 columns each, in the TMEM
+// columns the accumulators at [0, 160) and [256, 416) leave free.
+constexpr int kRotASlots = 3;
+__device__ __forceinline__ uint32_t rot_a_hi(int slot) {
+  return slot == 0 ? 160u : (slot == 1 ? 224u : 448u);
+}
+__device__ __forceinline__ uint32_t rot_a_lo(int slot) {
+  return slot == 0 ? 192u : (slot == 1 ? 416u : 480u);
+}
+constexpr int kTmemRotThreads = 448;  // producer, MMA, 8 split warps, 4 epilogue warps
+
+__global__ void __launch_bounds__(kTmemRotThreads, 1)
+rotate_tc_tmem_kernel(const __grid_constant__ CUtensorMap tmX,
+                      const __grid_constant__ CUtensorMap tmCh,
+                      const __grid_constant__ CUtensorMap tmCl, int64_t n, int k, int m,
+                      int m_tiles, int64_t total_tiles, float* __restrict__ Y, int64_t ldy,
+                      float alpha, float beta, int use_beta, int upper_tri, int* status) {
+  extern __shared__ uint8_t dyn_smem[];
+  const Smem sm = carve(dyn_smem, status);
+  // Accumulator full / empty and A-slot free barriers, after the TMEM address slot.
+  uint64_t* accf = reinterpret_cast<uint64_t*>(sm.tmem_slot + 2);
+  uint64_t* acce = accf + 2;
+  uint64_t* afree = acce + 2;
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+      mbar_init(&sm.split[s], 8);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
+    for (int b = 0; b < kRotASlots; ++b) mbar_init(&afree[b], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(sm.tmem_slot)),
+                 "r"(kPersistTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *sm.tmem_slot;
+  const int nkb_full = (k + kKB - 1) / kKB;
+  auto tile_nkb = [&](int j0) {
+    return upper_tri ? (min(k, j0 + kN) + kKB - 1) / kKB : nkb_full;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t g = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; ok && t < total_tiles; t += gridDim.x) {
+        const int j0 = static_cast<int>(t % m_tiles) * kN;
+        const int r0 = static_cast<int>((t / m_tiles) * kM);
+        const int nkb = tile_nkb(j0);
+        for (int kb = 0; kb < nkb; ++kb, ++g) {
+          const int s = static_cast<int>(g % kStages);
+          const uint32_t ph = (g / kStages) & 1u;
+          if (!mbar_wait(&sm.empty[s], ph ^ 1u, 1, sm.status)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&sm.full[s], kABytes + 2 * kBBytes);
+          tma_load_2d(sm.a_hi(s), &tmX, kb * kKB, r0, &sm.full[s]);
+          tma_load_2d(sm.b_hi(s), &tmCh, kb * kKB, j0, &sm.full[s]);
+          tma_load_2d(sm.b_lo(s), &tmCl, kb * kKB, j0, &sm.full[s]);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_tf32(false, false);
+      uint32_t g = 0;
+      int lt = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; ok && t < total_tiles; t += gridDim.x, ++lt) {
+        const int j0 = static_cast<int>(t % m_tiles) * kN;
+        const int nkb = tile_nkb(j0);
+        const int b = lt & 1;
+        if (lt >= 2 &&
+            !mbar_wait(&acce[b], static_cast<uint32_t>((lt >> 1) - 1) & 1u, 5, sm.status))
+          break;
+        tc_fence_after();
+        const uint32_t acc_tmem = tmem + static_cast<uint32_t>(b) * kAccStride;
+        for (int kb = 0; kb < nkb; ++kb, ++g) {
+          const int s = static_cast<int>(g % kStages);
+          const uint32_t ph = (g / kStages) & 1u;
+          const int slot = static_cast<int>(g % kRotASlots);
+          if (!mbar_wait(&sm.split[s], ph, 3, sm.status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t ahi = tmem + rot_a_hi(slot), alo = tmem + rot_a_lo(slot);
+          const uint32_t bh = smem_u32(sm.b_hi(s)), bl = smem_u32(sm.b_lo(s));
+#pragma unroll
+          for (int kk = 0; kk < kKB / 8; ++kk) {
+            const uint32_t a_h = ahi + static_cast<uint32_t>(kk * 8);
+            const uint32_t a_l = alo + static_cast<uint32_t>(kk * 8);
+            const uint64_t dbh = smem_desc(bh + kk * 32u, 16u, 1024u, kLayoutSW128);
+            const uint64_t dbl = smem_desc(bl + kk * 32u, 16u, 1024u, kLayoutSW128);
+            const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+            umma_tf32_ta(acc_tmem, a_h, dbh, idesc, acc);
+            umma_tf32_ta(acc_tmem, a_h, dbl, idesc, 1u);
+            umma_tf32_ta(acc_tmem, a_l, dbh, idesc, 1u);
+          }
+          umma_commit(&sm.empty[s]);
+          umma_commit(&afree[slot]);
+        }
+        if (!ok) break;
+        umma_commit(&accf[b]);
+      }
+    }
+    __syncwarp();
+  } else if (warp < 10) {
+    // split warps: warp w owns TMEM lanes 32 (w % 4) .. + 31 = rows of the X tile and
+    // half (w - 2) / 4 of the stage's 32 K columns
+    const int q = warp % 4;
+    const int h = (warp - 2) / 4;
+    const int r = q * 32 + lane;
+    const uint32_t lane_base = tmem + (static_cast<uint32_t>(q * 32) << 16);
+    uint32_t g = 0;
+    bool ok = true;
+    for (int64_t t = blockIdx.x; ok && t < total_tiles; t += gridDim.x) {
+      const int j0 = static_cast<int>(t % m_tiles) * kN;
+      const int nkb = tile_nkb(j0);
+      for (int kb = 0; kb < nkb; ++kb, ++g) {
+        const int s = static_cast<int>(g % kStages);
+        const uint32_t ph = (g / kStages) & 1u;
+        const int slot = static_cast<int>(g % kRotASlots);
+        if (!__all_sync(0xffffffffu, mbar_wait(&sm.full[s], ph, 2, sm.status))) {
+          ok = false;
+          break;
+        }
+        if (g >= static_cast<uint32_t>(kRotASlots) &&
+            !__all_sync(0xffffffffu,
+                        mbar_wait(&afree[slot], ((g / kRotASlots) - 1) & 1u, 6, sm.status))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        // row r of the tile: 128 bytes, 16-byte chunk j stored at j ^ (r % 8) (128-byte
+        // swizzle of the TMA box); this warp takes chunks 4h .. 4h + 3
+        const uint8_t* rowp = reinterpret_cast<const uint8_t*>(sm.a_hi(s)) + r * 128;
+        uint32_t hi[16], lo[16];
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const int j = 4 * h + jj;
+          const float4 v = *reinterpret_cast<const float4*>(rowp + ((j ^ (r & 7)) * 16));
+          float4 hv, lv;
+          split4(v, hv, lv);
+          hi[4 * jj] = __float_as_uint(hv.x);
+          hi[4 * jj + 1] = __float_as_uint(hv.y);
+          hi[4 * jj + 2] = __float_as_uint(hv.z);
+          hi[4 * jj + 3] = __float_as_uint(hv.w);
+          lo[4 * jj] = __float_as_uint(lv.x);
+          lo[4 * jj + 1] = __float_as_uint(lv.y);
+          lo[4 * jj + 2] = __float_as_uint(lv.z);
+          lo[4 * jj + 3] = __float_as_uint(lv.w);
+        }
+        tmem_st16(lane_base + rot_a_hi(slot) + 16u * h, reinterpret_cast<const float*>(hi));
+        tmem_st16(lane_base + rot_a_lo(slot) + 16u * h, reinterpret_cast<const float*>(lo));
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.split[s]);
+      }
+    }
+  } else {
+    const int q = warp % 4;
+    int lt = 0;
+    for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x, ++lt) {
+      const int j0 = static_cast<int>(t % m_tiles) * kN;
+      const int64_t r0 = (t / m_tiles) * kM;
+      const int b = lt & 1;
+      if (!mbar_wait(&accf[b], static_cast<uint32_t>(lt >> 1) & 1u, 4, sm.status)) break;
+      tc_fence_after();
+      const int64_t r = r0 + q * 32 + lane;
+      const uint32_t base = tmem + static_cast<uint32_t>(b) * kAccStride +
+                            (static_cast<uint32_t>(q * 32) << 16);
+      for (int c = 0; c < kN; c += 16) {
+        float v[16];
+        tmem_ld16(base + c, v);
+        if (r >= n) continue;
+        float* yr = Y + r * ldy + j0 + c;
+        if (j0 + c + 16 <= m) {
+#pragma unroll
+          for (int e = 0; e < 16; e += 4) {
+            float4 o = make_float4(alpha * v[e], alpha * v[e + 1], alpha * v[e + 2],
+                                   alpha * v[e + 3]);
+            if (use_beta) {
+              const float4 y = *reinterpret_cast<const float4*>(yr + e);
+              o.x = fmaf(beta, y.x, o.x);
+              o.y = fmaf(beta, y.y, o.y);
+              o.z = fmaf(beta, y.z, o.z);
+              o.w = fmaf(beta, y.w, o.w);
+            }
+            *reinterpret_cast<float4*>(yr + e) = o;
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            if (j0 + c + e < m) {
+              float out = alpha * v[e];
+              if (use_beta) out = fmaf(beta, yr[e], out);
+              yr[e] = out;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[b]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kPersistTmemCols)
+                 : "memory");
+  }
+}
+
 __global__ void wait_probe_kernel(int* status, long long limit, int code) {
   __shared__ __align__(8) uint64_t bar;
   if (threadIdx.x == 0) {
@@ -1121,13 +1388,20 @@ void rotate_tc(const float* X, int64_t ldx, const double* C, int64_t ldc, float*
       FE_CHECK_CUDA(cudaFuncSetAttribute(rotate_tc_persistent_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kSmemBytes));
+      FE_CHECK_CUDA(cudaFuncSetAttribute(rotate_tc_tmem_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kSmemBytes));
     });
     const int64_t ctas = std::min<int64_t>(total_tiles, num_sms());
-    rotate_tc_persistent_kernel<<<static_cast<unsigned>(ctas), kPersistThreads, kSmemBytes, s>>>(
+    const bool tmem_a = g_rotate_persistent == 2;
+    auto kern = tmem_a ? rotate_tc_tmem_kernel : rotate_tc_persistent_kernel;
+    kern<<<static_cast<unsigned>(ctas), tmem_a ? kTmemRotThreads : kPersistThreads, kSmemBytes,
+           s>>>(
         mx, mh, ml, n, static_cast<int>(k), static_cast<int>(m), static_cast<int>(m_tiles),
         total_tiles, Y, ldy, static_cast<float>(alpha), static_cast<float>(beta), beta != 0.0,
         upper_tri ? 1 : 0, current_status_word());
-    check_launch("rotate_tc_persistent_kernel");
+    check_launch(g_rotate_persistent == 2 ? "rotate_tc_tmem_kernel"
+                                          : "rotate_tc_persistent_kernel");
     return;
   }
   dim3 grid(static_cast<unsigned>(row_tiles * m_tiles));
@@ -1194,8 +1468,10 @@ extern "C" int fe_set_cheb_wave_kernel(int32_t mode) {
 
 extern "C" int fe_set_tc_rotate_kernel(int32_t mode) {
   return fe::guarded("fe_set_tc_rotate_kernel", [&] {
-    FE_REQUIRE(mode >= 0 && mode <= 1, "mode must be 0 or 1");
-    fe::set_rotate_persistent(mode == 0 ? 1 : 0);
+    FE_REQUIRE(mode >= 0 && mode <= 2, "mode must be 0, 1 or 2");
+    // 0: persistent, X split in registers into TMEM; 1: one CTA per tile; 2: persistent,
+    // X split in shared memory
+    fe::set_rotate_persistent(mode == 0 ? 2 : (mode == 1 ? 0 : 1));
   });
 }
 

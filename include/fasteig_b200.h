@@ -239,9 +239,11 @@ int fe_csr_autotune(fe_csr_t A, int64_t ncols, int32_t precision, void* stream, 
  * differ only in the order of the rounded additions. */
 int fe_set_f64_gemm_kernel(int32_t mode);
 /* 3xTF32 rotation kernel for 16-byte aligned outputs, for all later calls:
- * 0 = default (persistent kernel, one CTA per SM looping over tiles with two
- * TMEM accumulators), 1 = one CTA per tile. Same arithmetic; unaligned outputs
- * always use the one-CTA-per-tile kernel with its staged epilogue. */
+ * 0 = default (persistent, one CTA per SM looping over tiles with two TMEM
+ * accumulators; X split into hi/lo in registers and read by the MMA from tensor
+ * memory), 1 = one CTA per tile, 2 = persistent with X split in shared memory.
+ * Same MMAs in the same order (bit-identical results); unaligned outputs always use
+ * the one-CTA-per-tile kernel with its staged epilogue. */
 int fe_set_tc_rotate_kernel(int32_t mode);
 
 /* ---------------------------------------------------------------------

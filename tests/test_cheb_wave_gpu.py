@@ -1,12 +1,14 @@
-"""Multi-step Chebyshev filter (cheb_wave_kernel, several filter steps per launch as a
-wavefront over row tiles) against one SpMM launch per step, through the C ABI.
+"""Multi-step Chebyshev filter (cheb_wave_kernel: several filter steps per launch, each
+step a level of warps trailing the previous one by the operator's bandwidth) against one
+SpMM launch per step, through the C ABI.
 
 The multi-step schedule changes only when each row is computed, not how: every row of
-every step runs the single-step row kernel's arithmetic, so results must be equal
-bit for bit (rtol = atol = 0) for both precisions, even and odd degrees, row counts
-that are not a multiple of the 64-row tile, blocks narrower than a full panel, and
-operators with a bandwidth of about n (each level waiting on nearly all of the
-previous one, or, where the window does not fit L2, one step per launch). The filter recurrence itself is checked against the oracle in
+every step runs the single-step row kernel's arithmetic, so results must be equal bit
+for bit (rtol = atol = 0) for both precisions, even and odd degrees, row counts that are
+not a multiple of the 1024-row completion block, blocks narrower than a full panel, and
+operators with a bandwidth of about n (each level waiting on nearly all of the previous
+one, or, where the window does not fit L2, one step per launch). The filter recurrence
+itself is checked against the oracle in
 test_kernels_gpu.py::test_cheb_filter_matches_oracle_recurrence.
 """
 import numpy as np
@@ -27,7 +29,7 @@ def _filter(dA, X0, degree, c, d, wave):
         ops.cheb_filter(dA, X, S, degree, c, d)
         torch.cuda.synchronize()
     finally:
-        fe.lib.fe_set_cheb_wave_kernel(1)
+        fe.lib.fe_set_cheb_wave_kernel(0)
     import ctypes
     status = np.zeros(1, dtype=np.int32)
     assert fe.lib.fe_device_status(status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), 1) == 0
@@ -78,7 +80,7 @@ def test_wave_filter_ragged_rows_and_strided_block():
                                          0.15, -1.1, None) == 0
         torch.cuda.synchronize()
         outs.append(X)
-    fe.lib.fe_set_cheb_wave_kernel(1)
+    fe.lib.fe_set_cheb_wave_kernel(0)
     assert torch.equal(outs[0], outs[1])
     assert torch.equal(outs[1][:, 320:], base[:, 320:])  # columns past ncols untouched
 
@@ -121,12 +123,12 @@ def test_wave_filter_solver_bitwise_equal():
         assert fe.lib.fe_set_cheb_wave_kernel(wave) == 0
         p = fe.fasteig_problem(dA, solver="Chebyshev")
         o = fe.fasteig_options()
-        for k, v in dict(solver="Chebyshev", nev=24, which="SR", tol=1e-8, maxiter=300, seed=1, degree=12, block=40,
-                         bounds="ritz", amplification=1e6, precision="mixed",
-                         locking="hard").items():
+        for k, v in dict(solver="Chebyshev", nev=24, which="SR", tol=1e-8, maxiter=300,
+                         seed=1, degree=12, block=40, bounds="ritz", amplification=1e6,
+                         precision="mixed", locking="hard").items():
             assert o.set(k, v), k
         p.solve(o, want_vectors=True)
         res.append((p.eigenvalues().copy(), p.stats["iterations"]))
-    fe.lib.fe_set_cheb_wave_kernel(1)
+    fe.lib.fe_set_cheb_wave_kernel(0)
     np.testing.assert_array_equal(res[0][0], res[1][0])
     assert res[0][1] == res[1][1]

@@ -104,7 +104,7 @@ def test_rotate_tf32x3_deflation_update_in_place(locked, sub):
     assert np.array_equal(V[:, :locked].double().cpu().numpy(), V64[:, :locked])
 
 
-@pytest.fixture(params=[0, 1], ids=["persistent", "per_tile"])
+@pytest.fixture(params=[0, 1, 2], ids=["persistent_tmem_a", "per_tile", "persistent_smem_split"])
 def rotate_kernel(request):
     import fasteig_b200 as fe
     assert fe.lib.fe_set_tc_rotate_kernel(request.param) == 0
@@ -116,9 +116,10 @@ def rotate_kernel(request):
                                    (33333, 320, 200), (131072, 64, 160)])
 @pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.0, 1.0)])
 def test_rotate_tf32x3_both_kernels(rotate_kernel, n, k, m, alpha, beta):
-    """The persistent (several tiles per CTA, alternating TMEM accumulators) and the
-    one-CTA-per-tile rotation give the same product within the 3xTF32 bound, and the
-    persistent one is bit-identical to the per-tile one (same MMAs, same order)."""
+    """The persistent rotations (several tiles per CTA, alternating TMEM accumulators;
+    X split in registers and read by the MMA from TMEM, or split in shared memory) and
+    the one-CTA-per-tile rotation give the same product within the 3xTF32 bound, and are
+    bit-identical to each other (same MMAs, same order)."""
     import fasteig_b200 as fe
     from fasteig_b200 import ops
     assert ops.device_status(clear=True) == 0
@@ -134,12 +135,12 @@ def test_rotate_tf32x3_both_kernels(rotate_kernel, n, k, m, alpha, beta):
     scale = np.abs(X64) @ np.abs(C64) + (abs(beta) * np.abs(Y64) if beta else 0.0)
     err = np.abs(Y.double().cpu().numpy() - ref)
     assert np.all(err <= (k + 4) * 2.0 ** -22 * scale + 1e-30), (err / scale).max()
-    other = 1 - rotate_kernel
-    assert fe.lib.fe_set_tc_rotate_kernel(other) == 0
-    Y2 = Y0.clone()
-    ops.rotate_tf32x3(X, Cm, Y2, alpha, beta)
-    torch.cuda.synchronize()
-    assert torch.equal(Y, Y2)
+    for other in {0, 1, 2} - {rotate_kernel}:
+        assert fe.lib.fe_set_tc_rotate_kernel(other) == 0
+        Y2 = Y0.clone()
+        ops.rotate_tf32x3(X, Cm, Y2, alpha, beta)
+        torch.cuda.synchronize()
+        assert torch.equal(Y, Y2), other
 
 
 @pytest.mark.parametrize("n,k,off", [(5000, 320, 0), (33333, 300, 1), (4096, 400, 3), (777, 130, 2)])
