@@ -55,8 +55,10 @@ def args_parse():
                         "whole subspace) or hard (over the active block only)")
     p.add_argument("--mixed-switch", type=float, default=1e-6,
                    help="FP32 locking threshold and FP32 -> FP64 switch of the mixed path")
-    p.add_argument("--tail-degree", type=int, default=0,
+    p.add_argument("--tail-degree", type=int, default=20,
                    help="mixed: filter degree of the FP64 cycles after the switch (0 = --degree)")
+    p.add_argument("--tail-guard", type=int, default=16,
+                   help="mixed: columns past nev kept in the FP64 cycles (0 = the whole block)")
     p.add_argument("--verbosity", type=int, default=0, help="solver log level (2: per cycle)")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison solve")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
@@ -463,6 +465,8 @@ def solve_opts(a, precision, seed, locking=None):
         assert o.set(k, v), k
     if a.tail_degree > 0 and precision == "mixed":
         assert o.set("tail_degree", a.tail_degree)
+    if a.tail_guard > 0 and precision == "mixed":
+        assert o.set("tail_guard", a.tail_guard)
     if a.verbosity:
         assert o.set("verbosity", a.verbosity)
     return o
@@ -779,6 +783,7 @@ def main():
             "impl_config": {"precision": "mixed (FP32 filter/SpMM/rotation, FP64-accumulated "
                                          "Gram, FP64 Cholesky/eig/residual, FP64 final sweeps)",
                             "mixed_switch": a.mixed_switch, "tail_degree": a.tail_degree or a.degree,
+                            "tail_guard": a.tail_guard or None,
                             "init": "device counter RNG",
                             "parallelism": f"replicas x{world}", "spmm_kernel_autotuned": tuned},
             "converged_pairs": converged, "latency_s": {"p50": lat[len(lat) // 2], "max": lat[-1]},

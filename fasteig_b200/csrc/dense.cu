@@ -455,6 +455,34 @@ __global__ void diag_scale_kernel(double* __restrict__ M, int rows, int cols, in
   *x *= both ? d[i] * d[j] : d[i];
 }
 
+// Residual split of an FP64 block for the projected operator of the mixed path's FP64
+// cycles: Y32 = float(Y), E32 = float(AY - Y diag(theta)) (row-major blocks).
+__global__ void shift_split_kernel(int64_t n, int k, const double* __restrict__ AY, int64_t lday,
+                                   const double* __restrict__ Y, int64_t ldy,
+                                   const double* __restrict__ theta, float* __restrict__ Y32,
+                                   float* __restrict__ E32, int64_t ld32) {
+  const int64_t total = n * k;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx / k;
+    const int j = static_cast<int>(idx % k);
+    const double y = Y[i * ldy + j];
+    Y32[i * ld32 + j] = static_cast<float>(y);
+    E32[i * ld32 + j] = static_cast<float>(AY[i * lday + j] - theta[j] * y);
+  }
+}
+
+// H[r, c] = G[r, c] theta[c] + H1[r, c] (column-major, leading dimension ld).
+__global__ void gram_shift_combine_kernel(int k, int64_t ld, const double* __restrict__ G,
+                                          const double* __restrict__ theta,
+                                          const double* __restrict__ H1, double* __restrict__ H) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<int64_t>(k) * k) return;
+  const int r = static_cast<int>(idx % k), c = static_cast<int>(idx / k);
+  const int64_t o = static_cast<int64_t>(c) * ld + r;
+  H[o] = fma(G[o], theta[c], H1[o]);
+}
+
 void small_gemm(bool trans_a, int64_t m, int64_t n, int64_t kk, double alpha, const double* A,
                 int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
                 cudaStream_t s) {
@@ -479,6 +507,27 @@ void diag_scale(double* M, int64_t rows, int64_t cols, int64_t ldm, const double
   diag_scale_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
       M, static_cast<int>(rows), static_cast<int>(cols), ldm, d, both ? 1 : 0);
   check_launch("diag_scale_kernel");
+}
+
+void shift_split(int64_t n, int64_t k, const double* AY, int64_t lday, const double* Y,
+                 int64_t ldy, const double* theta, float* Y32, float* E32, int64_t ld32,
+                 cudaStream_t s) {
+  if (n <= 0 || k <= 0) return;
+  const int64_t total = n * k;
+  const unsigned blocks =
+      static_cast<unsigned>(std::min<int64_t>((total + 255) / 256, 8LL * num_sms()));
+  shift_split_kernel<<<blocks, 256, 0, s>>>(n, static_cast<int>(k), AY, lday, Y, ldy, theta, Y32,
+                                            E32, ld32);
+  check_launch("shift_split_kernel");
+}
+
+void gram_shift_combine(int64_t k, int64_t ld, const double* G, const double* theta,
+                        const double* H1, double* H, cudaStream_t s) {
+  if (k <= 0) return;
+  const int64_t total = k * k;
+  gram_shift_combine_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
+      static_cast<int>(k), ld, G, theta, H1, H);
+  check_launch("gram_shift_combine_kernel");
 }
 
 void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s) {

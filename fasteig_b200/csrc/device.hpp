@@ -66,6 +66,13 @@ void potrf_upper(double* G, int64_t k, int64_t ldg, int32_t* info, cudaStream_t 
 void trinv_upper(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
                  cudaStream_t s);
 void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s);
+// Y32 = float(Y), E32 = float(AY - Y diag(theta)) (n x k row-major blocks), and
+// H = G diag(theta) + H1 (k x k column-major, leading dimension ld).
+void shift_split(int64_t n, int64_t k, const double* AY, int64_t lday, const double* Y,
+                 int64_t ldy, const double* theta, float* Y32, float* E32, int64_t ld32,
+                 cudaStream_t s);
+void gram_shift_combine(int64_t k, int64_t ld, const double* G, const double* theta,
+                        const double* H1, double* H, cudaStream_t s);
 // Small column-major FP64 products: C = alpha op(A) B + beta C, op(A) = A or A^T.
 void small_gemm(bool trans_a, int64_t m, int64_t n, int64_t kk, double alpha, const double* A,
                 int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,

@@ -65,6 +65,7 @@ struct Options {
   std::string locking = "soft";    // Chebyshev: soft (reference) | hard
   int64_t tail_degree = 0;         // Chebyshev mixed: filter degree of the FP64 cycles (0 = degree)
   int64_t tail_guard = 0;          // Chebyshev mixed: columns past nev in the FP64 cycles (0 = all)
+  std::string tail_rr = "split";   // Chebyshev mixed FP64 cycles: Y^T A Y as split | fp64
   int64_t inject_wait_timeout = 0;  // test hook: status code of a forced bounded-wait timeout
   // Chebyshev hard locking: Rayleigh-Ritz with the Cholesky QR rotation folded in
   // ("fused", the default of precision=mixed) or Cholesky QR then Rayleigh-Ritz as
@@ -141,7 +142,11 @@ struct Options {
     else if (k == "mixed_switch") mixed_switch = as_double(v);
     else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
     else if (k == "tail_degree") tail_degree = as_int(v);
-    else if (k == "tail_guard") {
+    else if (k == "tail_rr") {
+      tail_rr = lower(v);
+      if (tail_rr != "split" && tail_rr != "fp64")
+        throw Error(FE_ERR_INVALID, "tail_rr must be split or fp64");
+    } else if (k == "tail_guard") {
       tail_guard = as_int(v);
       if (tail_guard < 0) throw Error(FE_ERR_INVALID, "tail_guard must be >= 0");
     }
@@ -576,7 +581,8 @@ void cholqr(Context& ctx, SmallState& sm, const T* src, int64_t lds, T* dst, int
 template <typename T>
 bool fused_rr(Context& ctx, SmallState& sm, ProjectedEig& eig, const Csr& A, double sign,
               const T* Y, int64_t ldy, T* AY, int64_t lday, T* X, int64_t ldx, int64_t n, int64_t k,
-              Stats& st) {
+              Stats& st, const double* theta = nullptr, float* y32 = nullptr,
+              float* e32 = nullptr, int64_t ld32 = 0) {
   cudaStream_t s = ctx.stream;
   const int64_t ld = sm.cap;
   double* G = sm.Gk.as<double>();
@@ -586,7 +592,21 @@ bool fused_rr(Context& ctx, SmallState& sm, ProjectedEig& eig, const Csr& A, dou
   csr_spmm<T>(A, Y, ldy, AY, lday, nullptr, 0, k, sign, 0.0, 0.0, s);
   st.spmm_launches += 1;
   gram_block<T>(sm, Y, ldy, Y, ldy, n, k, k, G, s);
-  gram_block<T>(sm, Y, ldy, AY, lday, n, k, k, H, s);
+  bool split = false;
+  if constexpr (std::is_same_v<T, double>) {
+    // FP64 columns with Ritz estimates theta (the mixed path's FP64 cycles): Y^T A Y =
+    // (Y^T Y) diag(theta) + Y^T E with E = AY - Y diag(theta) about a residual's size
+    // against AY, so Y^T E needs only FP32-level relative accuracy (split-TF32 tensor
+    // cores on FP32 copies of Y and E); Y^T Y stays an FP64 Gram.
+    if (theta && y32 && e32) {
+      shift_split(n, k, AY, lday, Y, ldy, theta, y32, e32, ld32, s);
+      double* H1 = sm.Tmp.as<double>();
+      gram_block<float>(sm, y32, ld32, e32, ld32, n, k, k, H1, s);
+      gram_shift_combine(k, ld, G, theta, H1, H, s);
+      split = true;
+    }
+  }
+  if (!split) gram_block<T>(sm, Y, ldy, AY, lday, n, k, k, H, s);
   auto factor = [&] {
     FE_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int32_t), s));
     inv_sqrt_diag(G, k, ld, d, s);
@@ -646,7 +666,9 @@ struct ChebLoop {
   bool refine = false;
   bool theta_ready = false;
   Block<float> r32, z0, z1;  // refined-filter blocks (allocated on first use)
-  DeviceBuffer wave_sync;    // multi-step filter's tickets and flags (allocated on first use)
+  DeviceBuffer wave_sync;    // multi-step filter's completion counters (allocated on first use)
+  DeviceBuffer theta_dev;    // Ritz estimates of the columns the refined filter ran on
+  bool theta_valid = false;  // set by refined_filter for the current cycle
   PhaseEvents ev;
 
   ChebLoop(Context& c, const Csr& a, const Options& o, SmallState& s, ProjectedEig& e, double sg,
@@ -677,6 +699,7 @@ struct ChebLoop {
                                         (act_pad - active) * sizeof(T), n, s));
     };
     FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, 4 * sizeof(int32_t), s));
+    theta_valid = false;
     ev.record(0, s);
     // 1. Filter Y = T_degree(c*op + d*I) X_active, in place on V's active columns.
     if (upper != cutoff) {
@@ -804,8 +827,14 @@ struct ChebLoop {
       ritz_in_v = Yq == b.Q.data() && aligned16(b.V.col(locked)) && b.V.ld % vw == 0;
       T* Xo = ritz_in_v ? b.V.col(locked) : (y_in_s ? b.Q.data() : b.S.data());
       const int64_t ldxo = ritz_in_v ? b.V.ld : (y_in_s ? b.Q.ld : b.S.ld);
+      // FP64 cycles after a refined filter: the projected operator from the residual
+      // split (fused_rr), on the refined filter's free FP32 blocks
+      const bool split = std::is_same_v<T, double> && theta_valid && opt.tail_rr == "split" &&
+                         z0.data() != nullptr;
       done = fused_rr<T>(ctx, sm, eig, A, sign, Yq, ldq, b.AQ.data(), b.AQ.ld, Xo, ldxo, n,
-                         active, st);
+                         active, st, split ? theta_dev.as<double>() : nullptr,
+                         split ? z0.data() : nullptr, split ? z1.data() : nullptr,
+                         split ? z0.ld : 0);
       if (!done) ritz_in_v = false;
       if (done && y_in_s && !ritz_in_v) {
         FE_CHECK_CUDA(cudaMemcpy2DAsync(b.S.data(), b.S.ld * sizeof(T), b.Q.data(),
@@ -899,8 +928,10 @@ struct ChebLoop {
       }
       tm[j] = tcur;
     }
-    DeviceBuffer d_delta(delta.size() * sizeof(float)), d_tm(tm.size() * sizeof(double)),
-        d_theta(theta.size() * sizeof(double));
+    DeviceBuffer d_delta(delta.size() * sizeof(float)), d_tm(tm.size() * sizeof(double));
+    if (theta_dev.bytes() < theta.size() * sizeof(double))
+      theta_dev.resize(theta.size() * sizeof(double));
+    DeviceBuffer& d_theta = theta_dev;
     ctx.to_device(d_delta.as<float>(), delta.data(), delta.size());
     ctx.to_device(d_tm.as<double>(), tm.data(), tm.size());
     ctx.to_device(d_theta.as<double>(), theta.data(), theta.size());
@@ -925,6 +956,7 @@ struct ChebLoop {
     }
     refine_finish(n, cols, d_tm.as<double>(), cur, ld32, X, ldx, s);
     ctx.sync();  // the host tables are released on return
+    theta_valid = true;
   }
 
   void filter(T* X, int64_t ldx, T* Sc, int64_t lds, int64_t cols, double c, double d) {

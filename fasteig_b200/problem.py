@@ -21,7 +21,7 @@ _INT_KEYS = ("n", "nev", "maxiter", "maxdim", "maxblks", "degree", "blksize", "v
              "inject_wait_timeout")
 _FLOAT_KEYS = ("tol", "shift", "amplification", "mixed_switch")
 _STR_KEYS = ("which", "solver", "precision", "bounds", "init", "logfile", "output_format",
-             "precond", "locking", "rr", "tail_filter")
+             "precond", "locking", "rr", "tail_filter", "tail_rr")
 
 
 class fasteig_options:  # noqa: N801 - reference class name

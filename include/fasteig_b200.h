@@ -331,7 +331,10 @@ int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ld
  * keeps locked pairs final and orthonormalizes and projects only the active
  * block; for precision=mixed also tail_degree=<filter degree of the FP64 cycles>,
  * tail_guard=<columns past nev kept in the FP64 cycles>, tail_filter=refined|fp64,
- * rr=fused|cholqr). B != NULL makes the problem
+ * tail_rr=split|fp64 (the FP64 cycles' projected operator Y^T A Y as
+ * (Y^T Y) diag(theta) + Y^T (AY - Y diag(theta)) with the small second term on the
+ * split-TF32 tensor cores, or as one FP64 Gram), rr=fused|cholqr). B != NULL makes the
+ * problem
  * generalized (A x = l B x, B symmetric positive definite): LOBPCG and Davidson
  * then work in the B metric (extension; the reference's are standard-only), and
  * Krylov-Schur runs the reference's B-metric Lanczos on B^-1 A with B^-1
