@@ -4,7 +4,9 @@
 // workspaces, bounded by solve_memory_bytes); every admitted solve runs on its
 // own stream with all of its state (subspace, Ritz values, locking) on the
 // device, so the work of concurrently admitted requests overlaps on the GPU and
-// requests that arrive while others run join as soon as memory frees up.
+// requests that arrive while others run join as soon as memory frees up. A request
+// whose allocation fails while other solves run beside it goes back to the head of
+// the queue once and runs when nothing else does.
 //
 // The reference serves nothing: fasteig_problem::solve (src/fasteig_problem.cpp:
 // 340-437) is one blocking solve per call. Each request here runs exactly that
@@ -42,6 +44,7 @@ struct fe_server {
     size_t bytes = 0;
     std::vector<double> eigenvalues, residuals, stats;
     int state = 0;  // 0 queued, 1 running, 2 done
+    int retries = 0;  // allocation failures retried alone
     int rc = FE_OK;
     std::string error;
     clock::time_point t_submit, t_start, t_end;
@@ -89,6 +92,19 @@ struct fe_server {
       });
       {
         std::lock_guard<std::mutex> lock(mu);
+        if (rc == FE_ERR_ALLOC && r->retries == 0 && running > 1) {
+          // Out of device memory while other solves ran beside it (the admission
+          // estimate is a bound on this solve alone, not on allocator fragmentation):
+          // back to the head of the queue, to run when nothing else does.
+          r->retries = 1;
+          in_use -= r->bytes;
+          --running;
+          r->bytes = std::max(r->bytes, budget);
+          r->state = 0;
+          queue.push_front(r);
+          cv_work.notify_all();
+          continue;
+        }
         r->rc = rc;
         if (rc != FE_OK) r->error = fe_last_error();
         r->t_end = clock::now();

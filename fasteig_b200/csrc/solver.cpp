@@ -3161,8 +3161,10 @@ size_t solve_memory_bytes(const Csr& A, const Csr* B, const char* options) {
   if (opt.solver == "chebyshev") {
     cap = nev + std::min(nev, n - nev);
     if (opt.block > 0) cap = std::max(nev, std::min(opt.block, n));
-    // FP64: 4 loop blocks + 2 initial; mixed adds 4 FP32 blocks (half size).
-    blocks = opt.precision == "mixed" ? 4 + 2 + 2 + 1 : 4 + 2 + 1;
+    // FP64: 4 loop blocks + 2 initial; mixed adds 4 FP32 blocks (half size), the
+    // refined filter's 3 FP32 blocks and the widened copy of an FP32 block that an
+    // FP64-accumulated Gram retry allocates for its duration.
+    blocks = opt.precision == "mixed" ? 4 + 2 + 2 + 1.5 + 1 + 1 : 4 + 2 + 1;
   } else if (opt.solver == "lobpcg") {
     cap = std::min<int64_t>(n, 3 * std::max<int64_t>(nev, opt.block));
     blocks = 12;
@@ -3178,8 +3180,18 @@ size_t solve_memory_bytes(const Csr& A, const Csr* B, const char* options) {
     blocks = 3;
   }
   (void)B;
-  const double bytes = blocks * static_cast<double>(n) * ld(cap) * 8.0 +
-                       2.0 * static_cast<double>(cap) * cap * 8.0 * 8.0 + (64u << 20);
+  // Workspaces: Gram partials (the split-TF32 Gram's per-chunk tiles dominate),
+  // residual sums, rotation operands, the eigensolver, the multi-step filter's
+  // counters, the k x k FP64 matrices, and slack for small buffers.
+  const size_t gram_ws = std::max(gram_workspace_bytes(n, cap, cap),
+                                  tc_gram_workspace_bytes(n, cap, cap));
+  const double ws = static_cast<double>(gram_ws) +
+                    static_cast<double>(residual_workspace_bytes(n, cap)) +
+                    static_cast<double>(tc_rotate_workspace_bytes(cap, cap)) +
+                    static_cast<double>(syevd_single_workspace_bytes(cap)) +
+                    static_cast<double>(wave_sync_bytes(n)) +
+                    16.0 * static_cast<double>(cap) * cap * 8.0 + (64u << 20);
+  const double bytes = blocks * static_cast<double>(n) * ld(cap) * 8.0 + ws;
   return static_cast<size_t>(bytes);
 }
 
