@@ -114,7 +114,19 @@ void trim_cache(int device) {
     cudaFree(b.ptr);
   }
 }
+
+// The stream-ordered pool keeps what solves freed (release threshold: all of it);
+// return the unused part to the device.
+void trim_pool(int device) {
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+}
 }  // namespace
+
+void release_cached_memory(int device) {
+  trim_cache(device);
+  trim_pool(device);
+}
 
 void* big_alloc(size_t bytes, cudaStream_t s, size_t* granted) {
   int dev = 0;
@@ -140,7 +152,7 @@ void* big_alloc(size_t bytes, cudaStream_t s, size_t* granted) {
   cudaError_t e = cudaMalloc(&p, want);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    trim_cache(dev);
+    release_cached_memory(dev);
     e = cudaMalloc(&p, want);
   }
   if (e != cudaSuccess) {

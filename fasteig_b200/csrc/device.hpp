@@ -104,6 +104,8 @@ cudaStream_t& alloc_stream();
 void retain_pool_memory(int device);
 // Large blocks (>= 64 MiB) of a solve: exact-size reuse across solves (see dense.cu).
 void* big_alloc(size_t bytes, cudaStream_t s, size_t* granted);
+// Frees the cached solve blocks and trims the stream-ordered pool of `device`.
+void release_cached_memory(int device);
 void big_free(void* p, size_t granted, cudaStream_t s);
 constexpr size_t kBigBlockBytes = size_t(64) << 20;
 
@@ -146,6 +148,13 @@ class DeviceBuffer {
       return;
     }
     cudaError_t e = s_ ? cudaMallocAsync(&p_, bytes, s_) : cudaMalloc(&p_, bytes);
+    if (e != cudaSuccess) {
+      // give back what the caches hold and try once more
+      cudaGetLastError();
+      int dev = 0;
+      if (cudaGetDevice(&dev) == cudaSuccess) release_cached_memory(dev);
+      e = s_ ? cudaMallocAsync(&p_, bytes, s_) : cudaMalloc(&p_, bytes);
+    }
     if (e != cudaSuccess) {
       p_ = nullptr;
       throw Error(FE_ERR_ALLOC, std::string("cudaMalloc(") + std::to_string(bytes) +

@@ -4,9 +4,11 @@
 // workspaces, bounded by solve_memory_bytes); every admitted solve runs on its
 // own stream with all of its state (subspace, Ritz values, locking) on the
 // device, so the work of concurrently admitted requests overlaps on the GPU and
-// requests that arrive while others run join as soon as memory frees up. A request
-// whose allocation fails while other solves run beside it goes back to the head of
-// the queue once and runs when nothing else does.
+// requests that arrive while others run join as soon as memory frees up. Blocks that
+// finished solves left in the library's caches are returned to the device when free
+// memory falls short of a request's bound; a request that still runs out of memory
+// while other solves run beside it goes back to the head of the queue once and runs
+// when nothing else does.
 //
 // The reference serves nothing: fasteig_problem::solve (src/fasteig_problem.cpp:
 // 340-437) is one blocking solve per call. Each request here runs exactly that
@@ -86,13 +88,28 @@ struct fe_server {
         r->state = 1;
         r->t_start = clock::now();
       }
+      // Memory that finished solves left in the library's caches is not in the
+      // admission budget: give it back when the device has less free than this
+      // request may take.
+      {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b < r->bytes + (r->bytes >> 3))
+          fe::release_cached_memory(device);
+        else
+          cudaGetLastError();
+      }
       const int rc = fe::guarded("fe_server request", [&] {
         fe::solve_problem(*r->A, r->B, r->options.c_str(), r->eigenvalues.data(),
                           r->residuals.data(), nullptr, r->stats.data());
       });
+      const std::string err = rc != FE_OK ? std::string(fe_last_error()) : std::string();
+      const bool out_of_memory =
+          rc == FE_ERR_ALLOC ||
+          (rc == FE_ERR_CUDA && err.find("out of memory") != std::string::npos);
+      if (out_of_memory && r->retries == 0) fe::release_cached_memory(device);
       {
         std::lock_guard<std::mutex> lock(mu);
-        if (rc == FE_ERR_ALLOC && r->retries == 0 && running > 1) {
+        if (out_of_memory && r->retries == 0 && running > 1) {
           // Out of device memory while other solves ran beside it (the admission
           // estimate is a bound on this solve alone, not on allocator fragmentation):
           // back to the head of the queue, to run when nothing else does.
@@ -106,7 +123,7 @@ struct fe_server {
           continue;
         }
         r->rc = rc;
-        if (rc != FE_OK) r->error = fe_last_error();
+        if (rc != FE_OK) r->error = err;
         r->t_end = clock::now();
         r->state = 2;
         in_use -= r->bytes;
