@@ -16,6 +16,7 @@ _LAZY = {
     "fasteig_options": ".problem",
     "fasteig_problem": ".problem",
     "batch_krylov_schur": ".problem",
+    "grouped_chebyshev": ".problem",
     "Server": ".problem",
 }
 

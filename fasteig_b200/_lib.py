@@ -74,6 +74,7 @@ _SIGS = {
     "fe_csr_autotune": (C.c_int, [vp, i64, C.c_int32, vp, vp]),
     "fe_batch_krylov_schur": (C.c_int, [C.c_int32, vp, vp, C.c_char_p, vp, vp, vp, vp, vp, vp]),
     "fe_csr_block_diag": (C.c_int, [C.c_int32, vp, vp]),
+    "fe_grouped_chebyshev": (C.c_int, [C.c_int32, vp, vp, vp, vp, vp, vp]),
     "fe_syevd_batched_f64": (C.c_int, [C.c_int32, vp, vp, i64, vp, vp, vp]),
     "fe_server_create": (C.c_int, [C.c_int32, C.c_int32, i64, vp]),
     "fe_server_submit": (C.c_int, [vp, vp, vp, C.c_char_p, vp]),

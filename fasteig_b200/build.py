@@ -22,7 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
               "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 SOURCES = ["spmm.cu", "blocks.cu", "dmma.cu", "dense.cu", "tc_gemm.cu", "batch_ks.cu",
-           "lanczos.cu", "ingest.cu", "syevd.cu", "solver.cpp", "server.cpp"]
+           "lanczos.cu", "ingest.cu", "syevd.cu", "group_kernels.cu", "solver.cpp", "grouped.cpp",
+           "server.cpp"]
 LIBS: list = []
 
 

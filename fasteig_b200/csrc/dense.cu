@@ -250,7 +250,10 @@ potrf_upper_kernel(double* G, int k, int64_t ldg, int32_t* info) {
 constexpr int kPotrfNB = 32;
 
 __global__ void __launch_bounds__(1024)
-potrf_upper_blocked_kernel(double* G, int k, int64_t ldg, int32_t* info) {
+potrf_upper_blocked_kernel(double* G, int k, int64_t ldg, int32_t* info, int64_t batch_stride) {
+  // batched: CTA b factors the matrix batch_stride doubles after the previous one
+  G += static_cast<int64_t>(blockIdx.x) * batch_stride;
+  if (info) info += blockIdx.x;
   extern __shared__ double psm[];
   double* panel = psm;                      // [k][32]: panel[l * 32 + r] = R[l, j0 + r]
   double* diag = psm + static_cast<size_t>(k) * kPotrfNB;  // [32][33]
@@ -334,7 +337,10 @@ potrf_upper_blocked_kernel(double* G, int k, int64_t ldg, int32_t* info) {
 
 // One warp per column c of Rinv: back substitution R x = e_c.
 __global__ void trinv_upper_kernel(const double* __restrict__ R, int64_t ldr,
-                                   double* __restrict__ Rinv, int64_t ldi, int k) {
+                                   double* __restrict__ Rinv, int64_t ldi, int k,
+                                   int64_t batch_stride) {
+  R += static_cast<int64_t>(blockIdx.y) * batch_stride;
+  Rinv += static_cast<int64_t>(blockIdx.y) * batch_stride;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
   const int lane = threadIdx.x % 32;
   if (warp >= k) return;
@@ -354,7 +360,8 @@ __global__ void trinv_upper_kernel(const double* __restrict__ R, int64_t ldr,
   }
 }
 
-__global__ void symmetrize_kernel(double* P, int k, int64_t ldp) {
+__global__ void symmetrize_kernel(double* P, int k, int64_t ldp, int64_t batch_stride) {
+  P += static_cast<int64_t>(blockIdx.y) * batch_stride;
   const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (idx >= static_cast<int64_t>(k) * k) return;
   const int r = static_cast<int>(idx % k);
@@ -383,7 +390,7 @@ void potrf_upper(double* G, int64_t k, int64_t ldg, int32_t* info, cudaStream_t 
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
       attr = true;
     }
-    potrf_upper_blocked_kernel<<<1, 1024, smem, s>>>(G, static_cast<int>(k), ldg, info);
+    potrf_upper_blocked_kernel<<<1, 1024, smem, s>>>(G, static_cast<int>(k), ldg, info, 0);
     check_launch("potrf_upper_blocked_kernel");
     return;
   }
@@ -398,8 +405,42 @@ void trinv_upper(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_
   FE_REQUIRE(R != Rinv, "trinv_upper: in-place inverse is not supported");
   const int64_t threads = k * 32;
   trinv_upper_kernel<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, s>>>(
-      R, ldr, Rinv, ldi, static_cast<int>(k));
+      R, ldr, Rinv, ldi, static_cast<int>(k), 0);
   check_launch("trinv_upper_kernel");
+}
+
+// Batched forms for grouped solves: `count` k x k matrices `stride` doubles apart,
+// one info word per matrix.
+void potrf_upper_batched(double* G, int64_t k, int64_t ldg, int64_t stride, int64_t count,
+                         int32_t* info, cudaStream_t s) {
+  FE_REQUIRE(k >= 1 && ldg >= k && count >= 1 && count <= 65535 && stride >= ldg * k,
+             "potrf_upper_batched: invalid shape");
+  const size_t smem = (static_cast<size_t>(k) * kPotrfNB + 32 * 33) * sizeof(double);
+  FE_REQUIRE(smem <= 200 * 1024, "potrf_upper_batched: k too large for the blocked kernel");
+  FE_CHECK_CUDA(cudaFuncSetAttribute(potrf_upper_blocked_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  potrf_upper_blocked_kernel<<<static_cast<unsigned>(count), 1024, smem, s>>>(
+      G, static_cast<int>(k), ldg, info, stride);
+  check_launch("potrf_upper_blocked_kernel");
+}
+
+void trinv_upper_batched(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
+                         int64_t stride, int64_t count, cudaStream_t s) {
+  FE_REQUIRE(k >= 1 && ldr >= k && ldi >= k && count >= 1 && count <= 65535,
+             "trinv_upper_batched: invalid shape");
+  const int64_t threads = k * 32;
+  dim3 grid(static_cast<unsigned>((threads + 255) / 256), static_cast<unsigned>(count));
+  trinv_upper_kernel<<<grid, 256, 0, s>>>(R, ldr, Rinv, ldi, static_cast<int>(k), stride);
+  check_launch("trinv_upper_kernel");
+}
+
+void symmetrize_batched(double* P, int64_t k, int64_t ldp, int64_t stride, int64_t count,
+                        cudaStream_t s) {
+  if (k <= 0 || count <= 0) return;
+  const int64_t total = k * k;
+  dim3 grid(static_cast<unsigned>((total + 255) / 256), static_cast<unsigned>(count));
+  symmetrize_kernel<<<grid, 256, 0, s>>>(P, static_cast<int>(k), ldp, stride);
+  check_launch("symmetrize_kernel");
 }
 
 // C = alpha op(A) B + beta C for small column-major FP64 matrices (projected
@@ -547,7 +588,7 @@ void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s) {
   if (k == 0) return;
   const int64_t total = k * k;
   symmetrize_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
-      P, static_cast<int>(k), ldp);
+      P, static_cast<int>(k), ldp, 0);
   check_launch("symmetrize_kernel");
 }
 

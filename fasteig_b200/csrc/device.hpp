@@ -66,6 +66,13 @@ void potrf_upper(double* G, int64_t k, int64_t ldg, int32_t* info, cudaStream_t 
 void trinv_upper(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
                  cudaStream_t s);
 void symmetrize(double* P, int64_t k, int64_t ldp, cudaStream_t s);
+// Batched k x k forms (grouped solves): `count` matrices `stride` doubles apart.
+void potrf_upper_batched(double* G, int64_t k, int64_t ldg, int64_t stride, int64_t count,
+                         int32_t* info, cudaStream_t s);
+void trinv_upper_batched(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
+                         int64_t stride, int64_t count, cudaStream_t s);
+void symmetrize_batched(double* P, int64_t k, int64_t ldp, int64_t stride, int64_t count,
+                        cudaStream_t s);
 // Y32 = float(Y), E32 = float(AY - Y diag(theta)) (n x k row-major blocks), and
 // H = G diag(theta) + H1 (k x k column-major, leading dimension ld).
 void shift_split(int64_t n, int64_t k, const double* AY, int64_t lday, const double* Y,
@@ -92,6 +99,9 @@ void syevd_single(double* A, int64_t lda, int64_t k, double* W, int32_t* info, v
 size_t syevd_workspace_bytes(int count, int64_t lda);
 void syevd_batched(int count, const int32_t* m_host, double* A, int64_t lda, double* W,
                    double* Z, int32_t* info, void* ws, size_t ws_bytes, cudaStream_t s);
+// Batched form with every matrix of size k and no host-to-device copy (capturable).
+void syevd_batched_uniform(int count, int64_t k, double* A, int64_t lda, double* W, double* Z,
+                           int32_t* info, void* ws, size_t ws_bytes, cudaStream_t s);
 
 // ---- owning device buffer --------------------------------------------------
 // Stream on which this thread's DeviceBuffer allocations are ordered (set for the

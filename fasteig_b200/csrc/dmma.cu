@@ -66,7 +66,7 @@ template <int VEC>
 __global__ void __launch_bounds__(kGThreads)
 gram_dmma_kernel(const double* __restrict__ X, int64_t ldx, const double* __restrict__ Y,
                  int64_t ldy, int64_t n, int k, int m, int64_t rows_per_chunk, int symmetric,
-                 double* __restrict__ partial) {
+                 double* __restrict__ partial, const int64_t* __restrict__ chunk_rows) {
   if (symmetric && blockIdx.x > blockIdx.y) return;  // lower tiles mirror the upper ones
   extern __shared__ double smem[];
   const int tid = threadIdx.x;
@@ -76,8 +76,12 @@ gram_dmma_kernel(const double* __restrict__ X, int64_t ldx, const double* __rest
   const int wj = (warp >> 1) * 32;
   const int i0 = blockIdx.x * kGT;
   const int j0 = blockIdx.y * kGT;
-  const int64_t r_begin = static_cast<int64_t>(blockIdx.z) * rows_per_chunk;
-  const int64_t r_end = min(n, r_begin + rows_per_chunk);
+  // Equal chunks of rows_per_chunk rows, or (grouped Grams) the row range
+  // [chunk_rows[2z], chunk_rows[2z+1]) of one problem of a concatenated block.
+  const int64_t r_begin =
+      chunk_rows ? chunk_rows[2 * blockIdx.z] : static_cast<int64_t>(blockIdx.z) * rows_per_chunk;
+  const int64_t r_end =
+      chunk_rows ? chunk_rows[2 * blockIdx.z + 1] : min(n, r_begin + rows_per_chunk);
   const int stages = static_cast<int>((r_end - r_begin + kGR - 1) / kGR);
 
   auto xs = [&](int buf) { return smem + static_cast<size_t>(buf) * 2 * kGR * kGLd; };
@@ -158,7 +162,7 @@ gram_dmma_kernel(const double* __restrict__ X, int64_t ldx, const double* __rest
 // inner dimension advances 16 per stage through a 3-stage ring. X rows are
 // staged 20 doubles apart (fragment: 8 rows x 4 doubles -> two wavefronts),
 // C rows 72 apart (4 rows x 8 doubles).
-constexpr int kRRows = 128;
+constexpr int kRRows = kRotateRowTile;
 constexpr int kRCols = 64;
 constexpr int kRK = 16;
 constexpr int kRStages = 3;
@@ -172,7 +176,11 @@ template <int VEC>
 __global__ void __launch_bounds__(kRThreads)
 rotate_dmma_kernel(const double* __restrict__ X, int64_t ldx, const double* __restrict__ C,
                    int64_t ldc, double* __restrict__ Y, int64_t ldy, int64_t n, int k, int m,
-                   double alpha, double beta, int use_beta, int upper_tri) {
+                   double alpha, double beta, int use_beta, int upper_tri,
+                   const int32_t* __restrict__ tile_member, int64_t c_stride) {
+  // Grouped rotation: row tile t of a concatenated block belongs to problem
+  // tile_member[t], whose coefficient matrix starts c_stride doubles further per problem.
+  if (tile_member) C += static_cast<int64_t>(tile_member[blockIdx.y]) * c_stride;
   extern __shared__ double smem[];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -286,13 +294,29 @@ void gram_partial_dmma(const double* X, int64_t ldx, const double* Y, int64_t ld
   auto kern = vec2 ? gram_dmma_kernel<2> : gram_dmma_kernel<1>;
   FE_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
   kern<<<grid, kGThreads, kGSmem, s>>>(X, ldx, Y, ldy, n, k, m, rows_per_chunk, symmetric ? 1 : 0,
-                                       partial);
+                                       partial, nullptr);
+  check_launch("gram_dmma_kernel");
+}
+
+// Grouped Gram partials: chunk z covers rows [chunk_rows[2z], chunk_rows[2z+1]) of
+// the concatenated blocks (each chunk inside one problem's rows).
+void gram_partial_dmma_ranges(const double* X, int64_t ldx, const double* Y, int64_t ldy, int k,
+                              int m, int chunks, const int64_t* chunk_rows, bool symmetric,
+                              double* partial, cudaStream_t s) {
+  const bool vec2 = aligned16(X) && aligned16(Y) && ldx % 2 == 0 && ldy % 2 == 0 && k % 2 == 0 &&
+                    m % 2 == 0;
+  FE_REQUIRE(chunks >= 1 && chunks <= 65535, "grouped Gram: chunk count out of range");
+  dim3 grid((k + kGT - 1) / kGT, (m + kGT - 1) / kGT, chunks);
+  auto kern = vec2 ? gram_dmma_kernel<2> : gram_dmma_kernel<1>;
+  FE_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+  kern<<<grid, kGThreads, kGSmem, s>>>(X, ldx, Y, ldy, 0, k, m, 0, symmetric ? 1 : 0, partial,
+                                       chunk_rows);
   check_launch("gram_dmma_kernel");
 }
 
 void rotate_dmma(const double* X, int64_t ldx, const double* C, int64_t ldc, double* Y,
                  int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
-                 cudaStream_t s, bool upper_tri) {
+                 cudaStream_t s, bool upper_tri, const int32_t* tile_member, int64_t c_stride) {
   const bool vec2 = aligned16(X) && ldx % 2 == 0 && k % 2 == 0;
   const int64_t row_tiles = (n + kRRows - 1) / kRRows;
   const int64_t col_tiles = (m + kRCols - 1) / kRCols;
@@ -306,7 +330,8 @@ void rotate_dmma(const double* X, int64_t ldx, const double* C, int64_t ldc, dou
     const int64_t r_off = base * kRRows;
     kern<<<grid, kRThreads, kRSmem, s>>>(X + r_off * ldx, ldx, C, ldc, Y + r_off * ldy, ldy,
                                          n - r_off, static_cast<int>(k), static_cast<int>(m),
-                                         alpha, beta, beta != 0.0 ? 1 : 0, upper_tri ? 1 : 0);
+                                         alpha, beta, beta != 0.0 ? 1 : 0, upper_tri ? 1 : 0,
+                                         tile_member ? tile_member + base : nullptr, c_stride);
     check_launch("rotate_dmma_kernel");
   }
 }

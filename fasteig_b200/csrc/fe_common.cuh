@@ -136,7 +136,14 @@ void gram_partial_dmma(const double* X, int64_t ldx, const double* Y, int64_t ld
                        bool symmetric, double* partial, cudaStream_t s);
 void rotate_dmma(const double* X, int64_t ldx, const double* C, int64_t ldc, double* Y,
                  int64_t ldy, int64_t n, int64_t k, int64_t m, double alpha, double beta,
-                 cudaStream_t s, bool upper_tri = false);
+                 cudaStream_t s, bool upper_tri = false, const int32_t* tile_member = nullptr,
+                 int64_t c_stride = 0);
+void gram_partial_dmma_ranges(const double* X, int64_t ldx, const double* Y, int64_t ldy, int k,
+                              int m, int chunks, const int64_t* chunk_rows, bool symmetric,
+                              double* partial, cudaStream_t s);
+// Row tile of the FP64 rotation kernel (grouped rotations pad every problem's rows
+// to a multiple of it).
+constexpr int kRotateRowTile = 128;
 
 }  // namespace fe
 

@@ -29,6 +29,7 @@
 #include <type_traits>
 
 #include "device.hpp"
+#include "grouped.hpp"
 
 namespace fe {
 namespace {
@@ -67,6 +68,7 @@ struct Options {
   int64_t tail_guard = 0;          // Chebyshev mixed: columns past nev in the FP64 cycles (0 = all)
   std::string tail_rr = "split";   // Chebyshev mixed FP64 cycles: Y^T A Y as split | fp64
   int64_t inject_wait_timeout = 0;  // test hook: status code of a forced bounded-wait timeout
+  bool group = false;  // request server: Chebyshev request may run in a grouped lane
   // Chebyshev hard locking: Rayleigh-Ritz with the Cholesky QR rotation folded in
   // ("fused", the default of precision=mixed) or Cholesky QR then Rayleigh-Ritz as
   // the reference orders them ("cholqr", the default of precision=fp64).
@@ -141,6 +143,7 @@ struct Options {
     else if (k == "init") init = lower(v);
     else if (k == "mixed_switch") mixed_switch = as_double(v);
     else if (k == "tensor_cores") tensor_cores = as_int(v) != 0;
+    else if (k == "group") group = as_int(v) != 0;
     else if (k == "tail_degree") tail_degree = as_int(v);
     else if (k == "tail_rr") {
       tail_rr = lower(v);
@@ -3139,6 +3142,72 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
     stats[10] = st.rr_ms;
     stats[11] = st.precise_grams;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Grouped Chebyshev members (grouped.cpp runs them): which requests may join a
+// group, and the per-problem setup the reference's ChebyshevSolver does before its
+// loop (src/ChebyshevSolver.cpp:67-129): option checks, the subspace width, and the
+// Lanczos spectral bounds (estimate_bounds_with_executor, :26-49).
+// ---------------------------------------------------------------------------
+
+// Subspace width of a grouped member: the solve's capacity (nev + min(nev, n - nev),
+// or `block`), rounded up to a multiple of 32 (members of one width share a group).
+static int64_t group_width_of(const Options& opt, int64_t n) {
+  int64_t cap = opt.nev + std::min(opt.nev, n - opt.nev);
+  if (opt.block > 0) cap = std::max(opt.nev, std::min(opt.block, n));
+  return (cap + 31) / 32 * 32;
+}
+
+bool chebyshev_group_key(const Csr& A, const Csr* B, const char* options, bool require_flag,
+                         int64_t* width, int64_t* degree) {
+  Options opt;
+  opt.parse(options);
+  if (require_flag && !opt.group) return false;
+  if (opt.solver != "chebyshev" || B != nullptr || A.rows != A.cols) return false;
+  if (opt.precision != "fp64" || opt.locking != "soft") return false;
+  if (opt.which != "sr" && opt.which != "lr") return false;
+  if (opt.nev < 1 || opt.nev > A.rows || opt.degree < 1) return false;
+  const int64_t w = group_width_of(opt, A.rows);
+  if (w > A.rows || w > 512) return false;
+  if (width) *width = w;
+  if (degree) *degree = opt.degree;
+  return true;
+}
+
+void chebyshev_group_setup(const Csr& A, const char* options, GroupSetup& g) {
+  Options opt;
+  opt.parse(options);
+  FE_REQUIRE(chebyshev_group_key(A, nullptr, options, false, nullptr, nullptr),
+             "grouped Chebyshev: request not eligible (standard FP64 Chebyshev with soft "
+             "locking and a width of at most 512 columns)");
+  FE_REQUIRE(opt.bounds == "reference" || opt.bounds == "ritz", "bounds must be reference or ritz");
+  FE_REQUIRE(opt.init == "host" || opt.init == "device", "init must be host or device");
+  g.n = A.rows;
+  g.nev = opt.nev;
+  g.width = group_width_of(opt, A.rows);
+  g.degree = opt.degree;
+  g.maxiter = opt.maxiter;
+  g.tol = opt.tol;
+  g.sign = opt.which == "lr" ? -1.0 : 1.0;
+  g.seed = opt.seed_or_default();
+  g.host_init = opt.init == "host";
+  g.ritz_bounds = opt.bounds == "ritz";
+  g.amplification = opt.amplification;
+  Context ctx;
+  {
+    // the filter operator c A + d I is written into each row's stored diagonal
+    DeviceBuffer bad(sizeof(int32_t));
+    csr_count_bad_diagonals(A, bad.as<int32_t>(), ctx.stream);
+    int32_t nbad = 0;
+    ctx.to_host(&nbad, bad.as<int32_t>(), 1);
+    ctx.sync();
+    FE_REQUIRE(nbad == 0, "grouped Chebyshev: every row needs exactly one stored diagonal "
+                          "entry (" + std::to_string(nbad) + " rows without)");
+  }
+  lanczos_bounds(ctx, A, g.sign, g.seed, g.host_init, g.lower, g.upper);
+  g.reference_cutoff = reference_cutoff(g.lower, g.upper, g.degree, 1.0e3);
+  g.ritz_cutoff_cap = reference_cutoff(g.lower, g.upper, g.degree, g.amplification);
 }
 
 // nev of an option string, validating every key as the solve will.

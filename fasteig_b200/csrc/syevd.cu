@@ -714,6 +714,15 @@ bool use_cluster_sytrd(int kmax, int optin, int dev) {
 
 }  // namespace
 
+namespace {
+void syevd_batched_prepared(int count, int kmax, const SyevdWs& w, double* A, int64_t lda,
+                            double* W, double* Z, int32_t* info, cudaStream_t s);
+__global__ void fill_sizes_kernel(int32_t* msz, int count, int32_t k) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) msz[i] = k;
+}
+}  // namespace
+
 size_t syevd_workspace_bytes(int count, int64_t lda) {
   return SyevdWs(nullptr, count, lda).total;
 }
@@ -730,6 +739,24 @@ void syevd_batched(int count, const int32_t* m_host, double* A, int64_t lda, dou
   SyevdWs w(ws, count, lda);
   FE_REQUIRE(ws && ws_bytes >= w.total, "syevd: workspace too small");
   FE_CHECK_CUDA(cudaMemcpyAsync(w.msz, m_host, sizeof(int32_t) * count, cudaMemcpyHostToDevice, s));
+  syevd_batched_prepared(count, kmax, w, A, lda, W, Z, info, s);
+}
+
+// All `count` matrices of size k: the sizes are written on the device, so the whole
+// sequence is stream-capturable (grouped solves replay it from a CUDA graph).
+void syevd_batched_uniform(int count, int64_t k, double* A, int64_t lda, double* W, double* Z,
+                           int32_t* info, void* ws, size_t ws_bytes, cudaStream_t s) {
+  FE_REQUIRE(count >= 1 && k >= 1 && k <= lda && k <= 8192, "syevd: invalid batch shape");
+  SyevdWs w(ws, count, lda);
+  FE_REQUIRE(ws && ws_bytes >= w.total, "syevd: workspace too small");
+  fill_sizes_kernel<<<(count + 127) / 128, 128, 0, s>>>(w.msz, count, static_cast<int32_t>(k));
+  check_launch("fill_sizes_kernel");
+  syevd_batched_prepared(count, static_cast<int>(k), w, A, lda, W, Z, info, s);
+}
+
+namespace {
+void syevd_batched_prepared(int count, int kmax, const SyevdWs& w, double* A, int64_t lda,
+                            double* W, double* Z, int32_t* info, cudaStream_t s) {
   FE_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int32_t) * count, s));
   const int optin = smem_optin();
   const int dev = current_device();
@@ -767,6 +794,7 @@ void syevd_batched(int count, const int32_t* m_host, double* A, int64_t lda, dou
     check_launch("ormtr_kernel");
   }
 }
+}  // namespace
 
 size_t syevd_single_workspace_bytes(int64_t k) {
   // reflector copy of A and the eigenvectors (k x k each), vectors, scratch

@@ -18,7 +18,7 @@ from ._lib import check, lib
 
 _INT_KEYS = ("n", "nev", "maxiter", "maxdim", "maxblks", "degree", "blksize", "verbosity",
              "print_every", "block", "tensor_cores", "tail_degree", "tail_guard",
-             "inject_wait_timeout")
+             "inject_wait_timeout", "group")
 _FLOAT_KEYS = ("tol", "shift", "amplification", "mixed_switch")
 _STR_KEYS = ("which", "solver", "precision", "bounds", "init", "logfile", "output_format",
              "precond", "locking", "rr", "tail_filter", "tail_rr")
@@ -306,6 +306,55 @@ def batch_krylov_schur(problems, nevs, opts: Optional[fasteig_options] = None,
         d["status"] = int(st)
     return out, dict(seconds=float(stats[0]), rounds=int(stats[1]), steps=int(stats[2]),
                      graph_launches=int(stats[3]))
+
+
+GROUP_STATS = 10
+
+
+def grouped_chebyshev(problems, opts, want_vectors: bool = False):
+    """Solve standard problems together with the grouped Chebyshev engine
+    (``fe_grouped_chebyshev``): problems of one subspace width and filter degree
+    advance as one group, a cycle of grouped kernels (one CUDA graph once the
+    membership is stable) per step, and leave as they converge. ``problems`` are
+    device ``CsrMatrix`` objects, ``opts`` one ``fasteig_options`` or one per
+    problem. Returns a list of dicts (eigenvalues, residual_norms, eigenvectors or
+    None, iterations, status, seconds, width, lower, upper) and the batch stats
+    (cycles, graph_replays, repacks)."""
+    problems = list(problems)
+    if not problems:
+        raise ValueError("empty batch")
+    if isinstance(opts, fasteig_options):
+        opts = [opts] * len(problems)
+    opts = list(opts)
+    if len(opts) != len(problems):
+        raise ValueError("one option set per problem is required")
+    count = len(problems)
+    texts = []
+    for o in opts:
+        o.validate()
+        texts.append(o.to_text().encode())
+    handles = (C.c_void_p * count)(*[p.handle for p in problems])
+    c_texts = (C.c_char_p * count)(*texts)
+    vals = [np.zeros(o.nev()) for o in opts]
+    res = [np.zeros(o.nev()) for o in opts]
+    vecs = [np.zeros(o.nev() * p.rows) if want_vectors else None for p, o in zip(problems, opts)]
+    pv = (C.c_void_p * count)(*[v.ctypes.data for v in vals])
+    pr = (C.c_void_p * count)(*[r.ctypes.data for r in res])
+    pe = (C.c_void_p * count)(*[v.ctypes.data if v is not None else None for v in vecs])
+    stats = np.zeros(count * GROUP_STATS)
+    check(lib.fe_grouped_chebyshev(count, C.cast(handles, C.c_void_p), C.cast(c_texts, C.c_void_p),
+                                   C.cast(pv, C.c_void_p), C.cast(pr, C.c_void_p),
+                                   C.cast(pe, C.c_void_p) if want_vectors else None,
+                                   stats.ctypes.data))
+    out = []
+    for i, (p, o) in enumerate(zip(problems, opts)):
+        st = stats[i * GROUP_STATS:(i + 1) * GROUP_STATS]
+        ev = vecs[i].reshape(o.nev(), p.rows).T if want_vectors else None
+        out.append(dict(eigenvalues=vals[i], residual_norms=res[i], eigenvectors=ev,
+                        iterations=int(st[0]), status=int(st[1]), seconds=float(st[2]),
+                        width=int(st[3]), lower=float(st[4]), upper=float(st[5])))
+    st = stats[:GROUP_STATS]
+    return out, dict(cycles=int(st[6]), graph_replays=int(st[7]), repacks=int(st[8]))
 
 
 class Server:

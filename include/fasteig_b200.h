@@ -370,6 +370,30 @@ int fe_batch_krylov_schur(int32_t count, const fe_csr_t* A, const int64_t* nev,
                           double* eigenvectors, int32_t* iterations, int32_t* status,
                           double* stats);
 
+/* ---------------------------------------------------------------------
+ * Grouped Chebyshev (extension; the reference runs one ChebyshevSolver::solve
+ * per problem, src/ChebyshevSolver.cpp:67-221): `count` standard problems A[p]
+ * (one device) with their own option strings, solved together. Problems of one
+ * subspace width (the solve's capacity rounded up to a multiple of 32) and
+ * filter degree form a group; each cycle of a group runs every member's filter,
+ * Cholesky QR and Rayleigh-Ritz in grouped kernels over the concatenated
+ * block-diagonal operator (one CUDA graph per cycle once membership is
+ * stable), and members leave as they converge. Eligible problems: solver
+ * Chebyshev, precision fp64, locking soft, which SR or LR, width <= 512, one
+ * stored diagonal entry per row. Each problem's arithmetic reads only its own
+ * rows, so its result does not depend on the rest of the batch.
+ * Results per problem: eigenvalues[p][nev_p], residual_norms[p][nev_p] (the
+ * reference's relative residual), eigenvectors[p] (n_p-by-nev_p column-major;
+ * the array or any entry may be NULL), stats[count * FE_GROUP_STATS] (may be
+ * NULL): cycles, status (0 converged, 1 at maxiter), seconds in the group,
+ * width, spectral lower and upper bounds, then the batch's total group cycles,
+ * graph replays and repacks, and the problem's status code.
+ * ------------------------------------------------------------------- */
+#define FE_GROUP_STATS 10
+int fe_grouped_chebyshev(int32_t count, const fe_csr_t* A, const char* const* options,
+                         double* const* eigenvalues, double* const* residual_norms,
+                         double* const* eigenvectors, double* stats);
+
 /* Block-diagonal operator of `count` CSR handles on one device (part p's rows and
  * columns follow those of parts 0..p-1); an SpMM on it is the grouped SpMM of
  * all parts in one launch (the reference applies one operator per process).
@@ -419,6 +443,12 @@ int fe_syevd_batched_f64(int32_t count, const int32_t* m, const double* A, int64
  *     submission, admitted memory bytes, start and end in seconds since the
  *     server was created) and forgets the request.
  *   fe_server_destroy: finishes running requests, drops queued ones.
+ * A request whose options carry group=1 and that fe_grouped_chebyshev accepts
+ * runs in a grouped lane instead (one per width and degree, beside the
+ * slots): it joins the lane's group at the next cycle boundary once its memory
+ * fits, advances with the other admitted members in grouped kernels, and leaves
+ * when it converges (continuous batching); its stats are the fe_solve layout
+ * with iterations, status, seconds and bounds filled.
  * ------------------------------------------------------------------- */
 typedef struct fe_server* fe_server_t;
 int fe_server_create(int32_t device, int32_t slots, int64_t memory_budget_bytes,
