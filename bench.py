@@ -79,6 +79,10 @@ def args_parse():
     p.add_argument("--requests", type=int, default=200,
                    help="serving: number of requests (the configuration names 10,000)")
     p.add_argument("--slots", type=int, default=6, help="serving: concurrent solves")
+    p.add_argument("--serving-chebyshev", default="grouped", choices=["grouped", "slots"],
+                   help="serving: Chebyshev requests in grouped lanes (FP64, continuous "
+                        "batching in grouped kernels) or in worker slots (mixed precision, "
+                        "one solve per request)")
     p.add_argument("--solve-only", default=None, choices=["mixed", "fp64"],
                    help="run exactly one solve of the workload at this precision and print its "
                         "stats (launch-list profiling driver; no bench line)")
@@ -299,7 +303,11 @@ def run_serving(a):
         solver = "Chebyshev" if rng.random() < 0.5 else "LOBPCG"
         o = fe.fasteig_options(H.n)
         kv = dict(solver=solver, nev=nev, which="SR", tol=tol, seed=1 + k, init="device")
-        if solver == "Chebyshev":
+        if solver == "Chebyshev" and a.serving_chebyshev == "grouped":
+            # FP64 Chebyshev in the grouped lane of its width: joins the lane's group
+            # between cycles and advances with the other admitted requests
+            kv.update(degree=16, bounds="ritz", amplification=1e6, maxiter=300, group=1)
+        elif solver == "Chebyshev":
             # mixed precision with hard locking; for tol 1e-8 the FP32 pairs lock at
             # 1e-6 before the FP64 cycles (the default 4e-6 floor where tol is 1e-6)
             kv.update(degree=16, bounds="ritz", amplification=1e6, maxiter=300,
@@ -336,6 +344,7 @@ def run_serving(a):
     for k in range(len(reqs)):
         results[k] = srv.wait(ids[k])
     makespan = time.perf_counter() - t_start
+    lane_stats = srv.stats()
     srv.close()
     lat = np.array([r["latency_s"] for r in results])
     conv = sum(int((r["residual_norms"] <= q[3]).sum()) for r, q in zip(results, reqs))
@@ -348,7 +357,9 @@ def run_serving(a):
                        "capacity_per_s": round(cap_rps, 3), "load": 0.8,
                        "n_range": [1e4, 1e6], "nev_range": [4, 128], "tol": [1e-6, 1e-8],
                        "solvers": ["Chebyshev", "LOBPCG"],
+                       "chebyshev_requests": a.serving_chebyshev,
                        "operators": "16 seeded matrices resident in HBM"},
+            "grouped_lanes": lane_stats,
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max())},
             "converged_pairs": conv, "requested_pairs": int(asked),

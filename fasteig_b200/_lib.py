@@ -80,6 +80,7 @@ _SIGS = {
     "fe_server_submit": (C.c_int, [vp, vp, vp, C.c_char_p, vp]),
     "fe_server_wait": (C.c_int, [vp, i64, C.c_double, vp, vp, vp]),
     "fe_server_destroy": (C.c_int, [vp]),
+    "fe_server_stats": (C.c_int, [vp, vp, C.c_int32]),
     "fe_gram_f64_noalloc": (C.c_int, [vp, i64, vp, i64, i64, i64, i64, vp, i64, vp]),
     "fe_gram_f64_noalloc_max_entries": (C.c_int64, []),
 }

@@ -10,12 +10,22 @@
 // while other solves run beside it goes back to the head of the queue once and runs
 // when nothing else does.
 //
+// Grouped lanes (continuous batching on the device): a request that asks for it
+// (group=1) and that the grouped Chebyshev engine accepts goes to the lane of its
+// width and degree instead of a worker slot. A lane is one host thread driving one
+// group: between two cycles it admits the lane's queued requests whose memory fits
+// the same budget, and every cycle advances all admitted members together in
+// grouped kernels (one CUDA graph while the membership is stable); members leave
+// as they converge and their memory returns to the budget.
+//
 // The reference serves nothing: fasteig_problem::solve (src/fasteig_problem.cpp:
-// 340-437) is one blocking solve per call. Each request here runs exactly that
-// solve (the same code path as fe_solve), so its result does not depend on what
-// else is in flight.
+// 340-437) is one blocking solve per call. Each worker request here runs exactly
+// that solve (the same code path as fe_solve), so its result does not depend on
+// what else is in flight; a grouped member's arithmetic reads only its own rows of
+// the group's blocks, so its result does not depend on the other members either.
 
 #include "device.hpp"
+#include "grouped.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -50,6 +60,13 @@ struct fe_server {
     int rc = FE_OK;
     std::string error;
     clock::time_point t_submit, t_start, t_end;
+    fe::GroupMember member;  // grouped lane requests
+  };
+  // One grouped lane per (width, degree): its queue and its driving thread.
+  struct Lane {
+    int64_t width = 0, degree = 0;
+    std::deque<Request*> pending;
+    std::thread thread;
   };
 
   int device = 0;
@@ -63,6 +80,12 @@ struct fe_server {
   std::deque<Request*> queue;
   std::map<int64_t, std::unique_ptr<Request>> requests;
   std::vector<std::thread> workers;
+  std::vector<std::unique_ptr<Lane>> lanes;
+  std::condition_variable cv_lane;
+  bool stopping_lanes = false;
+  // counters of the grouped lanes (fe_server_stats)
+  int64_t grouped_served = 0, group_cycles = 0, group_replays = 0, group_repacks = 0;
+  int64_t max_group_members = 0;
 
   // Head-of-line admission: the oldest request starts when it fits the budget,
   // or when nothing is running (a request larger than the budget still runs,
@@ -131,6 +154,116 @@ struct fe_server {
       }
       cv_done.notify_all();
       cv_work.notify_all();
+      cv_lane.notify_all();
+    }
+  }
+
+  void finish_request(Request* r, int rc, const std::string& error) {
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      r->rc = rc;
+      if (rc != FE_OK) r->error = error;
+      r->t_end = clock::now();
+      r->state = 2;
+      in_use -= r->bytes;
+      --running;
+    }
+    cv_done.notify_all();
+    cv_work.notify_all();
+    cv_lane.notify_all();
+  }
+
+  void lane_loop(Lane* L) {
+    cudaSetDevice(device);
+    std::unique_ptr<fe::ChebGroup> group;
+    size_t active = 0;
+    std::vector<fe::GroupMember*> done;
+    int64_t last_replays = 0, last_repacks = 0;  // this lane's group counters already added
+    while (true) {
+      std::vector<Request*> admit;
+      {
+        std::unique_lock<std::mutex> lock(mu);
+        auto admissible = [&] {
+          return !L->pending.empty() &&
+                 (running == 0 || in_use + L->pending.front()->bytes <= budget);
+        };
+        if (active == 0)
+          cv_lane.wait(lock, [&] { return (stopping_lanes && L->pending.empty()) || admissible(); });
+        if (active == 0 && L->pending.empty() && stopping_lanes) return;
+        while (admissible()) {
+          Request* r = L->pending.front();
+          L->pending.pop_front();
+          in_use += r->bytes;
+          ++running;
+          r->state = 1;
+          r->t_start = clock::now();
+          admit.push_back(r);
+        }
+      }
+      for (Request* r : admit) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b < r->bytes + (r->bytes >> 3))
+          fe::release_cached_memory(device);
+        else
+          cudaGetLastError();
+        // per-member setup (option checks, Lanczos bounds) on its own stream
+        const int rc = fe::guarded("fe_server grouped request", [&] {
+          r->member.A = r->A;
+          r->member.tag = r;
+          fe::chebyshev_group_setup(*r->A, r->options.c_str(), r->member.g);
+          if (!group) group.reset(new fe::ChebGroup(device, L->width, L->degree));
+          group->join(&r->member);
+        });
+        if (rc != FE_OK) {
+          finish_request(r, rc, fe_last_error());
+          continue;
+        }
+        ++active;
+      }
+      if (!group || group->empty()) continue;
+      done.clear();
+      const int rc = fe::guarded("fe_server grouped cycle", [&] {
+        {
+          std::lock_guard<std::mutex> lock(mu);
+          max_group_members = std::max<int64_t>(max_group_members, group->size());
+        }
+        group->launch_cycle();
+        group->finish_cycle(done);
+      });
+      if (rc != FE_OK) {
+        const std::string err = fe_last_error();
+        group->fail_all(rc, err, done);
+      }
+      {
+        std::lock_guard<std::mutex> lock(mu);
+        group_cycles += rc == FE_OK ? 1 : 0;
+        group_replays += group->graph_replays - last_replays;
+        group_repacks += group->repacks - last_repacks;
+        last_replays = group->graph_replays;
+        last_repacks = group->repacks;
+      }
+      for (fe::GroupMember* m : done) {
+        Request* r = static_cast<Request*>(m->tag);
+        std::copy(m->eigenvalues.begin(), m->eigenvalues.end(), r->eigenvalues.begin());
+        std::copy(m->residuals.begin(), m->residuals.end(), r->residuals.begin());
+        r->stats[0] = static_cast<double>(m->iterations);
+        r->stats[1] = m->converged ? 0.0 : 1.0;
+        r->stats[2] = m->seconds;
+        r->stats[3] = static_cast<double>(m->iterations * (L->degree + 1));
+        r->stats[5] = static_cast<double>(m->iterations);
+        r->stats[6] = m->g.lower;
+        r->stats[7] = m->g.upper;
+        {
+          std::lock_guard<std::mutex> lock(mu);
+          ++grouped_served;
+        }
+        --active;
+        finish_request(r, m->rc, m->error);
+      }
+      if (rc != FE_OK) {
+        group.reset();  // a fresh group (and stream) for the next members
+        last_replays = last_repacks = 0;
+      }
     }
   }
 };
@@ -169,6 +302,10 @@ extern "C" int fe_server_submit(fe_server_t srv, fe_csr_t A, fe_csr_t B, const c
     // in a worker).
     r->nev = fe::options_nev(r->options.c_str());
     FE_REQUIRE(r->nev >= 1 && r->nev <= A->m.rows, "nev must be in [1, n]");
+    int64_t width = 0, degree = 0;
+    const bool grouped =
+        fe::chebyshev_group_key(A->m, r->B, r->options.c_str(), true, &width, &degree);
+    if (grouped) r->bytes = fe::group_member_bytes(A->m, width);
     r->eigenvalues.assign(r->nev, 0.0);
     r->residuals.assign(r->nev, 0.0);
     r->stats.assign(12, 0.0);
@@ -178,10 +315,39 @@ extern "C" int fe_server_submit(fe_server_t srv, fe_csr_t A, fe_csr_t B, const c
       FE_REQUIRE(!srv->stopping, "server is shutting down");
       r->id = srv->next_id++;
       *request_id = r->id;
-      srv->queue.push_back(r.get());
+      if (grouped) {
+        fe_server::Lane* lane = nullptr;
+        for (auto& l : srv->lanes)
+          if (l->width == width && l->degree == degree) lane = l.get();
+        if (!lane) {
+          srv->lanes.emplace_back(new fe_server::Lane);
+          lane = srv->lanes.back().get();
+          lane->width = width;
+          lane->degree = degree;
+          lane->thread = std::thread([s = srv, lane] { s->lane_loop(lane); });
+        }
+        lane->pending.push_back(r.get());
+      } else {
+        srv->queue.push_back(r.get());
+      }
       srv->requests.emplace(r->id, std::move(r));
     }
     srv->cv_work.notify_one();
+    srv->cv_lane.notify_all();
+  });
+}
+
+extern "C" int fe_server_stats(fe_server_t srv, double* out, int32_t count) {
+  return fe::guarded("fe_server_stats", [&] {
+    FE_REQUIRE(srv && out && count >= 0, "null argument");
+    std::lock_guard<std::mutex> lock(srv->mu);
+    const double v[] = {static_cast<double>(srv->grouped_served),
+                        static_cast<double>(srv->group_cycles),
+                        static_cast<double>(srv->group_replays),
+                        static_cast<double>(srv->group_repacks),
+                        static_cast<double>(srv->lanes.size()),
+                        static_cast<double>(srv->max_group_members)};
+    for (int32_t i = 0; i < count; ++i) out[i] = i < 6 ? v[i] : 0.0;
   });
 }
 
@@ -235,19 +401,27 @@ extern "C" int fe_server_destroy(fe_server_t srv) {
     {
       // Let admitted requests finish; queued ones are dropped (and reported so).
       std::unique_lock<std::mutex> lock(srv->mu);
-      for (auto* r : srv->queue) {
+      auto drop = [](fe_server::Request* r) {
         r->state = 2;
         r->rc = FE_ERR_INVALID;
         r->error = "fe_server: server destroyed before the request ran";
         r->t_start = r->t_end = fe_server::clock::now();
-      }
+      };
+      for (auto* r : srv->queue) drop(r);
       srv->queue.clear();
+      for (auto& l : srv->lanes) {
+        for (auto* r : l->pending) drop(r);
+        l->pending.clear();
+      }
       srv->cv_done.notify_all();
       srv->cv_done.wait(lock, [&] { return srv->running == 0; });
       srv->stopping = true;
+      srv->stopping_lanes = true;
     }
     srv->cv_work.notify_all();
+    srv->cv_lane.notify_all();
     for (auto& t : srv->workers) t.join();
+    for (auto& l : srv->lanes) l->thread.join();
     delete srv;
   });
 }

@@ -402,6 +402,14 @@ class Server:
                     latency_s=float(stats[14]), admitted_bytes=int(stats[15]),
                     start_s=float(stats[16]), end_s=float(stats[17]))
 
+    def stats(self) -> dict:
+        """Counters of the grouped lanes (requests submitted with group=1)."""
+        out = np.zeros(6)
+        check(lib.fe_server_stats(self.handle, out.ctypes.data, 6))
+        keys = ("grouped_served", "group_cycles", "graph_replays", "repacks", "lanes",
+                "max_group_members")
+        return {k: int(v) for k, v in zip(keys, out)}
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             check(lib.fe_server_destroy(self.handle))

@@ -458,6 +458,9 @@ int fe_server_submit(fe_server_t server, fe_csr_t A, fe_csr_t B, const char* opt
 int fe_server_wait(fe_server_t server, int64_t request_id, double timeout_seconds,
                    double* eigenvalues, double* residual_norms, double* stats);
 int fe_server_destroy(fe_server_t server);
+/* Counters of the grouped lanes, out[count] (up to 6): requests served grouped,
+ * group cycles, graph replays, repacks, lanes, largest group seen. */
+int fe_server_stats(fe_server_t server, double* out, int32_t count);
 
 #ifdef __cplusplus
 }

@@ -97,3 +97,47 @@ def test_server_pending_and_bad_options():
         bad2.set("nev", H.n + 1)
         with pytest.raises(FastEigError, match="nev"):
             srv.submit(A, bad2, solver="Chebyshev")
+
+
+def test_server_grouped_lanes():
+    """Requests with group=1 run in grouped lanes (one per width and degree): they
+    join a group between cycles, advance together, and each result is the one the
+    same problem gets alone in a group (bit-identical for same-stencil groups,
+    1e-11 otherwise), meeting tol. Worker-slot requests run beside them."""
+    from fasteig_b200 import CsrMatrix, Server, grouped_chebyshev
+    from fasteig_b200 import matrices as M
+    specs = [(13, "star1", 10), (12, "star1", 12), (14, "star1", 8), (11, "star1", 14),
+             (12, "star2", 20), (13, "star2", 24)]
+    Hs = [M.laplacian_wells(s, wells=6, seed=50 + i, stencil=st) for i, (s, st, _) in enumerate(specs)]
+    mats = [CsrMatrix(H.n, H.rowptr, H.colind, H.values) for H in Hs]
+
+    def gopts(H, nev):
+        o = options("Chebyshev", nev, 1e-8, H.n)
+        assert o.set("group", 1)
+        return o
+
+    alone = [grouped_chebyshev([A], [gopts(H, nev)])[0][0]
+             for H, A, (_, _, nev) in zip(Hs, mats, specs)]
+    lob = requests()[1]
+    lob_A = CsrMatrix(lob[0].n, lob[0].rowptr, lob[0].colind, lob[0].values)
+    with Server(slots=2) as srv:
+        ids = [srv.submit(A, gopts(H, nev)) for H, A, (_, _, nev) in zip(Hs, mats, specs)]
+        lid = srv.submit(lob_A, options("LOBPCG", lob[2], lob[3], lob[0].n))
+        results = [srv.wait(i) for i in ids]
+        lres = srv.wait(lid)
+        st = srv.stats()
+    assert np.all(lres["residual_norms"] <= lob[3])
+    assert st["grouped_served"] == len(specs)
+    assert st["lanes"] == 2  # widths 32 and 64 at degree 10
+    assert st["max_group_members"] >= 2
+    assert st["graph_replays"] > 0
+    for k, (r, a) in enumerate(zip(results, alone)):
+        assert np.all(r["residual_norms"] <= 1e-8), k
+        if specs[k][1] == "star1" and specs[k][2] <= 16:  # the all-7-point width-32 lane
+            assert np.array_equal(r["eigenvalues"], a["eigenvalues"]), k
+            assert r["iterations"] == a["iterations"]
+        else:
+            np.testing.assert_allclose(r["eigenvalues"], a["eigenvalues"], rtol=1e-11,
+                                       atol=1e-12)
+    spans = sorted((r["start_s"], r["end_s"]) for r in results)
+    assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
