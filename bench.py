@@ -71,7 +71,7 @@ def args_parse():
                         "driver; prints per-launch CUDA-event times, no bench line)")
     p.add_argument("--launches", type=int, default=4)
     p.add_argument("--workload", default="chebyshev_wells",
-                   choices=["chebyshev_wells", "batch_ks", "generalized", "serving"],
+                   choices=["chebyshev_wells", "batch_ks", "generalized", "serving", "grouped"],
                    help="chebyshev_wells (default bench line): 128^3 well problem; batch_ks: "
                         "512 independent 2D problems on the batched Krylov-Schur engine; "
                         "generalized: 80^3 27-point K u = l M u by LOBPCG and Davidson")
@@ -273,6 +273,64 @@ def run_generalized(a):
                                           "precond": "jacobi"}, **extra),
                           "converged_pairs": conv, "iterations": p.last_iterations(),
                           "spmm_launches": p.stats["spmm_launches"]}), flush=True)
+    return 0
+
+
+def run_grouped(a):
+    """Grouped Chebyshev against one solve per problem: 48 standard problems (3D 7- or
+    13-point Laplacian + Gaussian wells, n log-uniform in [1e4, 2e5], nev uniform in
+    8..48, tol 1e-8, FP64 Chebyshev of degree 16 with Ritz-damped bounds) solved by
+    one fe_grouped_chebyshev call (groups per width advancing together in grouped
+    kernels) and by fe_solve one after the other with the same options. Prints one
+    line per arm."""
+    import numpy as np
+    import torch
+    import fasteig_b200 as fe
+    from fasteig_b200 import matrices as M
+    torch.cuda.set_device(0)
+    rng = np.random.Generator(np.random.PCG64(11))
+    probs = []
+    for i in range(48):
+        n_target = math.exp(rng.uniform(math.log(1e4), math.log(2e5)))
+        side = max(8, int(round(n_target ** (1.0 / 3.0))))
+        stencil = "star1" if i % 2 == 0 else "star2"
+        H = M.laplacian_wells(side, wells=16, seed=300 + i, stencil=stencil)
+        nev = int(rng.integers(8, 49))
+        o = fe.fasteig_options(H.n)
+        for k, v in dict(solver="Chebyshev", nev=nev, which="SR", tol=1e-8, maxiter=400,
+                         seed=1 + i, degree=16, bounds="ritz", amplification=1e6,
+                         init="device").items():
+            assert o.set(k, v), k
+        probs.append((H, fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values), o, nev))
+    mats = [A for _, A, _, _ in probs]
+    opts = [o for _, _, o, _ in probs]
+    asked = sum(nev for *_, nev in probs)
+    # warm-up: one small group and one solve (kernel loading, pools)
+    fe.grouped_chebyshev(mats[:2], opts[:2])
+    fe.fasteig_problem(mats[0], solver="Chebyshev").solve(opts[0], want_vectors=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out, batch = fe.grouped_chebyshev(mats, opts)
+    t_group = time.perf_counter() - t0
+    conv_g = sum(int((r["residual_norms"] <= 1e-8).sum()) for r in out)
+    t0 = time.perf_counter()
+    conv_s = 0
+    for A, o in zip(mats, opts):
+        p = fe.fasteig_problem(A, solver="Chebyshev")
+        p.solve(o, want_vectors=False)
+        conv_s += int((p.residual_norms() <= 1e-8).sum())
+    t_seq = time.perf_counter() - t0
+    cfg = {"workload": "grouped_chebyshev_48", "problems": 48, "n_range": [1e4, 2e5],
+           "nev_range": [8, 48], "tol": 1e-8, "degree": 16, "sum_n": int(sum(H.n for H, *_ in probs)),
+           "requested_pairs": int(asked)}
+    for impl, sec, conv, extra in (("grouped", t_group, conv_g, {"batch": batch,
+                                                                 "widths": sorted({r["width"] for r in out})}),
+                                   ("one_solve_per_problem", t_seq, conv_s, {})):
+        print(json.dumps(dict({"metric": METRIC, "value": round(conv / sec, 3), "unit": UNIT,
+                               "n_gpus": 1, "steps": 1, "warmup": 1,
+                               "ms_per_step": round(sec * 1e3, 1), "higher_is_better": True,
+                               "dtype": "f64", "data": "synthetic", "impl": impl, "config": cfg,
+                               "converged_pairs": conv}, **extra)), flush=True)
     return 0
 
 
@@ -649,6 +707,8 @@ def main():
         return run_batch_ks(a)
     if a.workload == "generalized":
         return run_generalized(a)
+    if a.workload == "grouped":
+        return run_grouped(a)
     if a.workload == "serving":
         return run_serving(a)
     import numpy as np

@@ -94,29 +94,50 @@ __global__ void gram_reduce_members_kernel(const double* __restrict__ partial, i
   G[static_cast<int64_t>(p) * stride + static_cast<int64_t>(j) * k + i] = s;
 }
 
-// One CTA per chunk (rows of one member), a thread per column: sums of
-// (AX - theta X)^2 and X^2 over the chunk's rows, in row order.
-__global__ void resid_partial_kernel(const double* __restrict__ AX, const double* __restrict__ X,
-                                     int64_t ld, int width, const int64_t* __restrict__ chunk_rows,
-                                     const int32_t* __restrict__ chunk_member,
-                                     const double* __restrict__ theta,
-                                     double* __restrict__ partial) {
+// One CTA per chunk (rows of one member): thread t takes column t % width (of a
+// 256-column slice) and every (256 / width)-th row, then the row lanes are added in
+// lane order through shared memory. Sums of (AX - theta X)^2 and X^2 per column.
+constexpr int kResidThreads = 256;
+
+__global__ void __launch_bounds__(kResidThreads)
+resid_partial_kernel(const double* __restrict__ AX, const double* __restrict__ X, int64_t ld,
+                     int width, const int64_t* __restrict__ chunk_rows,
+                     const int32_t* __restrict__ chunk_member, const double* __restrict__ theta,
+                     double* __restrict__ partial) {
+  __shared__ double red[2][kResidThreads];
   const int c = blockIdx.x;
   const int p = chunk_member[c];
   const int64_t r0 = chunk_rows[2 * c];
   const int64_t r1 = chunk_rows[2 * c + 1];
-  for (int j = threadIdx.x; j < width; j += blockDim.x) {
-    const double th = theta[static_cast<int64_t>(p) * width + j];
+  const int slice = min(width, kResidThreads);
+  const int lanes = kResidThreads / slice;
+  const int col = threadIdx.x % slice;
+  const int lane = threadIdx.x / slice;
+  for (int j0 = 0; j0 < width; j0 += slice) {
+    const int j = j0 + col;
     double rs = 0.0, xs = 0.0;
+    if (lane < lanes && j < width) {
+      const double th = theta[static_cast<int64_t>(p) * width + j];
 #pragma unroll 4
-    for (int64_t r = r0; r < r1; ++r) {
-      const double x = X[r * ld + j];
-      const double d = AX[r * ld + j] - th * x;
-      rs = fma(d, d, rs);
-      xs = fma(x, x, xs);
+      for (int64_t r = r0 + lane; r < r1; r += lanes) {
+        const double x = X[r * ld + j];
+        const double d = AX[r * ld + j] - th * x;
+        rs = fma(d, d, rs);
+        xs = fma(x, x, xs);
+      }
     }
-    partial[static_cast<int64_t>(c) * 2 * width + j] = rs;
-    partial[static_cast<int64_t>(c) * 2 * width + width + j] = xs;
+    red[0][threadIdx.x] = rs;
+    red[1][threadIdx.x] = xs;
+    __syncthreads();
+    if (lane == 0 && j < width) {
+      for (int l = 1; l < lanes; ++l) {
+        rs += red[0][l * slice + col];
+        xs += red[1][l * slice + col];
+      }
+      partial[static_cast<int64_t>(c) * 2 * width + j] = rs;
+      partial[static_cast<int64_t>(c) * 2 * width + width + j] = xs;
+    }
+    __syncthreads();
   }
 }
 
@@ -190,7 +211,7 @@ void group_residuals(const double* AX, const double* X, int64_t ld, int width, i
                      const int32_t* member_chunks, const double* theta, double* partial,
                      double* rel, cudaStream_t s) {
   const int threads = std::min(256, (width + 31) / 32 * 32);
-  resid_partial_kernel<<<static_cast<unsigned>(chunks), threads, 0, s>>>(
+  resid_partial_kernel<<<static_cast<unsigned>(chunks), kResidThreads, 0, s>>>(
       AX, X, ld, width, chunk_rows, chunk_member, theta, partial);
   check_launch("resid_partial_kernel");
   resid_finish_kernel<<<static_cast<unsigned>(members), threads, 0, s>>>(partial, width,
