@@ -57,6 +57,7 @@ _SIGS = {
     "fe_column_norms_f32": (C.c_int, [vp, i64, i64, i64, vp, vp, sz, vp]),
     "fe_potrf_upper_f64": (C.c_int, [vp, i64, i64, vp, vp]),
     "fe_trinv_upper_f64": (C.c_int, [vp, i64, vp, i64, i64, vp]),
+    "fe_chol_inv_upper_batched_f64": (C.c_int, [C.c_int32, vp, i64, i64, vp, i64, vp, vp]),
     "fe_symmetrize_f64": (C.c_int, [vp, i64, i64, vp]),
     "fe_convert_f64_to_f32": (C.c_int, [vp, i64, vp, i64, i64, i64, vp]),
     "fe_convert_f32_to_f64": (C.c_int, [vp, i64, vp, i64, i64, i64, vp]),
@@ -71,6 +72,7 @@ _SIGS = {
     "fe_set_cheb_wave_kernel": (C.c_int, [C.c_int32]),
     "fe_set_f64_gemm_kernel": (C.c_int, [C.c_int32]),
     "fe_set_tc_rotate_kernel": (C.c_int, [C.c_int32]),
+    "fe_set_syevd_kernel": (C.c_int, [C.c_int32]),
     "fe_csr_autotune": (C.c_int, [vp, i64, C.c_int32, vp, vp]),
     "fe_batch_krylov_schur": (C.c_int, [C.c_int32, vp, vp, C.c_char_p, vp, vp, vp, vp, vp, vp]),
     "fe_csr_block_diag": (C.c_int, [C.c_int32, vp, vp]),

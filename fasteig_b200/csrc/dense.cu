@@ -360,6 +360,76 @@ __global__ void trinv_upper_kernel(const double* __restrict__ R, int64_t ldr,
   }
 }
 
+// Cholesky G = R^T R and R^{-1} of one small SPD matrix (k <= kCholSmallMax) per CTA,
+// with the whole matrix in shared memory (column-major, ld k + 1 so a row and a column
+// both fall on distinct banks): right-looking factorization (a warp per trailing
+// column), then the upper-triangular inverse column by column in place,
+// R^{-1}[0:j, j] = -R^{-1}[0:j, 0:j] R[0:j, j] / R_jj (the order of LAPACK's trti2).
+// Only G's upper triangle is read; R^{-1} is written with a zero lower triangle, and
+// info = j + 1 for a non-positive or non-finite pivot j (R^{-1} is then not written).
+constexpr int kCholSmallMax = 128;
+constexpr int kCholSmallThreads = 512;
+
+__global__ void __launch_bounds__(kCholSmallThreads)
+chol_inv_small_kernel(const double* __restrict__ G, int k, int64_t ldg, int64_t stride_g,
+                      double* __restrict__ Rinv, int64_t ldi, int64_t stride_i,
+                      int32_t* __restrict__ info) {
+  extern __shared__ double csm[];
+  __shared__ int failed;
+  const int ld = k + 1;
+  double* A = csm;           // k x ld
+  double* tmp = csm + k * ld;  // k
+  G += static_cast<int64_t>(blockIdx.x) * stride_g;
+  Rinv += static_cast<int64_t>(blockIdx.x) * stride_i;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  constexpr int kWarps = kCholSmallThreads / 32;
+  for (int c = warp; c < k; c += kWarps)
+    for (int r = lane; r <= c; r += 32) A[r + c * ld] = G[r + static_cast<int64_t>(c) * ldg];
+  if (tid == 0) failed = 0;
+  __syncthreads();
+  for (int j = 0; j < k; ++j) {
+    if (tid == 0) {
+      const double d = A[j + j * ld];
+      if (!(d > 0.0) || !isfinite(d)) failed = j + 1;
+      else A[j + j * ld] = sqrt(d);
+    }
+    __syncthreads();
+    if (failed) break;
+    const double inv = 1.0 / A[j + j * ld];
+    for (int c = j + 1 + tid; c < k; c += kCholSmallThreads) A[j + c * ld] *= inv;
+    __syncthreads();
+    // trailing update of the upper triangle: A[a][c] -= R[j][a] R[j][c], j < a <= c
+    for (int c = j + 1 + warp; c < k; c += kWarps) {
+      const double rjc = A[j + c * ld];
+      for (int a = j + 1 + lane; a <= c; a += 32) A[a + c * ld] -= A[j + a * ld] * rjc;
+    }
+    __syncthreads();
+  }
+  if (failed) {
+    if (tid == 0 && info) info[blockIdx.x] = failed;
+    return;
+  }
+  for (int j = 0; j < k; ++j) {
+    for (int i = tid; i < j; i += kCholSmallThreads) tmp[i] = A[i + j * ld];
+    __syncthreads();
+    const double djj = 1.0 / A[j + j * ld];
+    for (int i = tid; i < j; i += kCholSmallThreads) {
+      double acc = 0.0;
+      for (int l = i; l < j; ++l) acc = fma(A[i + l * ld], tmp[l], acc);
+      A[i + j * ld] = -djj * acc;
+    }
+    __syncthreads();
+    if (tid == 0) A[j + j * ld] = djj;
+  }
+  __syncthreads();
+  for (int c = warp; c < k; c += kWarps)
+    for (int r = lane; r < k; r += 32)
+      Rinv[r + static_cast<int64_t>(c) * ldi] = r <= c ? A[r + c * ld] : 0.0;
+  if (tid == 0 && info) info[blockIdx.x] = 0;
+}
+
 __global__ void symmetrize_kernel(double* P, int k, int64_t ldp, int64_t batch_stride) {
   P += static_cast<int64_t>(blockIdx.y) * batch_stride;
   const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -432,6 +502,26 @@ void trinv_upper_batched(const double* R, int64_t ldr, double* Rinv, int64_t ldi
   dim3 grid(static_cast<unsigned>((threads + 255) / 256), static_cast<unsigned>(count));
   trinv_upper_kernel<<<grid, 256, 0, s>>>(R, ldr, Rinv, ldi, static_cast<int>(k), stride);
   check_launch("trinv_upper_kernel");
+}
+
+size_t chol_inv_small_smem(int64_t k) {
+  return (static_cast<size_t>(k) * (k + 1) + k) * sizeof(double);
+}
+
+bool chol_inv_small_fits(int64_t k) { return k >= 1 && k <= kCholSmallMax; }
+
+void chol_inv_upper_batched(const double* G, int64_t k, int64_t ldg, int64_t stride_g,
+                            double* Rinv, int64_t ldi, int64_t stride_i, int64_t count,
+                            int32_t* info, cudaStream_t s) {
+  FE_REQUIRE(chol_inv_small_fits(k) && ldg >= k && ldi >= k && count >= 1 && count <= 65535,
+             "chol_inv_upper_batched: invalid shape (k must be in [1, 128])");
+  const size_t smem = chol_inv_small_smem(k);
+  FE_CHECK_CUDA(cudaFuncSetAttribute(chol_inv_small_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(chol_inv_small_smem(kCholSmallMax))));
+  chol_inv_small_kernel<<<static_cast<unsigned>(count), kCholSmallThreads, smem, s>>>(
+      G, static_cast<int>(k), ldg, stride_g, Rinv, ldi, stride_i, info);
+  check_launch("chol_inv_small_kernel");
 }
 
 void symmetrize_batched(double* P, int64_t k, int64_t ldp, int64_t stride, int64_t count,
@@ -731,6 +821,17 @@ extern "C" int fe_trinv_upper_f64(const double* R, int64_t ldr, double* Rinv, in
                                   int64_t k, void* stream) {
   return guarded("fe_trinv_upper_f64",
                  [&] { fe::trinv_upper(R, ldr, Rinv, ldi, k, fe::as_stream(stream)); });
+}
+
+extern "C" int fe_chol_inv_upper_batched_f64(int32_t count, const double* G, int64_t ldg,
+                                             int64_t k, double* Rinv, int64_t ldi,
+                                             int32_t* info, void* stream) {
+  return guarded("fe_chol_inv_upper_batched_f64", [&] {
+    FE_REQUIRE(count >= 0 && (count == 0 || (G && Rinv && info)), "null argument");
+    if (count == 0) return;
+    fe::chol_inv_upper_batched(G, k, ldg, ldg * k, Rinv, ldi, ldi * k, count, info,
+                               fe::as_stream(stream));
+  });
 }
 
 extern "C" int fe_symmetrize_f64(double* P, int64_t k, int64_t ldp, void* stream) {

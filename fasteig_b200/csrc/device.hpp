@@ -73,6 +73,12 @@ void trinv_upper_batched(const double* R, int64_t ldr, double* Rinv, int64_t ldi
                          int64_t stride, int64_t count, cudaStream_t s);
 void symmetrize_batched(double* P, int64_t k, int64_t ldp, int64_t stride, int64_t count,
                         cudaStream_t s);
+// Cholesky and upper-triangular inverse in one launch for k <= 128 (one CTA per
+// matrix, shared memory): Rinv = chol(G)^{-1}; info[p] = first failed pivot + 1 or 0.
+bool chol_inv_small_fits(int64_t k);
+void chol_inv_upper_batched(const double* G, int64_t k, int64_t ldg, int64_t stride_g,
+                            double* Rinv, int64_t ldi, int64_t stride_i, int64_t count,
+                            int32_t* info, cudaStream_t s);
 // Y32 = float(Y), E32 = float(AY - Y diag(theta)) (n x k row-major blocks), and
 // H = G diag(theta) + H1 (k x k column-major, leading dimension ld).
 void shift_split(int64_t n, int64_t k, const double* AY, int64_t lday, const double* Y,

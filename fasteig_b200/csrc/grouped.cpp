@@ -387,8 +387,13 @@ void ChebGroup::launch_cycle() {
                                I.gpart.as<double>(), s);
       group_gram_reduce(I.gpart.as<double>(), static_cast<int>(b), static_cast<int>(b), G,
                         I.member_chunks.as<int32_t>(), true, I.Gm.as<double>(), bb, s);
-      potrf_upper_batched(I.Gm.as<double>(), b, b, bb, G, inf, s);
-      trinv_upper_batched(I.Gm.as<double>(), b, I.Rinv.as<double>(), b, b, bb, G, s);
+      if (chol_inv_small_fits(b)) {
+        chol_inv_upper_batched(I.Gm.as<double>(), b, b, bb, I.Rinv.as<double>(), b, bb, G, inf,
+                               s);
+      } else {
+        potrf_upper_batched(I.Gm.as<double>(), b, b, bb, G, inf, s);
+        trinv_upper_batched(I.Gm.as<double>(), b, I.Rinv.as<double>(), b, b, bb, G, s);
+      }
       rotate_dmma(B[src], b, I.Rinv.as<double>(), b, B[dst], b, R, b, b, 1.0, 0.0, s, true,
                   I.tile_member.as<int32_t>(), bb);
     };

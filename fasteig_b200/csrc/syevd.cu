@@ -687,9 +687,16 @@ void set_max_smem_once(const void* kernel, int bytes, int dev, int slot) {
   if (tracked) done[slot][dev] = true;
 }
 
+// Tridiagonalization kernel: 0 = by size (below), 1 = one CTA per matrix, 2 = the
+// 8-CTA cluster wherever it fits.
+int g_sytrd_mode = 0;
+constexpr int kClusterMinDim = 0;
+
 // The cluster tridiagonalization runs when its shared memory fits and the device can
 // co-schedule one cluster of kClu such CTAs (asked once per device and size).
 bool use_cluster_sytrd(int kmax, int optin, int dev) {
+  if (g_sytrd_mode == 1) return false;
+  if (g_sytrd_mode == 0 && kmax < kClusterMinDim) return false;
   const size_t smem = sytrd_cluster_smem(kmax);
   if (smem + 1024 > static_cast<size_t>(optin)) return false;
   set_max_smem_once(reinterpret_cast<const void*>(sytrd_cluster_kernel), optin - 256, dev, 1);
@@ -822,6 +829,13 @@ void syevd_single(double* A, int64_t lda, int64_t k, double* W, int32_t* info, v
 }
 
 }  // namespace fe
+
+extern "C" int fe_set_syevd_kernel(int32_t mode) {
+  return fe::guarded("fe_set_syevd_kernel", [&] {
+    FE_REQUIRE(mode >= 0 && mode <= 2, "syevd kernel mode must be 0, 1 or 2");
+    fe::g_sytrd_mode = mode;
+  });
+}
 
 extern "C" size_t fe_syevd_f64_workspace_bytes(int64_t k) {
   return k <= 0 ? 0 : fe::syevd_single_workspace_bytes(k);

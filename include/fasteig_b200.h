@@ -245,6 +245,10 @@ int fe_set_f64_gemm_kernel(int32_t mode);
  * Same MMAs in the same order (bit-identical results); unaligned outputs always use
  * the one-CTA-per-tile kernel with its staged epilogue. */
 int fe_set_tc_rotate_kernel(int32_t mode);
+/* Tridiagonalization kernel of the symmetric eigensolver (process-wide): 0 (default)
+ * by matrix size, 1 one CTA per matrix, 2 the 8-CTA cluster wherever it fits. The
+ * eigenvalues and vectors agree to rounding between the kernels. */
+int fe_set_syevd_kernel(int32_t mode);
 
 /* ---------------------------------------------------------------------
  * One Lanczos step on the device (replaces KrylovSubspace::build_one,
@@ -306,6 +310,14 @@ int fe_potrf_upper_f64(double* G, int64_t k, int64_t ldg, int32_t* info, void* s
 /* Rinv = R^{-1} for an upper-triangular k-by-k R (both column-major). */
 int fe_trinv_upper_f64(const double* R, int64_t ldr, double* Rinv, int64_t ldi, int64_t k,
                        void* stream);
+/* Cholesky and inverse in one launch for a batch of small SPD matrices (k <= 128,
+ * matrix p column-major at G + p*ldg*k, upper triangle read): Rinv + p*ldi*k gets
+ * chol(G_p)^{-1} (upper triangular, zero below), info[p] (device) 0 or the failed
+ * pivot + 1. One CTA per matrix with the matrix in shared memory (the reference
+ * factors and solves one projected matrix at a time, src/core/Orthogonalization.cpp:
+ * 211-235). Asynchronous on `stream`. */
+int fe_chol_inv_upper_batched_f64(int32_t count, const double* G, int64_t ldg, int64_t k,
+                                  double* Rinv, int64_t ldi, int32_t* info, void* stream);
 /* P = (P + P^T) / 2 in place (src/core/RitzExtraction.cpp:103). */
 int fe_symmetrize_f64(double* P, int64_t k, int64_t ldp, void* stream);
 

@@ -110,3 +110,41 @@ def test_grouped_rejects_ineligible():
     H = problem(10, "star1", 41)
     with pytest.raises(FastEigError, match="not eligible"):
         grouped_chebyshev([csr(H)], [opts(H.n, 8, precision="mixed")])
+
+
+@pytest.mark.parametrize("k", [1, 7, 32, 64, 96, 128])
+def test_chol_inv_batched(k):
+    """fe_chol_inv_upper_batched_f64: R^{-1} of chol(G) for a batch (one CTA per
+    matrix, shared memory) against numpy; a non-SPD member reports its pivot and
+    leaves the others unaffected."""
+    import torch
+    import fasteig_b200 as fe
+    rng = np.random.default_rng(k)
+    count = 3
+    Gs = []
+    for p in range(count):
+        M = rng.standard_normal((k, k))
+        Gs.append(M @ M.T + k * np.eye(k))
+    if k > 1:
+        Gs[1] = Gs[1].copy()
+        Gs[1][k // 2, k // 2] = -1.0  # not positive definite
+        Gs[1][k // 2, :k // 2] = 0.0
+        Gs[1][:k // 2, k // 2] = 0.0
+    host = np.stack([g.T.copy() for g in Gs])  # column-major per matrix
+    dG = torch.from_numpy(host).cuda()
+    dR = torch.full((count, k, k), np.nan, dtype=torch.float64, device="cuda")
+    info = torch.full((count,), -7, dtype=torch.int32, device="cuda")
+    assert fe.lib.fe_chol_inv_upper_batched_f64(count, dG.data_ptr(), k, k, dR.data_ptr(), k,
+                                                info.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    inf = info.cpu().numpy()
+    for p in range(count):
+        if k > 1 and p == 1:
+            assert inf[p] >= 1
+            continue
+        assert inf[p] == 0
+        Rinv = dR[p].cpu().numpy().T  # column-major -> matrix
+        R = np.linalg.cholesky(Gs[p]).T
+        ref = np.linalg.inv(R)
+        assert np.allclose(np.tril(Rinv, -1), 0.0)
+        assert np.abs(Rinv - ref).max() <= 1e-12 * np.abs(ref).max() * k

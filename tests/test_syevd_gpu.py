@@ -99,3 +99,31 @@ def test_batched_syevd_past_jacobi_limit():
     for p, (m, A) in enumerate(zip(sizes, As)):
         check(A, Wh[p, :m], Zh[p, :m, :m].T)
     assert np.array_equal(dA.cpu().numpy(), mats)  # input untouched
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("k", [32, 96, 160])
+def test_syevd_tridiagonalization_kernels(mode, k):
+    """Both tridiagonalization kernels (one CTA, 8-CTA cluster) give the spectrum of
+    numpy.linalg.eigh to 1e-12 * ||A|| and orthonormal vectors."""
+    import fasteig_b200 as fe
+    rng = np.random.default_rng(k + mode)
+    M = rng.standard_normal((k, k))
+    A = M + M.T
+    dA = torch.from_numpy(A.copy()).cuda()
+    W = torch.zeros(k, dtype=torch.float64, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    need = fe.lib.fe_syevd_f64_workspace_bytes(k)
+    ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+    assert fe.lib.fe_set_syevd_kernel(mode) == 0
+    try:
+        assert fe.lib.fe_syevd_f64(dA.data_ptr(), k, k, W.data_ptr(), info.data_ptr(),
+                                   ws.data_ptr(), need, None) == 0
+        torch.cuda.synchronize()
+    finally:
+        fe.lib.fe_set_syevd_kernel(0)
+    assert int(info.item()) == 0
+    scale = np.abs(A).sum(axis=1).max()
+    assert np.abs(W.cpu().numpy() - np.linalg.eigvalsh(A)).max() <= 1e-12 * scale
+    Z = dA.cpu().numpy().reshape(k, k).T  # column-major eigenvectors
+    assert np.abs(Z.T @ Z - np.eye(k)).max() <= 1e-12 * k
