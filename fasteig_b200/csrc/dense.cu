@@ -361,47 +361,58 @@ __global__ void trinv_upper_kernel(const double* __restrict__ R, int64_t ldr,
 }
 
 // Cholesky G = R^T R and R^{-1} of one small SPD matrix (k <= kCholSmallMax) per CTA,
-// with the whole matrix in shared memory (column-major, ld k + 1 so a row and a column
-// both fall on distinct banks): right-looking factorization (a warp per trailing
-// column), then the upper-triangular inverse column by column in place,
-// R^{-1}[0:j, j] = -R^{-1}[0:j, 0:j] R[0:j, j] / R_jj (the order of LAPACK's trti2).
+// with the matrix in shared memory, padded to a multiple of 32 with the identity
+// (column-major, ld kp + 1 so a row and a column both fall on distinct banks).
+//  1. Right-looking factorization, two barriers per pivot: every thread reads the
+//     pivot and forms its square root and reciprocal itself, row j is scaled, then
+//     the trailing upper triangle is updated (a warp per column).
+//  2. Blocked inverse in 32 x 32 blocks: each warp inverts one diagonal block by back
+//     substitution (a lane per column, no barrier), then block column J of R^{-1}
+//     for J = 1, 2, ...: T_I = sum_{L=I}^{J-1} R^{-1}_IL R_LJ for every I < J, and
+//     R^{-1}_IJ = -T_I R^{-1}_JJ (from R^{-1} R = I), two barriers per block column.
 // Only G's upper triangle is read; R^{-1} is written with a zero lower triangle, and
 // info = j + 1 for a non-positive or non-finite pivot j (R^{-1} is then not written).
 constexpr int kCholSmallMax = 128;
 constexpr int kCholSmallThreads = 512;
+constexpr int kCholBlk = 32;
+constexpr int kCholBlkLd = kCholBlk + 1;
+
+__host__ __device__ constexpr int chol_small_pad(int k) { return (k + kCholBlk - 1) / kCholBlk * kCholBlk; }
 
 __global__ void __launch_bounds__(kCholSmallThreads)
 chol_inv_small_kernel(const double* __restrict__ G, int k, int64_t ldg, int64_t stride_g,
                       double* __restrict__ Rinv, int64_t ldi, int64_t stride_i,
                       int32_t* __restrict__ info) {
   extern __shared__ double csm[];
-  __shared__ int failed;
-  const int ld = k + 1;
-  double* A = csm;           // k x ld
-  double* tmp = csm + k * ld;  // k
+  const int kp = chol_small_pad(k);
+  const int nb = kp / kCholBlk;
+  const int ld = kp + 1;
+  double* A = csm;                               // kp x ld
+  double* dinv = A + static_cast<size_t>(kp) * ld;  // 1 / R_jj
+  double* S = dinv + kp;                         // nb diagonal-block inverses, 32 x 33 each
+  double* T = S + nb * kCholBlk * kCholBlkLd;    // nb - 1 (at least 1) products
   G += static_cast<int64_t>(blockIdx.x) * stride_g;
   Rinv += static_cast<int64_t>(blockIdx.x) * stride_i;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
   constexpr int kWarps = kCholSmallThreads / 32;
-  for (int c = warp; c < k; c += kWarps)
-    for (int r = lane; r <= c; r += 32) A[r + c * ld] = G[r + static_cast<int64_t>(c) * ldg];
-  if (tid == 0) failed = 0;
+  for (int c = warp; c < kp; c += kWarps)
+    for (int r = lane; r <= c; r += 32)
+      A[r + c * ld] = (c < k) ? G[r + static_cast<int64_t>(c) * ldg] : (r == c ? 1.0 : 0.0);
   __syncthreads();
-  for (int j = 0; j < k; ++j) {
-    if (tid == 0) {
-      const double d = A[j + j * ld];
-      if (!(d > 0.0) || !isfinite(d)) failed = j + 1;
-      else A[j + j * ld] = sqrt(d);
+  int failed = 0;
+  for (int j = 0; j < kp; ++j) {
+    const double d = A[j + j * ld];
+    if (!(d > 0.0) || !isfinite(d)) {
+      failed = j + 1;
+      break;
     }
+    const double inv = 1.0 / sqrt(d);
+    for (int c = j + 1 + tid; c < kp; c += kCholSmallThreads) A[j + c * ld] *= inv;
+    if (tid == 0) dinv[j] = inv;
     __syncthreads();
-    if (failed) break;
-    const double inv = 1.0 / A[j + j * ld];
-    for (int c = j + 1 + tid; c < k; c += kCholSmallThreads) A[j + c * ld] *= inv;
-    __syncthreads();
-    // trailing update of the upper triangle: A[a][c] -= R[j][a] R[j][c], j < a <= c
-    for (int c = j + 1 + warp; c < k; c += kWarps) {
+    for (int c = j + 1 + warp; c < kp; c += kWarps) {
       const double rjc = A[j + c * ld];
       for (int a = j + 1 + lane; a <= c; a += 32) A[a + c * ld] -= A[j + a * ld] * rjc;
     }
@@ -411,22 +422,62 @@ chol_inv_small_kernel(const double* __restrict__ G, int k, int64_t ldg, int64_t 
     if (tid == 0 && info) info[blockIdx.x] = failed;
     return;
   }
-  for (int j = 0; j < k; ++j) {
-    for (int i = tid; i < j; i += kCholSmallThreads) tmp[i] = A[i + j * ld];
-    __syncthreads();
-    const double djj = 1.0 / A[j + j * ld];
-    for (int i = tid; i < j; i += kCholSmallThreads) {
+  // diagonal blocks: warp w, lane c computes column c of (R_ww)^{-1}
+  if (warp < nb) {
+    const int o = warp * kCholBlk;
+    double* Sw = S + warp * kCholBlk * kCholBlkLd;
+    const int c = lane;
+    Sw[c + c * kCholBlkLd] = dinv[o + c];
+    for (int i = c - 1; i >= 0; --i) {
       double acc = 0.0;
-      for (int l = i; l < j; ++l) acc = fma(A[i + l * ld], tmp[l], acc);
-      A[i + j * ld] = -djj * acc;
+      for (int l = i + 1; l <= c; ++l)
+        acc = fma(A[(o + i) + (o + l) * ld], Sw[l + c * kCholBlkLd], acc);
+      Sw[i + c * kCholBlkLd] = -acc * dinv[o + i];
     }
-    __syncthreads();
-    if (tid == 0) A[j + j * ld] = djj;
+    for (int i = c + 1; i < kCholBlk; ++i) Sw[i + c * kCholBlkLd] = 0.0;
   }
   __syncthreads();
-  for (int c = warp; c < k; c += kWarps)
-    for (int r = lane; r < k; r += 32)
-      Rinv[r + static_cast<int64_t>(c) * ldi] = r <= c ? A[r + c * ld] : 0.0;
+  for (int J = 1; J < nb; ++J) {
+    const int count = J * kCholBlk * kCholBlk;
+    for (int e = tid; e < count; e += kCholSmallThreads) {
+      const int I = e / (kCholBlk * kCholBlk);
+      const int rc = e % (kCholBlk * kCholBlk);
+      const int c = rc / kCholBlk, r = rc % kCholBlk;
+      const double* SI = S + I * kCholBlk * kCholBlkLd;
+      double acc = 0.0;
+      for (int m = r; m < kCholBlk; ++m)  // (R_II)^{-1} is upper triangular
+        acc = fma(SI[r + m * kCholBlkLd], A[(I * kCholBlk + m) + (J * kCholBlk + c) * ld], acc);
+      for (int L = I + 1; L < J; ++L)
+        for (int m = 0; m < kCholBlk; ++m)
+          acc = fma(A[(I * kCholBlk + r) + (L * kCholBlk + m) * ld],
+                    A[(L * kCholBlk + m) + (J * kCholBlk + c) * ld], acc);
+      T[I * kCholBlk * kCholBlkLd + r + c * kCholBlkLd] = acc;
+    }
+    __syncthreads();
+    const double* SJ = S + J * kCholBlk * kCholBlkLd;
+    for (int e = tid; e < count; e += kCholSmallThreads) {
+      const int I = e / (kCholBlk * kCholBlk);
+      const int rc = e % (kCholBlk * kCholBlk);
+      const int c = rc / kCholBlk, r = rc % kCholBlk;
+      const double* TI = T + I * kCholBlk * kCholBlkLd;
+      double acc = 0.0;
+      for (int m = 0; m <= c; ++m) acc = fma(TI[r + m * kCholBlkLd], SJ[m + c * kCholBlkLd], acc);
+      A[(I * kCholBlk + r) + (J * kCholBlk + c) * ld] = -acc;
+    }
+    __syncthreads();
+  }
+  for (int c = warp; c < k; c += kWarps) {
+    for (int r = lane; r < k; r += 32) {
+      double v = 0.0;
+      if (r <= c) {
+        v = (r / kCholBlk == c / kCholBlk)
+                ? S[(c / kCholBlk) * kCholBlk * kCholBlkLd + (r % kCholBlk) +
+                    (c % kCholBlk) * kCholBlkLd]
+                : A[r + c * ld];
+      }
+      Rinv[r + static_cast<int64_t>(c) * ldi] = v;
+    }
+  }
   if (tid == 0 && info) info[blockIdx.x] = 0;
 }
 
@@ -505,7 +556,11 @@ void trinv_upper_batched(const double* R, int64_t ldr, double* Rinv, int64_t ldi
 }
 
 size_t chol_inv_small_smem(int64_t k) {
-  return (static_cast<size_t>(k) * (k + 1) + k) * sizeof(double);
+  const int64_t kp = chol_small_pad(static_cast<int>(k));
+  const int64_t nb = kp / kCholBlk;
+  return static_cast<size_t>(kp * (kp + 1) + kp +
+                             (nb + std::max<int64_t>(nb - 1, 1)) * kCholBlk * kCholBlkLd) *
+         sizeof(double);
 }
 
 bool chol_inv_small_fits(int64_t k) { return k >= 1 && k <= kCholSmallMax; }

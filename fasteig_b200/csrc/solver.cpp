@@ -544,6 +544,18 @@ void rotate_block(SmallState& sm, const T* X, int64_t ldx, const double* C, T* Y
   rotate<T>(X, ldx, C, sm.cap, Y, ldy, n, k, m, alpha, beta, s, upper_tri);
 }
 
+// R^{-1} of chol(G) into Rinv, info as potrf_upper: one fused shared-memory launch for
+// k <= 128; otherwise the factorization in G (which then holds R) and the inverse.
+void chol_inverse(double* G, int64_t k, int64_t ldg, double* Rinv, int64_t ldi, int32_t* info,
+                  cudaStream_t s) {
+  if (chol_inv_small_fits(k)) {
+    chol_inv_upper_batched(G, k, ldg, 0, Rinv, ldi, 0, 1, info, s);
+  } else {
+    potrf_upper(G, k, ldg, info, s);
+    trinv_upper(G, ldg, Rinv, ldi, k, s);
+  }
+}
+
 // Cholesky QR of src (n x k) into dst: G = src^T src, R = chol(G), dst = src R^{-1}
 // (cuda_cholesky_qr_in_place, src/core/Orthogonalization.cpp:185-246).
 // The rank-loss flag accumulates into info[slot]. With tensor-core Grams, a
@@ -555,7 +567,7 @@ void cholqr(Context& ctx, SmallState& sm, const T* src, int64_t lds, T* dst, int
   double* G = sm.G.as<double>();
   int32_t* info = sm.info.as<int32_t>() + slot;
   gram_block<T>(sm, src, lds, src, lds, n, k, k, G, s);
-  potrf_upper(G, k, sm.cap, info, s);
+  chol_inverse(G, k, sm.cap, sm.Rinv.as<double>(), sm.cap, info, s);
   if (sizeof(T) == 4 && sm.tensor_cores) {
     int32_t h = 0;
     ctx.to_host(&h, info, 1);
@@ -563,10 +575,9 @@ void cholqr(Context& ctx, SmallState& sm, const T* src, int64_t lds, T* dst, int
     if (h != 0) {
       sm.precise_grams += 1;
       gram_block<T>(sm, src, lds, src, lds, n, k, k, G, s, /*precise=*/true);
-      potrf_upper(G, k, sm.cap, info, s);
+      chol_inverse(G, k, sm.cap, sm.Rinv.as<double>(), sm.cap, info, s);
     }
   }
-  trinv_upper(G, sm.cap, sm.Rinv.as<double>(), sm.cap, k, s);
   rotate_block<T>(sm, src, lds, sm.Rinv.as<double>(), dst, ldd, n, k, k, 1.0, 0.0, s,
                   /*upper_tri=*/true);
 }
@@ -610,11 +621,12 @@ bool fused_rr(Context& ctx, SmallState& sm, ProjectedEig& eig, const Csr& A, dou
     }
   }
   if (!split) gram_block<T>(sm, Y, ldy, AY, lday, n, k, k, H, s);
+  double* Rinv = sm.Rinv.as<double>();
   auto factor = [&] {
     FE_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int32_t), s));
     inv_sqrt_diag(G, k, ld, d, s);
     diag_scale(G, k, k, ld, d, true, s);
-    potrf_upper(G, k, ld, info, s);
+    chol_inverse(G, k, ld, Rinv, ld, info, s);
     int32_t h = 0;
     ctx.to_host(&h, info, 1);
     ctx.sync();
@@ -631,9 +643,7 @@ bool fused_rr(Context& ctx, SmallState& sm, ProjectedEig& eig, const Csr& A, dou
     }
   }
   diag_scale(H, k, k, ld, d, true, s);
-  double* Rinv = sm.Rinv.as<double>();
   double* Tm = sm.Tmp.as<double>();
-  trinv_upper(G, ld, Rinv, ld, k, s);
   small_gemm(false, k, k, k, 1.0, H, ld, Rinv, ld, 0.0, Tm, ld, s);    // H R^-1
   small_gemm(true, k, k, k, 1.0, Rinv, ld, Tm, ld, 0.0, H, ld, s);     // R^-T H R^-1
   symmetrize(H, k, ld, s);
@@ -1770,12 +1780,11 @@ struct GenBlockOpsT {
     gram_block<T>(sm, X, ld, BX, ld, n, b, b, G, s);
     symmetrize(G, b, sm.cap, s);
     FE_CHECK_CUDA(cudaMemsetAsync(sm.info.get(), 0, sizeof(int32_t), s));
-    potrf_upper(G, b, sm.cap, sm.info.as<int32_t>(), s);
+    chol_inverse(G, b, sm.cap, sm.Rinv.as<double>(), sm.cap, sm.info.as<int32_t>(), s);
     int32_t info = 0;
     ctx.to_host(&info, sm.info.as<int32_t>(), 1);
     ctx.sync();
     if (info != 0) throw Error(FE_ERR_NOT_SPD, std::string(what) + ": weighted QR failed.");
-    trinv_upper(G, sm.cap, sm.Rinv.as<double>(), sm.cap, b, s);
     rotate_block<T>(sm, X, ld, sm.Rinv.as<double>(), tmp, ld, n, b, b, 1.0, 0.0, s);
     rotate_block<T>(sm, BX, ld, sm.Rinv.as<double>(), tmpB, ld, n, b, b, 1.0, 0.0, s);
     copy(X, tmp, b);
