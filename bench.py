@@ -220,6 +220,9 @@ def run_batch_ks(a):
         rounds, steps = st["rounds"], st["steps"]
     sec = sum(times) / len(times)
     n_total = sum(H.n for H, _ in probs)
+    cpu = None
+    if rank == 0 and not a.no_cpu:
+        cpu = batch_ks_cpu_sample(probs, a.tol)
     line = {"metric": METRIC, "value": round(conv / sec, 3), "unit": UNIT, "n_gpus": 1,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(sec * 1e3, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -231,8 +234,37 @@ def run_batch_ks(a):
             "converged_pairs": conv, "restart_rounds": rounds, "lanczos_steps": steps,
             "latency_s": {"p50": sorted(times)[len(times) // 2], "max": max(times)},
             "csr_upload_s": round(upload_s, 2)}
+    if cpu:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0
+
+
+def batch_ks_cpu_sample(probs, tol, budget_s=15.0):
+    """cpu_baseline of the batch line: the oracle's Krylov-Schur (the restatement of
+    src/KrylovSchurSolver.cpp:28-160, scipy sparse SpMV and NumPy reorthogonalization)
+    on the batch's problems in order, one after another, until budget_s of host time
+    has run (the problems are i.i.d. draws, so the first ones are a fair sample)."""
+    import numpy as np
+    from oracle import oracle as O
+    from oracle import cpu as ocpu
+    t_all, pairs, done, rows = 0.0, 0, 0, 0
+    for H, nev in probs:
+        A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
+        t = time.perf_counter()
+        r = O.krylov_schur_solve(A, nev, tol=tol, maxiter=5000, which="sr", seed=1)
+        t_all += time.perf_counter() - t
+        pairs += int((np.asarray(r.residual_norms) <= tol).sum())
+        done += 1
+        rows += H.n
+        if t_all >= budget_s:
+            break
+    return {"value": round(pairs / t_all, 3), "unit": UNIT, "cores": ocpu.host_threads(),
+            "kind": "port",
+            "sample": f"oracle Krylov-Schur on the first {done} of the batch's problems "
+                      f"({rows} rows, {pairs} converged pairs) one after another, "
+                      f"{t_all:.1f} s of host time (scipy SpMV on one thread, NumPy BLAS "
+                      f"reorthogonalization on the host threads)"}
 
 
 def run_generalized(a):
