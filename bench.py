@@ -79,10 +79,12 @@ def args_parse():
     p.add_argument("--requests", type=int, default=200,
                    help="serving: number of requests (the configuration names 10,000)")
     p.add_argument("--slots", type=int, default=6, help="serving: concurrent solves")
-    p.add_argument("--serving-chebyshev", default="grouped", choices=["grouped", "slots"],
-                   help="serving: Chebyshev requests in grouped lanes (FP64, continuous "
-                        "batching in grouped kernels) or in worker slots (mixed precision, "
-                        "one solve per request)")
+    p.add_argument("--serving-chebyshev", default="grouped",
+                   choices=["grouped", "grouped-fp64", "slots"],
+                   help="serving: Chebyshev requests in grouped lanes (continuous batching in "
+                        "grouped kernels; mixed precision: FP32 filter to the FP32 floor, or "
+                        "FP64 throughout) or in worker slots (mixed precision with hard "
+                        "locking, one solve per request)")
     p.add_argument("--solve-only", default=None, choices=["mixed", "fp64"],
                    help="run exactly one solve of the workload at this precision and print its "
                         "stats (launch-list profiling driver; no bench line)")
@@ -322,49 +324,64 @@ def run_grouped(a):
     torch.cuda.set_device(0)
     rng = np.random.Generator(np.random.PCG64(11))
     probs = []
+    specs = []
     for i in range(48):
         n_target = math.exp(rng.uniform(math.log(1e4), math.log(2e5)))
         side = max(8, int(round(n_target ** (1.0 / 3.0))))
         stencil = "star1" if i % 2 == 0 else "star2"
         H = M.laplacian_wells(side, wells=16, seed=300 + i, stencil=stencil)
         nev = int(rng.integers(8, 49))
-        o = fe.fasteig_options(H.n)
-        for k, v in dict(solver="Chebyshev", nev=nev, which="SR", tol=1e-8, maxiter=400,
-                         seed=1 + i, degree=16, bounds="ritz", amplification=1e6,
-                         init="device").items():
-            assert o.set(k, v), k
-        probs.append((H, fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values), o, nev))
-    mats = [A for _, A, _, _ in probs]
-    opts = [o for _, _, o, _ in probs]
+        probs.append((H, fe.CsrMatrix(H.n, H.rowptr, H.colind, H.values), nev))
+    mats = [A for _, A, _ in probs]
     asked = sum(nev for *_, nev in probs)
-    # warm-up: one small group and one solve (kernel loading, pools)
-    fe.grouped_chebyshev(mats[:2], opts[:2])
-    fe.fasteig_problem(mats[0], solver="Chebyshev").solve(opts[0], want_vectors=False)
-    torch.cuda.synchronize()
-    torch.cuda.profiler.start()  # a profiler capture (if any) covers the grouped call
-    t0 = time.perf_counter()
-    out, batch = fe.grouped_chebyshev(mats, opts)
-    t_group = time.perf_counter() - t0
-    torch.cuda.profiler.stop()
-    conv_g = sum(int((r["residual_norms"] <= 1e-8).sum()) for r in out)
-    t0 = time.perf_counter()
-    conv_s = 0
-    for A, o in zip(mats, opts):
-        p = fe.fasteig_problem(A, solver="Chebyshev")
-        p.solve(o, want_vectors=False)
-        conv_s += int((p.residual_norms() <= 1e-8).sum())
-    t_seq = time.perf_counter() - t0
+
+    def options(precision):
+        out = []
+        for i, (H, _, nev) in enumerate(probs):
+            o = fe.fasteig_options(H.n)
+            for k, v in dict(solver="Chebyshev", nev=nev, which="SR", tol=1e-8, maxiter=400,
+                             seed=1 + i, degree=16, bounds="ritz", amplification=1e6,
+                             init="device", precision=precision).items():
+                assert o.set(k, v), k
+            out.append(o)
+        return out
+
     cfg = {"workload": "grouped_chebyshev_48", "problems": 48, "n_range": [1e4, 2e5],
-           "nev_range": [8, 48], "tol": 1e-8, "degree": 16, "sum_n": int(sum(H.n for H, *_ in probs)),
-           "requested_pairs": int(asked)}
-    for impl, sec, conv, extra in (("grouped", t_group, conv_g, {"batch": batch,
-                                                                 "widths": sorted({r["width"] for r in out})}),
-                                   ("one_solve_per_problem", t_seq, conv_s, {})):
-        print(json.dumps(dict({"metric": METRIC, "value": round(conv / sec, 3), "unit": UNIT,
-                               "n_gpus": 1, "steps": 1, "warmup": 1,
-                               "ms_per_step": round(sec * 1e3, 1), "higher_is_better": True,
-                               "dtype": "f64", "data": "synthetic", "impl": impl, "config": cfg,
-                               "converged_pairs": conv}, **extra)), flush=True)
+           "nev_range": [8, 48], "tol": 1e-8, "degree": 16,
+           "sum_n": int(sum(H.n for H, *_ in probs)), "requested_pairs": int(asked)}
+    for precision in ("fp64", "mixed"):
+        opts = options(precision)
+        # warm-up: one small group and one solve (kernel loading, pools)
+        fe.grouped_chebyshev(mats[:2], opts[:2])
+        fe.fasteig_problem(mats[0], solver="Chebyshev").solve(opts[0], want_vectors=False)
+        torch.cuda.synchronize()
+        if precision == "fp64":
+            torch.cuda.profiler.start()  # a profiler capture (if any) covers this call
+        t0 = time.perf_counter()
+        out, batch = fe.grouped_chebyshev(mats, opts)
+        t_group = time.perf_counter() - t0
+        if precision == "fp64":
+            torch.cuda.profiler.stop()
+        conv_g = sum(int((r["residual_norms"] <= 1e-8).sum()) for r in out)
+        t0 = time.perf_counter()
+        conv_s = 0
+        for A, o in zip(mats, opts):
+            p = fe.fasteig_problem(A, solver="Chebyshev")
+            p.solve(o, want_vectors=False)
+            conv_s += int((p.residual_norms() <= 1e-8).sum())
+        t_seq = time.perf_counter() - t0
+        dtype = "f64" if precision == "fp64" else "f32+f64"
+        grouped_extra = {"batch": batch, "widths": sorted({r["width"] for r in out}),
+                         "fp32_cycles": int(sum(r["fp32_iterations"] for r in out)),
+                         "cycles": int(sum(r["iterations"] for r in out))}
+        for impl, sec, conv, extra in (("grouped", t_group, conv_g, grouped_extra),
+                                       ("one_solve_per_problem", t_seq, conv_s, {})):
+            print(json.dumps(dict({"metric": METRIC, "value": round(conv / sec, 3), "unit": UNIT,
+                                   "n_gpus": 1, "steps": 1, "warmup": 1,
+                                   "ms_per_step": round(sec * 1e3, 1), "higher_is_better": True,
+                                   "dtype": dtype, "data": "synthetic", "impl": impl,
+                                   "config": dict(cfg, precision=precision),
+                                   "converged_pairs": conv}, **extra)), flush=True)
     return 0
 
 
@@ -395,10 +412,15 @@ def run_serving(a):
         solver = "Chebyshev" if rng.random() < 0.5 else "LOBPCG"
         o = fe.fasteig_options(H.n)
         kv = dict(solver=solver, nev=nev, which="SR", tol=tol, seed=1 + k, init="device")
-        if solver == "Chebyshev" and a.serving_chebyshev == "grouped":
-            # FP64 Chebyshev in the grouped lane of its width: joins the lane's group
-            # between cycles and advances with the other admitted requests
+        if solver == "Chebyshev" and a.serving_chebyshev.startswith("grouped"):
+            # the grouped lane of its width: joins the lane's group between cycles and
+            # advances with the other admitted requests (mixed: in the FP32-filter group
+            # until its FP32 floor, then in the FP64 one)
             kv.update(degree=16, bounds="ritz", amplification=1e6, maxiter=300, group=1)
+            if a.serving_chebyshev == "grouped":
+                kv.update(precision="mixed")
+                if tol < 1e-6:
+                    kv.update(mixed_switch=1e-6)
         elif solver == "Chebyshev":
             # mixed precision with hard locking; for tol 1e-8 the FP32 pairs lock at
             # 1e-6 before the FP64 cycles (the default 4e-6 floor where tol is 1e-6)

@@ -58,9 +58,10 @@ __global__ void bad_diagonal_kernel(const int32_t* __restrict__ rowptr,
 
 // One thread per row: the scaled operator c A + d I of the row's member (the
 // reference's filter operator, src/ChebyshevSolver.cpp:231-245).
+template <typename T>
 __global__ void rescale_kernel(const int32_t* __restrict__ rowptr,
                                const int32_t* __restrict__ colind,
-                               const double* __restrict__ plain, double* __restrict__ scaled,
+                               const double* __restrict__ plain, T* __restrict__ scaled,
                                int64_t rows, const int32_t* __restrict__ tile_member,
                                const double* __restrict__ cd) {
   for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < rows;
@@ -69,7 +70,7 @@ __global__ void rescale_kernel(const int32_t* __restrict__ rowptr,
     const double c = cd[2 * p];
     const double d = cd[2 * p + 1];
     for (int32_t j = rowptr[r]; j < rowptr[r + 1]; ++j)
-      scaled[j] = c * plain[j] + (colind[j] == r ? d : 0.0);
+      scaled[j] = static_cast<T>(c * plain[j] + (colind[j] == r ? d : 0.0));
   }
 }
 
@@ -190,7 +191,16 @@ void group_rescale(const int32_t* rowptr, const int32_t* colind, const double* p
                    double* scaled, int64_t rows, const int32_t* tile_member, const double* cd,
                    cudaStream_t s) {
   if (rows == 0) return;
-  rescale_kernel<<<grid_for(rows, kPackThreads), kPackThreads, 0, s>>>(
+  rescale_kernel<double><<<grid_for(rows, kPackThreads), kPackThreads, 0, s>>>(
+      rowptr, colind, plain, scaled, rows, tile_member, cd);
+  check_launch("rescale_kernel");
+}
+
+void group_rescale_f32(const int32_t* rowptr, const int32_t* colind, const double* plain,
+                       float* scaled, int64_t rows, const int32_t* tile_member, const double* cd,
+                       cudaStream_t s) {
+  if (rows == 0) return;
+  rescale_kernel<float><<<grid_for(rows, kPackThreads), kPackThreads, 0, s>>>(
       rowptr, colind, plain, scaled, rows, tile_member, cd);
   check_launch("rescale_kernel");
 }

@@ -96,7 +96,7 @@ void filter_scaling(double cutoff, double upper, double* c, double* d) {
 
 }  // namespace
 
-size_t group_member_bytes(const Csr& A, int64_t width) {
+size_t group_member_bytes(const Csr& A, int64_t width, bool mixed) {
   const int64_t n_pad = round_up(std::max<int64_t>(A.rows, 1), kTile);
   const double blk = static_cast<double>(n_pad) * width * 8.0;
   const double csr = static_cast<double>(n_pad + 1) * 4.0 + static_cast<double>(A.nnz) * 20.0;
@@ -105,16 +105,20 @@ size_t group_member_bytes(const Csr& A, int64_t width) {
                     8.0 * width * width * 8.0 +
                     static_cast<double>(syevd_workspace_bytes(1, width));
   const double bounds = static_cast<double>(A.rows) * 26.0 * 8.0;  // Lanczos basis at join
-  // blocks plus the new Ritz block of a repack, two operator copies during a repack
-  return static_cast<size_t>((kBlocks + 1) * blk + 2.0 * csr + ws + bounds) + (size_t(16) << 20);
+  // blocks plus the new Ritz block of a repack, two operator copies during a repack;
+  // mixed: three FP32 filter blocks, the FP32 operator values, the carried Ritz block
+  const double extra = mixed ? 2.5 * blk + static_cast<double>(A.nnz) * 8.0 : 0.0;
+  return static_cast<size_t>((kBlocks + 1) * blk + 2.0 * csr + ws + bounds + extra) +
+         (size_t(16) << 20);
 }
 
 struct ChebGroup::Impl {
   int64_t R = 0, NNZ = 0, tiles = 0, chunks = 0;
   int G = 0;
   int64_t max_row_nnz = 0;
-  DeviceBuffer rowptr, colind, plain, scaled;
+  DeviceBuffer rowptr, colind, plain, scaled, scaled32;
   DeviceBuffer blk[kBlocks];
+  DeviceBuffer f32[3];  // FP32 filter ring of an FP32-filter group
   DeviceBuffer tile_member, chunk_rows, chunk_member, member_chunks;
   DeviceBuffer gpart, rpart, Gm, Rinv, Q, theta, rel, info, cd, syevd_ws;
   PinnedBuffer cd_h, theta_h, rel_h, info_h;
@@ -133,8 +137,8 @@ struct ChebGroup::Impl {
   ~Impl() { drop_graph(); }
 };
 
-ChebGroup::ChebGroup(int device, int64_t width, int64_t degree)
-    : impl_(new Impl), device_(device), width_(width), degree_(degree) {
+ChebGroup::ChebGroup(int device, int64_t width, int64_t degree, bool fp32_filter)
+    : impl_(new Impl), device_(device), width_(width), degree_(degree), fp32_(fp32_filter) {
   FE_REQUIRE(width >= 32 && width % 32 == 0 && width <= 512, "grouped Chebyshev: invalid width");
   FE_REQUIRE(degree >= 1, "grouped Chebyshev: degree must be >= 1");
   FE_CHECK_CUDA(cudaSetDevice(device));
@@ -158,10 +162,19 @@ void ChebGroup::join(GroupMember* m) {
   FE_REQUIRE(m && m->A, "grouped Chebyshev: null member");
   FE_REQUIRE(m->g.width == width_ && m->g.degree == degree_,
              "grouped Chebyshev: member width or degree differs from the group's");
+  FE_REQUIRE(!fp32_ || m->g.mixed, "grouped Chebyshev: FP64 member in an FP32-filter group");
   m->fresh = true;
-  m->iterations = 0;
-  m->t_join = std::chrono::steady_clock::now();
-  m->cutoff = m->g.reference_cutoff;
+  if (m->switched) {
+    // from the FP32-filter group of its width: keeps its cycle count, interval and
+    // Ritz block (m->carry)
+    m->switched = false;
+  } else {
+    m->iterations = 0;
+    m->fp32_iterations = 0;
+    m->worst_history.clear();
+    m->t_join = std::chrono::steady_clock::now();
+    m->cutoff = m->g.reference_cutoff;
+  }
   joining_.push_back(m);
   impl_->dirty = true;
 }
@@ -240,6 +253,8 @@ void ChebGroup::launch_cycle() {
     I.colind.release();
     I.plain.release();
     I.scaled.release();
+    I.scaled32.release();
+    for (auto& f : I.f32) f.release();
     I.gpart.release();
     I.rpart.release();
 
@@ -249,6 +264,13 @@ void ChebGroup::launch_cycle() {
     for (GroupMember* m : order) {
       if (!m->fresh) continue;
       double* dst = X.as<double>() + m->row0 * b;
+      if (m->carry.get()) {
+        // Ritz block carried over from the FP32-filter group (same width and padding)
+        FE_CHECK_CUDA(cudaMemcpyAsync(dst, m->carry.get(),
+                                      static_cast<size_t>(m->n_pad) * b * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, s));
+        continue;
+      }
       if (m->g.host_init) {
         std::mt19937 rng(m->g.seed);
         std::uniform_real_distribution<double> dist(-1.0, 1.0);
@@ -273,7 +295,15 @@ void ChebGroup::launch_cycle() {
     I.rowptr.resize(static_cast<size_t>(R + 1) * sizeof(int32_t));
     I.colind.resize(static_cast<size_t>(std::max<int64_t>(NNZ, 1)) * sizeof(int32_t));
     I.plain.resize(static_cast<size_t>(std::max<int64_t>(NNZ, 1)) * sizeof(double));
-    I.scaled.resize(static_cast<size_t>(std::max<int64_t>(NNZ, 1)) * sizeof(double));
+    if (fp32_) {
+      I.scaled32.resize(static_cast<size_t>(std::max<int64_t>(NNZ, 1)) * sizeof(float));
+      for (auto& f : I.f32) {
+        f.resize(static_cast<size_t>(R) * b * sizeof(float));
+        FE_CHECK_CUDA(cudaMemsetAsync(f.get(), 0, static_cast<size_t>(R) * b * sizeof(float), s));
+      }
+    } else {
+      I.scaled.resize(static_cast<size_t>(std::max<int64_t>(NNZ, 1)) * sizeof(double));
+    }
     for (GroupMember* m : order)
       group_pack_member(*m->A, m->row0, m->n_pad, m->nz0, m->g.sign, I.rowptr.as<int32_t>(),
                         I.colind.as<int32_t>(), I.plain.as<double>(), s);
@@ -293,7 +323,8 @@ void ChebGroup::launch_cycle() {
       op->max_row_nnz = maxnz;
       op->bandwidth = -1;
     }
-    I.op_scaled.val64 = I.scaled.as<double>();
+    I.op_scaled.val64 = fp32_ ? nullptr : I.scaled.as<double>();
+    I.op_scaled.val32 = fp32_ ? I.scaled32.as<float>() : nullptr;
     I.op_plain.val64 = I.plain.as<double>();
 
     // Tables: row tile -> member, chunk -> rows and member, member -> chunks.
@@ -320,6 +351,7 @@ void ChebGroup::launch_cycle() {
     upload(I.member_chunks, member_chunks.data(), member_chunks.size() * sizeof(int32_t));
     upload(I.chunk_rows, chunk_rows.data(), chunk_rows.size() * sizeof(int64_t));
     FE_CHECK_CUDA(cudaStreamSynchronize(s));  // host tables leave scope
+    for (GroupMember* m : order) m->carry.release();  // copied (the stream is idle)
 
     // Workspaces.
     const size_t bb = static_cast<size_t>(b) * b * sizeof(double);
@@ -368,16 +400,34 @@ void ChebGroup::launch_cycle() {
     int32_t* info = I.info.as<int32_t>();
     FE_CHECK_CUDA(cudaMemcpyAsync(I.cd.get(), I.cd_h.as<double>(), 2 * G * sizeof(double),
                                   cudaMemcpyHostToDevice, s));
-    group_rescale(I.rowptr.as<int32_t>(), I.colind.as<int32_t>(), I.plain.as<double>(),
-                  I.scaled.as<double>(), R, I.tile_member.as<int32_t>(), I.cd.as<double>(), s);
-    // 2. filter: step k's result in ring slot k mod 3
-    csr_spmm<double>(I.op_scaled, B[0], b, B[1], b, nullptr, 0, b, 1.0, 0.0, 0.0, s);
-    for (int64_t k = 2; k <= degree_; ++k) {
-      const int prev = static_cast<int>((k - 2) % 3), cur = static_cast<int>((k - 1) % 3),
-                next = static_cast<int>(k % 3);
-      csr_spmm<double>(I.op_scaled, B[cur], b, B[next], b, B[prev], b, b, 2.0, 0.0, -1.0, s);
+    // 2. filter: step k's result in ring slot k mod 3 (FP32 groups: an FP32 ring,
+    // the result widened into slot 1 of the FP64 blocks)
+    int res = static_cast<int>(degree_ % 3);
+    if (fp32_) {
+      group_rescale_f32(I.rowptr.as<int32_t>(), I.colind.as<int32_t>(), I.plain.as<double>(),
+                        I.scaled32.as<float>(), R, I.tile_member.as<int32_t>(),
+                        I.cd.as<double>(), s);
+      float* F[3] = {I.f32[0].as<float>(), I.f32[1].as<float>(), I.f32[2].as<float>()};
+      convert<double, float>(B[0], b, F[0], b, R, b, s);
+      csr_spmm<float>(I.op_scaled, F[0], b, F[1], b, nullptr, 0, b, 1.0, 0.0, 0.0, s);
+      for (int64_t k = 2; k <= degree_; ++k) {
+        const int prev = static_cast<int>((k - 2) % 3), cur = static_cast<int>((k - 1) % 3),
+                  next = static_cast<int>(k % 3);
+        csr_spmm<float>(I.op_scaled, F[cur], b, F[next], b, F[prev], b, b, 2.0, 0.0, -1.0, s);
+      }
+      convert<float, double>(F[res], b, B[1], b, R, b, s);
+      res = 1;
+    } else {
+      group_rescale(I.rowptr.as<int32_t>(), I.colind.as<int32_t>(), I.plain.as<double>(),
+                    I.scaled.as<double>(), R, I.tile_member.as<int32_t>(), I.cd.as<double>(),
+                    s);
+      csr_spmm<double>(I.op_scaled, B[0], b, B[1], b, nullptr, 0, b, 1.0, 0.0, 0.0, s);
+      for (int64_t k = 2; k <= degree_; ++k) {
+        const int prev = static_cast<int>((k - 2) % 3), cur = static_cast<int>((k - 1) % 3),
+                  next = static_cast<int>(k % 3);
+        csr_spmm<double>(I.op_scaled, B[cur], b, B[next], b, B[prev], b, b, 2.0, 0.0, -1.0, s);
+      }
     }
-    const int res = static_cast<int>(degree_ % 3);
     // 3. Cholesky QR twice, ending in a slot other than 0 (slot 0 receives X)
     const int s1 = res == 0 ? 1 : (res == 1 ? 2 : 1);
     const int s2 = res == 0 ? 2 : res;
@@ -458,7 +508,9 @@ void ChebGroup::finish_cycle(std::vector<GroupMember*>& done) {
   if (!launched_) return;
   launched_ = false;
   FE_CHECK_CUDA(cudaStreamSynchronize(stream_));
+  AllocOn on(stream_);
   ++cycles;
+  bool carried = false;
   Impl& I = *impl_;
   const int64_t b = width_;
   const double* theta = I.theta_h.as<double>();
@@ -468,6 +520,7 @@ void ChebGroup::finish_cycle(std::vector<GroupMember*>& done) {
   for (int p = 0; p < I.G; ++p) {
     GroupMember* m = members_[p];
     ++m->iterations;
+    if (fp32_) ++m->fp32_iterations;
     const double* th = theta + static_cast<int64_t>(p) * b;
     const double* rl = rel + static_cast<int64_t>(p) * b;
     bool finite = true;
@@ -484,6 +537,24 @@ void ChebGroup::finish_cycle(std::vector<GroupMember*>& done) {
     double worst = 0.0;
     for (int64_t j = 0; j < m->g.nev; ++j) worst = std::max(worst, rl[j]);
     const bool converged = rc == FE_OK && worst <= m->g.tol;
+    if (fp32_ && rc == FE_OK && !converged && m->iterations < m->g.maxiter) {
+      // Leave the FP32 filter at its residual floor, or when it stops reducing the
+      // worst residual (no 30 % gain over three cycles), as the mixed single solve.
+      m->worst_history.push_back(worst);
+      const size_t h = m->worst_history.size();
+      const bool stalled = h >= 4 && worst > 0.7 * m->worst_history[h - 4];
+      if (worst <= std::max(m->g.tol, m->g.mixed_switch) || stalled) {
+        if (m->g.ritz_bounds) m->cutoff = std::min(th[b - 1], m->g.ritz_cutoff_cap);
+        m->carry.resize(static_cast<size_t>(m->n_pad) * b * sizeof(double));
+        FE_CHECK_CUDA(cudaMemcpyAsync(m->carry.get(), I.blk[0].as<double>() + m->row0 * b,
+                                      static_cast<size_t>(m->n_pad) * b * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, stream_));
+        m->switched = true;
+        carried = true;
+        done.push_back(m);
+        continue;
+      }
+    }
     if (rc == FE_OK && !converged && m->iterations < m->g.maxiter) {
       // bounds=ritz: damp up to the largest Ritz value of the subspace, capped so the
       // amplification at `lower` stays within the requested one.
@@ -515,6 +586,7 @@ void ChebGroup::finish_cycle(std::vector<GroupMember*>& done) {
         std::chrono::duration<double>(std::chrono::steady_clock::now() - m->t_join).count();
     done.push_back(m);
   }
+  if (carried) FE_CHECK_CUDA(cudaStreamSynchronize(stream_));
   if (keep.size() != members_.size()) {
     members_ = keep;
     I.dirty = true;
@@ -545,16 +617,18 @@ extern "C" int fe_grouped_chebyshev(int32_t count, const fe_csr_t* A, const char
       m.A = &A[p]->m;
       m.want_vectors = eigenvectors && eigenvectors[p];
       fe::chebyshev_group_setup(*m.A, options[p], m.g);
-      fe::ChebGroup* g = nullptr;
-      for (auto& x : groups)
-        if (x->width() == m.g.width && x->degree() == m.g.degree) g = x.get();
-      if (!g) {
-        groups.emplace_back(new fe::ChebGroup(device, m.g.width, m.g.degree));
-        g = groups.back().get();
-      }
-      g->join(&m);
     }
-    std::vector<fe::GroupMember*> done;
+    // one group per (width, degree, filter precision); mixed members start in the
+    // FP32-filter group and move to the FP64 one at their floor
+    auto group_for = [&](const fe::GroupMember& m, bool fp32) {
+      for (auto& x : groups)
+        if (x->width() == m.g.width && x->degree() == m.g.degree && x->fp32_filter() == fp32)
+          return x.get();
+      groups.emplace_back(new fe::ChebGroup(device, m.g.width, m.g.degree, fp32));
+      return groups.back().get();
+    };
+    for (auto& m : members) group_for(m, m.g.mixed)->join(&m);
+    std::vector<fe::GroupMember*> done, moving;
     int64_t cycles = 0, replays = 0, repacks = 0;
     while (true) {
       bool any = false;
@@ -564,7 +638,14 @@ extern "C" int fe_grouped_chebyshev(int32_t count, const fe_csr_t* A, const char
         any = true;
       }
       if (!any) break;
-      for (auto& g : groups) g->finish_cycle(done);
+      moving.clear();
+      for (size_t i = 0; i < groups.size(); ++i) {
+        done.clear();
+        groups[i]->finish_cycle(done);
+        for (fe::GroupMember* m : done)
+          if (m->switched) moving.push_back(m);
+      }
+      for (fe::GroupMember* m : moving) group_for(*m, false)->join(m);
     }
     for (auto& g : groups) {
       cycles += g->cycles;
@@ -594,6 +675,7 @@ extern "C" int fe_grouped_chebyshev(int32_t count, const fe_csr_t* A, const char
         st[7] = static_cast<double>(replays);
         st[8] = static_cast<double>(repacks);
         st[9] = static_cast<double>(m.rc);
+        st[10] = static_cast<double>(m.fp32_iterations);
       }
     }
     if (first_error)

@@ -7,7 +7,10 @@
 // Each member runs the reference's ChebyshevSolver cycle (src/ChebyshevSolver.cpp:
 // 145-205: filter, Cholesky QR, Rayleigh-Ritz, residual check), with the whole
 // subspace filtered every cycle (this backend's soft locking) and the member's
-// width rounded up to a multiple of 32 columns.
+// width rounded up to a multiple of 32 columns. A group filters in FP64 or, for
+// precision=mixed members until their FP32 floor, in FP32 (everything after the
+// filter stays FP64); a mixed member at its floor moves to the FP64 group of its
+// width with its Ritz block.
 #pragma once
 
 #include "device.hpp"
@@ -26,19 +29,22 @@ struct GroupSetup {
   // for bounds=ritz, the cap at the requested amplification
   double reference_cutoff = 0, ritz_cutoff_cap = 0;
   bool ritz_bounds = false, host_init = true;
+  bool mixed = false;          // FP32 filter until the FP32 floor, then FP64
+  double mixed_switch = 4e-6;  // the floor: leave FP32 when the worst residual is below
   unsigned seed = 1;
 };
 
-// Whether a request may run in a group (standard FP64 Chebyshev, soft locking,
-// width <= 512), with its group key (width, degree). With require_flag the option
-// string must also ask for it (group=1).
+// Whether a request may run in a group (standard Chebyshev, FP64 or mixed, soft
+// locking, width <= 512), with its group key (width, degree). With require_flag the
+// option string must also ask for it (group=1).
 bool chebyshev_group_key(const Csr& A, const Csr* B, const char* options, bool require_flag,
-                         int64_t* width, int64_t* degree);
+                         int64_t* width, int64_t* degree, bool* mixed = nullptr);
 // Option checks and the Lanczos spectral bounds of one member (its own stream).
 void chebyshev_group_setup(const Csr& A, const char* options, GroupSetup& g);
 // Device memory one member adds to its group (blocks, operator copy, workspaces),
-// including the transient of a repack.
-size_t group_member_bytes(const Csr& A, int64_t width);
+// including the transient of a repack; `mixed` adds the FP32 filter blocks and the
+// Ritz block carried to the FP64 group.
+size_t group_member_bytes(const Csr& A, int64_t width, bool mixed = false);
 
 struct GroupMember {
   const Csr* A = nullptr;
@@ -47,8 +53,13 @@ struct GroupMember {
   bool want_vectors = false;
   // results, valid once the member left its group
   std::vector<double> eigenvalues, residuals, vectors;  // vectors: column-major n x nev
-  int64_t iterations = 0;
+  int64_t iterations = 0, fp32_iterations = 0;
   bool converged = false;
+  // set when a mixed member leaves its FP32 group at the floor: it is not done and
+  // joins the FP64 group of its width with `carry` (its n_pad x width FP64 Ritz rows)
+  bool switched = false;
+  DeviceBuffer carry;
+  std::vector<double> worst_history;
   int rc = FE_OK;
   std::string error;
   double seconds = 0;
@@ -61,13 +72,14 @@ struct GroupMember {
 
 class ChebGroup {
  public:
-  ChebGroup(int device, int64_t width, int64_t degree);
+  ChebGroup(int device, int64_t width, int64_t degree, bool fp32_filter = false);
   ~ChebGroup();
   ChebGroup(const ChebGroup&) = delete;
   ChebGroup& operator=(const ChebGroup&) = delete;
 
   int64_t width() const { return width_; }
   int64_t degree() const { return degree_; }
+  bool fp32_filter() const { return fp32_; }
   bool empty() const { return members_.empty() && joining_.empty(); }
   size_t size() const { return members_.size() + joining_.size(); }
   cudaStream_t stream() const { return stream_; }
@@ -78,7 +90,8 @@ class ChebGroup {
   // when members joined or left) ...
   void launch_cycle();
   // ... then wait for it and move the members that finished (converged, at
-  // maxiter, or failed) to `done`.
+  // maxiter, or failed) to `done`; in an FP32-filter group, members at their FP32
+  // floor leave to `done` too with `switched` set (not finished).
   void finish_cycle(std::vector<GroupMember*>& done);
   // Device failure of a whole cycle: every member leaves with this error.
   void fail_all(int rc, const std::string& error, std::vector<GroupMember*>& done);
@@ -90,6 +103,7 @@ class ChebGroup {
   std::unique_ptr<Impl> impl_;
   int device_;
   int64_t width_, degree_;
+  bool fp32_;
   cudaStream_t stream_ = nullptr;
   std::vector<GroupMember*> members_, joining_;
   bool launched_ = false;
@@ -108,6 +122,9 @@ void csr_count_bad_diagonals(const Csr& A, int32_t* count, cudaStream_t s);
 void group_rescale(const int32_t* rowptr, const int32_t* colind, const double* plain,
                    double* scaled, int64_t rows, const int32_t* tile_member, const double* cd,
                    cudaStream_t s);
+void group_rescale_f32(const int32_t* rowptr, const int32_t* colind, const double* plain,
+                       float* scaled, int64_t rows, const int32_t* tile_member, const double* cd,
+                       cudaStream_t s);
 // Sum of the Gram partials of each member's chunks into its k x m matrix
 // (column-major, ld k, `stride` doubles apart).
 void group_gram_reduce(const double* partial, int k, int m, int members,

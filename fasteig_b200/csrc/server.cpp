@@ -175,10 +175,12 @@ struct fe_server {
 
   void lane_loop(Lane* L) {
     cudaSetDevice(device);
-    std::unique_ptr<fe::ChebGroup> group;
+    // the lane's groups: [0] FP64 filter, [1] FP32 filter (mixed members until their
+    // FP32 floor, then they move to [0])
+    std::unique_ptr<fe::ChebGroup> groups[2];
     size_t active = 0;
     std::vector<fe::GroupMember*> done;
-    int64_t last_replays = 0, last_repacks = 0;  // this lane's group counters already added
+    int64_t last_replays[2] = {0, 0}, last_repacks[2] = {0, 0};  // counters already added
     while (true) {
       std::vector<Request*> admit;
       {
@@ -211,8 +213,9 @@ struct fe_server {
           r->member.A = r->A;
           r->member.tag = r;
           fe::chebyshev_group_setup(*r->A, r->options.c_str(), r->member.g);
-          if (!group) group.reset(new fe::ChebGroup(device, L->width, L->degree));
-          group->join(&r->member);
+          const int gi = r->member.g.mixed ? 1 : 0;
+          if (!groups[gi]) groups[gi].reset(new fe::ChebGroup(device, L->width, L->degree, gi == 1));
+          groups[gi]->join(&r->member);
         });
         if (rc != FE_OK) {
           finish_request(r, rc, fe_last_error());
@@ -220,29 +223,51 @@ struct fe_server {
         }
         ++active;
       }
-      if (!group || group->empty()) continue;
+      bool any = false;
+      for (auto& g : groups) any = any || (g && !g->empty());
+      if (!any) continue;
       done.clear();
       const int rc = fe::guarded("fe_server grouped cycle", [&] {
+        int64_t members = 0;
+        for (auto& g : groups) {
+          if (!g || g->empty()) continue;
+          members += static_cast<int64_t>(g->size());
+          g->launch_cycle();
+        }
         {
           std::lock_guard<std::mutex> lock(mu);
-          max_group_members = std::max<int64_t>(max_group_members, group->size());
+          max_group_members = std::max<int64_t>(max_group_members, members);
         }
-        group->launch_cycle();
-        group->finish_cycle(done);
+        for (auto& g : groups)
+          if (g) g->finish_cycle(done);
       });
       if (rc != FE_OK) {
         const std::string err = fe_last_error();
-        group->fail_all(rc, err, done);
+        for (auto& g : groups)
+          if (g) g->fail_all(rc, err, done);
       }
       {
         std::lock_guard<std::mutex> lock(mu);
         group_cycles += rc == FE_OK ? 1 : 0;
-        group_replays += group->graph_replays - last_replays;
-        group_repacks += group->repacks - last_repacks;
-        last_replays = group->graph_replays;
-        last_repacks = group->repacks;
+        for (int gi = 0; gi < 2; ++gi) {
+          if (!groups[gi]) continue;
+          group_replays += groups[gi]->graph_replays - last_replays[gi];
+          group_repacks += groups[gi]->repacks - last_repacks[gi];
+          last_replays[gi] = groups[gi]->graph_replays;
+          last_repacks[gi] = groups[gi]->repacks;
+        }
       }
       for (fe::GroupMember* m : done) {
+        if (m->switched && m->rc == FE_OK) {
+          // at its FP32 floor: on to the FP64 group of the lane
+          const int jrc = fe::guarded("fe_server grouped request", [&] {
+            if (!groups[0]) groups[0].reset(new fe::ChebGroup(device, L->width, L->degree, false));
+            groups[0]->join(m);
+          });
+          if (jrc == FE_OK) continue;
+          m->rc = jrc;
+          m->error = fe_last_error();
+        }
         Request* r = static_cast<Request*>(m->tag);
         std::copy(m->eigenvalues.begin(), m->eigenvalues.end(), r->eigenvalues.begin());
         std::copy(m->residuals.begin(), m->residuals.end(), r->residuals.begin());
@@ -250,7 +275,8 @@ struct fe_server {
         r->stats[1] = m->converged ? 0.0 : 1.0;
         r->stats[2] = m->seconds;
         r->stats[3] = static_cast<double>(m->iterations * (L->degree + 1));
-        r->stats[5] = static_cast<double>(m->iterations);
+        r->stats[4] = static_cast<double>(m->fp32_iterations);
+        r->stats[5] = static_cast<double>(m->iterations - m->fp32_iterations);
         r->stats[6] = m->g.lower;
         r->stats[7] = m->g.upper;
         {
@@ -261,8 +287,10 @@ struct fe_server {
         finish_request(r, m->rc, m->error);
       }
       if (rc != FE_OK) {
-        group.reset();  // a fresh group (and stream) for the next members
-        last_replays = last_repacks = 0;
+        for (int gi = 0; gi < 2; ++gi) {  // fresh groups (and streams) for the next members
+          groups[gi].reset();
+          last_replays[gi] = last_repacks[gi] = 0;
+        }
       }
     }
   }
@@ -303,9 +331,10 @@ extern "C" int fe_server_submit(fe_server_t srv, fe_csr_t A, fe_csr_t B, const c
     r->nev = fe::options_nev(r->options.c_str());
     FE_REQUIRE(r->nev >= 1 && r->nev <= A->m.rows, "nev must be in [1, n]");
     int64_t width = 0, degree = 0;
-    const bool grouped =
-        fe::chebyshev_group_key(A->m, r->B, r->options.c_str(), true, &width, &degree);
-    if (grouped) r->bytes = fe::group_member_bytes(A->m, width);
+    bool mixed = false;
+    const bool grouped = fe::chebyshev_group_key(A->m, r->B, r->options.c_str(), true, &width,
+                                                 &degree, &mixed);
+    if (grouped) r->bytes = fe::group_member_bytes(A->m, width, mixed);
     r->eigenvalues.assign(r->nev, 0.0);
     r->residuals.assign(r->nev, 0.0);
     r->stats.assign(12, 0.0);

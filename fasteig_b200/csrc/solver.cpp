@@ -3169,18 +3169,19 @@ static int64_t group_width_of(const Options& opt, int64_t n) {
 }
 
 bool chebyshev_group_key(const Csr& A, const Csr* B, const char* options, bool require_flag,
-                         int64_t* width, int64_t* degree) {
+                         int64_t* width, int64_t* degree, bool* mixed) {
   Options opt;
   opt.parse(options);
   if (require_flag && !opt.group) return false;
   if (opt.solver != "chebyshev" || B != nullptr || A.rows != A.cols) return false;
-  if (opt.precision != "fp64" || opt.locking != "soft") return false;
+  if ((opt.precision != "fp64" && opt.precision != "mixed") || opt.locking != "soft") return false;
   if (opt.which != "sr" && opt.which != "lr") return false;
   if (opt.nev < 1 || opt.nev > A.rows || opt.degree < 1) return false;
   const int64_t w = group_width_of(opt, A.rows);
   if (w > A.rows || w > 512) return false;
   if (width) *width = w;
   if (degree) *degree = opt.degree;
+  if (mixed) *mixed = opt.precision == "mixed";
   return true;
 }
 
@@ -3188,8 +3189,8 @@ void chebyshev_group_setup(const Csr& A, const char* options, GroupSetup& g) {
   Options opt;
   opt.parse(options);
   FE_REQUIRE(chebyshev_group_key(A, nullptr, options, false, nullptr, nullptr),
-             "grouped Chebyshev: request not eligible (standard FP64 Chebyshev with soft "
-             "locking and a width of at most 512 columns)");
+             "grouped Chebyshev: request not eligible (standard FP64 or mixed Chebyshev with "
+             "soft locking and a width of at most 512 columns)");
   FE_REQUIRE(opt.bounds == "reference" || opt.bounds == "ritz", "bounds must be reference or ritz");
   FE_REQUIRE(opt.init == "host" || opt.init == "device", "init must be host or device");
   g.n = A.rows;
@@ -3203,6 +3204,8 @@ void chebyshev_group_setup(const Csr& A, const char* options, GroupSetup& g) {
   g.host_init = opt.init == "host";
   g.ritz_bounds = opt.bounds == "ritz";
   g.amplification = opt.amplification;
+  g.mixed = opt.precision == "mixed";
+  g.mixed_switch = opt.mixed_switch;
   Context ctx;
   {
     // the filter operator c A + d I is written into each row's stored diagonal

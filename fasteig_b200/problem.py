@@ -308,7 +308,7 @@ def batch_krylov_schur(problems, nevs, opts: Optional[fasteig_options] = None,
                      graph_launches=int(stats[3]))
 
 
-GROUP_STATS = 10
+GROUP_STATS = 11
 
 
 def grouped_chebyshev(problems, opts, want_vectors: bool = False):
@@ -352,7 +352,8 @@ def grouped_chebyshev(problems, opts, want_vectors: bool = False):
         ev = vecs[i].reshape(o.nev(), p.rows).T if want_vectors else None
         out.append(dict(eigenvalues=vals[i], residual_norms=res[i], eigenvectors=ev,
                         iterations=int(st[0]), status=int(st[1]), seconds=float(st[2]),
-                        width=int(st[3]), lower=float(st[4]), upper=float(st[5])))
+                        width=int(st[3]), lower=float(st[4]), upper=float(st[5]),
+                        fp32_iterations=int(st[10])))
     st = stats[:GROUP_STATS]
     return out, dict(cycles=int(st[6]), graph_replays=int(st[7]), repacks=int(st[8]))
 

@@ -391,17 +391,21 @@ int fe_batch_krylov_schur(int32_t count, const fe_csr_t* A, const int64_t* nev,
  * Cholesky QR and Rayleigh-Ritz in grouped kernels over the concatenated
  * block-diagonal operator (one CUDA graph per cycle once membership is
  * stable), and members leave as they converge. Eligible problems: solver
- * Chebyshev, precision fp64, locking soft, which SR or LR, width <= 512, one
- * stored diagonal entry per row. Each problem's arithmetic reads only its own
- * rows, so its result does not depend on the rest of the batch.
+ * Chebyshev, precision fp64 or mixed, locking soft, which SR or LR, width <=
+ * 512, one stored diagonal entry per row. Mixed problems filter in FP32 (the
+ * rest of each cycle in FP64) in the FP32-filter group of their width until
+ * their residuals reach the FP32 floor (mixed_switch) or stall, then continue in
+ * the FP64 group. Each problem's arithmetic reads only its own rows, so its
+ * result does not depend on the rest of the batch.
  * Results per problem: eigenvalues[p][nev_p], residual_norms[p][nev_p] (the
  * reference's relative residual), eigenvectors[p] (n_p-by-nev_p column-major;
  * the array or any entry may be NULL), stats[count * FE_GROUP_STATS] (may be
  * NULL): cycles, status (0 converged, 1 at maxiter), seconds in the group,
  * width, spectral lower and upper bounds, then the batch's total group cycles,
- * graph replays and repacks, and the problem's status code.
+ * graph replays and repacks, the problem's status code, and its FP32-filter
+ * cycles.
  * ------------------------------------------------------------------- */
-#define FE_GROUP_STATS 10
+#define FE_GROUP_STATS 11
 int fe_grouped_chebyshev(int32_t count, const fe_csr_t* A, const char* const* options,
                          double* const* eigenvalues, double* const* residual_norms,
                          double* const* eigenvectors, double* stats);

@@ -109,7 +109,7 @@ def test_grouped_rejects_ineligible():
     from fasteig_b200 import FastEigError, grouped_chebyshev
     H = problem(10, "star1", 41)
     with pytest.raises(FastEigError, match="not eligible"):
-        grouped_chebyshev([csr(H)], [opts(H.n, 8, precision="mixed")])
+        grouped_chebyshev([csr(H)], [opts(H.n, 8, locking="hard")])
 
 
 @pytest.mark.parametrize("k", [1, 7, 32, 64, 96, 128])
@@ -148,3 +148,28 @@ def test_chol_inv_batched(k):
         ref = np.linalg.inv(R)
         assert np.allclose(np.tril(Rinv, -1), 0.0)
         assert np.abs(Rinv - ref).max() <= 1e-12 * np.abs(ref).max() * k
+
+
+def test_grouped_mixed_precision():
+    """precision=mixed members filter in FP32 in the FP32-filter group of their width,
+    move to the FP64 group at their floor, and end with the FP64 path's pairs (tol
+    1e-8 and 1e-6); alone and in a same-stencil group the results are bit-identical."""
+    from fasteig_b200 import grouped_chebyshev
+    specs = [(12, "star1", 8, 1e-8), (13, "star1", 12, 1e-8), (11, "star1", 10, 1e-6),
+             (12, "star2", 20, 1e-8)]
+    Hs = [problem(s, st, 60 + i) for i, (s, st, _, _) in enumerate(specs)]
+    mats = [csr(H) for H in Hs]
+    o = [opts(H.n, nev, tol=tol, precision="mixed") for H, (_, _, nev, tol) in zip(Hs, specs)]
+    out, batch = grouped_chebyshev(mats, o)
+    for H, (_, _, nev, tol), r in zip(Hs, specs, out):
+        assert r["status"] == 0
+        assert np.all(r["residual_norms"] <= tol)
+        assert r["fp32_iterations"] >= 1
+        lam = r["eigenvalues"]
+        ref = np.linalg.eigvalsh(dense(H))[:nev]
+        bound = tol * (1.0 + np.abs(lam)) * 1.01 + 1e-12
+        assert np.all(np.abs(lam - ref) <= bound)
+    assert any(r["iterations"] > r["fp32_iterations"] for r in out)  # some FP64 cycles ran
+    alone, _ = grouped_chebyshev(mats[:1], o[:1])
+    assert np.array_equal(alone[0]["eigenvalues"], out[0]["eigenvalues"])
+    assert alone[0]["iterations"] == out[0]["iterations"]

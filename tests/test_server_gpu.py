@@ -116,12 +116,18 @@ def test_server_grouped_lanes():
         assert o.set("group", 1)
         return o
 
-    alone = [grouped_chebyshev([A], [gopts(H, nev)])[0][0]
-             for H, A, (_, _, nev) in zip(Hs, mats, specs)]
+    def gopts_any(k, H, nev):
+        o = gopts(H, nev)
+        if k % 2 == 1:
+            assert o.set("precision", "mixed")  # FP32-filter group, then the FP64 one
+        return o
+
+    gopts_k = [gopts_any(k, H, nev) for k, (H, (_, _, nev)) in enumerate(zip(Hs, specs))]
+    alone = [grouped_chebyshev([A], [o])[0][0] for A, o in zip(mats, gopts_k)]
     lob = requests()[1]
     lob_A = CsrMatrix(lob[0].n, lob[0].rowptr, lob[0].colind, lob[0].values)
     with Server(slots=2) as srv:
-        ids = [srv.submit(A, gopts(H, nev)) for H, A, (_, _, nev) in zip(Hs, mats, specs)]
+        ids = [srv.submit(A, o) for A, o in zip(mats, gopts_k)]
         lid = srv.submit(lob_A, options("LOBPCG", lob[2], lob[3], lob[0].n))
         results = [srv.wait(i) for i in ids]
         lres = srv.wait(lid)
