@@ -8,7 +8,8 @@
 //      the concatenated values (c_p, d_p from the member's bounds and cutoff);
 //   2. the filter recurrence Y_1 = (cA + dI) X, Y_k = 2 (cA + dI) Y_{k-1} - Y_{k-2}
 //      (src/ChebyshevSolver.cpp:231-256): `degree` SpMMs over the concatenated
-//      operator, every member's rows in each launch;
+//      operator, every member's rows in each launch (an FP32-filter group runs them on
+//      FP32 copies of X and of the scaled values and widens the result to FP64);
 //   3. Cholesky QR, twice (thin_qr_in_place with QrMethod::Cholesky): grouped Gram
 //      (each member's rows in its own chunks), batched Cholesky and triangular
 //      inverse, grouped rotation (each row tile with its member's R^-1);
