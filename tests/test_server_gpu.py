@@ -147,3 +147,21 @@ def test_server_grouped_lanes():
                                        atol=1e-12)
     spans = sorted((r["start_s"], r["end_s"]) for r in results)
     assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
+
+
+def test_server_destroy_with_queued_grouped_requests():
+    """Destroying a server while grouped-lane requests wait (a 1-byte budget admits one
+    request at a time) drops the queued ones and returns once the running one is done."""
+    import time
+    from fasteig_b200 import CsrMatrix, Server
+    from fasteig_b200 import matrices as M
+    Hs = [M.laplacian_wells(11 + i, wells=4, seed=80 + i) for i in range(4)]
+    mats = [CsrMatrix(H.n, H.rowptr, H.colind, H.values) for H in Hs]
+    srv = Server(slots=1, memory_budget_bytes=1)
+    for H, A in zip(Hs, mats):
+        o = options("Chebyshev", 8, 1e-8, H.n)
+        assert o.set("group", 1)
+        srv.submit(A, o)
+    t0 = time.perf_counter()
+    srv.close()
+    assert time.perf_counter() - t0 < 60.0
