@@ -30,6 +30,7 @@
 
 #include "device.hpp"
 #include "grouped.hpp"
+#include "tridiag.hpp"
 
 namespace fe {
 namespace {
@@ -54,6 +55,7 @@ struct Options {
   bool has_seed = false;
   unsigned seed = 1;
   int verbosity = 0;
+  int64_t print_every = 0;  // LanczosSolver: convergence checked every print_every steps (0: 5)
   // extensions
   std::string precision = "fp64";  // fp64 | mixed
   int64_t block = 0;               // Chebyshev subspace capacity override (0 = reference rule)
@@ -171,8 +173,9 @@ struct Options {
       if (precond != "none" && precond != "jacobi")
         throw Error(FE_ERR_INVALID, "precond must be none or jacobi");
     }
-    else if (k == "print_every" || k == "logfile" || k == "output_format" || k == "gpu_backend" ||
-             k == "shift" || k == "n") {
+    else if (k == "print_every") print_every = as_int(v);
+    else if (k == "logfile" || k == "output_format" || k == "gpu_backend" || k == "shift" ||
+             k == "n") {
       // accepted for deck compatibility; no effect on this backend
     } else {
       throw Error(FE_ERR_INVALID, "unknown option: " + k);
@@ -2175,43 +2178,53 @@ struct MassSolver {
 // src/core/KrylovSubspace.cpp:162-178; Gram-Schmidt weighted by BV), converged pairs are
 // verified by their true residual ||A y - l B y|| / ((1+|l|) ||B y||) and the status is 1
 // when they are not (src/KrylovSchurSolver.cpp:136-140).
-void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* eigenvalues,
-                        double* residuals, double* eigenvectors, Stats& st) {
-  const int64_t n = A.rows, nev = opt.nev;
-  if (n <= 0) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: n must be > 0.");
-  if (nev <= 0 || nev > n) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: nev must be in [1,n].");
-  if (opt.maxiter <= 0) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: maxiter must be > 0.");
-  const std::string which = opt.which;
-  if (which == "sai")
-    throw Error(FE_ERR_UNSUPPORTED,
-                "KrylovSchurSolver: SAI needs a shift-invert factorization (out of scope here).");
-  if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
-    throw Error(FE_ERR_INVALID, "KrylovSchurSolver: invalid which option (use SR/LR/SM/LM/BE/SAI).");
-  const double tol = opt.tol;
-  const int64_t m = std::min<int64_t>(std::max<int64_t>({2 * nev, 20, opt.maxdim}), n);
-  const unsigned seed = opt.seed_or_default();
-  const bool host_init = opt.init == "host";
-  Context ctx;
-  cudaStream_t s = ctx.stream;
-  SmallState sm;
-  sm.allocate(n, m, false);
-  Block<double> V, Y, BV;
-  V.allocate(n, m);
-  Y.allocate(n, m);
-  if (B) BV.allocate(n, m);
-  const int64_t ld = V.ld;
-  DeviceBuffer f(n * sizeof(double)), w(n * sizeof(double)), h(m * sizeof(double)),
-      hs(m * sizeof(double)), nrm(sizeof(double)), C(static_cast<size_t>(m) * m * sizeof(double));
-  DeviceBuffer bf, aw;
+// Scalar Lanczos recurrence of KrylovSubspace::build_one (src/core/KrylovSubspace.cpp:
+// 125-259) on the device: basis V (n x cap, and BV = B V in the B metric), residual f,
+// two-pass classical Gram-Schmidt, a fresh seeded random vector on breakdown
+// (restart_residual, :251-259), and the projected tridiagonal T (column-major, on the
+// host) that the Krylov-Schur and plain Lanczos drivers diagonalize. In the generalized
+// case the operator is B^-1 A with B^-1 applied by conjugate gradients (MassSolver).
+struct ScalarLanczos {
+  Context& ctx;
+  const Csr& A;
+  const Csr* B;
+  int64_t n, cap;
+  unsigned seed;
+  bool host_init;
+  Stats& st;
+  cudaStream_t s;
+  Block<double> V, BV;
+  int64_t ld = 0;
+  DeviceBuffer f, w, h, hs, nrm, bf, aw, gws, rws;
   std::unique_ptr<MassSolver> mass;
-  if (B) {
-    bf.resize(n * sizeof(double));
-    aw.resize(n * sizeof(double));
-    mass.reset(new MassSolver(ctx, *B));
+  std::vector<double> T;
+  double beta_next = 0.0;
+  int64_t restart_row = -1;
+
+  ScalarLanczos(Context& c, const Csr& A_, const Csr* B_, int64_t cap_, unsigned seed_,
+                bool host_init_, Stats& st_)
+      : ctx(c), A(A_), B(B_), n(A_.rows), cap(cap_), seed(seed_), host_init(host_init_), st(st_),
+        s(c.stream) {
+    V.allocate(n, cap);
+    if (B) BV.allocate(n, cap);
+    ld = V.ld;
+    f.resize(n * sizeof(double));
+    w.resize(n * sizeof(double));
+    h.resize(cap * sizeof(double));
+    hs.resize(cap * sizeof(double));
+    nrm.resize(sizeof(double));
+    if (B) {
+      bf.resize(n * sizeof(double));
+      aw.resize(n * sizeof(double));
+      mass.reset(new MassSolver(ctx, *B));
+    }
+    gws.resize(std::max<size_t>(gram_workspace_bytes(n, cap, 1), 64));
+    rws.resize(std::max<size_t>(residual_workspace_bytes(n, cap), 64));
+    T.assign(static_cast<size_t>(cap) * cap, 0.0);
+    random_into(f.as<double>(), seed);
   }
-  DeviceBuffer gws(std::max<size_t>(gram_workspace_bytes(n, m, 1), 64));
-  DeviceBuffer rws(std::max<size_t>(residual_workspace_bytes(n, m), 64));
-  auto random_into = [&](double* dst, unsigned sd) {
+  double& t(int64_t r, int64_t c) { return T[static_cast<size_t>(c) * cap + r]; }
+  void random_into(double* dst, unsigned sd) {
     if (host_init) {
       std::mt19937 rng(sd);
       std::uniform_real_distribution<double> dist(-1.0, 1.0);
@@ -2221,9 +2234,9 @@ void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* 
     } else {
       fill_uniform<double>(dst, 1, n, 1, sd, s);
     }
-  };
+  }
   // ||x|| (standard) or the B-norm sqrt(x . Bx) with Bx kept in bf (generalized).
-  auto norm = [&](const double* x) {
+  double norm(const double* x) {
     if (B) {
       csr_spmm<double>(*B, x, 1, bf.as<double>(), 1, nullptr, 0, 1, 1.0, 0.0, 0.0, s);
       st.spmm_launches += 1;
@@ -2237,10 +2250,10 @@ void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* 
     ctx.to_host(&r, nrm.as<double>(), 1);
     ctx.sync();
     return r;
-  };
+  }
   // f = src - V_k (W_k^T src), twice (W = BV with B, else V); returns the last coefficient.
-  const double* W = B ? BV.data() : V.data();
-  auto orthogonalize = [&](int64_t k, const double* src) {
+  double orthogonalize(int64_t k, const double* src) {
+    const double* W = B ? BV.data() : V.data();
     vec_axpby(n, 1.0, src, 1, 0.0, f.as<double>(), 1, s);
     if (k == 0) return 0.0;
     gram<double>(W, ld, f.as<double>(), 1, n, k, 1, h.as<double>(), k, gws.get(), gws.bytes(), s);
@@ -2253,14 +2266,11 @@ void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* 
     ctx.to_host(&b, hs.as<double>() + k - 1, 1);
     ctx.sync();
     return a + b;
-  };
-  std::vector<double> T(static_cast<size_t>(m) * m, 0.0);
-  auto t = [&](int64_t r, int64_t c) -> double& { return T[static_cast<size_t>(c) * m + r]; };
-  double beta_next = 0.0;
-  int64_t restart_row = -1;
-  random_into(f.as<double>(), seed);
-  auto expand = [&](int64_t begin) {
-    for (int64_t col = begin; col < m; ++col) {
+  }
+  // Basis columns [begin, end): normalize the residual into V[:, col], apply the
+  // operator, orthogonalize, record alpha and beta in T.
+  void expand(int64_t begin, int64_t end) {
+    for (int64_t col = begin; col < end; ++col) {
       bool restarted = false;
       double beta = norm(f.as<double>());
       if (!std::isfinite(beta))
@@ -2296,8 +2306,153 @@ void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* 
       t(col, col) = alpha;
       if (col == restart_row) restart_row = -1;
     }
+  }
+};
+
+// LanczosSolver::solve (src/LanczosSolver.cpp:29-163): one scalar Lanczos chain of up to
+// maxiter basis vectors with full two-pass reorthogonalization and no restart. From nev
+// vectors on, every check_every-th step (print_every, else 5) and at maxiter, the
+// projected tridiagonal is diagonalized and the chain stops when the nev wanted Ritz
+// pairs' estimates |beta_m z_{m-1,j}| / (1 + |theta_j|) are all below tol (in the B
+// metric the formed pairs must also pass their true residual check, and a chain that
+// broke down keeps going to recover multiplicity). The returned pairs are formed from
+// the basis on the device and their residuals recomputed (evaluate_ritz_pairs).
+void lanczos_solve(const Csr& A, const Csr* B, const Options& opt, double* eigenvalues,
+                   double* residuals, double* eigenvectors, Stats& st) {
+  const int64_t n = A.rows, nev = opt.nev, maxiter = opt.maxiter;
+  if (maxiter <= 0) throw Error(FE_ERR_INVALID, "LanczosSolver: maxiter must be > 0.");
+  if (nev <= 0) throw Error(FE_ERR_INVALID, "LanczosSolver: nev must be > 0.");
+  if (maxiter < nev) throw Error(FE_ERR_INVALID, "LanczosSolver: maxiter must be >= nev.");
+  if (maxiter > n) throw Error(FE_ERR_INVALID, "LanczosSolver: maxiter must be <= n.");
+  const std::string which = opt.which;
+  if (which == "sai")
+    throw Error(FE_ERR_UNSUPPORTED,
+                "LanczosSolver: SAI needs a shift-invert factorization (out of scope here).");
+  if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
+    throw Error(FE_ERR_INVALID, "LanczosSolver: invalid which option (use SR/LR/SM/LM/BE/SAI).");
+  const double tol = opt.tol;
+  const int64_t check_every = opt.print_every > 0 ? opt.print_every : 5;
+  Context ctx;
+  cudaStream_t s = ctx.stream;
+  SmallState sm;
+  sm.allocate(n, nev, false);
+  ScalarLanczos lz(ctx, A, B, maxiter, opt.seed_or_default(), opt.init == "host", st);
+  Block<double> Y;
+  Y.allocate(n, nev);
+  DeviceBuffer C(static_cast<size_t>(maxiter) * nev * sizeof(double));
+  // Ritz values (wanted order), their estimates, and the selected eigenvectors of T_m:
+  // the projected matrix is tridiagonal, so only the eigenvalues the selection can
+  // need are found (bisection) and only the wanted vectors (inverse iteration).
+  std::vector<double> lam_s, rel_s, Cs;
+  auto snapshot = [&](int64_t m) {
+    std::vector<double> dd(m), ee(m > 1 ? m - 1 : 0);
+    for (int64_t i = 0; i < m; ++i) dd[i] = lz.t(i, i);
+    for (int64_t i = 0; i + 1 < m; ++i) ee[i] = lz.t(i + 1, i);
+    TridiagEig tr(dd, ee, static_cast<int>(m));
+    const std::vector<int> cand =
+        tridiag_candidates(tr, static_cast<int>(nev), which.c_str());
+    std::vector<double> cw(cand.size());
+    for (size_t c = 0; c < cand.size(); ++c) cw[c] = tr.eigenvalue(cand[c]);
+    const std::vector<int32_t> order = select_indices(cw, which);
+    const int64_t k = std::min(nev, m);
+    lam_s.assign(k, 0.0);
+    rel_s.assign(k, 0.0);
+    Cs.assign(static_cast<size_t>(m) * k, 0.0);
+    std::vector<std::vector<double>> vecs(k);
+    for (int64_t j = 0; j < k; ++j) {
+      const double theta = cw[order[j]];
+      std::vector<const std::vector<double>*> cluster;
+      for (int64_t i = 0; i < j; ++i)
+        if (std::fabs(lam_s[i] - theta) <= 1e-3 * tr.tnorm) cluster.push_back(&vecs[i]);
+      vecs[j] = tr.vector(theta, static_cast<unsigned>(j), cluster);
+      lam_s[j] = theta;
+      rel_s[j] = std::fabs(lz.beta_next * vecs[j][m - 1]) / (1.0 + std::fabs(theta));
+      std::copy(vecs[j].begin(), vecs[j].end(), Cs.begin() + static_cast<size_t>(j) * m);
+    }
   };
-  expand(0);
+  // evaluate_ritz_pairs: Y = V[:, :m] Csel, residuals of the formed pairs
+  std::vector<double> vals(nev), res(nev), vecs;
+  auto form = [&](int64_t m) {
+    ctx.to_device(C.as<double>(), Cs.data(), Cs.size());
+    rotate<double>(lz.V.data(), lz.ld, C.as<double>(), m, Y.data(), Y.ld, n, m, nev, 1.0, 0.0,
+                   s);
+    std::copy(lam_s.begin(), lam_s.end(), vals.begin());
+    if (eigenvectors) vecs.resize(static_cast<size_t>(n) * nev);
+    finish_results(ctx, sm, A, B, Y.data(), Y.ld, n, nev, vals.data(), res.data(),
+                   eigenvectors ? vecs.data() : nullptr);
+    bool ok = true;
+    for (double r : res) ok = ok && r <= tol;
+    return ok;
+  };
+  bool breakdown = false, converged = false, formed = false, verified = false;
+  int64_t it_stop = maxiter;
+  for (int64_t it = 0; it < maxiter; ++it) {
+    lz.expand(it, it + 1);
+    const double alpha = lz.t(it, it);
+    const double beta = it > 0 ? lz.t(it, it - 1) : 0.0;
+    breakdown = breakdown || lz.beta_next <= 64.0 * std::numeric_limits<double>::epsilon() *
+                                                 std::max({1.0, std::fabs(alpha), std::fabs(beta)});
+    const int64_t m = it + 1;
+    const bool do_check = m >= nev && (m % check_every == 0 || m == maxiter);
+    if (!do_check) continue;
+    const bool resolve_multiplicity = B && breakdown && m < maxiter;
+    snapshot(m);
+    double worst = 0.0;
+    for (double r : rel_s) worst = std::max(worst, r);
+    if (opt.verbosity >= 2)
+      std::fprintf(stderr, "[fe] lanczos step %lld worst estimate %.3e\n",
+                   static_cast<long long>(m), worst);
+    if (!resolve_multiplicity && worst < tol) {
+      if (B) {
+        verified = form(m);
+        formed = true;
+        if (!verified) continue;
+      }
+      converged = true;
+      it_stop = m;
+      break;
+    }
+  }
+  if (!converged) snapshot(maxiter);
+  if (!formed || !converged) verified = form(it_stop);
+  for (int64_t j = 0; j < nev; ++j) {
+    eigenvalues[j] = vals[j];
+    residuals[j] = res[j];
+  }
+  if (eigenvectors) std::memcpy(eigenvectors, vecs.data(), vecs.size() * sizeof(double));
+  st.status = (B && !verified) ? 1 : 0;
+  st.iterations = static_cast<double>(it_stop);
+  st.fp64_iterations = st.iterations;
+}
+
+void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* eigenvalues,
+                        double* residuals, double* eigenvectors, Stats& st) {
+  const int64_t n = A.rows, nev = opt.nev;
+  if (n <= 0) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: n must be > 0.");
+  if (nev <= 0 || nev > n) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: nev must be in [1,n].");
+  if (opt.maxiter <= 0) throw Error(FE_ERR_INVALID, "KrylovSchurSolver: maxiter must be > 0.");
+  const std::string which = opt.which;
+  if (which == "sai")
+    throw Error(FE_ERR_UNSUPPORTED,
+                "KrylovSchurSolver: SAI needs a shift-invert factorization (out of scope here).");
+  if (which != "sr" && which != "lr" && which != "sm" && which != "lm" && which != "be")
+    throw Error(FE_ERR_INVALID, "KrylovSchurSolver: invalid which option (use SR/LR/SM/LM/BE/SAI).");
+  const double tol = opt.tol;
+  const int64_t m = std::min<int64_t>(std::max<int64_t>({2 * nev, 20, opt.maxdim}), n);
+  Context ctx;
+  cudaStream_t s = ctx.stream;
+  SmallState sm;
+  sm.allocate(n, m, false);
+  ScalarLanczos lz(ctx, A, B, m, opt.seed_or_default(), opt.init == "host", st);
+  Block<double>& V = lz.V;
+  Block<double>& BV = lz.BV;
+  Block<double> Y;
+  Y.allocate(n, m);
+  const int64_t ld = lz.ld;
+  DeviceBuffer C(static_cast<size_t>(m) * m * sizeof(double));
+  std::vector<double>& T = lz.T;
+  auto t = [&](int64_t r, int64_t c) -> double& { return lz.t(r, c); };
+  lz.expand(0, m);
   std::unique_ptr<ProjectedEig> deig;
   DeviceBuffer Td;
   if (m > 96) {  // large projected matrices: the device eigensolver
@@ -2321,7 +2476,7 @@ void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* 
     std::vector<double> lam_s(m), rel_s(m);
     for (int64_t j = 0; j < m; ++j) {
       lam_s[j] = lam[idx[j]];
-      rel_s[j] = std::fabs(beta_next * Z[static_cast<size_t>(idx[j]) * m + m - 1]) /
+      rel_s[j] = std::fabs(lz.beta_next * Z[static_cast<size_t>(idx[j]) * m + m - 1]) /
                  (1.0 + std::fabs(lam_s[j]));
     }
     int64_t nconv = 0;
@@ -2382,12 +2537,12 @@ void krylov_schur_solve(const Csr& A, const Csr* B, const Options& opt, double* 
     std::fill(T.begin(), T.end(), 0.0);
     for (int64_t j = 0; j < retained; ++j) {
       t(j, j) = lam_s[j];
-      const double coupling = beta_next * Z[static_cast<size_t>(idx[j]) * m + m - 1];
+      const double coupling = lz.beta_next * Z[static_cast<size_t>(idx[j]) * m + m - 1];
       t(retained, j) = coupling;
       t(j, retained) = coupling;
     }
-    restart_row = retained;
-    expand(retained);
+    lz.restart_row = retained;
+    lz.expand(retained, m);
   }
   throw Error(FE_ERR_INVALID, "KrylovSchurSolver: unreachable solve termination.");
 }
@@ -3125,6 +3280,9 @@ void solve_problem(const Csr& A, const Csr* B, const char* options, double* eige
   } else if (opt.solver == "krylovschur") {
     if (B) check_pair(A, *B);
     krylov_schur_solve(A, B, opt, eigenvalues, residual_norms, eigenvectors, st);
+  } else if (opt.solver == "lanczos") {
+    if (B) check_pair(A, *B);
+    lanczos_solve(A, B, opt, eigenvalues, residual_norms, eigenvectors, st);
   } else {
     throw Error(FE_ERR_UNSUPPORTED, "solver not available on this backend: " + opt.solver);
   }

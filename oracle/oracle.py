@@ -940,6 +940,59 @@ def krylov_schur_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
     raise RuntimeError("KrylovSchurSolver: unreachable solve termination.")
 
 
+def lanczos_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
+                  which: str = "sr", seed: int = 1, print_every: int = 0,
+                  B: Optional[Csr] = None) -> SolveResult:
+    """LanczosSolver::solve (src/LanczosSolver.cpp:29-163): one scalar Lanczos chain of up
+    to maxiter vectors, no restart; from nev vectors on, every check_every-th step
+    (print_every, else 5) and at maxiter the projected tridiagonal is diagonalized and
+    the chain stops when every wanted estimate |beta_m z_{m-1,j}| / (1 + |theta_j|) is
+    below tol (B metric: the formed pairs must pass their residual check too, and a
+    chain that broke down keeps going to recover multiplicity). Generalized problems
+    use the B^-1 A operator of krylov_schur_solve."""
+    n = A.rows
+    which = which.lower()
+    if maxiter <= 0:
+        raise ValueError("LanczosSolver: maxiter must be > 0.")
+    if nev <= 0:
+        raise ValueError("LanczosSolver: nev must be > 0.")
+    if maxiter < nev:
+        raise ValueError("LanczosSolver: maxiter must be >= nev.")
+    if maxiter > n:
+        raise ValueError("LanczosSolver: maxiter must be <= n.")
+    Hs = A.scipy()
+    if B is None:
+        A_apply, B_apply = (lambda v: Hs @ v), None
+    else:
+        import scipy.sparse.linalg as spla
+        lu = spla.splu(B.scipy().tocsc())
+        Bs = B.scipy()
+        A_apply = (lambda v: lu.solve(Hs @ v))
+        B_apply = (lambda v: Bs @ v)
+    lz = _Lanczos(A_apply, random_vector(n, seed), maxiter, seed, B_apply)
+    check_every = print_every if print_every > 0 else 5
+    breakdown = False
+    for it in range(maxiter):
+        beta_prev = lz.T[it, it - 1] if it > 0 else 0.0
+        lz.step(it)
+        alpha = lz.T[it, it]
+        breakdown = breakdown or lz.beta_next <= 64.0 * EPS * max(1.0, abs(alpha), abs(beta_prev))
+        m = it + 1
+        if not (m >= nev and (m % check_every == 0 or m == maxiter)):
+            continue
+        resolve_multiplicity = B is not None and breakdown and m < maxiter
+        lam, rel, C = lz.snapshot(m, nev, which)
+        if not resolve_multiplicity and rel.max() < tol:
+            Y, res = evaluate_ritz_pairs(A, B, lz.V, m, lam, C)
+            if B is not None and not np.all(res <= tol):
+                continue
+            return SolveResult(lam.copy(), Y, res, m, 0)
+    lam, rel, C = lz.snapshot(maxiter, nev, which)
+    Y, res = evaluate_ritz_pairs(A, B, lz.V, maxiter, lam, C)
+    status = 1 if (B is not None and not np.all(res <= tol)) else 0
+    return SolveResult(lam.copy(), Y, res, maxiter, status)
+
+
 def _cgs2(V: np.ndarray, k: int, src: np.ndarray) -> np.ndarray:
     """Two-pass classical Gram-Schmidt of one vector against V[:, :k]
     (CpuMultiVector::orthogonalize_active_columns, src/core/MultiVector.cpp:153-185)."""
