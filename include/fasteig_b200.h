@@ -330,13 +330,14 @@ int fe_convert_f32_to_f64(const float* src, int64_t lds, double* dst, int64_t ld
                           int64_t n, int64_t m, void* stream);
 
 /* ---------------------------------------------------------------------
- * Solver entry point (replaces fasteig_problem::solve for the Chebyshev,
- * LOBPCG, Davidson and Krylov-Schur solvers on the CUDA executor,
- * src/fasteig_problem.cpp:340-437, src/fasteig_solver.cpp:131-168).
+ * Solver entry point (replaces fasteig_problem::solve for the Lanczos,
+ * Chebyshev, LOBPCG, Davidson, Krylov-Schur and block Krylov-Schur solvers on the
+ * CUDA executor, src/fasteig_problem.cpp:340-437, src/fasteig_solver.cpp:131-168).
  * The problem is given as host CSR (full symmetric storage, as
  * build_csr_from_sparse_matrix produces) and options as "key=value" lines
  * with the reference's keys (src/fasteig_options.cpp:51-112: nev, maxiter,
- * maxdim, maxblks, degree, which, solver, tol, seed, blksize) plus
+ * maxdim, maxblks, degree, which, solver, tol, seed, blksize, print_every:
+ * the Lanczos convergence-check interval) plus
  * extensions (precision=fp64|mixed, block=<cols>, bounds=reference|ritz,
  * precond=none|jacobi, init=host|device, mixed_switch=<FP32 floor>,
  * locking=soft|hard: Chebyshev soft locking is the reference's, hard locking
