@@ -187,6 +187,8 @@ void ChebGroup::fail_all(int rc, const std::string& error, std::vector<GroupMemb
     for (GroupMember* m : *list) {
       m->rc = rc;
       m->error = error;
+      m->switched = false;
+      m->carry.release();  // while the stream it was allocated on still exists
       m->seconds =
           std::chrono::duration<double>(std::chrono::steady_clock::now() - m->t_join).count();
       done.push_back(m);
@@ -609,8 +611,9 @@ extern "C" int fe_grouped_chebyshev(int32_t count, const fe_csr_t* A, const char
                "null or empty batch");
     const int device = A[0] ? A[0]->m.device : 0;
     FE_CHECK_CUDA(cudaSetDevice(device));
-    std::vector<fe::GroupMember> members(count);
+    // groups before members: a member's carried block is freed on its group's stream
     std::vector<std::unique_ptr<fe::ChebGroup>> groups;
+    std::vector<fe::GroupMember> members(count);
     for (int32_t p = 0; p < count; ++p) {
       FE_REQUIRE(A[p] && A[p]->m.device == device, "null CSR handle or operator on another device");
       FE_REQUIRE(eigenvalues[p] && residual_norms[p], "null result arrays");

@@ -241,10 +241,11 @@ struct fe_server {
         for (auto& g : groups)
           if (g) g->finish_cycle(done);
       });
+      std::string cycle_error;
       if (rc != FE_OK) {
-        const std::string err = fe_last_error();
+        cycle_error = fe_last_error();
         for (auto& g : groups)
-          if (g) g->fail_all(rc, err, done);
+          if (g) g->fail_all(rc, cycle_error, done);
       }
       {
         std::lock_guard<std::mutex> lock(mu);
@@ -258,7 +259,7 @@ struct fe_server {
         }
       }
       for (fe::GroupMember* m : done) {
-        if (m->switched && m->rc == FE_OK) {
+        if (m->switched && m->rc == FE_OK && rc == FE_OK) {
           // at its FP32 floor: on to the FP64 group of the lane
           const int jrc = fe::guarded("fe_server grouped request", [&] {
             if (!groups[0]) groups[0].reset(new fe::ChebGroup(device, L->width, L->degree, false));
@@ -267,7 +268,13 @@ struct fe_server {
           if (jrc == FE_OK) continue;
           m->rc = jrc;
           m->error = fe_last_error();
+        } else if (m->switched) {
+          // moved out of its FP32 group in a cycle that failed in the other group
+          m->rc = rc != FE_OK ? rc : m->rc;
+          m->error = cycle_error;
         }
+        m->switched = false;
+        m->carry.release();
         Request* r = static_cast<Request*>(m->tag);
         std::copy(m->eigenvalues.begin(), m->eigenvalues.end(), r->eigenvalues.begin());
         std::copy(m->residuals.begin(), m->residuals.end(), r->residuals.begin());
