@@ -592,6 +592,59 @@ def chebyshev_filter_window(H_apply, X: np.ndarray, degree: int, cutoff: float,
     return cur
 
 
+def grouped_chebyshev_member(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
+                             maxiter: int = 1000, which: str = "sr", seed: int = 1,
+                             block: Optional[int] = None, bounds: str = "reference",
+                             amplification: float = 1e3) -> SolveResult:
+    """One member of the grouped Chebyshev engine (an extension; each member runs the
+    cycle of ChebyshevSolver::solve, src/ChebyshevSolver.cpp:145-205): a subspace of the
+    solve's capacity (nev + min(nev, n - nev), or block) rounded up to a multiple of 32
+    columns, started from the reference's seeded random block and filtered whole every
+    cycle (no initial QR, no locking); the reference's filter on its Lanczos bounds
+    (bounds=reference) or damped to the largest Ritz value of the subspace, capped at the
+    requested amplification (bounds=ritz); Cholesky QR twice; Rayleigh-Ritz with
+    W = A Y; the reference's relative residuals; done when the first nev are <= tol or at
+    maxiter. FP64 (the engine's FP64 groups)."""
+    n = A.rows
+    which = which.lower()
+    if which not in ("sr", "lr"):
+        raise ValueError("grouped Chebyshev: only SR and LR are supported.")
+    sign = -1.0 if which == "lr" else 1.0
+    cap = nev + min(nev, n - nev) if not block else max(nev, min(block, n))
+    width = (cap + 31) // 32 * 32
+    if width > n:
+        raise ValueError("grouped Chebyshev: width exceeds n")
+    ops = NumpyChebyshevOps(A, sign)
+    lower, upper = estimate_bounds(ops.apply, n, seed)
+
+    def ref_cutoff(amp):
+        xlb = math.cosh(math.acosh(amp) / degree)
+        return (2.0 * lower + upper * (xlb - 1.0)) / (1.0 + xlb)
+
+    cutoff = ref_cutoff(1e3)
+    cap_cut = ref_cutoff(amplification) if bounds == "ritz" else None
+    X = random_block(n, width, seed)
+    for it in range(1, maxiter + 1):
+        Y = X if upper == cutoff else chebyshev_filter_window(ops.apply, X, degree, cutoff, upper)
+        for _ in range(2):
+            info, Y, _ = cholesky_qr(Y)
+            if info != 0:
+                raise RuntimeError("ChebyshevSolver: Cholesky QR failed during filtering.")
+        W = ops.apply(Y)
+        H = Y.T @ W
+        theta, Q = np.linalg.eigh(0.5 * (H + H.T))
+        X = Y @ Q
+        AX = W @ Q
+        rel = np.linalg.norm(AX - X * theta, axis=0) / ((1.0 + np.abs(theta)) *
+                                                         np.linalg.norm(X, axis=0))
+        if rel[:nev].max() <= tol or it == maxiter:
+            return SolveResult(sign * theta[:nev], X[:, :nev], rel[:nev], it,
+                               0 if rel[:nev].max() <= tol else 1)
+        if cap_cut is not None:
+            cutoff = min(theta[-1], cap_cut)
+    raise RuntimeError("grouped Chebyshev: unreachable")
+
+
 class NumpyChebyshevOps:
     """Operator applications of the Chebyshev loop with SciPy/NumPy (the parity path)."""
 

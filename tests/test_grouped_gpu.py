@@ -173,3 +173,24 @@ def test_grouped_mixed_precision():
     alone, _ = grouped_chebyshev(mats[:1], o[:1])
     assert np.array_equal(alone[0]["eigenvalues"], out[0]["eigenvalues"])
     assert alone[0]["iterations"] == out[0]["iterations"]
+
+
+def test_grouped_matches_oracle_member():
+    """Each member against the oracle's restatement of the engine's per-member cycle
+    (oracle.grouped_chebyshev_member: the reference's seeded start block, Lanczos bounds,
+    filter, Cholesky QR twice, Rayleigh-Ritz, residuals): same cycle count, eigenvalues
+    to 1e-9 relative."""
+    from fasteig_b200 import grouped_chebyshev
+    from oracle import oracle as O
+    specs = [(12, "star1", 8, "SR"), (11, "star2", 12, "SR"), (12, "star2", 8, "LR")]
+    Hs = [problem(s, st, 70 + i) for i, (s, st, _, _) in enumerate(specs)]
+    out, _ = grouped_chebyshev([csr(H) for H in Hs],
+                               [opts(H.n, nev, which=w) for H, (_, _, nev, w) in zip(Hs, specs)])
+    for H, (_, _, nev, w), r in zip(Hs, specs, out):
+        A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
+        ref = O.grouped_chebyshev_member(A, nev, degree=10, tol=1e-8, maxiter=600,
+                                         which=w.lower(), seed=3, bounds="ritz",
+                                         amplification=1e6)
+        assert abs(r["iterations"] - ref.iterations) <= 1, (r["iterations"], ref.iterations)
+        np.testing.assert_allclose(r["eigenvalues"], ref.eigenvalues, rtol=1e-9, atol=1e-11)
+        assert np.all(r["residual_norms"] <= 1e-8)

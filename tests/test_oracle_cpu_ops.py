@@ -57,3 +57,20 @@ def test_cycles_generator_yields_every_cycle(wells10):
         progs.append((p.iteration, p.converged, p.result is not None))
     assert progs[-1][1] and progs[-1][2]
     assert [i for i, _, _ in progs] == list(range(1, len(progs) + 1))
+
+
+@pytest.mark.parametrize("which", ["sr", "lr"])
+def test_oracle_grouped_member_against_dense(which):
+    """The oracle's restatement of one grouped Chebyshev member (whole-subspace filter,
+    Cholesky QR twice, Rayleigh-Ritz) reaches tol with the dense spectrum's pairs."""
+    from fasteig_b200 import matrices as M
+    from oracle import oracle as O
+    H = M.laplacian_wells(11, wells=6, seed=9, stencil="star2")
+    A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
+    r = O.grouped_chebyshev_member(A, 10, degree=10, tol=1e-8, maxiter=400, which=which,
+                                   seed=3, bounds="ritz", amplification=1e6)
+    w = np.linalg.eigvalsh(A.scipy().toarray())
+    exp = w[:10] if which == "sr" else w[::-1][:10]
+    assert r.status == 0
+    np.testing.assert_allclose(r.eigenvalues, exp, rtol=1e-10, atol=1e-10)
+    assert np.all(r.residual_norms <= 1e-8)
