@@ -1282,26 +1282,7 @@ void finish_results(Context& ctx, SmallState& sm, const Csr& A, const Csr* B, co
 // Reference selection order (lanczos_select_ritz_indices,
 // src/core/RitzExtraction.cpp:162-179; sort_indices, include/fasteig_solver.hpp:58-82).
 std::vector<int32_t> select_indices(const std::vector<double>& w, const std::string& which) {
-  const int m = static_cast<int>(w.size());
-  std::vector<int32_t> idx(m);
-  for (int i = 0; i < m; ++i) idx[i] = i;
-  if (which == "be") {
-    int pos = 0;
-    for (int i = 0; i < m / 2; ++i) {
-      idx[pos++] = m - 1 - i;
-      idx[pos++] = i;
-    }
-    if (m % 2 == 1) idx[pos] = m / 2;
-    return idx;
-  }
-  auto key = [&](int i) {
-    if (which == "sr") return w[i];
-    if (which == "lr") return -w[i];
-    if (which == "sm") return std::fabs(w[i]);
-    return -std::fabs(w[i]);  // lm
-  };
-  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return key(a) < key(b); });
-  return idx;
+  return ritz_order(w, which);
 }
 
 // Device Rayleigh-Ritz (extract_projected_ritz_pairs, src/core/RitzExtraction.cpp:65-141):

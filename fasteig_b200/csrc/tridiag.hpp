@@ -152,6 +152,33 @@ struct TridiagEig {
   }
 };
 
+// Reference selection order of Ritz values w (ascending) by `which`
+// (lanczos_select_ritz_indices, src/core/RitzExtraction.cpp:162-179; sort_indices,
+// include/fasteig_solver.hpp:58-82): sr, lr, sm, lm by a stable sort on the key, be
+// alternating from the largest and the smallest.
+inline std::vector<int32_t> ritz_order(const std::vector<double>& w, const std::string& which) {
+  const int m = static_cast<int>(w.size());
+  std::vector<int32_t> idx(m);
+  for (int i = 0; i < m; ++i) idx[i] = i;
+  if (which == "be") {
+    int pos = 0;
+    for (int i = 0; i < m / 2; ++i) {
+      idx[pos++] = m - 1 - i;
+      idx[pos++] = i;
+    }
+    if (m % 2 == 1) idx[pos] = m / 2;
+    return idx;
+  }
+  auto key = [&](int i) {
+    if (which == "sr") return w[i];
+    if (which == "lr") return -w[i];
+    if (which == "sm") return std::fabs(w[i]);
+    return -std::fabs(w[i]);  // lm
+  };
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return key(a) < key(b); });
+  return idx;
+}
+
 // Eigenvalue indices (ascending order) that a selection of `nev` pairs by `which`
 // (sr, lr, sm, lm, be) can draw from: both ends for lr/lm/be and sr, the window
 // around zero for sm; all of them when the window covers the spectrum.

@@ -30,5 +30,20 @@ int main() {
     for (double v : x) std::printf("%.17g ", v);
     std::printf("\n");
   }
+  // The snapshot's shortcut: selecting nev pairs among the candidate eigenvalues only
+  // must give the selection over all of them. One line per (which, nev): 1 if equal.
+  for (const char* which : {"sr", "lr", "sm", "lm", "be"}) {
+    for (int nev : {1, 3, std::max(1, m / 3)}) {
+      if (nev > m) continue;
+      const std::vector<int32_t> full = fe::ritz_order(w, which);
+      const std::vector<int> cand = fe::tridiag_candidates(t, nev, which);
+      std::vector<double> cw;
+      for (int c : cand) cw.push_back(t.eigenvalue(c));
+      const std::vector<int32_t> part = fe::ritz_order(cw, which);
+      bool same = true;
+      for (int j = 0; j < nev; ++j) same = same && cw[part[j]] == w[full[j]];
+      std::printf("select %s %d %d\n", which, nev, same ? 1 : 0);
+    }
+  }
   return 0;
 }

@@ -3,7 +3,9 @@ bisection on Sturm counts, inverse iteration with cluster reorthogonalization),
 compiled with g++ through tests/cpp/tridiag_check.cpp and checked against
 scipy.linalg.eigh_tridiagonal: eigenvalues to 1e-13 ||T||, residuals of the vectors to
 1e-12 ||T||, orthonormality to 1e-10, on random, graded, split (zero coupling),
-Wilkinson (close pairs) and Lanczos (the oracle's chain on SiO) tridiagonals."""
+Wilkinson (close pairs) and Lanczos (the oracle's chain on SiO) tridiagonals; and the
+snapshot's shortcut (bisection only for the eigenvalues a selection of nev pairs by
+sr/lr/sm/lm/be can draw from) selects what the full spectrum selects."""
 import shutil
 import subprocess
 from pathlib import Path
@@ -34,6 +36,8 @@ def run(exe, d, e):
     lines = r.stdout.split("\n")
     w = np.array([float(x) for x in lines[:m]])
     V = np.array([[float(x) for x in ln.split()] for ln in lines[m:2 * m]]).T
+    sel = [ln.split() for ln in lines[2 * m:] if ln.startswith("select")]
+    assert sel and all(s[3] == "1" for s in sel), [s for s in sel if s[3] != "1"]
     return w, V
 
 
