@@ -124,3 +124,24 @@ def test_chebyshev_hard_locking_extension_against_dense(which):
     soft = O.chebyshev_solve(A, 24, degree=16, tol=1e-8, maxiter=300, seed=1, block=32,
                              bounds="ritz", amplification=1e6, which=which)
     assert res.iterations <= soft.iterations + 1
+
+
+@pytest.mark.parametrize("which", ["lr", "sm", "lm", "be"])
+def test_oracle_lanczos_selections_against_dense(which):
+    """The oracle's LanczosSolver chain selects the reference's order (SR/LR/SM/LM/BE)
+    and converges to the dense spectrum's pairs."""
+    import scipy.sparse as sp
+    from fasteig_b200 import matrices as M
+    H = M.laplacian_uniform_potential(9, dim=3, seed=5)
+    A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
+    shifted = sp.csr_matrix(A.scipy() - 6.0 * sp.identity(H.n))  # spectrum on both sides of 0
+    dense = shifted.toarray()
+    S = O.Csr(H.n, H.n, shifted.indptr.astype(np.int32), shifted.indices.astype(np.int32),
+              shifted.data)
+    res = O.lanczos_solve(S, 4, tol=1e-9, maxiter=H.n, which=which, seed=2)
+    w = np.linalg.eigvalsh(dense)
+    order = {"lr": np.argsort(-w, kind="stable"), "sm": np.argsort(np.abs(w), kind="stable"),
+             "lm": np.argsort(-np.abs(w), kind="stable"),
+             "be": np.array([len(w) - 1, 0, len(w) - 2, 1])}[which]
+    np.testing.assert_allclose(res.eigenvalues, w[order[:4]], rtol=1e-8, atol=1e-9)
+    assert np.all(res.residual_norms <= 1e-9)
