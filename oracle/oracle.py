@@ -1205,6 +1205,82 @@ def block_krylov_schur_solve(A: Csr, nev: int, blksize: int, tol: float = 1e-8,
     raise RuntimeError("BlockKrylovSchurSolver: unreachable solve termination.")
 
 
+def block_lanczos_solve(A: Csr, nev: int, blksize: int, tol: float = 1e-8,
+                        maxiter: int = 1000, which: str = "sr", seed: int = 1) -> SolveResult:
+    """BlockLanczosSolver::solve (src/BlockLanczosSolver.cpp:24-176) for standard problems:
+    one block Krylov chain (BlockKrylovSubspace, src/core/KrylovSubspace.cpp:261-437: the
+    seeded random block, block apply, two-pass block Gram-Schmidt against the active
+    basis, complete_block_qr of the residual block) of up to maxiter blocks with no
+    restart; after every block from iter * blksize >= nev on, the block-tridiagonal
+    projection is diagonalized and the chain stops when every wanted estimate
+    ||beta y_last|| / (1 + |theta|) is below tol; the pairs are then formed from the
+    basis and their residuals evaluated (evaluate_ritz_pairs)."""
+    n = A.rows
+    which = which.lower()
+    b = int(blksize)
+    if n <= 0:
+        raise ValueError("BlockLanczosSolver: n must be > 0.")
+    if nev <= 0:
+        raise ValueError("BlockLanczosSolver: nev must be > 0.")
+    if maxiter <= 0:
+        raise ValueError("BlockLanczosSolver: maxiter must be > 0.")
+    if b <= 0:
+        raise ValueError("BlockLanczosSolver: blksize must be > 0.")
+    if b > n or nev > n:
+        raise ValueError("BlockLanczosSolver: blksize and nev must be <= n.")
+    max_blocks = int(maxiter)
+    if max_blocks * b < nev:
+        raise ValueError("BlockLanczosSolver: need maxiter*blksize >= nev.")
+    if which not in ("sr", "lr", "sm", "lm", "be"):
+        raise ValueError("BlockLanczosSolver: invalid which option.")
+    Hs = A.scipy()
+    cap_blocks = min(max_blocks, 1 + (n - 1) // b, 32) + 1  # grown on demand
+
+    basis = np.zeros((n, cap_blocks * b))
+    _, Q0, _ = complete_block_qr(basis, 0, random_block(n, b, seed), seed, 0.0)
+    basis[:, :b] = Q0
+    T = np.zeros((cap_blocks * b, cap_blocks * b))
+    beta = np.zeros((b, b))
+
+    def snapshot(m):
+        w, Z = np.linalg.eigh(T[:m, :m])
+        tail = 1 + (m - 1) % b
+        last = np.zeros((b, m))
+        last[:tail] = Z[m - tail:, :]
+        idx = select_ritz_indices(w, which)[:min(nev, m)]
+        rel = np.linalg.norm(beta @ last[:, idx], axis=0) / (1.0 + np.abs(w[idx]))
+        return w[idx], rel, Z[:, idx]
+
+    for it in range(1, max_blocks + 1):
+        if (it + 1) * b > basis.shape[1]:
+            grow = basis.shape[1]
+            basis = np.concatenate([basis, np.zeros((n, grow))], axis=1)
+            T2 = np.zeros((T.shape[0] + grow, T.shape[1] + grow))
+            T2[:T.shape[0], :T.shape[1]] = T
+            T = T2
+        Z = Hs @ basis[:, (it - 1) * b:it * b]
+        active = min(n, it * b)
+        _, Rres, H = block_gram_schmidt(basis, active, Z)
+        width = 1 + (active - 1) % b
+        diag = np.zeros((b, b))
+        diag[:width, :width] = H[H.shape[0] - width:, :width]
+        scale = float(np.linalg.norm(np.linalg.norm(Z, axis=0)))
+        _, Qn, coupling = complete_block_qr(basis, active, Rres, seed + it * b, scale)
+        basis[:, it * b:(it + 1) * b] = Qn
+        row, nrow = (it - 1) * b, it * b
+        T[row:row + b, row:row + b] = diag
+        T[nrow:nrow + b, row:row + b] = coupling
+        T[row:row + b, nrow:nrow + b] = coupling.T
+        beta = coupling
+        if it * b < nev and it < max_blocks:
+            continue
+        lam, rel, C = snapshot(active)
+        if rel.size and rel.max() < tol or it == max_blocks or active == n:
+            Y, res = evaluate_ritz_pairs(A, None, basis, active, lam, C)
+            return SolveResult(lam.copy(), Y, res, it, 0)
+    raise RuntimeError("BlockLanczosSolver: unreachable solve termination.")
+
+
 # --------------------------------------------------------------------------
 # Reference spectra: tests/scripts/ref_eigs.py (parse) and run_case.py (select)
 # --------------------------------------------------------------------------

@@ -2,7 +2,8 @@
 
 * std::mt19937 + uniform_real_distribution(-1,1) (src/core/Executor.cpp:20-62)
   against the g++ build of oracle/rng_golden.cpp (tests/golden/mt19937.json).
-* SiO.mtx, SR k=5, for Chebyshev, LOBPCG, Davidson, Krylov-Schur and Lanczos against the
+* SiO.mtx, SR k=5, for Chebyshev, LOBPCG, Davidson, Krylov-Schur, Lanczos and block
+  Lanczos against the
   ScaLAPACK spectrum tests/reference/SiO.out.121mpi, with the reference
   harness's rule |l - l_ref| <= 1e-10 + 1e-10 |l_ref| and residual <= 1e-8
   (tests/scripts/run_case.py:27-33,246-260; deck seed 1, tol 1e-8, maxiter 2000).
@@ -61,7 +62,7 @@ def _check_sr5(res, spectra, A):
 
 
 @pytest.mark.parametrize("solver", ["chebyshev", "lobpcg", "davidson", "krylovschur",
-                                    "lanczos"])
+                                    "lanczos", "blocklanczos"])
 def test_sio_sr5_against_scalapack_spectrum(solver, sio, spectra):
     if solver == "chebyshev":
         res = O.chebyshev_solve(sio, 5, degree=10, **SR5)
@@ -71,9 +72,12 @@ def test_sio_sr5_against_scalapack_spectrum(solver, sio, spectra):
         res = O.davidson_solve(sio, 5, **SR5)
     elif solver == "krylovschur":
         res = O.krylov_schur_solve(sio, 5, maxdim=40, **SR5)
-    else:
+    elif solver == "lanczos":
         # LanczosSolver: one chain, maxiter <= n (the deck's 2000 fits n = 33,401)
         res = O.lanczos_solve(sio, 5, **SR5)
+    else:
+        # BlockLanczosSolver with the deck's blksize 10
+        res = O.block_lanczos_solve(sio, 5, 10, **SR5)
     _check_sr5(res, spectra, sio)
 
 
