@@ -361,8 +361,12 @@ def grouped_chebyshev(problems, opts, want_vectors: bool = False):
 class Server:
     """Request server over ``fe_server_*``: requests (operator + options) are
     admitted as worker slots and device memory free up, run concurrently on their
-    own streams, and are collected with ``wait``. Keep each request's CsrMatrix
-    alive until it is collected."""
+    own streams, and are collected with ``wait``. Chebyshev requests whose options
+    set ``group=1`` (FP64 or mixed precision, soft locking) run instead in the grouped
+    lane of their subspace width and degree: they join the lane's group between
+    filter cycles and advance with the other admitted members in grouped kernels
+    (``stats()`` reports the lanes' counters). Keep each request's CsrMatrix alive
+    until it is collected."""
 
     PENDING = 1
 
