@@ -84,6 +84,35 @@ def random_vector(size: int, seed: int = 1) -> np.ndarray:
     return mt19937_uniform(size, seed)
 
 
+def leading_block(v0: np.ndarray, n: int, b: int, solver: str) -> np.ndarray:
+    """The block solvers' warm start: v0.leftCols(blksize), which must exist
+    (src/BlockLanczosSolver.cpp:73-79, src/BlockKrylovSchurSolver.cpp:91-99)."""
+    v0 = np.asarray(v0, dtype=np.float64)
+    if v0.ndim == 1:
+        v0 = v0[:, None]
+    if v0.shape[0] != n or v0.shape[1] < b:
+        raise ValueError(f"{solver}: v0 must have shape n x at least blksize.")
+    return v0[:, :b].copy()
+
+
+def warm_start(X: np.ndarray, v0: Optional[np.ndarray], max_cols: int, solver: str) -> np.ndarray:
+    """The solvers' warm start over their seeded random block (fasteig_options::v0; e.g.
+    src/ChebyshevSolver.cpp:96-103, src/LOBPCGSolver.cpp:49-56,
+    src/DavidsonSolver.cpp:60-71): the first min(max_cols, v0 columns) columns of X are
+    v0's."""
+    if v0 is None:
+        return X
+    v0 = np.asarray(v0, dtype=np.float64)
+    if v0.ndim == 1:
+        v0 = v0[:, None]
+    if v0.shape[0] != X.shape[0]:
+        raise ValueError(f"{solver}: v0 row count does not match the problem.")
+    k = min(max_cols, v0.shape[1])
+    X = X.copy()
+    X[:, :k] = v0[:, :k]
+    return X
+
+
 # --------------------------------------------------------------------------
 # CSR matrices: include/core/CsrMatrix.hpp:18-27, src/core/CsrMatrix.cpp
 # --------------------------------------------------------------------------
@@ -677,12 +706,13 @@ def chebyshev_solve(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
                     maxiter: int = 1000, which: str = "sr", seed: int = 1,
                     block: Optional[int] = None, record_history: bool = False,
                     bounds: str = "reference", amplification: float = math.inf,
-                    locking: str = "soft", ops=None) -> SolveResult:
+                    locking: str = "soft", ops=None,
+                    v0: Optional[np.ndarray] = None) -> SolveResult:
     """ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221); runs
     chebyshev_cycles to the end and returns its result."""
     prog = None
     for prog in chebyshev_cycles(A, nev, degree, tol, maxiter, which, seed, block,
-                                 record_history, bounds, amplification, locking, ops):
+                                 record_history, bounds, amplification, locking, ops, v0):
         pass
     return prog.result
 
@@ -691,7 +721,7 @@ def chebyshev_cycles(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
                      maxiter: int = 1000, which: str = "sr", seed: int = 1,
                      block: Optional[int] = None, record_history: bool = False,
                      bounds: str = "reference", amplification: float = math.inf,
-                     locking: str = "soft", ops=None):
+                     locking: str = "soft", ops=None, v0: Optional[np.ndarray] = None):
     """ChebyshevSolver::solve (src/ChebyshevSolver.cpp:67-221), one filter cycle per
     ``next()``: the first call also runs the set-up (random block, Cholesky QR,
     Lanczos bounds). Yields a ChebyshevProgress after every cycle; the last one
@@ -723,7 +753,7 @@ def chebyshev_cycles(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
     H_apply = ops.apply
     norms = getattr(ops, "residual_norms", None)
     capacity = nev + min(nev, n - nev) if block is None else max(nev, min(block, n))
-    vectors = random_block(n, capacity, seed)
+    vectors = warm_start(random_block(n, capacity, seed), v0, nev, "ChebyshevSolver")
     info, vectors, _ = cholesky_qr(vectors)
     if info != 0:
         raise RuntimeError("ChebyshevSolver: initial Cholesky QR failed.")
@@ -819,7 +849,8 @@ def chebyshev_cycles(A: Csr, nev: int, degree: int = 10, tol: float = 1e-8,
 
 
 def lobpcg_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
-                 which: str = "sr", seed: int = 1) -> SolveResult:
+                 which: str = "sr", seed: int = 1,
+                 v0: Optional[np.ndarray] = None) -> SolveResult:
     """LOBPCGSolver::solve (src/LOBPCGSolver.cpp:25-174): unpreconditioned LOBPCG,
     block width nev, soft locking."""
     n = A.rows
@@ -831,7 +862,7 @@ def lobpcg_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
     sign = -1.0 if which == "lr" else 1.0
     Hs = A.scipy()
     H_apply = (lambda X: sign * (Hs @ X))
-    X = random_block(n, nev, seed)
+    X = warm_start(random_block(n, nev, seed), v0, nev, "LOBPCGSolver")
     _, X, _ = householder_qr(X)
     capacity = min(n, 3 * nev)
     AX = H_apply(X)
@@ -876,7 +907,8 @@ def lobpcg_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
 
 
 def davidson_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
-                   which: str = "sr", seed: int = 1, maxblks: int = 10) -> SolveResult:
+                   which: str = "sr", seed: int = 1, maxblks: int = 10,
+                   v0: Optional[np.ndarray] = None) -> SolveResult:
     """DavidsonSolver::solve (src/DavidsonSolver.cpp:27-264): block Davidson with thick
     restart and unpreconditioned corrections; locktol = min(1e-5, tol) (:126)."""
     n = A.rows
@@ -885,7 +917,7 @@ def davidson_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
         raise ValueError("DavidsonSolver: nev must be in [1,n].")
     Hs = A.scipy()
     H_apply = (lambda X: Hs @ X)
-    V0 = random_block(n, nev, seed)
+    V0 = warm_start(random_block(n, nev, seed), v0, nev, "DavidsonSolver")
     info, V0, _ = cholesky_qr(V0)
     if info != 0:
         raise RuntimeError("DavidsonSolver: initial Cholesky QR failed.")
@@ -933,7 +965,7 @@ def davidson_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
 
 def krylov_schur_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
                        which: str = "sr", seed: int = 1, maxdim: int = 0,
-                       B: Optional[Csr] = None) -> SolveResult:
+                       B: Optional[Csr] = None, v0: Optional[np.ndarray] = None) -> SolveResult:
     """KrylovSchurSolver::solve (src/KrylovSchurSolver.cpp:28-160), standard problems
     (B is None) and the B-metric Lanczos of src/core/KrylovSubspace.cpp:162-178 with an
     explicit B^{-1}A operator for generalized problems (the reference's cuDSS/LU
@@ -951,7 +983,9 @@ def krylov_schur_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
         Bs = B.scipy()
         A_apply = (lambda v: lu.solve(Hs @ v))
         B_apply = (lambda v: Bs @ v)
-    lz = _Lanczos(A_apply, random_vector(n, seed), m, seed, B_apply)
+    start = random_vector(n, seed) if v0 is None else \
+        warm_start(np.zeros((n, 1)), v0, 1, "KrylovSchurSolver")[:, 0]  # v0.col(0) (:68-70)
+    lz = _Lanczos(A_apply, start, m, seed, B_apply)
     for col in range(m):
         lz.step(col)
     for it in range(1, maxiter + 1):
@@ -995,7 +1029,7 @@ def krylov_schur_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
 
 def lanczos_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
                   which: str = "sr", seed: int = 1, print_every: int = 0,
-                  B: Optional[Csr] = None) -> SolveResult:
+                  B: Optional[Csr] = None, v0: Optional[np.ndarray] = None) -> SolveResult:
     """LanczosSolver::solve (src/LanczosSolver.cpp:29-163): one scalar Lanczos chain of up
     to maxiter vectors, no restart; from nev vectors on, every check_every-th step
     (print_every, else 5) and at maxiter the projected tridiagonal is diagonalized and
@@ -1022,7 +1056,9 @@ def lanczos_solve(A: Csr, nev: int, tol: float = 1e-8, maxiter: int = 1000,
         Bs = B.scipy()
         A_apply = (lambda v: lu.solve(Hs @ v))
         B_apply = (lambda v: Bs @ v)
-    lz = _Lanczos(A_apply, random_vector(n, seed), maxiter, seed, B_apply)
+    start = random_vector(n, seed) if v0 is None else \
+        warm_start(np.zeros((n, 1)), v0, 1, "LanczosSolver")[:, 0]  # v0.col(0)
+    lz = _Lanczos(A_apply, start, maxiter, seed, B_apply)
     check_every = print_every if print_every > 0 else 5
     breakdown = False
     for it in range(maxiter):
@@ -1112,7 +1148,7 @@ def complete_block_qr(basis: np.ndarray, active_cols: int, source: np.ndarray, s
 
 def block_krylov_schur_solve(A: Csr, nev: int, blksize: int, tol: float = 1e-8,
                              maxiter: int = 1000, which: str = "sr", seed: int = 1,
-                             maxdim: int = 0) -> SolveResult:
+                             maxdim: int = 0, v0: Optional[np.ndarray] = None) -> SolveResult:
     """BlockKrylovSchurSolver::solve (src/BlockKrylovSchurSolver.cpp:26-215) for standard
     problems: BlockKrylovSubspace expansion (src/core/KrylovSubspace.cpp:261-437: block
     apply, two-pass block Gram-Schmidt, complete_block_qr of the residual block),
@@ -1146,7 +1182,8 @@ def block_krylov_schur_solve(A: Csr, nev: int, blksize: int, tol: float = 1e-8,
     snapshot_count = max(nev, retained_dim)
     Hs = A.scipy()
     basis = np.zeros((n, projection_dim))
-    _, Q0, _ = complete_block_qr(basis, 0, random_block(n, b, seed), seed, 0.0)
+    first = random_block(n, b, seed) if v0 is None else leading_block(v0, n, b, "BlockKrylovSchurSolver")
+    _, Q0, _ = complete_block_qr(basis, 0, first, seed, 0.0)
     basis[:, :b] = Q0
     T = np.zeros((projection_dim, projection_dim))
     beta = np.zeros((b, b))
@@ -1206,7 +1243,8 @@ def block_krylov_schur_solve(A: Csr, nev: int, blksize: int, tol: float = 1e-8,
 
 
 def block_lanczos_solve(A: Csr, nev: int, blksize: int, tol: float = 1e-8,
-                        maxiter: int = 1000, which: str = "sr", seed: int = 1) -> SolveResult:
+                        maxiter: int = 1000, which: str = "sr", seed: int = 1,
+                        v0: Optional[np.ndarray] = None) -> SolveResult:
     """BlockLanczosSolver::solve (src/BlockLanczosSolver.cpp:24-176) for standard problems:
     one block Krylov chain (BlockKrylovSubspace, src/core/KrylovSubspace.cpp:261-437: the
     seeded random block, block apply, two-pass block Gram-Schmidt against the active
@@ -1237,7 +1275,8 @@ def block_lanczos_solve(A: Csr, nev: int, blksize: int, tol: float = 1e-8,
     cap_blocks = min(max_blocks, 1 + (n - 1) // b, 32) + 1  # grown on demand
 
     basis = np.zeros((n, cap_blocks * b))
-    _, Q0, _ = complete_block_qr(basis, 0, random_block(n, b, seed), seed, 0.0)
+    first = random_block(n, b, seed) if v0 is None else leading_block(v0, n, b, "BlockLanczosSolver")
+    _, Q0, _ = complete_block_qr(basis, 0, first, seed, 0.0)
     basis[:, :b] = Q0
     T = np.zeros((cap_blocks * b, cap_blocks * b))
     beta = np.zeros((b, b))

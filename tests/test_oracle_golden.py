@@ -149,3 +149,30 @@ def test_oracle_lanczos_selections_against_dense(which):
              "be": np.array([len(w) - 1, 0, len(w) - 2, 1])}[which]
     np.testing.assert_allclose(res.eigenvalues, w[order[:4]], rtol=1e-8, atol=1e-9)
     assert np.all(res.residual_norms <= 1e-9)
+
+
+@pytest.mark.parametrize("solver", ["chebyshev", "lobpcg", "davidson", "krylovschur",
+                                    "lanczos", "blocklanczos", "blockkrylovschur"])
+def test_oracle_warm_start(solver):
+    """fasteig_options::v0 semantics in the oracle: restarted from its own converged
+    vectors a solver returns the same pairs in at most as many iterations; a v0 with the
+    wrong row count is rejected as the reference rejects it."""
+    from fasteig_b200 import matrices as M
+    H = M.laplacian_wells(9, wells=4, seed=3)
+    A = O.Csr(H.n, H.n, H.rowptr, H.colind, H.values)
+    kw = dict(tol=1e-9, maxiter=400, seed=1)
+    run = {"chebyshev": lambda **x: O.chebyshev_solve(A, 5, degree=8, **kw, **x),
+           "lobpcg": lambda **x: O.lobpcg_solve(A, 5, **kw, **x),
+           "davidson": lambda **x: O.davidson_solve(A, 5, **kw, **x),
+           "krylovschur": lambda **x: O.krylov_schur_solve(A, 5, maxdim=30, **kw, **x),
+           "lanczos": lambda **x: O.lanczos_solve(A, 5, **kw, **x),
+           "blocklanczos": lambda **x: O.block_lanczos_solve(A, 5, 5, **kw, **x),
+           "blockkrylovschur": lambda **x: O.block_krylov_schur_solve(A, 5, 5, maxdim=30, **kw,
+                                                                     **x)}[solver]
+    cold = run()
+    warm = run(v0=cold.eigenvectors)
+    np.testing.assert_allclose(warm.eigenvalues, cold.eigenvalues, rtol=1e-9, atol=1e-10)
+    assert np.all(warm.residual_norms <= 1e-9)
+    assert warm.iterations <= cold.iterations
+    with pytest.raises(ValueError, match="v0"):
+        run(v0=np.ones((H.n - 1, 5)))
