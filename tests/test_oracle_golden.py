@@ -176,3 +176,10 @@ def test_oracle_warm_start(solver):
     assert warm.iterations <= cold.iterations
     with pytest.raises(ValueError, match="v0"):
         run(v0=np.ones((H.n - 1, 5)))
+
+
+def test_sio_lr5_block_lanczos(sio, spectra):
+    res = O.block_lanczos_solve(sio, 5, 10, which="lr", **SR5)
+    exp = spectra["SiO"]["highest"][::-1][:5]
+    assert all(O.eigenvalue_check(res.eigenvalues, exp)), (res.eigenvalues, exp)
+    assert np.all(res.residual_norms <= 1e-8)
